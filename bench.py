@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark: bundle-adjustment time to 1e-6 relative cost on one B200.
+
+A step is one Levenberg–Marquardt solve of the BAL-shaped workload (default
+bal1k: 1,000 cameras, 200,000 points, ~1.1M observations) from its initial
+estimates until the accepted cost is within 1e-6 relative of the f64 oracle's
+final cost (tests/golden/<workload>_oracle.json). `value` is the device time
+of that solve with all inputs resident in HBM (CUDA events on the library
+stream); `e2e` is the same metric through the public C ABI from host arrays
+(problem upload, solve, parameter read-back inside the timed region).
+
+Forms: `fast` = FP32 bulk storage and Krylov vectors with FP64 dots, cost and
+outer refinement, preconditioned by the exact 9x9 diagonal blocks of the
+reduced system; `f64` = the reference arithmetic (f64 everywhere, block-Jacobi
+on the B blocks as in fagra's Schur backend). Multi-GPU runs are independent
+replicas (the path has no exchange step); value = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+REL = 1e-6
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
+    ap.add_argument("--workload", default="bal1k")
+    ap.add_argument("--forms", default="fast,f64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def gold(workload: str) -> dict:
+    return json.loads((ROOT / "tests" / "golden" / f"{workload}_oracle.json").read_text())
+
+
+def target_counts(g: dict) -> tuple[int, int, float]:
+    """(linearizations, CG iterations, seconds) the oracle needed to first reach the target."""
+    target = g["final_cost"] * (1 + REL)
+    for i, c in enumerate(g["accepted_costs"]):
+        if c <= target:
+            return i + 2, g["accepted_cg"][i], g["accepted_seconds"][i]
+    return g["linearizations"], g["cg_iterations"], g["seconds"]
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_sample(data, g, cg_sample: int = 4) -> dict:
+    """Times the oracle (sequential f64 restatement, 1 core) on a bounded
+    sample of the workload: one cost evaluation, one linearization with damping
+    preparation, and `cg_sample` CG iterations of one damped solve. The
+    time-to-target estimate scales these by the oracle's own counts."""
+    import oracle
+    bal = oracle.Bal.from_data(data)
+    s = oracle.Schur(9 * data.num_cameras, 9, 3)
+    s.prepare(bal.dimension())
+    t0 = time.perf_counter()
+    bal.cost()
+    t_cost = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bal.linearize(s)
+    s.prepare_damping(1e-6)
+    t_lin = time.perf_counter() - t0
+    s.max_iterations = cg_sample
+    t0 = time.perf_counter()
+    s.solve_damped(1e-3)
+    t_cg = (time.perf_counter() - t0) / cg_sample
+    n_lin, n_cg, _ = target_counts(g)
+    attempts = g.get("solves", n_lin)
+    est = n_lin * t_lin + n_cg * t_cg + (attempts + 1) * t_cost
+    return dict(value=est, t_lin=t_lin, t_cg=t_cg, t_cost=t_cost, n_lin=n_lin, n_cg=n_cg,
+                sample=f"{data.name}: 1 cost + 1 linearization/damping prep + {cg_sample} CG iterations, "
+                       f"scaled by the oracle's {n_lin} linearizations and {n_cg} CG iterations to the target")
+
+
+# ------------------------------------------------------------------ GPU legs
+class Clocks:
+    """nvidia-smi clock/throttle sampler running during a timed region."""
+
+    def __init__(self, device: int):
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path.parent.mkdir(exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.send_signal(signal.SIGTERM)
+        self.proc.wait(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=mx, reasons=sorted(reasons),
+                    samples=len(sm))
+
+
+def run_gpu(args, rank: int, world: int, device: int):
+    import numpy as np
+    import torch
+    import fagra_b200 as fg
+    from fagra_b200 import synthetic, _lib
+    import ctypes as C
+
+    torch.cuda.set_device(device)
+    stream = torch.cuda.ExternalStream(fg.device_stream(device), device=device)
+    g = gold(args.workload)
+    target = g["final_cost"] * (1 + REL)
+    data = synthetic.generate(args.workload)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    def barrier():
+        if dist:
+            tdist.barrier()
+        torch.cuda.synchronize(device)
+
+    opts = fg.OptimizeOptions(50, 1e-8, 0.0, 0.0)
+    forms = {"fast": dict(precision="f32", preconditioner="schur_diagonal"),
+             "f64": dict(precision="f64", preconditioner="retained_blocks")}
+    results = {}
+    head = args.forms.split(",")[0]
+    problem = fg.BalProblem.from_data(data, device=device)
+    clocks_info = None
+    launches = None
+    for name in args.forms.split(","):
+        kw = forms[name]
+        backend = fg.Schur(9 * data.num_cameras, 9, 3, device=device, **kw)
+        lmo = fg.LmOptions().c()
+        oo = opts.c()
+
+        def step():
+            _lib.lib.fg_bal_restore_initial(problem._bal_handle)
+            rep, st = _lib.ReportC(), _lib.LmStatisticsC()
+            code = _lib.lib.fg_lm_solve_bal_to_cost(backend.handle, problem._bal_handle, C.byref(oo),
+                                                    C.byref(lmo), target, C.byref(rep), C.byref(st))
+            return code, rep, st
+
+        for _ in range(args.warmup):
+            step()
+        barrier()
+        if name == head:
+            clk = Clocks(device)
+            l0 = fg.kernel_launches()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        per = []
+        for _ in range(args.steps):
+            code, rep, st = step()
+            per.append(dict(code=code, termination=rep.termination, cost=st.cost, accepted=st.accepted_steps,
+                            rejected=st.rejected_steps, cg=st.linear_iterations, lin=st.linearizations))
+        ev[1].record(stream)
+        barrier()
+        secs = ev[0].elapsed_time(ev[1]) * 1e-3 / args.steps
+        if name == head:
+            launches = (fg.kernel_launches() - l0) // args.steps
+            clocks_info = clk.stop()
+        reached = all(p["termination"] == 5 for p in per)
+        results[name] = dict(seconds=secs, reached_target=reached, cg_iterations=per[-1]["cg"],
+                             linearizations=per[-1]["lin"], accepted=per[-1]["accepted"],
+                             rejected=per[-1]["rejected"], final_cost=per[-1]["cost"],
+                             rel_cost_error=(per[-1]["cost"] - g["final_cost"]) / g["final_cost"], **kw)
+        if name == head:
+            # roofline of the dominant kernel: the reduced-operator application
+            problem.linearize(backend)
+            backend.prepare_damping(1e-6)
+            sec_op, bytes_op = C.c_double(), C.c_double()
+            fg.errors.raise_for_status(_lib.lib.fg_schur_time_operator(backend.handle, 1e-3, 50, C.byref(sec_op),
+                                                                        C.byref(bytes_op)))
+            results[name]["operator"] = dict(seconds=sec_op.value, bytes=bytes_op.value)
+            head_backend = backend
+    # e2e: public C ABI from host arrays
+    e2e = None
+    if not args.no_e2e:
+        kw = forms[head]
+        backend = head_backend
+        cams = np.ascontiguousarray(data.cameras)
+        pts = np.ascontiguousarray(data.points)
+        oc, op, px = (np.ascontiguousarray(a) for a in (data.obs_camera, data.obs_point, data.obs_pixel))
+        h2d = cams.nbytes + pts.nbytes + oc.nbytes + op.nbytes + px.nbytes
+        d2h = cams.nbytes + pts.nbytes
+        lmo, oo = fg.LmOptions().c(), opts.c()
+
+        def e2e_step():
+            p = fg.BalProblem(cams, pts, oc, op, px, device=device)
+            rep, st = _lib.ReportC(), _lib.LmStatisticsC()
+            code = _lib.lib.fg_lm_solve_bal_to_cost(backend.handle, p._bal_handle, C.byref(oo), C.byref(lmo),
+                                                    target, C.byref(rep), C.byref(st))
+            c2, p2 = p.parameters()
+            p.close()
+            return code, rep.termination
+
+        e2e_step()
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        ev[1].record(stream)
+        barrier()
+        e2e = dict(value=ev[0].elapsed_time(ev[1]) * 1e-3 / args.steps, unit="s", h2d_bytes_per_step=h2d,
+                   d2h_bytes_per_step=d2h)
+    return data, g, results, head, clocks_info, launches, e2e
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from fagra_b200 import synthetic
+        g = gold(args.workload)
+        data = synthetic.generate(args.workload)
+        for _ in range(args.warmup):
+            cpu_sample(data, g, cg_sample=2)
+        t0 = time.perf_counter()
+        samples = [cpu_sample(data, g) for _ in range(args.steps)]
+        wall = (time.perf_counter() - t0) / args.steps
+        v = statistics.median(s["value"] for s in samples)
+        line = dict(metric=f"BA time to 1e-6 relative cost ({args.workload})", value=v, unit="s", n_gpus=args.gpus,
+                    steps=args.steps, warmup=args.warmup, ms_per_step=wall * 1e3, higher_is_better=False,
+                    scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+                    config=dict(workload=args.workload, form="f64 CPU restatement (oracle port), Schur-CG "
+                                "block-Jacobi on B, 1e-10 CG tolerance"),
+                    cpu_baseline=dict(value=v, unit="s", cores=1, kind="port", sample=samples[0]["sample"]),
+                    e2e=dict(value=v, unit="s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    data, g, results, head, clocks_info, launches, e2e = run_gpu(args, rank, world, local)
+    import torch
+    vals = {k: v["seconds"] for k, v in results.items()}
+    if world > 1:
+        import torch.distributed as tdist
+        t = torch.tensor([vals[head]] + ([e2e["value"]] if e2e else []), device=f"cuda:{local}", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        vals[head] = float(t[0])
+        if e2e:
+            e2e["value"] = float(t[1])
+    if rank == 0:
+        pk, src = peaks()
+        op = results[head].get("operator", {})
+        achieved = op["bytes"] / op["seconds"] / 1e9 if op.get("seconds") else None
+        traffic = None
+        tf = ROOT / "profiles" / "operator_traffic.json"
+        if tf.exists():
+            tj = json.loads(tf.read_text()).get(args.workload, {}).get(results[head]["precision"])
+            traffic = tj
+        line = dict(
+            metric=f"BA time to 1e-6 relative cost ({args.workload})", value=vals[head], unit="s", n_gpus=world,
+            steps=args.steps, warmup=args.warmup, ms_per_step=vals[head] * 1e3, higher_is_better=False,
+            scaling="weak", vs_baseline=None,
+            dtype="f32 bulk + f64 reductions" if results[head]["precision"] == "f32" else "f64",
+            data="synthetic",
+            config=dict(workload=f"{args.workload}: {data.num_cameras} cameras, {data.num_points} points, "
+                                 f"{data.num_observations} observations; LM until cost <= (1+1e-6) x f64 oracle "
+                                 f"cost {g['final_cost']:.6f}",
+                        form=head, parallelism=f"replicas x{world}",
+                        l2="inputs larger than L2 (cross blocks alone are 119 MB in f32, 238 MB in f64)"),
+            forms={k: {kk: vv for kk, vv in v.items() if kk != "operator"} for k, v in results.items()},
+            speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,
+            pcg_iterations=results[head]["cg_iterations"],
+            roofline=dict(bound="hbm", kernel="reduced operator (k_points + k_cams)", achieved=achieved, peak=pk,
+                          peak_source=src, unit="GB/s", frac=(achieved / pk) if achieved else None,
+                          algorithmic_bytes_per_launch=op.get("bytes"), seconds_per_launch=op.get("seconds"),
+                          traffic=traffic),
+            clocks=clocks_info, gpu_launches=launches, e2e=e2e)
+        if world == 1 and not args.no_cpu_baseline:
+            cs = cpu_sample(data, g)
+            line["cpu_baseline"] = dict(value=cs["value"], unit="s", cores=1, kind="port", sample=cs["sample"])
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,234 @@
+"""Python face of the device backend, shaped like fagra's Rust API.
+
+`Schur` mirrors `fagra::Schur` (src/schur.rs): public fields `max_iterations`,
+`relative_tolerance`, `collect_timings`; the LeastSquaresBackend methods
+(src/optimization.rs:131-169); `statistics()`, `diagnostics()`, `timings()`.
+Every numerical step runs in libfagra_b200.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Iterable, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib, size_t, ptrdiff_t, dptr
+from .errors import raise_for_status
+
+TERMINATIONS = {0: None, 1: "Converged", 2: "IterationLimit", 3: "NotPositiveDefinite", 4: "NonFinite"}
+PRECISIONS = {"f64": 0, "f32": 1}
+PRECONDITIONERS = {"retained_blocks": 0, "schur_diagonal": 1}
+
+
+@dataclass
+class DampedStep:
+    """src/optimization.rs:171-177 (delta copied out of the pinned mirror)."""
+    delta: np.ndarray
+    predicted_reduction: float
+
+
+@dataclass
+class LinearSolveWork:
+    solves: int
+    iterations: int
+
+
+@dataclass
+class SchurDiagnostics:
+    termination: Optional[str]
+    iterations: int
+    damping: float
+    estimated_relative_residual: Optional[float]
+    reduced_relative_residual: Optional[float]
+    scaled_relative_residual: Optional[float]
+    original_relative_residual: Optional[float]
+    refinements: int
+
+
+@dataclass
+class SchurTimings:
+    preparation: float
+    factorization: float
+    linear_solve: float
+    products: float
+    preconditioner: float
+    verification: float
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(dptr)
+
+
+class Schur:
+    """Device Schur-PCG backend: `Schur::new(retained, retained_width, eliminated_width)`."""
+
+    def __init__(self, retained_dimension: int, retained_block_width: int, eliminated_block_width: int, *,
+                 precision: str = "f64", preconditioner: str = "retained_blocks", device: int = 0):
+        o = _lib.SchurOptions()
+        lib.fg_schur_default_options(C.byref(o))
+        o.precision = PRECISIONS[precision]
+        o.preconditioner = PRECONDITIONERS[preconditioner]
+        o.device = device
+        self._opts = o
+        h = C.c_void_p()
+        raise_for_status(lib.fg_schur_create(retained_dimension, retained_block_width, eliminated_block_width,
+                                             C.byref(o), C.byref(h)))
+        self._h = h
+        self.retained = retained_dimension
+        self.widths = (retained_block_width, eliminated_block_width)
+        self.precision = precision
+        self.device = device
+
+    # ---- public fields
+    def _get(self, name):
+        return getattr(self._opts, name)
+
+    def _set(self, name, value):
+        setattr(self._opts, name, value)
+        raise_for_status(lib.fg_schur_set_options(self._h, C.byref(self._opts)))
+
+    max_iterations = property(lambda s: s._get("max_iterations"), lambda s, v: s._set("max_iterations", v))
+    relative_tolerance = property(lambda s: s._get("relative_tolerance"),
+                                  lambda s, v: s._set("relative_tolerance", v))
+    collect_timings = property(lambda s: bool(s._get("collect_timings")),
+                               lambda s, v: s._set("collect_timings", int(bool(v))))
+    preconditioner = property(lambda s: {v: k for k, v in PRECONDITIONERS.items()}[s._get("preconditioner")],
+                              lambda s, v: s._set("preconditioner", PRECONDITIONERS[v]))
+    refinement_inner_tolerance = property(lambda s: s._get("refinement_inner_tolerance"),
+                                          lambda s, v: s._set("refinement_inner_tolerance", v))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.fg_backend_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- LeastSquaresBackend
+    def prepare(self, dimension: int) -> None:
+        raise_for_status(lib.fg_backend_prepare(self._h, dimension))
+        self._dim = dimension
+
+    def clear(self) -> None:
+        raise_for_status(lib.fg_backend_clear(self._h))
+
+    def accumulate(self, residual: Sequence[float], jacobians: Iterable[Tuple[int, np.ndarray]]) -> None:
+        accumulate_into(self._h, residual, jacobians)
+
+    def gradient_norm(self) -> float:
+        out = C.c_double()
+        raise_for_status(lib.fg_backend_gradient_norm(self._h, C.byref(out)))
+        return out.value
+
+    def solve(self) -> np.ndarray:
+        p = dptr()
+        n = size_t()
+        raise_for_status(lib.fg_backend_solve(self._h, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0)
+
+    def prepare_damping(self, min_column_norm: float) -> None:
+        raise_for_status(lib.fg_backend_prepare_damping(self._h, min_column_norm))
+
+    def solve_damped(self, damping: float) -> DampedStep:
+        p = dptr()
+        n = size_t()
+        pred = C.c_double()
+        raise_for_status(lib.fg_backend_solve_damped(self._h, damping, C.byref(p), C.byref(n), C.byref(pred)))
+        delta = np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0)
+        return DampedStep(delta, pred.value)
+
+    def linear_solve_work(self) -> LinearSolveWork:
+        s, i, a = size_t(), size_t(), C.c_int()
+        raise_for_status(lib.fg_backend_linear_solve_work(self._h, C.byref(s), C.byref(i), C.byref(a)))
+        return LinearSolveWork(s.value, i.value)
+
+    statistics = linear_solve_work
+
+    def diagnostics(self) -> SchurDiagnostics:
+        d = _lib.SchurDiagnosticsC()
+        raise_for_status(lib.fg_schur_get_diagnostics(self._h, C.byref(d)))
+        opt = lambda flag, v: v if flag else None  # noqa: E731
+        return SchurDiagnostics(TERMINATIONS[d.termination], d.iterations, d.damping,
+                                opt(d.has_estimated, d.estimated_relative_residual),
+                                opt(d.has_reduced, d.reduced_relative_residual),
+                                opt(d.has_scaled, d.scaled_relative_residual),
+                                opt(d.has_original, d.original_relative_residual), d.refinements)
+
+    def timings(self) -> SchurTimings:
+        t = _lib.SchurTimingsC()
+        raise_for_status(lib.fg_schur_get_timings(self._h, C.byref(t)))
+        return SchurTimings(t.preparation, t.factorization, t.linear_solve, t.products, t.preconditioner,
+                            t.verification)
+
+    # ---- structure / model export (index maps in the reference layouts)
+    def structure(self) -> dict:
+        sizes = [size_t() for _ in range(6)]
+        raise_for_status(lib.fg_schur_structure_sizes(self._h, *[C.byref(s) for s in sizes]))
+        nb, ne, nv, nvar, rows, cols = (s.value for s in sizes)
+        b5 = np.zeros((max(nb, 1), 5), np.uint64)
+        e4 = np.zeros((max(ne, 1), 4), np.uint64)
+        own = np.zeros(max(cols, 1), np.uint64)
+        v3 = np.zeros((max(nvar, 1), 3), np.uint64)
+        u64 = C.POINTER(C.c_uint64)
+        raise_for_status(lib.fg_schur_export_structure(
+            self._h, b5.ctypes.data_as(u64), e4.ctypes.data_as(u64), own.ctypes.data_as(u64),
+            v3.ctypes.data_as(u64)))
+        return dict(blocks=b5[:nb], edges=e4[:ne], owners=own[:cols], variables=v3[:nvar], rows=rows, cols=cols,
+                    nvalues=nv)
+
+    def model(self, damping_ready: bool = True) -> dict:
+        s = self.structure()
+        nv, rows, cols = s["nvalues"], s["rows"], s["cols"]
+        var = s["variables"]
+        ngram = int(sum(int(w) * int(w) for w in var[:, 1])) if len(var) else 0
+        cw, pw = self.widths
+        out = dict(values=np.zeros(max(nv, 1)), negative_residual=np.zeros(max(rows, 1)),
+                   gradient=np.zeros(max(cols, 1)), scales=np.zeros(max(cols, 1)), gram=np.zeros(max(ngram, 1)),
+                   cross=np.zeros(max(len(s["edges"]) * cw * pw, 1)))
+        raise_for_status(lib.fg_schur_export_model(self._h, *[_dp(out[k]) for k in
+                                                              ("values", "negative_residual", "gradient", "scales",
+                                                               "gram", "cross")]))
+        out["values"] = out["values"][:nv]
+        out["negative_residual"] = out["negative_residual"][:rows]
+        out["gradient"] = out["gradient"][:cols]
+        out["scales"] = out["scales"][:cols]
+        out["gram"] = out["gram"][:ngram]
+        out["cross"] = out["cross"][:len(s["edges"]) * cw * pw]
+        return out
+
+    def reduced_apply(self, damping: float, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros_like(x)
+        raise_for_status(lib.fg_schur_reduced_apply(self._h, damping, _dp(x), _dp(y)))
+        return y
+
+
+def accumulate_into(handle, residual, jacobians) -> None:
+    """Emit one residual with its (column offset, Jacobian) blocks through the C ABI."""
+    r = np.ascontiguousarray(np.asarray(residual, dtype=np.float64).reshape(-1))
+    blocks = [(int(c), np.asarray(j, dtype=np.float64)) for c, j in jacobians]
+    nb = len(blocks)
+    cols = (size_t * max(nb, 1))(*[c for c, _ in blocks])
+    widths = (size_t * max(nb, 1))()
+    ptrs = (dptr * max(nb, 1))()
+    rs = (ptrdiff_t * max(nb, 1))()
+    cs = (ptrdiff_t * max(nb, 1))()
+    keep = []
+    for k, (_, j) in enumerate(blocks):
+        j2 = j.reshape(len(r), -1) if j.ndim != 2 else j
+        keep.append(j2)
+        widths[k] = j2.shape[1]
+        ptrs[k] = j2.ctypes.data_as(dptr)
+        rs[k] = j2.strides[0] // 8
+        cs[k] = j2.strides[1] // 8
+    raise_for_status(lib.fg_backend_accumulate(handle, len(r), _dp(r), nb, cols, widths, ptrs, rs, cs))

@@ -1,0 +1,378 @@
+// Device BAL problem: fagra's examples/bal/model.rs (Projection, Frame batch per
+// camera) with the Stage/Accept/Reject transaction of src/optimization.rs:432-487
+// kept on the device. Observations are stored in emission order.
+#include "bal.cuh"
+#include "kernels.cuh"
+#include <algorithm>
+#include <atomic>
+
+namespace fg {
+
+namespace {
+std::atomic<uint64_t> g_next_id{1};
+}
+
+// Per camera: rotation R (row major) from the unit quaternion exp(w/2)
+// (nalgebra UnitQuaternion::from_scaled_axis + to_rotation_matrix) and the
+// additive angle-axis right factor I - aK + bK^2 (model.rs:126-146).
+__global__ void k_bal_camera_prep(int64_t nc, const double* cams, double* prep) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double* w = cams + 9 * c;
+  double v0 = w[0] / 2, v1 = w[1] / 2, v2 = w[2] / 2;
+  double nn = v0 * v0 + v1 * v1 + v2 * v2;
+  const double eps = 2.220446049250313e-16;
+  double qw, qi, qj, qk;
+  if (nn <= eps * eps) {
+    qw = 1; qi = qj = qk = 0;
+  } else {
+    double n = sqrt(nn), s = sin(n) / n;
+    qw = cos(n); qi = v0 * s; qj = v1 * s; qk = v2 * s;
+  }
+  double ww = qw * qw, ii = qi * qi, jj = qj * qj, kk = qk * qk;
+  double ij = qi * qj * 2, wk = qw * qk * 2, wj = qw * qj * 2, ik = qi * qk * 2, jk = qj * qk * 2, wi = qw * qi * 2;
+  double* R = prep + 18 * c;
+  R[0] = ww + ii - jj - kk; R[1] = ij - wk; R[2] = wj + ik;
+  R[3] = wk + ij; R[4] = ww - ii + jj - kk; R[5] = jk - wi;
+  R[6] = ik - wj; R[7] = wi + jk; R[8] = ww - ii - jj + kk;
+  double t2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  double a, b;
+  if (t2 < 1e-8) {
+    a = 0.5 - t2 / 24. + t2 * t2 / 720.;
+    b = 1. / 6. - t2 / 120. + t2 * t2 / 5040.;
+  } else {
+    double t = sqrt(t2);
+    a = (1. - cos(t)) / t2;
+    b = (t - sin(t)) / (t2 * t);
+  }
+  double K[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
+  double* Rt = prep + 18 * c + 9;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double k2 = 0;
+      for (int k = 0; k < 3; ++k) k2 += K[3 * i + k] * K[3 * k + j];
+      Rt[3 * i + j] = (i == j ? 1.0 : 0.0) - a * K[3 * i + j] + b * k2;
+    }
+}
+
+struct ObsEval {
+  double p[3], q[2], r2, radial, pixel[2];
+  bool ok;
+};
+__device__ __forceinline__ ObsEval bal_eval(const double* R, const double* cam, const double* X) {
+  ObsEval o;
+  for (int i = 0; i < 3; ++i) o.p[i] = R[3 * i] * X[0] + R[3 * i + 1] * X[1] + R[3 * i + 2] * X[2] + cam[3 + i];
+  o.q[0] = -o.p[0] / o.p[2];
+  o.q[1] = -o.p[1] / o.p[2];
+  o.r2 = o.q[0] * o.q[0] + o.q[1] * o.q[1];
+  o.radial = 1. + cam[7] * o.r2 + cam[8] * o.r2 * o.r2;
+  double s = cam[6] * o.radial;
+  o.pixel[0] = s * o.q[0];
+  o.pixel[1] = s * o.q[1];
+  o.ok = !(o.p[2] == 0.) && isfinite(o.pixel[0]) && isfinite(o.pixel[1]);
+  return o;
+}
+
+// Reprojection residual and Jacobians (model.rs:157-185, 214-236) for every
+// observation k in emission order, written in the packed block layout:
+// values[24k .. 24k+18) = camera block (2x9 column major), [24k+18, 24k+24) =
+// point block (2x3 column major), negres[2k..2k+1] = -r.
+template <class TS>
+__global__ void k_bal_linearize(int64_t no, const uint32_t* oc, const uint32_t* op, const double* px,
+                                const double* cams, const double* pts, const double* prep, TS* values,
+                                double* negres, int* error) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= no) return;
+  uint32_t c = oc[k], pi = op[k];
+  const double* cam = cams + 9 * (int64_t)c;
+  const double* R = prep + 18 * (int64_t)c;
+  const double* right = R + 9;
+  double X[3] = {pts[3 * (int64_t)pi], pts[3 * (int64_t)pi + 1], pts[3 * (int64_t)pi + 2]};
+  ObsEval o = bal_eval(R, cam, X);
+  double r[2] = {o.pixel[0] - px[2 * k], o.pixel[1] - px[2 * k + 1]};
+  double f = cam[6], k1 = cam[7], k2 = cam[8];
+  double cc = 2. * k1 + 4. * k2 * o.r2;
+  double dq0 = f * (o.radial + cc * o.q[0] * o.q[0]), dq1 = f * (cc * o.q[0] * o.q[1]);
+  double dq2 = f * (cc * o.q[1] * o.q[0]), dq3 = f * (o.radial + cc * o.q[1] * o.q[1]);
+  double iz = -1. / o.p[2], iz2x = o.p[0] / (o.p[2] * o.p[2]), iz2y = o.p[1] / (o.p[2] * o.p[2]);
+  // dp = dq * [[-1/z, 0, x/z^2], [0, -1/z, y/z^2]]
+  double dp[6] = {dq0 * iz, dq1 * iz, dq0 * iz2x + dq1 * iz2y, dq2 * iz, dq3 * iz, dq2 * iz2x + dq3 * iz2y};
+  // t1 = dp * (-R); t2 = t1 * skew(X); t3 = t2 * right
+  double K[9] = {0, -X[2], X[1], X[2], 0, -X[0], -X[1], X[0], 0};
+  double t1[6], t2[6], t3[6];
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s1 = 0;
+      for (int m = 0; m < 3; ++m) s1 += dp[3 * i + m] * -R[3 * m + j];
+      t1[3 * i + j] = s1;
+    }
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s2 = 0;
+      for (int m = 0; m < 3; ++m) s2 += t1[3 * i + m] * K[3 * m + j];
+      t2[3 * i + j] = s2;
+    }
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s3 = 0;
+      for (int m = 0; m < 3; ++m) s3 += t2[3 * i + m] * right[3 * m + j];
+      t3[3 * i + j] = s3;
+    }
+  double jc[18], jp[6];
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 2; ++i) {
+      jc[2 * j + i] = t3[3 * i + j];
+      jc[2 * (3 + j) + i] = dp[3 * i + j];
+    }
+  for (int i = 0; i < 2; ++i) {
+    jc[12 + i] = o.radial * o.q[i];
+    jc[14 + i] = f * o.r2 * o.q[i];
+    jc[16 + i] = f * o.r2 * o.r2 * o.q[i];
+  }
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int m = 0; m < 3; ++m) s += dp[3 * i + m] * R[3 * m + j];
+      jp[2 * j + i] = s;
+    }
+  bool ok = o.ok && isfinite(r[0]) && isfinite(r[1]);
+  TS* v = values + 24 * k;
+  for (int i = 0; i < 18; ++i) {
+    v[i] = (TS)jc[i];
+    ok = ok && isfinite(jc[i]);
+  }
+  for (int i = 0; i < 6; ++i) {
+    v[18 + i] = (TS)jp[i];
+    ok = ok && isfinite(jp[i]);
+  }
+  negres[2 * k] = -r[0];
+  negres[2 * k + 1] = -r[1];
+  if (!ok) atomicOr(error, 1);
+}
+
+// Error-free addition (Knuth TwoSum) for compensated cost reductions.
+__device__ __forceinline__ void two_sum(double a, double b, double* s, double* e) {
+  double x = a + b;
+  double bv = x - a;
+  double av = x - bv;
+  *s = x;
+  *e = (a - av) + (b - bv);
+}
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, double blo) {
+  double s, e;
+  two_sum(hi, bhi, &s, &e);
+  e += lo + blo;
+  two_sum(s, e, &hi, &lo);
+}
+
+// Sum of 0.5 |r|^2 over observations (Frame::cost) in double-double, with
+// an error flag for invalid projections. out[0] = cost, out[1] = error.
+__global__ void k_bal_cost(int64_t no, const uint32_t* oc, const uint32_t* op, const double* px, const double* cams,
+                           const double* pts, const double* prep, double* partials, unsigned* counter, double* out) {
+  double hi = 0, lo = 0, bad = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < no; k += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t c = oc[k], pi = op[k];
+    double X[3] = {pts[3 * (int64_t)pi], pts[3 * (int64_t)pi + 1], pts[3 * (int64_t)pi + 2]};
+    ObsEval o = bal_eval(prep + 18 * (int64_t)c, cams + 9 * (int64_t)c, X);
+    double r0 = o.pixel[0] - px[2 * k], r1 = o.pixel[1] - px[2 * k + 1];
+    double v = 0.5 * (r0 * r0 + r1 * r1);
+    if (!o.ok || !isfinite(v)) bad = 1;
+    else dd_add(hi, lo, v, 0.0);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double h2 = __shfl_down_sync(0xffffffffu, hi, o), l2 = __shfl_down_sync(0xffffffffu, lo, o);
+    double b2 = __shfl_down_sync(0xffffffffu, bad, o);
+    dd_add(hi, lo, h2, l2);
+    bad = fmax(bad, b2);
+  }
+  __shared__ double sh[32][3];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) { sh[warp][0] = hi; sh[warp][1] = lo; sh[warp][2] = bad; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    for (int w = 1; w < nw; ++w) {
+      dd_add(hi, lo, sh[w][0], sh[w][1]);
+      bad = fmax(bad, sh[w][2]);
+    }
+    partials[3 * blockIdx.x] = hi;
+    partials[3 * blockIdx.x + 1] = lo;
+    partials[3 * blockIdx.x + 2] = bad;
+  }
+  if (arrive_last(counter)) {
+    if (threadIdx.x == 0) {
+      double H = 0, Lo = 0, B = 0;
+      for (unsigned b = 0; b < gridDim.x; ++b) {
+        dd_add(H, Lo, ((volatile double*)partials)[3 * b], ((volatile double*)partials)[3 * b + 1]);
+        B = fmax(B, ((volatile double*)partials)[3 * b + 2]);
+      }
+      out[0] = H + Lo;
+      out[1] = B;
+      *counter = 0;
+    }
+  }
+}
+
+// Trial retraction x + delta for additive Camera/Point variables.
+__global__ void k_bal_stage(int64_t nc9, int64_t np3, const double* cams, const double* pts, const double* delta,
+                            double* tcams, double* tpts) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < nc9) tcams[i] = cams[i] + delta[i];
+  else if (i < nc9 + np3) tpts[i - nc9] = pts[i - nc9] + delta[i];
+}
+
+fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const double* pp, const uint32_t* ocam,
+                           const uint32_t* opt, const double* pix, int device, bool on_device) {
+  id = g_next_id.fetch_add(1);
+  dev = device;
+  nc = c; np = p; no = o;
+  FG_TRY(select_device(dev));
+  FG_TRY(device_stream(dev, &st));
+  nsm = sm_count(dev);
+  std::vector<uint32_t> hc(o), hp(o);
+  std::vector<double> hx(2 * o);
+  if (on_device) {
+    if (o) {
+      FG_CUDA(cudaMemcpy(hc.data(), ocam, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+      FG_CUDA(cudaMemcpy(hp.data(), opt, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+      FG_CUDA(cudaMemcpy(hx.data(), pix, 2 * o * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+  } else {
+    std::copy(ocam, ocam + o, hc.begin());
+    std::copy(opt, opt + o, hp.begin());
+    std::copy(pix, pix + 2 * o, hx.begin());
+  }
+  for (size_t i = 0; i < o; ++i)
+    if (hc[i] >= nc || hp[i] >= np || !std::isfinite(hx[2 * i]) || !std::isfinite(hx[2 * i + 1])) {
+      set_error("invalid observation index or value");
+      return FG_INVALID_EMISSION;
+    }
+  // Emission order: frames in camera order, factors in insertion order.
+  std::vector<size_t> off(nc + 1, 0);
+  for (size_t i = 0; i < o; ++i) off[hc[i] + 1]++;
+  for (size_t i = 0; i < nc; ++i) off[i + 1] += off[i];
+  order.assign(o, 0);
+  for (size_t i = 0; i < o; ++i) order[off[hc[i]]++] = i;
+  h_oc.resize(o);
+  h_op.resize(o);
+  std::vector<double> ex(2 * o);
+  for (size_t k = 0; k < o; ++k) {
+    h_oc[k] = hc[order[k]];
+    h_op[k] = hp[order[k]];
+    ex[2 * k] = hx[2 * order[k]];
+    ex[2 * k + 1] = hx[2 * order[k] + 1];
+  }
+  FG_TRY(upload(oc, h_oc.data(), o, st));
+  FG_TRY(upload(op, h_op.data(), o, st));
+  FG_TRY(upload(px, ex.data(), 2 * o, st));
+  FG_TRY(cams.resize(std::max<size_t>(9 * nc, 1)));
+  FG_TRY(pts.resize(std::max<size_t>(3 * np, 1)));
+  FG_TRY(tcams.resize(std::max<size_t>(9 * nc, 1)));
+  FG_TRY(tpts.resize(std::max<size_t>(3 * np, 1)));
+  FG_TRY(prep.resize(std::max<size_t>(18 * nc, 1)));
+  FG_TRY(tprep.resize(std::max<size_t>(18 * nc, 1)));
+  FG_TRY(partials.resize(3 * 4096));
+  FG_TRY(counters.resize(4));
+  FG_TRY(result.resize(4));
+  FG_TRY(h_result.resize(4));
+  FG_TRY(h_flag.resize(2));
+  FG_TRY(d_flag.resize(2));
+  FG_CUDA(cudaMemsetAsync(counters.get(), 0, 4 * sizeof(unsigned), st));
+  auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (nc) FG_CUDA(cudaMemcpyAsync(cams.get(), cp, 9 * nc * sizeof(double), kind, st));
+  if (np) FG_CUDA(cudaMemcpyAsync(pts.get(), pp, 3 * np * sizeof(double), kind, st));
+  FG_TRY(init_cams.resize(std::max<size_t>(9 * nc, 1)));
+  FG_TRY(init_pts.resize(std::max<size_t>(3 * np, 1)));
+  if (nc) FG_CUDA(cudaMemcpyAsync(init_cams.get(), cams.get(), 9 * nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (np) FG_CUDA(cudaMemcpyAsync(init_pts.get(), pts.get(), 3 * np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  return FG_OK;
+}
+
+fg_status BalProblem::restore_initial() {
+  if (nc) FG_CUDA(cudaMemcpyAsync(cams.get(), init_cams.get(), 9 * nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (np) FG_CUDA(cudaMemcpyAsync(pts.get(), init_pts.get(), 3 * np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  trial_active = false;
+  return FG_OK;
+}
+
+fg_status BalProblem::set_parameters(const double* cp, const double* pp) {
+  if (nc) FG_CUDA(cudaMemcpyAsync(cams.get(), cp, 9 * nc * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (np) FG_CUDA(cudaMemcpyAsync(pts.get(), pp, 3 * np * sizeof(double), cudaMemcpyHostToDevice, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  trial_active = false;
+  return FG_OK;
+}
+
+fg_status BalProblem::get_parameters(double* cp, double* pp) {
+  if (cp && nc) FG_CUDA(cudaMemcpyAsync(cp, cams.get(), 9 * nc * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (pp && np) FG_CUDA(cudaMemcpyAsync(pp, pts.get(), 3 * np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  return FG_OK;
+}
+
+fg_status BalProblem::cost(bool trial, double* out) {
+  const double* C = trial ? tcams.get() : cams.get();
+  const double* P = trial ? tpts.get() : pts.get();
+  double* R = trial ? tprep.get() : prep.get();
+  if (nc) FG_LAUNCH(k_bal_camera_prep, grid_for(nc, 128), 128, 0, st, (int64_t)nc, C, R);
+  unsigned g = std::min<unsigned>(grid_for(std::max<size_t>(no, 1), 256), 4 * nsm);
+  FG_LAUNCH(k_bal_cost, g, 256, 0, st, (int64_t)no, oc.get(), op.get(), px.get(), C, P, R, partials.get(),
+            counters.get(), result.get());
+  FG_CUDA(cudaMemcpyAsync(h_result.get(), result.get(), 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  double c = h_result.get()[0];
+  if (h_result.get()[1] != 0 || !std::isfinite(c) || c < 0) {  // checked_cost, storage.rs:612-618
+    set_error("invalid BAL evaluation");
+    return FG_INVALID_EVALUATION;
+  }
+  *out = c;
+  return FG_OK;
+}
+
+fg_status BalProblem::linearize(Backend* b) {
+  FG_TRY(b->clear());
+  FG_TRY(b->bind_bal(id, nc, np, no, h_oc.data(), h_op.data()));
+  if (nc) FG_LAUNCH(k_bal_camera_prep, grid_for(nc, 128), 128, 0, st, (int64_t)nc, cams.get(), prep.get());
+  FG_CUDA(cudaMemsetAsync(d_flag.get(), 0, sizeof(int), st));
+  if (no) {
+    if (b->is_f32()) {
+      FG_LAUNCH(k_bal_linearize<float>, grid_for(no, 128), 128, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
+                cams.get(), pts.get(), prep.get(), (float*)b->values_device(), b->negres_device(), d_flag.get());
+    } else {
+      FG_LAUNCH(k_bal_linearize<double>, grid_for(no, 128), 128, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
+                cams.get(), pts.get(), prep.get(), (double*)b->values_device(), b->negres_device(), d_flag.get());
+    }
+  }
+  FG_CUDA(cudaMemcpyAsync(h_flag.get(), d_flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  b->mark_device_model(2 * no);
+  if (h_flag.get()[0]) {
+    set_error("invalid BAL linearization");
+    return FG_INVALID_EVALUATION;
+  }
+  return FG_OK;
+}
+
+fg_status BalProblem::stage(const double* d_delta) {
+  size_t n = 9 * nc + 3 * np;
+  if (n) FG_LAUNCH(k_bal_stage, grid_for(n, 256), 256, 0, st, (int64_t)(9 * nc), (int64_t)(3 * np), cams.get(),
+                   pts.get(), d_delta, tcams.get(), tpts.get());
+  trial_active = true;
+  return FG_OK;
+}
+
+void BalProblem::accept() {
+  if (trial_active) {
+    std::swap(cams.ptr, tcams.ptr);
+    std::swap(cams.cap, tcams.cap);
+    std::swap(pts.ptr, tpts.ptr);
+    std::swap(pts.cap, tpts.cap);
+    trial_active = false;
+  }
+}
+
+void BalProblem::reject() { trial_active = false; }
+
+}  // namespace fg

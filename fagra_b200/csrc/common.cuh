@@ -1,0 +1,147 @@
+// Shared infrastructure: status plumbing, device/pinned buffers, the per-device
+// library stream, launch accounting and small device reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <atomic>
+#include <cmath>
+#include <limits>
+#include "../../include/fagra_b200.h"
+
+namespace fg {
+
+void set_error(const std::string& text);
+fg_status cuda_status(cudaError_t e, const char* what);
+extern std::atomic<uint64_t> g_launches;
+
+#define FG_CUDA(call)                                         \
+  do {                                                        \
+    cudaError_t e__ = (call);                                 \
+    if (e__ != cudaSuccess) return ::fg::cuda_status(e__, #call); \
+  } while (0)
+#define FG_TRY(expr)                  \
+  do {                                \
+    fg_status s__ = (expr);           \
+    if (s__ != FG_OK) return s__;     \
+  } while (0)
+// Launch bookkeeping: every kernel launch goes through FG_LAUNCH so the library
+// can report how many of its kernels ran.
+#define FG_LAUNCH(kernel, grid, block, smem, stream, ...)                      \
+  do {                                                                         \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                \
+    ::fg::g_launches.fetch_add(1, std::memory_order_relaxed);                  \
+    cudaError_t e__ = cudaGetLastError();                                      \
+    if (e__ != cudaSuccess) return ::fg::cuda_status(e__, #kernel);            \
+  } while (0)
+
+fg_status device_stream(int device, cudaStream_t* out);
+fg_status select_device(int device);
+int sm_count(int device);
+
+// Grow-only device buffer: a warm workspace never reallocates.
+template <class T>
+struct DBuf {
+  T* ptr = nullptr;
+  size_t n = 0, cap = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { if (ptr) cudaFree(ptr); }
+  fg_status resize(size_t count) {
+    if (count > cap) {
+      if (ptr) cudaFree(ptr);
+      ptr = nullptr;
+      cap = 0;
+      size_t want = count + count / 8 + 16;
+      cudaError_t e = cudaMalloc(&ptr, want * sizeof(T));
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation failed");
+        return FG_OUT_OF_MEMORY;
+      }
+      cap = want;
+    }
+    n = count;
+    return FG_OK;
+  }
+  T* get() const { return ptr; }
+  size_t size() const { return n; }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// Grow-only pinned host buffer.
+template <class T>
+struct HBuf {
+  T* ptr = nullptr;
+  size_t n = 0, cap = 0;
+  HBuf() = default;
+  HBuf(const HBuf&) = delete;
+  HBuf& operator=(const HBuf&) = delete;
+  ~HBuf() { if (ptr) cudaFreeHost(ptr); }
+  fg_status resize(size_t count) {
+    if (count > cap) {
+      T* fresh = nullptr;
+      size_t want = count + count / 8 + 16;
+      cudaError_t e = cudaMallocHost(&fresh, want * sizeof(T));
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("pinned allocation failed");
+        return FG_OUT_OF_MEMORY;
+      }
+      if (ptr) {
+        std::memcpy(fresh, ptr, n * sizeof(T));
+        cudaFreeHost(ptr);
+      }
+      ptr = fresh;
+      cap = want;
+    }
+    n = count;
+    return FG_OK;
+  }
+  T* get() const { return ptr; }
+  size_t size() const { return n; }
+};
+
+template <class T>
+fg_status upload(DBuf<T>& d, const T* h, size_t count, cudaStream_t s) {
+  FG_TRY(d.resize(count));
+  if (count) FG_CUDA(cudaMemcpyAsync(d.ptr, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  return FG_OK;
+}
+
+// Event-pair timer on the library stream (used for SchurTimings).
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  bool armed = false;
+  ~EventTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  void start(cudaStream_t s) {
+    if (!a) { cudaEventCreate(&a); cudaEventCreate(&b); }
+    cudaEventRecord(a, s);
+    armed = true;
+  }
+  double stop(cudaStream_t s) {  // seconds; synchronizes on the end event
+    if (!armed) return 0;
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    armed = false;
+    return ms * 1e-3;
+  }
+};
+
+inline unsigned grid_for(size_t n, unsigned block) {
+  size_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 0x7fffffffu) g = 0x7fffffffu;
+  return (unsigned)g;
+}
+
+}  // namespace fg

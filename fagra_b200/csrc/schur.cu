@@ -1,0 +1,789 @@
+// Schur backend host orchestration: fagra's `Schur` (src/schur.rs) with all
+// numerical work on the device. Host code only validates emissions, stages
+// them (src/linear_model.rs:180-210 packing) and builds integer index maps.
+#include "kernels.cuh"
+#include "fastpath.cuh"
+#include <algorithm>
+#include <numeric>
+
+namespace fg {
+
+namespace {
+
+// Widths with compiled specializations; other widths (<= MAXW) use runtime loops.
+#define FG_DISPATCH_WIDTHS(cw, pw, BODY)                     \
+  do {                                                        \
+    if ((cw) == 9 && (pw) == 3) { constexpr int CW_ = 9, PW_ = 3; BODY; }      \
+    else if ((cw) == 6 && (pw) == 3) { constexpr int CW_ = 6, PW_ = 3; BODY; } \
+    else if ((cw) == 2 && (pw) == 2) { constexpr int CW_ = 2, PW_ = 2; BODY; } \
+    else if ((cw) == 1 && (pw) == 1) { constexpr int CW_ = 1, PW_ = 1; BODY; } \
+    else { constexpr int CW_ = 0, PW_ = 0; BODY; }                             \
+  } while (0)
+
+template <class T>
+struct TypeTag {};
+
+}  // namespace
+
+template <class TS>
+class SchurImpl final : public Backend {
+ public:
+  // ---- configuration (src/schur.rs:116-143)
+  fg_schur_options opt;
+  size_t retained, cw, pw;
+  int dev;
+  cudaStream_t st = nullptr;
+  int nsm = 148;
+
+  // ---- prepared sizes
+  size_t dim = 0, nC = 0, nP = 0;
+  bool ready = false;
+
+  // ---- statistics / diagnostics
+  size_t solves = 0, iterations = 0;
+  fg_schur_diagnostics diag{};
+  fg_schur_timings tim{};
+
+  // ---- host staging for generic emissions (LinearizedModel layout)
+  std::vector<HostBlock> h_blocks;
+  std::vector<double> h_values, h_negres;
+  std::vector<HostEdge> h_edges;
+  size_t h_rows = 0;
+  // structure of the last upload (to skip rebuilding identical index maps)
+  std::vector<HostBlock> up_blocks;
+  std::vector<HostEdge> up_edges;
+  size_t up_rows = 0;
+  bool structure_valid = false;
+
+  // ---- model source
+  enum Source { NONE, HOST, DEVICE_BAL } source = NONE;
+  bool device_model_current = false;  // device values/negres are current
+  bool gradient_current = false;
+  uint64_t bal_bound = 0;             // id of the BAL structure currently bound
+  size_t bal_obs = 0;
+
+  // ---- device model and index maps
+  size_t rows = 0, nblocks = 0, nedges = 0, nvalues = 0, nemissions = 0;
+  DBuf<DBlockMeta> d_blocks;
+  DBuf<DEdgeMeta> d_edges;
+  DBuf<int64_t> d_var_off, d_var_blk, d_pt_edge_off, d_pt_edge, d_cam_edge_off, d_cam_edge, d_emi_off;
+  DBuf<uint8_t> d_observed;
+  std::vector<uint8_t> h_observed;
+  DBuf<TS> d_values;
+  DBuf<double> d_negres;
+
+  // ---- numerics
+  DBuf<double> d_g, d_scales, d_work, d_rhs, d_zred, d_step, d_tmpd, d_qd, d_jd;
+  DBuf<TS> d_gram, d_factors, d_precond, d_cross;
+  DBuf<TS> d_x, d_r, d_z, d_pp, d_q, d_t;  // PCG vectors in the storage precision
+  DBuf<double> d_partials, d_norm;
+  DBuf<unsigned> d_counters;
+  DBuf<PcgState> d_pcg;
+  DBuf<VerifyState> d_ver;
+  HBuf<double> h_step, h_scalar;
+  HBuf<PcgState> h_pcg;
+  HBuf<VerifyState> h_ver;
+  HBuf<unsigned> h_count;
+  FastPath<TS> fast;  // specialized BAL (9,3) single-pass reduced operator
+
+  Layout layout() const {
+    Layout L;
+    L.retained = (int64_t)retained;
+    L.dim = (int64_t)dim;
+    L.cw = (int32_t)cw;
+    L.pw = (int32_t)pw;
+    L.nC = (int32_t)nC;
+    L.nP = (int32_t)nP;
+    return L;
+  }
+
+  SchurImpl(size_t r, size_t c, size_t p, const fg_schur_options& o) : opt(o), retained(r), cw(c), pw(p), dev(o.device) {}
+
+  fg_status init() {
+    FG_TRY(select_device(dev));
+    FG_TRY(device_stream(dev, &st));
+    nsm = sm_count(dev);
+    FG_TRY(d_pcg.resize(1));
+    FG_TRY(d_ver.resize(1));
+    FG_TRY(h_pcg.resize(1));
+    FG_TRY(h_ver.resize(1));
+    FG_TRY(h_count.resize(4));
+    FG_TRY(h_scalar.resize(4));
+    FG_TRY(d_counters.resize(8));
+    FG_TRY(d_norm.resize(4));
+    FG_CUDA(cudaMemsetAsync(d_pcg.get(), 0, sizeof(PcgState), st));
+    FG_CUDA(cudaMemsetAsync(d_ver.get(), 0, sizeof(VerifyState), st));
+    FG_CUDA(cudaMemsetAsync(d_counters.get(), 0, 8 * sizeof(unsigned), st));
+    FG_TRY(d_partials.resize(8 * 65536));
+    return FG_OK;
+  }
+
+  // ------------------------------------------------------------------ trait
+  fg_status set_options(const fg_schur_options& o) override {
+    int keep = dev;
+    opt = o;
+    opt.device = keep;
+    return FG_OK;
+  }
+
+  fg_status prepare(size_t dimension) override {  // src/schur.rs:409-431
+    ready = false;
+    solves = iterations = 0;
+    diag = fg_schur_diagnostics{};
+    tim = fg_schur_timings{};
+    if (cw == 0 || pw == 0 || retained > dimension || retained % cw || (dimension - retained) % pw ||
+        opt.max_iterations == 0 || !(opt.relative_tolerance >= 0 && opt.relative_tolerance < 1)) {
+      set_error("Schur prepare: invalid partition or controls");
+      return FG_INVALID_OPTIONS;
+    }
+    FG_TRY(select_device(dev));
+    if (dimension != dim) structure_valid = false;
+    dim = dimension;
+    nC = retained / cw;
+    nP = (dim - retained) / pw;
+    FG_TRY(d_g.resize(dim));
+    FG_TRY(d_scales.resize(dim));
+    FG_TRY(d_work.resize(dim));
+    FG_TRY(d_step.resize(dim));
+    FG_TRY(d_tmpd.resize(std::max(dim, (size_t)1)));
+    FG_TRY(d_rhs.resize(retained));
+    FG_TRY(d_zred.resize(retained));
+    FG_TRY(d_qd.resize(retained));
+    FG_TRY(h_step.resize(dim));
+    FG_TRY(d_x.resize(retained));
+    FG_TRY(d_r.resize(retained));
+    FG_TRY(d_z.resize(retained));
+    FG_TRY(d_pp.resize(retained));
+    FG_TRY(d_q.resize(retained));
+    FG_TRY(d_t.resize(nP * pw));
+    size_t ng = nC * cw * cw + nP * pw * pw;
+    FG_TRY(d_gram.resize(ng));
+    FG_TRY(d_factors.resize(ng));
+    FG_TRY(d_precond.resize(ng));
+    FG_TRY(d_observed.resize(nC + nP));
+    return clear();
+  }
+
+  fg_status clear() override {  // src/schur.rs:432-437
+    ready = false;
+    h_blocks.clear();
+    h_values.clear();
+    h_negres.clear();
+    h_edges.clear();
+    h_rows = 0;
+    source = HOST;
+    device_model_current = false;
+    gradient_current = false;
+    return FG_OK;
+  }
+
+  fg_status accumulate(size_t nrows, const double* r, size_t nb, const size_t* bcols, const size_t* widths,
+                       const double* const* jac, const ptrdiff_t* rs, const ptrdiff_t* cs) override {
+    // src/schur.rs:438-482 structure validation, then LinearizedModel packing.
+    ready = false;
+    if (source != HOST) clear();
+    if (nrows && !r) return FG_NULL_ARGUMENT;
+    if (nb && (!bcols || !widths || !jac || !rs || !cs)) return FG_NULL_ARGUMENT;
+    bool has_l = false, has_r = false;
+    size_t lcol = 0, lidx = 0, rcol = 0, ridx = 0;
+    size_t start = h_blocks.size();
+    for (size_t i = 0; i < nb; ++i) {
+      size_t col = bcols[i], end = col + widths[i];
+      if (end < col || end > dim) return FG_DIMENSION_MISMATCH;
+      if (col < retained) {
+        if (col % cw || widths[i] != cw || end > retained || has_l) return FG_UNSUPPORTED_STRUCTURE;
+        has_l = true; lcol = col; lidx = start + i;
+      } else {
+        if ((col - retained) % pw || widths[i] != pw || has_r) return FG_UNSUPPORTED_STRUCTURE;
+        has_r = true; rcol = col - retained; ridx = start + i;
+      }
+      if (widths[i] && nrows && !jac[i]) return FG_NULL_ARGUMENT;
+    }
+    size_t row = h_rows;
+    h_rows += nrows;
+    for (size_t i = 0; i < nrows; ++i) h_negres.push_back(-r[i]);
+    for (size_t b = 0; b < nb; ++b) {
+      h_blocks.push_back({row, bcols[b], nrows, widths[b], h_values.size()});
+      for (size_t j = 0; j < widths[b]; ++j)
+        for (size_t i = 0; i < nrows; ++i) h_values.push_back(jac[b][(ptrdiff_t)i * rs[b] + (ptrdiff_t)j * cs[b]]);
+    }
+    if (has_l && has_r) h_edges.push_back({lcol, rcol, lidx, ridx});
+    device_model_current = false;
+    gradient_current = false;
+    return FG_OK;
+  }
+
+  // Build and upload index maps for a structure (host integer bookkeeping).
+  fg_status build_structure(const std::vector<HostBlock>& blocks, const std::vector<HostEdge>& edges, size_t nrows) {
+    rows = nrows;
+    nblocks = blocks.size();
+    nedges = edges.size();
+    size_t nvar = nC + nP;
+    std::vector<DBlockMeta> mb(nblocks);
+    std::vector<int64_t> var_of(nblocks), var_off(nvar + 1, 0), var_blk(nblocks);
+    for (size_t i = 0; i < nblocks; ++i) {
+      const HostBlock& b = blocks[i];
+      mb[i] = {(int64_t)b.row, (int64_t)b.start, (int64_t)b.col, (int32_t)b.rows, (int32_t)b.cols};
+      int64_t v = b.col < retained ? (int64_t)(b.col / cw) : (int64_t)(nC + (b.col - retained) / pw);
+      var_of[i] = b.cols ? v : -1;
+      if (b.cols) var_off[v + 1]++;
+    }
+    for (size_t v = 0; v < nvar; ++v) var_off[v + 1] += var_off[v];
+    {
+      std::vector<int64_t> fill(var_off.begin(), var_off.end() - 1);
+      for (size_t i = 0; i < nblocks; ++i)
+        if (var_of[i] >= 0) var_blk[fill[var_of[i]]++] = (int64_t)i;
+    }
+    h_observed.assign(nvar, 0);
+    for (size_t v = 0; v < nvar; ++v) h_observed[v] = var_off[v + 1] > var_off[v];
+    std::vector<DEdgeMeta> me(nedges);
+    std::vector<int64_t> pt_off(nP + 1, 0), cam_off(nC + 1, 0), pt_e(nedges), cam_e(nedges);
+    for (size_t e = 0; e < nedges; ++e) {
+      me[e] = {(int32_t)(edges[e].retained / cw), (int32_t)(edges[e].eliminated / pw), (int64_t)edges[e].lblk,
+               (int64_t)edges[e].rblk};
+      pt_off[me[e].pt + 1]++;
+      cam_off[me[e].cam + 1]++;
+    }
+    for (size_t p = 0; p < nP; ++p) pt_off[p + 1] += pt_off[p];
+    for (size_t c = 0; c < nC; ++c) cam_off[c + 1] += cam_off[c];
+    {
+      std::vector<int64_t> fp(pt_off.begin(), pt_off.end() - 1), fc(cam_off.begin(), cam_off.end() - 1);
+      for (size_t e = 0; e < nedges; ++e) {
+        pt_e[fp[me[e].pt]++] = (int64_t)e;
+        cam_e[fc[me[e].cam]++] = (int64_t)e;
+      }
+    }
+    // emissions: consecutive blocks sharing a row start
+    std::vector<int64_t> emi;
+    for (size_t i = 0; i < nblocks; ++i)
+      if (i == 0 || blocks[i].row != blocks[i - 1].row || blocks[i].rows == 0) emi.push_back((int64_t)i);
+    emi.push_back((int64_t)nblocks);
+    nemissions = emi.size() - 1;
+    FG_TRY(upload(d_blocks, mb.data(), mb.size(), st));
+    FG_TRY(upload(d_edges, me.data(), me.size(), st));
+    FG_TRY(upload(d_var_off, var_off.data(), var_off.size(), st));
+    FG_TRY(upload(d_var_blk, var_blk.data(), var_blk.size(), st));
+    FG_TRY(upload(d_pt_edge_off, pt_off.data(), pt_off.size(), st));
+    FG_TRY(upload(d_pt_edge, pt_e.data(), pt_e.size(), st));
+    FG_TRY(upload(d_cam_edge_off, cam_off.data(), cam_off.size(), st));
+    FG_TRY(upload(d_cam_edge, cam_e.data(), cam_e.size(), st));
+    FG_TRY(upload(d_emi_off, emi.data(), emi.size(), st));
+    FG_TRY(upload(d_observed, h_observed.data(), h_observed.size(), st));
+    FG_TRY(d_cross.resize(std::max<size_t>(nedges * cw * pw, 1)));
+    FG_TRY(d_jd.resize(std::max<size_t>(rows, 1)));
+    // synchronize so host vectors may be released safely
+    FG_CUDA(cudaStreamSynchronize(st));
+    structure_valid = true;
+    fast.invalidate();
+    return FG_OK;
+  }
+
+  static bool same_blocks(const std::vector<HostBlock>& a, const std::vector<HostBlock>& b) {
+    if (a.size() != b.size()) return false;
+    for (size_t i = 0; i < a.size(); ++i)
+      if (a[i].row != b[i].row || a[i].col != b[i].col || a[i].rows != b[i].rows || a[i].cols != b[i].cols ||
+          a[i].start != b[i].start)
+        return false;
+    return true;
+  }
+  static bool same_edges(const std::vector<HostEdge>& a, const std::vector<HostEdge>& b) {
+    if (a.size() != b.size()) return false;
+    for (size_t i = 0; i < a.size(); ++i)
+      if (a[i].retained != b[i].retained || a[i].eliminated != b[i].eliminated || a[i].lblk != b[i].lblk ||
+          a[i].rblk != b[i].rblk)
+        return false;
+    return true;
+  }
+
+  // Upload host emissions and compute the gradient on the device.
+  fg_status sync_model() {
+    if (source == HOST && !device_model_current) {
+      if (!structure_valid || bal_bound || up_rows != h_rows || !same_blocks(up_blocks, h_blocks) ||
+          !same_edges(up_edges, h_edges)) {
+        bal_bound = 0;
+        FG_TRY(build_structure(h_blocks, h_edges, h_rows));
+        up_blocks = h_blocks;
+        up_edges = h_edges;
+        up_rows = h_rows;
+      }
+      nvalues = h_values.size();
+      FG_TRY(d_values.resize(std::max<size_t>(nvalues, 1)));
+      if (nvalues) {
+        if (std::is_same<TS, double>::value) {
+          FG_CUDA(cudaMemcpyAsync(d_values.get(), h_values.data(), nvalues * sizeof(double), cudaMemcpyHostToDevice, st));
+        } else {
+          std::vector<TS> conv(h_values.begin(), h_values.end());
+          FG_CUDA(cudaMemcpyAsync(d_values.get(), conv.data(), nvalues * sizeof(TS), cudaMemcpyHostToDevice, st));
+          FG_CUDA(cudaStreamSynchronize(st));
+        }
+      }
+      FG_TRY(upload(d_negres, h_negres.data(), h_negres.size(), st));
+      if (d_negres.cap == 0) FG_TRY(d_negres.resize(1));
+      FG_CUDA(cudaStreamSynchronize(st));
+      device_model_current = true;
+      gradient_current = false;
+    }
+    if (source == NONE) return FG_INVALID_OPTIONS;
+    if (!gradient_current) {
+      if (dim) FG_LAUNCH(k_gradient<TS>, grid_for(dim, NT), NT, 0, st, layout(), d_var_off.get(), d_var_blk.get(),
+                         d_blocks.get(), d_values.get(), d_negres.get(), d_g.get());
+      gradient_current = true;
+    }
+    return FG_OK;
+  }
+
+  // max |x| over a device array; returns INVALID_EVALUATION on nonfinite.
+  template <class T>
+  fg_status device_norm_inf(const T* x, size_t n, double* out) {
+    if (n == 0) { *out = 0; return FG_OK; }
+    unsigned g = std::min<unsigned>(grid_for(n, NT), 4 * nsm);
+    FG_LAUNCH(k_norm_inf<T>, g, NT, 0, st, (int64_t)n, x, d_partials.get(), d_counters.get() + 3, d_norm.get());
+    FG_CUDA(cudaMemcpyAsync(h_scalar.get(), d_norm.get(), 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (h_scalar.get()[1] != 0) {
+      set_error("nonfinite value");
+      return FG_INVALID_EVALUATION;
+    }
+    *out = h_scalar.get()[0];
+    return FG_OK;
+  }
+
+  fg_status gradient_norm(double* out) override {  // src/schur.rs:483-485
+    FG_TRY(sync_model());
+    return device_norm_inf(d_g.get(), dim, out);
+  }
+
+  fg_status prepare_damping(double floor) override {  // src/schur.rs:490-526
+    ready = false;
+    EventTimer tm;
+    if (opt.collect_timings) tm.start(st);
+    if (!std::isfinite(floor) || floor <= 0) {
+      set_error("min_column_norm must be finite and positive");
+      return FG_INVALID_OPTIONS;
+    }
+    FG_TRY(sync_model());
+    Layout L = layout();
+    if (dim) {
+      FG_LAUNCH(k_scales_raw<TS>, grid_for(dim, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(), d_blocks.get(),
+                d_values.get(), d_scales.get());
+      double m;
+      FG_TRY(device_norm_inf(d_scales.get(), dim, &m));
+      FG_LAUNCH(k_floor, grid_for(dim, NT), NT, 0, st, (int64_t)dim, d_scales.get(), floor);
+    }
+    size_t ng = nC * cw * cw + nP * pw * pw;
+    if (ng) {
+      FG_CUDA(cudaMemsetAsync(d_gram.get(), 0, ng * sizeof(TS), st));
+      if (nC) FG_LAUNCH(k_gram<TS>, grid_for(nC * cw * cw, NT), NT, 0, st, L, (int64_t)0, (int64_t)nC, (int)cw,
+                        d_var_off.get(), d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
+      if (nP) FG_LAUNCH(k_gram<TS>, grid_for(nP * pw * pw, NT), NT, 0, st, L, (int64_t)nC, (int64_t)nP, (int)pw,
+                        d_var_off.get(), d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
+    }
+    if (nedges) {
+      FG_LAUNCH(k_cross<TS>, grid_for(nedges * cw * pw, NT), NT, 0, st, (int64_t)nedges, (int)cw, (int)pw,
+                d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_cross.get());
+      double m;
+      FG_TRY(device_norm_inf(d_cross.get(), nedges * cw * pw, &m));
+    }
+    FG_TRY(fast.prepare(*this));
+    ready = true;
+    if (opt.collect_timings) tim.preparation += tm.stop(st);
+    return FG_OK;
+  }
+
+  // Factor B and C blocks (+ the optional S_cc preconditioner) for lambda.
+  fg_status factor(double lambda, unsigned* fallbacks) {
+    Layout L = layout();
+    FG_CUDA(cudaMemsetAsync(d_counters.get() + 4, 0, sizeof(unsigned), st));
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      if (nC) FG_LAUNCH((k_factor<CW_, TS>), grid_for(nC, 128), 128, 0, st, L, (int64_t)0, (int64_t)nC, (int)cw,
+                        d_observed.get(), d_gram.get(), d_factors.get(), lambda, d_counters.get() + 4);
+      if (nP) FG_LAUNCH((k_factor<PW_, TS>), grid_for(nP, 128), 128, 0, st, L, (int64_t)nC, (int64_t)nP, (int)pw,
+                        d_observed.get(), d_gram.get(), d_factors.get(), lambda, d_counters.get() + 4);
+    });
+    FG_CUDA(cudaMemcpyAsync(h_count.get(), d_counters.get() + 4, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    *fallbacks = h_count.get()[0];
+    if (*fallbacks == 0 && opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL && nC) {
+      FG_DISPATCH_WIDTHS(cw, pw, {
+        FG_LAUNCH((k_schur_diag_factor<CW_, PW_, TS>), grid_for(nC, 64), 64, 0, st, L, d_cam_edge_off.get(),
+                  d_cam_edge.get(), d_edges.get(), d_cross.get(), d_observed.get(), d_gram.get(), d_factors.get(),
+                  d_precond.get(), lambda);
+      });
+    }
+    return FG_OK;
+  }
+  const TS* precond_factors() const {
+    return opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL ? d_precond.get() : d_factors.get();
+  }
+
+  // out = ax * x + [B x] - E C^-1 E^T x for a double or storage-precision vector.
+  template <class TV>
+  fg_status apply_reduced(PView<TV> x, double lambda, double ax, bool use_gram, TV* t, TV* out, double* partials,
+                          PcgState* pst) {
+    Layout L = layout();
+    const int* done = pst ? &pst->done : nullptr;
+    if (fast.enabled() && use_gram && ax == lambda) return fast.apply(*this, x, lambda, out, partials, pst);
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      if (nP) FG_LAUNCH((k_points<CW_, PW_, TS, TV>), grid_for(nP, 128), 128, 0, st, L, d_pt_edge_off.get(),
+                        d_pt_edge.get(), d_edges.get(), d_cross.get(), d_factors.get(), d_observed.get(), x, lambda, t,
+                        done);
+      if (nC) FG_LAUNCH((k_cams<CW_, PW_, TS, TV>), grid_for(nC * 32, NT), NT, 0, st, L, d_cam_edge_off.get(),
+                        d_cam_edge.get(), d_edges.get(), d_cross.get(), t, d_gram.get(), d_observed.get(), x, ax,
+                        (int)use_gram, out, partials, pst);
+    });
+    return FG_OK;
+  }
+
+  // PCG on S z = b (faer's CG restated, see kernels.cuh). b is a double
+  // retained vector; the solution lands in d_x (storage precision).
+  fg_status pcg(const double* b, double lambda, double rel_tol, size_t max_iters, unsigned* its, int* term,
+                double* rel_est) {
+    Layout L = layout();
+    PcgState* ps = d_pcg.get();
+    unsigned gvec = std::min<unsigned>(grid_for(retained, NT), 4 * nsm);
+    {
+      PcgState init{};
+      init.max_iterations = (unsigned)std::min<size_t>(max_iters, 0xffffffffu);
+      FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+      FG_CUDA(cudaStreamSynchronize(st));
+    }
+    FG_LAUNCH(k_pcg_init<TS>, gvec, NT, 0, st, (int64_t)retained, b, d_x.get(), d_r.get(), d_pp.get(),
+              d_partials.get(), ps, rel_tol);
+    unsigned gc = grid_for(std::max<size_t>(nC, 1), NT);
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      FG_LAUNCH((k_pcg_precond_init<CW_, TS, TS>), gc, NT, 0, st, L, d_r.get(), d_z.get(), precond_factors(),
+                d_observed.get(), lambda, d_partials.get(), ps);
+    });
+    double* tsum = d_partials.get() + 4 * 65536;
+    size_t launched = 0, batch = 4;
+    EventTimer tprod;
+    for (;;) {
+      FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+      FG_CUDA(cudaStreamSynchronize(st));
+      if (h_pcg.get()->done) break;
+      if (launched >= max_iters + 2) break;  // device enforces the limit; host bound is a guard
+      for (size_t k = 0; k < batch; ++k) {
+        PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
+        FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
+        FG_DISPATCH_WIDTHS(cw, pw, {
+          FG_LAUNCH((k_update<CW_, TS, TS>), gc, NT, 0, st, L, d_x.get(), d_r.get(), d_z.get(), d_pp.get(), d_q.get(),
+                    precond_factors(), d_observed.get(), lambda, d_partials.get(), ps);
+        });
+      }
+      launched += batch;
+      batch = std::min<size_t>(batch * 2, 64);
+    }
+    const PcgState& h = *h_pcg.get();
+    *its = h.iterations;
+    *term = h.done ? h.termination : FG_TERM_ITERATION_LIMIT;
+    *rel_est = h.bnorm > 0 ? std::sqrt(h.rr) / h.bnorm : 0.0;
+    return FG_OK;
+  }
+
+  fg_status solve_damped(double lambda, double* predicted, bool copy_to_host) override {
+    diag = fg_schur_diagnostics{};
+    diag.damping = lambda;
+    if (!ready || !std::isfinite(lambda) || lambda < 0) {
+      set_error("solve_damped requires prepare_damping and a finite nonnegative lambda");
+      return FG_INVALID_OPTIONS;
+    }
+    solves += 1;
+    EventTimer tf, tl, tv;
+    if (opt.collect_timings) tf.start(st);
+    unsigned fallbacks = 0;
+    FG_TRY(factor(lambda, &fallbacks));
+    if (fallbacks) {  // src/schur.rs:209-215
+      if (opt.collect_timings) tim.factorization += tf.stop(st);
+      diag.termination = FG_TERM_NOT_POSITIVE_DEFINITE;
+      set_error("local block factorization failed");
+      return FG_LINEAR_SOLVE_FAILED;
+    }
+    Layout L = layout();
+    // scaled_work = -g/D; eliminated part through C^-1; reduced rhs (src/schur.rs:216-242)
+    FG_TRY(launch_neg_scaled_gradient());
+    FG_TRY(launch_point_solve(lambda));
+    FG_TRY(launch_rhs());
+    if (opt.collect_timings) { tim.factorization += tf.stop(st); tl.start(st); }
+
+    unsigned its = 0;
+    int term = FG_TERM_NONE;
+    double est = 0;
+    size_t refinements = 0;
+    if (std::is_same<TS, double>::value) {
+      FG_TRY(pcg(d_rhs.get(), lambda, opt.relative_tolerance, opt.max_iterations, &its, &term, &est));
+      FG_TRY(launch_widen(d_x.get(), d_zred.get(), retained));
+      iterations += its;
+      diag.iterations = its;
+    } else {
+      FG_TRY(refine(lambda, &its, &term, &est, &refinements));
+    }
+    diag.termination = term;
+    diag.refinements = refinements;
+    if (term == FG_TERM_CONVERGED) {
+      diag.estimated_relative_residual = est;
+      diag.has_estimated = 1;
+    }
+    if (opt.collect_timings) { tim.linear_solve += tl.stop(st); tv.start(st); }
+    // recover step (src/schur.rs:312-344) and verify (src/schur.rs:346-397)
+    FG_TRY(launch_recover(lambda));
+    double pred = 0;
+    fg_status vs = verify(lambda, &pred);
+    if (opt.collect_timings) tim.verification += tv.stop(st);
+    if (vs != FG_OK) return vs;
+    if (copy_to_host) {
+      FG_CUDA(cudaMemcpyAsync(h_step.get(), d_step.get(), dim * sizeof(double), cudaMemcpyDeviceToHost, st));
+      FG_CUDA(cudaStreamSynchronize(st));
+    }
+    if (diag.termination != FG_TERM_CONVERGED) {
+      set_error("reduced CG did not converge");
+      return FG_LINEAR_SOLVE_FAILED;
+    }
+    *predicted = pred;
+    return FG_OK;
+  }
+
+  // FP32 bulk with FP64 outer refinement of the reduced system: each round
+  // forms res = b - S z in FP64 arithmetic, solves S d = res with FP32 PCG to
+  // refinement_inner_tolerance, and accumulates z += d in FP64.
+  fg_status refine(double lambda, unsigned* its_out, int* term_out, double* est_out, size_t* rounds) {
+    size_t budget = opt.max_iterations;
+    unsigned total = 0;
+    int term = FG_TERM_ITERATION_LIMIT;
+    double est = 0;
+    FG_CUDA(cudaMemsetAsync(d_zred.get(), 0, retained * sizeof(double), st));
+    double bnorm = 0;
+    FG_TRY(device_dot(d_rhs.get(), d_rhs.get(), retained, &bnorm));
+    bnorm = std::sqrt(bnorm);
+    size_t k = 0;
+    for (;; ++k) {
+      // res = b - S z (FP64 arithmetic); res stored in d_work[0..retained)
+      double rnorm = 0;
+      FG_TRY(reduced_residual_d(lambda, d_zred.get(), d_work.get(), &rnorm));
+      est = bnorm > 0 ? rnorm / bnorm : rnorm;
+      if (bnorm == 0 || est < opt.relative_tolerance) { term = FG_TERM_CONVERGED; break; }
+      if (k >= opt.max_refinements || budget == 0) { term = FG_TERM_ITERATION_LIMIT; break; }
+      unsigned its = 0;
+      int t = 0;
+      double e = 0;
+      double inner = std::max(opt.refinement_inner_tolerance, opt.relative_tolerance);
+      FG_TRY(pcg(d_work.get(), lambda, inner, budget, &its, &t, &e));
+      total += its;
+      budget = its >= budget ? 0 : budget - its;
+      if (t == FG_TERM_NOT_POSITIVE_DEFINITE) { term = t; break; }
+      FG_TRY(launch_axpy_widen(d_x.get(), d_zred.get(), retained));
+    }
+    iterations += total;
+    diag.iterations = total;
+    *its_out = total;
+    *term_out = term;
+    *est_out = est;
+    *rounds = k;
+    return FG_OK;
+  }
+
+  // ---- kernels launched by solve_damped (defined below as members)
+  fg_status launch_neg_scaled_gradient();
+  fg_status launch_point_solve(double lambda);
+  fg_status launch_rhs();
+  fg_status launch_widen(const TS* x, double* out, size_t n);
+  fg_status launch_axpy_widen(const TS* x, double* out, size_t n);
+  fg_status launch_recover(double lambda);
+  fg_status verify(double lambda, double* predicted);
+  fg_status device_dot(const double* a, const double* b, size_t n, double* out);
+  fg_status reduced_residual_d(double lambda, const double* z, double* res, double* rnorm);
+
+  // ------------------------------------------------------------- accessors
+  fg_status step_norm_inf(double* out) override { return device_norm_inf(d_step.get(), dim, out); }
+  const double* step_host() const override { return h_step.get(); }
+  const double* step_device() const override { return d_step.get(); }
+  size_t dimension() const override { return dim; }
+  void work(size_t* s, size_t* i) const override { *s = solves; *i = iterations; }
+  void diagnostics(fg_schur_diagnostics* d) const override { *d = diag; }
+  void timings(fg_schur_timings* t) const override { *t = tim; }
+  bool is_f32() const override { return !std::is_same<TS, double>::value; }
+  int device() const override { return dev; }
+  cudaStream_t stream() const override { return st; }
+  void* values_device() override { return d_values.get(); }
+  double* negres_device() override { return d_negres.get(); }
+  void mark_device_model(size_t nrows) override {
+    source = DEVICE_BAL;
+    rows = nrows;
+    device_model_current = true;
+    gradient_current = false;
+    ready = false;
+  }
+
+  fg_status bind_bal(uint64_t id, size_t cams, size_t pts, size_t obs, const uint32_t* ocam,
+                     const uint32_t* opt_) override {
+    if (cw != 9 || pw != 3) return FG_UNSUPPORTED_STRUCTURE;
+    if (retained != 9 * cams || dim != 9 * cams + 3 * pts) return FG_DIMENSION_MISMATCH;
+    if (bal_bound == id && structure_valid) return FG_OK;
+    // Emission order: one Frame batch per camera, factors in insertion order.
+    std::vector<HostBlock> blocks(2 * obs);
+    std::vector<HostEdge> edges(obs);
+    for (size_t k = 0; k < obs; ++k) {
+      blocks[2 * k] = {2 * k, 9 * (size_t)ocam[k], 2, 9, 24 * k};
+      blocks[2 * k + 1] = {2 * k, 9 * cams + 3 * (size_t)opt_[k], 2, 3, 24 * k + 18};
+      edges[k] = {9 * (size_t)ocam[k], 3 * (size_t)opt_[k], 2 * k, 2 * k + 1};
+    }
+    FG_TRY(build_structure(blocks, edges, 2 * obs));
+    up_blocks.clear();
+    up_edges.clear();
+    nvalues = 24 * obs;
+    FG_TRY(d_values.resize(std::max<size_t>(nvalues, 1)));
+    FG_TRY(d_negres.resize(std::max<size_t>(2 * obs, 1)));
+    bal_bound = id;
+    bal_obs = obs;
+    return FG_OK;
+  }
+
+  fg_status structure_sizes(size_t* nb, size_t* ne, size_t* nv, size_t* nvar, size_t* r, size_t* c) override {
+    FG_TRY(sync_model());
+    size_t vars = 0;
+    for (uint8_t o : h_observed) vars += o;
+    if (nb) *nb = nblocks;
+    if (ne) *ne = nedges;
+    if (nv) *nv = nvalues;
+    if (nvar) *nvar = vars;
+    if (r) *r = rows;
+    if (c) *c = dim;
+    return FG_OK;
+  }
+
+  fg_status export_structure(uint64_t* b5, uint64_t* e4, uint64_t* owners, uint64_t* v3) override {
+    FG_TRY(sync_model());
+    std::vector<DBlockMeta> mb(nblocks);
+    std::vector<DEdgeMeta> me(nedges);
+    if (nblocks) FG_CUDA(cudaMemcpy(mb.data(), d_blocks.get(), nblocks * sizeof(DBlockMeta), cudaMemcpyDeviceToHost));
+    if (nedges) FG_CUDA(cudaMemcpy(me.data(), d_edges.get(), nedges * sizeof(DEdgeMeta), cudaMemcpyDeviceToHost));
+    if (b5)
+      for (size_t i = 0; i < nblocks; ++i) {
+        b5[5 * i] = mb[i].row; b5[5 * i + 1] = mb[i].col; b5[5 * i + 2] = mb[i].rows;
+        b5[5 * i + 3] = mb[i].cols; b5[5 * i + 4] = mb[i].start;
+      }
+    if (e4)
+      for (size_t e = 0; e < nedges; ++e) {
+        e4[4 * e] = (uint64_t)me[e].cam * cw; e4[4 * e + 1] = (uint64_t)me[e].pt * pw;
+        e4[4 * e + 2] = me[e].lblk; e4[4 * e + 3] = me[e].rblk;
+      }
+    // First-appearance variable ids (block_factors.rs:52-87).
+    std::vector<uint64_t> own(dim, UINT64_MAX);
+    std::vector<uint64_t> vars;
+    for (size_t i = 0; i < nblocks; ++i) {
+      if (mb[i].cols == 0) continue;
+      size_t col = mb[i].col;
+      if (own[col] == UINT64_MAX) {
+        uint64_t id = vars.size() / 3;
+        size_t gstart = vars.empty() ? 0 : vars[vars.size() - 1] + vars[vars.size() - 2] * vars[vars.size() - 2];
+        vars.push_back(col); vars.push_back(mb[i].cols); vars.push_back(gstart);
+        for (size_t c = col; c < col + mb[i].cols; ++c) own[c] = id;
+      }
+    }
+    if (owners) std::copy(own.begin(), own.end(), owners);
+    if (v3) std::copy(vars.begin(), vars.end(), v3);
+    return FG_OK;
+  }
+
+  fg_status export_model(double* values, double* negres, double* g, double* scales, double* gram,
+                         double* cross) override {
+    FG_TRY(sync_model());
+    FG_CUDA(cudaStreamSynchronize(st));
+    auto fetch = [&](const TS* src, size_t n, double* dst) -> fg_status {
+      if (!dst || !n) return FG_OK;
+      std::vector<TS> tmp(n);
+      FG_CUDA(cudaMemcpy(tmp.data(), src, n * sizeof(TS), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < n; ++i) dst[i] = (double)tmp[i];
+      return FG_OK;
+    };
+    FG_TRY(fetch(d_values.get(), nvalues, values));
+    if (negres && rows) FG_CUDA(cudaMemcpy(negres, d_negres.get(), rows * sizeof(double), cudaMemcpyDeviceToHost));
+    if (g && dim) FG_CUDA(cudaMemcpy(g, d_g.get(), dim * sizeof(double), cudaMemcpyDeviceToHost));
+    if (scales && dim && ready) FG_CUDA(cudaMemcpy(scales, d_scales.get(), dim * sizeof(double), cudaMemcpyDeviceToHost));
+    if (gram && ready) {
+      // first-appearance order, packed w*w per variable
+      std::vector<uint64_t> v3;
+      size_t nvar = 0;
+      for (uint8_t o : h_observed) nvar += o;
+      v3.resize(3 * nvar);
+      FG_TRY(export_structure(nullptr, nullptr, nullptr, v3.data()));
+      size_t ng = nC * cw * cw + nP * pw * pw;
+      std::vector<double> all(ng);
+      FG_TRY(fetch(d_gram.get(), ng, all.data()));
+      for (size_t i = 0; i < nvar; ++i) {
+        size_t col = v3[3 * i], w = v3[3 * i + 1], start = v3[3 * i + 2];
+        size_t go = col < retained ? (col / cw) * cw * cw : nC * cw * cw + ((col - retained) / pw) * pw * pw;
+        for (size_t k = 0; k < w * w; ++k) gram[start + k] = all[go + k];
+      }
+    }
+    if (cross && ready) FG_TRY(fetch(d_cross.get(), nedges * cw * pw, cross));
+    return FG_OK;
+  }
+
+  fg_status time_operator(double lambda, size_t reps, double* seconds, double* bytes) override {
+    if (!ready) return FG_INVALID_OPTIONS;
+    unsigned fb = 0;
+    FG_TRY(factor(lambda, &fb));
+    FG_CUDA(cudaMemsetAsync(d_z.get(), 0, retained * sizeof(TS), st));
+    PView<TS> pv{d_z.get(), nullptr, nullptr};
+    FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), nullptr, nullptr));  // warm
+    cudaEvent_t a, b;
+    FG_CUDA(cudaEventCreate(&a));
+    FG_CUDA(cudaEventCreate(&b));
+    FG_CUDA(cudaEventRecord(a, st));
+    for (size_t k = 0; k < reps; ++k) FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), nullptr, nullptr));
+    FG_CUDA(cudaEventRecord(b, st));
+    FG_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *seconds = reps ? ms * 1e-3 / (double)reps : 0.0;
+    double s = (double)sizeof(TS);
+    // cross blocks + edge index, point factor (lower) + edge offset, camera Gram (lower) + x + y
+    *bytes = (double)nedges * (cw * pw * s + 4.0) + (double)nP * (pw * (pw + 1) / 2 * s + 4.0) +
+             (double)nC * (cw * (cw + 1) / 2 * s + 2.0 * cw * s);
+    return FG_OK;
+  }
+
+  fg_status reduced_apply(double lambda, const double* x, double* y) override {
+    if (!ready) return FG_INVALID_OPTIONS;
+    unsigned fb = 0;
+    FG_TRY(factor(lambda, &fb));
+    FG_CUDA(cudaMemcpyAsync(d_work.get(), x, retained * sizeof(double), cudaMemcpyHostToDevice, st));
+    PView<double> pv{d_work.get(), nullptr, nullptr};
+    FG_TRY(apply_reduced<double>(pv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr));
+    FG_CUDA(cudaMemcpyAsync(y, d_qd.get(), retained * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    return FG_OK;
+  }
+};
+
+}  // namespace fg
+
+#include "schur_solve.cuh"
+
+namespace fg {
+
+fg_status make_schur(size_t retained, size_t cw, size_t pw, const fg_schur_options& o, Backend** out) {
+  if (cw > (size_t)MAXW || pw > (size_t)MAXW) {
+    set_error("block widths above 16 are not supported");
+    return FG_INVALID_OPTIONS;
+  }
+  if (o.precision == FG_PRECISION_F32_REFINED) {
+    auto* b = new SchurImpl<float>(retained, cw, pw, o);
+    fg_status s = b->init();
+    if (s != FG_OK) { delete b; return s; }
+    *out = b;
+  } else if (o.precision == FG_PRECISION_F64) {
+    auto* b = new SchurImpl<double>(retained, cw, pw, o);
+    fg_status s = b->init();
+    if (s != FG_OK) { delete b; return s; }
+    *out = b;
+  } else {
+    set_error("unknown precision");
+    return FG_INVALID_OPTIONS;
+  }
+  return FG_OK;
+}
+
+}  // namespace fg

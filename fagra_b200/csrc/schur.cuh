@@ -1,0 +1,84 @@
+// Device Schur backend: the GPU implementation of fagra's `Schur` linear
+// backend (src/schur.rs) over a block-sparse linearization (src/linear_model.rs).
+#pragma once
+#include "common.cuh"
+
+namespace fg {
+
+// Jacobian block in the reference layout (src/linear_model.rs:12-19).
+struct DBlockMeta {
+  int64_t row, start, col;
+  int32_t rows, cols;
+};
+// Schur edge (src/schur.rs:93-99) with partition-local variable indices.
+struct DEdgeMeta {
+  int32_t cam, pt;  // retained / eliminated variable index
+  int64_t lblk, rblk;
+};
+struct HostBlock {
+  size_t row, col, rows, cols, start;
+};
+struct HostEdge {
+  size_t retained, eliminated, lblk, rblk;  // column offsets (partition local) + block ids
+};
+
+// PCG / verification scalars living on the device (one per backend).
+struct PcgState {
+  double rz, pq, alpha, beta, rr, bnorm, threshold;
+  double rz_new;
+  int done, termination;
+  unsigned iterations, max_iterations;
+  unsigned counter0, counter1, counter2, pad;
+};
+struct VerifyState {
+  double jd2;        // ||J delta||^2
+  double gd;         // g . delta
+  double nr2, g2;    // ||normal residual||^2, ||g||^2 (original coordinates)
+  double snr2, sg2;  // scaled by 1/D
+  double red2, rhs2; // ||S z - b||^2, ||b||^2
+  int nonfinite_step;
+  unsigned counter0, counter1, pad;
+};
+
+class Backend {
+ public:
+  virtual ~Backend() {}
+  virtual fg_status set_options(const fg_schur_options& o) = 0;
+  virtual fg_status prepare(size_t dimension) = 0;
+  virtual fg_status clear() = 0;
+  virtual fg_status accumulate(size_t rows, const double* r, size_t nb, const size_t* cols, const size_t* widths,
+                               const double* const* jac, const ptrdiff_t* rs, const ptrdiff_t* cs) = 0;
+  virtual fg_status gradient_norm(double* out) = 0;
+  virtual fg_status prepare_damping(double floor) = 0;
+  virtual fg_status solve_damped(double lambda, double* predicted, bool copy_to_host) = 0;
+  virtual fg_status step_norm_inf(double* out) = 0;
+  virtual const double* step_host() const = 0;
+  virtual const double* step_device() const = 0;
+  virtual size_t dimension() const = 0;
+  virtual void work(size_t* solves, size_t* iterations) const = 0;
+  virtual void diagnostics(fg_schur_diagnostics* d) const = 0;
+  virtual void timings(fg_schur_timings* t) const = 0;
+  virtual fg_status structure_sizes(size_t* nb, size_t* ne, size_t* nv, size_t* nvar, size_t* rows, size_t* cols) = 0;
+  virtual fg_status export_structure(uint64_t* b5, uint64_t* e4, uint64_t* owners, uint64_t* v3) = 0;
+  virtual fg_status export_model(double* values, double* negres, double* g, double* scales, double* gram,
+                                 double* cross) = 0;
+  virtual fg_status reduced_apply(double lambda, const double* x, double* y) = 0;
+  virtual fg_status time_operator(double lambda, size_t reps, double* seconds, double* bytes) = 0;
+  // Device BAL path: bind an implicit BAL structure and expose raw model storage.
+  virtual fg_status bind_bal(uint64_t problem_id, size_t cameras, size_t points, size_t observations,
+                             const uint32_t* order_cam, const uint32_t* order_pt) = 0;
+  virtual void* values_device() = 0;   // T*, packed Jacobian values
+  virtual double* negres_device() = 0;  // -r
+  virtual bool is_f32() const = 0;
+  virtual void mark_device_model(size_t rows) = 0;
+  virtual int device() const = 0;
+  virtual cudaStream_t stream() const = 0;
+};
+
+fg_status make_schur(size_t retained, size_t cw, size_t pw, const fg_schur_options& o, Backend** out);
+
+}  // namespace fg
+
+struct fg_backend {
+  fg::Backend* impl;
+};

@@ -1,0 +1,325 @@
+// Right-hand side, back-substitution and verification of one damped Schur
+// attempt (src/schur.rs:204-247, 312-397; src/linear_model.rs:233-282).
+#pragma once
+
+namespace fg {
+
+static __global__ void k_neg_scaled_gradient(int64_t n, const double* g, const double* d, double* out) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < n) out[j] = -g[j] / d[j];
+}
+
+// In place w_p = C_p^-1 w_p for every eliminated variable (block_factors.rs:178-204).
+template <int PW, class TS>
+static __global__ void k_point_solve(Layout L, const TS* factors, const uint8_t* observed, double* w, double lambda) {
+  int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (pt >= L.nP) return;
+  const int pw = PW ? PW : L.pw;
+  constexpr int PM = PW ? PW : MAXW;
+  double v[PM];
+  double* base = w + L.retained + pt * pw;
+  for (int p = 0; p < pw; ++p) v[p] = base[p];
+  int64_t var = L.nC + pt;
+  if (observed[var]) llt_solve<PW, TS, double>(factors + L.gram_offset(var), v, pw);
+  else if (lambda != 0) for (int p = 0; p < pw; ++p) v[p] /= lambda;
+  for (int p = 0; p < pw; ++p) base[p] = v[p];
+}
+
+template <class TS>
+static __global__ void k_widen(int64_t n, const TS* x, double* out, int accumulate) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < n) out[j] = accumulate ? out[j] + (double)x[j] : (double)x[j];
+}
+
+// z_p = C_p^-1 (-g_p/D_p - sum_e E_e^T z_c); step = z / D (src/schur.rs:312-344).
+template <int CW, int PW, class TS>
+static __global__ void k_recover_points(Layout L, const int64_t* pt_edge_off, const int64_t* pt_edge, const DEdgeMeta* edges,
+                                 const TS* cross, const TS* factors, const uint8_t* observed, const double* g,
+                                 const double* scales, const double* zred, double lambda, double* step) {
+  int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (pt >= L.nP) return;
+  const int cw = CW ? CW : L.cw, pw = PW ? PW : L.pw;
+  constexpr int PM = PW ? PW : MAXW;
+  double acc[PM];
+  int64_t base = L.retained + pt * pw;
+  for (int p = 0; p < pw; ++p) acc[p] = -g[base + p] / scales[base + p];
+  for (int64_t k = pt_edge_off[pt]; k < pt_edge_off[pt + 1]; ++k) {
+    int64_t e = pt_edge[k];
+    int64_t cam = edges[e].cam;
+    const TS* E = cross + e * (int64_t)cw * pw;
+    for (int p = 0; p < pw; ++p) {
+      double s = 0;
+      for (int c = 0; c < cw; ++c) s += (double)E[p * cw + c] * zred[cam * cw + c];
+      acc[p] -= s;
+    }
+  }
+  int64_t var = L.nC + pt;
+  if (observed[var]) llt_solve<PW, TS, double>(factors + L.gram_offset(var), acc, pw);
+  else if (lambda != 0) for (int p = 0; p < pw; ++p) acc[p] /= lambda;
+  for (int p = 0; p < pw; ++p) step[base + p] = acc[p] / scales[base + p];
+}
+
+static __global__ void k_step_cams(int64_t n, const double* zred, const double* scales, double* step) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < n) step[j] = zred[j] / scales[j];
+}
+
+// jd = J delta per emission (src/linear_model.rs:39-55); partial ||J delta||^2.
+template <class TS>
+static __global__ void k_jdelta(int64_t nemi, const int64_t* emi_off, const DBlockMeta* blocks, const TS* values,
+                         const double* delta, double* jd, double* partials, VerifyState* vs) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double s2 = 0;
+  if (e < nemi) {
+    int64_t b0 = emi_off[e], b1 = emi_off[e + 1];
+    if (b1 > b0) {
+      DBlockMeta f = blocks[b0];
+      for (int i = 0; i < f.rows; ++i) {
+        double y = 0;
+        for (int64_t b = b0; b < b1; ++b) {
+          DBlockMeta m = blocks[b];
+          const TS* v = values + m.start + i;
+          for (int j = 0; j < m.cols; ++j) y += (double)v[(int64_t)j * m.rows] * delta[m.col + j];
+        }
+        jd[f.row + i] = y;
+        s2 += y * y;
+      }
+    }
+  }
+  double v[1] = {s2};
+  block_sums<1>(v);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+  if (arrive_last(&vs->counter0)) {
+    double tot[1];
+    finish_sums<1>(partials, tot);
+    if (threadIdx.x == 0) {
+      vs->jd2 = tot[0];
+      vs->counter0 = 0;
+    }
+  }
+}
+
+// Full damped normal residual J^T (J delta + r) + lambda D^2 delta per
+// coordinate (src/linear_model.rs:254-281) with every norm the diagnostics need.
+template <class TS>
+static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
+                                  const TS* values, const double* jd, const double* negres, const double* g,
+                                  const double* scales, const double* delta, double lambda, double* partials,
+                                  VerifyState* vs) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (j < L.dim) {
+    int64_t v;
+    int off;
+    L.locate(j, &v, &off);
+    double nr = 0;
+    for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
+      DBlockMeta b = blocks[var_blk[k]];
+      const TS* col = values + b.start + (int64_t)off * b.rows;
+      double s = 0;
+      for (int i = 0; i < b.rows; ++i) s += (double)col[i] * (jd[b.row + i] - negres[b.row + i]);
+      nr += s;
+    }
+    double s = scales[j], d = delta[j];
+    nr += (lambda * (s * d)) * s;
+    double gj = g[j];
+    acc[0] = nr * nr;
+    acc[1] = gj * gj;
+    acc[2] = (nr / s) * (nr / s);
+    acc[3] = (gj / s) * (gj / s);
+    acc[4] = gj * d;
+    acc[5] = isfinite(d) ? 0.0 : 1.0;
+  }
+  block_sums<6>(acc);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 6; ++k) partials[6 * blockIdx.x + k] = acc[k];
+  if (arrive_last(&vs->counter1)) {
+    double tot[6];
+    finish_sums<6>(partials, tot);
+    if (threadIdx.x == 0) {
+      vs->nr2 = tot[0];
+      vs->g2 = tot[1];
+      vs->snr2 = tot[2];
+      vs->sg2 = tot[3];
+      vs->gd = tot[4];
+      vs->nonfinite_step = tot[5] != 0;
+      vs->counter1 = 0;
+    }
+  }
+}
+
+// res = rhs - q (or q - rhs with sign -1); sums ||res||^2 and ||rhs||^2 into out2.
+static __global__ void k_sub_norms(int64_t n, const double* q, const double* rhs, double sign, double* res, double* partials,
+                            unsigned* counter, double* out2) {
+  double a = 0, b = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double r = sign * (rhs[i] - q[i]);
+    if (res) res[i] = r;
+    a += r * r;
+    b += rhs[i] * rhs[i];
+  }
+  double v[2] = {a, b};
+  block_sums<2>(v);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = v[0];
+    partials[2 * blockIdx.x + 1] = v[1];
+  }
+  if (arrive_last(counter)) {
+    double tot[2];
+    finish_sums<2>(partials, tot);
+    if (threadIdx.x == 0) {
+      out2[0] = tot[0];
+      out2[1] = tot[1];
+      *counter = 0;
+    }
+  }
+}
+
+static __global__ void k_dot(int64_t n, const double* a, const double* b, double* partials, unsigned* counter, double* out) {
+  double s = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  double v[1] = {s};
+  block_sums<1>(v);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+  if (arrive_last(counter)) {
+    double tot[1];
+    finish_sums<1>(partials, tot);
+    if (threadIdx.x == 0) {
+      out[0] = tot[0];
+      *counter = 0;
+    }
+  }
+}
+
+template <class TS>
+fg_status SchurImpl<TS>::launch_neg_scaled_gradient() {
+  if (dim) FG_LAUNCH(k_neg_scaled_gradient, grid_for(dim, NT), NT, 0, st, (int64_t)dim, d_g.get(), d_scales.get(),
+                     d_work.get());
+  return FG_OK;
+}
+
+template <class TS>
+fg_status SchurImpl<TS>::launch_point_solve(double lambda) {
+  if (!nP) return FG_OK;
+  Layout L = layout();
+  FG_DISPATCH_WIDTHS(cw, pw, {
+    FG_LAUNCH((k_point_solve<PW_, TS>), grid_for(nP, 128), 128, 0, st, L, d_factors.get(), d_observed.get(),
+              d_work.get(), lambda);
+  });
+  return FG_OK;
+}
+
+template <class TS>
+fg_status SchurImpl<TS>::launch_rhs() {
+  if (!nC) return FG_OK;
+  Layout L = layout();
+  PView<double> w{d_work.get(), nullptr, nullptr};
+  FG_DISPATCH_WIDTHS(cw, pw, {
+    FG_LAUNCH((k_cams<CW_, PW_, TS, double>), grid_for(nC * 32, NT), NT, 0, st, L, d_cam_edge_off.get(),
+              d_cam_edge.get(), d_edges.get(), d_cross.get(), d_work.get() + retained, d_gram.get(),
+              d_observed.get(), w, 1.0, 0, d_rhs.get(), (double*)nullptr, (PcgState*)nullptr);
+  });
+  return FG_OK;
+}
+
+template <class TS>
+fg_status SchurImpl<TS>::launch_widen(const TS* x, double* out, size_t n) {
+  if (n) FG_LAUNCH(k_widen<TS>, grid_for(n, NT), NT, 0, st, (int64_t)n, x, out, 0);
+  return FG_OK;
+}
+template <class TS>
+fg_status SchurImpl<TS>::launch_axpy_widen(const TS* x, double* out, size_t n) {
+  if (n) FG_LAUNCH(k_widen<TS>, grid_for(n, NT), NT, 0, st, (int64_t)n, x, out, 1);
+  return FG_OK;
+}
+
+template <class TS>
+fg_status SchurImpl<TS>::launch_recover(double lambda) {
+  Layout L = layout();
+  if (retained) FG_LAUNCH(k_step_cams, grid_for(retained, NT), NT, 0, st, (int64_t)retained, d_zred.get(),
+                          d_scales.get(), d_step.get());
+  if (nP) {
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      FG_LAUNCH((k_recover_points<CW_, PW_, TS>), grid_for(nP, 128), 128, 0, st, L, d_pt_edge_off.get(),
+                d_pt_edge.get(), d_edges.get(), d_cross.get(), d_factors.get(), d_observed.get(), d_g.get(),
+                d_scales.get(), d_zred.get(), lambda, d_step.get());
+    });
+  }
+  return FG_OK;
+}
+
+template <class TS>
+fg_status SchurImpl<TS>::device_dot(const double* a, const double* b, size_t n, double* out) {
+  if (!n) { *out = 0; return FG_OK; }
+  unsigned g = std::min<unsigned>(grid_for(n, NT), 4 * nsm);
+  FG_LAUNCH(k_dot, g, NT, 0, st, (int64_t)n, a, b, d_partials.get(), d_counters.get() + 5, d_norm.get());
+  FG_CUDA(cudaMemcpyAsync(h_scalar.get(), d_norm.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  *out = h_scalar.get()[0];
+  return FG_OK;
+}
+
+// res = rhs - S z in FP64 arithmetic; returns ||res||.
+template <class TS>
+fg_status SchurImpl<TS>::reduced_residual_d(double lambda, const double* z, double* res, double* rnorm) {
+  if (!retained) { *rnorm = 0; return FG_OK; }
+  PView<double> pv{z, nullptr, nullptr};
+  FG_TRY(apply_reduced<double>(pv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr));
+  unsigned g = std::min<unsigned>(grid_for(retained, NT), 4 * nsm);
+  FG_LAUNCH(k_sub_norms, g, NT, 0, st, (int64_t)retained, d_qd.get(), d_rhs.get(), 1.0, res, d_partials.get(),
+            d_counters.get() + 6, d_norm.get());
+  FG_CUDA(cudaMemcpyAsync(h_scalar.get(), d_norm.get(), 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  *rnorm = std::sqrt(h_scalar.get()[0]);
+  return FG_OK;
+}
+
+// src/schur.rs:346-397 with src/linear_model.rs:254-282.
+template <class TS>
+fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
+  Layout L = layout();
+  VerifyState* vs = d_ver.get();
+  FG_CUDA(cudaMemsetAsync(vs, 0, sizeof(VerifyState), st));
+  double red2 = 0, rhs2 = 0;
+  if (retained) {
+    PView<double> pv{d_zred.get(), nullptr, nullptr};
+    FG_TRY(apply_reduced<double>(pv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr));
+    unsigned g = std::min<unsigned>(grid_for(retained, NT), 4 * nsm);
+    FG_LAUNCH(k_sub_norms, g, NT, 0, st, (int64_t)retained, d_qd.get(), d_rhs.get(), -1.0, (double*)nullptr,
+              d_partials.get(), d_counters.get() + 6, d_norm.get() + 2);
+  }
+  if (rows) FG_CUDA(cudaMemsetAsync(d_jd.get(), 0, rows * sizeof(double), st));
+  if (nemissions)
+    FG_LAUNCH(k_jdelta<TS>, grid_for(nemissions, NT), NT, 0, st, (int64_t)nemissions, d_emi_off.get(), d_blocks.get(),
+              d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
+  if (dim)
+    FG_LAUNCH(k_normal_residual<TS>, grid_for(dim, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(),
+              d_blocks.get(), d_values.get(), d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
+              lambda, d_partials.get() + 4 * 65536, vs);
+  FG_CUDA(cudaMemcpyAsync(h_ver.get(), vs, sizeof(VerifyState), cudaMemcpyDeviceToHost, st));
+  if (retained) FG_CUDA(cudaMemcpyAsync(h_scalar.get() + 2, d_norm.get() + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FG_CUDA(cudaStreamSynchronize(st));
+  if (retained) { red2 = h_scalar.get()[2]; rhs2 = h_scalar.get()[3]; }
+  const VerifyState& v = *h_ver.get();
+  auto rel = [](double n, double r) { return r == 0 ? n : n / r; };
+  diag.reduced_relative_residual = rel(std::sqrt(red2), std::sqrt(rhs2));
+  diag.has_reduced = 1;
+  diag.original_relative_residual = rel(std::sqrt(v.nr2), std::sqrt(v.g2));
+  diag.has_original = 1;
+  diag.scaled_relative_residual = rel(std::sqrt(v.snr2), std::sqrt(v.sg2));
+  diag.has_scaled = 1;
+  double pred = -v.gd - 0.5 * v.jd2;
+  bool bad = v.nonfinite_step || !std::isfinite(pred) || !std::isfinite(diag.reduced_relative_residual) ||
+             !std::isfinite(diag.original_relative_residual) || !std::isfinite(diag.scaled_relative_residual) ||
+             (diag.has_estimated && !std::isfinite(diag.estimated_relative_residual));
+  if (bad) {
+    diag.termination = FG_TERM_NONFINITE;
+    set_error("nonfinite step or residual");
+    return FG_LINEAR_SOLVE_FAILED;
+  }
+  *predicted = pred;
+  return FG_OK;
+}
+
+}  // namespace fg

@@ -1,0 +1,283 @@
+/*
+ * fagra_b200 — C ABI of a B200 (sm_100a) linear-solve and linearization backend
+ * for the fagra factor-graph library.
+ *
+ * Each entry point below replaces one method of fagra's statically dispatched
+ * linear-backend trait or one step of its optimizers; the citation beside it
+ * names the fagra source it stands in for (paths inside the fagra repository).
+ * A Rust `impl LeastSquaresBackend for GpuSchur` binds these symbols 1:1.
+ *
+ * Conventions
+ *  - Every call returns fg_status (0 = FG_OK); no call aborts the process.
+ *  - Scalars cross the boundary as double; FG_PRECISION_* selects the device
+ *    storage precision of the bulk data (Jacobians, blocks, Krylov vectors).
+ *  - A handle owns all of its device and pinned host buffers. Pointers handed
+ *    back (the step delta) borrow handle storage and stay valid until the next
+ *    call on that handle, as DampedStep<'_> borrows the backend in fagra.
+ *  - Calls on one handle are not thread-safe (fagra uses &mut self). All work
+ *    of one device runs on one library stream, see fg_device_stream().
+ */
+#ifndef FAGRA_B200_H
+#define FAGRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define FG_API extern "C" __attribute__((visibility("default")))
+#else
+#define FG_API __attribute__((visibility("default")))
+#endif
+
+/* src/error.rs:19-76 — SolverError and EvaluationError variants, one code each. */
+typedef enum {
+  FG_OK = 0,
+  FG_DUPLICATE_COVARIANCE_BLOCK = 1, /* SolverError::DuplicateCovarianceBlock */
+  FG_SINGULAR_INFORMATION = 2,       /* SolverError::SingularInformation */
+  FG_INVALID_INFORMATION = 3,        /* SolverError::InvalidInformation */
+  FG_INVALID_RANK_TOLERANCE = 4,     /* SolverError::InvalidRankTolerance */
+  FG_BATCH_NOT_EMPTY = 5,            /* SolverError::BatchNotEmpty */
+  FG_INVALID_OPTIONS = 6,            /* SolverError::InvalidOptions */
+  FG_KEY_ERROR = 7,                  /* SolverError::Key */
+  FG_LINEAR_SOLVE_FAILED = 8,        /* SolverError::LinearSolveFailed (LM retries) */
+  FG_NO_CONVERGENCE = 9,             /* SolverError::NoConvergence */
+  FG_NO_PROGRESS = 10,               /* SolverError::NoProgress */
+  FG_INVALID_EVALUATION = 20,        /* EvaluationError::InvalidEvaluation */
+  FG_DIMENSION_MISMATCH = 21,        /* EvaluationError::DimensionMismatch */
+  FG_INVALID_EMISSION = 22,          /* EvaluationError::InvalidEmission */
+  FG_UNSUPPORTED_STRUCTURE = 23,     /* EvaluationError::UnsupportedStructure */
+  FG_CUDA_ERROR = 40,                /* a CUDA runtime call failed; see fg_last_error() */
+  FG_OUT_OF_MEMORY = 41,             /* device or pinned allocation failed */
+  FG_DEVICE_TIMEOUT = 42,            /* a bounded device-side wait gave up */
+  FG_NULL_ARGUMENT = 43,             /* a required pointer argument was NULL */
+  FG_NO_DEVICE = 44                  /* no CUDA device (the product has no CPU fallback) */
+} fg_status;
+
+/* src/schur.rs:31-41 SchurTermination (+ 0 = None) */
+typedef enum {
+  FG_TERM_NONE = 0,
+  FG_TERM_CONVERGED = 1,
+  FG_TERM_ITERATION_LIMIT = 2,
+  FG_TERM_NOT_POSITIVE_DEFINITE = 3,
+  FG_TERM_NONFINITE = 4
+} fg_termination;
+
+typedef enum {
+  FG_PRECISION_F64 = 0,        /* everything in f64: the reference arithmetic */
+  FG_PRECISION_F32_REFINED = 1 /* f32 bulk; f64 dots, norms, cost and refinement residual */
+} fg_precision;
+
+typedef enum {
+  FG_PRECOND_RETAINED_BLOCKS = 0, /* (B + lambda I) block-Jacobi, src/schur.rs:658-682 */
+  FG_PRECOND_SCHUR_DIAGONAL = 1   /* exact 9x9 diagonal blocks of S (docs/schur-performance.md:155-159) */
+} fg_preconditioner;
+
+/* src/schur.rs:116-143 public fields, plus device-side choices. */
+typedef struct {
+  size_t max_iterations;     /* CG iteration limit per attempt; default 1000 */
+  double relative_tolerance; /* reduced-residual tolerance in [0,1); default max(1e-10, 128 eps) */
+  int collect_timings;       /* default 0 */
+  int precision;             /* fg_precision; default FG_PRECISION_F64 */
+  int preconditioner;        /* fg_preconditioner; default FG_PRECOND_RETAINED_BLOCKS */
+  int device;                /* CUDA device ordinal; default 0 */
+  double refinement_inner_tolerance; /* FP32 mode: relative tolerance of each inner solve; default 1e-4 */
+  size_t max_refinements;    /* FP32 mode: outer refinement limit; default 30 */
+} fg_schur_options;
+
+/* src/schur.rs:44-60 SchurDiagnostics (has_* = Some) */
+typedef struct {
+  int termination; /* fg_termination */
+  size_t iterations;
+  double damping;
+  double estimated_relative_residual;
+  double reduced_relative_residual;
+  double scaled_relative_residual;
+  double original_relative_residual;
+  int has_estimated, has_reduced, has_scaled, has_original;
+  size_t refinements; /* FP32 mode: outer refinement steps in this attempt */
+} fg_schur_diagnostics;
+
+/* src/schur.rs:75-91 SchurTimings, seconds, device event time. */
+typedef struct {
+  double preparation, factorization, linear_solve, products, preconditioner, verification;
+} fg_schur_timings;
+
+typedef struct fg_backend fg_backend;
+typedef struct fg_bal_problem fg_bal_problem;
+
+/* ---- library ---------------------------------------------------------- */
+FG_API const char* fg_version(void);
+FG_API const char* fg_last_error(void);   /* thread-local text of the last non-FG_OK status */
+FG_API fg_status fg_device_count(int* count);
+/* The CUDA stream every call on `device` runs on (cudaStream_t as void*). */
+FG_API fg_status fg_device_stream(int device, void** stream);
+/* Kernel launches issued by this library since load (all devices). */
+FG_API uint64_t fg_kernel_launches(void);
+
+/* ---- Schur backend: LeastSquaresBackend (src/optimization.rs:131-169) ---- */
+FG_API void fg_schur_default_options(fg_schur_options* out);
+/* Schur::new (src/schur.rs:149-178) */
+FG_API fg_status fg_schur_create(size_t retained_dimension, size_t retained_block_width,
+                                 size_t eliminated_block_width, const fg_schur_options* options,
+                                 fg_backend** out);
+FG_API void fg_backend_destroy(fg_backend* backend);
+/* Update the public fields (max_iterations, relative_tolerance, collect_timings,
+ * preconditioner) between calls, as Rust code assigns them (src/schur.rs:117-125). */
+FG_API fg_status fg_schur_set_options(fg_backend* backend, const fg_schur_options* options);
+/* LeastSquaresBackend::prepare (src/schur.rs:409-431) */
+FG_API fg_status fg_backend_prepare(fg_backend* backend, size_t dimension);
+/* LeastSquaresBackend::clear (src/schur.rs:432-437) */
+FG_API fg_status fg_backend_clear(fg_backend* backend);
+/* LeastSquaresBackend::accumulate (src/schur.rs:438-482, src/linear_model.rs:180-210).
+ * residual[rows]; block k has column offset cols[k], width widths[k] and its
+ * Jacobian element (i,j) at jacobians[k][i*row_strides[k] + j*col_strides[k]]. */
+FG_API fg_status fg_backend_accumulate(fg_backend* backend, size_t rows, const double* residual,
+                                       size_t nblocks, const size_t* cols, const size_t* widths,
+                                       const double* const* jacobians, const ptrdiff_t* row_strides,
+                                       const ptrdiff_t* col_strides);
+/* LeastSquaresBackend::gradient_norm (src/schur.rs:483-485) */
+FG_API fg_status fg_backend_gradient_norm(fg_backend* backend, double* out);
+/* LeastSquaresBackend::solve (src/schur.rs:486-489) */
+FG_API fg_status fg_backend_solve(fg_backend* backend, const double** delta, size_t* len);
+/* LeastSquaresBackend::prepare_damping (src/schur.rs:490-526) */
+FG_API fg_status fg_backend_prepare_damping(fg_backend* backend, double min_column_norm);
+/* LeastSquaresBackend::solve_damped (src/schur.rs:527-545). On FG_OK, *delta
+ * borrows a pinned host copy of the step (len = dimension). */
+FG_API fg_status fg_backend_solve_damped(fg_backend* backend, double lambda, const double** delta,
+                                         size_t* len, double* predicted_reduction);
+/* Device-resident variant: the step stays on the device (*delta_device is a
+ * device pointer of `dimension` doubles); no device-to-host copy. */
+FG_API fg_status fg_backend_solve_damped_device(fg_backend* backend, double lambda,
+                                                const double** delta_device,
+                                                double* predicted_reduction);
+/* LeastSquaresBackend::linear_solve_work (src/schur.rs:403-408) */
+FG_API fg_status fg_backend_linear_solve_work(const fg_backend* backend, size_t* solves,
+                                              size_t* iterations, int* available);
+/* Schur::diagnostics / Schur::timings (src/schur.rs:183-190) */
+FG_API fg_status fg_schur_get_diagnostics(const fg_backend* backend, fg_schur_diagnostics* out);
+FG_API fg_status fg_schur_get_timings(const fg_backend* backend, fg_schur_timings* out);
+
+/* Structure export for bit-exact index-map checks: sizes, then the maps in the
+ * reference's own layouts — Jacobian blocks {row,col,rows,cols,start}
+ * (src/linear_model.rs:12-19), Schur edges {retained,eliminated,
+ * retained_jacobian,eliminated_jacobian} (src/schur.rs:93-99), the owner map
+ * with first-appearance block ids (src/linear_model/block_factors.rs:52-87) and
+ * variable blocks {col,width,start}. Any output pointer may be NULL. */
+FG_API fg_status fg_schur_structure_sizes(fg_backend* backend, size_t* nblocks, size_t* nedges,
+                                          size_t* nvalues, size_t* nvariables, size_t* rows,
+                                          size_t* cols);
+FG_API fg_status fg_schur_export_structure(fg_backend* backend, uint64_t* blocks5, uint64_t* edges4,
+                                           uint64_t* owners, uint64_t* variables3);
+/* Model values in the reference layouts (f64 copies): packed Jacobian values,
+ * -r, gradient, column scales, Gram blocks (first-appearance order, column
+ * major) and cross blocks cross[(e*pw+p)*cw+c] (src/schur.rs:516). */
+FG_API fg_status fg_schur_export_model(fg_backend* backend, double* values, double* negative_residual,
+                                       double* gradient, double* scales, double* gram, double* cross);
+/* One application of the reduced operator S = lambda I + B - E C^-1 E^T
+ * (src/schur.rs:606-652) to a host vector x of length retained_dimension;
+ * requires prepare_damping. */
+FG_API fg_status fg_schur_reduced_apply(fg_backend* backend, double lambda, const double* x, double* y);
+
+/* ---- Device BAL problem: examples/bal/model.rs Frame + Reprojection ------ */
+/* Cameras are 9 doubles [w(3), t(3), f, k1, k2], points 3 doubles; observation
+ * i links obs_camera[i] and obs_point[i] with pixel obs_pixel[2i..2i+1].
+ * Observations are grouped into one Frame batch per camera in insertion order
+ * (src/optimization.rs:367-389), which fixes the emission order. */
+FG_API fg_status fg_bal_create(size_t cameras, size_t points, size_t observations,
+                               const double* camera_params, const double* point_params,
+                               const uint32_t* obs_camera, const uint32_t* obs_point,
+                               const double* obs_pixel, int device, fg_bal_problem** out);
+/* Same, from device-resident arrays (device pointers on `device`). */
+FG_API fg_status fg_bal_create_device(size_t cameras, size_t points, size_t observations,
+                                      const double* camera_params, const double* point_params,
+                                      const uint32_t* obs_camera, const uint32_t* obs_point,
+                                      const double* obs_pixel, int device, fg_bal_problem** out);
+FG_API void fg_bal_destroy(fg_bal_problem* problem);
+FG_API fg_status fg_bal_set_parameters(fg_bal_problem* problem, const double* camera_params,
+                                       const double* point_params);
+FG_API fg_status fg_bal_get_parameters(fg_bal_problem* problem, double* camera_params,
+                                       double* point_params);
+/* Frame::cost summed over frames (examples/bal/model.rs:201-213, src/optimization.rs:419-430) */
+FG_API fg_status fg_bal_cost(fg_bal_problem* problem, double* cost);
+/* Workspace::linearize for BAL frames (src/optimization.rs:229-265 +
+ * examples/bal/model.rs:214-236): residuals and Jacobians straight into the
+ * backend's block storage, in emission order. */
+FG_API fg_status fg_bal_linearize(fg_bal_problem* problem, fg_backend* backend);
+
+/* ---- Optimizers (src/optimization/levenberg_marquardt.rs, gauss_newton.rs) ---- */
+/* src/optimization.rs:40-84 */
+typedef struct {
+  size_t max_iterations;
+  double gradient_tolerance, step_tolerance, cost_tolerance;
+} fg_optimize_options;
+/* src/optimization/levenberg_marquardt.rs:17-46 */
+typedef struct {
+  double initial_damping, min_damping, max_damping, min_column_norm, acceptance_threshold;
+  size_t max_trials;
+} fg_lm_options;
+/* src/optimization.rs:86-112; termination: 1 NoVariables, 2 GradientTolerance,
+ * 3 StepTolerance, 4 CostTolerance */
+typedef struct {
+  size_t iterations;
+  double initial_cost, final_cost;
+  int termination;
+} fg_optimize_report;
+/* LmStatistics + LmWork (levenberg_marquardt.rs:84-173); last_rejection:
+ * 0 None, 1 LinearSolve, 2 Prediction, 3 InvalidEvaluation, 4 PoorAgreement */
+typedef struct {
+  size_t linearizations, attempts, rejected_steps, accepted_steps, cost_evaluations;
+  double damping, cost, gradient_norm, step_norm;
+  int has_cost, has_gradient_norm, has_step_norm, last_rejection;
+  size_t linear_solves, linear_iterations;
+  int linear_work_available;
+} fg_lm_statistics;
+/* on_accept observer (levenberg_marquardt.rs:208-210) */
+typedef void (*fg_accept_callback)(void* user, const fg_lm_statistics* statistics);
+
+FG_API void fg_optimize_default_options(fg_optimize_options* out);
+FG_API void fg_lm_default_options(fg_lm_options* out);
+
+/* LevenbergMarquardt::solve_batch_with_outcome on a device BAL problem. */
+FG_API fg_status fg_lm_solve_bal(fg_backend* backend, fg_bal_problem* problem,
+                                 const fg_optimize_options* options, const fg_lm_options* lm_options,
+                                 fg_optimize_report* report, fg_lm_statistics* statistics,
+                                 fg_accept_callback on_accept, void* user);
+/* Same LM, additionally stopping (termination 5, "CostTarget") as soon as an
+ * accepted cost is <= target_cost: the time-to-cost measurement of
+ * examples/bal.rs:14-34 (which records when the accepted cost first crosses a
+ * fraction of the initial cost) turned into a stop. */
+FG_API fg_status fg_lm_solve_bal_to_cost(fg_backend* backend, fg_bal_problem* problem,
+                                         const fg_optimize_options* options, const fg_lm_options* lm_options,
+                                         double target_cost, fg_optimize_report* report,
+                                         fg_lm_statistics* statistics);
+/* Reset the device parameters to the values the problem was created with. */
+FG_API fg_status fg_bal_restore_initial(fg_bal_problem* problem);
+/* Mean device time (CUDA events on the library stream) of one application of
+ * the reduced operator at `lambda`, over `repetitions` back-to-back calls;
+ * requires prepare_damping. bytes_out receives the algorithmic bytes one
+ * application must move (cross blocks, indices, point factors, camera Gram
+ * blocks, input and output vectors). */
+FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size_t repetitions,
+                                        double* seconds_per_apply, double* bytes_out);
+
+/* GaussNewton::solve_batch on a device BAL problem. */
+FG_API fg_status fg_gn_solve_bal(fg_backend* backend, fg_bal_problem* problem,
+                                 const fg_optimize_options* options, fg_optimize_report* report);
+
+/* Host-evaluated problems (any factor family): additive real coordinates of
+ * the given dimension; the caller evaluates cost at x and emits each residual
+ * through fg_backend_accumulate on the backend it is handed. */
+typedef struct {
+  size_t dimension;
+  int (*cost)(void* user, const double* x, double* out);
+  int (*linearize)(void* user, const double* x, fg_backend* backend);
+} fg_problem_callbacks;
+FG_API fg_status fg_lm_optimize(fg_backend* backend, const fg_problem_callbacks* problem, void* user,
+                                double* x, const fg_optimize_options* options,
+                                const fg_lm_options* lm_options, fg_optimize_report* report,
+                                fg_lm_statistics* statistics);
+FG_API fg_status fg_gn_optimize(fg_backend* backend, const fg_problem_callbacks* problem, void* user,
+                                double* x, const fg_optimize_options* options,
+                                fg_optimize_report* report);
+
+#endif /* FAGRA_B200_H */

@@ -1,0 +1,416 @@
+"""ORACLE — test infrastructure only.
+
+ctypes face of oracle/liboracle.so, the sequential f64 CPU restatement of
+fagra's hot path (see oracle.cpp for the per-function citations). Only the
+test suite, __graft_entry__.smoke() and bench.py's CPU-baseline legs use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+size_t = C.c_size_t
+ptrdiff_t = C.c_ssize_t
+dptr = C.POINTER(C.c_double)
+
+
+def _load():
+    if not LIB.exists():
+        from .build import build
+        build()
+    return C.CDLL(str(LIB))
+
+
+lib = _load()
+
+
+class Diag(C.Structure):
+    _fields_ = [("termination", C.c_int), ("iterations", size_t), ("damping", C.c_double),
+                ("estimated", C.c_double), ("reduced", C.c_double), ("scaled", C.c_double),
+                ("original", C.c_double), ("has_estimated", C.c_int), ("has_reduced", C.c_int),
+                ("has_scaled", C.c_int), ("has_original", C.c_int)]
+
+
+class OptOpts(C.Structure):
+    _fields_ = [("max_iterations", size_t), ("gradient_tolerance", C.c_double), ("step_tolerance", C.c_double),
+                ("cost_tolerance", C.c_double)]
+
+
+class LmOpts(C.Structure):
+    _fields_ = [("initial_damping", C.c_double), ("min_damping", C.c_double), ("max_damping", C.c_double),
+                ("min_column_norm", C.c_double), ("acceptance_threshold", C.c_double), ("max_trials", size_t)]
+
+
+class Report(C.Structure):
+    _fields_ = [("iterations", size_t), ("initial_cost", C.c_double), ("final_cost", C.c_double),
+                ("termination", C.c_int)]
+
+
+class LmStats(C.Structure):
+    _fields_ = [("linearizations", size_t), ("attempts", size_t), ("rejected_steps", size_t),
+                ("accepted_steps", size_t), ("cost_evaluations", size_t), ("damping", C.c_double),
+                ("cost", C.c_double), ("gradient_norm", C.c_double), ("step_norm", C.c_double),
+                ("has_cost", C.c_int), ("has_gradient_norm", C.c_int), ("has_step_norm", C.c_int),
+                ("last_rejection", C.c_int), ("linear_solves", size_t), ("linear_iterations", size_t)]
+
+
+ACCEPT = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LmStats))
+COST = C.CFUNCTYPE(C.c_int, C.c_void_p, dptr, dptr)
+LIN = C.CFUNCTYPE(C.c_int, C.c_void_p, dptr, C.c_void_p)
+
+_sig = {
+    "or_bal_project": (C.c_int, [dptr, dptr, dptr]),
+    "or_bal_jacobians": (None, [dptr, dptr, dptr, dptr]),
+    "or_rotation": (None, [dptr, dptr]),
+    "or_schur_create": (C.c_void_p, [size_t, size_t, size_t]),
+    "or_schur_destroy": (None, [C.c_void_p]),
+    "or_schur_set_limits": (None, [C.c_void_p, size_t, C.c_double]),
+    "or_schur_prepare": (C.c_int, [C.c_void_p, size_t]),
+    "or_schur_clear": (None, [C.c_void_p]),
+    "or_schur_accumulate": (C.c_int, [C.c_void_p, size_t, dptr, size_t, C.POINTER(size_t), C.POINTER(size_t),
+                                      C.POINTER(dptr), C.POINTER(ptrdiff_t), C.POINTER(ptrdiff_t)]),
+    "or_schur_gradient_norm": (C.c_int, [C.c_void_p, dptr]),
+    "or_schur_prepare_damping": (C.c_int, [C.c_void_p, C.c_double]),
+    "or_schur_solve_damped": (C.c_int, [C.c_void_p, C.c_double, dptr, dptr]),
+    "or_schur_solve": (C.c_int, [C.c_void_p, dptr]),
+    "or_schur_work": (None, [C.c_void_p, C.POINTER(size_t), C.POINTER(size_t)]),
+    "or_schur_diagnostics": (None, [C.c_void_p, C.POINTER(Diag)]),
+    "or_schur_sizes": (None, [C.c_void_p] + [C.POINTER(size_t)] * 7),
+    "or_schur_export": (None, [C.c_void_p] + [C.POINTER(size_t)] * 4 + [dptr] * 6),
+    "or_schur_reduced_apply": (None, [C.c_void_p, C.c_double, dptr, dptr]),
+    "or_schur_reduced_rhs": (None, [C.c_void_p, dptr]),
+    "or_model_create": (C.c_void_p, [size_t]),
+    "or_model_destroy": (None, [C.c_void_p]),
+    "or_model_accumulate": (C.c_int, [C.c_void_p, size_t, dptr, size_t, C.POINTER(size_t), C.POINTER(size_t),
+                                      C.POINTER(dptr), C.POINTER(ptrdiff_t), C.POINTER(ptrdiff_t)]),
+    "or_model_prepare_scales": (C.c_int, [C.c_void_p, C.c_double]),
+    "or_model_verify": (None, [C.c_void_p, dptr, C.c_double, dptr, dptr, dptr]),
+    "or_model_state": (None, [C.c_void_p, dptr, dptr]),
+    "or_blockfactors_run": (C.c_int, [size_t, size_t, size_t, C.POINTER(size_t), dptr, size_t, dptr, dptr, size_t,
+                                      C.POINTER(size_t)]),
+    "or_bal_create": (C.c_void_p, [size_t, size_t, size_t, dptr, dptr, C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_uint32), dptr]),
+    "or_bal_destroy": (None, [C.c_void_p]),
+    "or_bal_cost": (C.c_int, [C.c_void_p, dptr]),
+    "or_bal_get": (None, [C.c_void_p, dptr, dptr]),
+    "or_bal_order": (None, [C.c_void_p, C.POINTER(size_t)]),
+    "or_bal_linearize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "or_lm_bal": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(LmOpts), C.POINTER(Report),
+                            C.POINTER(LmStats), ACCEPT, C.c_void_p]),
+    "or_gn_bal": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(Report)]),
+    "or_cbproblem_create": (C.c_void_p, [size_t, dptr, COST, LIN, C.c_void_p]),
+    "or_cbproblem_destroy": (None, [C.c_void_p]),
+    "or_cbproblem_get": (None, [C.c_void_p, dptr]),
+    "or_cbproblem_emit": (C.c_int, [C.c_void_p, size_t, dptr, size_t, C.POINTER(size_t), C.POINTER(size_t),
+                                    C.POINTER(dptr), C.POINTER(ptrdiff_t), C.POINTER(ptrdiff_t)]),
+    "or_lm_cb": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(LmOpts), C.POINTER(Report),
+                           C.POINTER(LmStats)]),
+    "or_gn_cb": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(Report)]),
+}
+for _n, (_r, _a) in _sig.items():
+    _f = getattr(lib, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+TERM = {0: None, 1: "Converged", 2: "IterationLimit", 3: "NotPositiveDefinite", 4: "NonFinite"}
+
+
+def _dp(a):
+    return a.ctypes.data_as(dptr)
+
+
+def pack_blocks(residual, jacobians):
+    r = np.ascontiguousarray(np.asarray(residual, np.float64).reshape(-1))
+    blocks = [(int(c), np.asarray(j, np.float64)) for c, j in jacobians]
+    nb = len(blocks)
+    cols = (size_t * max(nb, 1))(*[c for c, _ in blocks])
+    widths = (size_t * max(nb, 1))()
+    ptrs = (dptr * max(nb, 1))()
+    rs = (ptrdiff_t * max(nb, 1))()
+    cs = (ptrdiff_t * max(nb, 1))()
+    keep = [r]
+    for k, (_, j) in enumerate(blocks):
+        j2 = j.reshape(len(r), -1) if j.ndim != 2 else j
+        keep.append(j2)
+        widths[k] = j2.shape[1]
+        ptrs[k] = j2.ctypes.data_as(dptr)
+        rs[k] = j2.strides[0] // 8
+        cs[k] = j2.strides[1] // 8
+    return (len(r), _dp(r), nb, cols, widths, ptrs, rs, cs), keep
+
+
+def project(cam, X):
+    cam = np.ascontiguousarray(cam, np.float64)
+    X = np.ascontiguousarray(X, np.float64)
+    pix = np.zeros(2)
+    st = lib.or_bal_project(_dp(cam), _dp(X), _dp(pix))
+    return pix, st
+
+
+def jacobians(cam, X):
+    cam = np.ascontiguousarray(cam, np.float64)
+    X = np.ascontiguousarray(X, np.float64)
+    jc = np.zeros(18)
+    jp = np.zeros(6)
+    lib.or_bal_jacobians(_dp(cam), _dp(X), _dp(jc), _dp(jp))
+    return jc.reshape(9, 2).T.copy(), jp.reshape(3, 2).T.copy()
+
+
+class Schur:
+    """Oracle Schur backend (src/schur.rs restated)."""
+
+    def __init__(self, retained, cw, pw):
+        self.h = lib.or_schur_create(retained, cw, pw)
+        self.retained, self.cw, self.pw = retained, cw, pw
+        self.max_iterations = 1000
+        self.relative_tolerance = max(1e-10, 128 * np.finfo(float).eps)
+        self.dim = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_schur_destroy(self.h)
+            self.h = None
+
+    def _limits(self):
+        lib.or_schur_set_limits(self.h, self.max_iterations, self.relative_tolerance)
+
+    def prepare(self, dim):
+        self._limits()
+        self.dim = dim
+        return lib.or_schur_prepare(self.h, dim)
+
+    def clear(self):
+        lib.or_schur_clear(self.h)
+
+    def accumulate(self, residual, jacobians):
+        args, keep = pack_blocks(residual, jacobians)
+        return lib.or_schur_accumulate(self.h, *args)
+
+    def gradient_norm(self):
+        out = C.c_double()
+        st = lib.or_schur_gradient_norm(self.h, C.byref(out))
+        return st, out.value
+
+    def prepare_damping(self, floor):
+        return lib.or_schur_prepare_damping(self.h, floor)
+
+    def solve_damped(self, lam):
+        self._limits()
+        d = np.zeros(self.dim)
+        p = C.c_double()
+        st = lib.or_schur_solve_damped(self.h, lam, _dp(d), C.byref(p))
+        return st, d, p.value
+
+    def solve(self):
+        self._limits()
+        d = np.zeros(self.dim)
+        st = lib.or_schur_solve(self.h, _dp(d))
+        return st, d
+
+    def work(self):
+        s, i = size_t(), size_t()
+        lib.or_schur_work(self.h, C.byref(s), C.byref(i))
+        return s.value, i.value
+
+    def diagnostics(self):
+        d = Diag()
+        lib.or_schur_diagnostics(self.h, C.byref(d))
+        o = lambda f, v: v if f else None  # noqa: E731
+        return dict(termination=TERM[d.termination], iterations=d.iterations, damping=d.damping,
+                    estimated=o(d.has_estimated, d.estimated), reduced=o(d.has_reduced, d.reduced),
+                    scaled=o(d.has_scaled, d.scaled), original=o(d.has_original, d.original))
+
+    def export(self):
+        sz = [size_t() for _ in range(7)]
+        lib.or_schur_sizes(self.h, *[C.byref(s) for s in sz])
+        nb, ne, nv, nvar, ngram, rows, cols = (s.value for s in sz)
+        b5 = np.zeros((max(nb, 1), 5), np.uint64)
+        e4 = np.zeros((max(ne, 1), 4), np.uint64)
+        own = np.zeros(max(cols, 1), np.uint64)
+        v3 = np.zeros((max(nvar, 1), 3), np.uint64)
+        vals, neg, g, sc = np.zeros(max(nv, 1)), np.zeros(max(rows, 1)), np.zeros(max(cols, 1)), np.zeros(max(cols, 1))
+        gram = np.zeros(max(ngram, 1))
+        cross = np.zeros(max(ne * self.cw * self.pw, 1))
+        sp = C.POINTER(size_t)
+        lib.or_schur_export(self.h, b5.ctypes.data_as(sp), e4.ctypes.data_as(sp), own.ctypes.data_as(sp),
+                            v3.ctypes.data_as(sp), _dp(vals), _dp(neg), _dp(g), _dp(sc), _dp(gram), _dp(cross))
+        return dict(blocks=b5[:nb], edges=e4[:ne], owners=own[:cols], variables=v3[:nvar], values=vals[:nv],
+                    negative_residual=neg[:rows], gradient=g[:cols], scales=sc[:cols], gram=gram[:ngram],
+                    cross=cross[:ne * self.cw * self.pw], rows=rows, cols=cols)
+
+    def reduced_apply(self, lam, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros_like(x)
+        lib.or_schur_reduced_apply(self.h, lam, _dp(x), _dp(y))
+        return y
+
+
+class Bal:
+    """Oracle BAL problem (examples/bal/model.rs Frame batches)."""
+
+    def __init__(self, cams, pts, oc, op, px):
+        self.cams = np.ascontiguousarray(np.asarray(cams, np.float64).reshape(-1, 9))
+        self.pts = np.ascontiguousarray(np.asarray(pts, np.float64).reshape(-1, 3))
+        self.oc = np.ascontiguousarray(np.asarray(oc, np.uint32))
+        self.op = np.ascontiguousarray(np.asarray(op, np.uint32))
+        self.px = np.ascontiguousarray(np.asarray(px, np.float64).reshape(-1, 2))
+        u32 = C.POINTER(C.c_uint32)
+        self.h = lib.or_bal_create(len(self.cams), len(self.pts), len(self.oc), _dp(self.cams), _dp(self.pts),
+                                   self.oc.ctypes.data_as(u32), self.op.ctypes.data_as(u32), _dp(self.px))
+
+    @classmethod
+    def from_data(cls, d):
+        return cls(d.cameras, d.points, d.obs_camera, d.obs_point, d.obs_pixel)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_bal_destroy(self.h)
+            self.h = None
+
+    def dimension(self):
+        return 9 * len(self.cams) + 3 * len(self.pts)
+
+    def cost(self):
+        out = C.c_double()
+        st = lib.or_bal_cost(self.h, C.byref(out))
+        return st, out.value
+
+    def parameters(self):
+        c = np.zeros_like(self.cams)
+        p = np.zeros_like(self.pts)
+        lib.or_bal_get(self.h, _dp(c), _dp(p))
+        return c, p
+
+    def linearize(self, schur: Schur):
+        return lib.or_bal_linearize(self.h, schur.h)
+
+    def lm(self, schur: Schur, max_iterations=20, gradient_tolerance=1e-8, step_tolerance=0.0, cost_tolerance=0.0,
+           lm_options=None, on_accept=None):
+        schur._limits()
+        o = OptOpts(max_iterations, gradient_tolerance, step_tolerance, cost_tolerance)
+        lo = LmOpts(*(lm_options or (1e-3, 1e-12, 1e12, 1e-6, 1e-4, 16)))
+        rep, st = Report(), LmStats()
+        cb = ACCEPT(lambda _u, s: on_accept(s.contents)) if on_accept else ACCEPT()
+        code = lib.or_lm_bal(schur.h, self.h, C.byref(o), C.byref(lo), C.byref(rep), C.byref(st), cb, None)
+        return code, rep, st
+
+    def gn(self, schur: Schur, max_iterations=20, gradient_tolerance=1e-8, step_tolerance=0.0, cost_tolerance=0.0):
+        schur._limits()
+        o = OptOpts(max_iterations, gradient_tolerance, step_tolerance, cost_tolerance)
+        rep = Report()
+        code = lib.or_gn_bal(schur.h, self.h, C.byref(o), C.byref(rep))
+        return code, rep
+
+
+class CallbackProblem:
+    """Host-evaluated problem for the oracle LM/GN (additive coordinates)."""
+
+    def __init__(self, x0, cost, linearize):
+        self.x0 = np.ascontiguousarray(np.asarray(x0, np.float64))
+        n = len(self.x0)
+
+        def cost_cb(_u, xp, out):
+            try:
+                out[0] = float(cost(np.ctypeslib.as_array(xp, shape=(n,)).copy() if n else np.zeros(0)))
+                return 0
+            except Exception as e:
+                return getattr(e, "code", 20)
+
+        def lin_cb(_u, xp, sink):
+            def emit(r, blocks):
+                args, keep = pack_blocks(r, blocks)
+                code = lib.or_cbproblem_emit(sink, *args)
+                if code:
+                    raise RuntimeError(code)
+            try:
+                linearize(np.ctypeslib.as_array(xp, shape=(n,)).copy() if n else np.zeros(0), emit)
+                return 0
+            except RuntimeError as e:
+                return int(e.args[0]) if e.args and isinstance(e.args[0], int) else 20
+            except Exception as e:
+                return getattr(e, "code", 20)
+
+        self._c = COST(cost_cb)
+        self._l = LIN(lin_cb)
+        self.h = lib.or_cbproblem_create(n, _dp(self.x0), self._c, self._l, None)
+        self.n = n
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_cbproblem_destroy(self.h)
+            self.h = None
+
+    @property
+    def x(self):
+        out = np.zeros(self.n)
+        lib.or_cbproblem_get(self.h, _dp(out))
+        return out
+
+    def lm(self, schur, max_iterations=50, gradient_tolerance=1e-8, step_tolerance=1e-10, cost_tolerance=1e-12,
+           lm_options=None):
+        schur._limits()
+        o = OptOpts(max_iterations, gradient_tolerance, step_tolerance, cost_tolerance)
+        lo = LmOpts(*(lm_options or (1e-3, 1e-12, 1e12, 1e-6, 1e-4, 16)))
+        rep, st = Report(), LmStats()
+        code = lib.or_lm_cb(schur.h, self.h, C.byref(o), C.byref(lo), C.byref(rep), C.byref(st))
+        return code, rep, st
+
+    def gn(self, schur, max_iterations=50, gradient_tolerance=1e-8, step_tolerance=1e-10, cost_tolerance=1e-12):
+        schur._limits()
+        o = OptOpts(max_iterations, gradient_tolerance, step_tolerance, cost_tolerance)
+        rep = Report()
+        code = lib.or_gn_cb(schur.h, self.h, C.byref(o), C.byref(rep))
+        return code, rep
+
+
+class Model:
+    """LinearizedModel alone (src/linear_model.rs) for its known-answer test."""
+
+    def __init__(self, dim):
+        self.h = lib.or_model_create(dim)
+        self.dim = dim
+        self.rows = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_model_destroy(self.h)
+            self.h = None
+
+    def accumulate(self, residual, jacobians):
+        args, keep = pack_blocks(residual, jacobians)
+        self.rows += args[0]
+        return lib.or_model_accumulate(self.h, *args)
+
+    def prepare_scales(self, floor):
+        return lib.or_model_prepare_scales(self.h, floor)
+
+    def verify(self, step, lam):
+        step = np.ascontiguousarray(step, np.float64)
+        out = np.zeros(4)
+        nr = np.zeros(self.dim)
+        ref = np.zeros(self.dim)
+        lib.or_model_verify(self.h, _dp(step), lam, _dp(out), _dp(nr), _dp(ref))
+        return dict(predicted=out[0], finite_step=bool(out[1]), residual_norm=out[2], reference_norm=out[3],
+                    normal_residual=nr, reference=ref)
+
+    def state(self):
+        g = np.zeros(self.dim)
+        neg = np.zeros(max(self.rows, 1))
+        lib.or_model_state(self.h, _dp(g), _dp(neg))
+        return g, neg[:self.rows]
+
+
+def block_factors_fallbacks(rows, cols, blocks5, values, scales, lambdas):
+    b5 = np.ascontiguousarray(np.asarray(blocks5, np.uint64).reshape(-1, 5)).astype(np.uint64)
+    vals = np.ascontiguousarray(np.asarray(values, np.float64))
+    sc = np.ascontiguousarray(np.asarray(scales, np.float64))
+    lam = np.ascontiguousarray(np.asarray(lambdas, np.float64))
+    out = np.zeros(len(lam), np.uint64)
+    sp = C.POINTER(size_t)
+    st = lib.or_blockfactors_run(rows, cols, len(b5), b5.ctypes.data_as(sp), _dp(vals), len(vals), _dp(sc),
+                                 _dp(lam), len(lam), out.ctypes.data_as(sp))
+    return st, [int(x) for x in out]

@@ -1,0 +1,31 @@
+"""Build the CPU oracle (test infrastructure): oracle/liboracle.so from oracle.cpp.
+
+The oracle is a plain f64 restatement of fagra's hot path used only as the
+checker by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs.
+"""
+from __future__ import annotations
+
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "oracle.cpp"
+OUT = HERE / "liboracle.so"
+
+
+def build(force: bool = False) -> Path:
+    if not force and OUT.exists() and OUT.stat().st_mtime >= SRC.stat().st_mtime:
+        return OUT
+    # -ffp-contract=off keeps the sequential f64 arithmetic free of fused
+    # multiply-adds, like the Rust reference.
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fopenmp",
+           str(SRC), "-o", str(OUT)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv))
