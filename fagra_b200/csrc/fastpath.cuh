@@ -1,22 +1,464 @@
-// Specialized reduced operator for BAL-shaped Schur systems (retained width 9,
-// eliminated width 3). Placeholder until the single-pass kernel lands: the
-// generic two-kernel operator is used while enabled() is false.
+// Single-pass reduced operator for BAL-shaped Schur systems (retained width 9,
+// eliminated width 3): y = lambda x + B x - E C^-1 E^T x with every cross
+// block read from HBM exactly once per application.
+//
+// Layout (rebuilt at prepare_damping): cross blocks in point-major order as
+// 28-word edge records [E (27, row p*9+c) | camera index + tile-local point
+// index], point records of 8 words [C^-1 packed lower (6) | tile-local first
+// edge | edge count], and tiles = contiguous point ranges holding at most TE
+// edges and TP points.
+//
+// k_fast_apply: one CTA per SM streams its tiles through shared memory with
+// cp.async.bulk (TMA, 1-D) into a two-stage mbarrier pipeline. Per tile:
+//   phase 1, thread per edge:  u_e = E_e^T x_cam            (x from L2)
+//   phase 2, thread per point: t_p = C_p^-1 sum_{e in p} u_e
+//   phase 3, thread per edge:  y_cam -= E_e t_p  (shared-memory atomics into a
+//                                                CTA-private 9C accumulator)
+// then flushes its accumulator to a per-CTA partial vector. No global atomics.
+// k_fast_reduce: q = lambda x + B x - sum_CTA partials, and the PCG step
+// length alpha from p.q in the last block.
 #pragma once
 #include "kernels.cuh"
+#include <vector>
 
 namespace fg {
 
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls and reports failure.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned limit) {
+  for (unsigned i = 0; i < limit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (i > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+template <class TS>
+struct RecWord;  // integer type filling the 28th word of an edge record
+template <>
+struct RecWord<float> {
+  using U = uint32_t;
+  __host__ __device__ static U pack(uint32_t cam, uint32_t lp) { return (cam & 0xFFFFFFu) | (lp << 24); }
+  __host__ __device__ static uint32_t cam(U w) { return w & 0xFFFFFFu; }
+  __host__ __device__ static uint32_t lp(U w) { return w >> 24; }
+};
+template <>
+struct RecWord<double> {
+  using U = uint64_t;
+  __host__ __device__ static U pack(uint32_t cam, uint32_t lp) { return (uint64_t)cam | ((uint64_t)lp << 32); }
+  __host__ __device__ static uint32_t cam(U w) { return (uint32_t)w; }
+  __host__ __device__ static uint32_t lp(U w) { return (uint32_t)(w >> 32); }
+};
+
+template <class TS>
+struct FastShape;  // tile geometry per storage precision (threads == edges per tile)
+template <>
+struct FastShape<float> {
+  static constexpr int TE = 512, TP = 256, NTHR = 512;
+};
+template <>
+struct FastShape<double> {
+  static constexpr int TE = 256, TP = 128, NTHR = 256;
+};
+
+// Edge records: rec[k] for point-major position k (edge pt_edge[k]).
+template <class TS>
+__global__ void k_fast_edge_records(int64_t nedges, const int64_t* pt_edge, const DEdgeMeta* edges,
+                                    const TS* cross, const uint32_t* local_point, TS* rec) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nedges * 28) return;
+  int64_t k = t / 28;
+  int w = (int)(t % 28);
+  int64_t e = pt_edge[k];
+  if (w < 27) {
+    rec[t] = cross[e * 27 + w];
+  } else {
+    using W = RecWord<TS>;
+    typename W::U word = W::pack((uint32_t)edges[e].cam, local_point[k]);
+    memcpy(&rec[t], &word, sizeof(word));
+  }
+}
+
+// Point records: packed lower C^-1 from the Cholesky factor L (C^-1 = L^-T L^-1),
+// plus the tile-local edge range (written once per structure, kept here).
+template <class TS>
+__global__ void k_fast_point_records(Layout L, const TS* factors, const uint8_t* observed, double lambda,
+                                     const uint32_t* local_first, const uint32_t* counts, TS* prec) {
+  int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (pt >= L.nP) return;
+  int64_t var = L.nC + pt;
+  double ci[6];
+  if (observed[var]) {
+    const TS* l = factors + L.gram_offset(var);  // column major 3x3 lower
+    double l00 = l[0], l10 = l[1], l20 = l[2], l11 = l[4], l21 = l[5], l22 = l[8];
+    // M = L^-1 (lower)
+    double m00 = 1.0 / l00, m11 = 1.0 / l11, m22 = 1.0 / l22;
+    double m10 = -l10 * m00 * m11;
+    double m21 = -l21 * m11 * m22;
+    double m20 = -(l20 * m00 + l21 * m10) * m22;
+    // C^-1 = M^T M, packed lower (00, 10, 20, 11, 21, 22)
+    ci[0] = m00 * m00 + m10 * m10 + m20 * m20;
+    ci[1] = m10 * m11 + m20 * m21;
+    ci[2] = m20 * m22;
+    ci[3] = m11 * m11 + m21 * m21;
+    ci[4] = m21 * m22;
+    ci[5] = m22 * m22;
+  } else {
+    double v = lambda != 0 ? 1.0 / lambda : 1.0;
+    ci[0] = v; ci[1] = 0; ci[2] = 0; ci[3] = v; ci[4] = 0; ci[5] = v;
+  }
+  TS* r = prec + pt * 8;
+  for (int i = 0; i < 6; ++i) r[i] = (TS)ci[i];
+  uint32_t a = local_first[pt], b = counts[pt];
+  if (sizeof(TS) == 4) {
+    memcpy(&r[6], &a, 4);
+    memcpy(&r[7], &b, 4);
+  } else {
+    uint64_t a8 = a, b8 = b;
+    memcpy(&r[6], &a8, 8);
+    memcpy(&r[7], &b8, 8);
+  }
+}
+
+template <class TS>
+__device__ __forceinline__ uint32_t rec_u32(const TS* p) {
+  if (sizeof(TS) == 4) {
+    uint32_t v;
+    memcpy(&v, p, 4);
+    return v;
+  }
+  uint64_t v;
+  memcpy(&v, p, 8);
+  return (uint32_t)v;
+}
+
+struct FastTiles {
+  const int64_t* pbeg;  // ntiles + 1
+  const int64_t* ebeg;  // ntiles + 1
+  int64_t ntiles;
+};
+
+template <class TS, class TV>
+struct FastSmem {
+  static constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP;
+  __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)TE * 28 * sizeof(TS) + (size_t)TP * 8 * sizeof(TS); }
+  static size_t bytes(int64_t ncam) {
+    size_t ys = (size_t)ncam * 9 * sizeof(TV);
+    ys = (ys + 127) & ~(size_t)127;
+    return ys + 2 * stage_bytes() + (size_t)TE * 3 * sizeof(TV) + (size_t)TP * 3 * sizeof(TV) + 64;
+  }
+};
+
+template <class TS, class TV>
+__global__ void __launch_bounds__(FastShape<TS>::NTHR, 1)
+    k_fast_apply(int64_t ncam, FastTiles tiles, const TS* erec, const TS* prec, const TV* x, TV* partials,
+                 const int* done, int* error) {
+  constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP, NTHR = FastShape<TS>::NTHR;
+  static_assert(TE == NTHR, "one edge per thread");
+  if (done && *done) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int tid = threadIdx.x;
+  const int64_t ny = ncam * 9;
+  size_t ys_bytes = ((size_t)ny * sizeof(TV) + 127) & ~(size_t)127;
+  TV* ys = reinterpret_cast<TV*>(smem);
+  unsigned char* stage_base = smem + ys_bytes;
+  const size_t sbytes = FastSmem<TS, TV>::stage_bytes();
+  TV* u = reinterpret_cast<TV*>(stage_base + 2 * sbytes);
+  TV* tp = u + TE * 3;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tp + TP * 3);
+
+  for (int64_t i = tid; i < ny; i += NTHR) ys[i] = 0;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  auto issue = [&](int64_t t, int s) {
+    int64_t e0 = tiles.ebeg[t], e1 = tiles.ebeg[t + 1], p0 = tiles.pbeg[t], p1 = tiles.pbeg[t + 1];
+    unsigned eb = (unsigned)((e1 - e0) * 28 * sizeof(TS)), pb = (unsigned)((p1 - p0) * 8 * sizeof(TS));
+    unsigned char* dst = stage_base + s * sbytes;
+    mbar_expect_tx(&bars[s], eb + pb);
+    if (eb) tma_load_1d(dst, erec + e0 * 28, eb, &bars[s]);
+    if (pb) tma_load_1d(dst + (size_t)TE * 28 * sizeof(TS), prec + p0 * 8, pb, &bars[s]);
+  };
+
+  const int64_t first = blockIdx.x, stride = gridDim.x;
+  if (tid == 0) {
+    if (first < tiles.ntiles) issue(first, 0);
+    if (first + stride < tiles.ntiles) issue(first + stride, 1);
+  }
+  bool failed = false;
+  int k = 0;
+  for (int64_t t = first; t < tiles.ntiles; t += stride, ++k) {
+    const int s = k & 1;
+    const unsigned parity = (k >> 1) & 1;
+    if (!mbar_wait_bounded(&bars[s], parity, 1u << 22)) {
+      failed = true;
+      break;
+    }
+    const TS* er = reinterpret_cast<const TS*>(stage_base + s * sbytes);
+    const TS* pr = er + (size_t)TE * 28;
+    const int ne = (int)(tiles.ebeg[t + 1] - tiles.ebeg[t]);
+    const int np = (int)(tiles.pbeg[t + 1] - tiles.pbeg[t]);
+    // phase 1: u_e = E_e^T x_cam
+    TV E[27];
+    uint32_t cam = 0, lp = 0;
+    if (tid < ne) {
+      const TS* rec = er + (size_t)tid * 28;
+#pragma unroll
+      for (int i = 0; i < 27; ++i) E[i] = (TV)rec[i];
+      uint32_t w = rec_u32<TS>(rec + 27);
+      if (sizeof(TS) == 4) {
+        cam = RecWord<float>::cam(w);
+        lp = RecWord<float>::lp(w);
+      } else {
+        uint64_t w8;
+        memcpy(&w8, rec + 27, 8);
+        cam = RecWord<double>::cam(w8);
+        lp = RecWord<double>::lp(w8);
+      }
+      TV xc[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) xc[c] = __ldg(x + (int64_t)cam * 9 + c);
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        TV acc = 0;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) acc += E[p * 9 + c] * xc[c];
+        u[tid * 3 + p] = acc;
+      }
+    }
+    __syncthreads();
+    // phase 2: t_p = C_p^-1 sum u
+    if (tid < np) {
+      const TS* r = pr + (size_t)tid * 8;
+      uint32_t f0 = rec_u32<TS>(r + 6), cnt = rec_u32<TS>(r + 7);
+      TV a0 = 0, a1 = 0, a2 = 0;
+      for (uint32_t e = f0; e < f0 + cnt; ++e) {
+        a0 += u[e * 3];
+        a1 += u[e * 3 + 1];
+        a2 += u[e * 3 + 2];
+      }
+      TV c0 = (TV)r[0], c1 = (TV)r[1], c2 = (TV)r[2], c3 = (TV)r[3], c4 = (TV)r[4], c5 = (TV)r[5];
+      tp[tid * 3] = c0 * a0 + c1 * a1 + c2 * a2;
+      tp[tid * 3 + 1] = c1 * a0 + c3 * a1 + c4 * a2;
+      tp[tid * 3 + 2] = c2 * a0 + c4 * a1 + c5 * a2;
+    }
+    __syncthreads();
+    // phase 3: y_cam -= E_e t_p
+    if (tid < ne) {
+      TV t0 = tp[lp * 3], t1 = tp[lp * 3 + 1], t2 = tp[lp * 3 + 2];
+      TV* y = ys + (int64_t)cam * 9;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
+    }
+    __syncthreads();  // stage s and u/tp free
+    if (tid == 0 && t + 2 * stride < tiles.ntiles) issue(t + 2 * stride, s);
+  }
+  if (failed) {
+    if (tid == 0) atomicExch(error, 1);
+    // drain: wait (bounded) for copies this CTA may still have in flight
+    for (int s = 0; s < 2; ++s) mbar_wait_bounded(&bars[s], ((k + s) >> 1) & 1, 1u << 16);
+  }
+  __syncthreads();
+  TV* out = partials + (int64_t)blockIdx.x * ny;
+  for (int64_t i = tid; i < ny; i += NTHR) out[i] = ys[i];
+}
+
+// q = lambda x + B x + sum_b partials[b]; optional p.q -> alpha (last block).
+template <class TS, class TV>
+__global__ void k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram, const uint8_t* observed,
+                              const TV* x, double lambda, TV* q, double* dparts, PcgState* st) {
+  if (st && st->done) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t ny = ncam * 9;
+  double dot = 0;
+  if (i < ny) {
+    int64_t cam = i / 9;
+    int r = (int)(i % 9);
+    TV v = (TV)lambda * x[i];
+    if (observed[cam]) {
+      const TS* g = gram + cam * 81;
+      const TV* xc = x + cam * 9;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        TS gv = j >= r ? g[r * 9 + j] : g[j * 9 + r];
+        v += (TV)gv * xc[j];
+      }
+    }
+    TV acc = 0;
+    for (int b = 0; b < nparts; ++b) acc += partials[(int64_t)b * ny + i];
+    v += acc;
+    q[i] = v;
+    dot = (double)x[i] * (double)v;
+  }
+  if (!st) return;
+  double s[1] = {dot};
+  block_sums<1>(s);
+  if (threadIdx.x == 0) dparts[blockIdx.x] = s[0];
+  if (arrive_last(&st->counter0)) {
+    double tot[1];
+    finish_sums<1>(dparts, tot);
+    if (threadIdx.x == 0) {
+      st->pq = tot[0];
+      if (!(tot[0] > 0)) {
+        st->done = 1;
+        st->termination = FG_TERM_NOT_POSITIVE_DEFINITE;
+      } else {
+        st->alpha = st->rz / tot[0];
+      }
+      st->counter0 = 0;
+    }
+  }
+}
+
 template <class TS>
 struct FastPath {
-  bool on = false;
-  bool enabled() const { return on; }
-  void invalidate() { on = false; }
+  bool on = false;          // records are current and the shape qualifies
+  bool structure = false;   // tiles and local indices built for the current structure
+  bool disabled = false;    // force the generic operator (tests)
+  int64_t ntiles = 0;
+  int grid = 0;
+  size_t smem = 0;
+  DBuf<int64_t> d_pbeg, d_ebeg;
+  DBuf<uint32_t> d_lp, d_lfirst, d_count;
+  DBuf<TS> d_erec, d_prec;
+  DBuf<float> d_parts_f;
+  DBuf<double> d_parts_d;
+  DBuf<int> d_error;
+
+  bool enabled() const { return on && !disabled; }
+  void invalidate() {
+    on = false;
+    structure = false;
+  }
+
+  // Tiles over point-major edges: greedy contiguous point ranges.
   template <class Impl>
-  fg_status prepare(Impl&) {
+  fg_status build(Impl& s, const std::vector<int64_t>& pt_off) {
+    constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP;
+    std::vector<int64_t> pbeg{0}, ebeg{0};
+    std::vector<uint32_t> lp(s.nedges), lfirst(s.nP), count(s.nP);
+    int64_t ecur = 0, pcur = 0;
+    for (int64_t p = 0; p < (int64_t)s.nP; ++p) {
+      int64_t c = pt_off[p + 1] - pt_off[p];
+      if (c > TE) return FG_OK;  // track longer than a tile: generic operator
+      if ((pt_off[p + 1] - ebeg.back()) > TE || (p + 1 - pbeg.back()) > TP) {
+        pbeg.push_back(p);
+        ebeg.push_back(pt_off[p]);
+      }
+      (void)ecur;
+      (void)pcur;
+    }
+    pbeg.push_back((int64_t)s.nP);
+    ebeg.push_back((int64_t)s.nedges);
+    ntiles = (int64_t)pbeg.size() - 1;
+    for (int64_t t = 0; t < ntiles; ++t)
+      for (int64_t p = pbeg[t]; p < pbeg[t + 1]; ++p) {
+        lfirst[p] = (uint32_t)(pt_off[p] - ebeg[t]);
+        count[p] = (uint32_t)(pt_off[p + 1] - pt_off[p]);
+        for (int64_t k = pt_off[p]; k < pt_off[p + 1]; ++k) lp[k] = (uint32_t)(p - pbeg[t]);
+      }
+    cudaStream_t st = s.st;
+    FG_TRY(upload(d_pbeg, pbeg.data(), pbeg.size(), st));
+    FG_TRY(upload(d_ebeg, ebeg.data(), ebeg.size(), st));
+    FG_TRY(upload(d_lp, lp.data(), lp.size(), st));
+    FG_TRY(upload(d_lfirst, lfirst.data(), lfirst.size(), st));
+    FG_TRY(upload(d_count, count.data(), count.size(), st));
+    FG_TRY(d_erec.resize(std::max<size_t>(s.nedges * 28, 1)));
+    FG_TRY(d_prec.resize(std::max<size_t>(s.nP * 8, 1)));
+    FG_TRY(d_error.resize(1));
+    FG_CUDA(cudaMemsetAsync(d_error.get(), 0, sizeof(int), st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    structure = true;
     return FG_OK;
   }
+
+  // Called at the end of prepare_damping: refresh edge records from the cross blocks.
+  template <class Impl>
+  fg_status prepare(Impl& s) {
+    on = false;
+    if (s.cw != 9 || s.pw != 3 || s.nC == 0 || s.nP == 0 || s.nedges == 0) return FG_OK;
+    size_t need = std::max(FastSmem<TS, double>::bytes((int64_t)s.nC), FastSmem<TS, TS>::bytes((int64_t)s.nC));
+    if (need > 220 * 1024) return FG_OK;  // accumulator does not fit one SM's shared memory
+    if (!structure) {
+      FG_TRY(build(s, s.h_pt_off));
+      if (!structure) return FG_OK;
+    }
+    FG_LAUNCH(k_fast_edge_records<TS>, grid_for(s.nedges * 28, 256), 256, 0, s.st, (int64_t)s.nedges,
+              s.d_pt_edge.get(), s.d_edges.get(), s.d_cross.get(), d_lp.get(), d_erec.get());
+    grid = sm_count(s.dev);
+    FG_TRY(d_parts_f.resize((size_t)grid * s.nC * 9));
+    FG_TRY(d_parts_d.resize((size_t)grid * s.nC * 9));
+    on = true;
+    return FG_OK;
+  }
+
+  // After each block factorization: refresh C^-1 in the point records.
+  template <class Impl>
+  fg_status refresh_points(Impl& s, double lambda) {
+    if (!on) return FG_OK;
+    FG_LAUNCH(k_fast_point_records<TS>, grid_for(s.nP, 256), 256, 0, s.st, s.layout(), s.d_factors.get(),
+              s.d_observed.get(), lambda, d_lfirst.get(), d_count.get(), d_prec.get());
+    return FG_OK;
+  }
+
+  // A bounded TMA wait that gave up leaves 1 in d_error.
+  template <class Impl>
+  fg_status check(Impl& s) {
+    if (!on) return FG_OK;
+    int h = 0;
+    FG_CUDA(cudaMemcpyAsync(&h, d_error.get(), sizeof(int), cudaMemcpyDeviceToHost, s.st));
+    FG_CUDA(cudaStreamSynchronize(s.st));
+    if (h) {
+      set_error("reduced operator: a bounded shared-memory pipeline wait timed out");
+      return FG_DEVICE_TIMEOUT;
+    }
+    return FG_OK;
+  }
+
   template <class Impl, class TV>
-  fg_status apply(Impl&, PView<TV>, double, TV*, double*, PcgState*) {
+  fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst) {
+    TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
+    size_t sm = FastSmem<TS, TV>::bytes((int64_t)s.nC);
+    auto kern = k_fast_apply<TS, TV>;
+    FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FastTiles tl{d_pbeg.get(), d_ebeg.get(), ntiles};
+    const int* done = pst ? &pst->done : nullptr;
+    FG_LAUNCH(kern, grid, FastShape<TS>::NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, parts,
+              done, d_error.get());
+    FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 256), 256, 0, s.st, (int64_t)s.nC, grid,
+              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, lambda, out, dparts, pst);
     return FG_OK;
   }
 };

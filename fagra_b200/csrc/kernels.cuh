@@ -88,9 +88,9 @@ struct Layout {
 // g = J^T r with r = -negres (src/linear_model.rs:199-207), per coordinate over
 // the variable's blocks in emission order.
 template <class TS>
-__global__ void k_gradient(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
-                           const TS* values, const double* negres, double* g) {
-  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void k_gradient(Layout L, int64_t j0, const int64_t* var_off, const int64_t* var_blk,
+                           const DBlockMeta* blocks, const TS* values, const double* negres, double* g) {
+  int64_t j = j0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= L.dim) return;
   int64_t v;
   int off;
@@ -108,9 +108,9 @@ __global__ void k_gradient(Layout L, const int64_t* var_off, const int64_t* var_
 
 // Column norms before flooring (src/linear_model.rs:211-224).
 template <class TS>
-__global__ void k_scales_raw(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
-                             const TS* values, double* scales) {
-  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void k_scales_raw(Layout L, int64_t j0, const int64_t* var_off, const int64_t* var_blk,
+                             const DBlockMeta* blocks, const TS* values, double* scales) {
+  int64_t j = j0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= L.dim) return;
   int64_t v;
   int off;
@@ -279,51 +279,6 @@ __global__ void k_factor(Layout L, int64_t first, int64_t count, int w_rt, const
   if (bad) atomicAdd(fallbacks, 1u);
 }
 
-// Exact diagonal blocks of the reduced system,
-// S_cc = lambda I + B_c - sum_{e in c} E_e C_p^-1 E_e^T, factored for the
-// Schur-diagonal preconditioner. One thread per retained variable; falls back
-// to the (B + lambda I) factor if S_cc does not factor.
-template <int CW, int PW, class TS>
-__global__ void k_schur_diag_factor(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge,
-                                    const DEdgeMeta* edges, const TS* cross, const uint8_t* observed,
-                                    const TS* gram, const TS* factors, TS* precond, double lambda) {
-  int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (cam >= L.nC) return;
-  const int cw = CW ? CW : L.cw, pw = PW ? PW : L.pw;
-  constexpr int CM = CW ? CW : MAXW;
-  constexpr int PM = PW ? PW : MAXW;
-  int64_t go = L.gram_offset(cam);
-  if (!observed[cam]) return;
-  double s[CM * CM];
-  for (int c = 0; c < cw; ++c)
-    for (int r = 0; r < cw; ++r) s[c * cw + r] = (r >= c ? (double)gram[go + c * cw + r] : 0.0) + (r == c ? lambda : 0.0);
-  for (int64_t k = cam_edge_off[cam]; k < cam_edge_off[cam + 1]; ++k) {
-    int64_t e = cam_edge[k];
-    int pt = edges[e].pt;
-    const TS* E = cross + e * (int64_t)cw * pw;
-    const TS* lc = factors + L.gram_offset(L.nC + pt);
-    // Y = C^-1 E^T columns: for each retained column c, y_c = C^-1 E[:, c]^T
-    double y[CM * PM];
-    for (int c = 0; c < cw; ++c) {
-      double b[PM];
-      for (int p = 0; p < pw; ++p) b[p] = (double)E[p * cw + c];
-      if (observed[L.nC + pt]) llt_solve<PW, TS, double>(lc, b, pw);
-      else if (lambda != 0) for (int p = 0; p < pw; ++p) b[p] /= lambda;
-      for (int p = 0; p < pw; ++p) y[c * pw + p] = b[p];
-    }
-    for (int c = 0; c < cw; ++c)
-      for (int r = c; r < cw; ++r) {
-        double acc = 0;
-        for (int p = 0; p < pw; ++p) acc += (double)E[p * cw + r] * y[c * pw + p];
-        s[c * cw + r] -= acc;
-      }
-  }
-  bool ok = chol_inplace<CW>(s, cw);
-  for (int c = 0; c < cw; ++c)
-    for (int r = 0; r < cw; ++r)
-      precond[go + c * cw + r] = ok ? (TS)(r >= c ? s[c * cw + r] : 0.0) : factors[go + c * cw + r];
-}
-
 // ---------------------------------------------------------------- vectors
 // A retained vector read either directly (pprev == nullptr) or as the PCG
 // search direction p = z + beta * p_prev.
@@ -451,11 +406,12 @@ __device__ __forceinline__ void precondition_one(const TS* pre, bool observed, d
   }
 }
 
-// PCG update for one retained variable per thread: p = z + beta p_prev;
-// x += alpha p; r -= alpha q; z = M^-1 r; partial r.r and r.z. The last block
-// counts the iteration and applies the stopping rules of faer's CG.
+// PCG update for one retained variable per thread: x += alpha p;
+// r -= alpha q; z = M^-1 r; partial r.r and r.z. The last block counts the
+// iteration, applies the stopping rules of faer's CG and forms the next
+// search direction p = z + beta p.
 template <int CW, class TS, class TV>
-__global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* pprev, const TV* q, const TS* pre,
+__global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* p, const TV* q, const TS* pre,
                          const uint8_t* observed, double lambda, double* partials, PcgState* st) {
   if (st->done) return;
   const int cw = CW ? CW : L.cw;
@@ -463,15 +419,13 @@ __global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* pprev, const TV* q, 
   int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double rr = 0, rz = 0;
   if (cam < L.nC) {
-    TV alpha = (TV)st->alpha, beta = (TV)st->beta;
+    TV alpha = (TV)st->alpha;
     TV rv[CM];
     for (int c = 0; c < cw; ++c) {
       int64_t i = cam * cw + c;
-      TV p = z[i] + beta * pprev[i];
-      x[i] += alpha * p;
+      x[i] += alpha * p[i];
       TV ri = r[i] - alpha * q[i];
       r[i] = ri;
-      pprev[i] = p;
       rv[c] = ri;
       rr += (double)ri * (double)ri;
     }
@@ -490,9 +444,12 @@ __global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* pprev, const TV* q, 
     partials[2 * blockIdx.x + 1] = s[1];
   }
   if (arrive_last(&st->counter1)) {
+    __shared__ int go_on;
+    __shared__ double beta_s;
     double tot[2];
     finish_sums<2>(partials, tot);
     if (threadIdx.x == 0) {
+      go_on = 0;
       st->iterations += 1;
       st->rr = tot[0];
       double rnorm = sqrt(tot[0]);
@@ -508,22 +465,32 @@ __global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* pprev, const TV* q, 
       } else {
         st->beta = tot[1] / st->rz;
         st->rz = tot[1];
+        beta_s = st->beta;
+        go_on = 1;
       }
       st->counter1 = 0;
+    }
+    __syncthreads();
+    if (go_on) {
+      TV b = (TV)beta_s;
+      int64_t n = (int64_t)L.nC * cw;
+      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        TV zi = ((volatile TV*)z)[i];
+        p[i] = zi + b * p[i];
+      }
     }
   }
 }
 
 // PCG start: r = b, x = 0, p_prev = 0, ||b|| and the threshold.
 template <class TV>
-__global__ void k_pcg_init(int64_t n, const double* b, TV* x, TV* r, TV* pprev, double* partials, PcgState* st,
+__global__ void k_pcg_init(int64_t n, const double* b, TV* x, TV* r, double* partials, PcgState* st,
                            double rel_tol) {
   double s = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     TV bi = (TV)b[i];
     r[i] = bi;
     x[i] = 0;
-    pprev[i] = 0;
     s += (double)bi * (double)bi;
   }
   double v[1] = {s};
@@ -551,9 +518,9 @@ __global__ void k_pcg_init(int64_t n, const double* b, TV* x, TV* r, TV* pprev, 
   }
 }
 
-// z = M^-1 r and rz = r.z at the start of CG.
+// z = M^-1 r, p = z and rz = r.z at the start of CG.
 template <int CW, class TS, class TV>
-__global__ void k_pcg_precond_init(Layout L, const TV* r, TV* z, const TS* pre, const uint8_t* observed,
+__global__ void k_pcg_precond_init(Layout L, const TV* r, TV* z, TV* p, const TS* pre, const uint8_t* observed,
                                    double lambda, double* partials, PcgState* st) {
   if (st->done) return;
   const int cw = CW ? CW : L.cw;
@@ -566,6 +533,7 @@ __global__ void k_pcg_precond_init(Layout L, const TV* r, TV* z, const TS* pre, 
     precondition_one<CW, TS, TV>(pre + L.gram_offset(cam), observed[cam], lambda, zv, cw);
     for (int c = 0; c < cw; ++c) {
       z[cam * cw + c] = zv[c];
+      p[cam * cw + c] = zv[c];
       rz += (double)r[cam * cw + c] * (double)zv[c];
     }
   }

@@ -2,6 +2,7 @@
 // numerical work on the device. Host code only validates emissions, stages
 // them (src/linear_model.rs:180-210 packing) and builds integer index maps.
 #include "kernels.cuh"
+#include "camside.cuh"
 #include "fastpath.cuh"
 #include <algorithm>
 #include <numeric>
@@ -73,7 +74,8 @@ class SchurImpl final : public Backend {
   DBuf<double> d_negres;
 
   // ---- numerics
-  DBuf<double> d_g, d_scales, d_work, d_rhs, d_zred, d_step, d_tmpd, d_qd, d_jd;
+  DBuf<double> d_g, d_scales, d_work, d_rhs, d_zred, d_step, d_tmpd, d_qd, d_jd, d_camjt;
+  std::vector<int64_t> h_pt_off;  // point -> first point-major edge (host copy)
   DBuf<TS> d_gram, d_factors, d_precond, d_cross;
   DBuf<TS> d_x, d_r, d_z, d_pp, d_q, d_t;  // PCG vectors in the storage precision
   DBuf<double> d_partials, d_norm;
@@ -149,6 +151,7 @@ class SchurImpl final : public Backend {
     FG_TRY(d_rhs.resize(retained));
     FG_TRY(d_zred.resize(retained));
     FG_TRY(d_qd.resize(retained));
+    FG_TRY(d_camjt.resize(retained));
     FG_TRY(h_step.resize(dim));
     FG_TRY(d_x.resize(retained));
     FG_TRY(d_r.resize(retained));
@@ -264,6 +267,7 @@ class SchurImpl final : public Backend {
     FG_TRY(upload(d_var_off, var_off.data(), var_off.size(), st));
     FG_TRY(upload(d_var_blk, var_blk.data(), var_blk.size(), st));
     FG_TRY(upload(d_pt_edge_off, pt_off.data(), pt_off.size(), st));
+    h_pt_off = pt_off;
     FG_TRY(upload(d_pt_edge, pt_e.data(), pt_e.size(), st));
     FG_TRY(upload(d_cam_edge_off, cam_off.data(), cam_off.size(), st));
     FG_TRY(upload(d_cam_edge, cam_e.data(), cam_e.size(), st));
@@ -325,8 +329,16 @@ class SchurImpl final : public Backend {
     }
     if (source == NONE) return FG_INVALID_OPTIONS;
     if (!gradient_current) {
-      if (dim) FG_LAUNCH(k_gradient<TS>, grid_for(dim, NT), NT, 0, st, layout(), d_var_off.get(), d_var_blk.get(),
-                         d_blocks.get(), d_values.get(), d_negres.get(), d_g.get());
+      Layout L = layout();
+      if (nC) {
+        FG_DISPATCH_WIDTHS(cw, pw, {
+          FG_LAUNCH((k_cam_jt<CW_, TS, CAM_GRADIENT>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(),
+                    d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), (const double*)nullptr, d_g.get());
+        });
+      }
+      if (dim > retained)
+        FG_LAUNCH(k_gradient<TS>, grid_for(dim - retained, NT), NT, 0, st, L, (int64_t)retained, d_var_off.get(),
+                  d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), d_g.get());
       gradient_current = true;
     }
     return FG_OK;
@@ -364,8 +376,16 @@ class SchurImpl final : public Backend {
     FG_TRY(sync_model());
     Layout L = layout();
     if (dim) {
-      FG_LAUNCH(k_scales_raw<TS>, grid_for(dim, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(), d_blocks.get(),
-                d_values.get(), d_scales.get());
+      if (nC) {
+        FG_DISPATCH_WIDTHS(cw, pw, {
+          FG_LAUNCH((k_cam_jt<CW_, TS, CAM_SQUARES>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(),
+                    d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), (const double*)nullptr,
+                    d_scales.get());
+        });
+      }
+      if (dim > retained)
+        FG_LAUNCH(k_scales_raw<TS>, grid_for(dim - retained, NT), NT, 0, st, L, (int64_t)retained, d_var_off.get(),
+                  d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get());
       double m;
       FG_TRY(device_norm_inf(d_scales.get(), dim, &m));
       FG_LAUNCH(k_floor, grid_for(dim, NT), NT, 0, st, (int64_t)dim, d_scales.get(), floor);
@@ -373,8 +393,12 @@ class SchurImpl final : public Backend {
     size_t ng = nC * cw * cw + nP * pw * pw;
     if (ng) {
       FG_CUDA(cudaMemsetAsync(d_gram.get(), 0, ng * sizeof(TS), st));
-      if (nC) FG_LAUNCH(k_gram<TS>, grid_for(nC * cw * cw, NT), NT, 0, st, L, (int64_t)0, (int64_t)nC, (int)cw,
-                        d_var_off.get(), d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
+      if (nC) {
+        FG_DISPATCH_WIDTHS(cw, pw, {
+          FG_LAUNCH((k_cam_gram<CW_, TS>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(),
+                    d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
+        });
+      }
       if (nP) FG_LAUNCH(k_gram<TS>, grid_for(nP * pw * pw, NT), NT, 0, st, L, (int64_t)nC, (int64_t)nP, (int)pw,
                         d_var_off.get(), d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
     }
@@ -405,11 +429,12 @@ class SchurImpl final : public Backend {
     *fallbacks = h_count.get()[0];
     if (*fallbacks == 0 && opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL && nC) {
       FG_DISPATCH_WIDTHS(cw, pw, {
-        FG_LAUNCH((k_schur_diag_factor<CW_, PW_, TS>), grid_for(nC, 64), 64, 0, st, L, d_cam_edge_off.get(),
+        FG_LAUNCH((k_cam_schur_diag<CW_, PW_, TS>), grid_for(nC * 32, 128), 128, 0, st, L, d_cam_edge_off.get(),
                   d_cam_edge.get(), d_edges.get(), d_cross.get(), d_observed.get(), d_gram.get(), d_factors.get(),
                   d_precond.get(), lambda);
       });
     }
+    if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
     return FG_OK;
   }
   const TS* precond_factors() const {
@@ -447,12 +472,12 @@ class SchurImpl final : public Backend {
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
       FG_CUDA(cudaStreamSynchronize(st));
     }
-    FG_LAUNCH(k_pcg_init<TS>, gvec, NT, 0, st, (int64_t)retained, b, d_x.get(), d_r.get(), d_pp.get(),
-              d_partials.get(), ps, rel_tol);
+    FG_LAUNCH(k_pcg_init<TS>, gvec, NT, 0, st, (int64_t)retained, b, d_x.get(), d_r.get(), d_partials.get(), ps,
+              rel_tol);
     unsigned gc = grid_for(std::max<size_t>(nC, 1), NT);
     FG_DISPATCH_WIDTHS(cw, pw, {
-      FG_LAUNCH((k_pcg_precond_init<CW_, TS, TS>), gc, NT, 0, st, L, d_r.get(), d_z.get(), precond_factors(),
-                d_observed.get(), lambda, d_partials.get(), ps);
+      FG_LAUNCH((k_pcg_precond_init<CW_, TS, TS>), gc, NT, 0, st, L, d_r.get(), d_z.get(), d_pp.get(),
+                precond_factors(), d_observed.get(), lambda, d_partials.get(), ps);
     });
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
@@ -463,7 +488,7 @@ class SchurImpl final : public Backend {
       if (h_pcg.get()->done) break;
       if (launched >= max_iters + 2) break;  // device enforces the limit; host bound is a guard
       for (size_t k = 0; k < batch; ++k) {
-        PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
+        PView<TS> pv{d_pp.get(), nullptr, nullptr};
         FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
         FG_DISPATCH_WIDTHS(cw, pw, {
           FG_LAUNCH((k_update<CW_, TS, TS>), gc, NT, 0, st, L, d_x.get(), d_r.get(), d_z.get(), d_pp.get(), d_q.get(),
@@ -473,6 +498,7 @@ class SchurImpl final : public Backend {
       launched += batch;
       batch = std::min<size_t>(batch * 2, 64);
     }
+    FG_TRY(fast.check(*this));
     const PcgState& h = *h_pcg.get();
     *its = h.iterations;
     *term = h.done ? h.termination : FG_TERM_ITERATION_LIMIT;
@@ -733,6 +759,7 @@ class SchurImpl final : public Backend {
     for (size_t k = 0; k < reps; ++k) FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), nullptr, nullptr));
     FG_CUDA(cudaEventRecord(b, st));
     FG_CUDA(cudaEventSynchronize(b));
+    FG_TRY(fast.check(*this));
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);

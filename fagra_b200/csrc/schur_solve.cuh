@@ -104,8 +104,8 @@ static __global__ void k_jdelta(int64_t nemi, const int64_t* emi_off, const DBlo
 template <class TS>
 static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
                                   const TS* values, const double* jd, const double* negres, const double* g,
-                                  const double* scales, const double* delta, double lambda, double* partials,
-                                  VerifyState* vs) {
+                                  const double* scales, const double* delta, double lambda, const double* camjt,
+                                  double* partials, VerifyState* vs) {
   int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   if (j < L.dim) {
@@ -113,7 +113,8 @@ static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const
     int off;
     L.locate(j, &v, &off);
     double nr = 0;
-    for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
+    if (camjt && j < L.retained) nr = camjt[j];
+    else for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
       DBlockMeta b = blocks[var_blk[k]];
       const TS* col = values + b.start + (int64_t)off * b.rows;
       double s = 0;
@@ -293,10 +294,16 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
   if (nemissions)
     FG_LAUNCH(k_jdelta<TS>, grid_for(nemissions, NT), NT, 0, st, (int64_t)nemissions, d_emi_off.get(), d_blocks.get(),
               d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
+  if (nC) {
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      FG_LAUNCH((k_cam_jt<CW_, TS, CAM_NORMAL>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(),
+                d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), d_jd.get(), d_camjt.get());
+    });
+  }
   if (dim)
     FG_LAUNCH(k_normal_residual<TS>, grid_for(dim, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(),
               d_blocks.get(), d_values.get(), d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
-              lambda, d_partials.get() + 4 * 65536, vs);
+              lambda, nC ? d_camjt.get() : (const double*)nullptr, d_partials.get() + 4 * 65536, vs);
   FG_CUDA(cudaMemcpyAsync(h_ver.get(), vs, sizeof(VerifyState), cudaMemcpyDeviceToHost, st));
   if (retained) FG_CUDA(cudaMemcpyAsync(h_scalar.get() + 2, d_norm.get() + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   FG_CUDA(cudaStreamSynchronize(st));
