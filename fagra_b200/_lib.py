@@ -25,8 +25,7 @@ class SchurOptions(C.Structure):
         ("precision", C.c_int),
         ("preconditioner", C.c_int),
         ("device", C.c_int),
-        ("refinement_inner_tolerance", C.c_double),
-        ("max_refinements", size_t),
+        ("residual_replacement", C.c_double),
     ]
 
 

@@ -96,8 +96,8 @@ class Schur:
                                lambda s, v: s._set("collect_timings", int(bool(v))))
     preconditioner = property(lambda s: {v: k for k, v in PRECONDITIONERS.items()}[s._get("preconditioner")],
                               lambda s, v: s._set("preconditioner", PRECONDITIONERS[v]))
-    refinement_inner_tolerance = property(lambda s: s._get("refinement_inner_tolerance"),
-                                          lambda s, v: s._set("refinement_inner_tolerance", v))
+    residual_replacement = property(lambda s: s._get("residual_replacement"),
+                                    lambda s, v: s._set("residual_replacement", v))
 
     @property
     def handle(self):

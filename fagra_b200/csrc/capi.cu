@@ -106,8 +106,7 @@ FG_API void fg_schur_default_options(fg_schur_options* o) {
   o->precision = FG_PRECISION_F64;
   o->preconditioner = FG_PRECOND_RETAINED_BLOCKS;
   o->device = 0;
-  o->refinement_inner_tolerance = 1e-4;
-  o->max_refinements = 30;
+  o->residual_replacement = 1e-2;
 }
 
 FG_API fg_status fg_schur_create(size_t retained, size_t cw, size_t pw, const fg_schur_options* options,

@@ -79,15 +79,16 @@ struct RecWord<double> {
 };
 
 template <class TS>
-struct FastShape;  // tile geometry per storage precision (threads == edges per tile)
+struct FastShape;  // tile geometry per storage precision: GT threads per group, one edge per thread
 template <>
 struct FastShape<float> {
-  static constexpr int TE = 512, TP = 256, NTHR = 512;
+  static constexpr int TE = 256, TP = 128, GT = 256;
 };
 template <>
 struct FastShape<double> {
-  static constexpr int TE = 256, TP = 128, NTHR = 256;
+  static constexpr int TE = 128, TP = 64, GT = 128;
 };
+constexpr int FAST_GROUPS = 2;  // independent tile pipelines per CTA sharing one accumulator
 
 // Edge records: rec[k] for point-major position k (edge pt_edge[k]).
 template <class TS>
@@ -169,36 +170,90 @@ struct FastTiles {
 template <class TS, class TV>
 struct FastSmem {
   static constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP;
-  __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)TE * 28 * sizeof(TS) + (size_t)TP * 8 * sizeof(TS); }
-  static size_t bytes(int64_t ncam) {
-    size_t ys = (size_t)ncam * 9 * sizeof(TV);
-    ys = (ys + 127) & ~(size_t)127;
-    return ys + 2 * stage_bytes() + (size_t)TE * 3 * sizeof(TV) + (size_t)TP * 3 * sizeof(TV) + 64;
+  __host__ __device__ static constexpr size_t stage_bytes() {
+    return (size_t)TE * 28 * sizeof(TS) + (size_t)TP * 8 * sizeof(TS);
+  }
+  __host__ __device__ static constexpr size_t vec_bytes(int64_t ncam) {
+    return ((size_t)ncam * 9 * sizeof(TV) + 127) & ~(size_t)127;
+  }
+  __host__ __device__ static constexpr size_t bytes(int64_t ncam, bool stage_x) {
+    return vec_bytes(ncam) * (stage_x ? 2 : 1) + FAST_GROUPS * 2 * stage_bytes() +
+           FAST_GROUPS * ((size_t)TE * 3 * sizeof(TV) + (size_t)TP * 3 * sizeof(TV)) + 64;
   }
 };
 
-template <class TS, class TV>
-__global__ void __launch_bounds__(FastShape<TS>::NTHR, 1)
-    k_fast_apply(int64_t ncam, FastTiles tiles, const TS* erec, const TS* prec, const TV* x, TV* partials,
-                 const int* done, int* error) {
-  constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP, NTHR = FastShape<TS>::NTHR;
-  static_assert(TE == NTHR, "one edge per thread");
-  if (done && *done) return;
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Loads the 27 cross values and the packed index word of one edge record with
+// 16-byte shared-memory loads.
+template <class TV>
+__device__ __forceinline__ void load_record(const float* rec, TV (&E)[27], uint32_t& cam, uint32_t& lp) {
+  const float4* v = reinterpret_cast<const float4*>(rec);
+  float f[28];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    float4 a = v[i];
+    f[4 * i] = a.x; f[4 * i + 1] = a.y; f[4 * i + 2] = a.z; f[4 * i + 3] = a.w;
+  }
+#pragma unroll
+  for (int i = 0; i < 27; ++i) E[i] = (TV)f[i];
+  uint32_t w = __float_as_uint(f[27]);
+  cam = RecWord<float>::cam(w);
+  lp = RecWord<float>::lp(w);
+}
+template <class TV>
+__device__ __forceinline__ void load_record(const double* rec, TV (&E)[27], uint32_t& cam, uint32_t& lp) {
+  const double2* v = reinterpret_cast<const double2*>(rec);
+  double f[28];
+#pragma unroll
+  for (int i = 0; i < 14; ++i) {
+    double2 a = v[i];
+    f[2 * i] = a.x; f[2 * i + 1] = a.y;
+  }
+#pragma unroll
+  for (int i = 0; i < 27; ++i) E[i] = (TV)f[i];
+  uint64_t w = (uint64_t)__double_as_longlong(f[27]);
+  cam = RecWord<double>::cam(w);
+  lp = RecWord<double>::lp(w);
+}
+
+// skip:  return at once when *skip != 0 (finished PCG)
+// gate:  return at once when *gate == 0 (conditional residual replacement)
+template <class TS, class TV, bool XS>
+__global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::GT, 1)
+    k_fast_apply(int64_t ncam, FastTiles tiles, const TS* erec, const TS* prec, const TV* z, const TV* pv,
+                 const double* beta, TV* partials, const int* skip, const int* gate, int* error) {
+  constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP, GT = FastShape<TS>::GT;
+  constexpr int NTHR = FAST_GROUPS * GT;
+  static_assert(TE == GT, "one edge per thread");
+  if (skip && *skip) return;
+  if (gate && !*gate) return;
   extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x;
+  const int g = tid / GT, gtid = tid % GT;
   const int64_t ny = ncam * 9;
-  size_t ys_bytes = ((size_t)ny * sizeof(TV) + 127) & ~(size_t)127;
+  const size_t vb = FastSmem<TS, TV>::vec_bytes(ncam);
   TV* ys = reinterpret_cast<TV*>(smem);
-  unsigned char* stage_base = smem + ys_bytes;
-  const size_t sbytes = FastSmem<TS, TV>::stage_bytes();
-  TV* u = reinterpret_cast<TV*>(stage_base + 2 * sbytes);
+  TV* xs = reinterpret_cast<TV*>(smem + vb);
+  unsigned char* stage_base = smem + vb * (XS ? 2 : 1);
+  constexpr size_t sbytes = FastSmem<TS, TV>::stage_bytes();
+  unsigned char* gstage = stage_base + (size_t)g * 2 * sbytes;
+  TV* u = reinterpret_cast<TV*>(stage_base + FAST_GROUPS * 2 * sbytes) + (size_t)g * (TE * 3 + TP * 3);
   TV* tp = u + TE * 3;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tp + TP * 3);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<TV*>(stage_base + FAST_GROUPS * 2 * sbytes) +
+                                               FAST_GROUPS * (TE * 3 + TP * 3));
+  uint64_t* gbar = bars + 2 * g;
 
-  for (int64_t i = tid; i < ny; i += NTHR) ys[i] = 0;
+  // x = z + beta p (PCG search direction formed on the fly) or x = z
+  const TV bv = pv ? (TV)*beta : (TV)0;
+  for (int64_t i = tid; i < ny; i += NTHR) {
+    ys[i] = 0;
+    if (XS) xs[i] = pv ? z[i] + bv * pv[i] : z[i];
+  }
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int i = 0; i < 2 * FAST_GROUPS; ++i) mbar_init(&bars[i], 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -206,14 +261,14 @@ __global__ void __launch_bounds__(FastShape<TS>::NTHR, 1)
   auto issue = [&](int64_t t, int s) {
     int64_t e0 = tiles.ebeg[t], e1 = tiles.ebeg[t + 1], p0 = tiles.pbeg[t], p1 = tiles.pbeg[t + 1];
     unsigned eb = (unsigned)((e1 - e0) * 28 * sizeof(TS)), pb = (unsigned)((p1 - p0) * 8 * sizeof(TS));
-    unsigned char* dst = stage_base + s * sbytes;
-    mbar_expect_tx(&bars[s], eb + pb);
-    if (eb) tma_load_1d(dst, erec + e0 * 28, eb, &bars[s]);
-    if (pb) tma_load_1d(dst + (size_t)TE * 28 * sizeof(TS), prec + p0 * 8, pb, &bars[s]);
+    unsigned char* dst = gstage + s * sbytes;
+    mbar_expect_tx(&gbar[s], eb + pb);
+    if (eb) tma_load_1d(dst, erec + e0 * 28, eb, &gbar[s]);
+    if (pb) tma_load_1d(dst + (size_t)TE * 28 * sizeof(TS), prec + p0 * 8, pb, &gbar[s]);
   };
 
-  const int64_t first = blockIdx.x, stride = gridDim.x;
-  if (tid == 0) {
+  const int64_t first = (int64_t)blockIdx.x * FAST_GROUPS + g, stride = (int64_t)gridDim.x * FAST_GROUPS;
+  if (gtid == 0) {
     if (first < tiles.ntiles) issue(first, 0);
     if (first + stride < tiles.ntiles) issue(first + stride, 1);
   }
@@ -222,46 +277,42 @@ __global__ void __launch_bounds__(FastShape<TS>::NTHR, 1)
   for (int64_t t = first; t < tiles.ntiles; t += stride, ++k) {
     const int s = k & 1;
     const unsigned parity = (k >> 1) & 1;
-    if (!mbar_wait_bounded(&bars[s], parity, 1u << 22)) {
+    if (!mbar_wait_bounded(&gbar[s], parity, 1u << 22)) {
       failed = true;
       break;
     }
-    const TS* er = reinterpret_cast<const TS*>(stage_base + s * sbytes);
+    const TS* er = reinterpret_cast<const TS*>(gstage + s * sbytes);
     const TS* pr = er + (size_t)TE * 28;
     const int ne = (int)(tiles.ebeg[t + 1] - tiles.ebeg[t]);
     const int np = (int)(tiles.pbeg[t + 1] - tiles.pbeg[t]);
     // phase 1: u_e = E_e^T x_cam
     TV E[27];
     uint32_t cam = 0, lp = 0;
-    if (tid < ne) {
-      const TS* rec = er + (size_t)tid * 28;
-#pragma unroll
-      for (int i = 0; i < 27; ++i) E[i] = (TV)rec[i];
-      uint32_t w = rec_u32<TS>(rec + 27);
-      if (sizeof(TS) == 4) {
-        cam = RecWord<float>::cam(w);
-        lp = RecWord<float>::lp(w);
-      } else {
-        uint64_t w8;
-        memcpy(&w8, rec + 27, 8);
-        cam = RecWord<double>::cam(w8);
-        lp = RecWord<double>::lp(w8);
-      }
+    if (gtid < ne) {
+      load_record<TV>(er + (size_t)gtid * 28, E, cam, lp);
       TV xc[9];
+      if (XS) {
 #pragma unroll
-      for (int c = 0; c < 9; ++c) xc[c] = __ldg(x + (int64_t)cam * 9 + c);
+        for (int c = 0; c < 9; ++c) xc[c] = xs[(int64_t)cam * 9 + c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          int64_t i = (int64_t)cam * 9 + c;
+          xc[c] = pv ? z[i] + bv * pv[i] : z[i];
+        }
+      }
 #pragma unroll
       for (int p = 0; p < 3; ++p) {
         TV acc = 0;
 #pragma unroll
         for (int c = 0; c < 9; ++c) acc += E[p * 9 + c] * xc[c];
-        u[tid * 3 + p] = acc;
+        u[gtid * 3 + p] = acc;
       }
     }
-    __syncthreads();
+    group_sync(1 + g, GT);
     // phase 2: t_p = C_p^-1 sum u
-    if (tid < np) {
-      const TS* r = pr + (size_t)tid * 8;
+    if (gtid < np) {
+      const TS* r = pr + (size_t)gtid * 8;
       uint32_t f0 = rec_u32<TS>(r + 6), cnt = rec_u32<TS>(r + 7);
       TV a0 = 0, a1 = 0, a2 = 0;
       for (uint32_t e = f0; e < f0 + cnt; ++e) {
@@ -270,57 +321,78 @@ __global__ void __launch_bounds__(FastShape<TS>::NTHR, 1)
         a2 += u[e * 3 + 2];
       }
       TV c0 = (TV)r[0], c1 = (TV)r[1], c2 = (TV)r[2], c3 = (TV)r[3], c4 = (TV)r[4], c5 = (TV)r[5];
-      tp[tid * 3] = c0 * a0 + c1 * a1 + c2 * a2;
-      tp[tid * 3 + 1] = c1 * a0 + c3 * a1 + c4 * a2;
-      tp[tid * 3 + 2] = c2 * a0 + c4 * a1 + c5 * a2;
+      tp[gtid * 3] = c0 * a0 + c1 * a1 + c2 * a2;
+      tp[gtid * 3 + 1] = c1 * a0 + c3 * a1 + c4 * a2;
+      tp[gtid * 3 + 2] = c2 * a0 + c4 * a1 + c5 * a2;
     }
-    __syncthreads();
+    group_sync(1 + g, GT);
     // phase 3: y_cam -= E_e t_p
-    if (tid < ne) {
+    if (gtid < ne) {
       TV t0 = tp[lp * 3], t1 = tp[lp * 3 + 1], t2 = tp[lp * 3 + 2];
       TV* y = ys + (int64_t)cam * 9;
 #pragma unroll
       for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
     }
-    __syncthreads();  // stage s and u/tp free
-    if (tid == 0 && t + 2 * stride < tiles.ntiles) issue(t + 2 * stride, s);
+    group_sync(1 + g, GT);  // stage s, u and tp free
+    if (gtid == 0 && t + 2 * stride < tiles.ntiles) issue(t + 2 * stride, s);
   }
   if (failed) {
-    if (tid == 0) atomicExch(error, 1);
-    // drain: wait (bounded) for copies this CTA may still have in flight
-    for (int s = 0; s < 2; ++s) mbar_wait_bounded(&bars[s], ((k + s) >> 1) & 1, 1u << 16);
+    if (gtid == 0) atomicExch(error, 1);
+    for (int s = 0; s < 2; ++s) mbar_wait_bounded(&gbar[s], ((k + s) >> 1) & 1, 1u << 16);
   }
   __syncthreads();
   TV* out = partials + (int64_t)blockIdx.x * ny;
   for (int64_t i = tid; i < ny; i += NTHR) out[i] = ys[i];
 }
 
-// q = lambda x + B x + sum_b partials[b]; optional p.q -> alpha (last block).
+// q = lambda x + B x + sum_b partials[b] with x = z (+ beta p); 32 coordinates
+// x 8 partial-vector chunks per block. Optional p.q -> alpha in the last block.
 template <class TS, class TV>
-__global__ void k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram, const uint8_t* observed,
-                              const TV* x, double lambda, TV* q, double* dparts, PcgState* st) {
+__global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram,
+                                                      const uint8_t* observed, const TV* z, const TV* pv,
+                                                      const double* beta, double lambda, TV* q, double* dparts,
+                                                      PcgState* st, const int* gate) {
   if (st && st->done) return;
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gate && !*gate) return;
+  __shared__ TV acc_s[8][33];
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
   const int64_t ny = ncam * 9;
-  double dot = 0;
+  const int64_t i = (int64_t)blockIdx.x * 32 + lx;
+  TV acc = 0;
   if (i < ny) {
+    int b = ly;
+    for (; b + 24 < nparts; b += 32) {
+      TV a0 = partials[(int64_t)b * ny + i], a1 = partials[(int64_t)(b + 8) * ny + i];
+      TV a2 = partials[(int64_t)(b + 16) * ny + i], a3 = partials[(int64_t)(b + 24) * ny + i];
+      acc += (a0 + a1) + (a2 + a3);
+    }
+    for (; b < nparts; b += 8) acc += partials[(int64_t)b * ny + i];
+  }
+  acc_s[ly][lx] = acc;
+  __syncthreads();
+  double dot = 0;
+  if (ly == 0 && i < ny) {
+    TV sum = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sum += acc_s[k][lx];
+    const TV bv = pv ? (TV)*beta : (TV)0;
     int64_t cam = i / 9;
     int r = (int)(i % 9);
-    TV v = (TV)lambda * x[i];
+    TV xi = pv ? z[i] + bv * pv[i] : z[i];
+    TV v = (TV)lambda * xi;
     if (observed[cam]) {
       const TS* g = gram + cam * 81;
-      const TV* xc = x + cam * 9;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
+        int64_t k = cam * 9 + j;
+        TV xj = pv ? z[k] + bv * pv[k] : z[k];
         TS gv = j >= r ? g[r * 9 + j] : g[j * 9 + r];
-        v += (TV)gv * xc[j];
+        v += (TV)gv * xj;
       }
     }
-    TV acc = 0;
-    for (int b = 0; b < nparts; ++b) acc += partials[(int64_t)b * ny + i];
-    v += acc;
+    v += sum;
     q[i] = v;
-    dot = (double)x[i] * (double)v;
+    dot = (double)xi * (double)v;
   }
   if (!st) return;
   double s[1] = {dot};
@@ -409,8 +481,10 @@ struct FastPath {
   fg_status prepare(Impl& s) {
     on = false;
     if (s.cw != 9 || s.pw != 3 || s.nC == 0 || s.nP == 0 || s.nedges == 0) return FG_OK;
-    size_t need = std::max(FastSmem<TS, double>::bytes((int64_t)s.nC), FastSmem<TS, TS>::bytes((int64_t)s.nC));
-    if (need > 220 * 1024) return FG_OK;  // accumulator does not fit one SM's shared memory
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    size_t need = std::max(FastSmem<TS, double>::bytes((int64_t)s.nC, false), FastSmem<TS, TS>::bytes((int64_t)s.nC, false));
+    if (need > (size_t)optin) return FG_OK;  // accumulator does not fit one SM's shared memory
     if (!structure) {
       FG_TRY(build(s, s.h_pt_off));
       if (!structure) return FG_OK;
@@ -447,18 +521,33 @@ struct FastPath {
     return FG_OK;
   }
 
+  // out = lambda x + B x - E C^-1 E^T x. pst != nullptr: PCG step (skips when
+  // finished, computes alpha). gate != nullptr: runs only while *gate != 0.
   template <class Impl, class TV>
-  fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst) {
+  fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst,
+                  const int* gate = nullptr) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
-    size_t sm = FastSmem<TS, TV>::bytes((int64_t)s.nC);
-    auto kern = k_fast_apply<TS, TV>;
-    FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    bool xs = FastSmem<TS, TV>::bytes((int64_t)s.nC, true) <= (size_t)optin;
+    size_t sm = FastSmem<TS, TV>::bytes((int64_t)s.nC, xs);
     FastTiles tl{d_pbeg.get(), d_ebeg.get(), ntiles};
-    const int* done = pst ? &pst->done : nullptr;
-    FG_LAUNCH(kern, grid, FastShape<TS>::NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, parts,
-              done, d_error.get());
-    FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 256), 256, 0, s.st, (int64_t)s.nC, grid,
-              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, lambda, out, dparts, pst);
+    const int* skip = pst ? &pst->done : nullptr;
+    constexpr int NTHR = FAST_GROUPS * FastShape<TS>::GT;
+    if (xs) {
+      auto kern = k_fast_apply<TS, TV, true>;
+      FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
+                parts, skip, gate, d_error.get());
+    } else {
+      auto kern = k_fast_apply<TS, TV, false>;
+      FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
+                parts, skip, gate, d_error.get());
+    }
+    FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
+              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, out, dparts, pst,
+              gate);
     return FG_OK;
   }
 };

@@ -295,8 +295,9 @@ struct PView {
 template <int CW, int PW, class TS, class TV>
 __global__ void k_points(Layout L, const int64_t* pt_edge_off, const int64_t* pt_edge, const DEdgeMeta* edges,
                          const TS* cross, const TS* factors, const uint8_t* observed, PView<TV> x, double lambda,
-                         TV* t, const int* done) {
+                         TV* t, const int* done, const int* gate) {
   if (done && *done) return;
+  if (gate && !*gate) return;
   int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (pt >= L.nP) return;
   const int cw = CW ? CW : L.cw, pw = PW ? PW : L.pw;
@@ -331,8 +332,9 @@ __global__ void k_points(Layout L, const int64_t* pt_edge_off, const int64_t* pt
 template <int CW, int PW, class TS, class TV>
 __global__ void k_cams(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge, const DEdgeMeta* edges,
                        const TS* cross, const TV* t, const TS* gram, const uint8_t* observed, PView<TV> x, double ax,
-                       int use_gram, TV* q, double* partials, PcgState* st) {
+                       int use_gram, TV* q, double* partials, PcgState* st, const int* gate) {
   if (st && st->done) return;
+  if (gate && !*gate) return;
   const int cw = CW ? CW : L.cw, pw = PW ? PW : L.pw;
   constexpr int CM = CW ? CW : MAXW;
   int lane = threadIdx.x & 31;
@@ -396,46 +398,84 @@ __global__ void k_cams(Layout L, const int64_t* cam_edge_off, const int64_t* cam
   }
 }
 
-// Apply the retained block preconditioner z = M^-1 r for one variable.
-template <int CW, class TS, class TV>
-__device__ __forceinline__ void precondition_one(const TS* pre, bool observed, double lambda, TV* r, int cw) {
-  if (observed) {
-    llt_solve<CW, TS, TV>(pre, r, cw);
-  } else if (lambda != 0) {
-    for (int c = 0; c < cw; ++c) r[c] /= (TV)lambda;
-  }
-}
-
-// PCG update for one retained variable per thread: x += alpha p;
-// r -= alpha q; z = M^-1 r; partial r.r and r.z. The last block counts the
-// iteration, applies the stopping rules of faer's CG and forms the next
-// search direction p = z + beta p.
-template <int CW, class TS, class TV>
-__global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* p, const TV* q, const TS* pre,
-                         const uint8_t* observed, double lambda, double* partials, PcgState* st) {
-  if (st->done) return;
+// ---------------------------------------------------------------- PCG (wide)
+// The retained preconditioner is applied through explicit inverses of its
+// 9x9 (CW x CW) blocks, Minv = L^-T L^-1 from the block Cholesky factor
+// (unobserved variables: I / lambda, as block_factors.rs:193-203), so the
+// PCG kernels can run one thread per coordinate.
+template <int CW, class TS>
+__global__ void k_precond_inverse(Layout L, const uint8_t* observed, const TS* pre, double lambda, TS* minv) {
+  int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (cam >= L.nC) return;
   const int cw = CW ? CW : L.cw;
   constexpr int CM = CW ? CW : MAXW;
-  int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  TS* out = minv + cam * (int64_t)cw * cw;
+  if (!observed[cam]) {
+    double v = lambda != 0 ? 1.0 / lambda : 1.0;
+    for (int i = 0; i < cw * cw; ++i) out[i] = (TS)((i % (cw + 1)) == 0 ? v : 0.0);
+    return;
+  }
+  const TS* l = pre + L.gram_offset(cam);  // column major lower
+  double m[CM * CM];                        // M = L^-1, column major lower
+  for (int j = 0; j < cw; ++j) {
+    for (int i = 0; i < cw; ++i) m[j * cw + i] = 0;
+    m[j * cw + j] = 1.0 / (double)l[j * cw + j];
+    for (int i = j + 1; i < cw; ++i) {
+      double s = 0;
+      for (int k = j; k < i; ++k) s += (double)l[k * cw + i] * m[j * cw + k];
+      m[j * cw + i] = -s / (double)l[i * cw + i];
+    }
+  }
+  for (int i = 0; i < cw; ++i)
+    for (int j = i; j < cw; ++j) {
+      double s = 0;
+      for (int k = j; k < cw; ++k) s += m[i * cw + k] * m[j * cw + k];  // (M^T M)_ij = sum_k M_ki M_kj
+      out[i * cw + j] = (TS)s;
+      out[j * cw + i] = (TS)s;
+    }
+}
+
+// PCG update, one thread per retained coordinate, 32 variables per block:
+// p = z + beta p; x += alpha p; r -= alpha q; z = Minv r (block local);
+// partial r.r and r.z. The last block applies faer's stopping rules and sets
+// beta for the next search direction, which its consumers form on the fly.
+// XD: the iterate is FP64 (mixed-precision mode) and convergence is deferred
+// to an FP64 residual replacement (see k_replace).
+template <int CW, class TS, class TX, bool MIXED>
+__global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q, const TS* minv,
+                              double* partials, PcgState* st) {
+  if (st->done) return;
+  const int cw = CW ? CW : L.cw;
+  extern __shared__ unsigned char sh_raw[];
+  TS* rs = reinterpret_cast<TS*>(sh_raw);
+  const int64_t n = (int64_t)L.nC * cw;
+  const int64_t base = (int64_t)blockIdx.x * (blockDim.x / cw) * cw;
+  const int lt = threadIdx.x;
+  const int64_t i = base + lt;
+  const bool active = lt < (int)(blockDim.x / cw) * cw && i < n;
   double rr = 0, rz = 0;
-  if (cam < L.nC) {
-    TV alpha = (TV)st->alpha;
-    TV rv[CM];
-    for (int c = 0; c < cw; ++c) {
-      int64_t i = cam * cw + c;
-      x[i] += alpha * p[i];
-      TV ri = r[i] - alpha * q[i];
-      r[i] = ri;
-      rv[c] = ri;
-      rr += (double)ri * (double)ri;
-    }
-    TV zv[CM];
-    for (int c = 0; c < cw; ++c) zv[c] = rv[c];
-    precondition_one<CW, TS, TV>(pre + L.gram_offset(cam), observed[cam], lambda, zv, cw);
-    for (int c = 0; c < cw; ++c) {
-      z[cam * cw + c] = zv[c];
-      rz += (double)rv[c] * (double)zv[c];
-    }
+  TS ri = 0;
+  if (active) {
+    TS pc = z[i] + (TS)st->beta * p[i];
+    double alpha = st->alpha;
+    if (MIXED) x[i] += (TX)(alpha * (double)pc);
+    else x[i] += (TX)((TS)alpha * pc);
+    ri = r[i] - (TS)alpha * q[i];
+    r[i] = ri;
+    p[i] = pc;
+    rr = (double)ri * (double)ri;
+  }
+  rs[lt] = ri;
+  __syncthreads();
+  if (active) {
+    int64_t cam = i / cw;
+    int c = (int)(i % cw);
+    const TS* m = minv + cam * (int64_t)cw * cw + (int64_t)c * cw;
+    const TS* rl = rs + (lt - c);
+    TS zi = 0;
+    for (int j = 0; j < cw; ++j) zi += m[j] * rl[j];
+    z[i] = zi;
+    rz = (double)ri * (double)zi;
   }
   double s[2] = {rr, rz};
   block_sums<2>(s);
@@ -444,61 +484,76 @@ __global__ void k_update(Layout L, TV* x, TV* r, TV* z, TV* p, const TV* q, cons
     partials[2 * blockIdx.x + 1] = s[1];
   }
   if (arrive_last(&st->counter1)) {
-    __shared__ int go_on;
-    __shared__ double beta_s;
     double tot[2];
     finish_sums<2>(partials, tot);
     if (threadIdx.x == 0) {
-      go_on = 0;
       st->iterations += 1;
       st->rr = tot[0];
-      double rnorm = sqrt(tot[0]);
-      if (rnorm < st->threshold) {
+      bool conv = sqrt(tot[0]) < st->threshold;
+      if (MIXED && (conv || st->iterations >= st->max_iterations)) {
+        st->done = 2;
+        st->replace = 1;
+      } else if (!MIXED && conv) {
         st->done = 1;
         st->termination = FG_TERM_CONVERGED;
       } else if (!(st->rz > 0)) {
         st->done = 1;
         st->termination = FG_TERM_NOT_POSITIVE_DEFINITE;
-      } else if (st->iterations >= st->max_iterations) {
+      } else if (!MIXED && st->iterations >= st->max_iterations) {
         st->done = 1;
         st->termination = FG_TERM_ITERATION_LIMIT;
       } else {
+        if (MIXED && tot[0] < st->delta2 * st->rr_last) st->replace = 1;
         st->beta = tot[1] / st->rz;
         st->rz = tot[1];
-        beta_s = st->beta;
-        go_on = 1;
       }
       st->counter1 = 0;
-    }
-    __syncthreads();
-    if (go_on) {
-      TV b = (TV)beta_s;
-      int64_t n = (int64_t)L.nC * cw;
-      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-        TV zi = ((volatile TV*)z)[i];
-        p[i] = zi + b * p[i];
-      }
     }
   }
 }
 
-// PCG start: r = b, x = 0, p_prev = 0, ||b|| and the threshold.
-template <class TV>
-__global__ void k_pcg_init(int64_t n, const double* b, TV* x, TV* r, double* partials, PcgState* st,
-                           double rel_tol) {
-  double s = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    TV bi = (TV)b[i];
-    r[i] = bi;
+// PCG start: r = b, x = 0, z = Minv r, p = 0, beta = 0, rz = r.z, ||b||.
+template <int CW, class TS, class TX>
+__global__ void k_pcg_start(Layout L, const double* b, TX* x, TS* r, TS* z, TS* p, const TS* minv, double* partials,
+                            PcgState* st, double rel_tol) {
+  const int cw = CW ? CW : L.cw;
+  extern __shared__ unsigned char sh_raw[];
+  TS* rs = reinterpret_cast<TS*>(sh_raw);
+  const int64_t n = (int64_t)L.nC * cw;
+  const int64_t base = (int64_t)blockIdx.x * (blockDim.x / cw) * cw;
+  const int lt = threadIdx.x;
+  const int64_t i = base + lt;
+  const bool active = lt < (int)(blockDim.x / cw) * cw && i < n;
+  double bb = 0, rz = 0;
+  TS ri = 0;
+  if (active) {
+    ri = (TS)b[i];
+    r[i] = ri;
     x[i] = 0;
-    s += (double)bi * (double)bi;
+    p[i] = 0;
+    bb = (double)ri * (double)ri;
   }
-  double v[1] = {s};
-  block_sums<1>(v);
-  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+  rs[lt] = ri;
+  __syncthreads();
+  if (active) {
+    int64_t cam = i / cw;
+    int c = (int)(i % cw);
+    const TS* m = minv + cam * (int64_t)cw * cw + (int64_t)c * cw;
+    const TS* rl = rs + (lt - c);
+    TS zi = 0;
+    for (int j = 0; j < cw; ++j) zi += m[j] * rl[j];
+    z[i] = zi;
+    rz = (double)ri * (double)zi;
+  }
+  double s[2] = {bb, rz};
+  block_sums<2>(s);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = s[0];
+    partials[2 * blockIdx.x + 1] = s[1];
+  }
   if (arrive_last(&st->counter2)) {
-    double tot[1];
-    finish_sums<1>(partials, tot);
+    double tot[2];
+    finish_sums<2>(partials, tot);
     if (threadIdx.x == 0) {
       double bn = sqrt(tot[0]);
       st->bnorm = bn;
@@ -507,6 +562,10 @@ __global__ void k_pcg_init(int64_t n, const double* b, TV* x, TV* r, double* par
       st->beta = 0;
       st->alpha = 0;
       st->rr = tot[0];
+      st->rr_last = tot[0];
+      st->rz = tot[1];
+      st->replace = 0;
+      st->replacements = 0;
       st->termination = FG_TERM_NONE;
       st->done = 0;
       if (bn == 0 || bn < st->threshold) {
@@ -518,34 +577,68 @@ __global__ void k_pcg_init(int64_t n, const double* b, TV* x, TV* r, double* par
   }
 }
 
-// z = M^-1 r, p = z and rz = r.z at the start of CG.
-template <int CW, class TS, class TV>
-__global__ void k_pcg_precond_init(Layout L, const TV* r, TV* z, TV* p, const TS* pre, const uint8_t* observed,
-                                   double lambda, double* partials, PcgState* st) {
-  if (st->done) return;
+// FP64 residual replacement, gated by st->replace: r = b - S xd (qd = S xd in
+// FP64 arithmetic), z = Minv r, rz = r.z. Ends the solve when the FP64 residual
+// meets the threshold; restarts the search direction (beta = 0) when the
+// recurrence had claimed convergence but the FP64 residual disagrees.
+template <int CW, class TS>
+__global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* r, TS* z, const TS* minv,
+                               double* partials, PcgState* st) {
+  if (!st->replace) return;
   const int cw = CW ? CW : L.cw;
-  constexpr int CM = CW ? CW : MAXW;
-  int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  double rz = 0;
-  if (cam < L.nC) {
-    TV zv[CM];
-    for (int c = 0; c < cw; ++c) zv[c] = r[cam * cw + c];
-    precondition_one<CW, TS, TV>(pre + L.gram_offset(cam), observed[cam], lambda, zv, cw);
-    for (int c = 0; c < cw; ++c) {
-      z[cam * cw + c] = zv[c];
-      p[cam * cw + c] = zv[c];
-      rz += (double)r[cam * cw + c] * (double)zv[c];
-    }
+  extern __shared__ unsigned char sh_raw[];
+  TS* rs = reinterpret_cast<TS*>(sh_raw);
+  const int64_t n = (int64_t)L.nC * cw;
+  const int64_t base = (int64_t)blockIdx.x * (blockDim.x / cw) * cw;
+  const int lt = threadIdx.x;
+  const int64_t i = base + lt;
+  const bool active = lt < (int)(blockDim.x / cw) * cw && i < n;
+  double rr = 0, rz = 0;
+  TS ri = 0;
+  if (active) {
+    double rt = b[i] - qd[i];
+    rr = rt * rt;
+    ri = (TS)rt;
+    r[i] = ri;
   }
-  double v[1] = {rz};
-  block_sums<1>(v);
-  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
-  if (arrive_last(&st->counter2)) {
-    double tot[1];
-    finish_sums<1>(partials, tot);
+  rs[lt] = ri;
+  __syncthreads();
+  if (active) {
+    int64_t cam = i / cw;
+    int c = (int)(i % cw);
+    const TS* m = minv + cam * (int64_t)cw * cw + (int64_t)c * cw;
+    const TS* rl = rs + (lt - c);
+    TS zi = 0;
+    for (int j = 0; j < cw; ++j) zi += m[j] * rl[j];
+    z[i] = zi;
+    rz = (double)ri * (double)zi;
+  }
+  double s[2] = {rr, rz};
+  block_sums<2>(s);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = s[0];
+    partials[2 * blockIdx.x + 1] = s[1];
+  }
+  if (arrive_last(&st->counter3)) {
+    double tot[2];
+    finish_sums<2>(partials, tot);
     if (threadIdx.x == 0) {
-      st->rz = tot[0];
-      st->counter2 = 0;
+      st->rr_last = tot[0];
+      st->rr = tot[0];
+      st->replacements += 1;
+      st->replace = 0;
+      st->rz = tot[1];
+      if (sqrt(tot[0]) < st->threshold) {
+        st->done = 1;
+        st->termination = FG_TERM_CONVERGED;
+      } else if (st->done == 2 && st->iterations >= st->max_iterations) {
+        st->done = 1;
+        st->termination = FG_TERM_ITERATION_LIMIT;
+      } else if (st->done == 2) {
+        st->done = 0;
+        st->beta = 0;
+      }
+      st->counter3 = 0;
     }
   }
 }

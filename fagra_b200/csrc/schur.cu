@@ -76,7 +76,7 @@ class SchurImpl final : public Backend {
   // ---- numerics
   DBuf<double> d_g, d_scales, d_work, d_rhs, d_zred, d_step, d_tmpd, d_qd, d_jd, d_camjt;
   std::vector<int64_t> h_pt_off;  // point -> first point-major edge (host copy)
-  DBuf<TS> d_gram, d_factors, d_precond, d_cross;
+  DBuf<TS> d_gram, d_factors, d_precond, d_cross, d_minv;
   DBuf<TS> d_x, d_r, d_z, d_pp, d_q, d_t;  // PCG vectors in the storage precision
   DBuf<double> d_partials, d_norm;
   DBuf<unsigned> d_counters;
@@ -163,6 +163,7 @@ class SchurImpl final : public Backend {
     FG_TRY(d_gram.resize(ng));
     FG_TRY(d_factors.resize(ng));
     FG_TRY(d_precond.resize(ng));
+    FG_TRY(d_minv.resize(std::max<size_t>(nC * cw * cw, 1)));
     FG_TRY(d_observed.resize(nC + nP));
     return clear();
   }
@@ -434,6 +435,12 @@ class SchurImpl final : public Backend {
                   d_precond.get(), lambda);
       });
     }
+    if (*fallbacks == 0 && nC) {
+      FG_DISPATCH_WIDTHS(cw, pw, {
+        FG_LAUNCH((k_precond_inverse<CW_, TS>), grid_for(nC, 64), 64, 0, st, L, d_observed.get(), precond_factors(),
+                  lambda, d_minv.get());
+      });
+    }
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
     return FG_OK;
   }
@@ -444,55 +451,60 @@ class SchurImpl final : public Backend {
   // out = ax * x + [B x] - E C^-1 E^T x for a double or storage-precision vector.
   template <class TV>
   fg_status apply_reduced(PView<TV> x, double lambda, double ax, bool use_gram, TV* t, TV* out, double* partials,
-                          PcgState* pst) {
+                          PcgState* pst, const int* gate = nullptr) {
     Layout L = layout();
     const int* done = pst ? &pst->done : nullptr;
-    if (fast.enabled() && use_gram && ax == lambda) return fast.apply(*this, x, lambda, out, partials, pst);
+    if (fast.enabled() && use_gram && ax == lambda) return fast.apply(*this, x, lambda, out, partials, pst, gate);
     FG_DISPATCH_WIDTHS(cw, pw, {
       if (nP) FG_LAUNCH((k_points<CW_, PW_, TS, TV>), grid_for(nP, 128), 128, 0, st, L, d_pt_edge_off.get(),
                         d_pt_edge.get(), d_edges.get(), d_cross.get(), d_factors.get(), d_observed.get(), x, lambda, t,
-                        done);
+                        done, gate);
       if (nC) FG_LAUNCH((k_cams<CW_, PW_, TS, TV>), grid_for(nC * 32, NT), NT, 0, st, L, d_cam_edge_off.get(),
                         d_cam_edge.get(), d_edges.get(), d_cross.get(), t, d_gram.get(), d_observed.get(), x, ax,
-                        (int)use_gram, out, partials, pst);
+                        (int)use_gram, out, partials, pst, gate);
     });
     return FG_OK;
   }
 
-  // PCG on S z = b (faer's CG restated, see kernels.cuh). b is a double
-  // retained vector; the solution lands in d_x (storage precision).
+  // Launch geometry of the wide PCG kernels: whole retained variables per block.
+  unsigned wide_block() const { return (unsigned)((256 / cw) * cw); }
+  unsigned wide_grid() const {
+    size_t per = 256 / cw;
+    return grid_for(std::max<size_t>((nC + per - 1) / per, 1), 1);
+  }
+
+  // PCG on S z = b: faer's CG restated (zero start, relative threshold on
+  // ||r||_2, callback before the test) with the retained block-Jacobi
+  // preconditioner. b is a double retained vector; the solution lands in d_x.
   fg_status pcg(const double* b, double lambda, double rel_tol, size_t max_iters, unsigned* its, int* term,
                 double* rel_est) {
     Layout L = layout();
     PcgState* ps = d_pcg.get();
-    unsigned gvec = std::min<unsigned>(grid_for(retained, NT), 4 * nsm);
     {
       PcgState init{};
       init.max_iterations = (unsigned)std::min<size_t>(max_iters, 0xffffffffu);
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
       FG_CUDA(cudaStreamSynchronize(st));
     }
-    FG_LAUNCH(k_pcg_init<TS>, gvec, NT, 0, st, (int64_t)retained, b, d_x.get(), d_r.get(), d_partials.get(), ps,
-              rel_tol);
-    unsigned gc = grid_for(std::max<size_t>(nC, 1), NT);
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
     FG_DISPATCH_WIDTHS(cw, pw, {
-      FG_LAUNCH((k_pcg_precond_init<CW_, TS, TS>), gc, NT, 0, st, L, d_r.get(), d_z.get(), d_pp.get(),
-                precond_factors(), d_observed.get(), lambda, d_partials.get(), ps);
+      FG_LAUNCH((k_pcg_start<CW_, TS, TS>), gw, bw, shm, st, L, b, d_x.get(), d_r.get(), d_z.get(), d_pp.get(),
+                d_minv.get(), d_partials.get(), ps, rel_tol);
     });
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
-    EventTimer tprod;
     for (;;) {
       FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
       FG_CUDA(cudaStreamSynchronize(st));
       if (h_pcg.get()->done) break;
       if (launched >= max_iters + 2) break;  // device enforces the limit; host bound is a guard
       for (size_t k = 0; k < batch; ++k) {
-        PView<TS> pv{d_pp.get(), nullptr, nullptr};
+        PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
         FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
         FG_DISPATCH_WIDTHS(cw, pw, {
-          FG_LAUNCH((k_update<CW_, TS, TS>), gc, NT, 0, st, L, d_x.get(), d_r.get(), d_z.get(), d_pp.get(), d_q.get(),
-                    precond_factors(), d_observed.get(), lambda, d_partials.get(), ps);
+          FG_LAUNCH((k_update_wide<CW_, TS, TS, false>), gw, bw, shm, st, L, d_x.get(), d_r.get(), d_z.get(),
+                    d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
         });
       }
       launched += batch;
@@ -568,42 +580,71 @@ class SchurImpl final : public Backend {
     return FG_OK;
   }
 
-  // FP32 bulk with FP64 outer refinement of the reduced system: each round
-  // forms res = b - S z in FP64 arithmetic, solves S d = res with FP32 PCG to
-  // refinement_inner_tolerance, and accumulates z += d in FP64.
+  // FP32 PCG with FP64 residual replacement (reliable updates): the Krylov
+  // recurrences run in the storage precision while the iterate accumulates in
+  // FP64; whenever the recurrence residual has fallen by residual_replacement
+  // (and before declaring convergence) it is replaced by b - S x evaluated in
+  // FP64 arithmetic. Convergence is only ever declared on that FP64 residual.
   fg_status refine(double lambda, unsigned* its_out, int* term_out, double* est_out, size_t* rounds) {
-    size_t budget = opt.max_iterations;
-    unsigned total = 0;
-    int term = FG_TERM_ITERATION_LIMIT;
-    double est = 0;
-    FG_CUDA(cudaMemsetAsync(d_zred.get(), 0, retained * sizeof(double), st));
-    double bnorm = 0;
-    FG_TRY(device_dot(d_rhs.get(), d_rhs.get(), retained, &bnorm));
-    bnorm = std::sqrt(bnorm);
-    size_t k = 0;
-    for (;; ++k) {
-      // res = b - S z (FP64 arithmetic); res stored in d_work[0..retained)
-      double rnorm = 0;
-      FG_TRY(reduced_residual_d(lambda, d_zred.get(), d_work.get(), &rnorm));
-      est = bnorm > 0 ? rnorm / bnorm : rnorm;
-      if (bnorm == 0 || est < opt.relative_tolerance) { term = FG_TERM_CONVERGED; break; }
-      if (k >= opt.max_refinements || budget == 0) { term = FG_TERM_ITERATION_LIMIT; break; }
-      unsigned its = 0;
-      int t = 0;
-      double e = 0;
-      double inner = std::max(opt.refinement_inner_tolerance, opt.relative_tolerance);
-      FG_TRY(pcg(d_work.get(), lambda, inner, budget, &its, &t, &e));
-      total += its;
-      budget = its >= budget ? 0 : budget - its;
-      if (t == FG_TERM_NOT_POSITIVE_DEFINITE) { term = t; break; }
-      FG_TRY(launch_axpy_widen(d_x.get(), d_zred.get(), retained));
+    Layout L = layout();
+    PcgState* ps = d_pcg.get();
+    double* xd = d_zred.get();
+    {
+      PcgState init{};
+      init.max_iterations = (unsigned)std::min<size_t>(opt.max_iterations, 0xffffffffu);
+      double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-2;
+      init.delta2 = d * d;
+      FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+      FG_CUDA(cudaStreamSynchronize(st));
     }
-    iterations += total;
-    diag.iterations = total;
-    *its_out = total;
-    *term_out = term;
-    *est_out = est;
-    *rounds = k;
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      FG_LAUNCH((k_pcg_start<CW_, TS, double>), gw, bw, shm, st, L, d_rhs.get(), xd, d_r.get(), d_z.get(),
+                d_pp.get(), d_minv.get(), d_partials.get(), ps, opt.relative_tolerance);
+    });
+    double* tsum = d_partials.get() + 4 * 65536;
+    size_t launched = 0, batch = 4;
+    const size_t max_iters = opt.max_iterations;
+    for (;;) {
+      FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+      FG_CUDA(cudaStreamSynchronize(st));
+      if (h_pcg.get()->done == 1) break;
+      if (launched >= max_iters + 8) break;  // guard; the device enforces the limit
+      for (size_t k = 0; k < batch; ++k) {
+        PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
+        FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
+        FG_DISPATCH_WIDTHS(cw, pw, {
+          FG_LAUNCH((k_update_wide<CW_, TS, double, true>), gw, bw, shm, st, L, xd, d_r.get(), d_z.get(),
+                    d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
+        });
+        if ((k & 3) == 3) FG_TRY(replacement(lambda, xd, ps));
+      }
+      launched += batch;
+      batch = std::min<size_t>(batch * 2, 64);
+    }
+    FG_TRY(fast.check(*this));
+    const PcgState& h = *h_pcg.get();
+    iterations += h.iterations;
+    diag.iterations = h.iterations;
+    *its_out = h.iterations;
+    *term_out = h.done == 1 ? h.termination : FG_TERM_ITERATION_LIMIT;
+    *est_out = h.bnorm > 0 ? std::sqrt(h.rr_last) / h.bnorm : 0.0;
+    *rounds = h.replacements;
+    return FG_OK;
+  }
+
+  // Gated FP64 residual replacement: runs only while the device flag is set.
+  fg_status replacement(double lambda, double* xd, PcgState* ps) {
+    Layout L = layout();
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
+    PView<double> xv{xd, nullptr, nullptr};
+    FG_TRY(apply_reduced<double>(xv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr, &ps->replace));
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      FG_LAUNCH((k_replace_wide<CW_, TS>), gw, bw, shm, st, L, d_rhs.get(), d_qd.get(), d_r.get(), d_z.get(),
+                d_minv.get(), d_partials.get(), ps);
+    });
     return FG_OK;
   }
 

@@ -25,10 +25,11 @@ struct HostEdge {
 // PCG / verification scalars living on the device (one per backend).
 struct PcgState {
   double rz, pq, alpha, beta, rr, bnorm, threshold;
-  double rz_new;
-  int done, termination;
-  unsigned iterations, max_iterations;
-  unsigned counter0, counter1, counter2, pad;
+  double rz_new, rr_last, delta2;
+  int done, termination;   // done: 0 running, 1 finished, 2 awaiting the FP64 residual verdict
+  int replace;             // 1: an FP64 residual replacement is due
+  unsigned iterations, max_iterations, replacements;
+  unsigned counter0, counter1, counter2, counter3;
 };
 struct VerifyState {
   double jd2;        // ||J delta||^2

@@ -219,7 +219,7 @@ fg_status SchurImpl<TS>::launch_rhs() {
   FG_DISPATCH_WIDTHS(cw, pw, {
     FG_LAUNCH((k_cams<CW_, PW_, TS, double>), grid_for(nC * 32, NT), NT, 0, st, L, d_cam_edge_off.get(),
               d_cam_edge.get(), d_edges.get(), d_cross.get(), d_work.get() + retained, d_gram.get(),
-              d_observed.get(), w, 1.0, 0, d_rhs.get(), (double*)nullptr, (PcgState*)nullptr);
+              d_observed.get(), w, 1.0, 0, d_rhs.get(), (double*)nullptr, (PcgState*)nullptr, (const int*)nullptr);
   });
   return FG_OK;
 }

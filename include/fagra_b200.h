@@ -80,8 +80,8 @@ typedef struct {
   int precision;             /* fg_precision; default FG_PRECISION_F64 */
   int preconditioner;        /* fg_preconditioner; default FG_PRECOND_RETAINED_BLOCKS */
   int device;                /* CUDA device ordinal; default 0 */
-  double refinement_inner_tolerance; /* FP32 mode: relative tolerance of each inner solve; default 1e-4 */
-  size_t max_refinements;    /* FP32 mode: outer refinement limit; default 30 */
+  double residual_replacement; /* FP32 mode: the recurrence residual is replaced by the FP64
+                                  residual b - S x each time it falls by this factor; default 1e-2 */
 } fg_schur_options;
 
 /* src/schur.rs:44-60 SchurDiagnostics (has_* = Some) */
@@ -94,7 +94,7 @@ typedef struct {
   double scaled_relative_residual;
   double original_relative_residual;
   int has_estimated, has_reduced, has_scaled, has_original;
-  size_t refinements; /* FP32 mode: outer refinement steps in this attempt */
+  size_t refinements; /* FP32 mode: FP64 residual replacements in this attempt */
 } fg_schur_diagnostics;
 
 /* src/schur.rs:75-91 SchurTimings, seconds, device event time. */
