@@ -77,12 +77,19 @@ __device__ __forceinline__ ObsEval bal_eval(const double* R, const double* cam, 
 // observation k in emission order, written in the packed block layout:
 // values[24k .. 24k+18) = camera block (2x9 column major), [24k+18, 24k+24) =
 // point block (2x3 column major), negres[2k..2k+1] = -r.
+// Block of LIN_T observations; the 24 values of each are staged in shared
+// memory (stride 25 words to spread banks) and stored with coalesced writes.
+constexpr int LIN_T = 128;
 template <class TS>
-__global__ void k_bal_linearize(int64_t no, const uint32_t* oc, const uint32_t* op, const double* px,
-                                const double* cams, const double* pts, const double* prep, TS* values,
-                                double* negres, int* error) {
-  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= no) return;
+__global__ void __launch_bounds__(LIN_T) k_bal_linearize(int64_t no, const uint32_t* oc, const uint32_t* op,
+                                                         const double* px, const double* cams, const double* pts,
+                                                         const double* prep, TS* values, double* negres, int* error) {
+  __shared__ TS tile[LIN_T * 25];
+  __shared__ double nr[LIN_T * 2];
+  const int64_t k0 = (int64_t)blockIdx.x * LIN_T;
+  const int64_t k = k0 + threadIdx.x;
+  const int nk = (int)min((int64_t)LIN_T, no - k0);
+  if (k < no) {
   uint32_t c = oc[k], pi = op[k];
   const double* cam = cams + 9 * (int64_t)c;
   const double* R = prep + 18 * (int64_t)c;
@@ -136,7 +143,7 @@ __global__ void k_bal_linearize(int64_t no, const uint32_t* oc, const uint32_t* 
       jp[2 * j + i] = s;
     }
   bool ok = o.ok && isfinite(r[0]) && isfinite(r[1]);
-  TS* v = values + 24 * k;
+  TS* v = tile + threadIdx.x * 25;
   for (int i = 0; i < 18; ++i) {
     v[i] = (TS)jc[i];
     ok = ok && isfinite(jc[i]);
@@ -145,9 +152,14 @@ __global__ void k_bal_linearize(int64_t no, const uint32_t* oc, const uint32_t* 
     v[18 + i] = (TS)jp[i];
     ok = ok && isfinite(jp[i]);
   }
-  negres[2 * k] = -r[0];
-  negres[2 * k + 1] = -r[1];
+  nr[2 * threadIdx.x] = -r[0];
+  nr[2 * threadIdx.x + 1] = -r[1];
   if (!ok) atomicOr(error, 1);
+  }
+  __syncthreads();
+  TS* out = values + 24 * k0;
+  for (int i = threadIdx.x; i < nk * 24; i += LIN_T) out[i] = tile[(i / 24) * 25 + (i % 24)];
+  for (int i = threadIdx.x; i < nk * 2; i += LIN_T) negres[2 * k0 + i] = nr[i];
 }
 
 // Error-free addition (Knuth TwoSum) for compensated cost reductions.
@@ -338,10 +350,10 @@ fg_status BalProblem::linearize(Backend* b) {
   FG_CUDA(cudaMemsetAsync(d_flag.get(), 0, sizeof(int), st));
   if (no) {
     if (b->is_f32()) {
-      FG_LAUNCH(k_bal_linearize<float>, grid_for(no, 128), 128, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
+      FG_LAUNCH(k_bal_linearize<float>, grid_for(no, LIN_T), LIN_T, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
                 cams.get(), pts.get(), prep.get(), (float*)b->values_device(), b->negres_device(), d_flag.get());
     } else {
-      FG_LAUNCH(k_bal_linearize<double>, grid_for(no, 128), 128, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
+      FG_LAUNCH(k_bal_linearize<double>, grid_for(no, LIN_T), LIN_T, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
                 cams.get(), pts.get(), prep.get(), (double*)b->values_device(), b->negres_device(), d_flag.get());
     }
   }

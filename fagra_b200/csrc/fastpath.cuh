@@ -476,26 +476,23 @@ struct FastPath {
     return FG_OK;
   }
 
-  // Called at the end of prepare_damping: refresh edge records from the cross blocks.
+  // Whether the BAL single-pass operator applies to this system; builds the
+  // tiles once per structure. The caller then writes the edge records.
   template <class Impl>
-  fg_status prepare(Impl& s) {
-    on = false;
-    if (s.cw != 9 || s.pw != 3 || s.nC == 0 || s.nP == 0 || s.nedges == 0) return FG_OK;
+  bool ready_for(Impl& s) {
+    if (disabled || s.cw != 9 || s.pw != 3 || s.nC == 0 || s.nP == 0 || s.nedges == 0) return false;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
-    size_t need = std::max(FastSmem<TS, double>::bytes((int64_t)s.nC, false), FastSmem<TS, TS>::bytes((int64_t)s.nC, false));
-    if (need > (size_t)optin) return FG_OK;  // accumulator does not fit one SM's shared memory
+    size_t need = std::max(FastSmem<TS, double>::bytes((int64_t)s.nC, false),
+                           FastSmem<TS, TS>::bytes((int64_t)s.nC, false));
+    if (need > (size_t)optin) return false;  // accumulator does not fit one SM's shared memory
     if (!structure) {
-      FG_TRY(build(s, s.h_pt_off));
-      if (!structure) return FG_OK;
+      if (build(s, s.h_pt_off) != FG_OK || !structure) return false;
     }
-    FG_LAUNCH(k_fast_edge_records<TS>, grid_for(s.nedges * 28, 256), 256, 0, s.st, (int64_t)s.nedges,
-              s.d_pt_edge.get(), s.d_edges.get(), s.d_cross.get(), d_lp.get(), d_erec.get());
     grid = sm_count(s.dev);
-    FG_TRY(d_parts_f.resize((size_t)grid * s.nC * 9));
-    FG_TRY(d_parts_d.resize((size_t)grid * s.nC * 9));
-    on = true;
-    return FG_OK;
+    if (d_parts_f.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
+    if (d_parts_d.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
+    return true;
   }
 
   // After each block factorization: refresh C^-1 in the point records.

@@ -199,7 +199,7 @@ __global__ void k_gram(Layout L, int64_t first, int64_t count, int w, const int6
 // Cross blocks E_e[p,c] (src/schur.rs:504-519), layout (e*pw+p)*cw+c.
 template <class TS>
 __global__ void k_cross(int64_t nedges, int cw, int pw, const DEdgeMeta* edges, const DBlockMeta* blocks,
-                        const TS* values, const double* scales, TS* cross) {
+                        const TS* values, const double* scales, TS* cross, int* bad) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int64_t per = (int64_t)cw * pw;
   if (t >= nedges * per) return;
@@ -212,6 +212,7 @@ __global__ void k_cross(int64_t nedges, int cw, int pw, const DEdgeMeta* edges, 
   double dl = scales[l.col + c], dr = scales[r.col + p];
   double s = 0;
   for (int i = 0; i < l.rows; ++i) s += ((double)lc[i] / dl) * ((double)rp[i] / dr);
+  if (!isfinite(s)) atomicOr(bad, 1);
   cross[t] = (TS)s;
 }
 

@@ -4,6 +4,7 @@
 #include "kernels.cuh"
 #include "camside.cuh"
 #include "fastpath.cuh"
+#include "setup.cuh"
 #include <algorithm>
 #include <numeric>
 
@@ -80,6 +81,7 @@ class SchurImpl final : public Backend {
   DBuf<TS> d_x, d_r, d_z, d_pp, d_q, d_t;  // PCG vectors in the storage precision
   DBuf<double> d_partials, d_norm;
   DBuf<unsigned> d_counters;
+  DBuf<int> d_flags;
   DBuf<PcgState> d_pcg;
   DBuf<VerifyState> d_ver;
   HBuf<double> h_step, h_scalar;
@@ -112,6 +114,7 @@ class SchurImpl final : public Backend {
     FG_TRY(h_count.resize(4));
     FG_TRY(h_scalar.resize(4));
     FG_TRY(d_counters.resize(8));
+    FG_TRY(d_flags.resize(4));
     FG_TRY(d_norm.resize(4));
     FG_CUDA(cudaMemsetAsync(d_pcg.get(), 0, sizeof(PcgState), st));
     FG_CUDA(cudaMemsetAsync(d_ver.get(), 0, sizeof(VerifyState), st));
@@ -333,7 +336,7 @@ class SchurImpl final : public Backend {
       Layout L = layout();
       if (nC) {
         FG_DISPATCH_WIDTHS(cw, pw, {
-          FG_LAUNCH((k_cam_jt<CW_, TS, CAM_GRADIENT>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(),
+          FG_LAUNCH((k_cam_jt_block<CW_, TS, CAM_GRADIENT>), (unsigned)nC, 128, 0, st, L, d_var_off.get(),
                     d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), (const double*)nullptr, d_g.get());
         });
       }
@@ -376,40 +379,42 @@ class SchurImpl final : public Backend {
     }
     FG_TRY(sync_model());
     Layout L = layout();
-    if (dim) {
-      if (nC) {
-        FG_DISPATCH_WIDTHS(cw, pw, {
-          FG_LAUNCH((k_cam_jt<CW_, TS, CAM_SQUARES>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(),
-                    d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), (const double*)nullptr,
-                    d_scales.get());
-        });
-      }
-      if (dim > retained)
-        FG_LAUNCH(k_scales_raw<TS>, grid_for(dim - retained, NT), NT, 0, st, L, (int64_t)retained, d_var_off.get(),
-                  d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get());
-      double m;
-      FG_TRY(device_norm_inf(d_scales.get(), dim, &m));
-      FG_LAUNCH(k_floor, grid_for(dim, NT), NT, 0, st, (int64_t)dim, d_scales.get(), floor);
+    int* bad = d_flags.get();
+    FG_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(int), st));
+    if (nC) {
+      FG_CUDA(cudaMemsetAsync(d_gram.get(), 0, nC * cw * cw * sizeof(TS), st));
+      FG_DISPATCH_WIDTHS(cw, pw, {
+        FG_LAUNCH((k_cam_scales_gram<CW_, TS>), (unsigned)nC, 128, 0, st, L, d_var_off.get(), d_var_blk.get(),
+                  d_blocks.get(), d_values.get(), floor, d_scales.get(), d_gram.get(), bad);
+      });
     }
-    size_t ng = nC * cw * cw + nP * pw * pw;
-    if (ng) {
-      FG_CUDA(cudaMemsetAsync(d_gram.get(), 0, ng * sizeof(TS), st));
-      if (nC) {
-        FG_DISPATCH_WIDTHS(cw, pw, {
-          FG_LAUNCH((k_cam_gram<CW_, TS>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(),
-                    d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
-        });
-      }
-      if (nP) FG_LAUNCH(k_gram<TS>, grid_for(nP * pw * pw, NT), NT, 0, st, L, (int64_t)nC, (int64_t)nP, (int)pw,
-                        d_var_off.get(), d_var_blk.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_gram.get());
+    if (nP) {
+      FG_DISPATCH_WIDTHS(cw, pw, {
+        FG_LAUNCH((k_point_scales_gram<PW_, TS>), grid_for(nP, 128), 128, 0, st, L, d_var_off.get(),
+                  d_var_blk.get(), d_blocks.get(), d_values.get(), floor, d_scales.get(), d_gram.get(), bad);
+      });
     }
     if (nedges) {
-      FG_LAUNCH(k_cross<TS>, grid_for(nedges * cw * pw, NT), NT, 0, st, (int64_t)nedges, (int)cw, (int)pw,
-                d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_cross.get());
-      double m;
-      FG_TRY(device_norm_inf(d_cross.get(), nedges * cw * pw, &m));
+      if (fast.ready_for(*this)) {
+        FG_LAUNCH(k_edge_records_fused<TS>, grid_for(nedges * (cw * pw + 1), 256), 256, 0, st, (int64_t)nedges,
+                  (int)cw, (int)pw, d_pt_edge.get(), d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(),
+                  fast.d_lp.get(), fast.d_erec.get(), d_cross.get(), bad + 1);
+        fast.on = true;
+      } else {
+        fast.on = false;
+        FG_LAUNCH(k_cross<TS>, grid_for(nedges * cw * pw, NT), NT, 0, st, (int64_t)nedges, (int)cw, (int)pw,
+                  d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_cross.get(), bad + 1);
+      }
+    } else {
+      fast.on = false;
     }
-    FG_TRY(fast.prepare(*this));
+    FG_CUDA(cudaMemcpyAsync(h_count.get(), bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (h_count.get()[0] || h_count.get()[1]) {
+      fast.on = false;
+      set_error("nonfinite column norm or cross block");
+      return FG_INVALID_EVALUATION;
+    }
     ready = true;
     if (opt.collect_timings) tim.preparation += tm.stop(st);
     return FG_OK;

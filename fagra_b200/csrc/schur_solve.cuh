@@ -296,7 +296,7 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
               d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
   if (nC) {
     FG_DISPATCH_WIDTHS(cw, pw, {
-      FG_LAUNCH((k_cam_jt<CW_, TS, CAM_NORMAL>), grid_for(nC * 32, NT), NT, 0, st, L, d_var_off.get(),
+      FG_LAUNCH((k_cam_jt_block<CW_, TS, CAM_NORMAL>), (unsigned)nC, 128, 0, st, L, d_var_off.get(),
                 d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), d_jd.get(), d_camjt.get());
     });
   }

@@ -1,0 +1,188 @@
+// Per-linearization setup kernels: column scales with their floor, normalized
+// Gram blocks, J^T v reductions and the cross-block edge records, fused so each
+// pass reads the Jacobian once. Nonfinite values raise a device flag that the
+// host reads once per prepare_damping (src/linear_model.rs:225 and
+// src/schur.rs:520 reject them with InvalidEvaluation).
+#pragma once
+#include "kernels.cuh"
+#include "fastpath.cuh"
+
+namespace fg {
+
+template <int N>
+__device__ __forceinline__ void block_allsums(double (&v)[N], double* sh /* >= 32*N */) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) sh[warp * N + k] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double s = 0;
+    for (int w = 0; w < nw; ++w) s += sh[w * N + k];
+    v[k] = s;
+  }
+  __syncthreads();
+}
+
+// One block per retained variable: raw column norms (hypot chain of
+// src/linear_model.rs:217-224), floored scales, and the normalized Gram block
+// (block_factors.rs:87-99), all from the variable's blocks.
+template <int CW, class TS>
+__global__ void k_cam_scales_gram(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
+                                  const TS* values, double floor, double* scales, TS* gram, int* bad) {
+  constexpr int CM = CW ? CW : MAXW;
+  constexpr int NL = CM * (CM + 1) / 2;
+  const int cw = CW ? CW : L.cw;
+  __shared__ double sh[32 * NL];
+  const int64_t cam = blockIdx.x;
+  if (cam >= L.nC) return;
+  const int64_t b0 = var_off[cam], b1 = var_off[cam + 1];
+  double sq[CM];
+  for (int c = 0; c < CM; ++c) sq[c] = 0;
+  for (int64_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
+    DBlockMeta b = blocks[var_blk[k]];
+    for (int c = 0; c < cw; ++c)
+      for (int i = 0; i < b.rows; ++i) {
+        double v = (double)values[b.start + (int64_t)c * b.rows + i];
+        sq[c] += v * v;
+      }
+  }
+  block_allsums<CM>(sq, sh);
+  double inv[CM];
+  for (int c = 0; c < cw; ++c) {
+    double raw = sqrt(sq[c]);
+    if (!isfinite(raw) && threadIdx.x == 0) atomicOr(bad, 1);
+    double d = fmax(raw, floor);
+    inv[c] = 1.0 / d;
+    if (threadIdx.x == 0) scales[cam * cw + c] = d;
+  }
+  double acc[NL];
+  for (int k = 0; k < NL; ++k) acc[k] = 0;
+  for (int64_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
+    DBlockMeta b = blocks[var_blk[k]];
+    for (int i = 0; i < b.rows; ++i) {
+      double jv[CM];
+      for (int c = 0; c < cw; ++c) jv[c] = (double)values[b.start + (int64_t)c * b.rows + i] * inv[c];
+      int idx = 0;
+      for (int c = 0; c < cw; ++c)
+        for (int r = c; r < cw; ++r) acc[idx++] += jv[c] * jv[r];
+    }
+  }
+  block_allsums<NL>(acc, sh);
+  TS* g = gram + L.gram_offset(cam);
+  int idx = 0;
+  for (int c = 0; c < cw; ++c)
+    for (int r = c; r < cw; ++r) {
+      if (threadIdx.x == (idx & (blockDim.x - 1))) g[c * cw + r] = (TS)acc[idx];
+      ++idx;
+    }
+}
+
+// One thread per eliminated variable: floored scales and normalized Gram block.
+template <int PW, class TS>
+__global__ void k_point_scales_gram(Layout L, const int64_t* var_off, const int64_t* var_blk,
+                                    const DBlockMeta* blocks, const TS* values, double floor, double* scales,
+                                    TS* gram, int* bad) {
+  constexpr int PM = PW ? PW : MAXW;
+  const int pw = PW ? PW : L.pw;
+  const int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (pt >= L.nP) return;
+  const int64_t v = L.nC + pt;
+  double sq[PM];
+  for (int p = 0; p < pw; ++p) sq[p] = 0;
+  for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
+    DBlockMeta b = blocks[var_blk[k]];
+    for (int p = 0; p < pw; ++p)
+      for (int i = 0; i < b.rows; ++i) {
+        double x = (double)values[b.start + (int64_t)p * b.rows + i];
+        sq[p] += x * x;
+      }
+  }
+  double inv[PM];
+  const int64_t base = L.retained + pt * pw;
+  for (int p = 0; p < pw; ++p) {
+    double raw = sqrt(sq[p]);
+    if (!isfinite(raw)) atomicOr(bad, 1);
+    double d = fmax(raw, floor);
+    scales[base + p] = d;
+    inv[p] = 1.0 / d;
+  }
+  double acc[PM * PM];
+  for (int k = 0; k < pw * pw; ++k) acc[k] = 0;
+  for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
+    DBlockMeta b = blocks[var_blk[k]];
+    for (int i = 0; i < b.rows; ++i) {
+      double jv[PM];
+      for (int p = 0; p < pw; ++p) jv[p] = (double)values[b.start + (int64_t)p * b.rows + i] * inv[p];
+      for (int c = 0; c < pw; ++c)
+        for (int r = c; r < pw; ++r) acc[c * pw + r] += jv[c] * jv[r];
+    }
+  }
+  TS* g = gram + L.gram_offset(v);
+  for (int c = 0; c < pw; ++c)
+    for (int r = 0; r < pw; ++r) g[c * pw + r] = (TS)(r >= c ? acc[c * pw + r] : 0.0);
+}
+
+// One block per retained variable: out[cam*cw + c] = sum over its blocks of
+// GRADIENT: sum_i J[i,c] r[row+i]; NORMAL: sum_i J[i,c] (jd - negres)[row+i].
+template <int CW, class TS, int MODE>
+__global__ void k_cam_jt_block(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
+                               const TS* values, const double* negres, const double* jd, double* out) {
+  constexpr int CM = CW ? CW : MAXW;
+  const int cw = CW ? CW : L.cw;
+  __shared__ double sh[32 * CM];
+  const int64_t cam = blockIdx.x;
+  if (cam >= L.nC) return;
+  double acc[CM];
+  for (int c = 0; c < CM; ++c) acc[c] = 0;
+  for (int64_t k = var_off[cam] + threadIdx.x; k < var_off[cam + 1]; k += blockDim.x) {
+    DBlockMeta b = blocks[var_blk[k]];
+    for (int i = 0; i < b.rows; ++i) {
+      double v = MODE == CAM_NORMAL ? jd[b.row + i] - negres[b.row + i] : -negres[b.row + i];
+      for (int c = 0; c < cw; ++c) acc[c] += (double)values[b.start + (int64_t)c * b.rows + i] * v;
+    }
+  }
+  block_allsums<CM>(acc, sh);
+  if (threadIdx.x == 0)
+    for (int c = 0; c < cw; ++c) out[cam * cw + c] = acc[c];
+}
+
+// Cross blocks E_e[p,c] = sum_rows (J_cam[:,c]/D)(J_pt[:,p]/D) (src/schur.rs:504-519),
+// one thread per (point-major edge, word): word < cw*pw writes the edge
+// record and the reference-layout cross array; the last word packs the
+// camera and tile-local point indices. Coalesced record writes.
+template <class TS>
+__global__ void k_edge_records_fused(int64_t nedges, int cw, int pw, const int64_t* pt_edge, const DEdgeMeta* edges,
+                                     const DBlockMeta* blocks, const TS* values, const double* scales,
+                                     const uint32_t* local_point, TS* rec, TS* cross, int* bad) {
+  const int W = cw * pw + 1;
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nedges * W) return;
+  int64_t k = t / W;
+  int w = (int)(t % W);
+  int64_t e = pt_edge[k];
+  DEdgeMeta ed = edges[e];
+  if (w < cw * pw) {
+    int p = w / cw, c = w % cw;
+    DBlockMeta l = blocks[ed.lblk], r = blocks[ed.rblk];
+    const TS* lc = values + l.start + (int64_t)c * l.rows;
+    const TS* rp = values + r.start + (int64_t)p * r.rows;
+    double dl = scales[l.col + c], dr = scales[r.col + p];
+    double s = 0;
+    for (int i = 0; i < l.rows; ++i) s += ((double)lc[i] / dl) * ((double)rp[i] / dr);
+    if (!isfinite(s)) atomicOr(bad, 1);
+    rec[t] = (TS)s;
+    cross[e * (int64_t)(cw * pw) + w] = (TS)s;
+  } else {
+    using Wd = RecWord<TS>;
+    typename Wd::U word = Wd::pack((uint32_t)ed.cam, local_point[k]);
+    memcpy(&rec[t], &word, sizeof(word));
+  }
+}
+
+}  // namespace fg
