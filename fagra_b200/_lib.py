@@ -147,6 +147,8 @@ SIGNATURES = {
     "fg_bal_get_parameters": (C.c_int, [C.c_void_p, dptr, dptr]),
     "fg_bal_cost": (C.c_int, [C.c_void_p, dptr]),
     "fg_bal_linearize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "fg_bal_cost_noalloc": (C.c_int, [size_t, size_t, size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "fg_optimize_default_options": (None, [C.POINTER(OptimizeOptionsC)]),
     "fg_lm_default_options": (None, [C.POINTER(LmOptionsC)]),
     "fg_lm_solve_bal": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptimizeOptionsC), C.POINTER(LmOptionsC),

@@ -55,24 +55,6 @@ __global__ void k_bal_camera_prep(int64_t nc, const double* cams, double* prep) 
     }
 }
 
-struct ObsEval {
-  double p[3], q[2], r2, radial, pixel[2];
-  bool ok;
-};
-__device__ __forceinline__ ObsEval bal_eval(const double* R, const double* cam, const double* X) {
-  ObsEval o;
-  for (int i = 0; i < 3; ++i) o.p[i] = R[3 * i] * X[0] + R[3 * i + 1] * X[1] + R[3 * i + 2] * X[2] + cam[3 + i];
-  o.q[0] = -o.p[0] / o.p[2];
-  o.q[1] = -o.p[1] / o.p[2];
-  o.r2 = o.q[0] * o.q[0] + o.q[1] * o.q[1];
-  o.radial = 1. + cam[7] * o.r2 + cam[8] * o.r2 * o.r2;
-  double s = cam[6] * o.radial;
-  o.pixel[0] = s * o.q[0];
-  o.pixel[1] = s * o.q[1];
-  o.ok = !(o.p[2] == 0.) && isfinite(o.pixel[0]) && isfinite(o.pixel[1]);
-  return o;
-}
-
 // Reprojection residual and Jacobians (model.rs:157-185, 214-236) for every
 // observation k in emission order, written in the packed block layout:
 // values[24k .. 24k+18) = camera block (2x9 column major), [24k+18, 24k+24) =
@@ -160,21 +142,6 @@ __global__ void __launch_bounds__(LIN_T) k_bal_linearize(int64_t no, const uint3
   TS* out = values + 24 * k0;
   for (int i = threadIdx.x; i < nk * 24; i += LIN_T) out[i] = tile[(i / 24) * 25 + (i % 24)];
   for (int i = threadIdx.x; i < nk * 2; i += LIN_T) negres[2 * k0 + i] = nr[i];
-}
-
-// Error-free addition (Knuth TwoSum) for compensated cost reductions.
-__device__ __forceinline__ void two_sum(double a, double b, double* s, double* e) {
-  double x = a + b;
-  double bv = x - a;
-  double av = x - bv;
-  *s = x;
-  *e = (a - av) + (b - bv);
-}
-__device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, double blo) {
-  double s, e;
-  two_sum(hi, bhi, &s, &e);
-  e += lo + blo;
-  two_sum(s, e, &hi, &lo);
 }
 
 // Sum of 0.5 |r|^2 over observations (Frame::cost) in double-double, with

@@ -5,6 +5,44 @@
 
 namespace fg {
 
+// Projection of one observation (examples/bal/model.rs:147-156) from the
+// per-camera rotation R (row major) and camera parameters.
+struct ObsEval {
+  double p[3], q[2], r2, radial, pixel[2];
+  bool ok;
+};
+__device__ __forceinline__ ObsEval bal_eval(const double* R, const double* cam, const double* X) {
+  ObsEval o;
+  for (int i = 0; i < 3; ++i) o.p[i] = R[3 * i] * X[0] + R[3 * i + 1] * X[1] + R[3 * i + 2] * X[2] + cam[3 + i];
+  o.q[0] = -o.p[0] / o.p[2];
+  o.q[1] = -o.p[1] / o.p[2];
+  o.r2 = o.q[0] * o.q[0] + o.q[1] * o.q[1];
+  o.radial = 1. + cam[7] * o.r2 + cam[8] * o.r2 * o.r2;
+  double s = cam[6] * o.radial;
+  o.pixel[0] = s * o.q[0];
+  o.pixel[1] = s * o.q[1];
+  o.ok = !(o.p[2] == 0.) && isfinite(o.pixel[0]) && isfinite(o.pixel[1]);
+  return o;
+}
+
+// Error-free addition (Knuth TwoSum) for compensated cost reductions.
+__device__ __forceinline__ void two_sum(double a, double b, double* s, double* e) {
+  double x = a + b;
+  double bv = x - a;
+  double av = x - bv;
+  *s = x;
+  *e = (a - av) + (b - bv);
+}
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, double blo) {
+  double s, e;
+  two_sum(hi, bhi, &s, &e);
+  e += lo + blo;
+  two_sum(s, e, &hi, &lo);
+}
+
+// Per-camera rotation and right factor (defined in bal.cu).
+__global__ void k_bal_camera_prep(int64_t nc, const double* cams, double* prep);
+
 struct BalProblem {
   uint64_t id = 0;
   int dev = 0, nsm = 148;

@@ -199,6 +199,19 @@ FG_API fg_status fg_bal_get_parameters(fg_bal_problem* problem, double* camera_p
                                        double* point_params);
 /* Frame::cost summed over frames (examples/bal/model.rs:201-213, src/optimization.rs:419-430) */
 FG_API fg_status fg_bal_cost(fg_bal_problem* problem, double* cost);
+/* No counterpart in the reference. The BAL objective (as fg_bal_cost) for
+ * callers that cannot let the library allocate device memory: every input and
+ * the output are caller-owned device pointers on `device`, and the scratch is a
+ * fixed file-scope device array (about 2.4 MB per GPU, held until exit).
+ * out[0] = cost, out[1] = 1 if any projection was invalid or an observation
+ * index was out of range. Enqueued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream); the result is ready when the stream reaches it.
+ * At most 16384 cameras (else FG_INVALID_OPTIONS). Calls share the scratch:
+ * calls that overlap on the GPU race and must be serialized by the caller. */
+FG_API fg_status fg_bal_cost_noalloc(size_t cameras, size_t points, size_t observations,
+                                     const double* camera_params, const double* point_params,
+                                     const uint32_t* obs_camera, const uint32_t* obs_point,
+                                     const double* obs_pixel, double* out, int device, void* stream);
 /* Workspace::linearize for BAL frames (src/optimization.rs:229-265 +
  * examples/bal/model.rs:214-236): residuals and Jacobians straight into the
  * backend's block storage, in emission order. */
