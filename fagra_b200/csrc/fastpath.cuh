@@ -350,7 +350,8 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::GT, 1)
 template <class TS, class TV>
 __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram,
                                                       const uint8_t* observed, const TV* z, const TV* pv,
-                                                      const double* beta, double lambda, TV* q, double* dparts,
+                                                      const double* beta, double lambda, const double* lam_dev,
+                                                      TV* q, double* dparts,
                                                       PcgState* st, const int* gate) {
   if (st && st->done) return;
   if (gate && !*gate) return;
@@ -379,7 +380,8 @@ __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, c
     int64_t cam = i / 9;
     int r = (int)(i % 9);
     TV xi = pv ? z[i] + bv * pv[i] : z[i];
-    TV v = (TV)lambda * xi;
+    const double lam = lam_dev ? *lam_dev : lambda;
+    TV v = (TV)lam * xi;
     if (observed[cam]) {
       const TS* g = gram + cam * 81;
 #pragma unroll
@@ -488,6 +490,7 @@ struct FastPath {
     if (need > (size_t)optin) return false;  // accumulator does not fit one SM's shared memory
     if (!structure) {
       if (build(s, s.h_pt_off) != FG_OK || !structure) return false;
+      attr_set[0][0] = attr_set[0][1] = attr_set[1][0] = attr_set[1][1] = 0;
     }
     grid = sm_count(s.dev);
     if (d_parts_f.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
@@ -520,31 +523,40 @@ struct FastPath {
 
   // out = lambda x + B x - E C^-1 E^T x. pst != nullptr: PCG step (skips when
   // finished, computes alpha). gate != nullptr: runs only while *gate != 0.
+  int optin = 0;
+  size_t attr_set[2][2] = {{0, 0}, {0, 0}};  // [TV is double][stage x] -> smem size already granted
+
   template <class Impl, class TV>
   fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst,
-                  const int* gate = nullptr) {
+                  const int* gate = nullptr, const double* lam_dev = nullptr) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
-    int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
     bool xs = FastSmem<TS, TV>::bytes((int64_t)s.nC, true) <= (size_t)optin;
     size_t sm = FastSmem<TS, TV>::bytes((int64_t)s.nC, xs);
+    size_t& granted = attr_set[std::is_same<TV, double>::value ? 1 : 0][xs ? 1 : 0];
     FastTiles tl{d_pbeg.get(), d_ebeg.get(), ntiles};
     const int* skip = pst ? &pst->done : nullptr;
     constexpr int NTHR = FAST_GROUPS * FastShape<TS>::GT;
     if (xs) {
       auto kern = k_fast_apply<TS, TV, true>;
-      FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      if (granted < sm) {
+        FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        granted = sm;
+      }
       FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
                 parts, skip, gate, d_error.get());
     } else {
       auto kern = k_fast_apply<TS, TV, false>;
-      FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      if (granted < sm) {
+        FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        granted = sm;
+      }
       FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
                 parts, skip, gate, d_error.get());
     }
     FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
-              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, out, dparts, pst,
-              gate);
+              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, out,
+              dparts, pst, gate);
     return FG_OK;
   }
 };

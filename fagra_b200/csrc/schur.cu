@@ -102,6 +102,7 @@ class SchurImpl final : public Backend {
   }
 
   SchurImpl(size_t r, size_t c, size_t p, const fg_schur_options& o) : opt(o), retained(r), cw(c), pw(p), dev(o.device) {}
+  ~SchurImpl() override { drop_graphs(); }
 
   fg_status init() {
     FG_TRY(select_device(dev));
@@ -142,6 +143,7 @@ class SchurImpl final : public Backend {
       return FG_INVALID_OPTIONS;
     }
     FG_TRY(select_device(dev));
+    drop_graphs();
     if (dimension != dim) structure_valid = false;
     dim = dimension;
     nC = retained / cw;
@@ -283,6 +285,7 @@ class SchurImpl final : public Backend {
     FG_CUDA(cudaStreamSynchronize(st));
     structure_valid = true;
     fast.invalidate();
+    drop_graphs();
     return FG_OK;
   }
 
@@ -456,10 +459,11 @@ class SchurImpl final : public Backend {
   // out = ax * x + [B x] - E C^-1 E^T x for a double or storage-precision vector.
   template <class TV>
   fg_status apply_reduced(PView<TV> x, double lambda, double ax, bool use_gram, TV* t, TV* out, double* partials,
-                          PcgState* pst, const int* gate = nullptr) {
+                          PcgState* pst, const int* gate = nullptr, const double* lam_dev = nullptr) {
     Layout L = layout();
     const int* done = pst ? &pst->done : nullptr;
-    if (fast.enabled() && use_gram && ax == lambda) return fast.apply(*this, x, lambda, out, partials, pst, gate);
+    if (fast.enabled() && use_gram && ax == lambda)
+      return fast.apply(*this, x, lambda, out, partials, pst, gate, lam_dev);
     FG_DISPATCH_WIDTHS(cw, pw, {
       if (nP) FG_LAUNCH((k_points<CW_, PW_, TS, TV>), grid_for(nP, 128), 128, 0, st, L, d_pt_edge_off.get(),
                         d_pt_edge.get(), d_edges.get(), d_cross.get(), d_factors.get(), d_observed.get(), x, lambda, t,
@@ -478,6 +482,68 @@ class SchurImpl final : public Backend {
     return grid_for(std::max<size_t>((nC + per - 1) / per, 1), 1);
   }
 
+  // ---- CUDA graph of GRAPH_ITERS PCG iterations on the single-pass operator.
+  // Every scalar the iteration needs (alpha, beta, lambda, stopping state)
+  // lives in PcgState on the device, so one instantiation serves every solve
+  // until buffers are reallocated (prepare / new structure).
+  static constexpr int GRAPH_ITERS = 8;
+  cudaGraphExec_t g_exec[2] = {nullptr, nullptr};
+  uint64_t g_nodes[2] = {0, 0};
+  void drop_graphs() {
+    for (int k = 0; k < 2; ++k) {
+      if (g_exec[k]) cudaGraphExecDestroy(g_exec[k]);
+      g_exec[k] = nullptr;
+    }
+  }
+  fg_status iteration_body(bool mixed, double* xd, PcgState* ps, double lambda, int k) {
+    Layout L = layout();
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
+    double* tsum = d_partials.get() + 4 * 65536;
+    PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
+    FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps, nullptr, &ps->lambda));
+    if (!mixed) {
+      FG_DISPATCH_WIDTHS(cw, pw, {
+        FG_LAUNCH((k_update_wide<CW_, TS, TS, false>), gw, bw, shm, st, L, d_x.get(), d_r.get(), d_z.get(),
+                  d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
+      });
+    } else {
+      FG_DISPATCH_WIDTHS(cw, pw, {
+        FG_LAUNCH((k_update_wide<CW_, TS, double, true>), gw, bw, shm, st, L, xd, d_r.get(), d_z.get(),
+                  d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
+      });
+      if ((k & 3) == 3) FG_TRY(replacement(lambda, xd, ps));
+    }
+    return FG_OK;
+  }
+  fg_status launch_graph(bool mixed, double* xd, PcgState* ps, double lambda) {
+    const int g = mixed ? 1 : 0;
+    if (!g_exec[g]) {
+      cudaGraph_t graph = nullptr;
+      uint64_t before = g_launches.load();
+      FG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      fg_status s = FG_OK;
+      for (int k = 0; k < GRAPH_ITERS && s == FG_OK; ++k) s = iteration_body(mixed, xd, ps, lambda, k);
+      cudaError_t e = cudaStreamEndCapture(st, &graph);
+      g_nodes[g] = g_launches.load() - before;
+      g_launches.fetch_sub(g_nodes[g]);  // captured, not launched
+      if (s != FG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return s;
+      }
+      FG_CUDA(e);
+      e = cudaGraphInstantiate(&g_exec[g], graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        g_exec[g] = nullptr;
+        return cuda_status(e, "cudaGraphInstantiate");
+      }
+    }
+    FG_CUDA(cudaGraphLaunch(g_exec[g], st));
+    g_launches.fetch_add(g_nodes[g]);
+    return FG_OK;
+  }
+
   // PCG on S z = b: faer's CG restated (zero start, relative threshold on
   // ||r||_2, callback before the test) with the retained block-Jacobi
   // preconditioner. b is a double retained vector; the solution lands in d_x.
@@ -488,6 +554,7 @@ class SchurImpl final : public Backend {
     {
       PcgState init{};
       init.max_iterations = (unsigned)std::min<size_t>(max_iters, 0xffffffffu);
+      init.lambda = lambda;
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
       FG_CUDA(cudaStreamSynchronize(st));
     }
@@ -499,11 +566,17 @@ class SchurImpl final : public Backend {
     });
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
+    const bool graphed = fast.enabled();
     for (;;) {
       FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
       FG_CUDA(cudaStreamSynchronize(st));
       if (h_pcg.get()->done) break;
       if (launched >= max_iters + 2) break;  // device enforces the limit; host bound is a guard
+      if (graphed) {
+        FG_TRY(launch_graph(false, nullptr, ps, lambda));
+        launched += GRAPH_ITERS;
+        continue;
+      }
       for (size_t k = 0; k < batch; ++k) {
         PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
         FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
@@ -597,6 +670,7 @@ class SchurImpl final : public Backend {
     {
       PcgState init{};
       init.max_iterations = (unsigned)std::min<size_t>(opt.max_iterations, 0xffffffffu);
+      init.lambda = lambda;
       double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-2;
       init.delta2 = d * d;
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
@@ -611,11 +685,17 @@ class SchurImpl final : public Backend {
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
     const size_t max_iters = opt.max_iterations;
+    const bool graphed = fast.enabled();
     for (;;) {
       FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
       FG_CUDA(cudaStreamSynchronize(st));
       if (h_pcg.get()->done == 1) break;
       if (launched >= max_iters + 8) break;  // guard; the device enforces the limit
+      if (graphed) {
+        FG_TRY(launch_graph(true, xd, ps, lambda));
+        launched += GRAPH_ITERS;
+        continue;
+      }
       for (size_t k = 0; k < batch; ++k) {
         PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
         FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
@@ -645,7 +725,8 @@ class SchurImpl final : public Backend {
     const unsigned bw = wide_block(), gw = wide_grid();
     const size_t shm = bw * sizeof(TS);
     PView<double> xv{xd, nullptr, nullptr};
-    FG_TRY(apply_reduced<double>(xv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr, &ps->replace));
+    FG_TRY(apply_reduced<double>(xv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr, &ps->replace,
+                                 &ps->lambda));
     FG_DISPATCH_WIDTHS(cw, pw, {
       FG_LAUNCH((k_replace_wide<CW_, TS>), gw, bw, shm, st, L, d_rhs.get(), d_qd.get(), d_r.get(), d_z.get(),
                 d_minv.get(), d_partials.get(), ps);

@@ -24,7 +24,7 @@ struct HostEdge {
 
 // PCG / verification scalars living on the device (one per backend).
 struct PcgState {
-  double rz, pq, alpha, beta, rr, bnorm, threshold;
+  double rz, pq, alpha, beta, rr, bnorm, threshold, lambda;
   double rz_new, rr_last, delta2;
   int done, termination;   // done: 0 running, 1 finished, 2 awaiting the FP64 residual verdict
   int replace;             // 1: an FP64 residual replacement is due
