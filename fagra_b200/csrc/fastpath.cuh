@@ -3,19 +3,22 @@
 // block read from HBM exactly once per application.
 //
 // Layout (rebuilt at prepare_damping): cross blocks in point-major order as
-// 28-word edge records [E (27, row p*9+c) | camera index + tile-local point
-// index], point records of 8 words [C^-1 packed lower (6) | tile-local first
-// edge | edge count], and tiles = contiguous point ranges holding at most TE
-// edges and TP points.
+// 28-word edge records [E (27, row p*9+c) | camera index + warp-tile-local
+// point index], point records of 8 words [C^-1 packed lower (6) | unused], and
+// warp tiles = contiguous point ranges of at most 32 edges; a stage is WPS
+// consecutive warp tiles.
 //
-// k_fast_apply: one CTA per SM streams its tiles through shared memory with
-// cp.async.bulk (TMA, 1-D) into a two-stage mbarrier pipeline. Per tile:
-//   phase 1, thread per edge:  u_e = E_e^T x_cam            (x from L2)
-//   phase 2, thread per point: t_p = C_p^-1 sum_{e in p} u_e
-//   phase 3, thread per edge:  y_cam -= E_e t_p  (shared-memory atomics into a
-//                                                CTA-private 9C accumulator)
-// then flushes its accumulator to a per-CTA partial vector. No global atomics.
-// k_fast_reduce: q = lambda x + B x - sum_CTA partials, and the PCG step
+// k_fast_apply: one CTA per SM; FAST_GROUPS groups of WPS warps each stream
+// their stages through shared memory with cp.async.bulk (TMA, 1-D) into a
+// two-stage mbarrier pipeline. Each warp owns one warp tile per stage:
+//   lane per edge:    u_e = E_e^T x_cam            (x staged in shared memory)
+//   segmented shuffle scan over the lanes of each point: sum_e u_e
+//   last lane of each point: t_p = C_p^-1 sum u
+//   lane per edge:    y_cam -= E_e t_p  (shared-memory atomics into a
+//                                       CTA-private 9C accumulator)
+// One group barrier per stage; the accumulator is flushed to a per-CTA
+// partial vector. No global atomics.
+// k_fast_reduce: q = lambda x + B x + sum_CTA partials, and the PCG step
 // length alpha from p.q in the last block.
 #pragma once
 #include "kernels.cuh"
@@ -79,40 +82,22 @@ struct RecWord<double> {
 };
 
 template <class TS>
-struct FastShape;  // tile geometry per storage precision: GT threads per group, one edge per thread
+struct FastShape;  // warps per stage (one warp tile of <= 32 edges per warp)
 template <>
 struct FastShape<float> {
-  static constexpr int TE = 256, TP = 128, GT = 256;
+  static constexpr int WPS = 8;
 };
 template <>
 struct FastShape<double> {
-  static constexpr int TE = 128, TP = 64, GT = 128;
+  static constexpr int WPS = 4;
 };
-constexpr int FAST_GROUPS = 2;  // independent tile pipelines per CTA sharing one accumulator
-
-// Edge records: rec[k] for point-major position k (edge pt_edge[k]).
-template <class TS>
-__global__ void k_fast_edge_records(int64_t nedges, const int64_t* pt_edge, const DEdgeMeta* edges,
-                                    const TS* cross, const uint32_t* local_point, TS* rec) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= nedges * 28) return;
-  int64_t k = t / 28;
-  int w = (int)(t % 28);
-  int64_t e = pt_edge[k];
-  if (w < 27) {
-    rec[t] = cross[e * 27 + w];
-  } else {
-    using W = RecWord<TS>;
-    typename W::U word = W::pack((uint32_t)edges[e].cam, local_point[k]);
-    memcpy(&rec[t], &word, sizeof(word));
-  }
-}
+constexpr int FAST_GROUPS = 2;  // independent stage pipelines per CTA sharing one accumulator
+constexpr int FAST_STAGES = 2;  // TMA stages per group
 
 // Point records: packed lower C^-1 from the Cholesky factor L (C^-1 = L^-T L^-1),
 // plus the tile-local edge range (written once per structure, kept here).
 template <class TS>
-__global__ void k_fast_point_records(Layout L, const TS* factors, const uint8_t* observed, double lambda,
-                                     const uint32_t* local_first, const uint32_t* counts, TS* prec) {
+__global__ void k_fast_point_records(Layout L, const TS* factors, const uint8_t* observed, double lambda, TS* prec) {
   int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (pt >= L.nP) return;
   int64_t var = L.nC + pt;
@@ -138,15 +123,8 @@ __global__ void k_fast_point_records(Layout L, const TS* factors, const uint8_t*
   }
   TS* r = prec + pt * 8;
   for (int i = 0; i < 6; ++i) r[i] = (TS)ci[i];
-  uint32_t a = local_first[pt], b = counts[pt];
-  if (sizeof(TS) == 4) {
-    memcpy(&r[6], &a, 4);
-    memcpy(&r[7], &b, 4);
-  } else {
-    uint64_t a8 = a, b8 = b;
-    memcpy(&r[6], &a8, 8);
-    memcpy(&r[7], &b8, 8);
-  }
+  r[6] = 0;
+  r[7] = 0;
 }
 
 template <class TS>
@@ -162,23 +140,23 @@ __device__ __forceinline__ uint32_t rec_u32(const TS* p) {
 }
 
 struct FastTiles {
-  const int64_t* pbeg;  // ntiles + 1
-  const int64_t* ebeg;  // ntiles + 1
-  int64_t ntiles;
+  const int64_t* wt_e0;  // nwt + 1: first point-major edge of each warp tile
+  const int64_t* wt_p0;  // nwt + 1: first point of each warp tile
+  int64_t nwt, nstages;
 };
 
 template <class TS, class TV>
 struct FastSmem {
-  static constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP;
+  static constexpr int WPS = FastShape<TS>::WPS, SE = WPS * 32;
   __host__ __device__ static constexpr size_t stage_bytes() {
-    return (size_t)TE * 28 * sizeof(TS) + (size_t)TP * 8 * sizeof(TS);
+    return (size_t)SE * 28 * sizeof(TS) + (size_t)SE * 8 * sizeof(TS);
   }
   __host__ __device__ static constexpr size_t vec_bytes(int64_t ncam) {
     return ((size_t)ncam * 9 * sizeof(TV) + 127) & ~(size_t)127;
   }
   __host__ __device__ static constexpr size_t bytes(int64_t ncam, bool stage_x) {
-    return vec_bytes(ncam) * (stage_x ? 2 : 1) + FAST_GROUPS * 2 * stage_bytes() +
-           FAST_GROUPS * ((size_t)TE * 3 * sizeof(TV) + (size_t)TP * 3 * sizeof(TV)) + 64;
+    return vec_bytes(ncam) * (stage_x ? 2 : 1) + 128 + FAST_GROUPS * FAST_STAGES * stage_bytes() +
+           (size_t)FAST_GROUPS * WPS * 96 * sizeof(TV);
   }
 };
 
@@ -222,123 +200,132 @@ __device__ __forceinline__ void load_record(const double* rec, TV (&E)[27], uint
 // skip:  return at once when *skip != 0 (finished PCG)
 // gate:  return at once when *gate == 0 (conditional residual replacement)
 template <class TS, class TV, bool XS>
-__global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::GT, 1)
+__global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
     k_fast_apply(int64_t ncam, FastTiles tiles, const TS* erec, const TS* prec, const TV* z, const TV* pv,
                  const double* beta, TV* partials, const int* skip, const int* gate, int* error) {
-  constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP, GT = FastShape<TS>::GT;
-  constexpr int NTHR = FAST_GROUPS * GT;
-  static_assert(TE == GT, "one edge per thread");
+  constexpr int WPS = FastShape<TS>::WPS, GT = WPS * 32, NTHR = FAST_GROUPS * GT, SE = WPS * 32;
   if (skip && *skip) return;
   if (gate && !*gate) return;
   extern __shared__ __align__(128) unsigned char smem[];
-  const int tid = threadIdx.x;
-  const int g = tid / GT, gtid = tid % GT;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int g = tid / GT, w = (tid % GT) >> 5, gtid = tid % GT;
   const int64_t ny = ncam * 9;
   const size_t vb = FastSmem<TS, TV>::vec_bytes(ncam);
   TV* ys = reinterpret_cast<TV*>(smem);
   TV* xs = reinterpret_cast<TV*>(smem + vb);
-  unsigned char* stage_base = smem + vb * (XS ? 2 : 1);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + vb * (XS ? 2 : 1));
+  unsigned char* stage_base = smem + vb * (XS ? 2 : 1) + 128;
   constexpr size_t sbytes = FastSmem<TS, TV>::stage_bytes();
-  unsigned char* gstage = stage_base + (size_t)g * 2 * sbytes;
-  TV* u = reinterpret_cast<TV*>(stage_base + FAST_GROUPS * 2 * sbytes) + (size_t)g * (TE * 3 + TP * 3);
-  TV* tp = u + TE * 3;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<TV*>(stage_base + FAST_GROUPS * 2 * sbytes) +
-                                               FAST_GROUPS * (TE * 3 + TP * 3));
-  uint64_t* gbar = bars + 2 * g;
+  unsigned char* gstage = stage_base + (size_t)g * FAST_STAGES * sbytes;
+  TV* tpw = reinterpret_cast<TV*>(stage_base + FAST_GROUPS * FAST_STAGES * sbytes) + (size_t)(g * WPS + w) * 96;
+  uint64_t* gbar = bars + FAST_STAGES * g;
+  volatile int* fail = reinterpret_cast<volatile int*>(bars + FAST_GROUPS * FAST_STAGES);  // one flag per group
 
-  // x = z + beta p (PCG search direction formed on the fly) or x = z
   const TV bv = pv ? (TV)*beta : (TV)0;
   for (int64_t i = tid; i < ny; i += NTHR) {
     ys[i] = 0;
     if (XS) xs[i] = pv ? z[i] + bv * pv[i] : z[i];
   }
   if (tid == 0) {
-    for (int i = 0; i < 2 * FAST_GROUPS; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < FAST_GROUPS * FAST_STAGES; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < FAST_GROUPS; ++i) fail[i] = 0;
     mbar_fence_init();
   }
   __syncthreads();
 
-  auto issue = [&](int64_t t, int s) {
-    int64_t e0 = tiles.ebeg[t], e1 = tiles.ebeg[t + 1], p0 = tiles.pbeg[t], p1 = tiles.pbeg[t + 1];
+  auto issue = [&](int64_t sidx, int b) {
+    int64_t wt0 = sidx * WPS, wt1 = min(wt0 + WPS, tiles.nwt);
+    int64_t e0 = tiles.wt_e0[wt0], e1 = tiles.wt_e0[wt1], p0 = tiles.wt_p0[wt0], p1 = tiles.wt_p0[wt1];
     unsigned eb = (unsigned)((e1 - e0) * 28 * sizeof(TS)), pb = (unsigned)((p1 - p0) * 8 * sizeof(TS));
-    unsigned char* dst = gstage + s * sbytes;
-    mbar_expect_tx(&gbar[s], eb + pb);
-    if (eb) tma_load_1d(dst, erec + e0 * 28, eb, &gbar[s]);
-    if (pb) tma_load_1d(dst + (size_t)TE * 28 * sizeof(TS), prec + p0 * 8, pb, &gbar[s]);
+    unsigned char* dst = gstage + b * sbytes;
+    mbar_expect_tx(&gbar[b], eb + pb);
+    if (eb) tma_load_1d(dst, erec + e0 * 28, eb, &gbar[b]);
+    if (pb) tma_load_1d(dst + (size_t)SE * 28 * sizeof(TS), prec + p0 * 8, pb, &gbar[b]);
   };
 
   const int64_t first = (int64_t)blockIdx.x * FAST_GROUPS + g, stride = (int64_t)gridDim.x * FAST_GROUPS;
-  if (gtid == 0) {
-    if (first < tiles.ntiles) issue(first, 0);
-    if (first + stride < tiles.ntiles) issue(first + stride, 1);
-  }
+  if (gtid == 0)
+    for (int b = 0; b < FAST_STAGES; ++b)
+      if (first + b * stride < tiles.nstages) issue(first + b * stride, b);
   bool failed = false;
   int k = 0;
-  for (int64_t t = first; t < tiles.ntiles; t += stride, ++k) {
-    const int s = k & 1;
-    const unsigned parity = (k >> 1) & 1;
-    if (!mbar_wait_bounded(&gbar[s], parity, 1u << 22)) {
+  for (int64_t sidx = first; sidx < tiles.nstages; sidx += stride, ++k) {
+    const int b = k % FAST_STAGES;
+    const unsigned parity = (k / FAST_STAGES) & 1;
+    // Bounded wait; a timeout is made uniform across the group through the
+    // flag read after the stage barrier, so no thread is left at the barrier.
+    const bool ok = mbar_wait_bounded(&gbar[b], parity, 1u << 22);
+    if (!ok) fail[g] = 1;
+    const int64_t wt = sidx * WPS + w;
+    if (ok && wt < tiles.nwt) {
+      const TS* er = reinterpret_cast<const TS*>(gstage + b * sbytes);
+      const TS* pr = er + (size_t)SE * 28;
+      const int64_t se0 = tiles.wt_e0[sidx * WPS], sp0 = tiles.wt_p0[sidx * WPS];
+      const int64_t e_lo = tiles.wt_e0[wt] - se0, p_lo = tiles.wt_p0[wt] - sp0;
+      const int cnt = (int)(tiles.wt_e0[wt + 1] - tiles.wt_e0[wt]);
+      TV E[27];
+      uint32_t cam = 0, lp = 0xFFFFu;
+      TV u0 = 0, u1 = 0, u2 = 0;
+      if (lane < cnt) {
+        load_record<TV>(er + (size_t)(e_lo + lane) * 28, E, cam, lp);
+        TV xc[9];
+        if (XS) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) xc[c] = xs[(int64_t)cam * 9 + c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) {
+            int64_t i = (int64_t)cam * 9 + c;
+            xc[c] = pv ? z[i] + bv * pv[i] : z[i];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          u0 += E[c] * xc[c];
+          u1 += E[9 + c] * xc[c];
+          u2 += E[18 + c] * xc[c];
+        }
+      }
+      // segmented inclusive scan over the lanes of each point
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        TV v0 = __shfl_up_sync(0xffffffffu, u0, off), v1 = __shfl_up_sync(0xffffffffu, u1, off);
+        TV v2 = __shfl_up_sync(0xffffffffu, u2, off);
+        uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
+        if (lane >= off && lo == lp) {
+          u0 += v0;
+          u1 += v1;
+          u2 += v2;
+        }
+      }
+      uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
+      bool last = lane < cnt && (lane == cnt - 1 || lpn != lp);
+      if (last) {
+        const TS* r = pr + (size_t)(p_lo + lp) * 8;
+        TV c0 = (TV)r[0], c1 = (TV)r[1], c2 = (TV)r[2], c3 = (TV)r[3], c4 = (TV)r[4], c5 = (TV)r[5];
+        tpw[lp * 3] = c0 * u0 + c1 * u1 + c2 * u2;
+        tpw[lp * 3 + 1] = c1 * u0 + c3 * u1 + c4 * u2;
+        tpw[lp * 3 + 2] = c2 * u0 + c4 * u1 + c5 * u2;
+      }
+      __syncwarp();
+      if (lane < cnt) {
+        TV t0 = tpw[lp * 3], t1 = tpw[lp * 3 + 1], t2 = tpw[lp * 3 + 2];
+        TV* y = ys + (int64_t)cam * 9;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
+      }
+      __syncwarp();
+    }
+    group_sync(1 + g, GT);  // every warp of the group is done with stage b
+    if (fail[g]) {
       failed = true;
       break;
     }
-    const TS* er = reinterpret_cast<const TS*>(gstage + s * sbytes);
-    const TS* pr = er + (size_t)TE * 28;
-    const int ne = (int)(tiles.ebeg[t + 1] - tiles.ebeg[t]);
-    const int np = (int)(tiles.pbeg[t + 1] - tiles.pbeg[t]);
-    // phase 1: u_e = E_e^T x_cam
-    TV E[27];
-    uint32_t cam = 0, lp = 0;
-    if (gtid < ne) {
-      load_record<TV>(er + (size_t)gtid * 28, E, cam, lp);
-      TV xc[9];
-      if (XS) {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) xc[c] = xs[(int64_t)cam * 9 + c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-          int64_t i = (int64_t)cam * 9 + c;
-          xc[c] = pv ? z[i] + bv * pv[i] : z[i];
-        }
-      }
-#pragma unroll
-      for (int p = 0; p < 3; ++p) {
-        TV acc = 0;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) acc += E[p * 9 + c] * xc[c];
-        u[gtid * 3 + p] = acc;
-      }
-    }
-    group_sync(1 + g, GT);
-    // phase 2: t_p = C_p^-1 sum u
-    if (gtid < np) {
-      const TS* r = pr + (size_t)gtid * 8;
-      uint32_t f0 = rec_u32<TS>(r + 6), cnt = rec_u32<TS>(r + 7);
-      TV a0 = 0, a1 = 0, a2 = 0;
-      for (uint32_t e = f0; e < f0 + cnt; ++e) {
-        a0 += u[e * 3];
-        a1 += u[e * 3 + 1];
-        a2 += u[e * 3 + 2];
-      }
-      TV c0 = (TV)r[0], c1 = (TV)r[1], c2 = (TV)r[2], c3 = (TV)r[3], c4 = (TV)r[4], c5 = (TV)r[5];
-      tp[gtid * 3] = c0 * a0 + c1 * a1 + c2 * a2;
-      tp[gtid * 3 + 1] = c1 * a0 + c3 * a1 + c4 * a2;
-      tp[gtid * 3 + 2] = c2 * a0 + c4 * a1 + c5 * a2;
-    }
-    group_sync(1 + g, GT);
-    // phase 3: y_cam -= E_e t_p
-    if (gtid < ne) {
-      TV t0 = tp[lp * 3], t1 = tp[lp * 3 + 1], t2 = tp[lp * 3 + 2];
-      TV* y = ys + (int64_t)cam * 9;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
-    }
-    group_sync(1 + g, GT);  // stage s, u and tp free
-    if (gtid == 0 && t + 2 * stride < tiles.ntiles) issue(t + 2 * stride, s);
+    if (gtid == 0 && sidx + FAST_STAGES * stride < tiles.nstages) issue(sidx + FAST_STAGES * stride, b);
   }
   if (failed) {
     if (gtid == 0) atomicExch(error, 1);
-    for (int s = 0; s < 2; ++s) mbar_wait_bounded(&gbar[s], ((k + s) >> 1) & 1, 1u << 16);
+    for (int b = 0; b < FAST_STAGES; ++b) mbar_wait_bounded(&gbar[b], ((k + b) / FAST_STAGES) & 1, 1u << 16);
   }
   __syncthreads();
   TV* out = partials + (int64_t)blockIdx.x * ny;
@@ -421,11 +408,10 @@ struct FastPath {
   bool on = false;          // records are current and the shape qualifies
   bool structure = false;   // tiles and local indices built for the current structure
   bool disabled = false;    // force the generic operator (tests)
-  int64_t ntiles = 0;
+  int64_t nwt = 0, nstages = 0;
   int grid = 0;
-  size_t smem = 0;
   DBuf<int64_t> d_pbeg, d_ebeg;
-  DBuf<uint32_t> d_lp, d_lfirst, d_count;
+  DBuf<uint32_t> d_lp;
   DBuf<TS> d_erec, d_prec;
   DBuf<float> d_parts_f;
   DBuf<double> d_parts_d;
@@ -437,38 +423,31 @@ struct FastPath {
     structure = false;
   }
 
-  // Tiles over point-major edges: greedy contiguous point ranges.
+  // Warp tiles over point-major edges: greedy contiguous point ranges of at
+  // most 32 edges; a point with more than 32 observations keeps the generic path.
   template <class Impl>
   fg_status build(Impl& s, const std::vector<int64_t>& pt_off) {
-    constexpr int TE = FastShape<TS>::TE, TP = FastShape<TS>::TP;
-    std::vector<int64_t> pbeg{0}, ebeg{0};
-    std::vector<uint32_t> lp(s.nedges), lfirst(s.nP), count(s.nP);
-    int64_t ecur = 0, pcur = 0;
+    std::vector<int64_t> e0{0}, p0{0};
+    std::vector<uint32_t> lp(s.nedges);
     for (int64_t p = 0; p < (int64_t)s.nP; ++p) {
       int64_t c = pt_off[p + 1] - pt_off[p];
-      if (c > TE) return FG_OK;  // track longer than a tile: generic operator
-      if ((pt_off[p + 1] - ebeg.back()) > TE || (p + 1 - pbeg.back()) > TP) {
-        pbeg.push_back(p);
-        ebeg.push_back(pt_off[p]);
+      if (c > 32) return FG_OK;
+      if ((pt_off[p + 1] - e0.back()) > 32 || (p + 1 - p0.back()) > 32) {
+        e0.push_back(pt_off[p]);
+        p0.push_back(p);
       }
-      (void)ecur;
-      (void)pcur;
     }
-    pbeg.push_back((int64_t)s.nP);
-    ebeg.push_back((int64_t)s.nedges);
-    ntiles = (int64_t)pbeg.size() - 1;
-    for (int64_t t = 0; t < ntiles; ++t)
-      for (int64_t p = pbeg[t]; p < pbeg[t + 1]; ++p) {
-        lfirst[p] = (uint32_t)(pt_off[p] - ebeg[t]);
-        count[p] = (uint32_t)(pt_off[p + 1] - pt_off[p]);
-        for (int64_t k = pt_off[p]; k < pt_off[p + 1]; ++k) lp[k] = (uint32_t)(p - pbeg[t]);
-      }
+    e0.push_back((int64_t)s.nedges);
+    p0.push_back((int64_t)s.nP);
+    nwt = (int64_t)e0.size() - 1;
+    for (int64_t t = 0; t < nwt; ++t)
+      for (int64_t p = p0[t]; p < p0[t + 1]; ++p)
+        for (int64_t k = pt_off[p]; k < pt_off[p + 1]; ++k) lp[k] = (uint32_t)(p - p0[t]);
+    nstages = (nwt + FastShape<TS>::WPS - 1) / FastShape<TS>::WPS;
     cudaStream_t st = s.st;
-    FG_TRY(upload(d_pbeg, pbeg.data(), pbeg.size(), st));
-    FG_TRY(upload(d_ebeg, ebeg.data(), ebeg.size(), st));
+    FG_TRY(upload(d_pbeg, p0.data(), p0.size(), st));
+    FG_TRY(upload(d_ebeg, e0.data(), e0.size(), st));
     FG_TRY(upload(d_lp, lp.data(), lp.size(), st));
-    FG_TRY(upload(d_lfirst, lfirst.data(), lfirst.size(), st));
-    FG_TRY(upload(d_count, count.data(), count.size(), st));
     FG_TRY(d_erec.resize(std::max<size_t>(s.nedges * 28, 1)));
     FG_TRY(d_prec.resize(std::max<size_t>(s.nP * 8, 1)));
     FG_TRY(d_error.resize(1));
@@ -503,7 +482,7 @@ struct FastPath {
   fg_status refresh_points(Impl& s, double lambda) {
     if (!on) return FG_OK;
     FG_LAUNCH(k_fast_point_records<TS>, grid_for(s.nP, 256), 256, 0, s.st, s.layout(), s.d_factors.get(),
-              s.d_observed.get(), lambda, d_lfirst.get(), d_count.get(), d_prec.get());
+              s.d_observed.get(), lambda, d_prec.get());
     return FG_OK;
   }
 
@@ -534,9 +513,9 @@ struct FastPath {
     bool xs = FastSmem<TS, TV>::bytes((int64_t)s.nC, true) <= (size_t)optin;
     size_t sm = FastSmem<TS, TV>::bytes((int64_t)s.nC, xs);
     size_t& granted = attr_set[std::is_same<TV, double>::value ? 1 : 0][xs ? 1 : 0];
-    FastTiles tl{d_pbeg.get(), d_ebeg.get(), ntiles};
+    FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
     const int* skip = pst ? &pst->done : nullptr;
-    constexpr int NTHR = FAST_GROUPS * FastShape<TS>::GT;
+    constexpr int NTHR = FAST_GROUPS * FastShape<TS>::WPS * 32;
     if (xs) {
       auto kern = k_fast_apply<TS, TV, true>;
       if (granted < sm) {
