@@ -197,12 +197,23 @@ __device__ __forceinline__ void load_record(const double* rec, TV (&E)[27], uint
   lp = RecWord<double>::lp(w);
 }
 
+// Modes of the edge-record pass (all read every record once):
+//   FAST_APPLY:   partials <- -E C^-1 E^T x                 (x = z + beta p)
+//   FAST_RHS:     partials <- -E w_p, w_p read per point     (src/schur.rs:230-242)
+//   FAST_RECOVER: step_p = C^-1 (w_p - sum_e E_e^T z_c) / D_p (src/schur.rs:319-343)
+enum FastMode { FAST_APPLY = 0, FAST_RHS = 1, FAST_RECOVER = 2 };
+struct FastExtra {
+  const double* wp;      // RHS: C^-1 (-g/D) per eliminated coordinate; RECOVER: g (index 3p+i)
+  const double* scales;  // RECOVER: D for eliminated coordinates (index 3p+i)
+  double* step;          // RECOVER: output, eliminated coordinates (index 3p+i)
+};
+
 // skip:  return at once when *skip != 0 (finished PCG)
 // gate:  return at once when *gate == 0 (conditional residual replacement)
-template <class TS, class TV, bool XS>
+template <class TS, class TV, bool XS, int MODE = FAST_APPLY>
 __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
     k_fast_apply(int64_t ncam, FastTiles tiles, const TS* erec, const TS* prec, const TV* z, const TV* pv,
-                 const double* beta, TV* partials, const int* skip, const int* gate, int* error) {
+                 const double* beta, TV* partials, const int* skip, const int* gate, int* error, FastExtra ex) {
   constexpr int WPS = FastShape<TS>::WPS, GT = WPS * 32, NTHR = FAST_GROUPS * GT, SE = WPS * 32;
   if (skip && *skip) return;
   if (gate && !*gate) return;
@@ -266,8 +277,9 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
       TV E[27];
       uint32_t cam = 0, lp = 0xFFFFu;
       TV u0 = 0, u1 = 0, u2 = 0;
-      if (lane < cnt) {
-        load_record<TV>(er + (size_t)(e_lo + lane) * 28, E, cam, lp);
+      const int64_t gp0 = tiles.wt_p0[wt];  // global index of the tile's first point
+      if (lane < cnt) load_record<TV>(er + (size_t)(e_lo + lane) * 28, E, cam, lp);
+      if (MODE != FAST_RHS && lane < cnt) {
         TV xc[9];
         if (XS) {
 #pragma unroll
@@ -300,15 +312,31 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
       }
       uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
       bool last = lane < cnt && (lane == cnt - 1 || lpn != lp);
-      if (last) {
+      if (MODE == FAST_RHS) {
+        if (last) {
+          const double* w3 = ex.wp + 3 * (gp0 + lp);
+          tpw[lp * 3] = (TV)w3[0];
+          tpw[lp * 3 + 1] = (TV)w3[1];
+          tpw[lp * 3 + 2] = (TV)w3[2];
+        }
+      } else if (last) {
         const TS* r = pr + (size_t)(p_lo + lp) * 8;
         TV c0 = (TV)r[0], c1 = (TV)r[1], c2 = (TV)r[2], c3 = (TV)r[3], c4 = (TV)r[4], c5 = (TV)r[5];
-        tpw[lp * 3] = c0 * u0 + c1 * u1 + c2 * u2;
-        tpw[lp * 3 + 1] = c1 * u0 + c3 * u1 + c4 * u2;
-        tpw[lp * 3 + 2] = c2 * u0 + c4 * u1 + c5 * u2;
+        if (MODE == FAST_RECOVER) {
+          const int64_t q = 3 * (gp0 + lp);
+          TV a0 = (TV)(-ex.wp[q] / ex.scales[q]) - u0, a1 = (TV)(-ex.wp[q + 1] / ex.scales[q + 1]) - u1;
+          TV a2 = (TV)(-ex.wp[q + 2] / ex.scales[q + 2]) - u2;
+          ex.step[q] = (double)(c0 * a0 + c1 * a1 + c2 * a2) / ex.scales[q];
+          ex.step[q + 1] = (double)(c1 * a0 + c3 * a1 + c4 * a2) / ex.scales[q + 1];
+          ex.step[q + 2] = (double)(c2 * a0 + c4 * a1 + c5 * a2) / ex.scales[q + 2];
+        } else {
+          tpw[lp * 3] = c0 * u0 + c1 * u1 + c2 * u2;
+          tpw[lp * 3 + 1] = c1 * u0 + c3 * u1 + c4 * u2;
+          tpw[lp * 3 + 2] = c2 * u0 + c4 * u1 + c5 * u2;
+        }
       }
       __syncwarp();
-      if (lane < cnt) {
+      if (MODE != FAST_RECOVER && lane < cnt) {
         TV t0 = tpw[lp * 3], t1 = tpw[lp * 3 + 1], t2 = tpw[lp * 3 + 2];
         TV* y = ys + (int64_t)cam * 9;
 #pragma unroll
@@ -328,6 +356,7 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
     for (int b = 0; b < FAST_STAGES; ++b) mbar_wait_bounded(&gbar[b], ((k + b) / FAST_STAGES) & 1, 1u << 16);
   }
   __syncthreads();
+  if (MODE == FAST_RECOVER) return;
   TV* out = partials + (int64_t)blockIdx.x * ny;
   for (int64_t i = tid; i < ny; i += NTHR) out[i] = ys[i];
 }
@@ -338,7 +367,7 @@ template <class TS, class TV>
 __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram,
                                                       const uint8_t* observed, const TV* z, const TV* pv,
                                                       const double* beta, double lambda, const double* lam_dev,
-                                                      TV* q, double* dparts,
+                                                      int use_gram, TV* q, double* dparts,
                                                       PcgState* st, const int* gate) {
   if (st && st->done) return;
   if (gate && !*gate) return;
@@ -369,7 +398,7 @@ __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, c
     TV xi = pv ? z[i] + bv * pv[i] : z[i];
     const double lam = lam_dev ? *lam_dev : lambda;
     TV v = (TV)lam * xi;
-    if (observed[cam]) {
+    if (use_gram && observed[cam]) {
       const TS* g = gram + cam * 81;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
@@ -523,7 +552,7 @@ struct FastPath {
         granted = sm;
       }
       FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
-                parts, skip, gate, d_error.get());
+                parts, skip, gate, d_error.get(), FastExtra{});
     } else {
       auto kern = k_fast_apply<TS, TV, false>;
       if (granted < sm) {
@@ -531,11 +560,48 @@ struct FastPath {
         granted = sm;
       }
       FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
-                parts, skip, gate, d_error.get());
+                parts, skip, gate, d_error.get(), FastExtra{});
     }
     FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
-              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, out,
+              (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
               dparts, pst, gate);
+    return FG_OK;
+  }
+
+  // rhs_c = w_c - sum_{e in c} E_e w_p (src/schur.rs:216-242) from the edge
+  // records; w is the scaled-gradient work vector with C^-1 already applied
+  // to its eliminated part.
+  template <class Impl>
+  fg_status rhs(Impl& s, const double* w, double* rhs_out) {
+    if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    size_t sm = FastSmem<TS, double>::bytes((int64_t)s.nC, false);
+    auto kern = k_fast_apply<TS, double, false, FAST_RHS>;
+    FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
+    FastExtra ex{w + s.retained, nullptr, nullptr};
+    FG_LAUNCH(kern, grid, FAST_GROUPS * FastShape<TS>::WPS * 32, sm, s.st, (int64_t)s.nC, tl, d_erec.get(),
+              d_prec.get(), w, (const double*)nullptr, (const double*)nullptr, d_parts_d.get(), (const int*)nullptr,
+              (const int*)nullptr, d_error.get(), ex);
+    FG_LAUNCH((k_fast_reduce<TS, double>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
+              (const double*)d_parts_d.get(), s.d_gram.get(), s.d_observed.get(), w, (const double*)nullptr,
+              (const double*)nullptr, 1.0, (const double*)nullptr, 0, rhs_out, (double*)nullptr, (PcgState*)nullptr,
+              (const int*)nullptr);
+    return FG_OK;
+  }
+
+  // step_p = C^-1 (-g_p/D_p - sum_{e in p} E_e^T z_c) / D_p for every point
+  // with observations (src/schur.rs:312-344); g is the gradient.
+  template <class Impl>
+  fg_status recover(Impl& s, const double* zred, const double* g, const double* scales, double* step) {
+    if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    size_t sm = FastSmem<TS, double>::bytes((int64_t)s.nC, false);
+    auto kern = k_fast_apply<TS, double, false, FAST_RECOVER>;
+    FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
+    FastExtra ex{g + s.retained, scales + s.retained, step + s.retained};
+    FG_LAUNCH(kern, grid, FAST_GROUPS * FastShape<TS>::WPS * 32, sm, s.st, (int64_t)s.nC, tl, d_erec.get(),
+              d_prec.get(), zred, (const double*)nullptr, (const double*)nullptr, d_parts_d.get(), (const int*)nullptr,
+              (const int*)nullptr, d_error.get(), ex);
     return FG_OK;
   }
 };

@@ -56,6 +56,8 @@ class SchurImpl final : public Backend {
   std::vector<HostEdge> up_edges;
   size_t up_rows = 0;
   bool structure_valid = false;
+  bool pure_pairs = false;     // every emission is exactly one camera-point edge
+  bool cross_current = false;  // d_cross holds this linearization's cross blocks
 
   // ---- model source
   enum Source { NONE, HOST, DEVICE_BAL } source = NONE;
@@ -268,6 +270,7 @@ class SchurImpl final : public Backend {
       if (i == 0 || blocks[i].row != blocks[i - 1].row || blocks[i].rows == 0) emi.push_back((int64_t)i);
     emi.push_back((int64_t)nblocks);
     nemissions = emi.size() - 1;
+    pure_pairs = nedges > 0 && nblocks == 2 * nedges && nemissions == nedges;
     FG_TRY(upload(d_blocks, mb.data(), mb.size(), st));
     FG_TRY(upload(d_edges, me.data(), me.size(), st));
     FG_TRY(upload(d_var_off, var_off.data(), var_off.size(), st));
@@ -399,12 +402,16 @@ class SchurImpl final : public Backend {
     }
     if (nedges) {
       if (fast.ready_for(*this)) {
-        FG_LAUNCH(k_edge_records_fused<TS>, grid_for(nedges * (cw * pw + 1), 256), 256, 0, st, (int64_t)nedges,
-                  (int)cw, (int)pw, d_pt_edge.get(), d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(),
-                  fast.d_lp.get(), fast.d_erec.get(), d_cross.get(), bad + 1);
+        // the reference-layout cross array is only needed by the generic
+        // right-hand side / back-substitution and the Schur-diagonal factor
+        cross_current = !pure_pairs || opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL;
+        FG_LAUNCH(k_edge_records2<TS>, grid_for(nedges, REC_T), REC_T, 0, st, (int64_t)nedges, d_pt_edge.get(),
+                  d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), fast.d_lp.get(), fast.d_erec.get(),
+                  cross_current ? d_cross.get() : (TS*)nullptr, bad + 1);
         fast.on = true;
       } else {
         fast.on = false;
+        cross_current = true;
         FG_LAUNCH(k_cross<TS>, grid_for(nedges * cw * pw, NT), NT, 0, st, (int64_t)nedges, (int)cw, (int)pw,
                   d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_cross.get(), bad + 1);
       }
@@ -437,6 +444,7 @@ class SchurImpl final : public Backend {
     FG_CUDA(cudaStreamSynchronize(st));
     *fallbacks = h_count.get()[0];
     if (*fallbacks == 0 && opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL && nC) {
+      FG_TRY(ensure_cross());
       FG_DISPATCH_WIDTHS(cw, pw, {
         FG_LAUNCH((k_cam_schur_diag<CW_, PW_, TS>), grid_for(nC * 32, 128), 128, 0, st, L, d_cam_edge_off.get(),
                   d_cam_edge.get(), d_edges.get(), d_cross.get(), d_observed.get(), d_gram.get(), d_factors.get(),
@@ -450,6 +458,15 @@ class SchurImpl final : public Backend {
       });
     }
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
+    return FG_OK;
+  }
+  // The reference-layout cross blocks on demand (the fast path skips them).
+  fg_status ensure_cross() {
+    if (cross_current || !nedges) return FG_OK;
+    FG_CUDA(cudaMemsetAsync(d_flags.get() + 1, 0, sizeof(int), st));
+    FG_LAUNCH(k_cross<TS>, grid_for(nedges * cw * pw, NT), NT, 0, st, (int64_t)nedges, (int)cw, (int)pw,
+              d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), d_cross.get(), d_flags.get() + 1);
+    cross_current = true;
     return FG_OK;
   }
   const TS* precond_factors() const {
@@ -868,7 +885,11 @@ class SchurImpl final : public Backend {
         for (size_t k = 0; k < w * w; ++k) gram[start + k] = all[go + k];
       }
     }
-    if (cross && ready) FG_TRY(fetch(d_cross.get(), nedges * cw * pw, cross));
+    if (cross && ready) {
+      FG_TRY(ensure_cross());
+      FG_CUDA(cudaStreamSynchronize(st));
+      FG_TRY(fetch(d_cross.get(), nedges * cw * pw, cross));
+    }
     return FG_OK;
   }
 

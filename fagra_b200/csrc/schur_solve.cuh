@@ -214,6 +214,7 @@ fg_status SchurImpl<TS>::launch_point_solve(double lambda) {
 template <class TS>
 fg_status SchurImpl<TS>::launch_rhs() {
   if (!nC) return FG_OK;
+  if (fast.enabled() && !cross_current) return fast.rhs(*this, d_work.get(), d_rhs.get());
   Layout L = layout();
   PView<double> w{d_work.get(), nullptr, nullptr};
   FG_DISPATCH_WIDTHS(cw, pw, {
@@ -240,6 +241,10 @@ fg_status SchurImpl<TS>::launch_recover(double lambda) {
   Layout L = layout();
   if (retained) FG_LAUNCH(k_step_cams, grid_for(retained, NT), NT, 0, st, (int64_t)retained, d_zred.get(),
                           d_scales.get(), d_step.get());
+  if (nP && fast.enabled() && !cross_current) {
+    FG_CUDA(cudaMemsetAsync(d_step.get() + retained, 0, (dim - retained) * sizeof(double), st));
+    return fast.recover(*this, d_zred.get(), d_g.get(), d_scales.get(), d_step.get());
+  }
   if (nP) {
     FG_DISPATCH_WIDTHS(cw, pw, {
       FG_LAUNCH((k_recover_points<CW_, PW_, TS>), grid_for(nP, 128), 128, 0, st, L, d_pt_edge_off.get(),

@@ -185,4 +185,59 @@ __global__ void k_edge_records_fused(int64_t nedges, int cw, int pw, const int64
   }
 }
 
+// Edge records for the single-pass operator (BAL 9/3 shape), one thread per
+// point-major edge: E_e[p,c] = sum_rows (J_cam[:,c]/D)(J_pt[:,p]/D) computed
+// from the Jacobian blocks once, staged in shared memory and stored to the
+// contiguous record range with coalesced writes. cross (optional) receives the
+// reference layout (e*3+p)*9+c for the generic kernels that still read it.
+constexpr int REC_T = 128;
+template <class TS>
+__global__ void __launch_bounds__(REC_T) k_edge_records2(int64_t nedges, const int64_t* pt_edge,
+                                                         const DEdgeMeta* edges, const DBlockMeta* blocks,
+                                                         const TS* values, const double* scales,
+                                                         const uint32_t* local_point, TS* rec, TS* cross, int* bad) {
+  __shared__ TS tile[REC_T * 29];
+  const int64_t k0 = (int64_t)blockIdx.x * REC_T, k = k0 + threadIdx.x;
+  const int nk = (int)min((int64_t)REC_T, nedges - k0);
+  if (k < nedges) {
+    const int64_t e = pt_edge[k];
+    const DEdgeMeta ed = edges[e];
+    const DBlockMeta l = blocks[ed.lblk], r = blocks[ed.rblk];
+    double ic[9], ip[3];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) ic[c] = 1.0 / scales[l.col + c];
+#pragma unroll
+    for (int p = 0; p < 3; ++p) ip[p] = 1.0 / scales[r.col + p];
+    double E[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) E[i] = 0;
+    for (int row = 0; row < l.rows; ++row) {
+      double jc[9], jp[3];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) jc[c] = (double)values[l.start + (int64_t)c * l.rows + row] * ic[c];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) jp[p] = (double)values[r.start + (int64_t)p * r.rows + row] * ip[p];
+#pragma unroll
+      for (int p = 0; p < 3; ++p)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) E[p * 9 + c] += jc[c] * jp[p];
+    }
+    bool ok = true;
+    TS* t = tile + threadIdx.x * 29;
+#pragma unroll
+    for (int i = 0; i < 27; ++i) {
+      ok = ok && isfinite(E[i]);
+      t[i] = (TS)E[i];
+    }
+    typename RecWord<TS>::U word = RecWord<TS>::pack((uint32_t)ed.cam, local_point[k]);
+    memcpy(&t[27], &word, sizeof(word));
+    if (!ok) atomicOr(bad, 1);
+    if (cross)
+      for (int i = 0; i < 27; ++i) cross[e * 27 + i] = t[i];
+  }
+  __syncthreads();
+  TS* out = rec + k0 * 28;
+  for (int i = threadIdx.x; i < nk * 28; i += REC_T) out[i] = tile[(i / 28) * 29 + (i % 28)];
+}
+
 }  // namespace fg
