@@ -227,6 +227,9 @@ def run_gpu(args, rank: int, world: int, device: int):
             fg.errors.raise_for_status(_lib.lib.fg_schur_time_operator(backend.handle, 1e-3, 50, C.byref(sec_op),
                                                                         C.byref(bytes_op)))
             results[name]["operator"] = dict(seconds=sec_op.value, bytes=bytes_op.value)
+            var, tuned = C.c_int(), (C.c_double * 2)()
+            _lib.lib.fg_schur_operator_info(backend.handle, C.byref(var), tuned)
+            results[name]["operator"].update(variant=var.value, tuned_seconds=[tuned[0], tuned[1]])
             head_backend = backend
     # e2e: public C ABI from host arrays
     e2e = None
@@ -325,7 +328,11 @@ def main():
             forms={k: {kk: vv for kk, vv in v.items() if kk != "operator"} for k, v in results.items()},
             speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,
             pcg_iterations=results[head]["cg_iterations"],
-            roofline=dict(bound="hbm", kernel="reduced operator (k_points + k_cams)", achieved=achieved, peak=pk,
+            roofline=dict(bound="hbm", kernel={0: "reduced operator, generic (k_points + k_cams)",
+                                               1: "reduced operator, TMA-staged single pass (k_fast_apply + k_fast_reduce)",
+                                               2: "reduced operator, direct-load single pass (k_fast_apply_direct + "
+                                                  "k_fast_reduce)"}.get(op.get("variant"), "reduced operator"),
+                          operator_variant_seconds=op.get("tuned_seconds"), achieved=achieved, peak=pk,
                           peak_source=src, unit="GB/s", frac=(achieved / pk) if achieved else None,
                           algorithmic_bytes_per_launch=op.get("bytes"), seconds_per_launch=op.get("seconds"),
                           traffic=traffic),

@@ -334,6 +334,12 @@ FG_API fg_status fg_schur_time_operator(fg_backend* b, double lambda, size_t rep
   FG_GUARD_BEGIN return b->impl->time_operator(lambda, reps, seconds, bytes);
   FG_GUARD_END
 }
+FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds2) {
+  FG_NEED(b);
+  if (!variant) return FG_NULL_ARGUMENT;
+  b->impl->operator_info(variant, seconds2);
+  return FG_OK;
+}
 FG_API fg_status fg_gn_solve_bal(fg_backend* b, fg_bal_problem* p, const fg_optimize_options* o,
                                  fg_optimize_report* rep) {
   FG_NEED(b);

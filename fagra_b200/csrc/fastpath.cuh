@@ -361,6 +361,111 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   for (int64_t i = tid; i < ny; i += NTHR) out[i] = ys[i];
 }
 
+// Direct variant of the FAST_APPLY pass: no shared-memory staging of records.
+// Each warp grid-strides over warp tiles; a lane loads its 112/224-byte record
+// with 16-byte global loads (a tile's records are contiguous, so a warp's
+// loads coalesce), reduces its point with the same segmented shuffle scan and
+// re-reads E from L1 for the scatter, which keeps registers low enough for
+// 1,024 threads per SM. No stage barriers; x staged in shared memory.
+constexpr int DIRECT_THREADS = 1024;
+template <class TS>
+__device__ __forceinline__ void load_cross_global(const TS* rec, float (&E)[27], uint32_t& cam, uint32_t& lp);
+template <>
+__device__ __forceinline__ void load_cross_global<float>(const float* rec, float (&E)[27], uint32_t& cam,
+                                                          uint32_t& lp) {
+  const float4* v = reinterpret_cast<const float4*>(rec);
+  float f[28];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    float4 a = __ldg(v + i);
+    f[4 * i] = a.x; f[4 * i + 1] = a.y; f[4 * i + 2] = a.z; f[4 * i + 3] = a.w;
+  }
+#pragma unroll
+  for (int i = 0; i < 27; ++i) E[i] = f[i];
+  uint32_t w = __float_as_uint(f[27]);
+  cam = RecWord<float>::cam(w);
+  lp = RecWord<float>::lp(w);
+}
+
+template <bool XS>
+__global__ void __launch_bounds__(DIRECT_THREADS, 1)
+    k_fast_apply_direct(int64_t ncam, FastTiles tiles, const float* erec, const float* prec, const float* z,
+                        const float* pv, const double* beta, float* partials, const int* skip, const int* gate) {
+  if (skip && *skip) return;
+  if (gate && !*gate) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  constexpr int NW = DIRECT_THREADS / 32;
+  const int64_t ny = ncam * 9;
+  const size_t vb = FastSmem<float, float>::vec_bytes(ncam);
+  float* ys = reinterpret_cast<float*>(smem);
+  float* xs = reinterpret_cast<float*>(smem + vb);
+  float* tpw = reinterpret_cast<float*>(smem + vb * (XS ? 2 : 1)) + w * 96;
+  const float bv = pv ? (float)*beta : 0.f;
+  for (int64_t i = tid; i < ny; i += DIRECT_THREADS) {
+    ys[i] = 0;
+    if (XS) xs[i] = pv ? z[i] + bv * pv[i] : z[i];
+  }
+  __syncthreads();
+  for (int64_t wt = (int64_t)blockIdx.x * NW + w; wt < tiles.nwt; wt += (int64_t)gridDim.x * NW) {
+    const int64_t e0 = tiles.wt_e0[wt];
+    const int cnt = (int)(tiles.wt_e0[wt + 1] - e0);
+    const int64_t p0 = tiles.wt_p0[wt];
+    const float* rec = erec + (e0 + lane) * 28;
+    uint32_t cam = 0, lp = 0xFFFFu;
+    float u0 = 0, u1 = 0, u2 = 0;
+    if (lane < cnt) {
+      float E[27];
+      load_cross_global<float>(rec, E, cam, lp);
+      float xc[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        int64_t i = (int64_t)cam * 9 + c;
+        xc[c] = XS ? xs[i] : (pv ? z[i] + bv * pv[i] : z[i]);
+      }
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        u0 += E[c] * xc[c];
+        u1 += E[9 + c] * xc[c];
+        u2 += E[18 + c] * xc[c];
+      }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      float v0 = __shfl_up_sync(0xffffffffu, u0, off), v1 = __shfl_up_sync(0xffffffffu, u1, off);
+      float v2 = __shfl_up_sync(0xffffffffu, u2, off);
+      uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
+      if (lane >= off && lo == lp) {
+        u0 += v0;
+        u1 += v1;
+        u2 += v2;
+      }
+    }
+    uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
+    if (lane < cnt && (lane == cnt - 1 || lpn != lp)) {
+      const float4* r = reinterpret_cast<const float4*>(prec + (p0 + lp) * 8);
+      float4 ca = __ldg(r), cb = __ldg(r + 1);
+      tpw[lp * 3] = ca.x * u0 + ca.y * u1 + ca.z * u2;
+      tpw[lp * 3 + 1] = ca.y * u0 + ca.w * u1 + cb.x * u2;
+      tpw[lp * 3 + 2] = ca.z * u0 + cb.x * u1 + cb.y * u2;
+    }
+    __syncwarp();
+    if (lane < cnt) {
+      float E[27];
+      uint32_t c2, l2;
+      load_cross_global<float>(rec, E, c2, l2);  // L1 hit: same lines as above
+      float t0 = tpw[lp * 3], t1 = tpw[lp * 3 + 1], t2 = tpw[lp * 3 + 2];
+      float* y = ys + (int64_t)cam * 9;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  float* out = partials + (int64_t)blockIdx.x * ny;
+  for (int64_t i = tid; i < ny; i += DIRECT_THREADS) out[i] = ys[i];
+}
+
 // q = lambda x + B x + sum_b partials[b] with x = z (+ beta p); 32 coordinates
 // x 8 partial-vector chunks per block. Optional p.q -> alpha in the last block.
 template <class TS, class TV>
@@ -447,9 +552,11 @@ struct FastPath {
   DBuf<int> d_error;
 
   bool enabled() const { return on && !disabled; }
+  bool tuned = false;  // operator variant chosen for the current structure
   void invalidate() {
     on = false;
     structure = false;
+    tuned = false;
   }
 
   // Warp tiles over point-major edges: greedy contiguous point ranges of at
@@ -534,10 +641,20 @@ struct FastPath {
   int optin = 0;
   size_t attr_set[2][2] = {{0, 0}, {0, 0}};  // [TV is double][stage x] -> smem size already granted
 
+  int variant = 1;  // FP32 operator: 1 = TMA-staged stages, 2 = direct global loads
+
   template <class Impl, class TV>
   fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst,
                   const int* gate = nullptr, const double* lam_dev = nullptr) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
+    if (std::is_same<TS, float>::value && std::is_same<TV, float>::value && variant == 2) {
+      FG_TRY(apply_direct(s, (const float*)x.z, (const float*)x.pprev, x.beta, (float*)parts,
+                          pst ? &pst->done : nullptr, gate));
+      FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
+                (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
+                dparts, pst, gate);
+      return FG_OK;
+    }
     if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
     bool xs = FastSmem<TS, TV>::bytes((int64_t)s.nC, true) <= (size_t)optin;
     size_t sm = FastSmem<TS, TV>::bytes((int64_t)s.nC, xs);
@@ -565,6 +682,34 @@ struct FastPath {
     FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
               (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
               dparts, pst, gate);
+    return FG_OK;
+  }
+
+  size_t direct_granted = 0;
+  template <class Impl>
+  fg_status apply_direct(Impl& s, const float* z, const float* pv, const double* beta, float* parts, const int* skip,
+                         const int* gate) {
+    if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    size_t vb = FastSmem<float, float>::vec_bytes((int64_t)s.nC);
+    size_t tpw = (size_t)(DIRECT_THREADS / 32) * 96 * sizeof(float);
+    bool xs = 2 * vb + tpw <= (size_t)optin;
+    size_t sm = vb * (xs ? 2 : 1) + tpw;
+    FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
+    if (xs) {
+      if (direct_granted < sm) {
+        FG_CUDA(cudaFuncSetAttribute(k_fast_apply_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        direct_granted = sm;
+      }
+      FG_LAUNCH(k_fast_apply_direct<true>, grid, DIRECT_THREADS, sm, s.st, (int64_t)s.nC, tl,
+                (const float*)d_erec.get(), (const float*)d_prec.get(), z, pv, beta, parts, skip, gate);
+    } else {
+      if (direct_granted < sm) {
+        FG_CUDA(cudaFuncSetAttribute(k_fast_apply_direct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        direct_granted = sm;
+      }
+      FG_LAUNCH(k_fast_apply_direct<false>, grid, DIRECT_THREADS, sm, s.st, (int64_t)s.nC, tl,
+                (const float*)d_erec.get(), (const float*)d_prec.get(), z, pv, beta, parts, skip, gate);
+    }
     return FG_OK;
   }
 

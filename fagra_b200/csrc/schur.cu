@@ -426,6 +426,7 @@ class SchurImpl final : public Backend {
       return FG_INVALID_EVALUATION;
     }
     ready = true;
+    FG_TRY(autotune_operator());
     if (opt.collect_timings) tim.preparation += tm.stop(st);
     return FG_OK;
   }
@@ -460,6 +461,52 @@ class SchurImpl final : public Backend {
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
     return FG_OK;
   }
+  // Operator autotuner: times each FP32 single-pass variant (TMA-staged
+  // stages, direct global loads) on this structure and keeps the faster one.
+  // Runs once per structure; the factorization it needs is redone by every solve.
+  double tuned_seconds[2] = {0, 0};
+  void operator_info(int* variant, double* seconds2) const override {
+    *variant = fast.enabled() ? fast.variant : 0;
+    if (seconds2) {
+      seconds2[0] = tuned_seconds[0];
+      seconds2[1] = tuned_seconds[1];
+    }
+  }
+  fg_status autotune_operator() {
+    if (!fast.on || !is_f32() || fast.tuned) return FG_OK;
+    unsigned fb = 0;
+    FG_TRY(factor(1.0, &fb));
+    if (fb) return FG_OK;
+    FG_CUDA(cudaMemsetAsync(d_z.get(), 0, retained * sizeof(TS), st));
+    PView<TS> pv{d_z.get(), nullptr, nullptr};
+    cudaEvent_t a, b;
+    FG_CUDA(cudaEventCreate(&a));
+    FG_CUDA(cudaEventCreate(&b));
+    float best = 1e30f;
+    int best_v = 1;
+    for (int v = 1; v <= 2; ++v) {
+      fast.variant = v;
+      FG_TRY(apply_reduced<TS>(pv, 1.0, 1.0, true, d_t.get(), d_q.get(), nullptr, nullptr));
+      cudaEventRecord(a, st);
+      for (int k = 0; k < 5; ++k) FG_TRY(apply_reduced<TS>(pv, 1.0, 1.0, true, d_t.get(), d_q.get(), nullptr, nullptr));
+      cudaEventRecord(b, st);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      tuned_seconds[v - 1] = ms * 1e-3 / 5;
+      if (ms < best) {
+        best = ms;
+        best_v = v;
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    fast.variant = best_v;
+    fast.tuned = true;
+    drop_graphs();
+    return FG_OK;
+  }
+
   // The reference-layout cross blocks on demand (the fast path skips them).
   fg_status ensure_cross() {
     if (cross_current || !nedges) return FG_OK;

@@ -65,6 +65,7 @@ class Backend {
                                  double* cross) = 0;
   virtual fg_status reduced_apply(double lambda, const double* x, double* y) = 0;
   virtual fg_status time_operator(double lambda, size_t reps, double* seconds, double* bytes) = 0;
+  virtual void operator_info(int* variant, double* seconds2) const = 0;
   // Device BAL path: bind an implicit BAL structure and expose raw model storage.
   virtual fg_status bind_bal(uint64_t problem_id, size_t cameras, size_t points, size_t observations,
                              const uint32_t* order_cam, const uint32_t* order_pt) = 0;

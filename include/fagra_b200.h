@@ -273,6 +273,12 @@ FG_API fg_status fg_bal_restore_initial(fg_bal_problem* problem);
 FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size_t repetitions,
                                         double* seconds_per_apply, double* bytes_out);
 
+/* The reduced-operator implementation the autotuner chose for the current
+ * structure: 0 generic (any widths), 1 TMA-staged single pass, 2 direct-load
+ * single pass; seconds[v-1] = measured time per application of variant v
+ * (0 if not measured). */
+FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds2);
+
 /* GaussNewton::solve_batch on a device BAL problem. */
 FG_API fg_status fg_gn_solve_bal(fg_backend* backend, fg_bal_problem* problem,
                                  const fg_optimize_options* options, fg_optimize_report* report);
