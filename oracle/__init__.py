@@ -58,6 +58,16 @@ class LmStats(C.Structure):
                 ("last_rejection", C.c_int), ("linear_solves", size_t), ("linear_iterations", size_t)]
 
 
+class LsmrDiag(C.Structure):
+    _fields_ = [("termination", C.c_int), ("iterations", size_t), ("finite_step", C.c_int),
+                ("estimated_absolute", C.c_double), ("estimated_relative", C.c_double),
+                ("original_absolute", C.c_double), ("original_relative", C.c_double),
+                ("scaled_absolute", C.c_double), ("scaled_relative", C.c_double),
+                ("min_scale", C.c_double), ("max_scale", C.c_double), ("damping", C.c_double),
+                ("block_fallbacks", size_t), ("has_estimated", C.c_int), ("has_original", C.c_int),
+                ("has_scaled", C.c_int), ("has_scales", C.c_int), ("has_damping", C.c_int)]
+
+
 ACCEPT = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LmStats))
 COST = C.CFUNCTYPE(C.c_int, C.c_void_p, dptr, dptr)
 LIN = C.CFUNCTYPE(C.c_int, C.c_void_p, dptr, C.c_void_p)
@@ -110,6 +120,12 @@ _sig = {
     "or_lm_cb": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(LmOpts), C.POINTER(Report),
                            C.POINTER(LmStats)]),
     "or_gn_cb": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(Report)]),
+    "or_lsmr_create": (C.c_void_p, []),
+    "or_lsmr_set": (None, [C.c_void_p, size_t, C.c_double, C.c_int, C.c_int]),
+    "or_lsmr_diagnostics": (None, [C.c_void_p, C.POINTER(LsmrDiag)]),
+    "or_lsmr_damped_products": (None, [C.c_void_p, C.c_double, C.c_int, dptr, dptr, dptr, dptr]),
+    "or_lsmr_precond": (None, [C.c_void_p, dptr, dptr, dptr, dptr]),
+    "or_lsmr_scales": (None, [C.c_void_p, dptr]),
 }
 for _n, (_r, _a) in _sig.items():
     _f = getattr(lib, _n)
@@ -247,6 +263,79 @@ class Schur:
         y = np.zeros_like(x)
         lib.or_schur_reduced_apply(self.h, lam, _dp(x), _dp(y))
         return y
+
+
+class Lsmr(Schur):
+    """Oracle LSMR backend (src/lsmr.rs restated; faer's LSMR per Fong & Saunders).
+
+    Shares the generic backend entry points with Schur; the options mirror the
+    reference's public fields."""
+
+    def __init__(self):  # noqa: D107 - Schur.__init__ is not called on purpose
+        self.h = lib.or_lsmr_create()
+        self.max_iterations = 1000
+        self.relative_tolerance = max(1e-10, 128 * np.finfo(float).eps)
+        self.diagonal_preconditioning = True
+        self.block_preconditioning = False
+        self.dim = 0
+        self.rows = 0
+
+    def _limits(self):
+        lib.or_lsmr_set(self.h, self.max_iterations, self.relative_tolerance, int(self.diagonal_preconditioning),
+                        int(self.block_preconditioning))
+
+    def prepare(self, dim):
+        self.rows = 0
+        return super().prepare(dim)
+
+    def clear(self):
+        self.rows = 0
+        super().clear()
+
+    def accumulate(self, residual, jacobians):
+        args, keep = pack_blocks(residual, jacobians)
+        st = lib.or_schur_accumulate(self.h, *args)
+        if st == 0:
+            self.rows += args[0]
+        return st
+
+    def prepare_damping(self, floor):
+        self._limits()
+        return super().prepare_damping(floor)
+
+    def diagnostics(self):
+        d = LsmrDiag()
+        lib.or_lsmr_diagnostics(self.h, C.byref(d))
+        o = lambda f, v: v if f else None  # noqa: E731
+        return dict(termination=TERM[d.termination], iterations=d.iterations, finite_step=bool(d.finite_step),
+                    estimated_absolute=o(d.has_estimated, d.estimated_absolute),
+                    estimated_relative=o(d.has_estimated, d.estimated_relative),
+                    original_absolute=o(d.has_original, d.original_absolute),
+                    original_relative=o(d.has_original, d.original_relative),
+                    scaled_absolute=o(d.has_scaled, d.scaled_absolute),
+                    scaled_relative=o(d.has_scaled, d.scaled_relative),
+                    min_scale=o(d.has_scales, d.min_scale), max_scale=o(d.has_scales, d.max_scale),
+                    damping=o(d.has_damping, d.damping), block_fallbacks=d.block_fallbacks)
+
+    def scales(self):
+        out = np.zeros(max(self.dim, 1))
+        lib.or_lsmr_scales(self.h, _dp(out))
+        return out[:self.dim]
+
+    def damped_products(self, lam, scaled, x, y):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        fwd = np.zeros(self.rows + self.dim)
+        tr = np.zeros(self.dim)
+        lib.or_lsmr_damped_products(self.h, lam, int(scaled), _dp(x), _dp(fwd), _dp(y), _dp(tr))
+        return fwd, tr
+
+    def precond(self, x, y):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        px, pty = np.zeros(self.dim), np.zeros(self.dim)
+        lib.or_lsmr_precond(self.h, _dp(x), _dp(px), _dp(y), _dp(pty))
+        return px, pty
 
 
 class Bal:

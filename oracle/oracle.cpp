@@ -436,17 +436,31 @@ struct Diagnostics {
   double estimated, reduced, scaled, original;
   int has_estimated, has_reduced, has_scaled, has_original;
 };
-struct Schur {
+// LeastSquaresBackend (optimization.rs:131-169) as the optimizers see it; the
+// step of the last solve is left in work.step.
+struct Linear {
+  StepWork work;
+  size_t solves = 0, iterations = 0;
+  virtual ~Linear() {}
+  virtual int prepare(size_t dim) = 0;
+  virtual void clear() = 0;
+  virtual int accumulate(size_t nrows, const double* r, size_t nb, const size_t* bcols, const size_t* widths,
+                         const double* const* jac, const ptrdiff_t* rs, const ptrdiff_t* cs) = 0;
+  virtual int gradient_norm(double* out) const = 0;
+  virtual int prepare_damping(double floor) = 0;
+  virtual int solve_damped(double lambda, double* predicted) = 0;
+  virtual int solve() = 0;
+};
+
+struct Schur : Linear {
   size_t max_iterations = 1000;
   double relative_tolerance = std::max(1e-10, std::numeric_limits<double>::epsilon() * 128.);
   size_t retained, cw, pw;
   Model model;
   BlockFactors blocks;
-  StepWork work;
   std::vector<Edge> edges;
   std::vector<double> cross, reduced_rhs, reduced_step, scaled_work, reduced_residual, tmp;
   bool ready = false;
-  size_t solves = 0, iterations = 0;
   Diagnostics diag{};
 
   void cross_apply(double* out, const double* rhs, bool transpose, double alpha) const {  // :558-582
@@ -480,7 +494,7 @@ struct Schur {
     blocks.solve_normal(z, retained, 0, lambda);
   }
 
-  int prepare(size_t dim) {  // :409-431
+  int prepare(size_t dim) override {  // :409-431
     ready = false;
     solves = iterations = 0;
     diag = Diagnostics{};
@@ -495,14 +509,14 @@ struct Schur {
     scaled_work.assign(dim, 0.);
     return OK;
   }
-  void clear() {  // :432-437
+  void clear() override {  // :432-437
     ready = false;
     edges.clear();
     cross.clear();
     model.clear();
   }
   int accumulate(size_t nrows, const double* r, size_t nb, const size_t* bcols, const size_t* widths,
-                 const double* const* jac, const ptrdiff_t* rs, const ptrdiff_t* cs) {  // :438-482
+                 const double* const* jac, const ptrdiff_t* rs, const ptrdiff_t* cs) override {  // :438-482
     ready = false;
     bool has_left = false, has_right = false;
     size_t lcol = 0, lidx = 0, rcol = 0, ridx = 0;
@@ -522,8 +536,8 @@ struct Schur {
     if (has_left && has_right) edges.push_back({lcol, rcol, lidx, ridx});
     return OK;
   }
-  int gradient_norm(double* out) const { return norm_inf(model.gradient.data(), model.cols, out); }
-  int prepare_damping(double floor) {  // :490-526
+  int gradient_norm(double* out) const override { return norm_inf(model.gradient.data(), model.cols, out); }
+  int prepare_damping(double floor) override {  // :490-526
     ready = false;
     int s = model.prepare_scales(floor);
     if (s) return s;
@@ -630,7 +644,7 @@ struct Schur {
     *predicted = v.predicted;
     return OK;
   }
-  int solve_damped(double lambda, double* predicted) {  // :527-545, :192-247
+  int solve_damped(double lambda, double* predicted) override {  // :527-545, :192-247
     diag = Diagnostics{};
     diag.damping = lambda;
     if (!ready || !is_fin(lambda) || lambda < 0) return INVALID_OPTIONS;
@@ -648,6 +662,312 @@ struct Schur {
     recover_step(lambda);
     return verify(lambda, predicted);
   }
+  int solve() override {  // :486-489
+    int s = prepare_damping(1e-6);
+    if (s) return s;
+    double predicted;
+    return solve_damped(0., &predicted);
+  }
+};
+
+// ------------------------------------------------------------------ LSMR
+// src/lsmr.rs:126-595 and src/lsmr/preconditioner.rs. The iterative core is
+// faer 0.24.4's matrix_free::lsmr (called at src/lsmr.rs:240-261; faer's
+// source is not part of the fagra tree), restated here from Fong & Saunders,
+// "LSMR: an iterative algorithm for sparse least-squares problems", SIAM J.
+// Sci. Comput. 33(5), 2011, Algorithm 1, for one right-hand side with:
+//  - a zero initial guess (InitialGuessStatus::Zero);
+//  - a right preconditioner M: the iteration runs on A M and returns x = M y;
+//  - the stopping test ||(A M)^T r|| <= rel_tol * ||(A M)^T b|| on the
+//    recurrence estimate |zetabar|, made before each iteration, so an
+//    iteration budget of k always performs k iterations when the start is
+//    not already converged (src/lsmr.rs:733-777 pins this: a system that one
+//    iteration solves exactly still reports IterationLimit at max 1);
+//  - the per-iteration callback counting iterations.
+// Zero norms leave the Golub-Kahan vector at zero instead of dividing.
+enum { MODE_IDENTITY = 0, MODE_DIAGONAL = 1, MODE_BLOCK = 2, MODE_NONE = -1 };
+struct LsmrDiagnostics {  // src/lsmr.rs:68-104 (has_* = Some)
+  int termination;
+  size_t iterations;
+  int finite_step;
+  double estimated_absolute, estimated_relative, original_absolute, original_relative, scaled_absolute,
+      scaled_relative, min_scale, max_scale, damping;
+  size_t block_fallbacks;
+  int has_estimated, has_original, has_scaled, has_scales, has_damping;
+};
+
+// y = op(x) for an operator of shape m x n and its transpose.
+struct LsmrOperator {
+  size_t m, n;
+  virtual ~LsmrOperator() {}
+  virtual void apply(const double* x, double* out) const = 0;            // out[m]
+  virtual void transpose_apply(const double* y, double* out) const = 0;  // out[n]
+};
+// FactorPreconditioner (preconditioner.rs): M = L^-T per block, M^T = L^-1;
+// absent factors make it the identity.
+struct LsmrPrecond {
+  const BlockFactors* factors = nullptr;
+  void apply(double* v) const {
+    if (factors) factors->apply_factor_inverse(v, false);
+  }
+  void transpose_apply(double* v) const {
+    if (factors) factors->apply_factor_inverse(v, true);
+  }
+};
+struct LsmrResult {
+  bool converged;
+  double abs_residual, rel_residual;
+};
+
+LsmrResult lsmr_core(const LsmrOperator& A, const LsmrPrecond& M, const double* b, double* x, double rel_tol,
+                     size_t max_iters, size_t* iterations) {
+  size_t m = A.m, n = A.n;
+  std::vector<double> u(b, b + m), v(n), t(n), h(n), hbar(n, 0.), y(n, 0.), w(m);
+  auto scale = [](std::vector<double>& z, double s) {
+    if (s > 0)
+      for (double& e : z) e /= s;
+  };
+  double beta = norm_l2(u.data(), m);
+  scale(u, beta);
+  A.transpose_apply(u.data(), v.data());
+  M.transpose_apply(v.data());
+  double alpha = norm_l2(v.data(), n);
+  scale(v, alpha);
+  double zetabar = alpha * beta, alphabar = alpha, rho = 1, rhobar = 1, cbar = 1, sbar = 0;
+  h = v;
+  double normar0 = alpha * beta, normar = normar0;
+  std::fill(x, x + n, 0.);
+  if (normar0 == 0) return {true, 0., 0.};
+  double threshold = rel_tol * normar0;
+  auto solution = [&]() {  // x = M y
+    t = y;
+    M.apply(t.data());
+    std::copy(t.begin(), t.end(), x);
+  };
+  for (size_t it = 0; it < max_iters; ++it) {
+    if (normar <= threshold) {
+      solution();
+      return {true, normar, normar / normar0};
+    }
+    // Golub-Kahan step on A M.
+    t = v;
+    M.apply(t.data());
+    A.apply(t.data(), w.data());
+    for (size_t i = 0; i < m; ++i) u[i] = w[i] - alpha * u[i];
+    beta = norm_l2(u.data(), m);
+    scale(u, beta);
+    A.transpose_apply(u.data(), t.data());
+    M.transpose_apply(t.data());
+    for (size_t j = 0; j < n; ++j) v[j] = t[j] - beta * v[j];
+    alpha = norm_l2(v.data(), n);
+    scale(v, alpha);
+    // Rotations (Algorithm 1, steps 4-5).
+    double rhoold = rho;
+    rho = std::hypot(alphabar, beta);
+    double c = alphabar / rho, s = beta / rho;
+    double thetanew = s * alpha;
+    alphabar = c * alpha;
+    double rhobarold = rhobar;
+    double thetabar = sbar * rho;
+    double crho = cbar * rho;
+    rhobar = std::hypot(crho, thetanew);
+    cbar = crho / rhobar;
+    sbar = thetanew / rhobar;
+    double zeta = cbar * zetabar;
+    zetabar = -sbar * zetabar;
+    // Updates (step 6).
+    double fhbar = thetabar * rho / (rhoold * rhobarold), fy = zeta / (rho * rhobar), fh = thetanew / rho;
+    for (size_t j = 0; j < n; ++j) {
+      hbar[j] = h[j] - fhbar * hbar[j];
+      y[j] += fy * hbar[j];
+      h[j] = v[j] - fh * h[j];
+    }
+    normar = std::fabs(zetabar);
+    ++*iterations;  // callback
+  }
+  solution();
+  return {false, normar, normar / normar0};
+}
+
+// Jacobian alone (the undamped solve) and the Damped augmented operator
+// [J D^-1; diag] / [J; diag] (src/lsmr.rs:128-224).
+struct JacobianOp : LsmrOperator {
+  const Model* model;
+  void apply(const double* x, double* out) const override { model->apply(x, out); }
+  void transpose_apply(const double* y, double* out) const override { model->transpose_apply(y, out); }
+};
+struct DampedOp : LsmrOperator {
+  const Model* model;
+  const double* diagonal;
+  const double* scales;  // null: no scaling
+  mutable std::vector<double> tmp;
+  void apply(const double* x, double* out) const override {
+    size_t r = model->rows, c = model->cols;
+    if (scales) {
+      tmp.resize(c);
+      for (size_t j = 0; j < c; ++j) tmp[j] = x[j] / scales[j];
+      model->apply(tmp.data(), out);
+    } else {
+      model->apply(x, out);
+    }
+    for (size_t j = 0; j < c; ++j) out[r + j] = diagonal[j] * x[j];
+  }
+  void transpose_apply(const double* y, double* out) const override {
+    size_t r = model->rows, c = model->cols;
+    model->transpose_apply(y, out);
+    for (size_t j = 0; j < c; ++j) {
+      if (scales) out[j] /= scales[j];
+      out[j] += diagonal[j] * y[r + j];
+    }
+  }
+};
+
+struct Lsmr : Linear {
+  size_t max_iterations = 1000;
+  double relative_tolerance = std::max(1e-10, std::numeric_limits<double>::epsilon() * 128.);
+  bool diagonal_preconditioning = true, block_preconditioning = false;
+  Model model;
+  BlockFactors blocks;
+  std::vector<double> diagonal, augmented_rhs;
+  int prepared_mode = MODE_NONE;
+  LsmrDiagnostics diag{};
+
+  int requested_mode() const {  // :391-399
+    return block_preconditioning ? MODE_BLOCK : diagonal_preconditioning ? MODE_DIAGONAL : MODE_IDENTITY;
+  }
+  // The shared solve() helper, src/lsmr.rs:228-288.
+  int run(const LsmrOperator& op, const LsmrPrecond& pre, const double* rhs) {
+    size_t n = op.n;
+    work.step.assign(n, 0.);
+    if (op.m == 0 || n == 0) {
+      diag.termination = T_CONVERGED;
+      diag.finite_step = 1;
+      return OK;
+    }
+    ++solves;
+    size_t its = 0;
+    LsmrResult res = lsmr_core(op, pre, rhs, work.step.data(), relative_tolerance, max_iterations, &its);
+    iterations += its;
+    diag.iterations += its;
+    diag.estimated_absolute = res.abs_residual;
+    diag.estimated_relative = res.rel_residual;
+    diag.has_estimated = 1;
+    double tmp;
+    diag.finite_step = norm_inf(work.step.data(), n, &tmp) == OK;
+    if (diag.finite_step && is_fin(res.abs_residual) && is_fin(res.rel_residual))
+      diag.termination = res.converged ? T_CONVERGED : T_ITERATION_LIMIT;
+    else
+      diag.termination = T_NONFINITE;
+    return diag.termination == T_CONVERGED ? OK : LINEAR_SOLVE_FAILED;
+  }
+  int prepare(size_t dim) override {  // :469-480
+    solves = iterations = 0;
+    diag = LsmrDiagnostics{};
+    prepared_mode = MODE_NONE;
+    if (max_iterations == 0 || !(relative_tolerance >= 0 && relative_tolerance < 1)) return INVALID_OPTIONS;
+    model.prepare(dim);
+    work.step.assign(dim, 0.);
+    return OK;
+  }
+  void clear() override {  // :482-485
+    prepared_mode = MODE_NONE;
+    model.clear();
+  }
+  int accumulate(size_t nrows, const double* r, size_t nb, const size_t* bcols, const size_t* widths,
+                 const double* const* jac, const ptrdiff_t* rs, const ptrdiff_t* cs) override {  // :487-494
+    prepared_mode = MODE_NONE;
+    for (size_t i = 0; i < nb; ++i)
+      if (bcols[i] + widths[i] < bcols[i] || bcols[i] + widths[i] > model.cols) return DIMENSION_MISMATCH;
+    return model.accumulate(nrows, r, nb, bcols, widths, jac, rs, cs);
+  }
+  int gradient_norm(double* out) const override { return norm_inf(model.gradient.data(), model.cols, out); }
+  int solve() override {  // :500-520
+    diag = LsmrDiagnostics{};
+    JacobianOp op;
+    op.m = model.rows;
+    op.n = model.cols;
+    op.model = &model;
+    return run(op, LsmrPrecond{}, model.negative_residual.data());
+  }
+  int prepare_damping(double floor) override {  // :521-546
+    prepared_mode = MODE_NONE;
+    int s = model.prepare_scales(floor);
+    if (s) return s;
+    int mode = requested_mode();
+    diagonal.assign(model.cols, 0.);
+    work.prepare_verification(model.rows, model.cols);
+    if (mode == MODE_BLOCK && (s = blocks.prepare(model))) return s;
+    augmented_rhs.assign(model.rows + model.cols, 0.);
+    std::copy(model.negative_residual.begin(), model.negative_residual.end(), augmented_rhs.begin());
+    prepared_mode = mode;
+    return OK;
+  }
+  // recover_and_verify, :418-456; returns the status, predicted in *predicted.
+  int recover_and_verify(double lambda, int mode, double* predicted) {
+    size_t n = model.cols;
+    if (mode != MODE_IDENTITY)
+      for (size_t j = 0; j < n; ++j) work.step[j] /= model.scales[j];
+    Verification v = verify_step(model, work, lambda);
+    diag.finite_step = v.finite_step;
+    if (mode != MODE_IDENTITY)
+      for (size_t j = 0; j < n; ++j) {
+        work.normal_residual[j] /= model.scales[j];
+        work.reference[j] /= model.scales[j];
+      }
+    if (mode == MODE_BLOCK) {
+      blocks.apply_factor_inverse(work.normal_residual.data(), true);
+      blocks.apply_factor_inverse(work.reference.data(), true);
+    }
+    double scaled_norm = norm_l2(work.normal_residual.data(), n);
+    double scaled_reference = norm_l2(work.reference.data(), n);
+    diag.original_absolute = v.residual_norm;
+    diag.original_relative = relative(v.residual_norm, v.reference_norm);
+    diag.scaled_absolute = scaled_norm;
+    diag.scaled_relative = relative(scaled_norm, scaled_reference);
+    diag.has_original = diag.has_scaled = 1;
+    if (!v.finite_step || !is_fin(v.residual_norm) || !is_fin(scaled_norm)) {
+      diag.termination = T_NONFINITE;
+      return LINEAR_SOLVE_FAILED;
+    }
+    *predicted = v.predicted;
+    return OK;
+  }
+  int solve_damped(double lambda, double* predicted) override {  // :548-585
+    diag = LsmrDiagnostics{};
+    int mode = prepared_mode;
+    if (mode == MODE_NONE || mode != requested_mode() || !is_fin(lambda) || lambda < 0) return INVALID_OPTIONS;
+    double root = std::sqrt(lambda);
+    bool scaled = mode != MODE_IDENTITY;
+    diag.damping = lambda;
+    diag.has_damping = 1;
+    if (model.cols) {
+      diag.min_scale = *std::min_element(model.scales.begin(), model.scales.end());
+      diag.max_scale = *std::max_element(model.scales.begin(), model.scales.end());
+      diag.has_scales = 1;
+    }
+    for (size_t j = 0; j < model.cols; ++j) diagonal[j] = scaled ? root : root * model.scales[j];
+    double tmp;
+    if (norm_inf(diagonal.data(), model.cols, &tmp)) {
+      diag.termination = T_NONFINITE;
+      return LINEAR_SOLVE_FAILED;
+    }
+    if (mode == MODE_BLOCK) diag.block_fallbacks = blocks.factor(lambda);
+    DampedOp op;
+    op.m = model.rows + model.cols;
+    op.n = model.cols;
+    op.model = &model;
+    op.diagonal = diagonal.data();
+    op.scales = scaled ? model.scales.data() : nullptr;
+    LsmrPrecond pre;
+    if (mode == MODE_BLOCK) pre.factors = &blocks;
+    int result = run(op, pre, augmented_rhs.data());
+    double p = 0;
+    int verified = recover_and_verify(lambda, mode, &p);
+    if (verified) return verified;
+    if (result) return result;
+    *predicted = p;
+    return OK;
+  }
 };
 
 // cross_apply indexes rhs/out with edge offsets relative to each partition;
@@ -660,7 +980,7 @@ struct Problem {
   virtual ~Problem() {}
   virtual size_t dimension() = 0;
   virtual int cost(bool trial, double* out) = 0;  // optimization.rs:419-430
-  virtual int linearize(Schur& s) = 0;             // :229-265
+  virtual int linearize(Linear& s) = 0;             // :229-265
   virtual int stage(const double* delta) = 0;      // :432-459
   virtual void accept() = 0;
   virtual void reject() = 0;
@@ -719,7 +1039,7 @@ struct BalProblem : Problem {
     return checked(OK, total);
   }
   // Frame::linearize, model.rs:214-236 through CheckedSink (optimization.rs:541-612).
-  int linearize(Schur& s) override {
+  int linearize(Linear& s) override {
     s.clear();
     for (size_t c = 0; c < nc; ++c) {
       if (frame_off[c] == frame_off[c + 1]) continue;
@@ -775,7 +1095,7 @@ struct CallbackProblem : Problem {
   cb_cost_t cb_cost;
   cb_linearize_t cb_lin;
   void* user;
-  Schur* sink = nullptr;
+  Linear* sink = nullptr;
   size_t dimension() override { return dim; }
   int cost(bool t, double* out) override {
     double c = 0;
@@ -783,7 +1103,7 @@ struct CallbackProblem : Problem {
     *out = c;
     return checked(st, c);
   }
-  int linearize(Schur& s) override {
+  int linearize(Linear& s) override {
     s.clear();
     sink = &s;
     return cb_lin(user, x.data(), this);
@@ -838,7 +1158,7 @@ int validate(const LmOptions& o) {  // levenberg_marquardt.rs:47-67
 }
 
 // levenberg_marquardt.rs:330-472
-int lm_optimize(Schur& s, Problem& pb, const OptimizeOptions& opt, const LmOptions& lo, Report* rep, LmStats* st,
+int lm_optimize(Linear& s, Problem& pb, const OptimizeOptions& opt, const LmOptions& lo, Report* rep, LmStats* st,
                 accept_cb_t on_accept, void* user) {
   *st = LmStats{};
   int e;
@@ -940,8 +1260,9 @@ int lm_optimize(Schur& s, Problem& pb, const OptimizeOptions& opt, const LmOptio
   }
 }
 
-// gauss_newton.rs:101-176 with the Schur backend's solve() (schur.rs:486-489).
-int gn_optimize(Schur& s, Problem& pb, const OptimizeOptions& opt, Report* rep) {
+// gauss_newton.rs:101-176; the backend's solve() is Schur's prepare_damping +
+// solve_damped(0) (schur.rs:486-489) or LSMR's undamped solve (lsmr.rs:500-520).
+int gn_optimize(Linear& s, Problem& pb, const OptimizeOptions& opt, Report* rep) {
   int e;
   if ((e = validate(opt))) return e;
   if ((e = s.prepare(pb.dimension()))) return e;
@@ -963,9 +1284,7 @@ int gn_optimize(Schur& s, Problem& pb, const OptimizeOptions& opt, Report* rep) 
     if ((e = s.gradient_norm(&g))) return e;
     if (g <= opt.gradient_tolerance) return report(2);
     if (its == opt.max_iterations) return NO_CONVERGENCE;
-    if ((e = s.prepare_damping(1e-6))) return e;
-    double pred;
-    if ((e = s.solve_damped(0.0, &pred))) return e;
+    if ((e = s.solve())) return e;
     double norm;
     if (norm_inf(s.work.step.data(), s.work.step.size(), &norm)) return LINEAR_SOLVE_FAILED;
     if (norm <= opt.step_tolerance) return report(3);
@@ -996,27 +1315,34 @@ OR_API void or_bal_jacobians(const double* cam, const double* X, double* jc, dou
 }
 OR_API void or_rotation(const double* w, double* R) { rotation_from_scaled_axis(w, R); }
 
+// Backend handles are Linear* (Schur or Lsmr); the prepare / clear /
+// accumulate / gradient / damping / solve / work entry points below dispatch
+// on the dynamic type.
+static Linear* LIN(void* h) { return (Linear*)h; }
+static Schur* SCH(void* h) { return static_cast<Schur*>(LIN(h)); }
+static Lsmr* LSM(void* h) { return static_cast<Lsmr*>(LIN(h)); }
+
 OR_API void* or_schur_create(size_t retained, size_t cw, size_t pw) {
   Schur* s = new Schur();
   s->retained = retained; s->cw = cw; s->pw = pw;
-  return s;
+  return (void*)(Linear*)s;
 }
-OR_API void or_schur_destroy(void* h) { delete (Schur*)h; }
+OR_API void or_schur_destroy(void* h) { delete LIN(h); }
 OR_API void or_schur_set_limits(void* h, size_t max_iterations, double rel_tol) {
-  ((Schur*)h)->max_iterations = max_iterations;
-  ((Schur*)h)->relative_tolerance = rel_tol;
+  SCH(h)->max_iterations = max_iterations;
+  SCH(h)->relative_tolerance = rel_tol;
 }
-OR_API int or_schur_prepare(void* h, size_t dim) { return ((Schur*)h)->prepare(dim); }
-OR_API void or_schur_clear(void* h) { ((Schur*)h)->clear(); }
+OR_API int or_schur_prepare(void* h, size_t dim) { return LIN(h)->prepare(dim); }
+OR_API void or_schur_clear(void* h) { LIN(h)->clear(); }
 OR_API int or_schur_accumulate(void* h, size_t rows, const double* r, size_t nb, const size_t* cols,
                                const size_t* widths, const double* const* jac, const ptrdiff_t* rs,
                                const ptrdiff_t* cs) {
-  return ((Schur*)h)->accumulate(rows, r, nb, cols, widths, jac, rs, cs);
+  return LIN(h)->accumulate(rows, r, nb, cols, widths, jac, rs, cs);
 }
-OR_API int or_schur_gradient_norm(void* h, double* out) { return ((Schur*)h)->gradient_norm(out); }
-OR_API int or_schur_prepare_damping(void* h, double floor) { return ((Schur*)h)->prepare_damping(floor); }
+OR_API int or_schur_gradient_norm(void* h, double* out) { return LIN(h)->gradient_norm(out); }
+OR_API int or_schur_prepare_damping(void* h, double floor) { return LIN(h)->prepare_damping(floor); }
 OR_API int or_schur_solve_damped(void* h, double lambda, double* delta, double* predicted) {
-  Schur* s = (Schur*)h;
+  Linear* s = LIN(h);
   double pred = 0;
   int st = s->solve_damped(lambda, &pred);
   if (st == OK || st == LINEAR_SOLVE_FAILED)
@@ -1025,22 +1351,60 @@ OR_API int or_schur_solve_damped(void* h, double lambda, double* delta, double* 
   return st;
 }
 OR_API int or_schur_solve(void* h, double* delta) {
-  Schur* s = (Schur*)h;
-  int st = s->prepare_damping(1e-6);
-  if (st) return st;
-  double pred;
-  st = s->solve_damped(0.0, &pred);
-  if (st == OK && delta) std::copy(s->work.step.begin(), s->work.step.end(), delta);
+  Linear* s = LIN(h);
+  int st = s->solve();
+  if ((st == OK || st == LINEAR_SOLVE_FAILED) && delta) std::copy(s->work.step.begin(), s->work.step.end(), delta);
   return st;
 }
 OR_API void or_schur_work(void* h, size_t* solves, size_t* iterations) {
-  *solves = ((Schur*)h)->solves;
-  *iterations = ((Schur*)h)->iterations;
+  *solves = LIN(h)->solves;
+  *iterations = LIN(h)->iterations;
 }
-OR_API void or_schur_diagnostics(void* h, Diagnostics* d) { *d = ((Schur*)h)->diag; }
+
+// LSMR backend (src/lsmr.rs).
+OR_API void* or_lsmr_create(void) { return (void*)(Linear*)new Lsmr(); }
+OR_API void or_lsmr_set(void* h, size_t max_iterations, double rel_tol, int diagonal, int block) {
+  Lsmr* s = LSM(h);
+  s->max_iterations = max_iterations;
+  s->relative_tolerance = rel_tol;
+  s->diagonal_preconditioning = diagonal != 0;
+  s->block_preconditioning = block != 0;
+}
+OR_API void or_lsmr_diagnostics(void* h, LsmrDiagnostics* d) { *d = LSM(h)->diag; }
+// The Damped operator at damping lambda (scaled: [J D^-1; sqrt(lambda) I],
+// else [J; sqrt(lambda) D]) applied to x[n] -> fwd[m+n] and to y[m+n] -> tr[n].
+OR_API void or_lsmr_damped_products(void* h, double lambda, int scaled, const double* x, double* fwd,
+                                    const double* y, double* tr) {
+  Lsmr* s = LSM(h);
+  std::vector<double> diagonal(s->model.cols);
+  for (size_t j = 0; j < diagonal.size(); ++j)
+    diagonal[j] = scaled ? std::sqrt(lambda) : std::sqrt(lambda) * s->model.scales[j];
+  DampedOp op;
+  op.m = s->model.rows + s->model.cols;
+  op.n = s->model.cols;
+  op.model = &s->model;
+  op.diagonal = diagonal.data();
+  op.scales = scaled ? s->model.scales.data() : nullptr;
+  op.apply(x, fwd);
+  op.transpose_apply(y, tr);
+}
+// Block factors of the last damped solve: L^-T x and L^-1 y per variable block.
+OR_API void or_lsmr_precond(void* h, const double* x, double* px, const double* y, double* pty) {
+  Lsmr* s = LSM(h);
+  size_t n = s->model.cols;
+  std::copy(x, x + n, px);
+  std::copy(y, y + n, pty);
+  s->blocks.apply_factor_inverse(px, false);
+  s->blocks.apply_factor_inverse(pty, true);
+}
+OR_API void or_lsmr_scales(void* h, double* scales) {
+  Lsmr* s = LSM(h);
+  std::copy(s->model.scales.begin(), s->model.scales.end(), scales);
+}
+OR_API void or_schur_diagnostics(void* h, Diagnostics* d) { *d = SCH(h)->diag; }
 OR_API void or_schur_sizes(void* h, size_t* nblocks, size_t* nedges, size_t* nvalues, size_t* nvar, size_t* ngram,
                            size_t* rows, size_t* cols) {
-  Schur* s = (Schur*)h;
+  Schur* s = SCH(h);
   *nblocks = s->model.blocks.size();
   *nedges = s->edges.size();
   *nvalues = s->model.values.size();
@@ -1052,7 +1416,7 @@ OR_API void or_schur_sizes(void* h, size_t* nblocks, size_t* nedges, size_t* nva
 // Structure and model export for bit-exact index-map and value checks.
 OR_API void or_schur_export(void* h, size_t* blocks5, size_t* edges4, size_t* owners, size_t* var3, double* values,
                             double* negres, double* gradient, double* scales, double* gram, double* cross) {
-  Schur* s = (Schur*)h;
+  Schur* s = SCH(h);
   for (size_t i = 0; i < s->model.blocks.size(); ++i) {
     const Block& b = s->model.blocks[i];
     size_t v[5] = {b.row, b.col, b.rows, b.cols, b.start};
@@ -1078,12 +1442,12 @@ OR_API void or_schur_export(void* h, size_t* blocks5, size_t* edges4, size_t* ow
 }
 // Reduced operator and preconditioner, for operator-level checks.
 OR_API void or_schur_reduced_apply(void* h, double lambda, const double* x, double* y) {
-  Schur* s = (Schur*)h;
+  Schur* s = SCH(h);
   s->blocks.factor(lambda);
   s->reduced_apply(x, y, lambda);
 }
 OR_API void or_schur_reduced_rhs(void* h, double* rhs) {
-  Schur* s = (Schur*)h;
+  Schur* s = SCH(h);
   std::copy(s->reduced_rhs.begin(), s->reduced_rhs.end(), rhs);
 }
 
@@ -1154,14 +1518,14 @@ OR_API void or_bal_order(void* h, size_t* order) {
   BalProblem* b = (BalProblem*)h;
   std::copy(b->order.begin(), b->order.end(), order);
 }
-OR_API int or_bal_linearize(void* bal, void* schur) { return ((BalProblem*)bal)->linearize(*(Schur*)schur); }
+OR_API int or_bal_linearize(void* bal, void* schur) { return ((BalProblem*)bal)->linearize(*(Linear*)schur); }
 
 OR_API int or_lm_bal(void* schur, void* bal, const OptimizeOptions* opt, const LmOptions* lo, Report* rep,
                      LmStats* st, accept_cb_t cb, void* user) {
-  return lm_optimize(*(Schur*)schur, *(BalProblem*)bal, *opt, *lo, rep, st, cb, user);
+  return lm_optimize(*(Linear*)schur, *(BalProblem*)bal, *opt, *lo, rep, st, cb, user);
 }
 OR_API int or_gn_bal(void* schur, void* bal, const OptimizeOptions* opt, Report* rep) {
-  return gn_optimize(*(Schur*)schur, *(BalProblem*)bal, *opt, rep);
+  return gn_optimize(*(Linear*)schur, *(BalProblem*)bal, *opt, rep);
 }
 
 // Callback problems (scalar/vector test graphs).
@@ -1189,8 +1553,8 @@ OR_API int or_cbproblem_emit(void* sink, size_t rows, const double* r, size_t nb
 }
 OR_API int or_lm_cb(void* schur, void* prob, const OptimizeOptions* opt, const LmOptions* lo, Report* rep,
                     LmStats* st) {
-  return lm_optimize(*(Schur*)schur, *(CallbackProblem*)prob, *opt, *lo, rep, st, nullptr, nullptr);
+  return lm_optimize(*(Linear*)schur, *(CallbackProblem*)prob, *opt, *lo, rep, st, nullptr, nullptr);
 }
 OR_API int or_gn_cb(void* schur, void* prob, const OptimizeOptions* opt, Report* rep) {
-  return gn_optimize(*(Schur*)schur, *(CallbackProblem*)prob, *opt, rep);
+  return gn_optimize(*(Linear*)schur, *(CallbackProblem*)prob, *opt, rep);
 }

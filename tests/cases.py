@@ -97,3 +97,63 @@ def twelve_point_bal():
         init.append(t + np.array([0.02, -0.03, 0.01]))
         pix.append(p)
     return cam[None, :], np.array(init), np.zeros(12, np.uint32), np.arange(12, dtype=np.uint32), np.array(pix)
+
+
+# ---------------------------------------------------------------- LSMR
+def lsmr_shared_columns():
+    """src/lsmr.rs:619-641: a 4x3 Jacobian whose rows 0-1 and 2-3 are emitted
+    as two 2-row residuals on the same three columns."""
+    J = np.array([[0.001, 2.0, 3.0], [0.002, -1.0, 4.0], [-0.001, 3.0, -2.0], [0.003, 1.0, 2.0]])
+    return J, [0, 2]
+
+
+def lsmr_product_vectors(n, m):
+    """src/lsmr.rs:642-643: x(i,k) = i + k - 1.25 and y(i,k) = 2i + k - 2.5."""
+    x = np.array([[i + k - 1.25 for k in range(2)] for i in range(n)])
+    y = np.array([[2 * i + k - 2.5 for k in range(2)] for i in range(m)])
+    return x, y
+
+
+def damped_dense(J, scales, lam, scaled):
+    """Dense Damped operator (src/lsmr.rs:128-224): [J D^-1; sqrt(lam) I] when
+    scaled, else [J; sqrt(lam) D]."""
+    n = J.shape[1]
+    top = J / scales[None, :] if scaled else J
+    diag = np.full(n, np.sqrt(lam)) if scaled else np.sqrt(lam) * scales
+    return np.vstack([top, np.diag(diag)])
+
+
+def lsmr_mixed_scale():
+    """src/lsmr.rs:783-788: columns spanning eight orders of magnitude and an
+    unused fourth column."""
+    J = np.array([[1e-4, 2.0, 0.0, 0.0], [2e-4, -1.0, 3e4, 0.0], [0.0, 1.0, -1e4, 0.0]])
+    return J, np.array([1.0, -2.0, 3.0])
+
+
+def lsmr_retry_system():
+    """src/lsmr.rs:860-863: a rank-deficient 3x3 system (third column zero)."""
+    J = np.array([[1.0, 2.0, 0.0], [3.0, -1.0, 0.0], [0.0, 1.0, 0.0]])
+    return J, np.array([-3.0, 2.0, 1.0])
+
+
+def lsmr_coupling_gap():
+    """src/lsmr.rs:907-910: a 4x5 Jacobian emitted as blocks (3, cols 3..5) and
+    (0, cols 0..2); column 2 is never touched."""
+    J = np.array([[1.0, 2.0, 0.0, 4.0, 2.0], [3.0, 1.0, 0.0, 2.0, 1.0], [2.0, 1.0, 0.0, 1.0, 3.0],
+                  [1.0, 1.0, 0.0, 3.0, 2.0]])
+    return J, np.array([1.0, -2.0, 3.0, -1.0])
+
+
+def lsmr_rectangular():
+    """src/lsmr.rs:1006-1041: a 3-row emission with a strided 3x2 view at
+    column 2 and a 3x2 block at column 0, then a 2-row emission at column 0.
+    Returns (emissions, dense J, r)."""
+    storage = np.arange(20, dtype=np.float64).reshape(5, 4)
+    ja = storage[1:4, 1:3]  # noncontiguous view
+    jb = np.array([[1.0, 0.0], [0.0, 2.0], [3.0, -1.0]])
+    jc = np.array([[2.0, 0.0], [0.0, 1.0]])
+    emissions = [(np.array([1.0, -2.0, 3.0]), [(2, ja), (0, jb)]), (np.array([-4.0, 5.0]), [(0, jc)])]
+    J = np.array([[1.0, 0.0, 5.0, 6.0], [0.0, 2.0, 9.0, 10.0], [3.0, -1.0, 13.0, 14.0], [2.0, 0.0, 0.0, 0.0],
+                  [0.0, 1.0, 0.0, 0.0]])
+    r = np.array([1.0, -2.0, 3.0, -4.0, 5.0])
+    return emissions, J, r
