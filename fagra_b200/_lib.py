@@ -51,6 +51,47 @@ class SchurTimingsC(C.Structure):
                 ("preparation", "factorization", "linear_solve", "products", "preconditioner", "verification")]
 
 
+class LsmrOptions(C.Structure):
+    _fields_ = [
+        ("max_iterations", size_t),
+        ("relative_tolerance", C.c_double),
+        ("diagonal_preconditioning", C.c_int),
+        ("block_preconditioning", C.c_int),
+        ("collect_timings", C.c_int),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class LsmrDiagnosticsC(C.Structure):
+    _fields_ = [
+        ("termination", C.c_int),
+        ("iterations", size_t),
+        ("finite_step", C.c_int),
+        ("estimated_absolute_residual", C.c_double),
+        ("estimated_relative_residual", C.c_double),
+        ("original_absolute_residual", C.c_double),
+        ("original_relative_residual", C.c_double),
+        ("scaled_absolute_residual", C.c_double),
+        ("scaled_relative_residual", C.c_double),
+        ("min_scale", C.c_double),
+        ("max_scale", C.c_double),
+        ("damping", C.c_double),
+        ("block_fallbacks", size_t),
+        ("has_estimated", C.c_int),
+        ("has_original", C.c_int),
+        ("has_scaled", C.c_int),
+        ("has_scales", C.c_int),
+        ("has_damping", C.c_int),
+    ]
+
+
+class LsmrTimingsC(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("preparation", "factorization", "linear_solve", "forward", "transpose", "preconditioner",
+                 "residual_checks")]
+
+
 class OptimizeOptionsC(C.Structure):
     _fields_ = [
         ("max_iterations", size_t),
@@ -164,6 +205,13 @@ SIGNATURES = {
                                  C.POINTER(LmStatisticsC)]),
     "fg_gn_optimize": (C.c_int, [C.c_void_p, C.POINTER(ProblemCallbacksC), C.c_void_p, dptr,
                                  C.POINTER(OptimizeOptionsC), C.POINTER(ReportC)]),
+    "fg_lsmr_default_options": (None, [C.POINTER(LsmrOptions)]),
+    "fg_lsmr_create": (C.c_int, [C.POINTER(LsmrOptions), C.POINTER(C.c_void_p)]),
+    "fg_lsmr_set_options": (C.c_int, [C.c_void_p, C.POINTER(LsmrOptions)]),
+    "fg_lsmr_get_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(LsmrDiagnosticsC)]),
+    "fg_lsmr_get_timings": (C.c_int, [C.c_void_p, C.POINTER(LsmrTimingsC)]),
+    "fg_lsmr_damped_products": (C.c_int, [C.c_void_p, C.c_double, C.c_int, dptr, dptr, dptr, dptr]),
+    "fg_lsmr_time_iteration": (C.c_int, [C.c_void_p, C.c_double, size_t, dptr, dptr]),
 }
 
 

@@ -213,6 +213,167 @@ class Schur:
         return y
 
 
+@dataclass
+class LsmrDiagnostics:
+    """src/lsmr.rs:68-104 (None where the reference has None)."""
+    termination: Optional[str]
+    iterations: int
+    finite_step: bool
+    estimated_absolute_residual: Optional[float]
+    estimated_relative_residual: Optional[float]
+    original_absolute_residual: Optional[float]
+    original_relative_residual: Optional[float]
+    scaled_absolute_residual: Optional[float]
+    scaled_relative_residual: Optional[float]
+    min_scale: Optional[float]
+    max_scale: Optional[float]
+    damping: Optional[float]
+    block_fallbacks: int
+
+
+@dataclass
+class LsmrTimings:
+    preparation: float
+    factorization: float
+    linear_solve: float
+    forward: float
+    transpose: float
+    preconditioner: float
+    residual_checks: float
+
+
+class Lsmr:
+    """Device LSMR backend: `Lsmr::default()` (src/lsmr.rs:339-362) with the public
+    fields `max_iterations`, `relative_tolerance`, `diagonal_preconditioning`,
+    `block_preconditioning` and `collect_timings`."""
+
+    def __init__(self, *, precision: str = "f64", device: int = 0):
+        o = _lib.LsmrOptions()
+        lib.fg_lsmr_default_options(C.byref(o))
+        o.precision = PRECISIONS[precision]
+        if precision == "f32":  # Lsmr::<f32>::default(): max(1e-10, 128 eps_f32)
+            o.relative_tolerance = max(1e-10, 128 * float(np.finfo(np.float32).eps))
+        o.device = device
+        self._opts = o
+        h = C.c_void_p()
+        raise_for_status(lib.fg_lsmr_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self.precision = precision
+        self.device = device
+        self._dim = 0
+        self._rows = 0
+
+    def _get(self, name):
+        return getattr(self._opts, name)
+
+    def _set(self, name, value):
+        setattr(self._opts, name, value)
+        raise_for_status(lib.fg_lsmr_set_options(self._h, C.byref(self._opts)))
+
+    max_iterations = property(lambda s: s._get("max_iterations"), lambda s, v: s._set("max_iterations", v))
+    relative_tolerance = property(lambda s: s._get("relative_tolerance"),
+                                  lambda s, v: s._set("relative_tolerance", v))
+    diagonal_preconditioning = property(lambda s: bool(s._get("diagonal_preconditioning")),
+                                        lambda s, v: s._set("diagonal_preconditioning", int(bool(v))))
+    block_preconditioning = property(lambda s: bool(s._get("block_preconditioning")),
+                                     lambda s, v: s._set("block_preconditioning", int(bool(v))))
+    collect_timings = property(lambda s: bool(s._get("collect_timings")),
+                               lambda s, v: s._set("collect_timings", int(bool(v))))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.fg_backend_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- LeastSquaresBackend
+    def prepare(self, dimension: int) -> None:
+        raise_for_status(lib.fg_backend_prepare(self._h, dimension))
+        self._dim = dimension
+        self._rows = 0
+
+    def clear(self) -> None:
+        raise_for_status(lib.fg_backend_clear(self._h))
+        self._rows = 0
+
+    def accumulate(self, residual: Sequence[float], jacobians: Iterable[Tuple[int, np.ndarray]]) -> None:
+        accumulate_into(self._h, residual, jacobians)
+        self._rows += int(np.asarray(residual).size)
+
+    def gradient_norm(self) -> float:
+        out = C.c_double()
+        raise_for_status(lib.fg_backend_gradient_norm(self._h, C.byref(out)))
+        return out.value
+
+    def solve(self) -> np.ndarray:
+        p = dptr()
+        n = size_t()
+        raise_for_status(lib.fg_backend_solve(self._h, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0)
+
+    def prepare_damping(self, min_column_norm: float) -> None:
+        raise_for_status(lib.fg_backend_prepare_damping(self._h, min_column_norm))
+
+    def solve_damped(self, damping: float) -> DampedStep:
+        p = dptr()
+        n = size_t()
+        pred = C.c_double()
+        raise_for_status(lib.fg_backend_solve_damped(self._h, damping, C.byref(p), C.byref(n), C.byref(pred)))
+        delta = np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0)
+        return DampedStep(delta, pred.value)
+
+    def linear_solve_work(self) -> LinearSolveWork:
+        s, i, a = size_t(), size_t(), C.c_int()
+        raise_for_status(lib.fg_backend_linear_solve_work(self._h, C.byref(s), C.byref(i), C.byref(a)))
+        return LinearSolveWork(s.value, i.value)
+
+    statistics = linear_solve_work
+
+    def diagnostics(self) -> LsmrDiagnostics:
+        d = _lib.LsmrDiagnosticsC()
+        raise_for_status(lib.fg_lsmr_get_diagnostics(self._h, C.byref(d)))
+        o = lambda flag, v: v if flag else None  # noqa: E731
+        return LsmrDiagnostics(TERMINATIONS[d.termination], d.iterations, bool(d.finite_step),
+                               o(d.has_estimated, d.estimated_absolute_residual),
+                               o(d.has_estimated, d.estimated_relative_residual),
+                               o(d.has_original, d.original_absolute_residual),
+                               o(d.has_original, d.original_relative_residual),
+                               o(d.has_scaled, d.scaled_absolute_residual),
+                               o(d.has_scaled, d.scaled_relative_residual),
+                               o(d.has_scales, d.min_scale), o(d.has_scales, d.max_scale),
+                               o(d.has_damping, d.damping), d.block_fallbacks)
+
+    def timings(self) -> LsmrTimings:
+        t = _lib.LsmrTimingsC()
+        raise_for_status(lib.fg_lsmr_get_timings(self._h, C.byref(t)))
+        return LsmrTimings(t.preparation, t.factorization, t.linear_solve, t.forward, t.transpose,
+                           t.preconditioner, t.residual_checks)
+
+    def damped_products(self, damping: float, scaled: bool, x: np.ndarray, y: np.ndarray):
+        """Damped operator products on the device: (A x, A^T y)."""
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        fwd = np.zeros(self._rows + self._dim)
+        tr = np.zeros(self._dim)
+        raise_for_status(lib.fg_lsmr_damped_products(self._h, damping, int(bool(scaled)), _dp(x), _dp(fwd), _dp(y),
+                                                     _dp(tr)))
+        return fwd, tr
+
+    def time_iteration(self, damping: float, repetitions: int = 64):
+        sec, by = C.c_double(), C.c_double()
+        raise_for_status(lib.fg_lsmr_time_iteration(self._h, damping, repetitions, C.byref(sec), C.byref(by)))
+        return sec.value, by.value
+
+
 def accumulate_into(handle, residual, jacobians) -> None:
     """Emit one residual with its (column offset, Jacobian) blocks through the C ABI."""
     r = np.ascontiguousarray(np.asarray(residual, dtype=np.float64).reshape(-1))

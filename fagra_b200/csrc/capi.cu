@@ -193,8 +193,10 @@ FG_API fg_status fg_backend_solve_damped_device(fg_backend* b, double lambda, co
 FG_API fg_status fg_backend_solve(fg_backend* b, const double** delta, size_t* len) {
   FG_NEED(b);
   FG_GUARD_BEGIN
-  FG_TRY(b->impl->prepare_damping(1e-6));
-  return fg_backend_solve_damped(b, 0.0, delta, len, nullptr);
+  FG_TRY(b->impl->solve_undamped(true));
+  if (delta) *delta = b->impl->step_host();
+  if (len) *len = b->impl->dimension();
+  return FG_OK;
   FG_GUARD_END
 }
 FG_API fg_status fg_backend_linear_solve_work(const fg_backend* b, size_t* solves, size_t* iterations,

@@ -223,10 +223,8 @@ fg_status gn_optimize(Backend* b, ProblemAdapter& pb, const fg_optimize_options&
     FG_TRY(b->gradient_norm(&g));
     if (g <= opt.gradient_tolerance) return report(2);
     if (its == opt.max_iterations) return FG_NO_CONVERGENCE;
-    // LeastSquaresBackend::solve for Schur: prepare_damping(1e-6) + solve_damped(0).
-    FG_TRY(b->prepare_damping(1e-6));
-    double pred;
-    FG_TRY(b->solve_damped(0.0, &pred, !dev));
+    // LeastSquaresBackend::solve (gauss_newton.rs:134).
+    FG_TRY(b->solve_undamped(!dev));
     double norm;
     if (b->step_norm_inf(&norm) != FG_OK) return FG_LINEAR_SOLVE_FAILED;
     if (norm <= opt.step_tolerance) return report(3);

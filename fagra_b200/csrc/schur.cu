@@ -127,6 +127,7 @@ class SchurImpl final : public Backend {
   }
 
   // ------------------------------------------------------------------ trait
+  int kind() const override { return 0; }
   fg_status set_options(const fg_schur_options& o) override {
     int keep = dev;
     opt = o;

@@ -44,7 +44,7 @@ struct VerifyState {
 class Backend {
  public:
   virtual ~Backend() {}
-  virtual fg_status set_options(const fg_schur_options& o) = 0;
+  virtual int kind() const = 0;  // 0 Schur, 1 LSMR
   virtual fg_status prepare(size_t dimension) = 0;
   virtual fg_status clear() = 0;
   virtual fg_status accumulate(size_t rows, const double* r, size_t nb, const size_t* cols, const size_t* widths,
@@ -52,20 +52,18 @@ class Backend {
   virtual fg_status gradient_norm(double* out) = 0;
   virtual fg_status prepare_damping(double floor) = 0;
   virtual fg_status solve_damped(double lambda, double* predicted, bool copy_to_host) = 0;
+  // LeastSquaresBackend::solve: Schur runs prepare_damping(1e-6) + solve_damped(0)
+  // (src/schur.rs:486-489); LSMR has its own undamped solve.
+  virtual fg_status solve_undamped(bool copy_to_host) {
+    FG_TRY(prepare_damping(1e-6));
+    double p = 0;
+    return solve_damped(0.0, &p, copy_to_host);
+  }
   virtual fg_status step_norm_inf(double* out) = 0;
   virtual const double* step_host() const = 0;
   virtual const double* step_device() const = 0;
   virtual size_t dimension() const = 0;
   virtual void work(size_t* solves, size_t* iterations) const = 0;
-  virtual void diagnostics(fg_schur_diagnostics* d) const = 0;
-  virtual void timings(fg_schur_timings* t) const = 0;
-  virtual fg_status structure_sizes(size_t* nb, size_t* ne, size_t* nv, size_t* nvar, size_t* rows, size_t* cols) = 0;
-  virtual fg_status export_structure(uint64_t* b5, uint64_t* e4, uint64_t* owners, uint64_t* v3) = 0;
-  virtual fg_status export_model(double* values, double* negres, double* g, double* scales, double* gram,
-                                 double* cross) = 0;
-  virtual fg_status reduced_apply(double lambda, const double* x, double* y) = 0;
-  virtual fg_status time_operator(double lambda, size_t reps, double* seconds, double* bytes) = 0;
-  virtual void operator_info(int* variant, double* seconds2) const = 0;
   // Device BAL path: bind an implicit BAL structure and expose raw model storage.
   virtual fg_status bind_bal(uint64_t problem_id, size_t cameras, size_t points, size_t observations,
                              const uint32_t* order_cam, const uint32_t* order_pt) = 0;
@@ -75,9 +73,42 @@ class Backend {
   virtual void mark_device_model(size_t rows) = 0;
   virtual int device() const = 0;
   virtual cudaStream_t stream() const = 0;
+
+  // Schur-only extras.
+  virtual fg_status set_options(const fg_schur_options&) { return not_schur(); }
+  virtual void diagnostics(fg_schur_diagnostics* d) const { *d = fg_schur_diagnostics{}; }
+  virtual void timings(fg_schur_timings* t) const { *t = fg_schur_timings{}; }
+  virtual fg_status structure_sizes(size_t*, size_t*, size_t*, size_t*, size_t*, size_t*) { return not_schur(); }
+  virtual fg_status export_structure(uint64_t*, uint64_t*, uint64_t*, uint64_t*) { return not_schur(); }
+  virtual fg_status export_model(double*, double*, double*, double*, double*, double*) { return not_schur(); }
+  virtual fg_status reduced_apply(double, const double*, double*) { return not_schur(); }
+  virtual fg_status time_operator(double, size_t, double*, double*) { return not_schur(); }
+  virtual void operator_info(int* variant, double* seconds2) const {
+    *variant = 0;
+    if (seconds2) seconds2[0] = seconds2[1] = 0;
+  }
+  // LSMR-only extras.
+  virtual fg_status set_lsmr_options(const fg_lsmr_options&) { return not_lsmr(); }
+  virtual void lsmr_diagnostics(fg_lsmr_diagnostics* d) const { *d = fg_lsmr_diagnostics{}; }
+  virtual void lsmr_timings(fg_lsmr_timings* t) const { *t = fg_lsmr_timings{}; }
+  virtual fg_status damped_products(double, int, const double*, double*, const double*, double*) {
+    return not_lsmr();
+  }
+  virtual fg_status time_iteration(double, size_t, double*, double*) { return not_lsmr(); }
+
+ protected:
+  static fg_status not_schur() {
+    set_error("not a Schur backend");
+    return FG_INVALID_OPTIONS;
+  }
+  static fg_status not_lsmr() {
+    set_error("not an LSMR backend");
+    return FG_INVALID_OPTIONS;
+  }
 };
 
 fg_status make_schur(size_t retained, size_t cw, size_t pw, const fg_schur_options& o, Backend** out);
+fg_status make_lsmr(const fg_lsmr_options& o, Backend** out);
 
 }  // namespace fg
 

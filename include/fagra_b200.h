@@ -178,6 +178,67 @@ FG_API fg_status fg_schur_export_model(fg_backend* backend, double* values, doub
  * requires prepare_damping. */
 FG_API fg_status fg_schur_reduced_apply(fg_backend* backend, double lambda, const double* x, double* y);
 
+/* ---- LSMR backend: src/lsmr.rs over the same LeastSquaresBackend entry points ----
+ * fg_backend_prepare / clear / accumulate / gradient_norm / prepare_damping /
+ * solve_damped / solve / linear_solve_work work on an LSMR handle exactly as on
+ * a Schur handle; fg_backend_solve is the undamped identity-preconditioned
+ * solve of Lsmr::solve (src/lsmr.rs:500-520). The fg_schur_* extras do not
+ * apply to it (FG_INVALID_OPTIONS). */
+
+/* src/lsmr.rs:306-337 public fields, plus device-side choices. */
+typedef struct {
+  size_t max_iterations;        /* inner iterations per solve, > 0; default 1000 */
+  double relative_tolerance;    /* in [0,1); default max(1e-10, 128 eps_f64); the reference's
+                                   f32 backend defaults to max(1e-10, 128 eps_f32) */
+  int diagonal_preconditioning; /* scale by column norms; default 1 */
+  int block_preconditioning;    /* variable-block Jacobi (implies scaling); default 0 */
+  int collect_timings;          /* default 0 */
+  int precision;                /* fg_precision: storage of J and the row vector; default F64 */
+  int device;                   /* CUDA device ordinal; default 0 */
+} fg_lsmr_options;
+
+/* src/lsmr.rs:68-104 LsmrDiagnostics (has_* = Some). termination uses
+ * fg_termination: NONE, CONVERGED, ITERATION_LIMIT or NONFINITE. */
+typedef struct {
+  int termination;
+  size_t iterations;
+  int finite_step;
+  double estimated_absolute_residual, estimated_relative_residual;
+  double original_absolute_residual, original_relative_residual;
+  double scaled_absolute_residual, scaled_relative_residual;
+  double min_scale, max_scale, damping;
+  size_t block_fallbacks;
+  int has_estimated, has_original, has_scaled, has_scales, has_damping;
+} fg_lsmr_diagnostics;
+
+/* src/lsmr.rs:38-56 LsmrTimings, seconds of device event time. forward covers
+ * the row pass, transpose the column-segment pass (with M^T), preconditioner
+ * the update pass (with M). */
+typedef struct {
+  double preparation, factorization, linear_solve, forward, transpose, preconditioner, residual_checks;
+} fg_lsmr_timings;
+
+FG_API void fg_lsmr_default_options(fg_lsmr_options* out);
+/* Lsmr::default (src/lsmr.rs:339-362) */
+FG_API fg_status fg_lsmr_create(const fg_lsmr_options* options, fg_backend** out);
+/* Assign the public fields between calls (src/lsmr.rs:306-323); a changed
+ * preconditioning mode needs a new prepare_damping before solve_damped. */
+FG_API fg_status fg_lsmr_set_options(fg_backend* backend, const fg_lsmr_options* options);
+/* Lsmr::diagnostics / Lsmr::timings (src/lsmr.rs:370-383) */
+FG_API fg_status fg_lsmr_get_diagnostics(const fg_backend* backend, fg_lsmr_diagnostics* out);
+FG_API fg_status fg_lsmr_get_timings(const fg_backend* backend, fg_lsmr_timings* out);
+/* The Damped operator of src/lsmr.rs:128-224 on the device at `lambda`:
+ * fwd[rows+n] = A x and tr[n] = A^T y with A = [J D^-1; sqrt(lambda) I]
+ * (scaled != 0) or [J; sqrt(lambda) D]; host vectors; requires prepare_damping. */
+FG_API fg_status fg_lsmr_damped_products(fg_backend* backend, double lambda, int scaled, const double* x,
+                                         double* fwd, const double* y, double* tr);
+/* Mean device time of one LSMR iteration (row pass, segment pass, update)
+ * at `lambda` in the prepared mode, over `repetitions` iterations; bytes_out
+ * receives the algorithmic bytes of one iteration (Jacobian values read
+ * twice, structure indices, row and column vectors). */
+FG_API fg_status fg_lsmr_time_iteration(fg_backend* backend, double lambda, size_t repetitions,
+                                        double* seconds_per_iteration, double* bytes_out);
+
 /* ---- Device BAL problem: examples/bal/model.rs Frame + Reprojection ------ */
 /* Cameras are 9 doubles [w(3), t(3), f, k1, k2], points 3 doubles; observation
  * i links obs_camera[i] and obs_point[i] with pixel obs_pixel[2i..2i+1].
