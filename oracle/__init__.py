@@ -126,6 +126,26 @@ _sig = {
     "or_lsmr_damped_products": (None, [C.c_void_p, C.c_double, C.c_int, dptr, dptr, dptr, dptr]),
     "or_lsmr_precond": (None, [C.c_void_p, dptr, dptr, dptr, dptr]),
     "or_lsmr_scales": (None, [C.c_void_p, dptr]),
+    "or_dense_normal_create": (C.c_void_p, []),
+    "or_dense_schur_create": (C.c_void_p, [size_t, C.POINTER(size_t), size_t]),
+    "or_dense_qr_create": (C.c_void_p, [C.c_double]),
+    "or_dense_qr_set_tolerance": (None, [C.c_void_p, C.c_double]),
+    "or_dense_normal_state": (None, [C.c_void_p, dptr, dptr]),
+    "or_dense_normal_information": (C.c_int, [C.c_void_p, C.c_double]),
+    "or_backend_covariance": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(size_t), size_t, C.c_double, dptr]),
+    "or_eliminate": (C.c_int, [size_t, size_t, dptr, size_t, C.c_double, dptr, dptr, dptr, C.POINTER(size_t),
+                               C.POINTER(size_t)]),
+    "or_pose_exp": (None, [dptr, dptr]),
+    "or_pose_log": (None, [dptr, dptr]),
+    "or_pose_compose": (None, [dptr, dptr, dptr]),
+    "or_pose_inverse": (None, [dptr, dptr]),
+    "or_pose_adjoint": (None, [dptr, dptr]),
+    "or_pose_right_jacobian": (None, [dptr, dptr]),
+    "or_pose_log_jacobian": (C.c_int, [dptr, dptr]),
+    "or_window_solve": (C.c_int, [size_t, dptr, dptr, size_t, C.POINTER(C.c_uint32), dptr, C.POINTER(OptOpts),
+                                  C.POINTER(LmOpts), size_t, C.POINTER(Report), C.POINTER(LmStats), dptr, dptr, dptr,
+                                  C.POINTER(size_t), C.POINTER(C.c_uint32), C.POINTER(size_t), C.POINTER(size_t)]),
+    "or_window_cost": (C.c_int, [size_t, dptr, dptr, size_t, C.POINTER(C.c_uint32), dptr, dptr]),
 }
 for _n, (_r, _a) in _sig.items():
     _f = getattr(lib, _n)
@@ -336,6 +356,167 @@ class Lsmr(Schur):
         px, pty = np.zeros(self.dim), np.zeros(self.dim)
         lib.or_lsmr_precond(self.h, _dp(x), _dp(px), _dp(y), _dp(pty))
         return px, pty
+
+
+class _Generic(Schur):
+    """Shared generic-backend calls (prepare/accumulate/damping/solve/work)."""
+
+    def __init__(self, handle, dim_hint=0):  # noqa: D107 - Schur.__init__ is not called on purpose
+        self.h = handle
+        self.dim = dim_hint
+        self.max_iterations = 1000
+        self.relative_tolerance = max(1e-10, 128 * np.finfo(float).eps)
+
+    def _limits(self):
+        pass
+
+    def covariance(self, columns, tol=64 * np.finfo(float).eps):
+        cols = np.ascontiguousarray(np.asarray(columns, np.uint64))
+        k = len(cols)
+        out = np.zeros(max(k * k, 1))
+        st = lib.or_backend_covariance(self.h, self._kind, cols.ctypes.data_as(C.POINTER(size_t)), k, tol, _dp(out))
+        return st, out[:k * k].reshape(k, k).T.copy()
+
+
+class DenseNormal(_Generic):
+    """DenseNormalCholesky (src/normal.rs)."""
+    _kind = 1
+
+    def __init__(self):
+        super().__init__(lib.or_dense_normal_create())
+
+    def state(self):
+        normal = np.zeros(max(self.dim * self.dim, 1))
+        rhs = np.zeros(max(self.dim, 1))
+        lib.or_dense_normal_state(self.h, _dp(normal), _dp(rhs))
+        return normal[:self.dim * self.dim].reshape(self.dim, self.dim).T.copy(), rhs[:self.dim]
+
+    def information(self, tol):
+        return lib.or_dense_normal_information(self.h, tol)
+
+
+class DenseSchur(_Generic):
+    """DenseSchur (src/dense_schur.rs): retained prefix + landmark widths."""
+    _kind = 2
+
+    def __init__(self, retained, widths=()):
+        w = (size_t * max(len(widths), 1))(*widths)
+        super().__init__(lib.or_dense_schur_create(retained, w, len(widths)))
+
+
+class DenseQr(_Generic):
+    """DenseQr (src/qr.rs)."""
+    _kind = 0
+
+    def __init__(self, relative_rank_tolerance=64 * np.finfo(float).eps):
+        super().__init__(lib.or_dense_qr_create(relative_rank_tolerance))
+
+    def set_tolerance(self, tol):
+        lib.or_dense_qr_set_tolerance(self.h, tol)
+
+
+def eliminate(rows, removed, tol=-1.0):
+    """Elimination::reduce (src/marginalization.rs:458-513) on row-major [J | r]."""
+    rows = np.ascontiguousarray(np.asarray(rows, np.float64))
+    m, width = rows.shape
+    n = width - 1
+    a = np.zeros(max(m * n, 1))
+    b = np.zeros(max(m, 1))
+    const = C.c_double()
+    rank, nrows = size_t(), size_t()
+    st = lib.or_eliminate(m, n, _dp(rows), removed, tol, _dp(a), _dp(b), C.byref(const), C.byref(rank),
+                          C.byref(nrows))
+    k, sep = nrows.value, n - removed
+    return st, a[:k * sep].reshape(sep, k).T.copy(), b[:k].copy(), const.value, rank.value
+
+
+def pose_exp(d):
+    d = np.ascontiguousarray(d, np.float64)
+    out = np.zeros(7)
+    lib.or_pose_exp(_dp(d), _dp(out))
+    return out
+
+
+def pose_log(p):
+    p = np.ascontiguousarray(p, np.float64)
+    out = np.zeros(6)
+    lib.or_pose_log(_dp(p), _dp(out))
+    return out
+
+
+def pose_compose(a, b):
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    out = np.zeros(7)
+    lib.or_pose_compose(_dp(a), _dp(b), _dp(out))
+    return out
+
+
+def pose_inverse(a):
+    a = np.ascontiguousarray(a, np.float64)
+    out = np.zeros(7)
+    lib.or_pose_inverse(_dp(a), _dp(out))
+    return out
+
+
+def pose_adjoint(p):
+    p = np.ascontiguousarray(p, np.float64)
+    out = np.zeros(36)
+    lib.or_pose_adjoint(_dp(p), _dp(out))
+    return out.reshape(6, 6)
+
+
+def pose_right_jacobian(d):
+    d = np.ascontiguousarray(d, np.float64)
+    out = np.zeros(36)
+    lib.or_pose_right_jacobian(_dp(d), _dp(out))
+    return out.reshape(6, 6)
+
+
+def pose_log_jacobian(d):
+    d = np.ascontiguousarray(d, np.float64)
+    out = np.zeros(36)
+    st = lib.or_pose_log_jacobian(_dp(d), _dp(out))
+    return st, out.reshape(6, 6)
+
+
+def window_solve(poses, prior, rel_ij, rel_z, removed=10, max_iterations=20, gradient_tolerance=1e-8,
+                 step_tolerance=1e-10, cost_tolerance=1e-12, lm_options=None):
+    """LM over DenseSchur(6n, []) for one pose-graph window, then square-root
+    marginalization of its oldest `removed` poses."""
+    poses = np.ascontiguousarray(np.array(poses, np.float64).reshape(-1, 7))
+    n = len(poses)
+    prior = np.ascontiguousarray(prior, np.float64)
+    ij = np.ascontiguousarray(np.asarray(rel_ij, np.uint32).reshape(-1, 2))
+    z = np.ascontiguousarray(np.asarray(rel_z, np.float64).reshape(-1, 7))
+    o = OptOpts(max_iterations, gradient_tolerance, step_tolerance, cost_tolerance)
+    lo = LmOpts(*(lm_options or (1e-3, 1e-12, 1e12, 1e-6, 1e-4, 16)))
+    rep, st = Report(), LmStats()
+    cap = 6 * n + 6
+    a = np.zeros(cap * cap)
+    b = np.zeros(cap)
+    const = C.c_double()
+    rows, nsep, rank = size_t(), size_t(), size_t()
+    sep = np.zeros(max(n, 1), np.uint32)
+    u32 = C.POINTER(C.c_uint32)
+    code = lib.or_window_solve(n, _dp(poses), _dp(prior), len(ij), ij.ctypes.data_as(u32), _dp(z), C.byref(o),
+                               C.byref(lo), removed, C.byref(rep), C.byref(st), _dp(a), _dp(b), C.byref(const),
+                               C.byref(rows), sep.ctypes.data_as(u32), C.byref(nsep), C.byref(rank))
+    k, s = rows.value, 6 * nsep.value
+    return dict(code=code, poses=poses, report=rep, stats=st, prior_a=a[:k * s].reshape(s, k).T.copy(),
+                prior_b=b[:k].copy(), prior_constant=const.value, separator=sep[:nsep.value].copy(),
+                rank=rank.value)
+
+
+def window_cost(poses, prior, rel_ij, rel_z):
+    poses = np.ascontiguousarray(np.array(poses, np.float64).reshape(-1, 7))
+    prior = np.ascontiguousarray(prior, np.float64)
+    ij = np.ascontiguousarray(np.asarray(rel_ij, np.uint32).reshape(-1, 2))
+    z = np.ascontiguousarray(np.asarray(rel_z, np.float64).reshape(-1, 7))
+    out = C.c_double()
+    st = lib.or_window_cost(len(poses), _dp(poses), _dp(prior), len(ij), ij.ctypes.data_as(C.POINTER(C.c_uint32)),
+                            _dp(z), C.byref(out))
+    return st, out.value
 
 
 class Bal:

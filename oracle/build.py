@@ -15,7 +15,8 @@ OUT = HERE / "liboracle.so"
 
 
 def build(force: bool = False) -> Path:
-    if not force and OUT.exists() and OUT.stat().st_mtime >= SRC.stat().st_mtime:
+    sources = [SRC, *HERE.glob("*.hpp")]
+    if not force and OUT.exists() and OUT.stat().st_mtime >= max(p.stat().st_mtime for p in sources):
         return OUT
     # -ffp-contract=off keeps the sequential f64 arithmetic free of fused
     # multiply-adds, like the Rust reference.

@@ -17,6 +17,10 @@
 //     per-iteration callback placed before the convergence test.
 //   src/optimization/levenberg_marquardt.rs:330-472  LM loop
 //   src/optimization/gauss_newton.rs:101-176         GN loop
+//   src/lsmr.rs:126-595 + faer's LSMR               LSMR backend (see its section)
+//   dense.hpp: DenseNormalCholesky, DenseSchur, DenseQr, square-root
+//     elimination and selected covariance; posegraph.hpp: SE(3) geometry and
+//     the pose-graph window workload.
 //
 // Parity pins: the reference's own known-answer tests (ported in tests/).
 // Iteration counts of faer's CG are not pinned by any reference test except
@@ -36,6 +40,10 @@ namespace {
 // Status codes shared with include/fagra_b200.h (same numbering).
 enum Status {
   OK = 0,
+  DUPLICATE_COVARIANCE_BLOCK = 1,
+  SINGULAR_INFORMATION = 2,
+  INVALID_INFORMATION = 3,
+  INVALID_RANK_TOLERANCE = 4,
   INVALID_OPTIONS = 6,
   LINEAR_SOLVE_FAILED = 8,
   NO_CONVERGENCE = 9,
@@ -973,6 +981,8 @@ struct Lsmr : Linear {
 // cross_apply indexes rhs/out with edge offsets relative to each partition;
 // the calls above pass partition base pointers, matching schur.rs:230-242,319-331.
 
+#include "dense.hpp"
+
 // ------------------------------------------------------ Problems for LM/GN
 // A problem exposes the callbacks the optimizers need; the BAL problem below
 // and the host-callback problem used by the scalar tests both implement it.
@@ -1300,6 +1310,8 @@ int gn_optimize(Linear& s, Problem& pb, const OptimizeOptions& opt, Report* rep)
   }
 }
 
+#include "posegraph.hpp"
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -1557,4 +1569,142 @@ OR_API int or_lm_cb(void* schur, void* prob, const OptimizeOptions* opt, const L
 }
 OR_API int or_gn_cb(void* schur, void* prob, const OptimizeOptions* opt, Report* rep) {
   return gn_optimize(*(Linear*)schur, *(CallbackProblem*)prob, *opt, rep);
+}
+
+// ---- Dense backends (src/normal.rs, src/dense_schur.rs, src/qr.rs); the
+// generic or_schur_* entry points above drive them.
+OR_API void* or_dense_normal_create(void) { return (void*)(Linear*)new DenseNormal(); }
+OR_API void* or_dense_schur_create(size_t retained, const size_t* widths, size_t nwidths) {
+  DenseSchur* s = new DenseSchur();
+  s->retained = retained;
+  s->widths.assign(widths, widths + nwidths);
+  return (void*)(Linear*)s;
+}
+OR_API void* or_dense_qr_create(double relative_rank_tolerance) {
+  DenseQr* q = new DenseQr();
+  q->relative_rank_tolerance = relative_rank_tolerance;
+  return (void*)(Linear*)q;
+}
+OR_API void or_dense_qr_set_tolerance(void* h, double tol) {
+  static_cast<DenseQr*>(LIN(h))->relative_rank_tolerance = tol;
+}
+// Dense normal state: lower triangle of J^T J (n*n column-major) and -J^T r.
+OR_API void or_dense_normal_state(void* h, double* normal, double* rhs) {
+  DenseNormal* d = static_cast<DenseNormal*>(LIN(h));
+  if (normal) std::copy(d->normal.begin(), d->normal.end(), normal);
+  if (rhs) std::copy(d->rhs.begin(), d->rhs.end(), rhs);
+}
+OR_API int or_dense_normal_information(void* h, double tol) {
+  return static_cast<DenseNormal*>(LIN(h))->information_factor(tol);
+}
+// Selected covariance of the backend's current model (covariance.rs:263-270):
+// kind 0 = Schur/LSMR/DenseQr (LinearizedModel::covariance), 1 = DenseNormal,
+// 2 = DenseSchur (retained selections). columns are model coordinates.
+OR_API int or_backend_covariance(void* h, int kind, const size_t* columns, size_t k, double tol, double* out) {
+  if (!(tol >= 0 && tol < 1)) return INVALID_RANK_TOLERANCE;
+  std::vector<size_t> cols(columns, columns + k);
+  std::vector<double> res;
+  int st;
+  Linear* b = LIN(h);
+  if (kind == 1) {
+    DenseNormal* d = static_cast<DenseNormal*>(b);
+    st = d->information_factor(tol);
+    if (!st) st = covariance_from_factor(d->normal.data(), d->n, nullptr, cols, res);
+  } else if (kind == 2) {
+    st = static_cast<DenseSchur*>(b)->covariance(cols, tol, res);
+  } else {
+    const Model* m = nullptr;
+    if (auto* s = dynamic_cast<Schur*>(b)) m = &s->model;
+    if (auto* l = dynamic_cast<Lsmr*>(b)) m = &l->model;
+    if (auto* q = dynamic_cast<DenseQr*>(b)) m = &q->model;
+    if (!m) return INVALID_OPTIONS;
+    DenseNormal normal;
+    st = model_covariance(*m, normal, cols, tol, res);
+  }
+  if (!st) std::copy(res.begin(), res.end(), out);
+  return st;
+}
+
+// ---- Square-root elimination (src/marginalization.rs:458-513).
+OR_API int or_eliminate(size_t m, size_t n, const double* rowmajor, size_t removed, double tol, double* a,
+                        double* b, double* constant, size_t* rank, size_t* rows) {
+  EliminationResult r;
+  int st = eliminate(m, n, rowmajor, removed, tol, r);
+  if (st) return st;
+  std::copy(r.a.begin(), r.a.end(), a);
+  std::copy(r.b.begin(), r.b.end(), b);
+  *constant = r.constant;
+  *rank = r.rank;
+  *rows = r.rows;
+  return OK;
+}
+
+// ---- SE(3) (examples/slam/geometry.rs); poses are [qw qx qy qz tx ty tz].
+static Pose3 P7(const double* p) {
+  Pose3 o;
+  std::copy(p, p + 4, o.q);
+  std::copy(p + 4, p + 7, o.t);
+  return o;
+}
+static void W7(const Pose3& p, double* o) {
+  std::copy(p.q, p.q + 4, o);
+  std::copy(p.t, p.t + 3, o + 4);
+}
+OR_API void or_pose_exp(const double* d, double* out) { W7(pose_exp(d), out); }
+OR_API void or_pose_log(const double* p, double* out) { pose_log(P7(p), out); }
+OR_API void or_pose_compose(const double* a, const double* b, double* out) { W7(compose(P7(a), P7(b)), out); }
+OR_API void or_pose_inverse(const double* a, double* out) { W7(inverse(P7(a)), out); }
+OR_API void or_pose_adjoint(const double* p, double* out) { pose_adjoint(P7(p), out); }
+OR_API void or_pose_right_jacobian(const double* d, double* out) { pose_right_jacobian(d, out); }
+OR_API int or_pose_log_jacobian(const double* d, double* out) { return log_jacobian(d, out); }
+
+// ---- Pose-graph windows: LM over DenseSchur(6n, []) then marginalization of
+// the oldest `removed` poses. poses[7n] in/out; rel_ij[2*nrel]; rel_z[7*nrel].
+OR_API int or_window_solve(size_t n, double* poses, const double* prior, size_t nrel, const uint32_t* rel_ij,
+                           const double* rel_z, const OptimizeOptions* opt, const LmOptions* lo, size_t removed,
+                           Report* rep, LmStats* st, double* prior_a, double* prior_b, double* prior_constant,
+                           size_t* prior_rows, uint32_t* separator, size_t* nseparator, size_t* rank) {
+  PoseWindow w;
+  w.x.resize(n);
+  for (size_t k = 0; k < n; ++k) w.x[k] = P7(poses + 7 * k);
+  w.prior = P7(prior);
+  w.rel.resize(nrel);
+  for (size_t k = 0; k < nrel; ++k) {
+    w.rel[k].i = rel_ij[2 * k];
+    w.rel[k].j = rel_ij[2 * k + 1];
+    w.rel[k].z = P7(rel_z + 7 * k);
+  }
+  DenseSchur solver;
+  solver.retained = 6 * n;
+  int code = lm_optimize(solver, w, *opt, *lo, rep, st, nullptr, nullptr);
+  for (size_t k = 0; k < n; ++k) W7(w.x[k], poses + 7 * k);
+  if (code != OK && code != NO_PROGRESS && code != NO_CONVERGENCE) return code;
+  if (removed) {
+    WindowPrior wp;
+    int s = marginalize_window(w, std::min(removed, n), wp);
+    if (s) return s;
+    std::copy(wp.elim.a.begin(), wp.elim.a.end(), prior_a);
+    std::copy(wp.elim.b.begin(), wp.elim.b.end(), prior_b);
+    *prior_constant = wp.elim.constant;
+    *prior_rows = wp.elim.rows;
+    *rank = wp.elim.rank;
+    std::copy(wp.separator.begin(), wp.separator.end(), separator);
+    *nseparator = wp.separator.size();
+  }
+  return code;
+}
+// Window cost at the given poses (PosePrior + relative factors).
+OR_API int or_window_cost(size_t n, const double* poses, const double* prior, size_t nrel, const uint32_t* rel_ij,
+                          const double* rel_z, double* out) {
+  PoseWindow w;
+  w.x.resize(n);
+  for (size_t k = 0; k < n; ++k) w.x[k] = P7(poses + 7 * k);
+  w.prior = P7(prior);
+  w.rel.resize(nrel);
+  for (size_t k = 0; k < nrel; ++k) {
+    w.rel[k].i = rel_ij[2 * k];
+    w.rel[k].j = rel_ij[2 * k + 1];
+    w.rel[k].z = P7(rel_z + 7 * k);
+  }
+  return w.cost(false, out);
 }
