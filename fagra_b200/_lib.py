@@ -92,6 +92,18 @@ class LsmrTimingsC(C.Structure):
                  "residual_checks")]
 
 
+class WindowReportC(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("termination", C.c_int),
+        ("iterations", size_t), ("linearizations", size_t), ("attempts", size_t), ("rejected_steps", size_t),
+        ("cost_evaluations", size_t), ("last_rejection", C.c_int),
+        ("initial_cost", C.c_double), ("final_cost", C.c_double), ("damping", C.c_double),
+        ("gradient_norm", C.c_double), ("step_norm", C.c_double),
+        ("prior_status", C.c_int), ("prior_rows", size_t), ("eliminated_rank", size_t),
+        ("separator_poses", size_t), ("prior_constant", C.c_double),
+    ]
+
+
 class OptimizeOptionsC(C.Structure):
     _fields_ = [
         ("max_iterations", size_t),
@@ -205,6 +217,18 @@ SIGNATURES = {
                                  C.POINTER(LmStatisticsC)]),
     "fg_gn_optimize": (C.c_int, [C.c_void_p, C.POINTER(ProblemCallbacksC), C.c_void_p, dptr,
                                  C.POINTER(OptimizeOptionsC), C.POINTER(ReportC)]),
+    "fg_windows_create": (C.c_int, [size_t, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                    size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "fg_windows_destroy": (None, [C.c_void_p]),
+    "fg_windows_prior_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                          C.POINTER(C.c_uint32)]),
+    "fg_windows_upload": (C.c_int, [C.c_void_p, dptr, dptr, dptr]),
+    "fg_windows_run": (C.c_int, [C.c_void_p, C.POINTER(OptimizeOptionsC), C.POINTER(LmOptionsC)]),
+    "fg_windows_download": (C.c_int, [C.c_void_p, dptr, C.POINTER(WindowReportC), dptr, dptr]),
+    "fg_windows_solve": (C.c_int, [C.c_void_p, dptr, dptr, dptr, C.POINTER(OptimizeOptionsC), C.POINTER(LmOptionsC),
+                                   C.POINTER(WindowReportC), dptr, dptr]),
+    "fg_windows_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), dptr]),
+    "fg_windows_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "fg_lsmr_default_options": (None, [C.POINTER(LsmrOptions)]),
     "fg_lsmr_create": (C.c_int, [C.POINTER(LsmrOptions), C.POINTER(C.c_void_p)]),
     "fg_lsmr_set_options": (C.c_int, [C.c_void_p, C.POINTER(LsmrOptions)]),

@@ -1,0 +1,253 @@
+"""Deterministic synthetic SE(3) pose-graph windows (the batched-window workload).
+
+A batch holds independent windows of uneven size. Window w has n_w poses
+(uniform in [min_poses, max_poses]); its factors are, in emission order,
+  - an anchor PosePrior on pose 0 (measurement = the true pose 0),
+  - relative-pose factors i -> i+1 (odometry) for every consecutive pair,
+  - round(loop_fraction * n_w) loop closures between distinct random pairs
+    (i, j) with j >= i + 2, no pair repeated.
+Relative measurements are z_ij = (x_i^-1 x_j) Exp([nt; nr]) with translation
+noise nt ~ N(0, 0.05^2) and rotation noise nr ~ N(0, 0.01^2) per component.
+True trajectories move about 1 m per step along the body x axis with small
+random turns; initial estimates are the dead-reckoned odometry chain from the
+true pose 0.
+
+Poses are 7 doubles [qw, qx, qy, qz, tx, ty, tz]; tangents are body-frame
+[v, w] with right increments (x (+) d = x Exp(d)), as in fagra's
+examples/slam/geometry.rs. All randomness is the counter-based generator of
+`synthetic` (seed, stream, index), so every window is reproducible alone.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .synthetic import normal, uniform
+
+
+def _qmul(a, b):
+    w = a[..., 0] * b[..., 0] - a[..., 1] * b[..., 1] - a[..., 2] * b[..., 2] - a[..., 3] * b[..., 3]
+    x = a[..., 0] * b[..., 1] + a[..., 1] * b[..., 0] + a[..., 2] * b[..., 3] - a[..., 3] * b[..., 2]
+    y = a[..., 0] * b[..., 2] - a[..., 1] * b[..., 3] + a[..., 2] * b[..., 0] + a[..., 3] * b[..., 1]
+    z = a[..., 0] * b[..., 3] + a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1] + a[..., 3] * b[..., 0]
+    return np.stack([w, x, y, z], axis=-1)
+
+
+def _qrot(q, v):
+    u = q[..., 1:]
+    t = 2.0 * np.cross(u, v)
+    return v + q[..., :1] * t + np.cross(u, t)
+
+
+def compose(a, b):
+    """SE(3) composition of (..., 7) poses."""
+    q = _qmul(a[..., :4], b[..., :4])
+    t = _qrot(a[..., :4], b[..., 4:]) + a[..., 4:]
+    return np.concatenate([q, t], axis=-1)
+
+
+def inverse(a):
+    qi = a[..., :4] * np.array([1.0, -1.0, -1.0, -1.0])
+    return np.concatenate([qi, -_qrot(qi, a[..., 4:])], axis=-1)
+
+
+def exp(d):
+    """SE(3) exponential of (..., 6) tangents [v, w] (closed form)."""
+    v, w = d[..., :3], d[..., 3:]
+    t2 = np.sum(w * w, axis=-1, keepdims=True)
+    th = np.sqrt(t2)
+    small = t2 < 1e-8
+    ths = np.where(small, 1.0, th)
+    a = np.where(small, 0.5 - t2 / 48.0, np.sin(0.5 * th) / ths)
+    qw = np.cos(0.5 * th)
+    b = np.where(small, 0.5 - t2 / 24.0, (1.0 - np.cos(th)) / np.where(small, 1.0, t2))
+    c = np.where(small, 1.0 / 6.0 - t2 / 120.0, (th - np.sin(th)) / np.where(small, 1.0, t2 * ths))
+    q = np.concatenate([qw, w * a], axis=-1)
+    q /= np.linalg.norm(q, axis=-1, keepdims=True)
+    wxv = np.cross(w, v)
+    t = v + b * wxv + c * np.cross(w, wxv)
+    return np.concatenate([q, t], axis=-1)
+
+
+@dataclass
+class WindowBatch:
+    sizes: np.ndarray        # (W,) poses per window
+    pose_offset: np.ndarray  # (W+1,)
+    poses: np.ndarray        # (sum n, 7) initial estimates
+    truth: np.ndarray        # (sum n, 7)
+    prior: np.ndarray        # (W, 7) anchor measurement on each window's pose 0
+    rel_offset: np.ndarray   # (W+1,)
+    rel_ij: np.ndarray       # (R, 2) uint32, window-local pose indices
+    rel_z: np.ndarray        # (R, 7)
+
+    @property
+    def windows(self) -> int:
+        return len(self.sizes)
+
+    def window(self, w: int):
+        p0, p1 = self.pose_offset[w], self.pose_offset[w + 1]
+        r0, r1 = self.rel_offset[w], self.rel_offset[w + 1]
+        return (self.poses[p0:p1].copy(), self.prior[w].copy(), self.rel_ij[r0:r1].copy(),
+                self.rel_z[r0:r1].copy())
+
+    def dimension(self, w: int) -> int:
+        return 6 * int(self.sizes[w])
+
+
+def _window(seed: int, w: int, n: int, loop_fraction: float):
+    base = 1000 + 16 * w
+    steps = normal(seed, base + 0, 6 * n).reshape(n, 6) * np.array([0.1, 0.1, 0.05, 0.02, 0.02, 0.1])
+    steps[:, 0] += 1.0
+    start = exp(normal(seed, base + 1, 6).reshape(6) * np.array([2.0, 2.0, 0.5, 0.1, 0.1, 1.0]))
+    truth = np.empty((n, 7))
+    truth[0] = start
+    for k in range(1, n):
+        truth[k] = compose(truth[k - 1], exp(steps[k]))
+    nl = int(round(loop_fraction * n))
+    pairs = []
+    seen = set()
+    draws = uniform(seed, base + 2, 8 * max(nl, 1) + 16)
+    pos = 0
+    while len(pairs) < nl and pos + 1 < len(draws) and n >= 3:
+        i = int(draws[pos] * n)
+        j = int(draws[pos + 1] * n)
+        pos += 2
+        i, j = min(i, j), max(i, j)
+        if j - i >= 2 and (i, j) not in seen:
+            seen.add((i, j))
+            pairs.append((i, j))
+    ij = [(k, k + 1) for k in range(n - 1)] + pairs
+    ij = np.array(ij, dtype=np.uint32).reshape(-1, 2)
+    noise = normal(seed, base + 3, 6 * len(ij)).reshape(-1, 6) * np.array([0.05] * 3 + [0.01] * 3)
+    rel = compose(inverse(truth[ij[:, 0]]), truth[ij[:, 1]])
+    z = compose(rel, exp(noise))
+    init = np.empty_like(truth)
+    init[0] = truth[0]
+    for k in range(1, n):
+        init[k] = compose(init[k - 1], z[k - 1])
+    return truth, init, truth[0].copy(), ij, z
+
+
+def generate(windows: int = 4096, *, min_poses: int = 20, max_poses: int = 300, loop_fraction: float = 0.1,
+             seed: int = 5) -> WindowBatch:
+    sizes = (min_poses + np.floor(uniform(seed, 900, windows) * (max_poses - min_poses + 1))).astype(np.int64)
+    truths, inits, priors, ijs, zs = [], [], [], [], []
+    for w in range(windows):
+        t, i, p, ij, z = _window(seed, w, int(sizes[w]), loop_fraction)
+        truths.append(t)
+        inits.append(i)
+        priors.append(p)
+        ijs.append(ij)
+        zs.append(z)
+    pose_offset = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    rel_offset = np.concatenate([[0], np.cumsum([len(x) for x in ijs])]).astype(np.int64)
+    return WindowBatch(sizes, pose_offset, np.concatenate(inits), np.concatenate(truths), np.stack(priors),
+                       rel_offset, np.concatenate(ijs).astype(np.uint32), np.concatenate(zs))
+
+
+# ---------------------------------------------------------------- device solver
+WINDOW_OPTIONS = dict(max_iterations=20, gradient_tolerance=1e-6, step_tolerance=1e-10, cost_tolerance=1e-12)
+
+
+class WindowSolver:
+    """All windows of a batch on the device: LM over an all-retained DenseSchur
+    per window, then square-root elimination of its oldest `removed` poses
+    (fg_windows_* in libfagra_b200.so)."""
+
+    def __init__(self, batch: WindowBatch, removed: int = 10, precision: str = "f64", device: int = 0):
+        import ctypes as C
+        from ._lib import lib
+        from .errors import raise_for_status
+        self._C, self._lib, self._raise = C, lib, raise_for_status
+        self.batch = batch
+        self.removed = removed
+        po = np.ascontiguousarray(batch.pose_offset, np.uint64)
+        ro = np.ascontiguousarray(batch.rel_offset, np.uint64)
+        ij = np.ascontiguousarray(batch.rel_ij, np.uint32)
+        h = C.c_void_p()
+        u64 = C.POINTER(C.c_uint64)
+        raise_for_status(lib.fg_windows_create(batch.windows, po.ctypes.data_as(u64), ro.ctypes.data_as(u64),
+                                               ij.ctypes.data_as(C.POINTER(C.c_uint32)), removed,
+                                               {"f64": 0, "f32": 1}[precision], device, C.byref(h)))
+        self._h = h
+        so = np.zeros(batch.windows + 1, np.uint64)
+        ao = np.zeros(batch.windows + 1, np.uint64)
+        raise_for_status(lib.fg_windows_prior_layout(h, so.ctypes.data_as(u64), ao.ctypes.data_as(u64), None))
+        sep = np.zeros(max(int(so[-1]), 1), np.uint32)
+        raise_for_status(lib.fg_windows_prior_layout(h, None, None, sep.ctypes.data_as(C.POINTER(C.c_uint32))))
+        self.separator_offset, self.a_offset = so.astype(np.int64), ao.astype(np.int64)
+        self.separators = sep[:int(so[-1])]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fg_windows_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _opts(self, options, lm):
+        from . import _lib
+        o = dict(WINDOW_OPTIONS, **(options or {}))
+        oc = _lib.OptimizeOptionsC(o["max_iterations"], o["gradient_tolerance"], o["step_tolerance"],
+                                   o["cost_tolerance"])
+        lc = _lib.LmOptionsC(*(lm or (1e-3, 1e-12, 1e12, 1e-6, 1e-4, 16)))
+        return oc, lc
+
+    def upload(self, poses=None):
+        C = self._C
+        dp = C.POINTER(C.c_double)
+        b = self.batch
+        x = np.ascontiguousarray(b.poses if poses is None else poses, np.float64)
+        pr = np.ascontiguousarray(b.prior, np.float64)
+        z = np.ascontiguousarray(b.rel_z, np.float64)
+        self._raise(self._lib.fg_windows_upload(self._h, x.ctypes.data_as(dp), pr.ctypes.data_as(dp),
+                                                z.ctypes.data_as(dp)))
+
+    def run(self, options=None, lm=None):
+        oc, lc = self._opts(options, lm)
+        C = self._C
+        self._raise(self._lib.fg_windows_run(self._h, C.byref(oc), C.byref(lc)))
+
+    def download(self):
+        from . import _lib
+        C = self._C
+        dp = C.POINTER(C.c_double)
+        b = self.batch
+        poses = np.zeros_like(b.poses)
+        reps = (_lib.WindowReportC * max(b.windows, 1))()
+        a = np.zeros(max(int(self.a_offset[-1]), 1))
+        bb = np.zeros(max(6 * int(self.separator_offset[-1]), 1))
+        self._raise(self._lib.fg_windows_download(self._h, poses.ctypes.data_as(dp), reps, a.ctypes.data_as(dp),
+                                                  bb.ctypes.data_as(dp)))
+        return poses, list(reps)[:b.windows], a, bb
+
+    def solve(self, options=None, lm=None):
+        self.upload()
+        self.run(options, lm)
+        return self.download()
+
+    def prior(self, w, report, a, b):
+        """(A, b, constant, separator poses) of window w from downloaded buffers."""
+        rows = int(report.prior_rows)
+        s0, s1 = int(self.separator_offset[w]), int(self.separator_offset[w + 1])
+        cols = 6 * (s1 - s0)
+        A = a[int(self.a_offset[w]):int(self.a_offset[w]) + rows * cols].reshape(cols, rows).T.copy()
+        return A, b[6 * s0:6 * s0 + rows].copy(), report.prior_constant
+
+    def tuning(self):
+        C = self._C
+        panel, per = C.c_int(), C.c_int()
+        ms = np.zeros(4)
+        self._lib.fg_windows_tuning(self._h, C.byref(panel), C.byref(per), ms.ctypes.data_as(C.POINTER(C.c_double)))
+        return panel.value, per.value, ms
+
+    def stream(self):
+        C = self._C
+        s = C.c_void_p()
+        self._lib.fg_windows_stream(self._h, C.byref(s))
+        return s.value or 0

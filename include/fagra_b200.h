@@ -340,6 +340,58 @@ FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size
  * (0 if not measured). */
 FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds2);
 
+/* ---- Batched pose-graph windows ----------------------------------------
+ * Thousands of independent SE(3) windows of uneven size solved in one
+ * persistent launch. Window w owns poses [pose_offset[w], pose_offset[w+1])
+ * (7 doubles each: qw qx qy qz tx ty tz) and relative-pose factors
+ * [rel_offset[w], rel_offset[w+1]) between window-local poses (i, j) with
+ * measurement z (7 doubles): r = Log(z^-1 x_i^-1 x_j), Jacobians from
+ * examples/slam/geometry.rs (log_jacobian, adjoint). Pose 0 of every window
+ * carries an anchor PosePrior (examples/slam.rs:26-56). Each window is solved
+ * by LevenbergMarquardt (levenberg_marquardt.rs:330-472) over an all-retained
+ * DenseSchur (src/dense_schur.rs) with dense Cholesky, then its oldest
+ * `removed_poses` poses are eliminated by the square-root reduction of
+ * src/marginalization.rs:458-513 into a prior (A, b, constant) on its
+ * separator poses (touched poses >= removed_poses, increasing). */
+typedef struct {
+  int status;      /* fg_status of the window's LM: FG_OK, FG_NO_PROGRESS, FG_NO_CONVERGENCE, ... */
+  int termination; /* when FG_OK: 2 GradientTolerance, 3 StepTolerance, 4 CostTolerance */
+  size_t iterations, linearizations, attempts, rejected_steps, cost_evaluations;
+  int last_rejection; /* 0 None, 1 LinearSolve, 2 Prediction, 3 InvalidEvaluation, 4 PoorAgreement */
+  double initial_cost, final_cost, damping, gradient_norm, step_norm;
+  int prior_status; /* fg_status of the elimination */
+  size_t prior_rows, eliminated_rank, separator_poses;
+  double prior_constant;
+} fg_window_report;
+typedef struct fg_windows fg_windows;
+/* precision: FG_PRECISION_F64 or FG_PRECISION_F32_REFINED (FP32 Cholesky,
+ * FP64 normal matrix, gradient, cost and two FP64 refinement passes per solve). */
+FG_API fg_status fg_windows_create(size_t windows, const uint64_t* pose_offset, const uint64_t* rel_offset,
+                                   const uint32_t* rel_ij, size_t removed_poses, int precision, int device,
+                                   fg_windows** out);
+FG_API void fg_windows_destroy(fg_windows* batch);
+/* Output layout of the priors (windows + 1 entries each): window w's separator
+ * poses are separators[separator_offset[w] .. separator_offset[w+1]) (window-
+ * local indices); its A is a column-major prior_rows x (6 * separator poses)
+ * matrix at a_offset[w] and its b starts at 6 * separator_offset[w]. */
+FG_API fg_status fg_windows_prior_layout(const fg_windows* batch, uint64_t* separator_offset,
+                                         uint64_t* a_offset, uint32_t* separators);
+/* Host -> device inputs, the device-only solve, device -> host results. */
+FG_API fg_status fg_windows_upload(fg_windows* batch, const double* poses, const double* priors,
+                                   const double* rel_z);
+FG_API fg_status fg_windows_run(fg_windows* batch, const fg_optimize_options* options,
+                                const fg_lm_options* lm_options);
+FG_API fg_status fg_windows_download(fg_windows* batch, double* poses, fg_window_report* reports,
+                                     double* prior_a, double* prior_b);
+/* upload + run + download; poses are updated in place. */
+FG_API fg_status fg_windows_solve(fg_windows* batch, double* poses, const double* priors, const double* rel_z,
+                                  const fg_optimize_options* options, const fg_lm_options* lm_options,
+                                  fg_window_report* reports, double* prior_a, double* prior_b);
+/* The autotuner's choice (panel width 16 or 32, CTAs per SM) and its sample
+ * timings in ms for {32/1, 32/2, 16/1, 16/2} (0 = not run). */
+FG_API fg_status fg_windows_tuning(const fg_windows* batch, int* panel, int* ctas_per_sm, double* ms4);
+FG_API fg_status fg_windows_stream(const fg_windows* batch, void** stream);
+
 /* GaussNewton::solve_batch on a device BAL problem. */
 FG_API fg_status fg_gn_solve_bal(fg_backend* backend, fg_bal_problem* problem,
                                  const fg_optimize_options* options, fg_optimize_report* report);
