@@ -51,8 +51,10 @@ struct WinDev {
   double* xt;               // 7 per pose (trial)
   const int64_t* inc_off;   // per global pose, CSR of incident relative factors
   const int32_t* inc;       // (factor << 1) | side, side 1 = j
-  double* fac;              // 78 per relative factor: r, Ji, Jj
-  double* pfac;             // 42 per window: r, J of the prior
+  double* fac;              // FS per relative factor: r, Ji, Jj, J d
+  double* pfac;             // PS per window: r, J, J d of the prior
+  const int64_t* tile_off;  // W+1: 64-row tiles of each window's coordinates
+  const int32_t* tile_cmin; // per tile: first 64-column tile of its rows' envelope
   const int64_t* mf_off;    // W+1: relative factors touching the eliminated poses
   const int32_t* mf;        // global factor indices
   const int64_t* sep_off;   // W+1: separator poses (window-local, increasing)
@@ -66,11 +68,15 @@ struct WinDev {
   double* G;                // per CTA: Nmax^2 symmetric scaled normal matrix
   void* F;                  // per CTA: Nmax^2 factor (TF)
   double* M;                // per CTA: marginalization system, column-major
+  double* V;                // per CTA: 4 x Nmax doubles (gradient, scales, step, residual)
+  void* TV;                 // per CTA: Nmax TF (factor-precision solve vector)
   size_t g_stride, m_stride;
   int nmax;
 };
 
 constexpr int WNT = 256;  // threads per CTA
+constexpr int FS = 84;    // doubles per relative factor in the scratch
+constexpr int PS = 48;    // doubles per window prior in the scratch
 constexpr int WCT = 64;   // trailing-update tile
 
 __device__ __forceinline__ double wsum(double v, double* red) {
@@ -150,15 +156,44 @@ __device__ inline double window_cost(const WinDev& D, int w, const double* X, do
 }
 
 // ------------------------------------------------------- dense kernels
+// Warp 0 factors the kb x kb diagonal block held in shared memory (row-major,
+// row stride CB+1; lane i owns row i); false on a non-positive or nonfinite
+// pivot (the same answer in every lane).
+template <class TF, int CB>
+__device__ bool warp_potrf(TF* Dg, int kb) {
+  const int lane = threadIdx.x & 31;
+  for (int j = 0; j < kb; ++j) {
+    TF d = Dg[j * (CB + 1) + j];
+    if (!(d > TF(0)) || !isfinite((double)d)) return false;
+    d = sqrt(d);
+    __syncwarp();
+    if (lane == j) Dg[j * (CB + 1) + j] = d;
+    TF lij = 0;
+    if (lane > j && lane < kb) {
+      lij = Dg[lane * (CB + 1) + j] / d;
+      Dg[lane * (CB + 1) + j] = lij;
+    }
+    __syncwarp();
+    if (lane > j && lane < kb)
+      for (int c = j + 1; c <= lane; ++c) Dg[lane * (CB + 1) + c] -= lij * Dg[c * (CB + 1) + j];
+    __syncwarp();
+  }
+  return true;
+}
+
 // In-place lower Cholesky of the n x n lower triangle of A (column-major,
 // leading dimension lda) by the whole CTA; false on a non-positive or
 // nonfinite pivot. sm holds CB x (CB+1) + 2 x WCT x (CB+1) TF values.
+// cmin[T] is the first 64-column tile that any row of 64-row tile T reaches
+// (its envelope, which Cholesky fill never leaves): tiles left of it are
+// exact zeros and are neither read nor written, so only the envelope tiles
+// of A need to be initialized.
 template <class TF, int CB>
-__device__ bool cta_cholesky(TF* A, int n, int lda, TF* sm, int* flag) {
+__device__ bool cta_cholesky(TF* A, int n, int lda, TF* sm, int* flag, const int32_t* cmin) {
   TF* Dg = sm;
   TF* PI = Dg + CB * (CB + 1);
   TF* PJ = PI + WCT * (CB + 1);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int k0 = 0; k0 < n; k0 += CB) {
     const int kb = min(CB, n - k0);
     for (int e = tid; e < kb * kb; e += WNT) {
@@ -166,32 +201,25 @@ __device__ bool cta_cholesky(TF* A, int n, int lda, TF* sm, int* flag) {
       if (r >= c) Dg[r * (CB + 1) + c] = A[(size_t)(k0 + c) * lda + k0 + r];
     }
     __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-      if (tid == 0) {
-        const TF d = Dg[j * (CB + 1) + j];
-        if (!(d > TF(0)) || !isfinite((double)d)) *flag = 1;
-        else Dg[j * (CB + 1) + j] = sqrt(d);
-      }
-      __syncthreads();
-      if (*flag) return false;
-      const TF djj = Dg[j * (CB + 1) + j];
-      for (int i = j + 1 + tid; i < kb; i += WNT) Dg[i * (CB + 1) + j] /= djj;
-      __syncthreads();
-      const int m = kb - j - 1;
-      for (int e = tid; e < m * m; e += WNT) {
-        const int i = j + 1 + e % m, c = j + 1 + e / m;
-        if (i >= c) Dg[i * (CB + 1) + c] -= Dg[i * (CB + 1) + j] * Dg[c * (CB + 1) + j];
-      }
-      __syncthreads();
+    if (warp == 0) {
+      const bool ok = warp_potrf<TF, CB>(Dg, kb);
+      if (lane == 0) *flag = ok ? 0 : 1;
     }
+    __syncthreads();
+    if (*flag) return false;
     for (int e = tid; e < kb * kb; e += WNT) {
       const int r = e % kb, c = e / kb;
       if (r >= c) A[(size_t)(k0 + c) * lda + k0 + r] = Dg[r * (CB + 1) + c];
     }
     const int t0 = k0 + kb;
     if (t0 >= n) break;  // kb == CB whenever rows remain below
+    // Row tiles (64 rows, aligned at 0) whose rows' envelopes start right of
+    // this panel hold exact zeros in it: skip them in the panel solve and the
+    // trailing update.
+    const int pc = k0 / WCT, T0 = t0 / WCT, nT = (n + WCT - 1) / WCT;
     // Panel: L[i, k0:k0+CB] = A[i, k0:k0+CB] L_kk^-T, one row per thread.
     for (int i = t0 + tid; i < n; i += WNT) {
+      if (cmin[i / WCT] > pc) continue;
       TF x[CB];
 #pragma unroll
       for (int q = 0; q < CB; ++q) x[q] = A[(size_t)(k0 + q) * lda + i];
@@ -208,16 +236,18 @@ __device__ bool cta_cholesky(TF* A, int n, int lda, TF* sm, int* flag) {
     __syncthreads();
     // Trailing update A[I, J] -= L[I, panel] L[J, panel]^T on lower tiles.
     const int tr = tid & 15, tc = tid >> 4;
-    for (int J0 = t0; J0 < n; J0 += WCT) {
-      const int nj = min(WCT, n - J0);
+    for (int JT = T0; JT < nT; ++JT) {
+      if (cmin[JT] > pc) continue;  // uniform across the CTA
+      const int J0 = max(JT * WCT, t0), nj = min(JT * WCT + WCT, n) - J0;
       for (int e = tid; e < WCT * CB; e += WNT) {
         const int r = e % WCT, q = e / WCT;
         PJ[r * (CB + 1) + q] = r < nj ? A[(size_t)(k0 + q) * lda + J0 + r] : TF(0);
       }
-      for (int I0 = J0; I0 < n; I0 += WCT) {
-        const int ni = min(WCT, n - I0);
+      for (int IT = JT; IT < nT; ++IT) {
+        if (cmin[IT] > pc) continue;
+        const int I0 = max(IT * WCT, t0), ni = min(IT * WCT + WCT, n) - I0;
         TF* P = PJ;
-        if (I0 != J0) {
+        if (IT != JT) {
           P = PI;
           for (int e = tid; e < WCT * CB; e += WNT) {
             const int r = e % WCT, q = e / WCT;
@@ -257,40 +287,60 @@ __device__ bool cta_cholesky(TF* A, int n, int lda, TF* sm, int* flag) {
   return true;
 }
 
-// v <- L^-T L^-1 v for the lower factor L (CTA; v in shared memory).
+// v <- L^-T L^-1 v for the lower factor L (whole CTA). The diagonal blocks are
+// staged in shared memory (Dg, CB x (CB+1)) and solved by warp 0 with
+// shuffles; the off-diagonal updates run one row per thread.
 template <class TF, int CB>
-__device__ void cta_llt_solve(const TF* L, int n, int lda, TF* v) {
-  const int tid = threadIdx.x;
+__device__ void cta_llt_solve(const TF* L, int n, int lda, TF* v, TF* Dg, const int32_t* cmin) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int k0 = 0; k0 < n; k0 += CB) {
     const int kb = min(CB, n - k0);
-    if (tid == 0)
-      for (int c = k0; c < k0 + kb; ++c) {
-        TF s = v[c];
-        for (int q = k0; q < c; ++q) s -= L[(size_t)q * lda + c] * v[q];
-        v[c] = s / L[(size_t)c * lda + c];
-      }
+    for (int e = tid; e < kb * kb; e += WNT) {
+      const int r = e % kb, c = e / kb;
+      if (r >= c) Dg[r * (CB + 1) + c] = L[(size_t)(k0 + c) * lda + k0 + r];
+    }
     __syncthreads();
+    if (warp == 0) {
+      TF x = lane < kb ? v[k0 + lane] : TF(0);
+      for (int c = 0; c < kb; ++c) {
+        const TF xc = __shfl_sync(0xffffffffu, x, c) / Dg[c * (CB + 1) + c];
+        if (lane == c) x = xc;
+        else if (lane > c && lane < kb) x -= Dg[lane * (CB + 1) + c] * xc;
+      }
+      if (lane < kb) v[k0 + lane] = x;
+    }
+    __syncthreads();
+    const int pc = k0 / WCT;
     for (int i = k0 + kb + tid; i < n; i += WNT) {
+      if (cmin[i / WCT] > pc) continue;
       TF s = v[i];
-      for (int q = k0; q < k0 + kb; ++q) s -= L[(size_t)q * lda + i] * v[q];
+      for (int q = 0; q < kb; ++q) s -= L[(size_t)(k0 + q) * lda + i] * v[k0 + q];
       v[i] = s;
     }
     __syncthreads();
   }
-  const int last = ((n - 1) / CB) * CB;
-  for (int k0 = last; k0 >= 0 && n > 0; k0 -= CB) {
+  const int last = n > 0 ? ((n - 1) / CB) * CB : -1;
+  for (int k0 = last; k0 >= 0; k0 -= CB) {
     const int kb = min(CB, n - k0);
-    if (tid == 0)
-      for (int c = k0 + kb - 1; c >= k0; --c) {
-        TF s = v[c];
-        for (int i = c + 1; i < k0 + kb; ++i) s -= L[(size_t)c * lda + i] * v[i];
-        v[c] = s / L[(size_t)c * lda + c];
-      }
+    for (int e = tid; e < kb * kb; e += WNT) {
+      const int r = e % kb, c = e / kb;
+      if (r >= c) Dg[r * (CB + 1) + c] = L[(size_t)(k0 + c) * lda + k0 + r];
+    }
     __syncthreads();
-    for (int q = tid; q < k0; q += WNT) {
+    if (warp == 0) {
+      TF x = lane < kb ? v[k0 + lane] : TF(0);
+      for (int c = kb - 1; c >= 0; --c) {
+        const TF xc = __shfl_sync(0xffffffffu, x, c) / Dg[c * (CB + 1) + c];
+        if (lane == c) x = xc;
+        else if (lane < c) x -= Dg[c * (CB + 1) + lane] * xc;
+      }
+      if (lane < kb) v[k0 + lane] = x;
+    }
+    __syncthreads();
+    for (int q = WCT * cmin[k0 / WCT] + tid; q < k0; q += WNT) {
       TF s = v[q];
-      const TF* col = L + (size_t)q * lda;
-      for (int i = k0; i < k0 + kb; ++i) s -= col[i] * v[i];
+      const TF* col = L + (size_t)q * lda + k0;
+      for (int i = 0; i < kb; ++i) s -= col[i] * v[k0 + i];
       v[q] = s;
     }
     __syncthreads();
@@ -388,18 +438,18 @@ __device__ void cta_qr(double* M, int m, int ncols, int r0, int c0, int w, int* 
   }
 }
 
-template <class TF, int CB>
-__global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
+template <class TF, int CB, int MINB>
+__global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ WinShared S;
   __shared__ int next;
-  double* g = reinterpret_cast<double*>(smem_raw);  // gradient
-  double* sc = g + D.nmax;                           // column scales
-  double* dv = sc + D.nmax;                          // scaled rhs / step (double)
-  double* wv = dv + D.nmax;                          // refinement residual (double)
-  TF* tv = reinterpret_cast<TF*>(wv + D.nmax);       // factor-precision solve vector
-  TF* csm = tv + D.nmax + 2;                         // Cholesky staging
-  double* qnorms = reinterpret_cast<double*>(csm);   // QR scratch (after the LM)
+  double* g = D.V + (size_t)blockIdx.x * 4 * D.nmax;  // gradient
+  double* sc = g + D.nmax;                              // column scales
+  double* dv = sc + D.nmax;                             // scaled rhs / step (double)
+  double* wv = dv + D.nmax;                             // refinement residual (double)
+  TF* tv = reinterpret_cast<TF*>(D.TV) + (size_t)blockIdx.x * D.nmax;  // factor-precision vector
+  TF* csm = reinterpret_cast<TF*>(smem_raw);            // Cholesky staging
+  double* qnorms = reinterpret_cast<double*>(smem_raw);  // QR scratch (after the LM)
   int* qperm = reinterpret_cast<int*>(qnorms + D.nmax + 8);
   double* G = D.G + blockIdx.x * D.g_stride;
   TF* F = reinterpret_cast<TF*>(D.F) + blockIdx.x * D.g_stride;
@@ -417,6 +467,8 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
     const int64_t f0 = D.rel_off[w], f1 = D.rel_off[w + 1];
     double* X = D.x + 7 * p0;
     double* XT = D.xt + 7 * p0;
+    const int32_t* cmin = D.tile_cmin + D.tile_off[w];
+    const int nT = (N + WCT - 1) / WCT;
     fg_window_report rep{};
     int status = FG_OK, term = 0;
     // ---- LevenbergMarquardt::optimize (levenberg_marquardt.rs:330-472)
@@ -433,13 +485,13 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
       // Linearize: factor residuals and Jacobians.
       double nb = 0;
       for (int64_t f = f0 + tid; f < f1; f += WNT) {
-        double* o = D.fac + 78 * f;
+        double* o = D.fac + FS * f;
         if (!rel_eval(D, f, X, o, o + 6, o + 42)) nb = 1;
         for (int k = 0; k < 78; ++k)
           if (!isfinite(o[k])) nb = 1;
       }
       if (tid == 0) {
-        double* o = D.pfac + 42 * (size_t)w;
+        double* o = D.pfac + PS * (size_t)w;
         if (!prior_eval(D, w, X, o, o + 6)) nb = 1;
       }
       if (wmax(nb, S.red) != 0) {
@@ -451,7 +503,7 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
       for (int p = tid; p < n; p += WNT) {
         double gg[6] = {0, 0, 0, 0, 0, 0}, ss[6] = {0, 0, 0, 0, 0, 0};
         if (p == 0) {
-          const double* o = D.pfac + 42 * (size_t)w;
+          const double* o = D.pfac + PS * (size_t)w;
           for (int c = 0; c < 6; ++c)
             for (int k = 0; k < 6; ++k) {
               gg[c] += o[6 + k * 6 + c] * o[k];
@@ -460,7 +512,7 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
         }
         for (int64_t e = D.inc_off[p0 + p]; e < D.inc_off[p0 + p + 1]; ++e) {
           const int32_t code = D.inc[e];
-          const double* o = D.fac + 78 * (int64_t)(code >> 1);
+          const double* o = D.fac + FS * (int64_t)(code >> 1);
           const double* J = o + ((code & 1) ? 42 : 6);
           for (int c = 0; c < 6; ++c)
             for (int k = 0; k < 6; ++k) {
@@ -495,40 +547,46 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
         status = FG_NO_CONVERGENCE;
         break;
       }
-      // prepare_damping: scaled normal matrix G = D^-1 J^T J D^-1, full symmetric.
-      for (int64_t e = tid; e < (int64_t)N * N; e += WNT) G[e] = 0;
+      // prepare_damping: lower triangle of the scaled normal matrix
+      // G = D^-1 J^T J D^-1 over the envelope tiles.
+      for (int T = 0; T < nT; ++T)
+        for (int C = cmin[T]; C <= T; ++C)
+          for (int e = tid; e < WCT * WCT; e += WNT) {
+            const int r = T * WCT + (e % WCT), c = C * WCT + (e / WCT);
+            if (r < N && c <= r) G[(size_t)c * N + r] = 0;
+          }
       __syncthreads();
       for (int p = tid; p < n; p += WNT) {
         double blk[36];
         for (int k = 0; k < 36; ++k) blk[k] = 0;
         if (p == 0) {
-          const double* J = D.pfac + 42 * (size_t)w + 6;
+          const double* J = D.pfac + PS * (size_t)w + 6;
           for (int a = 0; a < 6; ++a)
-            for (int b = 0; b < 6; ++b)
+            for (int b = 0; b <= a; ++b)
               for (int k = 0; k < 6; ++k) blk[a * 6 + b] += J[k * 6 + a] * J[k * 6 + b];
         }
         for (int64_t e = D.inc_off[p0 + p]; e < D.inc_off[p0 + p + 1]; ++e) {
           const int32_t code = D.inc[e];
-          const double* J = D.fac + 78 * (int64_t)(code >> 1) + ((code & 1) ? 42 : 6);
+          const double* J = D.fac + FS * (int64_t)(code >> 1) + ((code & 1) ? 42 : 6);
           for (int a = 0; a < 6; ++a)
-            for (int b = 0; b < 6; ++b)
+            for (int b = 0; b <= a; ++b)
               for (int k = 0; k < 6; ++k) blk[a * 6 + b] += J[k * 6 + a] * J[k * 6 + b];
         }
         for (int a = 0; a < 6; ++a)
-          for (int b = 0; b < 6; ++b)
+          for (int b = 0; b <= a; ++b)
             G[(size_t)(6 * p + b) * N + 6 * p + a] = blk[a * 6 + b] / (sc[6 * p + a] * sc[6 * p + b]);
       }
       for (int64_t f = f0 + tid; f < f1; f += WNT) {
         const int i = (int)D.rel_ij[2 * f], j = (int)D.rel_ij[2 * f + 1];
-        const double* Ji = D.fac + 78 * f + 6;
-        const double* Jj = D.fac + 78 * f + 42;
+        const double* Ji = D.fac + FS * f + 6;
+        const double* Jj = D.fac + FS * f + 42;
         for (int a = 0; a < 6; ++a)
           for (int b = 0; b < 6; ++b) {
             double v = 0;
             for (int k = 0; k < 6; ++k) v += Ji[k * 6 + a] * Jj[k * 6 + b];
             v /= sc[6 * i + a] * sc[6 * j + b];
-            atomicAdd(&G[(size_t)(6 * j + b) * N + 6 * i + a], v);
-            atomicAdd(&G[(size_t)(6 * i + a) * N + 6 * j + b], v);
+            const int row = i > j ? 6 * i + a : 6 * j + b, col = i > j ? 6 * j + b : 6 * i + a;
+            atomicAdd(&G[(size_t)col * N + row], v);
           }
       }
       __syncthreads();
@@ -542,38 +600,83 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
         rep.damping = damping;
         int rejection = 0;
         // solve_damped: (G + damping I) z = -g / D, delta = z / D.
-        for (int64_t e = tid; e < (int64_t)N * N; e += WNT) {
-          const int r = (int)(e % N), c = (int)(e / N);
-          if (r >= c) F[e] = (TF)(G[e] + (r == c ? damping : 0.0));
-        }
+        for (int T = 0; T < nT; ++T)
+          for (int C = cmin[T]; C <= T; ++C)
+            for (int e = tid; e < WCT * WCT; e += WNT) {
+              const int r = T * WCT + (e % WCT), c = C * WCT + (e / WCT);
+              if (r < N && c <= r) {
+                const size_t k = (size_t)c * N + r;
+                F[k] = (TF)(G[k] + (r == c ? damping : 0.0));
+              }
+            }
         for (int c = tid; c < N; c += WNT) dv[c] = -g[c] / sc[c];
         if (tid == 0) S.flag = 0;
         __syncthreads();
-        bool ok = cta_cholesky<TF, CB>(F, N, N, csm, &S.flag);
+        bool ok = cta_cholesky<TF, CB>(F, N, N, csm, &S.flag, cmin);
         __syncthreads();
         if (ok) {
           if (std::is_same<TF, double>::value) {
-            cta_llt_solve<TF, CB>(F, N, N, reinterpret_cast<TF*>(dv));
+            cta_llt_solve<TF, CB>(F, N, N, reinterpret_cast<TF*>(dv), csm, cmin);
           } else {
-            // FP32 factor, FP64 refinement: z += F^-1 (b - (G + damping I) z).
+            // FP32 factor, FP64 refinement: z += F^-1 (b - (G + damping I) z)
+            // until the FP64 residual is below 1e-14 |b| or O.refine passes.
+            double bn = 0;
             for (int c = tid; c < N; c += WNT) {
               wv[c] = dv[c];
+              bn += dv[c] * dv[c];
               dv[c] = 0;
             }
-            __syncthreads();
+            bn = wsum(bn, S.red);
             for (int it = 0; it <= O.refine; ++it) {
               for (int c = tid; c < N; c += WNT) tv[c] = (TF)wv[c];
               __syncthreads();
-              cta_llt_solve<TF, CB>(F, N, N, tv);
+              cta_llt_solve<TF, CB>(F, N, N, tv, csm, cmin);
               for (int c = tid; c < N; c += WNT) dv[c] += (double)tv[c];
               __syncthreads();
-              if (it == O.refine) break;
-              for (int r = tid; r < N; r += WNT) {
-                double s = -g[r] / sc[r] - damping * dv[r];
-                for (int c = 0; c < N; ++c) s -= G[(size_t)c * N + r] * dv[c];
-                wv[r] = s;
+              // Residual from the factor Jacobians: G z = D^-1 J^T (J (D^-1 z)).
+              for (int64_t f = f0 + tid; f < f1; f += WNT) {
+                const int i = (int)D.rel_ij[2 * f], j = (int)D.rel_ij[2 * f + 1];
+                double* o = D.fac + FS * f;
+                for (int a = 0; a < 6; ++a) {
+                  double u = 0;
+                  for (int k = 0; k < 6; ++k)
+                    u += o[6 + a * 6 + k] * dv[6 * i + k] / sc[6 * i + k] + o[42 + a * 6 + k] * dv[6 * j + k] / sc[6 * j + k];
+                  o[78 + a] = u;
+                }
+              }
+              if (tid == 0) {
+                double* o = D.pfac + PS * (size_t)w;
+                for (int a = 0; a < 6; ++a) {
+                  double u = 0;
+                  for (int k = 0; k < 6; ++k) u += o[6 + a * 6 + k] * dv[k] / sc[k];
+                  o[42 + a] = u;
+                }
               }
               __syncthreads();
+              double rn = 0;
+              for (int p = tid; p < n; p += WNT) {
+                double y[6] = {0, 0, 0, 0, 0, 0};
+                if (p == 0) {
+                  const double* o = D.pfac + PS * (size_t)w;
+                  for (int c = 0; c < 6; ++c)
+                    for (int k = 0; k < 6; ++k) y[c] += o[6 + k * 6 + c] * o[42 + k];
+                }
+                for (int64_t e = D.inc_off[p0 + p]; e < D.inc_off[p0 + p + 1]; ++e) {
+                  const int32_t code = D.inc[e];
+                  const double* o = D.fac + FS * (int64_t)(code >> 1);
+                  const double* J = o + ((code & 1) ? 42 : 6);
+                  for (int c = 0; c < 6; ++c)
+                    for (int k = 0; k < 6; ++k) y[c] += J[k * 6 + c] * o[78 + k];
+                }
+                for (int c = 0; c < 6; ++c) {
+                  const int r = 6 * p + c;
+                  const double s = -g[r] / sc[r] - damping * dv[r] - y[c] / sc[r];
+                  wv[r] = s;
+                  rn += s * s;
+                }
+              }
+              rn = wsum(rn, S.red);
+              if (!(rn > 1e-28 * bn)) break;
             }
           }
           // delta, prediction -g.d - |J d|^2 / 2 (DenseSchur::solve_damped + verify_step)
@@ -589,8 +692,8 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
           double jd = 0;
           for (int64_t f = f0 + tid; f < f1; f += WNT) {
             const int i = (int)D.rel_ij[2 * f], j = (int)D.rel_ij[2 * f + 1];
-            const double* Ji = D.fac + 78 * f + 6;
-            const double* Jj = D.fac + 78 * f + 42;
+            const double* Ji = D.fac + FS * f + 6;
+            const double* Jj = D.fac + FS * f + 42;
             for (int a = 0; a < 6; ++a) {
               double u = 0;
               for (int k = 0; k < 6; ++k) u += Ji[a * 6 + k] * dv[6 * i + k] + Jj[a * 6 + k] * dv[6 * j + k];
@@ -598,7 +701,7 @@ __global__ void __launch_bounds__(WNT) k_windows(WinDev D, WinOptions O) {
             }
           }
           if (tid == 0) {
-            const double* J = D.pfac + 42 * (size_t)w + 6;
+            const double* J = D.pfac + PS * (size_t)w + 6;
             for (int a = 0; a < 6; ++a) {
               double u = 0;
               for (int k = 0; k < 6; ++k) u += J[a * 6 + k] * dv[k];
@@ -760,16 +863,18 @@ struct WindowsImpl {
   int precision = FG_PRECISION_F64;
   size_t W = 0, P = 0, R = 0;
   int removed = 10;
-  std::vector<int64_t> pose_off, rel_off, sep_off, a_off, mf_off, inc_off;
+  std::vector<int64_t> pose_off, rel_off, sep_off, a_off, mf_off, inc_off, tile_off;
+  std::vector<int32_t> tile_cmin;
   std::vector<uint32_t> rel_ij, sep;
   std::vector<int32_t> inc, mf, order;
   int nmax = 0;
   size_t mcap = 0;
-  DBuf<int64_t> d_pose_off, d_rel_off, d_inc_off, d_mf_off, d_sep_off, d_a_off;
+  DBuf<int64_t> d_pose_off, d_rel_off, d_inc_off, d_mf_off, d_sep_off, d_a_off, d_tile_off;
+  DBuf<int32_t> d_tile_cmin;
   DBuf<uint32_t> d_rel_ij, d_sep, d_queue;
   DBuf<int32_t> d_inc, d_mf, d_order;
-  DBuf<double> d_x, d_xt, d_prior, d_rel_z, d_fac, d_pfac, d_pa, d_pb, d_G, d_M;
-  DBuf<unsigned char> d_F;
+  DBuf<double> d_x, d_xt, d_prior, d_rel_z, d_fac, d_pfac, d_pa, d_pb, d_G, d_M, d_V;
+  DBuf<unsigned char> d_F, d_TV;
   DBuf<fg_window_report> d_reports;
   // autotuned launch
   int variant = -1, ctas_per_sm = 1;
@@ -785,34 +890,47 @@ struct WindowsImpl {
 
   size_t smem_bytes(int cb) const {
     const size_t tf = precision == FG_PRECISION_F64 ? 8 : 4;
-    size_t b = 4 * (size_t)nmax * 8 + ((size_t)nmax + 2) * tf;
-    size_t chol = ((size_t)cb * (cb + 1) + 2 * (size_t)WCT * (cb + 1)) * tf;
-    size_t qr = ((size_t)nmax + 8) * 8 + (size_t)nmax * 4;
-    return b + std::max(chol, qr) + 64;
+    const size_t chol = ((size_t)cb * (cb + 1) + 2 * (size_t)WCT * (cb + 1)) * tf;
+    const size_t qr = ((size_t)nmax + 8) * 8 + (size_t)nmax * 4;
+    return std::max(chol, qr) + 64;
   }
 };
 
 namespace {
 // Raise the dynamic shared-memory cap of every variant once per handle
 // (outside any stream capture).
-template <class TF, int CB>
+template <class TF, int CB, int MINB>
 fg_status prime_variant() {
-  FG_CUDA(cudaFuncSetAttribute(k_windows<TF, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+  FG_CUDA(cudaFuncSetAttribute(k_windows<TF, CB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
   return FG_OK;
 }
-template <class TF, int CB>
-fg_status launch_variant(WindowsImpl& h, const WinDev& D, const WinOptions& O, int grid) {
-  FG_LAUNCH((k_windows<TF, CB>), grid, WNT, h.smem_bytes(CB), h.st, D, O);
+template <class TF>
+fg_status prime_all() {
+  FG_TRY((prime_variant<TF, 32, 1>()));
+  FG_TRY((prime_variant<TF, 32, 2>()));
+  FG_TRY((prime_variant<TF, 16, 2>()));
+  FG_TRY((prime_variant<TF, 16, 3>()));
   return FG_OK;
+}
+template <class TF, int CB, int MINB>
+fg_status launch_variant(WindowsImpl& h, const WinDev& D, const WinOptions& O, int grid) {
+  FG_LAUNCH((k_windows<TF, CB, MINB>), grid, WNT, h.smem_bytes(CB), h.st, D, O);
+  return FG_OK;
+}
+// Variants: 0 = panel 32 / 1 CTA per SM, 1 = 32 / 2, 2 = 16 / 2, 3 = 16 / 3
+// (register budgets follow the CTAs per SM).
+template <class TF>
+fg_status launch_tf(WindowsImpl& h, int variant, const WinDev& D, const WinOptions& O, int grid) {
+  switch (variant) {
+    case 0: return launch_variant<TF, 32, 1>(h, D, O, grid);
+    case 1: return launch_variant<TF, 32, 2>(h, D, O, grid);
+    case 2: return launch_variant<TF, 16, 2>(h, D, O, grid);
+    default: return launch_variant<TF, 16, 3>(h, D, O, grid);
+  }
 }
 fg_status launch(WindowsImpl& h, int variant, const WinDev& D, const WinOptions& O, int grid) {
-  const bool f64 = h.precision == FG_PRECISION_F64;
-  switch (variant & 1) {
-    case 0:
-      return f64 ? launch_variant<double, 16>(h, D, O, grid) : launch_variant<float, 16>(h, D, O, grid);
-    default:
-      return f64 ? launch_variant<double, 32>(h, D, O, grid) : launch_variant<float, 32>(h, D, O, grid);
-  }
+  return h.precision == FG_PRECISION_F64 ? launch_tf<double>(h, variant, D, O, grid)
+                                         : launch_tf<float>(h, variant, D, O, grid);
 }
 }  // namespace
 
@@ -856,7 +974,7 @@ fg_status windows_view(WindowsImpl& h, const fg_optimize_options& o, const fg_lm
   O->max_iterations = (unsigned)std::min<size_t>(o.max_iterations, 0xffffffffu);
   O->max_trials = (unsigned)std::min<size_t>(lo.max_trials, 0xffffffffu);
   O->removed = h.removed;
-  O->refine = 2;
+  O->refine = 8;
   WinDev d{};
   d.W = (int)h.W;
   d.pose_off = h.d_pose_off.get();
@@ -875,6 +993,8 @@ fg_status windows_view(WindowsImpl& h, const fg_optimize_options& o, const fg_lm
   d.sep_off = h.d_sep_off.get();
   d.sep = h.d_sep.get();
   d.a_off = h.d_a_off.get();
+  d.tile_off = h.d_tile_off.get();
+  d.tile_cmin = h.d_tile_cmin.get();
   d.prior_a = h.d_pa.get();
   d.prior_b = h.d_pb.get();
   d.reports = h.d_reports.get();
@@ -898,6 +1018,8 @@ fg_status ensure_slots(WindowsImpl& h, int slots) {
   FG_TRY(h.d_G.resize(std::max<size_t>(g * slots, 1)));
   FG_TRY(h.d_F.resize(std::max<size_t>(g * slots * tf, 1)));
   FG_TRY(h.d_M.resize(std::max<size_t>(h.mcap * slots, 1)));
+  FG_TRY(h.d_V.resize(std::max<size_t>(4 * (size_t)h.nmax * slots, 1)));
+  FG_TRY(h.d_TV.resize(std::max<size_t>((size_t)h.nmax * slots * tf, 1)));
   h.slots = slots;
   return FG_OK;
 }
@@ -913,6 +1035,8 @@ fg_status run_once(WindowsImpl& h, int variant, int per_sm, const WinDev& D0, co
   D.G = h.d_G.get();
   D.F = h.d_F.get();
   D.M = h.d_M.get();
+  D.V = h.d_V.get();
+  D.TV = h.d_TV.get();
   EventTimer t;
   if (ms) t.start(h.st);
   FG_CUDA(cudaMemsetAsync(h.d_queue.get(), 0, sizeof(unsigned), h.st));
@@ -1045,6 +1169,27 @@ FG_API fg_status fg_windows_create(size_t windows, const uint64_t* pose_offset, 
         return fail(FG_UNSUPPORTED_STRUCTURE);
       }
     }
+    // Envelope of each window's normal matrix: row block p starts at pose
+    // env[p] = min(p, lowest neighbour); per 64-row tile, its first 64-column tile.
+    h.tile_off.assign(windows + 1, 0);
+    h.tile_cmin.clear();
+    for (size_t w = 0; w < windows; ++w) {
+      const int64_t n = h.pose_off[w + 1] - h.pose_off[w], N = 6 * n;
+      std::vector<int64_t> env(n);
+      for (int64_t p = 0; p < n; ++p) env[p] = p;
+      for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
+        const int64_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
+        const int64_t hi = std::max(i, j), lo = std::min(i, j);
+        env[hi] = std::min(env[hi], lo);
+      }
+      const int64_t nT = (N + 63) / 64;
+      for (int64_t T = 0; T < nT; ++T) {
+        int64_t first = T * 64;
+        for (int64_t r = T * 64; r < std::min(N, T * 64 + 64); ++r) first = std::min(first, 6 * env[r / 6]);
+        h.tile_cmin.push_back((int32_t)(first / 64));
+      }
+      h.tile_off[w + 1] = (int64_t)h.tile_cmin.size();
+    }
     for (size_t p = 0; p < h.P; ++p) cnt[p + 1] += cnt[p];
     h.inc_off = cnt;
     h.inc.assign(std::max<int64_t>(cnt[h.P], 1), 0);
@@ -1085,6 +1230,10 @@ FG_API fg_status fg_windows_create(size_t windows, const uint64_t* pose_offset, 
     if (sv.empty()) sv.push_back(0);
     if ((s = upload(h.d_sep, sv.data(), sv.size(), st))) return fail(s);
     if ((s = upload(h.d_a_off, h.a_off.data(), h.a_off.size(), st))) return fail(s);
+    if ((s = upload(h.d_tile_off, h.tile_off.data(), h.tile_off.size(), st))) return fail(s);
+    std::vector<int32_t> tc = h.tile_cmin;
+    if (tc.empty()) tc.push_back(0);
+    if ((s = upload(h.d_tile_cmin, tc.data(), tc.size(), st))) return fail(s);
     std::vector<int32_t> ord = h.order;
     if (ord.empty()) ord.push_back(0);
     if ((s = upload(h.d_order, ord.data(), ord.size(), st))) return fail(s);
@@ -1093,8 +1242,8 @@ FG_API fg_status fg_windows_create(size_t windows, const uint64_t* pose_offset, 
     if ((s = h.d_xt.resize(std::max<size_t>(7 * h.P, 1)))) return fail(s);
     if ((s = h.d_prior.resize(std::max<size_t>(7 * windows, 1)))) return fail(s);
     if ((s = h.d_rel_z.resize(std::max<size_t>(7 * h.R, 1)))) return fail(s);
-    if ((s = h.d_fac.resize(std::max<size_t>(78 * h.R, 1)))) return fail(s);
-    if ((s = h.d_pfac.resize(std::max<size_t>(42 * windows, 1)))) return fail(s);
+    if ((s = h.d_fac.resize(std::max<size_t>(FS * h.R, 1)))) return fail(s);
+    if ((s = h.d_pfac.resize(std::max<size_t>(PS * windows, 1)))) return fail(s);
     if ((s = h.d_pa.resize(std::max<int64_t>(h.a_off[windows], 1)))) return fail(s);
     if ((s = h.d_pb.resize(std::max<int64_t>(6 * h.sep_off[windows], 1)))) return fail(s);
     if ((s = h.d_reports.resize(std::max<size_t>(windows, 1)))) return fail(s);
@@ -1142,15 +1291,13 @@ FG_API fg_status fg_windows_run(fg_windows* H, const fg_optimize_options* o, con
   WinDev D;
   WinOptions O;
   FG_TRY(windows_view(h, *o, *lo, &D, &O));
-  if (h.smem_bytes(32) > 220 * 1024) {
+  if (h.smem_bytes(32) > 100 * 1024) {
     set_error("window too large for the shared-memory working set");
     return FG_UNSUPPORTED_STRUCTURE;
   }
   if (h.variant < 0) {
-    FG_TRY((prime_variant<double, 16>()));
-    FG_TRY((prime_variant<double, 32>()));
-    FG_TRY((prime_variant<float, 16>()));
-    FG_TRY((prime_variant<float, 32>()));
+    FG_TRY(prime_all<double>());
+    FG_TRY(prime_all<float>());
     // Autotune on the largest scheduled windows (a sample of at most four
     // CTAs' worth per SM): time each (panel width, CTAs per SM) schedule once,
     // keep the fastest and restore the poses the sample moved.
@@ -1158,27 +1305,26 @@ FG_API fg_status fg_windows_run(fg_windows* H, const fg_optimize_options* o, con
     DBuf<double> saved;
     FG_TRY(saved.resize(std::max<size_t>(7 * h.P, 1)));
     FG_CUDA(cudaMemcpyAsync(saved.get(), h.d_x.get(), 7 * h.P * sizeof(double), cudaMemcpyDeviceToDevice, h.st));
-    int best = 1, best_per = 1;
+    const int per_sm[4] = {1, 2, 2, 3};
+    const int panel[4] = {32, 32, 16, 16};
+    int best = 0;
     float best_ms = 0;
-    const int cand[4][2] = {{1, 1}, {1, 2}, {0, 1}, {0, 2}};
     for (int c = 0; c < 4; ++c) {
-      const int per = cand[c][1];
-      const size_t sm = h.smem_bytes(cand[c][0] ? 32 : 16);
-      if (per == 2 && 2 * sm > 220 * 1024) continue;
+      const size_t sm = h.smem_bytes(panel[c]) + 2048;
+      if ((size_t)per_sm[c] * sm > 220 * 1024) continue;
       float ms = 0;
       FG_CUDA(cudaMemcpyAsync(h.d_x.get(), saved.get(), 7 * h.P * sizeof(double), cudaMemcpyDeviceToDevice, h.st));
-      FG_TRY(run_once(h, cand[c][0], per, D, O, sample, &ms));
+      FG_TRY(run_once(h, c, per_sm[c], D, O, sample, &ms));
       h.tuned_ms[c] = ms;
       if (best_ms == 0 || ms < best_ms) {
         best_ms = ms;
-        best = cand[c][0];
-        best_per = per;
+        best = c;
       }
     }
     FG_CUDA(cudaMemcpyAsync(h.d_x.get(), saved.get(), 7 * h.P * sizeof(double), cudaMemcpyDeviceToDevice, h.st));
     FG_CUDA(cudaStreamSynchronize(h.st));
     h.variant = best;
-    h.ctas_per_sm = best_per;
+    h.ctas_per_sm = per_sm[best];
   }
   return run_graph(h, D, O);
 }
@@ -1213,7 +1359,7 @@ FG_API fg_status fg_windows_solve(fg_windows* H, double* poses, const double* pr
 FG_API fg_status fg_windows_tuning(const fg_windows* H, int* panel, int* ctas_per_sm, double* ms4) {
   if (!H) return FG_NULL_ARGUMENT;
   const WindowsImpl& h = H->impl;
-  if (panel) *panel = h.variant < 0 ? 0 : (h.variant ? 32 : 16);
+  if (panel) *panel = h.variant < 0 ? 0 : (h.variant < 2 ? 32 : 16);
   if (ctas_per_sm) *ctas_per_sm = h.ctas_per_sm;
   if (ms4)
     for (int k = 0; k < 4; ++k) ms4[k] = h.tuned_ms[k];

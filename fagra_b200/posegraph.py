@@ -95,15 +95,8 @@ class WindowBatch:
         return 6 * int(self.sizes[w])
 
 
-def _window(seed: int, w: int, n: int, loop_fraction: float):
+def _loop_pairs(seed: int, w: int, n: int, loop_fraction: float):
     base = 1000 + 16 * w
-    steps = normal(seed, base + 0, 6 * n).reshape(n, 6) * np.array([0.1, 0.1, 0.05, 0.02, 0.02, 0.1])
-    steps[:, 0] += 1.0
-    start = exp(normal(seed, base + 1, 6).reshape(6) * np.array([2.0, 2.0, 0.5, 0.1, 0.1, 1.0]))
-    truth = np.empty((n, 7))
-    truth[0] = start
-    for k in range(1, n):
-        truth[k] = compose(truth[k - 1], exp(steps[k]))
     nl = int(round(loop_fraction * n))
     pairs = []
     seen = set()
@@ -117,33 +110,54 @@ def _window(seed: int, w: int, n: int, loop_fraction: float):
         if j - i >= 2 and (i, j) not in seen:
             seen.add((i, j))
             pairs.append((i, j))
-    ij = [(k, k + 1) for k in range(n - 1)] + pairs
-    ij = np.array(ij, dtype=np.uint32).reshape(-1, 2)
-    noise = normal(seed, base + 3, 6 * len(ij)).reshape(-1, 6) * np.array([0.05] * 3 + [0.01] * 3)
-    rel = compose(inverse(truth[ij[:, 0]]), truth[ij[:, 1]])
-    z = compose(rel, exp(noise))
-    init = np.empty_like(truth)
-    init[0] = truth[0]
-    for k in range(1, n):
-        init[k] = compose(init[k - 1], z[k - 1])
-    return truth, init, truth[0].copy(), ij, z
+    return pairs
 
 
 def generate(windows: int = 4096, *, min_poses: int = 20, max_poses: int = 300, loop_fraction: float = 0.1,
              seed: int = 5) -> WindowBatch:
     sizes = (min_poses + np.floor(uniform(seed, 900, windows) * (max_poses - min_poses + 1))).astype(np.int64)
-    truths, inits, priors, ijs, zs = [], [], [], [], []
-    for w in range(windows):
-        t, i, p, ij, z = _window(seed, w, int(sizes[w]), loop_fraction)
-        truths.append(t)
-        inits.append(i)
-        priors.append(p)
+    W, nmax = windows, int(sizes.max()) if windows else 0
+    scale = np.array([0.1, 0.1, 0.05, 0.02, 0.02, 0.1])
+    steps = np.zeros((W, nmax, 6))
+    start = np.zeros((W, 6))
+    ijs, noises = [], []
+    for w in range(W):
+        n = int(sizes[w])
+        base = 1000 + 16 * w
+        steps[w, :n] = normal(seed, base + 0, 6 * n).reshape(n, 6) * scale
+        steps[w, :n, 0] += 1.0
+        start[w] = normal(seed, base + 1, 6).reshape(6) * np.array([2.0, 2.0, 0.5, 0.1, 0.1, 1.0])
+        ij = np.array([(k, k + 1) for k in range(n - 1)] + _loop_pairs(seed, w, n, loop_fraction),
+                      dtype=np.uint32).reshape(-1, 2)
         ijs.append(ij)
-        zs.append(z)
+        noises.append(normal(seed, base + 3, 6 * len(ij)).reshape(-1, 6) * np.array([0.05] * 3 + [0.01] * 3))
+    # True trajectories, all windows at once (entries past a window's end are unused).
+    truth = np.zeros((W, nmax, 7))
+    truth[:, 0] = exp(start)
+    step_exp = exp(steps)
+    for k in range(1, nmax):
+        truth[:, k] = compose(truth[:, k - 1], step_exp[:, k])
     pose_offset = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
     rel_offset = np.concatenate([[0], np.cumsum([len(x) for x in ijs])]).astype(np.int64)
-    return WindowBatch(sizes, pose_offset, np.concatenate(inits), np.concatenate(truths), np.stack(priors),
-                       rel_offset, np.concatenate(ijs).astype(np.uint32), np.concatenate(zs))
+    flat_truth = np.concatenate([truth[w, :sizes[w]] for w in range(W)]) if W else np.zeros((0, 7))
+    rel_ij = np.concatenate(ijs).astype(np.uint32) if W else np.zeros((0, 2), np.uint32)
+    owner = np.repeat(np.arange(W), np.diff(rel_offset))
+    gi = pose_offset[owner] + rel_ij[:, 0]
+    gj = pose_offset[owner] + rel_ij[:, 1]
+    rel = compose(inverse(flat_truth[gi]), flat_truth[gj])
+    z = compose(rel, exp(np.concatenate(noises))) if W else np.zeros((0, 7))
+    # Dead-reckoned initial estimates: factor k of a window is odometry k -> k+1.
+    odo = np.zeros((W, max(nmax - 1, 0), 7))
+    odo[..., 0] = 1.0
+    for w in range(W):
+        n = int(sizes[w])
+        odo[w, :n - 1] = z[rel_offset[w]:rel_offset[w] + n - 1]
+    init = np.zeros((W, nmax, 7))
+    init[:, 0] = truth[:, 0]
+    for k in range(1, nmax):
+        init[:, k] = compose(init[:, k - 1], odo[:, k - 1])
+    flat_init = np.concatenate([init[w, :sizes[w]] for w in range(W)]) if W else np.zeros((0, 7))
+    return WindowBatch(sizes, pose_offset, flat_init, flat_truth, truth[:, 0].copy(), rel_offset, rel_ij, z)
 
 
 # ---------------------------------------------------------------- device solver

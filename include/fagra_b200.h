@@ -388,7 +388,7 @@ FG_API fg_status fg_windows_solve(fg_windows* batch, double* poses, const double
                                   const fg_optimize_options* options, const fg_lm_options* lm_options,
                                   fg_window_report* reports, double* prior_a, double* prior_b);
 /* The autotuner's choice (panel width 16 or 32, CTAs per SM) and its sample
- * timings in ms for {32/1, 32/2, 16/1, 16/2} (0 = not run). */
+ * timings in ms for {32/1, 32/2, 16/2, 16/3} (0 = not run or not resident). */
 FG_API fg_status fg_windows_tuning(const fg_windows* batch, int* panel, int* ctas_per_sm, double* ms4);
 FG_API fg_status fg_windows_stream(const fg_windows* batch, void** stream);
 
