@@ -11,7 +11,8 @@ package is its Python face, shaped like fagra's Rust API:
 """
 from ._lib import device_count, kernel_launches, last_error, device_stream, LIB_PATH  # noqa: F401
 from .errors import *  # noqa: F401,F403
-from .backend import Schur, Lsmr, DampedStep, SchurDiagnostics, SchurTimings, LsmrDiagnostics, LsmrTimings  # noqa: F401
+from .backend import (Schur, Lsmr, DampedStep, SchurDiagnostics, SchurTimings, LsmrDiagnostics,  # noqa: F401
+                      LsmrTimings, DenseNormalCholesky, DenseSchur, DenseQr)
 from .optimize import (LevenbergMarquardt, GaussNewton, OptimizeOptions, LmOptions, LmStatistics,  # noqa: F401
                        LmOutcome, LmWork, CallbackProblem, OptimizeReport)
 from .bal import BalProblem  # noqa: F401

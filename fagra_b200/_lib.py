@@ -229,6 +229,11 @@ SIGNATURES = {
                                    C.POINTER(WindowReportC), dptr, dptr]),
     "fg_windows_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), dptr]),
     "fg_windows_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "fg_dense_normal_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "fg_dense_schur_create": (C.c_int, [size_t, C.POINTER(size_t), size_t, C.c_int, C.POINTER(C.c_void_p)]),
+    "fg_dense_qr_create": (C.c_int, [C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
+    "fg_dense_qr_set_tolerance": (C.c_int, [C.c_void_p, C.c_double]),
+    "fg_backend_covariance": (C.c_int, [C.c_void_p, C.POINTER(size_t), size_t, C.c_double, dptr]),
     "fg_lsmr_default_options": (None, [C.POINTER(LsmrOptions)]),
     "fg_lsmr_create": (C.c_int, [C.POINTER(LsmrOptions), C.POINTER(C.c_void_p)]),
     "fg_lsmr_set_options": (C.c_int, [C.c_void_p, C.POINTER(LsmrOptions)]),

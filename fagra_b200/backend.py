@@ -393,3 +393,100 @@ def accumulate_into(handle, residual, jacobians) -> None:
         rs[k] = j2.strides[0] // 8
         cs[k] = j2.strides[1] // 8
     raise_for_status(lib.fg_backend_accumulate(handle, len(r), _dp(r), nb, cols, widths, ptrs, rs, cs))
+
+
+class _DenseBackend:
+    """Shared LeastSquaresBackend calls of the dense device backends."""
+
+    _h = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.fg_backend_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def prepare(self, dimension: int) -> None:
+        raise_for_status(lib.fg_backend_prepare(self._h, dimension))
+        self._dim = dimension
+
+    def clear(self) -> None:
+        raise_for_status(lib.fg_backend_clear(self._h))
+
+    def accumulate(self, residual, jacobians) -> None:
+        accumulate_into(self._h, residual, jacobians)
+
+    def gradient_norm(self) -> float:
+        out = C.c_double()
+        raise_for_status(lib.fg_backend_gradient_norm(self._h, C.byref(out)))
+        return out.value
+
+    def solve(self) -> np.ndarray:
+        p, n = dptr(), size_t()
+        raise_for_status(lib.fg_backend_solve(self._h, C.byref(p), C.byref(n)))
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0)
+
+    def prepare_damping(self, min_column_norm: float) -> None:
+        raise_for_status(lib.fg_backend_prepare_damping(self._h, min_column_norm))
+
+    def solve_damped(self, damping: float) -> DampedStep:
+        p, n, pred = dptr(), size_t(), C.c_double()
+        raise_for_status(lib.fg_backend_solve_damped(self._h, damping, C.byref(p), C.byref(n), C.byref(pred)))
+        delta = np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0)
+        return DampedStep(delta, pred.value)
+
+    def covariance(self, columns, relative_pivot_tolerance: float = 64 * np.finfo(float).eps) -> np.ndarray:
+        """Selected inverse information in selection order (src/covariance.rs:225-255)."""
+        cols = (size_t * max(len(columns), 1))(*[int(c) for c in columns])
+        k = len(columns)
+        out = np.zeros(max(k * k, 1))
+        raise_for_status(lib.fg_backend_covariance(self._h, cols, k, relative_pivot_tolerance, _dp(out)))
+        return out[:k * k].reshape(k, k).T.copy()
+
+
+class DenseNormalCholesky(_DenseBackend):
+    """Device DenseNormalCholesky (src/normal.rs)."""
+
+    def __init__(self, *, device: int = 0):
+        h = C.c_void_p()
+        raise_for_status(lib.fg_dense_normal_create(device, C.byref(h)))
+        self._h = h
+
+
+class DenseSchur(_DenseBackend):
+    """Device DenseSchur (src/dense_schur.rs): retained prefix + landmark widths."""
+
+    def __init__(self, retained_dimension: int, eliminated_widths=(), *, device: int = 0):
+        w = (size_t * max(len(eliminated_widths), 1))(*[int(x) for x in eliminated_widths])
+        h = C.c_void_p()
+        raise_for_status(lib.fg_dense_schur_create(retained_dimension, w, len(eliminated_widths), device,
+                                                   C.byref(h)))
+        self._h = h
+
+
+class DenseQr(_DenseBackend):
+    """Device DenseQr (src/qr.rs)."""
+
+    def __init__(self, relative_rank_tolerance: float = 64 * np.finfo(float).eps, *, device: int = 0):
+        h = C.c_void_p()
+        raise_for_status(lib.fg_dense_qr_create(relative_rank_tolerance, device, C.byref(h)))
+        self._h = h
+        self._tol = relative_rank_tolerance
+
+    @property
+    def relative_rank_tolerance(self):
+        return self._tol
+
+    @relative_rank_tolerance.setter
+    def relative_rank_tolerance(self, v):
+        raise_for_status(lib.fg_dense_qr_set_tolerance(self._h, v))
+        self._tol = v

@@ -340,6 +340,28 @@ FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size
  * (0 if not measured). */
 FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds2);
 
+/* ---- Dense direct backends on the same LeastSquaresBackend entry points ----
+ * fg_backend_prepare / clear / accumulate / gradient_norm / prepare_damping /
+ * solve_damped / solve and fg_backend_destroy drive them like the sparse
+ * backends. Systems are factored by one thread block: they are meant for
+ * bounded windows (a few thousand coordinates), as in the reference. */
+/* DenseNormalCholesky::default (src/normal.rs:22-63); solve() factors in place
+ * (a later prepare_damping needs a fresh model, normal.rs:154-160). */
+FG_API fg_status fg_dense_normal_create(int device, fg_backend** out);
+/* DenseSchur::new(retained_dimension, eliminated_widths) (src/dense_schur.rs:63-90) */
+FG_API fg_status fg_dense_schur_create(size_t retained_dimension, const size_t* eliminated_widths,
+                                       size_t count, int device, fg_backend** out);
+/* DenseQr { relative_rank_tolerance, .. } (src/qr.rs:24-63) */
+FG_API fg_status fg_dense_qr_create(double relative_rank_tolerance, int device, fg_backend** out);
+FG_API fg_status fg_dense_qr_set_tolerance(fg_backend* backend, double relative_rank_tolerance);
+/* CovarianceBackend::covariance (src/covariance.rs:263-270) + SelectedCovariance
+ * (:225-255) for a dense backend's current model: out (k x k, column-major) =
+ * the selected block of the undamped inverse information, columns in
+ * selection order; relative_pivot_tolerance is CovarianceOptions'
+ * (default 64 eps). DenseSchur accepts retained columns only. */
+FG_API fg_status fg_backend_covariance(fg_backend* backend, const size_t* columns, size_t k,
+                                       double relative_pivot_tolerance, double* out);
+
 /* ---- Batched pose-graph windows ----------------------------------------
  * Thousands of independent SE(3) windows of uneven size solved in one
  * persistent launch. Window w owns poses [pose_offset[w], pose_offset[w+1])
