@@ -45,6 +45,11 @@ def parse():
     ap.add_argument("--forms", default="fast,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows"],
+                    help="ba: Schur-PCG time to cost (default); lsmr: the same with the LSMR backend; "
+                         "windows: the batched pose-graph windows")
+    ap.add_argument("--windows", type=int, default=4096)
+    ap.add_argument("--max-poses", type=int, default=300)
     return ap.parse_args()
 
 
@@ -264,8 +269,155 @@ def run_gpu(args, rank: int, world: int, device: int):
     return data, g, results, head, clocks_info, launches, e2e
 
 
+def run_windows(args, device: int) -> dict:
+    """Batched SE(3) pose-graph windows: every window solved by LM over an
+    all-retained dense Schur system, then its oldest 10 poses eliminated."""
+    import numpy as np
+    import torch
+    import fagra_b200 as fg
+    from fagra_b200 import posegraph
+    torch.cuda.set_device(device)
+    batch = posegraph.generate(args.windows, max_poses=args.max_poses)
+    solver = posegraph.WindowSolver(batch, removed=10, precision="f64", device=device)
+    stream = torch.cuda.ExternalStream(solver.stream(), device=device)
+    for _ in range(args.warmup):
+        solver.upload()
+        solver.run()
+    torch.cuda.synchronize(device)
+    clk = Clocks(device)
+    l0 = fg.kernel_launches()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    times = []
+    for _ in range(args.steps):
+        solver.upload()
+        ev[0].record(stream)
+        solver.run()
+        ev[1].record(stream)
+        torch.cuda.synchronize(device)
+        times.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+    launches = (fg.kernel_launches() - l0) // args.steps
+    clocks = clk.stop()
+    poses, reps, a, b = solver.download()
+    attempts = np.array([r.attempts for r in reps], dtype=np.float64)
+    n6 = 6.0 * batch.sizes.astype(np.float64)
+    dense_flops = float(np.sum(attempts * n6 ** 3 / 3.0))
+    value = statistics.median(times)
+    # e2e: host arrays in, host results out, through fg_windows_solve
+    e2e_times = []
+    h2d = batch.poses.nbytes + batch.prior.nbytes + batch.rel_z.nbytes
+    d2h = batch.poses.nbytes + len(reps) * 160 + 8 * int(solver.a_offset[-1]) + 48 * int(solver.separator_offset[-1])
+    if not args.no_e2e:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            solver.solve()
+            e2e_times.append(time.perf_counter() - t0)
+    status = np.bincount([r.status for r in reps], minlength=11).tolist()
+    line = dict(metric=f"pose-graph windows solved ({args.windows} windows, LM + marginalization)", value=value,
+                unit="s", n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=value * 1e3,
+                higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                config=dict(workload=f"{args.windows} SE(3) windows of 20-{args.max_poses} poses ({len(batch.poses)} poses, "
+                                     f"{len(batch.rel_ij)} relative factors), odometry + 10% loop closures, anchor "
+                                     f"prior; LM (20 iterations, gradient tolerance 1e-6) over a dense Schur system, "
+                                     f"then square-root elimination of the oldest 10 poses",
+                            tuning=dict(zip(("panel", "ctas_per_sm"), solver.tuning()[:2])),
+                            l2="per-window working sets are reused from L2; the batch (63 MB of poses and "
+                               "factors, 2.3 GB of per-CTA dense workspace) exceeds it"),
+                lm_trials=int(attempts.sum()), window_status=status,
+                dense_equivalent_tflops=dense_flops / value / 1e12,
+                roofline=dict(bound="fp64", achieved=dense_flops / value / 1e12, peak=37.0, unit="TFLOP/s",
+                              peak_source="nominal B200 FP64 (no measured FP64 peak in MEASURED_PEAKS.json)",
+                              frac=dense_flops / value / 1e12 / 37.0,
+                              note="dense-equivalent Cholesky FLOP (attempts x (6n)^3/3); the kernel skips "
+                                   "exact-zero envelope tiles, so executed FLOP are fewer", traffic=None),
+                clocks=clocks, gpu_launches=launches,
+                e2e=dict(value=statistics.median(e2e_times) if e2e_times else None, unit="s",
+                         h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h))
+    if not args.no_cpu_baseline:
+        import oracle
+        # bounded sample: the smallest windows up to ~20 s of oracle time, scaled by
+        # (attempts x n^3) to the whole batch
+        order = np.argsort(batch.sizes)
+        done, t_cpu, work = 0, 0.0, 0.0
+        for w in order[::max(1, len(order) // 64)]:
+            poses_w, prior, ij, z = batch.window(int(w))
+            t0 = time.perf_counter()
+            ref = oracle.window_solve(poses_w, prior, ij, z, removed=10, **posegraph.WINDOW_OPTIONS)
+            t_cpu += time.perf_counter() - t0
+            work += ref["stats"].attempts * (6.0 * len(poses_w)) ** 3
+            done += 1
+            if t_cpu > 20:
+                break
+        total_work = float(np.sum(attempts * n6 ** 3))
+        v = t_cpu * total_work / work
+        line["cpu_baseline"] = dict(value=v, unit="s", cores=1, kind="port",
+                                    sample=f"{done} windows of the batch solved by the oracle in {t_cpu:.1f} s, "
+                                           f"scaled by attempts x (6n)^3 to the batch")
+    return line
+
+
+def run_lsmr(args, device: int) -> dict:
+    """BAL time to cost with the LSMR backend (block-Jacobi, f64 and f32 storage)."""
+    import numpy as np
+    import torch
+    import ctypes as C
+    import fagra_b200 as fg
+    from fagra_b200 import synthetic, _lib
+    torch.cuda.set_device(device)
+    stream = torch.cuda.ExternalStream(fg.device_stream(device), device=device)
+    g = gold(args.workload)
+    target = g["final_cost"] * (1 + REL)
+    data = synthetic.generate(args.workload)
+    problem = fg.BalProblem.from_data(data, device=device)
+    res = {}
+    for prec in ("f64", "f32"):
+        b = fg.Lsmr(precision=prec, device=device)
+        b.block_preconditioning = True
+        b.relative_tolerance = 1e-10
+        b.max_iterations = 100000
+        oo, lmo = fg.OptimizeOptions(50, 1e-8, 0.0, 0.0).c(), fg.LmOptions().c()
+
+        def step():
+            _lib.lib.fg_bal_restore_initial(problem._bal_handle)
+            rep, st = _lib.ReportC(), _lib.LmStatisticsC()
+            code = _lib.lib.fg_lm_solve_bal_to_cost(b.handle, problem._bal_handle, C.byref(oo), C.byref(lmo),
+                                                    target, C.byref(rep), C.byref(st))
+            return rep, st
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(device)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            rep, st = step()
+        ev[1].record(stream)
+        torch.cuda.synchronize(device)
+        secs = ev[0].elapsed_time(ev[1]) * 1e-3 / args.steps
+        problem.linearize(b)
+        b.prepare_damping(1e-6)
+        it_s, it_b = b.time_iteration(1e-3, 256)
+        res[prec] = dict(seconds=secs, reached_target=rep.termination == 5, lsmr_iterations=st.linear_iterations,
+                         final_cost=st.cost, iteration_seconds=it_s, iteration_bytes=it_b)
+    pk, src = peaks()
+    head = res["f64"]
+    ach = head["iteration_bytes"] / head["iteration_seconds"] / 1e9
+    return dict(metric=f"BA time to 1e-6 relative cost with block-Jacobi LSMR ({args.workload})",
+                value=head["seconds"], unit="s", n_gpus=1, steps=args.steps, warmup=args.warmup,
+                ms_per_step=head["seconds"] * 1e3, higher_is_better=False, scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic", config=dict(workload=args.workload, form="lsmr block-Jacobi f64"),
+                forms=res, roofline=dict(bound="hbm", kernel="LSMR iteration (k_lsmr_rows + k_lsmr_segments + "
+                                         "k_lsmr_update)", achieved=ach, peak=pk, peak_source=src, unit="GB/s",
+                                         frac=ach / pk, traffic=None), e2e=None)
+
+
 def main():
     args = parse()
+    if args.suite != "ba" and args.impl != "reference":
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        line = run_windows(args, local) if args.suite == "windows" else run_lsmr(args, local)
+        print(json.dumps(line), flush=True)
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
