@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
     ap.add_argument("--workload", default="bal1k")
-    ap.add_argument("--forms", default="fast,f64")
+    ap.add_argument("--forms", default="learned,fast,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows"],
@@ -150,6 +150,22 @@ class Clocks:
                     samples=len(sm))
 
 
+def train_network(fg, synthetic, workload: str, device: int, problems: int = 2) -> tuple:
+    """Learned preconditioner trained (untimed) on reduced camera systems of LM
+    runs over problems of the workload's shape with other seeds."""
+    net = fg.LearnedPreconditioner(seed=7, device=device)
+    t0 = time.perf_counter()
+    for k in range(problems):
+        d = synthetic.generate(workload, seed=200 + k)
+        be = fg.Schur(9 * d.num_cameras, 9, 3, precision="f32", device=device)
+        net.collect(fg.BalProblem.from_data(d, device=device), be, fg.OptimizeOptions(max_iterations=4), probes=8,
+                    seed=1000 * k)
+    before = net.mean_loss()
+    net.train(steps=400, learning_rate=1e-3)
+    return net, dict(systems=net.system_count(), loss_before=before, loss_after=net.mean_loss(),
+                     train_seconds=time.perf_counter() - t0, training_problems=f"{problems} x {workload} seeds 200+")
+
+
 def run_gpu(args, rank: int, world: int, device: int):
     import numpy as np
     import torch
@@ -174,7 +190,8 @@ def run_gpu(args, rank: int, world: int, device: int):
     opts = fg.OptimizeOptions(50, 1e-8, 0.0, 0.0)
     # fast: FP32 bulk + FP64 residual replacement, CG tolerance 1e-8 (the per-step
     # linear-residual bar); f64: fagra's Schur arithmetic and default tolerance.
-    forms = {"fast": dict(precision="f32", preconditioner="retained_blocks", tol=1e-8),
+    forms = {"learned": dict(precision="f32", preconditioner="learned", tol=1e-8),
+             "fast": dict(precision="f32", preconditioner="retained_blocks", tol=1e-8),
              "f64": dict(precision="f64", preconditioner="retained_blocks", tol=1e-10),
              "f32": dict(precision="f32", preconditioner="retained_blocks", tol=1e-10),
              "f64sd": dict(precision="f64", preconditioner="schur_diagonal", tol=1e-10),
@@ -192,6 +209,20 @@ def run_gpu(args, rank: int, world: int, device: int):
         kw["relative_tolerance"] = tol
         lmo = fg.LmOptions().c()
         oo = opts.c()
+        learned_info = None
+        if kw["preconditioner"] == "learned":
+            net, learned_info = train_network(fg, synthetic, args.workload, device)
+            backend.attach_learned(net)
+            # the one-time block-Jacobi comparison, on the first LM system (untimed)
+            _lib.lib.fg_bal_restore_initial(problem._bal_handle)
+            backend.prepare(problem.dimension())
+            problem.linearize(backend)
+            backend.prepare_damping(lmo.min_column_norm)
+            backend.solve_damped(lmo.initial_damping)
+            di = backend.diagnostics()
+            learned_info["comparison"] = dict(damping=lmo.initial_damping, learned_iterations=di.learned_iterations,
+                                              block_jacobi_iterations=di.block_jacobi_iterations,
+                                              kept=di.preconditioner_used)
 
         def step():
             _lib.lib.fg_bal_restore_initial(problem._bal_handle)
@@ -224,6 +255,8 @@ def run_gpu(args, rank: int, world: int, device: int):
                              linearizations=per[-1]["lin"], accepted=per[-1]["accepted"],
                              rejected=per[-1]["rejected"], final_cost=per[-1]["cost"],
                              rel_cost_error=(per[-1]["cost"] - g["final_cost"]) / g["final_cost"], **kw)
+        if learned_info:
+            results[name]["network"] = learned_info
         if name == head:
             # roofline of the dominant kernel: the reduced-operator application
             problem.linearize(backend)

@@ -16,5 +16,6 @@ from .backend import (Schur, Lsmr, DampedStep, SchurDiagnostics, SchurTimings, L
 from .optimize import (LevenbergMarquardt, GaussNewton, OptimizeOptions, LmOptions, LmStatistics,  # noqa: F401
                        LmOutcome, LmWork, CallbackProblem, OptimizeReport)
 from .bal import BalProblem  # noqa: F401
+from .learned import LearnedPreconditioner  # noqa: F401
 
 __version__ = "0.1.0"

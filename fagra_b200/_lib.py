@@ -43,6 +43,10 @@ class SchurDiagnosticsC(C.Structure):
         ("has_scaled", C.c_int),
         ("has_original", C.c_int),
         ("refinements", size_t),
+        ("preconditioner_used", C.c_int),
+        ("learned_fallback", C.c_int),
+        ("learned_iterations", size_t),
+        ("block_jacobi_iterations", size_t),
     ]
 
 
@@ -241,6 +245,22 @@ SIGNATURES = {
     "fg_lsmr_get_timings": (C.c_int, [C.c_void_p, C.POINTER(LsmrTimingsC)]),
     "fg_lsmr_damped_products": (C.c_int, [C.c_void_p, C.c_double, C.c_int, dptr, dptr, dptr, dptr]),
     "fg_lsmr_time_iteration": (C.c_int, [C.c_void_p, C.c_double, size_t, dptr, dptr]),
+    "fg_gnn_create": (C.c_int, [C.c_uint64, C.c_int, C.POINTER(C.c_void_p)]),
+    "fg_gnn_destroy": (None, [C.c_void_p]),
+    "fg_gnn_parameter_count": (C.c_int, [C.c_void_p, C.POINTER(size_t)]),
+    "fg_gnn_get_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "fg_gnn_set_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "fg_schur_capture_system": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, size_t, C.c_uint64, C.c_int,
+                                          C.POINTER(size_t)]),
+    "fg_gnn_import_system": (C.c_int, [C.c_void_p, size_t, size_t, size_t, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                       C.POINTER(C.c_uint8), C.POINTER(size_t)]),
+    "fg_gnn_system_count": (C.c_int, [C.c_void_p, C.POINTER(size_t)]),
+    "fg_gnn_system_size": (C.c_int, [C.c_void_p, size_t, C.POINTER(size_t), C.POINTER(size_t), C.POINTER(size_t)]),
+    "fg_gnn_export_system": (C.c_int, [C.c_void_p, size_t, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_uint8), dptr]),
+    "fg_gnn_clear_systems": (C.c_int, [C.c_void_p]),
+    "fg_gnn_evaluate": (C.c_int, [C.c_void_p, size_t, dptr, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "fg_gnn_train": (C.c_int, [C.c_void_p, size_t, C.c_double, dptr]),
+    "fg_schur_attach_learned": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 
 

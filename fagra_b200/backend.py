@@ -19,7 +19,7 @@ from .errors import raise_for_status
 
 TERMINATIONS = {0: None, 1: "Converged", 2: "IterationLimit", 3: "NotPositiveDefinite", 4: "NonFinite"}
 PRECISIONS = {"f64": 0, "f32": 1}
-PRECONDITIONERS = {"retained_blocks": 0, "schur_diagonal": 1}
+PRECONDITIONERS = {"retained_blocks": 0, "schur_diagonal": 1, "learned": 2}
 
 
 @dataclass
@@ -45,6 +45,12 @@ class SchurDiagnostics:
     scaled_relative_residual: Optional[float]
     original_relative_residual: Optional[float]
     refinements: int
+    # learned preconditioner only: the preconditioner whose step was kept, the
+    # fallback taken (None, "failed", "more_iterations") and both solves' counts
+    preconditioner_used: str = "retained_blocks"
+    learned_fallback: Optional[str] = None
+    learned_iterations: int = 0
+    block_jacobi_iterations: int = 0
 
 
 @dataclass
@@ -102,6 +108,12 @@ class Schur:
     @property
     def handle(self):
         return self._h
+
+    def attach_learned(self, network) -> None:
+        """Attach (None: detach) the network used by preconditioner="learned".
+        Re-arms the one-time block-Jacobi comparison."""
+        raise_for_status(lib.fg_schur_attach_learned(self._h, network.handle if network is not None else None))
+        self._learned = network  # the backend holds a pointer: keep the network alive
 
     def close(self):
         if getattr(self, "_h", None):
@@ -162,7 +174,10 @@ class Schur:
                                 opt(d.has_estimated, d.estimated_relative_residual),
                                 opt(d.has_reduced, d.reduced_relative_residual),
                                 opt(d.has_scaled, d.scaled_relative_residual),
-                                opt(d.has_original, d.original_relative_residual), d.refinements)
+                                opt(d.has_original, d.original_relative_residual), d.refinements,
+                                {v: k for k, v in PRECONDITIONERS.items()}[d.preconditioner_used],
+                                (None, "failed", "more_iterations")[d.learned_fallback], d.learned_iterations,
+                                d.block_jacobi_iterations)
 
     def timings(self) -> SchurTimings:
         t = _lib.SchurTimingsC()

@@ -342,6 +342,18 @@ FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* sec
   b->impl->operator_info(variant, seconds2);
   return FG_OK;
 }
+FG_API fg_status fg_schur_attach_learned(fg_backend* b, fg_gnn* g) {
+  FG_NEED(b);
+  FG_GUARD_BEGIN return b->impl->attach_learned(g);
+  FG_GUARD_END
+}
+FG_API fg_status fg_schur_capture_system(fg_backend* b, fg_gnn* g, double lambda, size_t probes, uint64_t seed,
+                                         int kind, size_t* index) {
+  FG_NEED(b);
+  if (!g || !index) return FG_NULL_ARGUMENT;
+  FG_GUARD_BEGIN return b->impl->capture_system(g, lambda, probes, seed, kind, index);
+  FG_GUARD_END
+}
 FG_API fg_status fg_gn_solve_bal(fg_backend* b, fg_bal_problem* p, const fg_optimize_options* o,
                                  fg_optimize_report* rep) {
   FG_NEED(b);

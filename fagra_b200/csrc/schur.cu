@@ -5,6 +5,7 @@
 #include "camside.cuh"
 #include "fastpath.cuh"
 #include "setup.cuh"
+#include "gnn.cuh"
 #include <algorithm>
 #include <numeric>
 
@@ -91,6 +92,12 @@ class SchurImpl final : public Backend {
   HBuf<VerifyState> h_ver;
   HBuf<unsigned> h_count;
   FastPath<TS> fast;  // specialized BAL (9,3) single-pass reduced operator
+  // learned preconditioner (FG_PRECOND_LEARNED): the attached network, whether
+  // the one-time block-Jacobi comparison has run, and whether it switched the
+  // network off for this backend
+  fg_gnn* learned = nullptr;
+  bool learned_compared = false, learned_off = false;
+  DBuf<double> d_keep;  // the learned solution while the comparison solve runs
 
   Layout layout() const {
     Layout L;
@@ -129,6 +136,11 @@ class SchurImpl final : public Backend {
   // ------------------------------------------------------------------ trait
   int kind() const override { return 0; }
   fg_status set_options(const fg_schur_options& o) override {
+    if (o.preconditioner < FG_PRECOND_RETAINED_BLOCKS || o.preconditioner > FG_PRECOND_LEARNED) {
+      set_error("unknown preconditioner");
+      return FG_INVALID_OPTIONS;
+    }
+    if (o.preconditioner != opt.preconditioner) learned_compared = learned_off = false;
     int keep = dev;
     opt = o;
     opt.device = keep;
@@ -405,7 +417,7 @@ class SchurImpl final : public Backend {
       if (fast.ready_for(*this)) {
         // the reference-layout cross array is only needed by the generic
         // right-hand side / back-substitution and the Schur-diagonal factor
-        cross_current = !pure_pairs || opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL;
+        cross_current = !pure_pairs || opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL || learned_active();
         FG_LAUNCH(k_edge_records2<TS>, grid_for(nedges, REC_T), REC_T, 0, st, (int64_t)nedges, d_pt_edge.get(),
                   d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), fast.d_lp.get(), fast.d_erec.get(),
                   cross_current ? d_cross.get() : (TS*)nullptr, bad + 1);
@@ -432,8 +444,38 @@ class SchurImpl final : public Backend {
     return FG_OK;
   }
 
-  // Factor B and C blocks (+ the optional S_cc preconditioner) for lambda.
-  fg_status factor(double lambda, unsigned* fallbacks) {
+  bool learned_active() const {
+    return opt.preconditioner == FG_PRECOND_LEARNED && learned != nullptr && !learned_off;
+  }
+  SchurView view_at(double lambda) const {
+    SchurView v;
+    v.L = layout();
+    v.factors = d_factors.get();
+    v.cross = d_cross.get();
+    v.f64 = std::is_same<TS, double>::value;
+    v.edges = d_edges.get();
+    v.nedges = (int64_t)nedges;
+    v.pt_edge_off = d_pt_edge_off.get();
+    v.pt_edge = d_pt_edge.get();
+    v.cam_edge_off = d_cam_edge_off.get();
+    v.cam_edge = d_cam_edge.get();
+    v.observed = d_observed.get();
+    v.lambda = lambda;
+    return v;
+  }
+  // Explicit block-Jacobi (or Schur-diagonal) inverses into d_minv.
+  fg_status write_block_inverses(double lambda) {
+    Layout L = layout();
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      FG_LAUNCH((k_precond_inverse<CW_, TS>), grid_for(nC, 64), 64, 0, st, L, d_observed.get(), precond_factors(),
+                lambda, d_minv.get());
+    });
+    return FG_OK;
+  }
+
+  // Factor B and C blocks (+ the optional S_cc preconditioner) for lambda;
+  // with `learned_blocks` the attached network then reshapes the inverses.
+  fg_status factor(double lambda, unsigned* fallbacks, bool learned_blocks = false) {
     Layout L = layout();
     FG_CUDA(cudaMemsetAsync(d_counters.get() + 4, 0, sizeof(unsigned), st));
     FG_DISPATCH_WIDTHS(cw, pw, {
@@ -453,14 +495,69 @@ class SchurImpl final : public Backend {
                   d_precond.get(), lambda);
       });
     }
-    if (*fallbacks == 0 && nC) {
-      FG_DISPATCH_WIDTHS(cw, pw, {
-        FG_LAUNCH((k_precond_inverse<CW_, TS>), grid_for(nC, 64), 64, 0, st, L, d_observed.get(), precond_factors(),
-                  lambda, d_minv.get());
-      });
+    if (*fallbacks == 0 && nC) FG_TRY(write_block_inverses(lambda));
+    if (*fallbacks == 0 && nC && learned_blocks) {
+      FG_TRY(ensure_cross());
+      unsigned nonfinite = 0;
+      FG_TRY(gnn_precondition(learned, view_at(lambda), d_minv.get(), st, &nonfinite));
     }
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
     return FG_OK;
+  }
+
+  fg_status attach_learned(fg_gnn* g) override {
+    if (g) FG_TRY(gnn_check(g, cw, pw, retained / cw, dev));
+    learned = g;
+    learned_compared = learned_off = false;
+    return FG_OK;
+  }
+
+  fg_status capture_system(fg_gnn* g, double lambda, size_t probes, uint64_t seed, int kind,
+                           size_t* index) override {
+    if (kind != 0 && kind != 1) {
+      set_error("probe kind must be 0 (products) or 1 (solves)");
+      return FG_INVALID_OPTIONS;
+    }
+    if (!ready || !std::isfinite(lambda) || lambda < 0) {
+      set_error("capturing a reduced system requires prepare_damping and a finite nonnegative lambda");
+      return FG_INVALID_OPTIONS;
+    }
+    FG_TRY(gnn_check(g, cw, pw, nC, dev));
+    unsigned fb = 0;
+    FG_TRY(factor(lambda, &fb));
+    if (fb) {
+      set_error("local block factorization failed");
+      return FG_LINEAR_SOLVE_FAILED;
+    }
+    FG_TRY(ensure_cross());
+    auto apply = [&](const double* x, double* y) -> fg_status {
+      PView<double> pv{const_cast<double*>(x), nullptr, nullptr};
+      FG_TRY(apply_reduced<double>(pv, lambda, lambda, true, d_tmpd.get(), y, nullptr, nullptr));
+      return FG_OK;
+    };
+    // S^-1 through the block-Jacobi PCG at the backend's tolerance; the work
+    // counters and diagnostics of the caller's solves are left untouched
+    auto solve = [&](const double* x, double* y) -> fg_status {
+      FG_CUDA(cudaMemcpyAsync(d_rhs.get(), x, retained * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      const size_t keep_iterations = iterations;
+      const fg_schur_diagnostics keep_diag = diag;
+      unsigned its = 0;
+      int term = FG_TERM_NONE;
+      double est = 0;
+      size_t ref = 0;
+      fg_status s = run_cg(lambda, &its, &term, &est, &ref);
+      iterations = keep_iterations;
+      diag = keep_diag;
+      FG_TRY(s);
+      if (term != FG_TERM_CONVERGED) {
+        set_error("reduced CG did not converge on a probe");
+        return FG_LINEAR_SOLVE_FAILED;
+      }
+      FG_CUDA(cudaMemcpyAsync(y, d_zred.get(), retained * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      return FG_OK;
+    };
+    if (kind == 1) return gnn_capture(g, view_at(lambda), probes, seed, 1, solve, d_work.get(), d_qd.get(), st, index);
+    return gnn_capture(g, view_at(lambda), probes, seed, 0, apply, d_work.get(), d_qd.get(), st, index);
   }
   // Operator autotuner: times each FP32 single-pass variant (TMA-staged
   // stages, direct global loads) on this structure and keeps the faster one.
@@ -672,7 +769,8 @@ class SchurImpl final : public Backend {
     EventTimer tf, tl, tv;
     if (opt.collect_timings) tf.start(st);
     unsigned fallbacks = 0;
-    FG_TRY(factor(lambda, &fallbacks));
+    const bool use_learned = learned_active();
+    FG_TRY(factor(lambda, &fallbacks, use_learned));
     if (fallbacks) {  // src/schur.rs:209-215
       if (opt.collect_timings) tim.factorization += tf.stop(st);
       diag.termination = FG_TERM_NOT_POSITIVE_DEFINITE;
@@ -690,13 +788,48 @@ class SchurImpl final : public Backend {
     int term = FG_TERM_NONE;
     double est = 0;
     size_t refinements = 0;
-    if (std::is_same<TS, double>::value) {
-      FG_TRY(pcg(d_rhs.get(), lambda, opt.relative_tolerance, opt.max_iterations, &its, &term, &est));
-      FG_TRY(launch_widen(d_x.get(), d_zred.get(), retained));
-      iterations += its;
-      diag.iterations = its;
-    } else {
-      FG_TRY(refine(lambda, &its, &term, &est, &refinements));
+    FG_TRY(run_cg(lambda, &its, &term, &est, &refinements));
+    diag.preconditioner_used = use_learned ? FG_PRECOND_LEARNED : opt.preconditioner;
+    if (use_learned) {
+      // Block-Jacobi stays the judge: it takes over when the learned PCG
+      // fails, and the first learned solve is compared against it once.
+      diag.learned_iterations = its;
+      const bool compare = !learned_compared;
+      if (term != FG_TERM_CONVERGED || compare) {
+        const bool keep = term == FG_TERM_CONVERGED;
+        if (keep) {
+          FG_TRY(d_keep.resize(std::max<size_t>(retained, 1)));
+          FG_CUDA(cudaMemcpyAsync(d_keep.get(), d_zred.get(), retained * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        }
+        FG_TRY(write_block_inverses(lambda));
+        unsigned its2 = 0;
+        int term2 = FG_TERM_NONE;
+        double est2 = 0;
+        size_t ref2 = 0;
+        FG_TRY(run_cg(lambda, &its2, &term2, &est2, &ref2));
+        diag.block_jacobi_iterations = its2;
+        if (!keep) {
+          diag.learned_fallback = 1;
+        } else {
+          learned_compared = true;
+          if (term2 == FG_TERM_CONVERGED && its2 < its) {
+            learned_off = true;
+            diag.learned_fallback = 2;
+          } else {
+            FG_CUDA(cudaMemcpyAsync(d_zred.get(), d_keep.get(), retained * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    st));
+            term2 = term;
+            est2 = est;
+            ref2 = refinements;
+          }
+        }
+        if (diag.learned_fallback) diag.preconditioner_used = FG_PRECOND_RETAINED_BLOCKS;
+        term = term2;
+        est = est2;
+        refinements += ref2;
+        its += its2;
+        diag.iterations = its;
+      }
     }
     diag.termination = term;
     diag.refinements = refinements;
@@ -721,6 +854,19 @@ class SchurImpl final : public Backend {
     }
     *predicted = pred;
     return FG_OK;
+  }
+
+  // One reduced solve with the inverses currently in d_minv; the solution
+  // lands in d_zred (f64).
+  fg_status run_cg(double lambda, unsigned* its, int* term, double* est, size_t* refinements) {
+    if (std::is_same<TS, double>::value) {
+      FG_TRY(pcg(d_rhs.get(), lambda, opt.relative_tolerance, opt.max_iterations, its, term, est));
+      FG_TRY(launch_widen(d_x.get(), d_zred.get(), retained));
+      iterations += *its;
+      diag.iterations = *its;
+      return FG_OK;
+    }
+    return refine(lambda, its, term, est, refinements);
   }
 
   // FP32 PCG with FP64 residual replacement (reliable updates): the Krylov

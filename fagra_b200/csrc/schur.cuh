@@ -83,6 +83,8 @@ class Backend {
   virtual fg_status export_model(double*, double*, double*, double*, double*, double*) { return not_schur(); }
   virtual fg_status reduced_apply(double, const double*, double*) { return not_schur(); }
   virtual fg_status time_operator(double, size_t, double*, double*) { return not_schur(); }
+  virtual fg_status attach_learned(fg_gnn*) { return not_schur(); }
+  virtual fg_status capture_system(fg_gnn*, double, size_t, uint64_t, int, size_t*) { return not_schur(); }
   virtual void operator_info(int* variant, double* seconds2) const {
     *variant = 0;
     if (seconds2) seconds2[0] = seconds2[1] = 0;

@@ -69,7 +69,9 @@ typedef enum {
 
 typedef enum {
   FG_PRECOND_RETAINED_BLOCKS = 0, /* (B + lambda I) block-Jacobi, src/schur.rs:658-682 */
-  FG_PRECOND_SCHUR_DIAGONAL = 1   /* exact 9x9 diagonal blocks of S (docs/schur-performance.md:155-159) */
+  FG_PRECOND_SCHUR_DIAGONAL = 1,  /* exact 9x9 diagonal blocks of S (docs/schur-performance.md:155-159) */
+  FG_PRECOND_LEARNED = 2          /* block-Jacobi reshaped by an attached fg_gnn, block-Jacobi fallback;
+                                     no reference counterpart */
 } fg_preconditioner;
 
 /* src/schur.rs:116-143 public fields, plus device-side choices. */
@@ -95,6 +97,14 @@ typedef struct {
   double original_relative_residual;
   int has_estimated, has_reduced, has_scaled, has_original;
   size_t refinements; /* FP32 mode: FP64 residual replacements in this attempt */
+  /* FG_PRECOND_LEARNED only (no reference counterpart): the preconditioner
+   * whose step was kept, 0 when the learned PCG ran without a fallback, 1
+   * when it met non-positive curvature or did not converge, 2 when the
+   * block-Jacobi comparison solve needed fewer iterations (the learned
+   * preconditioner is then switched off for this backend); iteration counts
+   * of the two solves of this attempt (0 when not run). `iterations` is their sum. */
+  int preconditioner_used, learned_fallback;
+  size_t learned_iterations, block_jacobi_iterations;
 } fg_schur_diagnostics;
 
 /* src/schur.rs:75-91 SchurTimings, seconds, device event time. */
@@ -104,6 +114,7 @@ typedef struct {
 
 typedef struct fg_backend fg_backend;
 typedef struct fg_bal_problem fg_bal_problem;
+typedef struct fg_gnn fg_gnn;
 
 /* ---- library ---------------------------------------------------------- */
 FG_API const char* fg_version(void);
@@ -339,6 +350,60 @@ FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size
  * single pass; seconds[v-1] = measured time per application of variant v
  * (0 if not measured). */
 FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds2);
+
+/* ---- Learned preconditioner (no reference counterpart) ----------------------
+ * A message-passing network over the camera covisibility graph of the reduced
+ * camera system. Per retained variable c it emits A_c = I + 0.1 tril(O_c) and
+ * the preconditioner block M_c = L_c^-T (A_c A_c^T + 1e-3 I) L_c^-1, where
+ * L_c L_c^T = B_c + lambda I is the block-Jacobi factor of src/schur.rs:658-682,
+ * so M is SPD and an untrained network (zero output layer) is block-Jacobi.
+ * Node features: P_c = L_c^-1 (sum_e E_e C_p^-1 E_e^T) L_c^-T (45 entries),
+ * degree, coupling, log10(lambda), trace(P_c); covisibility weights
+ * s_ij = sqrt(sum_shared p ||G_ip G_jp^T||_F^2), G_e = L_c^-1 E_e L_p^-T,
+ * row-normalized. Three layers h_l = h_{l-1} + relu([h_{l-1}, A h_{l-1}] W_l + b_l),
+ * hidden width 64; BF16 weights and operands, FP32 accumulation (tensor cores).
+ * Training systems are reduced camera systems of an attached Schur backend;
+ * the loss is mean ||x - M_hat S_hat x||^2 over Gaussian whitened probes x.
+ * Supports retained widths <= 9, eliminated widths <= 4, <= 16384 retained
+ * variables. Handles are not thread safe. */
+FG_API fg_status fg_gnn_create(uint64_t seed, int device, fg_gnn** out);
+FG_API void fg_gnn_destroy(fg_gnn* gnn);
+/* Parameters are FP32 masters, flat: W_in (64x64, row = input), b_in (64),
+ * {W_l (128x64), b_l (64)} for l = 1..3, W_out (64x64), b_out (64). */
+FG_API fg_status fg_gnn_parameter_count(const fg_gnn* gnn, size_t* count);
+FG_API fg_status fg_gnn_get_parameters(fg_gnn* gnn, float* out);
+/* Replaces the parameters and resets the Adam state. */
+FG_API fg_status fg_gnn_set_parameters(fg_gnn* gnn, const float* parameters);
+/* Captures the reduced camera system of a Schur backend (after
+ * prepare_damping) at `lambda` as a training system with `probes` probe
+ * pairs in whitened coordinates: kind 0 draws x Gaussian and applies
+ * y = S_hat x; kind 1 draws y Gaussian and solves S_hat x = y with the
+ * backend's block-Jacobi PCG (work counters untouched). index receives its
+ * position. */
+FG_API fg_status fg_schur_capture_system(fg_backend* schur, fg_gnn* gnn, double lambda, size_t probes,
+                                         uint64_t seed, int kind, size_t* index);
+/* A training system from host arrays: features C x 64, adjacency C x C
+ * (rounded to bf16), probes K x C x width for x and y = S_hat x, mask C. */
+FG_API fg_status fg_gnn_import_system(fg_gnn* gnn, size_t cameras, size_t width, size_t probes,
+                                      const float* features, const float* adjacency, const float* probe_x,
+                                      const float* probe_y, const uint8_t* mask, size_t* index);
+FG_API fg_status fg_gnn_system_count(const fg_gnn* gnn, size_t* count);
+FG_API fg_status fg_gnn_system_size(const fg_gnn* gnn, size_t index, size_t* cameras, size_t* width,
+                                    size_t* probes);
+/* Copies a system back (any pointer may be NULL); adjacency as float. */
+FG_API fg_status fg_gnn_export_system(fg_gnn* gnn, size_t index, float* features, float* adjacency,
+                                      float* probe_x, float* probe_y, uint8_t* mask, double* damping);
+FG_API fg_status fg_gnn_clear_systems(fg_gnn* gnn);
+/* Loss of one system; when gradient (parameter_count floats) is non-NULL also
+ * the backward pass, and outputs (C x 64) receives the network output O. */
+FG_API fg_status fg_gnn_evaluate(fg_gnn* gnn, size_t index, double* loss, float* gradient, float* outputs);
+/* `steps` Adam steps (beta 0.9 / 0.999), one captured system per step in a
+ * shuffled cycle; mean_loss = mean loss over the steps (before each update). */
+FG_API fg_status fg_gnn_train(fg_gnn* gnn, size_t steps, double learning_rate, double* mean_loss);
+/* Attaches (or, with NULL, detaches) the network used by FG_PRECOND_LEARNED.
+ * The backend keeps a pointer: the network must outlive the attachment.
+ * Attaching re-arms the one-time block-Jacobi comparison. */
+FG_API fg_status fg_schur_attach_learned(fg_backend* schur, fg_gnn* gnn);
 
 /* ---- Dense direct backends on the same LeastSquaresBackend entry points ----
  * fg_backend_prepare / clear / accumulate / gradient_norm / prepare_damping /
