@@ -45,9 +45,10 @@ def parse():
     ap.add_argument("--forms", default="learned,fast,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows"],
+    ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows", "learned"],
                     help="ba: Schur-PCG time to cost (default); lsmr: the same with the LSMR backend; "
-                         "windows: the batched pose-graph windows")
+                         "windows: the batched pose-graph windows; learned: the learned preconditioner's "
+                         "training and inference steps")
     ap.add_argument("--windows", type=int, default=4096)
     ap.add_argument("--max-poses", type=int, default=300)
     return ap.parse_args()
@@ -265,9 +266,9 @@ def run_gpu(args, rank: int, world: int, device: int):
             fg.errors.raise_for_status(_lib.lib.fg_schur_time_operator(backend.handle, 1e-3, 50, C.byref(sec_op),
                                                                         C.byref(bytes_op)))
             results[name]["operator"] = dict(seconds=sec_op.value, bytes=bytes_op.value)
-            var, tuned = C.c_int(), (C.c_double * 2)()
+            var, tuned = C.c_int(), (C.c_double * 3)()
             _lib.lib.fg_schur_operator_info(backend.handle, C.byref(var), tuned)
-            results[name]["operator"].update(variant=var.value, tuned_seconds=[tuned[0], tuned[1]])
+            results[name]["operator"].update(variant=var.value, tuned_seconds=list(tuned))
             head_backend = backend
     # e2e: public C ABI from host arrays
     e2e = None
@@ -388,6 +389,47 @@ def run_windows(args, device: int) -> dict:
     return line
 
 
+def run_learned(args, device: int) -> dict:
+    """The learned preconditioner's own costs: one training step (forward,
+    loss, backward, Adam) and one forward evaluation on reduced camera systems
+    of the workload, with the tensor-core FLOPs of their GEMMs."""
+    import torch
+    import fagra_b200 as fg
+    from fagra_b200 import synthetic
+    torch.cuda.set_device(device)
+    stream = torch.cuda.ExternalStream(fg.device_stream(device), device=device)
+    net, info = train_network(fg, synthetic, args.workload, device, problems=1)
+    C = net.export_system(0)["features"].shape[0]
+    # GEMM FLOPs: forward 2C(64*64 + 3(C*64 + 128*64) + 64*64); backward twice that
+    fwd = 2.0 * C * (64 * 64 + 3 * (C * 64 + 128 * 64) + 64 * 64)
+    for _ in range(args.warmup):
+        net.train(1, 1e-4)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
+    net.train(args.steps * 10, 1e-4)
+    ev[1].record(stream)
+    ev[2].record(stream)
+    for _ in range(args.steps * 10):
+        net.evaluate(0)
+    ev[3].record(stream)
+    torch.cuda.synchronize(device)
+    n = args.steps * 10
+    t_train = ev[0].elapsed_time(ev[1]) * 1e-3 / n
+    t_fwd = ev[2].elapsed_time(ev[3]) * 1e-3 / n
+    pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("bf16_tflops") if (
+        ROOT / "MEASURED_PEAKS.json").exists() else None
+    achieved = 3 * fwd / t_train / 1e12
+    return dict(metric=f"learned preconditioner training step ({args.workload} reduced camera systems)",
+                value=t_train, unit="s", n_gpus=1, steps=n, warmup=args.warmup, ms_per_step=t_train * 1e3,
+                higher_is_better=False, scaling="weak", vs_baseline=None, dtype="bf16 operands, f32 accumulate",
+                data="synthetic", config=dict(workload=args.workload, cameras=C, network="3 layers, hidden 64",
+                                              training=info),
+                forward_seconds=t_fwd,
+                roofline=dict(bound="tensor", unit="TFLOP/s", achieved=achieved, peak=pk,
+                              frac=(achieved / pk) if pk else None, flops_per_step=3 * fwd,
+                              note="GEMMs of 16-64 CTAs: latency-bound at this size"))
+
+
 def run_lsmr(args, device: int) -> dict:
     """BAL time to cost with the LSMR backend (block-Jacobi, f64 and f32 storage)."""
     import numpy as np
@@ -448,7 +490,7 @@ def main():
         local = int(os.environ.get("LOCAL_RANK", "0"))
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
-        line = run_windows(args, local) if args.suite == "windows" else run_lsmr(args, local)
+        line = {"windows": run_windows, "lsmr": run_lsmr, "learned": run_learned}[args.suite](args, local)
         print(json.dumps(line), flush=True)
         return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -516,7 +558,10 @@ def main():
             roofline=dict(bound="hbm", kernel={0: "reduced operator, generic (k_points + k_cams)",
                                                1: "reduced operator, TMA-staged single pass (k_fast_apply + k_fast_reduce)",
                                                2: "reduced operator, direct-load single pass (k_fast_apply_direct + "
-                                                  "k_fast_reduce)"}.get(op.get("variant"), "reduced operator"),
+                                                  "k_fast_reduce)",
+                                               3: "reduced operator, prefetching direct-load single pass "
+                                                  "(k_fast_apply_pf + k_fast_reduce)"}.get(op.get("variant"),
+                                                                                           "reduced operator"),
                           operator_variant_seconds=op.get("tuned_seconds"), achieved=achieved, peak=pk,
                           peak_source=src, unit="GB/s", frac=(achieved / pk) if achieved else None,
                           algorithmic_bytes_per_launch=op.get("bytes"), seconds_per_launch=op.get("seconds"),

@@ -26,6 +26,7 @@ class SchurOptions(C.Structure):
         ("preconditioner", C.c_int),
         ("device", C.c_int),
         ("residual_replacement", C.c_double),
+        ("operator_variant", C.c_int),
     ]
 
 

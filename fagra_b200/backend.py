@@ -104,6 +104,13 @@ class Schur:
                               lambda s, v: s._set("preconditioner", PRECONDITIONERS[v]))
     residual_replacement = property(lambda s: s._get("residual_replacement"),
                                     lambda s, v: s._set("residual_replacement", v))
+    operator_variant = property(lambda s: s._get("operator_variant"), lambda s, v: s._set("operator_variant", v))
+
+    def operator_info(self):
+        """(variant in use, measured seconds per application of variants 1..3)."""
+        var, sec = C.c_int(), (C.c_double * 3)()
+        raise_for_status(lib.fg_schur_operator_info(self._h, C.byref(var), sec))
+        return var.value, list(sec)
 
     @property
     def handle(self):

@@ -107,6 +107,7 @@ FG_API void fg_schur_default_options(fg_schur_options* o) {
   o->preconditioner = FG_PRECOND_RETAINED_BLOCKS;
   o->device = 0;
   o->residual_replacement = 1e-2;
+  o->operator_variant = 0;
 }
 
 FG_API fg_status fg_schur_create(size_t retained, size_t cw, size_t pw, const fg_schur_options* options,
@@ -336,10 +337,10 @@ FG_API fg_status fg_schur_time_operator(fg_backend* b, double lambda, size_t rep
   FG_GUARD_BEGIN return b->impl->time_operator(lambda, reps, seconds, bytes);
   FG_GUARD_END
 }
-FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds2) {
+FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds3) {
   FG_NEED(b);
   if (!variant) return FG_NULL_ARGUMENT;
-  b->impl->operator_info(variant, seconds2);
+  b->impl->operator_info(variant, seconds3);
   return FG_OK;
 }
 FG_API fg_status fg_schur_attach_learned(fg_backend* b, fg_gnn* g) {

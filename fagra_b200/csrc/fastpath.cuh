@@ -466,6 +466,130 @@ __global__ void __launch_bounds__(DIRECT_THREADS, 1)
   for (int64_t i = tid; i < ny; i += DIRECT_THREADS) out[i] = ys[i];
 }
 
+// Prefetching variant of the direct pass: 512 threads per SM, and each warp
+// issues the 16-byte loads of its NEXT warp tile (records and tile bounds)
+// into registers before it works on the current one, so the HBM latency of
+// one tile overlaps the shuffle scan, the point solve and the shared-memory
+// scatter of the previous tile. E stays in registers for the scatter (no
+// L1 re-read).
+constexpr int PF_THREADS = 512;
+template <bool XS>
+__global__ void __launch_bounds__(PF_THREADS, 1)
+    k_fast_apply_pf(int64_t ncam, FastTiles tiles, const float* erec, const float* prec, const float* z,
+                    const float* pv, const double* beta, float* partials, const int* skip, const int* gate) {
+  if (skip && *skip) return;
+  if (gate && !*gate) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  constexpr int NW = PF_THREADS / 32;
+  const int64_t ny = ncam * 9;
+  const size_t vb = FastSmem<float, float>::vec_bytes(ncam);
+  float* ys = reinterpret_cast<float*>(smem);
+  float* xs = reinterpret_cast<float*>(smem + vb);
+  float* tpw = reinterpret_cast<float*>(smem + vb * (XS ? 2 : 1)) + w * 96;
+  const float bv = pv ? (float)*beta : 0.f;
+  for (int64_t i = tid; i < ny; i += PF_THREADS) {
+    ys[i] = 0;
+    if (XS) xs[i] = pv ? z[i] + bv * pv[i] : z[i];
+  }
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * NW;
+  int64_t wt = (int64_t)blockIdx.x * NW + w;
+  float4 nb[7];
+  int ncnt = 0;
+  int64_t np0 = 0;
+  if (wt < tiles.nwt) {
+    const int64_t e0 = tiles.wt_e0[wt];
+    ncnt = (int)(tiles.wt_e0[wt + 1] - e0);
+    np0 = tiles.wt_p0[wt];
+    if (lane < ncnt) {
+      const float4* v = reinterpret_cast<const float4*>(erec + (e0 + lane) * 28);
+#pragma unroll
+      for (int i = 0; i < 7; ++i) nb[i] = __ldg(v + i);
+    }
+  }
+  for (; wt < tiles.nwt; wt += stride) {
+    // take the prefetched tile
+    const int cnt = ncnt;
+    const int64_t p0 = np0;
+    float E[27];
+    uint32_t cam = 0, lp = 0xFFFFu;
+    if (lane < cnt) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        E[4 * i] = nb[i].x;
+        E[4 * i + 1] = nb[i].y;
+        E[4 * i + 2] = nb[i].z;
+        E[4 * i + 3] = nb[i].w;
+      }
+      E[24] = nb[6].x;
+      E[25] = nb[6].y;
+      E[26] = nb[6].z;
+      const uint32_t wd = __float_as_uint(nb[6].w);
+      cam = RecWord<float>::cam(wd);
+      lp = RecWord<float>::lp(wd);
+    }
+    // issue the next tile's loads
+    const int64_t wn = wt + stride;
+    ncnt = 0;
+    if (wn < tiles.nwt) {
+      const int64_t e0 = tiles.wt_e0[wn];
+      ncnt = (int)(tiles.wt_e0[wn + 1] - e0);
+      np0 = tiles.wt_p0[wn];
+      if (lane < ncnt) {
+        const float4* v = reinterpret_cast<const float4*>(erec + (e0 + lane) * 28);
+#pragma unroll
+        for (int i = 0; i < 7; ++i) nb[i] = __ldg(v + i);
+      }
+    }
+    float u0 = 0, u1 = 0, u2 = 0;
+    if (lane < cnt) {
+      float xc[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        const int64_t i = (int64_t)cam * 9 + c;
+        xc[c] = XS ? xs[i] : (pv ? z[i] + bv * pv[i] : z[i]);
+      }
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        u0 += E[c] * xc[c];
+        u1 += E[9 + c] * xc[c];
+        u2 += E[18 + c] * xc[c];
+      }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      float v0 = __shfl_up_sync(0xffffffffu, u0, off), v1 = __shfl_up_sync(0xffffffffu, u1, off);
+      float v2 = __shfl_up_sync(0xffffffffu, u2, off);
+      uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
+      if (lane >= off && lo == lp) {
+        u0 += v0;
+        u1 += v1;
+        u2 += v2;
+      }
+    }
+    const uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
+    if (lane < cnt && (lane == cnt - 1 || lpn != lp)) {
+      const float4* r = reinterpret_cast<const float4*>(prec + (p0 + lp) * 8);
+      float4 ca = __ldg(r), cb = __ldg(r + 1);
+      tpw[lp * 3] = ca.x * u0 + ca.y * u1 + ca.z * u2;
+      tpw[lp * 3 + 1] = ca.y * u0 + ca.w * u1 + cb.x * u2;
+      tpw[lp * 3 + 2] = ca.z * u0 + cb.x * u1 + cb.y * u2;
+    }
+    __syncwarp();
+    if (lane < cnt) {
+      const float t0 = tpw[lp * 3], t1 = tpw[lp * 3 + 1], t2 = tpw[lp * 3 + 2];
+      float* y = ys + (int64_t)cam * 9;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  float* out = partials + (int64_t)blockIdx.x * ny;
+  for (int64_t i = tid; i < ny; i += PF_THREADS) out[i] = ys[i];
+}
+
 // q = lambda x + B x + sum_b partials[b] with x = z (+ beta p); 32 coordinates
 // x 8 partial-vector chunks per block. Optional p.q -> alpha in the last block.
 template <class TS, class TV>
@@ -641,15 +765,15 @@ struct FastPath {
   int optin = 0;
   size_t attr_set[2][2] = {{0, 0}, {0, 0}};  // [TV is double][stage x] -> smem size already granted
 
-  int variant = 1;  // FP32 operator: 1 = TMA-staged stages, 2 = direct global loads
+  int variant = 1;  // FP32 operator: 1 = TMA-staged stages, 2 = direct global loads, 3 = prefetching direct
 
   template <class Impl, class TV>
   fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst,
                   const int* gate = nullptr, const double* lam_dev = nullptr) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
-    if (std::is_same<TS, float>::value && std::is_same<TV, float>::value && variant == 2) {
+    if (std::is_same<TS, float>::value && std::is_same<TV, float>::value && (variant == 2 || variant == 3)) {
       FG_TRY(apply_direct(s, (const float*)x.z, (const float*)x.pprev, x.beta, (float*)parts,
-                          pst ? &pst->done : nullptr, gate));
+                          pst ? &pst->done : nullptr, gate, variant == 3));
       FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
                 (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
                 dparts, pst, gate);
@@ -685,16 +809,27 @@ struct FastPath {
     return FG_OK;
   }
 
-  size_t direct_granted = 0;
+  size_t direct_granted = 0, pf_granted = 0;
   template <class Impl>
   fg_status apply_direct(Impl& s, const float* z, const float* pv, const double* beta, float* parts, const int* skip,
-                         const int* gate) {
+                         const int* gate, bool prefetch) {
     if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
     size_t vb = FastSmem<float, float>::vec_bytes((int64_t)s.nC);
-    size_t tpw = (size_t)(DIRECT_THREADS / 32) * 96 * sizeof(float);
+    size_t tpw = (size_t)((prefetch ? PF_THREADS : DIRECT_THREADS) / 32) * 96 * sizeof(float);
     bool xs = 2 * vb + tpw <= (size_t)optin;
     size_t sm = vb * (xs ? 2 : 1) + tpw;
     FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
+    if (prefetch) {
+      auto kern = xs ? k_fast_apply_pf<true> : k_fast_apply_pf<false>;
+      if (pf_granted < sm) {
+        FG_CUDA(cudaFuncSetAttribute(k_fast_apply_pf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        FG_CUDA(cudaFuncSetAttribute(k_fast_apply_pf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        pf_granted = sm;
+      }
+      FG_LAUNCH(kern, grid, PF_THREADS, sm, s.st, (int64_t)s.nC, tl, (const float*)d_erec.get(),
+                (const float*)d_prec.get(), z, pv, beta, parts, skip, gate);
+      return FG_OK;
+    }
     if (xs) {
       if (direct_granted < sm) {
         FG_CUDA(cudaFuncSetAttribute(k_fast_apply_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

@@ -140,7 +140,12 @@ class SchurImpl final : public Backend {
       set_error("unknown preconditioner");
       return FG_INVALID_OPTIONS;
     }
+    if (o.operator_variant < 0 || o.operator_variant > NVARIANTS) {
+      set_error("operator_variant must be 0 (autotune) or 1..3");
+      return FG_INVALID_OPTIONS;
+    }
     if (o.preconditioner != opt.preconditioner) learned_compared = learned_off = false;
+    if (o.operator_variant != opt.operator_variant) fast.tuned = false;
     int keep = dev;
     opt = o;
     opt.device = keep;
@@ -560,18 +565,24 @@ class SchurImpl final : public Backend {
     return gnn_capture(g, view_at(lambda), probes, seed, 0, apply, d_work.get(), d_qd.get(), st, index);
   }
   // Operator autotuner: times each FP32 single-pass variant (TMA-staged
-  // stages, direct global loads) on this structure and keeps the faster one.
-  // Runs once per structure; the factorization it needs is redone by every solve.
-  double tuned_seconds[2] = {0, 0};
-  void operator_info(int* variant, double* seconds2) const override {
+  // stages, direct global loads, prefetching direct loads) on this structure
+  // and keeps the fastest. Runs once per structure; the factorization it needs
+  // is redone by every solve.
+  static constexpr int NVARIANTS = 3;
+  double tuned_seconds[NVARIANTS] = {0, 0, 0};
+  void operator_info(int* variant, double* seconds) const override {
     *variant = fast.enabled() ? fast.variant : 0;
-    if (seconds2) {
-      seconds2[0] = tuned_seconds[0];
-      seconds2[1] = tuned_seconds[1];
-    }
+    if (seconds)
+      for (int v = 0; v < NVARIANTS; ++v) seconds[v] = tuned_seconds[v];
   }
   fg_status autotune_operator() {
     if (!fast.on || !is_f32() || fast.tuned) return FG_OK;
+    if (opt.operator_variant >= 1 && opt.operator_variant <= NVARIANTS) {
+      fast.variant = opt.operator_variant;
+      fast.tuned = true;
+      drop_graphs();
+      return FG_OK;
+    }
     unsigned fb = 0;
     FG_TRY(factor(1.0, &fb));
     if (fb) return FG_OK;
@@ -582,16 +593,17 @@ class SchurImpl final : public Backend {
     FG_CUDA(cudaEventCreate(&b));
     float best = 1e30f;
     int best_v = 1;
-    for (int v = 1; v <= 2; ++v) {
+    for (int v = 1; v <= NVARIANTS; ++v) {
       fast.variant = v;
       FG_TRY(apply_reduced<TS>(pv, 1.0, 1.0, true, d_t.get(), d_q.get(), nullptr, nullptr));
       cudaEventRecord(a, st);
-      for (int k = 0; k < 5; ++k) FG_TRY(apply_reduced<TS>(pv, 1.0, 1.0, true, d_t.get(), d_q.get(), nullptr, nullptr));
+      for (int k = 0; k < 10; ++k)
+        FG_TRY(apply_reduced<TS>(pv, 1.0, 1.0, true, d_t.get(), d_q.get(), nullptr, nullptr));
       cudaEventRecord(b, st);
       cudaEventSynchronize(b);
       float ms = 0;
       cudaEventElapsedTime(&ms, a, b);
-      tuned_seconds[v - 1] = ms * 1e-3 / 5;
+      tuned_seconds[v - 1] = ms * 1e-3 / 10;
       if (ms < best) {
         best = ms;
         best_v = v;

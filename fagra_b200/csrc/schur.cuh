@@ -85,9 +85,9 @@ class Backend {
   virtual fg_status time_operator(double, size_t, double*, double*) { return not_schur(); }
   virtual fg_status attach_learned(fg_gnn*) { return not_schur(); }
   virtual fg_status capture_system(fg_gnn*, double, size_t, uint64_t, int, size_t*) { return not_schur(); }
-  virtual void operator_info(int* variant, double* seconds2) const {
+  virtual void operator_info(int* variant, double* seconds3) const {
     *variant = 0;
-    if (seconds2) seconds2[0] = seconds2[1] = 0;
+    if (seconds3) seconds3[0] = seconds3[1] = seconds3[2] = 0;
   }
   // LSMR-only extras.
   virtual fg_status set_lsmr_options(const fg_lsmr_options&) { return not_lsmr(); }

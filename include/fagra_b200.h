@@ -84,6 +84,8 @@ typedef struct {
   int device;                /* CUDA device ordinal; default 0 */
   double residual_replacement; /* FP32 mode: the recurrence residual is replaced by the FP64
                                   residual b - S x each time it falls by this factor; default 1e-2 */
+  int operator_variant;        /* FP32 BAL-shaped systems: 0 = autotune (default), 1..3 = force the
+                                  reduced-operator variant of fg_schur_operator_info */
 } fg_schur_options;
 
 /* src/schur.rs:44-60 SchurDiagnostics (has_* = Some) */
@@ -347,9 +349,9 @@ FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size
 
 /* The reduced-operator implementation the autotuner chose for the current
  * structure: 0 generic (any widths), 1 TMA-staged single pass, 2 direct-load
- * single pass; seconds[v-1] = measured time per application of variant v
- * (0 if not measured). */
-FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds2);
+ * single pass, 3 prefetching direct-load single pass; seconds3[v-1] (may be
+ * NULL) = measured time per application of variant v (0 if not measured). */
+FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds3);
 
 /* ---- Learned preconditioner (no reference counterpart) ----------------------
  * A message-passing network over the camera covisibility graph of the reduced

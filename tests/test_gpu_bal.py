@@ -141,3 +141,30 @@ def test_bal_reduced_operator_matches_oracle(precision, tol, lam):
     ref = o.reduced_apply(lam, x)
     got = b.reduced_apply(lam, x)
     assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref)
+
+
+def test_fp32_operator_variants_give_the_same_step():
+    """Each FP32 single-pass operator variant (TMA-staged, direct, prefetching
+    direct), forced instead of autotuned, drives the FP32 PCG to the same step
+    (FP32 storage perturbs the system itself at ~1e-7, hence the looser bound
+    against the f64 step)."""
+    d = synthetic.generate("bal1k", cameras=64, points=8000, seed=5)
+    steps, its = {}, {}
+    for variant in (0, 1, 2, 3):
+        b = fg.Schur(9 * d.num_cameras, 9, 3, precision="f64" if variant == 0 else "f32")
+        if variant:
+            b.operator_variant = variant
+        p = fg.BalProblem.from_data(d)
+        b.prepare(p.dimension())
+        p.linearize(b)
+        b.prepare_damping(1e-6)
+        steps[variant] = b.solve_damped(1e-3).delta
+        its[variant] = b.diagnostics().iterations
+        if variant:
+            assert b.operator_info()[0] == variant
+            assert b.diagnostics().reduced_relative_residual < 1e-8
+    ref = np.linalg.norm(steps[0])
+    for v in (1, 2, 3):
+        assert np.linalg.norm(steps[v] - steps[0]) <= 1e-4 * ref, v
+        assert np.linalg.norm(steps[v] - steps[1]) <= 1e-6 * ref, v
+        assert abs(its[v] - its[1]) <= 2, (v, its)
