@@ -67,6 +67,16 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(dptr)
 
 
+def _covariance(handle, columns, tol: float) -> np.ndarray:
+    """CovarianceBackend::covariance + SelectedCovariance (src/covariance.rs:225-270):
+    the selected block of the undamped inverse information, selection order."""
+    cols = (size_t * max(len(columns), 1))(*[int(c) for c in columns])
+    k = len(columns)
+    out = np.zeros(max(k * k, 1))
+    raise_for_status(lib.fg_backend_covariance(handle, cols, k, tol, _dp(out)))
+    return out[:k * k].reshape(k, k).T.copy()
+
+
 class Schur:
     """Device Schur-PCG backend: `Schur::new(retained, retained_width, eliminated_width)`."""
 
@@ -228,6 +238,11 @@ class Schur:
         out["cross"] = out["cross"][:len(s["edges"]) * cw * pw]
         return out
 
+    def covariance(self, columns, relative_pivot_tolerance: float = 64 * np.finfo(float).eps) -> np.ndarray:
+        """Schur delegates to LinearizedModel::covariance (src/schur.rs:548-556): a
+        dense normal matrix of the cached Jacobian, then the selected inverse."""
+        return _covariance(self._h, columns, relative_pivot_tolerance)
+
     def reduced_apply(self, damping: float, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64)
         y = np.zeros_like(x)
@@ -318,6 +333,10 @@ class Lsmr:
             pass
 
     # ---- LeastSquaresBackend
+    def covariance(self, columns, relative_pivot_tolerance: float = 64 * np.finfo(float).eps) -> np.ndarray:
+        """Lsmr delegates to LinearizedModel::covariance (src/lsmr.rs:598-604)."""
+        return _covariance(self._h, columns, relative_pivot_tolerance)
+
     def prepare(self, dimension: int) -> None:
         raise_for_status(lib.fg_backend_prepare(self._h, dimension))
         self._dim = dimension
@@ -467,12 +486,7 @@ class _DenseBackend:
         return DampedStep(delta, pred.value)
 
     def covariance(self, columns, relative_pivot_tolerance: float = 64 * np.finfo(float).eps) -> np.ndarray:
-        """Selected inverse information in selection order (src/covariance.rs:225-255)."""
-        cols = (size_t * max(len(columns), 1))(*[int(c) for c in columns])
-        k = len(columns)
-        out = np.zeros(max(k * k, 1))
-        raise_for_status(lib.fg_backend_covariance(self._h, cols, k, relative_pivot_tolerance, _dp(out)))
-        return out[:k * k].reshape(k, k).T.copy()
+        return _covariance(self._h, columns, relative_pivot_tolerance)
 
 
 class DenseNormalCholesky(_DenseBackend):

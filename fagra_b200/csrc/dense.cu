@@ -26,6 +26,7 @@
 #include "dense.cuh"
 #include <algorithm>
 #include <set>
+#include <memory>
 
 namespace fg {
 
@@ -832,13 +833,50 @@ FG_API fg_status fg_dense_qr_set_tolerance(fg_backend* b, double tol) {
   static_cast<DenseImpl*>(b->impl)->set_qr_tolerance(tol);
   return FG_OK;
 }
+// LinearizedModel::covariance (src/linear_model.rs:122-167), which Schur and
+// Lsmr delegate to: a DenseNormalCholesky over the cached Jacobian, replayed
+// one row group at a time (blocks sharing row and rows; empty groups skipped)
+// with -r as the residual, then the selected covariance of that normal matrix.
+static fg_status model_covariance(Backend* src, const size_t* columns, size_t k, double tol, double* out) {
+  HostModel m;
+  FG_TRY(src->model_host(&m));
+  DenseImpl* normal = nullptr;
+  FG_TRY(make_dense(DK_NORMAL, src->device(), &normal));
+  std::unique_ptr<DenseImpl> hold(normal);
+  FG_TRY(normal->prepare(m.cols));
+  FG_TRY(normal->clear());
+  std::vector<size_t> cols, widths;
+  std::vector<const double*> jac;
+  std::vector<ptrdiff_t> rs, cs;
+  size_t start = 0;
+  while (start < m.blocks.size()) {
+    const HostBlock& first = m.blocks[start];
+    if (first.rows == 0) {
+      ++start;
+      continue;
+    }
+    size_t end = start + 1;
+    while (end < m.blocks.size() && m.blocks[end].row == first.row && m.blocks[end].rows == first.rows) ++end;
+    cols.clear(); widths.clear(); jac.clear(); rs.clear(); cs.clear();
+    for (size_t i = start; i < end; ++i) {
+      const HostBlock& b = m.blocks[i];
+      cols.push_back(b.col);
+      widths.push_back(b.cols);
+      jac.push_back(m.values.data() + b.start);
+      rs.push_back(1);
+      cs.push_back((ptrdiff_t)b.rows);
+    }
+    FG_TRY(normal->accumulate(first.rows, m.negres.data() + first.row, end - start, cols.data(), widths.data(),
+                              jac.data(), rs.data(), cs.data()));
+    start = end;
+  }
+  return normal->covariance(columns, k, tol, out);
+}
+
 FG_API fg_status fg_backend_covariance(fg_backend* b, const size_t* columns, size_t k, double tol, double* out) {
   if (!b || !b->impl || (k && (!columns || !out))) return FG_NULL_ARGUMENT;
-  if (b->impl->kind() < 2) {
-    set_error("covariance is served by the dense backends");
-    return FG_UNSUPPORTED_STRUCTURE;
-  }
   try {
+    if (b->impl->kind() < 2) return model_covariance(b->impl, columns, k, tol, out);
     return static_cast<DenseImpl*>(b->impl)->covariance(columns, k, tol, out);
   } catch (...) {
     set_error("unexpected host exception");

@@ -382,6 +382,35 @@ class LsmrImpl final : public Backend {
     return FG_OK;
   }
 
+  // The linearization in the reference layout: emission k has rows
+  // [h_erow[k], h_erow[k+1]), blocks [h_eblk[k], h_eblk[k+1]) and its values
+  // start at h_eval[k], each block column-major.
+  fg_status model_host(HostModel* m) override {
+    FG_TRY(sync_model());
+    const size_t ne = h_eval.size();
+    m->rows = rows;
+    m->cols = dim;
+    m->blocks.clear();
+    for (size_t k = 0; k < ne; ++k) {
+      const size_t r0 = (size_t)h_erow[k], nr = (size_t)(h_erow[k + 1] - h_erow[k]);
+      size_t start = (size_t)h_eval[k];
+      for (int64_t b = h_eblk[k]; b < h_eblk[k + 1]; ++b) {
+        m->blocks.push_back(HostBlock{r0, (size_t)h_bcol[b], nr, (size_t)h_bcols[b], start});
+        start += nr * (size_t)h_bcols[b];
+      }
+    }
+    m->values.assign(std::max<size_t>(nvalues, 1), 0.0);
+    m->negres.assign(std::max<size_t>(rows, 1), 0.0);
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (nvalues) {
+      std::vector<TS> tmp(nvalues);
+      FG_CUDA(cudaMemcpy(tmp.data(), d_values.get(), nvalues * sizeof(TS), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < nvalues; ++i) m->values[i] = (double)tmp[i];
+    }
+    if (rows) FG_CUDA(cudaMemcpy(m->negres.data(), d_negres.get(), rows * sizeof(double), cudaMemcpyDeviceToHost));
+    return FG_OK;
+  }
+
   // ------------------------------------------------------------ test hooks
   fg_status damped_products(double lambda, int scaled, const double* x, double* fwd, const double* y,
                             double* tr) override {

@@ -1026,6 +1026,22 @@ class SchurImpl final : public Backend {
     return FG_OK;
   }
 
+  fg_status model_host(HostModel* m) override {
+    size_t nb = 0, nv = 0, r = 0, c = 0;
+    FG_TRY(structure_sizes(&nb, nullptr, &nv, nullptr, &r, &c));
+    std::vector<uint64_t> b5(5 * std::max<size_t>(nb, 1));
+    FG_TRY(export_structure(b5.data(), nullptr, nullptr, nullptr));
+    m->rows = r;
+    m->cols = c;
+    m->values.assign(std::max<size_t>(nv, 1), 0.0);
+    m->negres.assign(std::max<size_t>(r, 1), 0.0);
+    FG_TRY(export_model(m->values.data(), m->negres.data(), nullptr, nullptr, nullptr, nullptr));
+    m->blocks.resize(nb);
+    for (size_t i = 0; i < nb; ++i)
+      m->blocks[i] = HostBlock{b5[5 * i], b5[5 * i + 1], b5[5 * i + 2], b5[5 * i + 3], b5[5 * i + 4]};
+    return FG_OK;
+  }
+
   fg_status export_structure(uint64_t* b5, uint64_t* e4, uint64_t* owners, uint64_t* v3) override {
     FG_TRY(sync_model());
     std::vector<DBlockMeta> mb(nblocks);

@@ -41,6 +41,15 @@ struct VerifyState {
   unsigned counter0, counter1, pad;
 };
 
+// A linearized model on the host in the reference layout (src/linear_model.rs:
+// 12-19, 95-105): Jacobian blocks {row, col, rows, cols, start} in emission
+// order, column-major values, and -r.
+struct HostModel {
+  size_t rows = 0, cols = 0;
+  std::vector<HostBlock> blocks;
+  std::vector<double> values, negres;
+};
+
 class Backend {
  public:
   virtual ~Backend() {}
@@ -74,6 +83,13 @@ class Backend {
   virtual int device() const = 0;
   virtual cudaStream_t stream() const = 0;
 
+  // The current linearization as a host model (Schur and LSMR), for the
+  // covariance both delegate to LinearizedModel::covariance (src/schur.rs:548-556,
+  // src/lsmr.rs:598-604).
+  virtual fg_status model_host(HostModel*) {
+    set_error("this backend keeps no linearized model");
+    return FG_UNSUPPORTED_STRUCTURE;
+  }
   // Schur-only extras.
   virtual fg_status set_options(const fg_schur_options&) { return not_schur(); }
   virtual void diagnostics(fg_schur_diagnostics* d) const { *d = fg_schur_diagnostics{}; }

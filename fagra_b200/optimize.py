@@ -142,6 +142,13 @@ class LevenbergMarquardt:
 
     optimize_with = solve_batch
 
+    def solve_batch_with_covariance(self, problem, options: Optional[OptimizeOptions] = None, columns=(),
+                                    relative_pivot_tolerance: float = 64 * np.finfo(float).eps):
+        """levenberg_marquardt.rs:218-231: solve, then the selected covariance of
+        the undamped model linearized at the final estimates."""
+        report = self.solve_batch(problem, options)
+        return report, _final_covariance(self._backend, problem, columns, relative_pivot_tolerance)
+
     def solve_batch_with_outcome(self, problem, options: Optional[OptimizeOptions] = None) -> LmOutcome:
         code, rep = self._run(problem, options or OptimizeOptions())
         s = self._stats
@@ -172,6 +179,25 @@ class GaussNewton:
         return OptimizeReport(rep.iterations, rep.initial_cost, rep.final_cost, TERMINATION[rep.termination])
 
     optimize_with = solve_batch
+
+    def solve_batch_with_covariance(self, problem, options: Optional[OptimizeOptions] = None, columns=(),
+                                    relative_pivot_tolerance: float = 64 * np.finfo(float).eps):
+        """gauss_newton.rs solve_batch_with_covariance: solve, then the selected
+        covariance of the model at the final estimates."""
+        report = self.solve_batch(problem, options)
+        return report, _final_covariance(self._backend, problem, columns, relative_pivot_tolerance)
+
+
+def _final_covariance(backend, problem, columns, tol):
+    """Workspace::covariance (src/optimization.rs:268-284): linearize at the final
+    estimates, then CovarianceBackend::covariance on that model."""
+    backend.prepare(problem.dimension() if hasattr(problem, "_bal_handle") else len(problem.x))
+    if hasattr(problem, "_bal_handle"):
+        problem.linearize(backend)
+    else:
+        backend.clear()
+        problem._linearize(problem.x.copy(), lambda r, blocks: backend.accumulate(r, blocks))
+    return backend.covariance(columns, tol)
 
 
 class CallbackProblem:

@@ -422,10 +422,13 @@ FG_API fg_status fg_dense_schur_create(size_t retained_dimension, const size_t* 
 FG_API fg_status fg_dense_qr_create(double relative_rank_tolerance, int device, fg_backend** out);
 FG_API fg_status fg_dense_qr_set_tolerance(fg_backend* backend, double relative_rank_tolerance);
 /* CovarianceBackend::covariance (src/covariance.rs:263-270) + SelectedCovariance
- * (:225-255) for a dense backend's current model: out (k x k, column-major) =
- * the selected block of the undamped inverse information, columns in
- * selection order; relative_pivot_tolerance is CovarianceOptions'
- * (default 64 eps). DenseSchur accepts retained columns only. */
+ * (:225-255) for a backend's current model: out (k x k, column-major) = the
+ * selected block of the undamped inverse information, columns in selection
+ * order; relative_pivot_tolerance is CovarianceOptions' (default 64 eps).
+ * DenseSchur accepts retained columns only. Schur and LSMR handles replay their
+ * cached Jacobian into a device DenseNormalCholesky first, as both delegate to
+ * LinearizedModel::covariance (src/schur.rs:548-556, src/lsmr.rs:598-604,
+ * src/linear_model.rs:122-167); that needs the dense n x n normal matrix. */
 FG_API fg_status fg_backend_covariance(fg_backend* backend, const size_t* columns, size_t k,
                                        double relative_pivot_tolerance, double* out);
 

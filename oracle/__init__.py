@@ -214,6 +214,14 @@ class Schur:
     def _limits(self):
         lib.or_schur_set_limits(self.h, self.max_iterations, self.relative_tolerance)
 
+    def covariance(self, columns, tol=64 * np.finfo(float).eps):
+        """LinearizedModel::covariance of the cached model (src/linear_model.rs:122-167)."""
+        cols = np.ascontiguousarray(np.asarray(columns, np.uint64))
+        k = len(cols)
+        out = np.zeros(max(k * k, 1))
+        st = lib.or_backend_covariance(self.h, 0, cols.ctypes.data_as(C.POINTER(size_t)), k, tol, _dp(out))
+        return st, out[:k * k].reshape(k, k).T.copy()
+
     def prepare(self, dim):
         self._limits()
         self.dim = dim
