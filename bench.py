@@ -38,11 +38,11 @@ REL = 1e-6
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
     ap.add_argument("--workload", default="bal1k")
-    ap.add_argument("--forms", default="learned,fast,f64")
+    ap.add_argument("--forms", default="learned,fastc,fast,f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows", "learned"],
@@ -121,24 +121,51 @@ class Clocks:
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.window = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self.t_start = time.time()
+            # the sampler needs a moment before its first line; the caller's
+            # warm-up runs meanwhile, and mark() brackets the timed region
+            for _ in range(40):
+                time.sleep(0.05)
+                if self.path.exists() and self.path.stat().st_size > 0:
+                    break
         except OSError:
             self.proc = None
+
+    def mark(self, begin: bool) -> None:
+        """Bracket the timed region (wall clock) so samples can be attributed."""
+        t = time.time()
+        self.window = (t, None) if begin else (self.window[0] if self.window else t, t)
 
     def stop(self) -> dict:
         if not self.proc:
             return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        time.sleep(0.1)
         self.proc.send_signal(signal.SIGTERM)
         self.proc.wait(timeout=10)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        t_end = time.time()
+        rows = []
         for line in self.path.read_text().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
+            if len(f) >= 9:
+                rows.append(f)
+        # sample i was taken ~ t_start + i * 50 ms; keep those inside the timed
+        # window (at least the one nearest to it)
+        if rows and self.window and self.window[1]:
+            step = max((t_end - self.t_start) / max(len(rows), 1), 1e-3)
+            times = [self.t_start + i * step for i in range(len(rows))]
+            inside = [r for r, t in zip(rows, times) if self.window[0] <= t <= self.window[1]]
+            if not inside:
+                mid = 0.5 * (self.window[0] + self.window[1])
+                inside = [min(zip(rows, times), key=lambda rt: abs(rt[1] - mid))[0]]
+            rows = inside
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for f in rows:
             try:
                 sm.append(float(f[1]))
                 mx = float(f[2])
@@ -190,8 +217,11 @@ def run_gpu(args, rank: int, world: int, device: int):
 
     opts = fg.OptimizeOptions(50, 1e-8, 0.0, 0.0)
     # fast: FP32 bulk + FP64 residual replacement, CG tolerance 1e-8 (the per-step
-    # linear-residual bar); f64: fagra's Schur arithmetic and default tolerance.
-    forms = {"learned": dict(precision="f32", preconditioner="learned", tol=1e-8),
+    # linear-residual bar); fastc: the same with the two-level PCG (gauge coarse
+    # correction); learned: fastc with the learned block preconditioner
+    # (block-Jacobi fallback); f64: fagra's Schur arithmetic and default tolerance.
+    forms = {"learned": dict(precision="f32", preconditioner="learned", coarse_correction=True, tol=1e-8),
+             "fastc": dict(precision="f32", preconditioner="retained_blocks", coarse_correction=True, tol=1e-8),
              "fast": dict(precision="f32", preconditioner="retained_blocks", tol=1e-8),
              "f64": dict(precision="f64", preconditioner="retained_blocks", tol=1e-10),
              "f32": dict(precision="f32", preconditioner="retained_blocks", tol=1e-10),
@@ -223,6 +253,8 @@ def run_gpu(args, rank: int, world: int, device: int):
             di = backend.diagnostics()
             learned_info["comparison"] = dict(damping=lmo.initial_damping, learned_iterations=di.learned_iterations,
                                               block_jacobi_iterations=di.block_jacobi_iterations,
+                                              learned_seconds=di.learned_seconds,
+                                              block_jacobi_seconds=di.block_jacobi_seconds,
                                               kept=di.preconditioner_used)
 
         def step():
@@ -232,12 +264,14 @@ def run_gpu(args, rank: int, world: int, device: int):
                                                     C.byref(lmo), target, C.byref(rep), C.byref(st))
             return code, rep, st
 
+        if name == head:
+            clk = Clocks(device)  # started before the warm-up so it samples from the first timed step
         for _ in range(args.warmup):
             step()
         barrier()
         if name == head:
-            clk = Clocks(device)
             l0 = fg.kernel_launches()
+            clk.mark(True)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         ev[0].record(stream)
         per = []
@@ -249,6 +283,7 @@ def run_gpu(args, rank: int, world: int, device: int):
         barrier()
         secs = ev[0].elapsed_time(ev[1]) * 1e-3 / args.steps
         if name == head:
+            clk.mark(False)
             launches = (fg.kernel_launches() - l0) // args.steps
             clocks_info = clk.stop()
         reached = all(p["termination"] == 5 for p in per)
@@ -314,12 +349,13 @@ def run_windows(args, device: int) -> dict:
     batch = posegraph.generate(args.windows, max_poses=args.max_poses)
     solver = posegraph.WindowSolver(batch, removed=10, precision="f64", device=device)
     stream = torch.cuda.ExternalStream(solver.stream(), device=device)
+    clk = Clocks(device)
     for _ in range(args.warmup):
         solver.upload()
         solver.run()
     torch.cuda.synchronize(device)
-    clk = Clocks(device)
     l0 = fg.kernel_launches()
+    clk.mark(True)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     times = []
     for _ in range(args.steps):
@@ -329,6 +365,7 @@ def run_windows(args, device: int) -> dict:
         ev[1].record(stream)
         torch.cuda.synchronize(device)
         times.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+    clk.mark(False)
     launches = (fg.kernel_launches() - l0) // args.steps
     clocks = clk.stop()
     poses, reps, a, b = solver.download()
@@ -550,7 +587,14 @@ def main():
             config=dict(workload=f"{args.workload}: {data.num_cameras} cameras, {data.num_points} points, "
                                  f"{data.num_observations} observations; LM until cost <= (1+1e-6) x f64 oracle "
                                  f"cost {g['final_cost']:.6f}",
-                        form=head, parallelism=f"replicas x{world}",
+                        form=head, form_description={
+                            "learned": "FP32 bulk + FP64 reductions, learned block preconditioner with block-Jacobi "
+                                       "fallback, two-level PCG (gauge coarse correction), CG tolerance 1e-8",
+                            "fastc": "FP32 bulk + FP64 reductions, block-Jacobi, two-level PCG (gauge coarse "
+                                     "correction), CG tolerance 1e-8",
+                            "fast": "FP32 bulk + FP64 reductions, block-Jacobi, CG tolerance 1e-8",
+                            "f64": "f64, block-Jacobi, CG tolerance 1e-10 (fagra's Schur arithmetic)"}.get(head, head),
+                        parallelism=f"replicas x{world}",
                         l2="inputs larger than L2 (cross blocks alone are 119 MB in f32, 238 MB in f64)"),
             forms={k: {kk: vv for kk, vv in v.items() if kk != "operator"} for k, v in results.items()},
             speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,

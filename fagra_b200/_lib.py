@@ -27,6 +27,7 @@ class SchurOptions(C.Structure):
         ("device", C.c_int),
         ("residual_replacement", C.c_double),
         ("operator_variant", C.c_int),
+        ("coarse_correction", C.c_int),
     ]
 
 
@@ -48,6 +49,9 @@ class SchurDiagnosticsC(C.Structure):
         ("learned_fallback", C.c_int),
         ("learned_iterations", size_t),
         ("block_jacobi_iterations", size_t),
+        ("learned_seconds", C.c_double),
+        ("block_jacobi_seconds", C.c_double),
+        ("coarse_vectors", size_t),
     ]
 
 

@@ -51,6 +51,9 @@ class SchurDiagnostics:
     learned_fallback: Optional[str] = None
     learned_iterations: int = 0
     block_jacobi_iterations: int = 0
+    coarse_vectors: int = 0
+    learned_seconds: float = 0.0
+    block_jacobi_seconds: float = 0.0
 
 
 @dataclass
@@ -81,11 +84,13 @@ class Schur:
     """Device Schur-PCG backend: `Schur::new(retained, retained_width, eliminated_width)`."""
 
     def __init__(self, retained_dimension: int, retained_block_width: int, eliminated_block_width: int, *,
-                 precision: str = "f64", preconditioner: str = "retained_blocks", device: int = 0):
+                 precision: str = "f64", preconditioner: str = "retained_blocks", coarse_correction: bool = False,
+                 device: int = 0):
         o = _lib.SchurOptions()
         lib.fg_schur_default_options(C.byref(o))
         o.precision = PRECISIONS[precision]
         o.preconditioner = PRECONDITIONERS[preconditioner]
+        o.coarse_correction = int(bool(coarse_correction))
         o.device = device
         self._opts = o
         h = C.c_void_p()
@@ -115,6 +120,8 @@ class Schur:
     residual_replacement = property(lambda s: s._get("residual_replacement"),
                                     lambda s, v: s._set("residual_replacement", v))
     operator_variant = property(lambda s: s._get("operator_variant"), lambda s, v: s._set("operator_variant", v))
+    coarse_correction = property(lambda s: bool(s._get("coarse_correction")),
+                                 lambda s, v: s._set("coarse_correction", int(bool(v))))
 
     def operator_info(self):
         """(variant in use, measured seconds per application of variants 1..3)."""
@@ -194,7 +201,8 @@ class Schur:
                                 opt(d.has_original, d.original_relative_residual), d.refinements,
                                 {v: k for k, v in PRECONDITIONERS.items()}[d.preconditioner_used],
                                 (None, "failed", "more_iterations")[d.learned_fallback], d.learned_iterations,
-                                d.block_jacobi_iterations)
+                                d.block_jacobi_iterations, d.coarse_vectors, d.learned_seconds,
+                                d.block_jacobi_seconds)
 
     def timings(self) -> SchurTimings:
         t = _lib.SchurTimingsC()

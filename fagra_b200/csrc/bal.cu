@@ -55,6 +55,40 @@ __global__ void k_bal_camera_prep(int64_t nc, const double* cams, double* prep) 
     }
 }
 
+// Camera part of the 7 similarity-gauge directions of bundle adjustment, in
+// the Jacobian's own coordinates (additive angle-axis w, translation t,
+// intrinsics): the reprojection residuals are invariant under X -> s Q X + d
+// with the cameras moved to R Q^T, s t - R Q^T d, so to first order
+//   rotation about world axis k:   dw = -J_r(w)^-1 e_k,  dt = 0
+//   translation along k:           dw = 0,              dt = -R e_k
+//   scale:                         dw = 0,              dt = t
+// with J_r(w) the right factor of the camera prep (the rotation Jacobian
+// d(R X)/dw = -R [X]x J_r(w) of k_bal_linearize). basis[j * 9nc + 9c + i].
+__global__ void k_bal_gauge(int64_t nc, const double* cams, const double* prep, double* basis) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double* R = prep + 18 * c;
+  const double* J = R + 9;
+  const double* t = cams + 9 * c + 3;
+  const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+                     J[2] * (J[3] * J[7] - J[4] * J[6]);
+  double inv[9] = {J[4] * J[8] - J[5] * J[7], J[2] * J[7] - J[1] * J[8], J[1] * J[5] - J[2] * J[4],
+                   J[5] * J[6] - J[3] * J[8], J[0] * J[8] - J[2] * J[6], J[2] * J[3] - J[0] * J[5],
+                   J[3] * J[7] - J[4] * J[6], J[1] * J[6] - J[0] * J[7], J[0] * J[4] - J[1] * J[3]};
+  const int64_t n = 9 * nc;
+  for (int j = 0; j < 7; ++j) {
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (j < 3) {
+      for (int i = 0; i < 3; ++i) v[i] = -inv[3 * i + j] / det;
+    } else if (j < 6) {
+      for (int i = 0; i < 3; ++i) v[3 + i] = -R[3 * i + (j - 3)];
+    } else {
+      for (int i = 0; i < 3; ++i) v[3 + i] = t[i];
+    }
+    for (int i = 0; i < 9; ++i) basis[j * n + 9 * c + i] = v[i];
+  }
+}
+
 // Reprojection residual and Jacobians (model.rs:157-185, 214-236) for every
 // observation k in emission order, written in the packed block layout:
 // values[24k .. 24k+18) = camera block (2x9 column major), [24k+18, 24k+24) =
@@ -327,6 +361,11 @@ fg_status BalProblem::linearize(Backend* b) {
   FG_CUDA(cudaMemcpyAsync(h_flag.get(), d_flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
   FG_CUDA(cudaStreamSynchronize(st));
   b->mark_device_model(2 * no);
+  if (nc) {  // the gauge directions at these estimates, for two-level PCG
+    FG_TRY(gauge.resize(7 * 9 * nc));
+    FG_LAUNCH(k_bal_gauge, grid_for(nc, 128), 128, 0, st, (int64_t)nc, cams.get(), prep.get(), gauge.get());
+    FG_TRY(b->set_coarse_basis(gauge.get(), 7));
+  }
   if (h_flag.get()[0]) {
     set_error("invalid BAL linearization");
     return FG_INVALID_EVALUATION;

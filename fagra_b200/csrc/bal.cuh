@@ -51,7 +51,7 @@ struct BalProblem {
   std::vector<size_t> order;  // emission position -> insertion index
   std::vector<uint32_t> h_oc, h_op;
   DBuf<uint32_t> oc, op;
-  DBuf<double> px, cams, pts, tcams, tpts, prep, tprep, partials, result, init_cams, init_pts;
+  DBuf<double> px, cams, pts, tcams, tpts, prep, tprep, partials, result, init_cams, init_pts, gauge;
   DBuf<unsigned> counters;
   DBuf<int> d_flag;
   HBuf<double> h_result;

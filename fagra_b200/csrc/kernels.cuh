@@ -442,9 +442,27 @@ __global__ void k_precond_inverse(Layout L, const uint8_t* observed, const TS* p
 // beta for the next search direction, which its consumers form on the fly.
 // XD: the iterate is FP64 (mixed-precision mode) and convergence is deferred
 // to an FP64 residual replacement (see k_replace).
-template <int CW, class TS, class TX, bool MIXED>
+// Two-level preconditioning (CO): z = Minv r + W c with c = G W^T r, where
+// W (nk <= MAXK rows of length 9C) spans a coarse space and G = (W^T S W)^-1.
+// The kernels add the nk partial dots W^T r to their block sums; the last
+// block forms c, adds d.c to r.z and leaves c for k_coarse_add, which adds
+// W c to z before any consumer reads it.
+constexpr int MAXK = 8;
+__device__ __forceinline__ double coarse_finish(const double* G, int nk, const double* d, PcgState* st) {
+  double extra = 0;
+  for (int i = 0; i < nk; ++i) {
+    double c = 0;
+    for (int j = 0; j < nk; ++j) c += G[i * nk + j] * d[j];
+    st->coarse[i] = c;
+    extra += d[i] * c;
+  }
+  st->coarse_pending = 1;
+  return extra;
+}
+
+template <int CW, class TS, class TX, bool MIXED, bool CO>
 __global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q, const TS* minv,
-                              double* partials, PcgState* st) {
+                              double* partials, PcgState* st, const TS* W, const double* G, int nk) {
   if (st->done) return;
   const int cw = CW ? CW : L.cw;
   extern __shared__ unsigned char sh_raw[];
@@ -478,16 +496,22 @@ __global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q,
     z[i] = zi;
     rz = (double)ri * (double)zi;
   }
-  double s[2] = {rr, rz};
-  block_sums<2>(s);
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = s[0];
-    partials[2 * blockIdx.x + 1] = s[1];
-  }
+  constexpr int K = CO ? 2 + MAXK : 2;
+  double s[K];
+  s[0] = rr;
+  s[1] = rz;
+  if (CO)
+#pragma unroll
+    for (int j = 0; j < MAXK; ++j) s[2 + j] = (active && j < nk) ? (double)W[j * n + i] * (double)ri : 0.0;
+  block_sums<K>(s);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[K * blockIdx.x + k] = s[k];
   if (arrive_last(&st->counter1)) {
-    double tot[2];
-    finish_sums<2>(partials, tot);
+    double tot[K];
+    finish_sums<K>(partials, tot);
     if (threadIdx.x == 0) {
+      if (CO) tot[1] += coarse_finish(G, nk, tot + 2, st);
       st->iterations += 1;
       st->rr = tot[0];
       bool conv = sqrt(tot[0]) < st->threshold;
@@ -514,9 +538,9 @@ __global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q,
 }
 
 // PCG start: r = b, x = 0, z = Minv r, p = 0, beta = 0, rz = r.z, ||b||.
-template <int CW, class TS, class TX>
+template <int CW, class TS, class TX, bool CO>
 __global__ void k_pcg_start(Layout L, const double* b, TX* x, TS* r, TS* z, TS* p, const TS* minv, double* partials,
-                            PcgState* st, double rel_tol) {
+                            PcgState* st, double rel_tol, const TS* W, const double* G, int nk) {
   const int cw = CW ? CW : L.cw;
   extern __shared__ unsigned char sh_raw[];
   TS* rs = reinterpret_cast<TS*>(sh_raw);
@@ -546,16 +570,24 @@ __global__ void k_pcg_start(Layout L, const double* b, TX* x, TS* r, TS* z, TS* 
     z[i] = zi;
     rz = (double)ri * (double)zi;
   }
-  double s[2] = {bb, rz};
-  block_sums<2>(s);
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = s[0];
-    partials[2 * blockIdx.x + 1] = s[1];
-  }
+  constexpr int K = CO ? 2 + MAXK : 2;
+  double s[K];
+  s[0] = bb;
+  s[1] = rz;
+  if (CO)
+#pragma unroll
+    for (int j = 0; j < MAXK; ++j) s[2 + j] = (active && j < nk) ? (double)W[j * n + i] * (double)ri : 0.0;
+  block_sums<K>(s);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[K * blockIdx.x + k] = s[k];
   if (arrive_last(&st->counter2)) {
-    double tot[2];
-    finish_sums<2>(partials, tot);
+    double tot[K];
+    finish_sums<K>(partials, tot);
     if (threadIdx.x == 0) {
+      st->coarse_pending = 0;
+      st->counter4 = 0;
+      if (CO) tot[1] += coarse_finish(G, nk, tot + 2, st);
       double bn = sqrt(tot[0]);
       st->bnorm = bn;
       st->threshold = rel_tol * bn;
@@ -582,9 +614,9 @@ __global__ void k_pcg_start(Layout L, const double* b, TX* x, TS* r, TS* z, TS* 
 // FP64 arithmetic), z = Minv r, rz = r.z. Ends the solve when the FP64 residual
 // meets the threshold; restarts the search direction (beta = 0) when the
 // recurrence had claimed convergence but the FP64 residual disagrees.
-template <int CW, class TS>
+template <int CW, class TS, bool CO>
 __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* r, TS* z, const TS* minv,
-                               double* partials, PcgState* st) {
+                               double* partials, PcgState* st, const TS* W, const double* G, int nk) {
   if (!st->replace) return;
   const int cw = CW ? CW : L.cw;
   extern __shared__ unsigned char sh_raw[];
@@ -614,16 +646,22 @@ __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* 
     z[i] = zi;
     rz = (double)ri * (double)zi;
   }
-  double s[2] = {rr, rz};
-  block_sums<2>(s);
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = s[0];
-    partials[2 * blockIdx.x + 1] = s[1];
-  }
+  constexpr int K = CO ? 2 + MAXK : 2;
+  double s[K];
+  s[0] = rr;
+  s[1] = rz;
+  if (CO)
+#pragma unroll
+    for (int j = 0; j < MAXK; ++j) s[2 + j] = (active && j < nk) ? (double)W[j * n + i] * (double)ri : 0.0;
+  block_sums<K>(s);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[K * blockIdx.x + k] = s[k];
   if (arrive_last(&st->counter3)) {
-    double tot[2];
-    finish_sums<2>(partials, tot);
+    double tot[K];
+    finish_sums<K>(partials, tot);
     if (threadIdx.x == 0) {
+      if (CO) tot[1] += coarse_finish(G, nk, tot + 2, st);
       st->rr_last = tot[0];
       st->rr = tot[0];
       st->replacements += 1;
@@ -642,6 +680,45 @@ __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* 
       st->counter3 = 0;
     }
   }
+}
+
+// z += W c for the pending coarse coefficients (see k_update_wide); the last
+// block clears the flag after every block has read it.
+template <class TS>
+__global__ void k_coarse_add(int64_t n, int nk, const TS* W, PcgState* st, TS* z) {
+  if (!st->coarse_pending) return;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) {
+    double acc = (double)z[i];
+    for (int j = 0; j < nk; ++j) acc += (double)W[j * n + i] * st->coarse[j];
+    z[i] = (TS)acc;
+  }
+  if (arrive_last(&st->counter4)) {
+    if (threadIdx.x == 0) {
+      st->coarse_pending = 0;
+      st->counter4 = 0;
+    }
+  }
+}
+
+// W = D * basis (scaled coordinates) in f64 and in the storage type.
+template <class TS>
+__global__ void k_coarse_scale(int64_t n, int nk, const double* basis, const double* scales, double* wd, TS* wt) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n * nk) return;
+  const double v = basis[k] * scales[k % n];
+  wd[k] = v;
+  wt[k] = (TS)v;
+}
+
+// E[a][b] = W_a . (S W)_b, one block per entry.
+template <class TS>
+__global__ void k_coarse_gram(int64_t n, int nk, const double* wd, const TS* sw, double* e) {
+  const int a = blockIdx.x / nk, b = blockIdx.x % nk;
+  double v[1] = {0};
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) v[0] += wd[a * n + i] * (double)sw[b * n + i];
+  block_sums<1>(v);
+  if (threadIdx.x == 0) e[a * nk + b] = v[0];
 }
 
 }  // namespace fg

@@ -98,6 +98,15 @@ class SchurImpl final : public Backend {
   fg_gnn* learned = nullptr;
   bool learned_compared = false, learned_off = false;
   DBuf<double> d_keep;  // the learned solution while the comparison solve runs
+  // two-level PCG (opt.coarse_correction): the problem's coarse basis
+  // (unscaled), W = D * basis in f64 and storage precision, S W, and
+  // G = (W^T S W)^-1 for the current damping
+  double learned_infer_seconds = 0;  // features + network of the comparison solve
+  int nk = 0;
+  bool coarse_on = false, basis_scaled = false;
+  DBuf<double> d_basis, d_Wd, d_E, d_G;
+  DBuf<TS> d_Wt, d_SWt;
+  const void* graph_coarse[3] = {nullptr, nullptr, nullptr};  // W, G, on: what the PCG graphs captured
 
   Layout layout() const {
     Layout L;
@@ -145,6 +154,7 @@ class SchurImpl final : public Backend {
       return FG_INVALID_OPTIONS;
     }
     if (o.preconditioner != opt.preconditioner) learned_compared = learned_off = false;
+    if (!o.coarse_correction) nk = 0;
     if (o.operator_variant != opt.operator_variant) fast.tuned = false;
     int keep = dev;
     opt = o;
@@ -195,6 +205,8 @@ class SchurImpl final : public Backend {
 
   fg_status clear() override {  // src/schur.rs:432-437
     ready = false;
+    nk = 0;
+    basis_scaled = false;
     h_blocks.clear();
     h_values.clear();
     h_negres.clear();
@@ -394,6 +406,7 @@ class SchurImpl final : public Backend {
   }
 
   fg_status prepare_damping(double floor) override {  // src/schur.rs:490-526
+    basis_scaled = false;  // new column scales
     ready = false;
     EventTimer tm;
     if (opt.collect_timings) tm.start(st);
@@ -446,6 +459,155 @@ class SchurImpl final : public Backend {
     ready = true;
     FG_TRY(autotune_operator());
     if (opt.collect_timings) tim.preparation += tm.stop(st);
+    return FG_OK;
+  }
+
+  fg_status set_coarse_basis(const double* basis, int k) override {
+    if (!opt.coarse_correction || k <= 0) return FG_OK;
+    if (k > MAXK) {
+      set_error("a coarse basis holds at most 8 vectors");
+      return FG_INVALID_OPTIONS;
+    }
+    FG_TRY(d_basis.resize((size_t)k * std::max<size_t>(retained, 1)));
+    if (retained)
+      FG_CUDA(cudaMemcpyAsync(d_basis.get(), basis, (size_t)k * retained * sizeof(double), cudaMemcpyDeviceToDevice,
+                              st));
+    nk = k;
+    basis_scaled = false;
+    return FG_OK;
+  }
+
+  // W = D * basis once the column scales of this linearization exist.
+  fg_status scale_basis() {
+    if (!nk || basis_scaled || !retained) return FG_OK;
+    const size_t n = (size_t)nk * retained;
+    FG_TRY(d_Wd.resize(n));
+    FG_TRY(d_Wt.resize(n));
+    FG_TRY(d_SWt.resize(n));
+    FG_TRY(d_E.resize(MAXK * MAXK));
+    FG_TRY(d_G.resize(MAXK * MAXK));
+    FG_LAUNCH(k_coarse_scale<TS>, grid_for(n, 256), 256, 0, st, (int64_t)retained, nk, d_basis.get(), d_scales.get(),
+              d_Wd.get(), d_Wt.get());
+    basis_scaled = true;
+    return FG_OK;
+  }
+
+  // G = (W^T S W)^-1 at lambda (nk reduced-operator applications); the
+  // two-level preconditioner stays off for this solve if W^T S W is not SPD,
+  // and above COARSE_MAX_DAMPING, where damping has already lifted the coarse
+  // modes into the block-Jacobi bulk (measured on BAL: 10 -> 13 iterations at
+  // lambda = 1, 50 -> 22 at 1e-4).
+  static constexpr double COARSE_MAX_DAMPING = 0.1;
+  fg_status prepare_coarse(double lambda) {
+    coarse_on = false;
+    if (!opt.coarse_correction || !nk || !retained || lambda > COARSE_MAX_DAMPING) return sync_graph_coarse();
+    FG_TRY(scale_basis());
+    // S W in the storage precision (the operator the PCG itself applies); the
+    // Gram W^T (S W) accumulates in f64
+    for (int j = 0; j < nk; ++j) {
+      PView<TS> pv{d_Wt.get() + (size_t)j * retained, nullptr, nullptr};
+      FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_SWt.get() + (size_t)j * retained, nullptr,
+                               nullptr));
+    }
+    FG_LAUNCH(k_coarse_gram<TS>, (unsigned)(nk * nk), 256, 0, st, (int64_t)retained, nk, d_Wd.get(),
+              (const TS*)d_SWt.get(), d_E.get());
+    double E[MAXK * MAXK], Lm[MAXK * MAXK] = {0}, G[MAXK * MAXK];
+    FG_CUDA(cudaMemcpyAsync(E, d_E.get(), (size_t)nk * nk * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    // Cholesky of the symmetrized E, then G = E^-1 column by column
+    for (int j = 0; j < nk; ++j) {
+      for (int i = j; i < nk; ++i) {
+        double v = 0.5 * (E[i * nk + j] + E[j * nk + i]);
+        for (int k = 0; k < j; ++k) v -= Lm[i * nk + k] * Lm[j * nk + k];
+        if (i == j) {
+          if (!(v > 0) || !std::isfinite(v)) return sync_graph_coarse();
+          Lm[j * nk + j] = std::sqrt(v);
+        } else {
+          Lm[i * nk + j] = v / Lm[j * nk + j];
+        }
+      }
+    }
+    for (int c = 0; c < nk; ++c) {
+      double y[MAXK];
+      for (int i = 0; i < nk; ++i) {
+        double v = i == c ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) v -= Lm[i * nk + k] * y[k];
+        y[i] = v / Lm[i * nk + i];
+      }
+      for (int i = nk - 1; i >= 0; --i) {
+        double v = y[i];
+        for (int k = i + 1; k < nk; ++k) v -= Lm[k * nk + i] * G[k * nk + c];
+        G[i * nk + c] = v / Lm[i * nk + i];
+      }
+    }
+    FG_CUDA(cudaMemcpyAsync(d_G.get(), G, (size_t)nk * nk * sizeof(double), cudaMemcpyHostToDevice, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    coarse_on = true;
+    return sync_graph_coarse();
+  }
+  // The PCG graphs bake in the kernel variants and the W / G pointers.
+  fg_status sync_graph_coarse() {
+    const void* now[3] = {coarse_on ? (const void*)d_Wt.get() : nullptr, coarse_on ? (const void*)d_G.get() : nullptr,
+                          coarse_on ? (const void*)this : nullptr};
+    if (now[0] != graph_coarse[0] || now[1] != graph_coarse[1] || now[2] != graph_coarse[2]) {
+      drop_graphs();
+      for (int k = 0; k < 3; ++k) graph_coarse[k] = now[k];
+    }
+    return FG_OK;
+  }
+
+  template <class TX>
+  fg_status launch_start(const double* b, TX* x, double rel_tol) {
+    Layout L = layout();
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
+    PcgState* ps = d_pcg.get();
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      if (coarse_on)
+        FG_LAUNCH((k_pcg_start<CW_, TS, TX, true>), gw, bw, shm, st, L, b, x, d_r.get(), d_z.get(), d_pp.get(),
+                  d_minv.get(), d_partials.get(), ps, rel_tol, (const TS*)d_Wt.get(), (const double*)d_G.get(), nk);
+      else
+        FG_LAUNCH((k_pcg_start<CW_, TS, TX, false>), gw, bw, shm, st, L, b, x, d_r.get(), d_z.get(), d_pp.get(),
+                  d_minv.get(), d_partials.get(), ps, rel_tol, (const TS*)nullptr, (const double*)nullptr, 0);
+    });
+    return launch_coarse_add();
+  }
+  template <class TX, bool MIXED>
+  fg_status launch_update(TX* x) {
+    Layout L = layout();
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
+    PcgState* ps = d_pcg.get();
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      if (coarse_on)
+        FG_LAUNCH((k_update_wide<CW_, TS, TX, MIXED, true>), gw, bw, shm, st, L, x, d_r.get(), d_z.get(), d_pp.get(),
+                  d_q.get(), d_minv.get(), d_partials.get(), ps, (const TS*)d_Wt.get(), (const double*)d_G.get(), nk);
+      else
+        FG_LAUNCH((k_update_wide<CW_, TS, TX, MIXED, false>), gw, bw, shm, st, L, x, d_r.get(), d_z.get(),
+                  d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps, (const TS*)nullptr,
+                  (const double*)nullptr, 0);
+    });
+    return launch_coarse_add();
+  }
+  fg_status launch_replace() {
+    Layout L = layout();
+    const unsigned bw = wide_block(), gw = wide_grid();
+    const size_t shm = bw * sizeof(TS);
+    PcgState* ps = d_pcg.get();
+    FG_DISPATCH_WIDTHS(cw, pw, {
+      if (coarse_on)
+        FG_LAUNCH((k_replace_wide<CW_, TS, true>), gw, bw, shm, st, L, d_rhs.get(), d_qd.get(), d_r.get(), d_z.get(),
+                  d_minv.get(), d_partials.get(), ps, (const TS*)d_Wt.get(), (const double*)d_G.get(), nk);
+      else
+        FG_LAUNCH((k_replace_wide<CW_, TS, false>), gw, bw, shm, st, L, d_rhs.get(), d_qd.get(), d_r.get(),
+                  d_z.get(), d_minv.get(), d_partials.get(), ps, (const TS*)nullptr, (const double*)nullptr, 0);
+    });
+    return launch_coarse_add();
+  }
+  fg_status launch_coarse_add() {
+    if (coarse_on)
+      FG_LAUNCH(k_coarse_add<TS>, grid_for(retained, 256), 256, 0, st, (int64_t)retained, nk, (const TS*)d_Wt.get(),
+                d_pcg.get(), d_z.get());
     return FG_OK;
   }
 
@@ -502,9 +664,12 @@ class SchurImpl final : public Backend {
     }
     if (*fallbacks == 0 && nC) FG_TRY(write_block_inverses(lambda));
     if (*fallbacks == 0 && nC && learned_blocks) {
+      EventTimer ti;
+      if (!learned_compared) ti.start(st);
       FG_TRY(ensure_cross());
       unsigned nonfinite = 0;
       FG_TRY(gnn_precondition(learned, view_at(lambda), d_minv.get(), st, &nonfinite));
+      if (!learned_compared) learned_infer_seconds = ti.stop(st);
     }
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
     return FG_OK;
@@ -677,15 +842,9 @@ class SchurImpl final : public Backend {
     PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
     FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps, nullptr, &ps->lambda));
     if (!mixed) {
-      FG_DISPATCH_WIDTHS(cw, pw, {
-        FG_LAUNCH((k_update_wide<CW_, TS, TS, false>), gw, bw, shm, st, L, d_x.get(), d_r.get(), d_z.get(),
-                  d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
-      });
+      FG_TRY((launch_update<TS, false>(d_x.get())));
     } else {
-      FG_DISPATCH_WIDTHS(cw, pw, {
-        FG_LAUNCH((k_update_wide<CW_, TS, double, true>), gw, bw, shm, st, L, xd, d_r.get(), d_z.get(),
-                  d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
-      });
+      FG_TRY((launch_update<double, true>(xd)));
       if ((k & 3) == 3) FG_TRY(replacement(lambda, xd, ps));
     }
     return FG_OK;
@@ -732,12 +891,7 @@ class SchurImpl final : public Backend {
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
       FG_CUDA(cudaStreamSynchronize(st));
     }
-    const unsigned bw = wide_block(), gw = wide_grid();
-    const size_t shm = bw * sizeof(TS);
-    FG_DISPATCH_WIDTHS(cw, pw, {
-      FG_LAUNCH((k_pcg_start<CW_, TS, TS>), gw, bw, shm, st, L, b, d_x.get(), d_r.get(), d_z.get(), d_pp.get(),
-                d_minv.get(), d_partials.get(), ps, rel_tol);
-    });
+    FG_TRY(launch_start<TS>(b, d_x.get(), rel_tol));
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
     const bool graphed = fast.enabled();
@@ -754,10 +908,7 @@ class SchurImpl final : public Backend {
       for (size_t k = 0; k < batch; ++k) {
         PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
         FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
-        FG_DISPATCH_WIDTHS(cw, pw, {
-          FG_LAUNCH((k_update_wide<CW_, TS, TS, false>), gw, bw, shm, st, L, d_x.get(), d_r.get(), d_z.get(),
-                    d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
-        });
+        FG_TRY((launch_update<TS, false>(d_x.get())));
       }
       launched += batch;
       batch = std::min<size_t>(batch * 2, 64);
@@ -794,37 +945,45 @@ class SchurImpl final : public Backend {
     FG_TRY(launch_neg_scaled_gradient());
     FG_TRY(launch_point_solve(lambda));
     FG_TRY(launch_rhs());
+    FG_TRY(prepare_coarse(lambda));
+    diag.coarse_vectors = coarse_on ? (size_t)nk : 0;
     if (opt.collect_timings) { tim.factorization += tf.stop(st); tl.start(st); }
 
     unsigned its = 0;
     int term = FG_TERM_NONE;
     double est = 0;
     size_t refinements = 0;
+    const bool compare = use_learned && !learned_compared;
+    EventTimer tc;
+    if (compare) tc.start(st);
     FG_TRY(run_cg(lambda, &its, &term, &est, &refinements));
+    if (compare) diag.learned_seconds = learned_infer_seconds + tc.stop(st);
     diag.preconditioner_used = use_learned ? FG_PRECOND_LEARNED : opt.preconditioner;
     if (use_learned) {
-      // Block-Jacobi stays the judge: it takes over when the learned PCG
-      // fails, and the first learned solve is compared against it once.
+      // Block-Jacobi stays the yardstick: it takes over when the learned PCG
+      // fails, and the first learned solve is compared against it once, on
+      // iterations and on device time including the network's inference.
       diag.learned_iterations = its;
-      const bool compare = !learned_compared;
       if (term != FG_TERM_CONVERGED || compare) {
         const bool keep = term == FG_TERM_CONVERGED;
         if (keep) {
           FG_TRY(d_keep.resize(std::max<size_t>(retained, 1)));
           FG_CUDA(cudaMemcpyAsync(d_keep.get(), d_zred.get(), retained * sizeof(double), cudaMemcpyDeviceToDevice, st));
         }
+        if (compare) tc.start(st);
         FG_TRY(write_block_inverses(lambda));
         unsigned its2 = 0;
         int term2 = FG_TERM_NONE;
         double est2 = 0;
         size_t ref2 = 0;
         FG_TRY(run_cg(lambda, &its2, &term2, &est2, &ref2));
+        if (compare) diag.block_jacobi_seconds = tc.stop(st);
         diag.block_jacobi_iterations = its2;
         if (!keep) {
           diag.learned_fallback = 1;
         } else {
           learned_compared = true;
-          if (term2 == FG_TERM_CONVERGED && its2 < its) {
+          if (term2 == FG_TERM_CONVERGED && (its2 < its || diag.block_jacobi_seconds < diag.learned_seconds)) {
             learned_off = true;
             diag.learned_fallback = 2;
           } else {
@@ -899,12 +1058,7 @@ class SchurImpl final : public Backend {
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
       FG_CUDA(cudaStreamSynchronize(st));
     }
-    const unsigned bw = wide_block(), gw = wide_grid();
-    const size_t shm = bw * sizeof(TS);
-    FG_DISPATCH_WIDTHS(cw, pw, {
-      FG_LAUNCH((k_pcg_start<CW_, TS, double>), gw, bw, shm, st, L, d_rhs.get(), xd, d_r.get(), d_z.get(),
-                d_pp.get(), d_minv.get(), d_partials.get(), ps, opt.relative_tolerance);
-    });
+    FG_TRY(launch_start<double>(d_rhs.get(), xd, opt.relative_tolerance));
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
     const size_t max_iters = opt.max_iterations;
@@ -922,10 +1076,7 @@ class SchurImpl final : public Backend {
       for (size_t k = 0; k < batch; ++k) {
         PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
         FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps));
-        FG_DISPATCH_WIDTHS(cw, pw, {
-          FG_LAUNCH((k_update_wide<CW_, TS, double, true>), gw, bw, shm, st, L, xd, d_r.get(), d_z.get(),
-                    d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps);
-        });
+        FG_TRY((launch_update<double, true>(xd)));
         if ((k & 3) == 3) FG_TRY(replacement(lambda, xd, ps));
       }
       launched += batch;
@@ -950,11 +1101,7 @@ class SchurImpl final : public Backend {
     PView<double> xv{xd, nullptr, nullptr};
     FG_TRY(apply_reduced<double>(xv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr, &ps->replace,
                                  &ps->lambda));
-    FG_DISPATCH_WIDTHS(cw, pw, {
-      FG_LAUNCH((k_replace_wide<CW_, TS>), gw, bw, shm, st, L, d_rhs.get(), d_qd.get(), d_r.get(), d_z.get(),
-                d_minv.get(), d_partials.get(), ps);
-    });
-    return FG_OK;
+    return launch_replace();
   }
 
   // ---- kernels launched by solve_damped (defined below as members)

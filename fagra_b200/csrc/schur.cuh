@@ -30,6 +30,11 @@ struct PcgState {
   int replace;             // 1: an FP64 residual replacement is due
   unsigned iterations, max_iterations, replacements;
   unsigned counter0, counter1, counter2, counter3;
+  // two-level preconditioner: c = G W^T r of the last z update, pending until
+  // k_coarse_add has added W c to z
+  double coarse[8];
+  int coarse_pending;
+  unsigned counter4;
 };
 struct VerifyState {
   double jd2;        // ||J delta||^2
@@ -90,6 +95,10 @@ class Backend {
     set_error("this backend keeps no linearized model");
     return FG_UNSUPPORTED_STRUCTURE;
   }
+  // A device problem's coarse basis for two-level PCG (k vectors of the
+  // retained length, row j at basis + j * retained, unscaled coordinates);
+  // backends that do not use one ignore it.
+  virtual fg_status set_coarse_basis(const double*, int) { return FG_OK; }
   // Schur-only extras.
   virtual fg_status set_options(const fg_schur_options&) { return not_schur(); }
   virtual void diagnostics(fg_schur_diagnostics* d) const { *d = fg_schur_diagnostics{}; }

@@ -86,6 +86,9 @@ typedef struct {
                                   residual b - S x each time it falls by this factor; default 1e-2 */
   int operator_variant;        /* FP32 BAL-shaped systems: 0 = autotune (default), 1..3 = force the
                                   reduced-operator variant of fg_schur_operator_info */
+  int coarse_correction;       /* 1: two-level PCG, z = M r + W (W^T S W)^-1 W^T r with the coarse
+                                  basis W a device problem supplies (BAL: the 7 similarity-gauge
+                                  directions of the cameras); 0 (default): the reference's PCG */
 } fg_schur_options;
 
 /* src/schur.rs:44-60 SchurDiagnostics (has_* = Some) */
@@ -102,11 +105,15 @@ typedef struct {
   /* FG_PRECOND_LEARNED only (no reference counterpart): the preconditioner
    * whose step was kept, 0 when the learned PCG ran without a fallback, 1
    * when it met non-positive curvature or did not converge, 2 when the
-   * block-Jacobi comparison solve needed fewer iterations (the learned
+   * block-Jacobi comparison solve needed fewer iterations or less device time
+   * than the learned solve plus the network's inference (the learned
    * preconditioner is then switched off for this backend); iteration counts
-   * of the two solves of this attempt (0 when not run). `iterations` is their sum. */
+   * of the two solves of this attempt (0 when not run), and the device
+   * seconds of the comparison. `iterations` is their sum. */
   int preconditioner_used, learned_fallback;
   size_t learned_iterations, block_jacobi_iterations;
+  double learned_seconds, block_jacobi_seconds;
+  size_t coarse_vectors; /* coarse basis size used by this attempt's PCG (0: one-level) */
 } fg_schur_diagnostics;
 
 /* src/schur.rs:75-91 SchurTimings, seconds, device event time. */
