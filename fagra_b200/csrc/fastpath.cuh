@@ -661,6 +661,157 @@ __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, c
   }
 }
 
+// Coarse Galerkin matrix of the two-level PCG in one pass over the edge
+// records: E(lambda) = W^T S W with S = lambda I + B - E C^-1 E^T, computed as
+//   lambda W^T W + sum_cam W_cam^T B_cam W_cam           (k_coarse_cams)
+//   - sum_p u_p^T C_p^-1 u_p, u_p = sum_{e in p} E_e^T W_cam(e)   (k_coarse_points)
+// instead of nk operator applications. k_coarse_points runs one thread per
+// point over its point-major records (no cross-lane traffic); W is staged
+// camera-major with a row stride of ws floats (a multiple of 4):
+// wc[cam * ws + a * 9 + c]. out: nk x nk, accumulated with atomics (zeroed by
+// the caller).
+constexpr int COARSE_THREADS = 256;
+template <class TS>
+__device__ __forceinline__ void coarse_record(const TS* rec, float (&E)[28]);
+template <>
+__device__ __forceinline__ void coarse_record<float>(const float* rec, float (&E)[28]) {
+  const float4* v = reinterpret_cast<const float4*>(rec);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    const float4 a = __ldg(v + i);
+    E[4 * i] = a.x; E[4 * i + 1] = a.y; E[4 * i + 2] = a.z; E[4 * i + 3] = a.w;
+  }
+}
+template <>
+__device__ __forceinline__ void coarse_record<double>(const double* rec, float (&E)[28]) {
+  const double2* v = reinterpret_cast<const double2*>(rec);
+#pragma unroll
+  for (int i = 0; i < 14; ++i) {
+    const double2 a = __ldg(v + i);
+    E[2 * i] = (float)a.x; E[2 * i + 1] = (float)a.y;
+  }
+}
+template <class TS, int NK>
+__global__ void __launch_bounds__(COARSE_THREADS)
+    k_coarse_points(int64_t npts, const int64_t* pt_off, const TS* erec, const TS* prec, const float* wc, int ws,
+                    double* out) {
+  const int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  constexpr int NL = NK * (NK + 1) / 2;
+  double acc[NL];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) acc[k] = 0;
+  if (pt < npts) {
+    float u[NK][3];
+#pragma unroll
+    for (int a = 0; a < NK; ++a) u[a][0] = u[a][1] = u[a][2] = 0.f;
+    for (int64_t e = pt_off[pt]; e < pt_off[pt + 1]; ++e) {
+      float E[28];
+      coarse_record<TS>(erec + e * 28, E);
+      typename RecWord<TS>::U word;
+      memcpy(&word, erec + e * 28 + 27, sizeof(word));
+      const float4* wv = reinterpret_cast<const float4*>(wc + (int64_t)RecWord<TS>::cam(word) * ws);
+      float x[(NK * 9 + 3) / 4 * 4];
+#pragma unroll
+      for (int i = 0; i < (NK * 9 + 3) / 4; ++i) {
+        const float4 a = __ldg(wv + i);
+        x[4 * i] = a.x; x[4 * i + 1] = a.y; x[4 * i + 2] = a.z; x[4 * i + 3] = a.w;
+      }
+#pragma unroll
+      for (int a = 0; a < NK; ++a)
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          float v = 0.f;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) v += E[p * 9 + c] * x[a * 9 + c];
+          u[a][p] += v;
+        }
+    }
+    const TS* r = prec + pt * 8;
+    const double c00 = r[0], c10 = r[1], c20 = r[2], c11 = r[3], c21 = r[4], c22 = r[5];
+    int idx = 0;
+#pragma unroll
+    for (int a = 0; a < NK; ++a) {
+      const double t0 = c00 * u[a][0] + c10 * u[a][1] + c20 * u[a][2];
+      const double t1 = c10 * u[a][0] + c11 * u[a][1] + c21 * u[a][2];
+      const double t2 = c20 * u[a][0] + c21 * u[a][1] + c22 * u[a][2];
+#pragma unroll
+      for (int b = 0; b <= a; ++b) acc[idx++] += (double)u[b][0] * t0 + (double)u[b][1] * t1 + (double)u[b][2] * t2;
+    }
+  }
+  __shared__ double sh[COARSE_THREADS / 32][NL];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[w][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NL) {
+    double v = 0;
+    for (int q = 0; q < COARSE_THREADS / 32; ++q) v += sh[q][threadIdx.x];
+    int a = 0, k = threadIdx.x;
+    while (k > a) k -= ++a;  // packed lower index -> (a, b = k)
+    atomicAdd(out + a * NK + k, -v);
+    if (a != k) atomicAdd(out + k * NK + a, -v);
+  }
+}
+
+// Camera part of the coarse matrix (thread per camera) and the camera-major
+// copy of W used by k_coarse_points. B_cam: the normalized Gram block (lower,
+// column major), wd: W row-major (nk x n).
+template <class TS>
+__global__ void k_coarse_cams(int64_t ncam, int nk, const double* wd, const TS* gram, const uint8_t* observed,
+                              double lambda, float* wc, int ws, double* out) {
+  const int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t n = ncam * 9;
+  double part[36];
+  for (int k = 0; k < 36; ++k) part[k] = 0;
+  if (cam < ncam) {
+    const TS* g = gram + cam * 81;
+    double w[8][9];
+    for (int a = 0; a < nk; ++a)
+      for (int c = 0; c < 9; ++c) {
+        w[a][c] = wd[a * n + cam * 9 + c];
+        wc[cam * ws + a * 9 + c] = (float)w[a][c];
+      }
+    for (int a = 0; a < nk; ++a) {
+      double bw[9];  // B w_a (B symmetric from its lower triangle)
+      for (int r = 0; r < 9; ++r) {
+        double v = 0;
+        if (observed[cam])
+          for (int c = 0; c < 9; ++c) v += (double)(r >= c ? g[c * 9 + r] : g[r * 9 + c]) * w[a][c];
+        bw[r] = v + lambda * w[a][r];
+      }
+      for (int b = 0; b <= a; ++b) {
+        double v = 0;
+        for (int r = 0; r < 9; ++r) v += w[b][r] * bw[r];
+        part[a * (a + 1) / 2 + b] = v;
+      }
+    }
+  }
+  __shared__ double sh[8][36];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int nl = nk * (nk + 1) / 2;
+  for (int k = 0; k < nl; ++k) {
+    double v = part[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[wp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int a = 0; a < nk; ++a)
+      for (int b = 0; b <= a; ++b) {
+        double v = 0;
+        for (int q = 0; q < nw; ++q) v += sh[q][a * (a + 1) / 2 + b];
+        atomicAdd(out + a * nk + b, v);
+        if (a != b) atomicAdd(out + b * nk + a, v);
+      }
+  }
+}
+
 template <class TS>
 struct FastPath {
   bool on = false;          // records are current and the shape qualifies
@@ -735,6 +886,25 @@ struct FastPath {
     if (d_parts_f.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
     if (d_parts_d.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
     return true;
+  }
+
+  // The coarse Galerkin matrix W^T S(lambda) W in two passes (cameras, then
+  // edges), nk <= 8 coarse vectors; out (device, nk x nk) is overwritten.
+  DBuf<float> d_wc;
+  // Only the 7-vector similarity gauge of BAL takes this path.
+  template <class Impl>
+  fg_status coarse_gram(Impl& s, double lambda, const double* wd, int nk, double* out) {
+    if (nk != 7) return FG_UNSUPPORTED_STRUCTURE;
+    constexpr int NK = 7, WS = (NK * 9 + 3) / 4 * 4;
+    FG_TRY(d_wc.resize((size_t)s.nC * WS));
+    FG_CUDA(cudaMemsetAsync(d_wc.get(), 0, (size_t)s.nC * WS * sizeof(float), s.st));
+    FG_CUDA(cudaMemsetAsync(out, 0, (size_t)nk * nk * sizeof(double), s.st));
+    FG_LAUNCH(k_coarse_cams<TS>, grid_for(s.nC, 256), 256, 0, s.st, (int64_t)s.nC, nk, wd, s.d_gram.get(),
+              s.d_observed.get(), lambda, d_wc.get(), WS, out);
+    FG_LAUNCH((k_coarse_points<TS, NK>), grid_for(s.nP, COARSE_THREADS), COARSE_THREADS, 0, s.st, (int64_t)s.nP,
+              s.d_pt_edge_off.get(), (const TS*)d_erec.get(), (const TS*)d_prec.get(), (const float*)d_wc.get(), WS,
+              out);
+    return FG_OK;
   }
 
   // After each block factorization: refresh C^-1 in the point records.

@@ -502,15 +502,20 @@ class SchurImpl final : public Backend {
     coarse_on = false;
     if (!opt.coarse_correction || !nk || !retained || lambda > COARSE_MAX_DAMPING) return sync_graph_coarse();
     FG_TRY(scale_basis());
-    // S W in the storage precision (the operator the PCG itself applies); the
-    // Gram W^T (S W) accumulates in f64
-    for (int j = 0; j < nk; ++j) {
-      PView<TS> pv{d_Wt.get() + (size_t)j * retained, nullptr, nullptr};
-      FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_SWt.get() + (size_t)j * retained, nullptr,
-                               nullptr));
+    if (fast.enabled() && nk == 7) {
+      // one pass over the edge records (BAL shape, the 7 gauge vectors)
+      FG_TRY(fast.coarse_gram(*this, lambda, d_Wd.get(), nk, d_E.get()));
+    } else {
+      // S W in the storage precision (the operator the PCG itself applies);
+      // the Gram W^T (S W) accumulates in f64
+      for (int j = 0; j < nk; ++j) {
+        PView<TS> pv{d_Wt.get() + (size_t)j * retained, nullptr, nullptr};
+        FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_SWt.get() + (size_t)j * retained, nullptr,
+                                 nullptr));
+      }
+      FG_LAUNCH(k_coarse_gram<TS>, (unsigned)(nk * nk), 256, 0, st, (int64_t)retained, nk, d_Wd.get(),
+                (const TS*)d_SWt.get(), d_E.get());
     }
-    FG_LAUNCH(k_coarse_gram<TS>, (unsigned)(nk * nk), 256, 0, st, (int64_t)retained, nk, d_Wd.get(),
-              (const TS*)d_SWt.get(), d_E.get());
     double E[MAXK * MAXK], Lm[MAXK * MAXK] = {0}, G[MAXK * MAXK];
     FG_CUDA(cudaMemcpyAsync(E, d_E.get(), (size_t)nk * nk * sizeof(double), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
@@ -1053,7 +1058,7 @@ class SchurImpl final : public Backend {
       PcgState init{};
       init.max_iterations = (unsigned)std::min<size_t>(opt.max_iterations, 0xffffffffu);
       init.lambda = lambda;
-      double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-2;
+      double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-3;
       init.delta2 = d * d;
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
       FG_CUDA(cudaStreamSynchronize(st));

@@ -31,54 +31,70 @@ __device__ __forceinline__ void block_allsums(double (&v)[N], double* sh /* >= 3
 
 // One block per retained variable: raw column norms (hypot chain of
 // src/linear_model.rs:217-224), floored scales, and the normalized Gram block
-// (block_factors.rs:87-99), all from the variable's blocks.
+// (block_factors.rs:87-99), all from the variable's blocks in ONE pass: the raw
+// Gram sum_i J_i^T J_i is accumulated and normalized afterwards,
+// G_rc = raw_rc / (d_r d_c), its diagonal giving the squared column norms.
+// Each thread walks four of the variable's blocks at a time so four
+// index -> block -> value load chains are in flight.
 template <int CW, class TS>
 __global__ void k_cam_scales_gram(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
                                   const TS* values, double floor, double* scales, TS* gram, int* bad) {
   constexpr int CM = CW ? CW : MAXW;
   constexpr int NL = CM * (CM + 1) / 2;
+  constexpr int U = 4;
   const int cw = CW ? CW : L.cw;
   __shared__ double sh[32 * NL];
   const int64_t cam = blockIdx.x;
   if (cam >= L.nC) return;
   const int64_t b0 = var_off[cam], b1 = var_off[cam + 1];
-  double sq[CM];
-  for (int c = 0; c < CM; ++c) sq[c] = 0;
-  for (int64_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
-    DBlockMeta b = blocks[var_blk[k]];
-    for (int c = 0; c < cw; ++c)
-      for (int i = 0; i < b.rows; ++i) {
-        double v = (double)values[b.start + (int64_t)c * b.rows + i];
-        sq[c] += v * v;
-      }
-  }
-  block_allsums<CM>(sq, sh);
-  double inv[CM];
-  for (int c = 0; c < cw; ++c) {
-    double raw = sqrt(sq[c]);
-    if (!isfinite(raw) && threadIdx.x == 0) atomicOr(bad, 1);
-    double d = fmax(raw, floor);
-    inv[c] = 1.0 / d;
-    if (threadIdx.x == 0) scales[cam * cw + c] = d;
-  }
   double acc[NL];
+#pragma unroll
   for (int k = 0; k < NL; ++k) acc[k] = 0;
-  for (int64_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
-    DBlockMeta b = blocks[var_blk[k]];
-    for (int i = 0; i < b.rows; ++i) {
-      double jv[CM];
-      for (int c = 0; c < cw; ++c) jv[c] = (double)values[b.start + (int64_t)c * b.rows + i] * inv[c];
-      int idx = 0;
-      for (int c = 0; c < cw; ++c)
-        for (int r = c; r < cw; ++r) acc[idx++] += jv[c] * jv[r];
+  for (int64_t k0 = b0 + threadIdx.x; k0 < b1; k0 += U * (int64_t)blockDim.x) {
+    DBlockMeta bm[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t k = k0 + u * (int64_t)blockDim.x;
+      if (k < b1) bm[u] = blocks[var_blk[k]];
+      else bm[u].rows = 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      for (int i = 0; i < bm[u].rows; ++i) {
+        double jv[CM];
+#pragma unroll
+        for (int c = 0; c < CM; ++c)
+          jv[c] = c < cw ? (double)values[bm[u].start + (int64_t)c * bm[u].rows + i] : 0.0;
+        int idx = 0;
+#pragma unroll
+        for (int c = 0; c < CM; ++c)
+#pragma unroll
+          for (int r = c; r < CM; ++r) acc[idx++] += jv[c] * jv[r];
+      }
     }
   }
   block_allsums<NL>(acc, sh);
-  TS* g = gram + L.gram_offset(cam);
+  double d[CM];
   int idx = 0;
-  for (int c = 0; c < cw; ++c)
-    for (int r = c; r < cw; ++r) {
-      if (threadIdx.x == (idx & (blockDim.x - 1))) g[c * cw + r] = (TS)acc[idx];
+#pragma unroll
+  for (int c = 0; c < CM; ++c) {
+    if (c < cw) {
+      const double raw = sqrt(acc[idx]);  // diagonal entry (c, c)
+      if (!isfinite(raw) && threadIdx.x == 0) atomicOr(bad, 1);
+      d[c] = fmax(raw, floor);
+      if (threadIdx.x == 0) scales[cam * cw + c] = d[c];
+    } else {
+      d[c] = 1.0;
+    }
+    idx += CM - c;
+  }
+  TS* g = gram + L.gram_offset(cam);
+  idx = 0;
+#pragma unroll
+  for (int c = 0; c < CM; ++c)
+#pragma unroll
+    for (int r = c; r < CM; ++r) {
+      if (c < cw && r < cw && threadIdx.x == (idx & (blockDim.x - 1))) g[c * cw + r] = (TS)(acc[idx] / (d[c] * d[r]));
       ++idx;
     }
 }
