@@ -213,11 +213,27 @@ __global__ void k_bal_cost(int64_t no, const uint32_t* oc, const uint32_t* op, c
     partials[3 * blockIdx.x + 2] = bad;
   }
   if (arrive_last(counter)) {
+    // the last block folds the per-block partials: thread-strided in
+    // double-double, then the same fixed shuffle / shared-memory tree
+    double H = 0, Lo = 0, B = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+      dd_add(H, Lo, ((volatile double*)partials)[3 * b], ((volatile double*)partials)[3 * b + 1]);
+      B = fmax(B, ((volatile double*)partials)[3 * b + 2]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double h2 = __shfl_down_sync(0xffffffffu, H, o), l2 = __shfl_down_sync(0xffffffffu, Lo, o);
+      double b2 = __shfl_down_sync(0xffffffffu, B, o);
+      dd_add(H, Lo, h2, l2);
+      B = fmax(B, b2);
+    }
+    __syncthreads();
+    if (lane == 0) { sh[warp][0] = H; sh[warp][1] = Lo; sh[warp][2] = B; }
+    __syncthreads();
     if (threadIdx.x == 0) {
-      double H = 0, Lo = 0, B = 0;
-      for (unsigned b = 0; b < gridDim.x; ++b) {
-        dd_add(H, Lo, ((volatile double*)partials)[3 * b], ((volatile double*)partials)[3 * b + 1]);
-        B = fmax(B, ((volatile double*)partials)[3 * b + 2]);
+      int nw = (blockDim.x + 31) >> 5;
+      for (int w = 1; w < nw; ++w) {
+        dd_add(H, Lo, sh[w][0], sh[w][1]);
+        B = fmax(B, sh[w][2]);
       }
       out[0] = H + Lo;
       out[1] = B;

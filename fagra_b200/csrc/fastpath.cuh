@@ -899,7 +899,7 @@ struct FastPath {
     FG_TRY(d_wc.resize((size_t)s.nC * WS));
     FG_CUDA(cudaMemsetAsync(d_wc.get(), 0, (size_t)s.nC * WS * sizeof(float), s.st));
     FG_CUDA(cudaMemsetAsync(out, 0, (size_t)nk * nk * sizeof(double), s.st));
-    FG_LAUNCH(k_coarse_cams<TS>, grid_for(s.nC, 256), 256, 0, s.st, (int64_t)s.nC, nk, wd, s.d_gram.get(),
+    FG_LAUNCH(k_coarse_cams<TS>, grid_for(s.nC, 32), 32, 0, s.st, (int64_t)s.nC, nk, wd, s.d_gram.get(),
               s.d_observed.get(), lambda, d_wc.get(), WS, out);
     FG_LAUNCH((k_coarse_points<TS, NK>), grid_for(s.nP, COARSE_THREADS), COARSE_THREADS, 0, s.st, (int64_t)s.nP,
               s.d_pt_edge_off.get(), (const TS*)d_erec.get(), (const TS*)d_prec.get(), (const float*)d_wc.get(), WS,

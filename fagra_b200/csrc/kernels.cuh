@@ -158,12 +158,21 @@ __global__ void k_norm_inf(int64_t n, const T* x, double* partials, unsigned* co
     partials[2 * blockIdx.x + 1] = bad;
   }
   if (arrive_last(counter)) {
+    double M = 0, B = 0;  // thread-strided over the partials, then a block max
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+      M = fmax(M, ((volatile double*)partials)[2 * b]);
+      B = fmax(B, ((volatile double*)partials)[2 * b + 1]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      M = fmax(M, __shfl_down_sync(0xffffffffu, M, o));
+      B = fmax(B, __shfl_down_sync(0xffffffffu, B, o));
+    }
+    __syncthreads();
+    if (lane == 0) { sm[warp] = M; sb[warp] = B; }
+    __syncthreads();
     if (threadIdx.x == 0) {
-      double M = 0, B = 0;
-      for (unsigned b = 0; b < gridDim.x; ++b) {
-        M = fmax(M, ((volatile double*)partials)[2 * b]);
-        B = fmax(B, ((volatile double*)partials)[2 * b + 1]);
-      }
+      int nw = (blockDim.x + 31) >> 5;
+      for (int w = 1; w < nw; ++w) { M = fmax(M, sm[w]); B = fmax(B, sb[w]); }
       out[0] = M;
       out[1] = B;
       *counter = 0;

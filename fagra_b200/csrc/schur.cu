@@ -102,6 +102,9 @@ class SchurImpl final : public Backend {
   // (unscaled), W = D * basis in f64 and storage precision, S W, and
   // G = (W^T S W)^-1 for the current damping
   double learned_infer_seconds = 0;  // features + network of the comparison solve
+  // the FP32 solve ended on an FP64 replacement residual of the z in d_zred
+  // (h_pcg holds it), so verification need not recompute S z - b
+  bool final_residual_known = false;
   int nk = 0;
   bool coarse_on = false, basis_scaled = false;
   DBuf<double> d_basis, d_Wd, d_E, d_G;
@@ -994,6 +997,7 @@ class SchurImpl final : public Backend {
           } else {
             FG_CUDA(cudaMemcpyAsync(d_zred.get(), d_keep.get(), retained * sizeof(double), cudaMemcpyDeviceToDevice,
                                     st));
+            final_residual_known = false;  // h_pcg describes the block-Jacobi solve
             term2 = term;
             est2 = est;
             ref2 = refinements;
@@ -1035,6 +1039,7 @@ class SchurImpl final : public Backend {
   // One reduced solve with the inverses currently in d_minv; the solution
   // lands in d_zred (f64).
   fg_status run_cg(double lambda, unsigned* its, int* term, double* est, size_t* refinements) {
+    final_residual_known = false;
     if (std::is_same<TS, double>::value) {
       FG_TRY(pcg(d_rhs.get(), lambda, opt.relative_tolerance, opt.max_iterations, its, term, est));
       FG_TRY(launch_widen(d_x.get(), d_zred.get(), retained));
@@ -1095,6 +1100,7 @@ class SchurImpl final : public Backend {
     *term_out = h.done == 1 ? h.termination : FG_TERM_ITERATION_LIMIT;
     *est_out = h.bnorm > 0 ? std::sqrt(h.rr_last) / h.bnorm : 0.0;
     *rounds = h.replacements;
+    final_residual_known = h.done == 1 && h.termination == FG_TERM_CONVERGED;
     return FG_OK;
   }
 

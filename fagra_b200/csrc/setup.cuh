@@ -109,39 +109,30 @@ __global__ void k_point_scales_gram(Layout L, const int64_t* var_off, const int6
   const int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (pt >= L.nP) return;
   const int64_t v = L.nC + pt;
-  double sq[PM];
-  for (int p = 0; p < pw; ++p) sq[p] = 0;
-  for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
-    DBlockMeta b = blocks[var_blk[k]];
-    for (int p = 0; p < pw; ++p)
-      for (int i = 0; i < b.rows; ++i) {
-        double x = (double)values[b.start + (int64_t)p * b.rows + i];
-        sq[p] += x * x;
-      }
-  }
-  double inv[PM];
-  const int64_t base = L.retained + pt * pw;
-  for (int p = 0; p < pw; ++p) {
-    double raw = sqrt(sq[p]);
-    if (!isfinite(raw)) atomicOr(bad, 1);
-    double d = fmax(raw, floor);
-    scales[base + p] = d;
-    inv[p] = 1.0 / d;
-  }
+  // one pass: the raw Gram, normalized afterwards (its diagonal gives the
+  // squared column norms), as k_cam_scales_gram
   double acc[PM * PM];
   for (int k = 0; k < pw * pw; ++k) acc[k] = 0;
   for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
     DBlockMeta b = blocks[var_blk[k]];
     for (int i = 0; i < b.rows; ++i) {
       double jv[PM];
-      for (int p = 0; p < pw; ++p) jv[p] = (double)values[b.start + (int64_t)p * b.rows + i] * inv[p];
+      for (int p = 0; p < pw; ++p) jv[p] = (double)values[b.start + (int64_t)p * b.rows + i];
       for (int c = 0; c < pw; ++c)
         for (int r = c; r < pw; ++r) acc[c * pw + r] += jv[c] * jv[r];
     }
   }
+  double d[PM];
+  const int64_t base = L.retained + pt * pw;
+  for (int p = 0; p < pw; ++p) {
+    double raw = sqrt(acc[p * pw + p]);
+    if (!isfinite(raw)) atomicOr(bad, 1);
+    d[p] = fmax(raw, floor);
+    scales[base + p] = d[p];
+  }
   TS* g = gram + L.gram_offset(v);
   for (int c = 0; c < pw; ++c)
-    for (int r = 0; r < pw; ++r) g[c * pw + r] = (TS)(r >= c ? acc[c * pw + r] : 0.0);
+    for (int r = 0; r < pw; ++r) g[c * pw + r] = (TS)(r >= c ? acc[c * pw + r] / (d[c] * d[r]) : 0.0);
 }
 
 // One block per retained variable: out[cam*cw + c] = sum over its blocks of
