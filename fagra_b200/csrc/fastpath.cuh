@@ -664,13 +664,14 @@ __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, c
 // Coarse Galerkin matrix of the two-level PCG in one pass over the edge
 // records: E(lambda) = W^T S W with S = lambda I + B - E C^-1 E^T, computed as
 //   lambda W^T W + sum_cam W_cam^T B_cam W_cam           (k_coarse_cams)
-//   - sum_p u_p^T C_p^-1 u_p, u_p = sum_{e in p} E_e^T W_cam(e)   (k_coarse_points)
-// instead of nk operator applications. k_coarse_points runs one thread per
-// point over its point-major records (no cross-lane traffic); W is staged
-// camera-major with a row stride of ws floats (a multiple of 4):
-// wc[cam * ws + a * 9 + c]. out: nk x nk, accumulated with atomics (zeroed by
-// the caller).
-constexpr int COARSE_THREADS = 256;
+//   - sum_p u_p^T C_p^-1 u_p, u_p = sum_{e in p} E_e^T W_cam(e)   (k_coarse_tiles)
+// instead of nk operator applications. k_coarse_tiles walks the operator's
+// warp tiles (lane per edge, 16-byte record loads), sums u over each point's
+// lanes with the same segmented shuffle scan, and the point's last lane adds
+// u^T C^-1 u. W is staged camera-major, coordinate-major, vector-minor with 8
+// slots: wc[cam * 72 + c * 8 + a]. out: nk x nk (nk = 7), accumulated with
+// atomics (zeroed by the caller).
+constexpr int COARSE_WARPS = 8;
 template <class TS>
 __device__ __forceinline__ void coarse_record(const TS* rec, float (&E)[28]);
 template <>
@@ -691,55 +692,67 @@ __device__ __forceinline__ void coarse_record<double>(const double* rec, float (
     E[2 * i] = (float)a.x; E[2 * i + 1] = (float)a.y;
   }
 }
-template <class TS, int NK>
-__global__ void __launch_bounds__(COARSE_THREADS)
-    k_coarse_points(int64_t npts, const int64_t* pt_off, const TS* erec, const TS* prec, const float* wc, int ws,
-                    double* out) {
-  const int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  constexpr int NL = NK * (NK + 1) / 2;
+template <class TS>
+__global__ void __launch_bounds__(COARSE_WARPS * 32)
+    k_coarse_tiles(FastTiles tiles, const TS* erec, const TS* prec, const float* wc, double* out) {
+  constexpr int NK = 7, NL = NK * (NK + 1) / 2;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double acc[NL];
 #pragma unroll
   for (int k = 0; k < NL; ++k) acc[k] = 0;
-  if (pt < npts) {
+  for (int64_t wt = (int64_t)blockIdx.x * COARSE_WARPS + w; wt < tiles.nwt; wt += (int64_t)gridDim.x * COARSE_WARPS) {
+    const int64_t e0 = tiles.wt_e0[wt];
+    const int cnt = (int)(tiles.wt_e0[wt + 1] - e0);
+    const int64_t p0 = tiles.wt_p0[wt];
     float u[NK][3];
 #pragma unroll
     for (int a = 0; a < NK; ++a) u[a][0] = u[a][1] = u[a][2] = 0.f;
-    for (int64_t e = pt_off[pt]; e < pt_off[pt + 1]; ++e) {
+    uint32_t lp = 0xFFFFu;
+    if (lane < cnt) {
       float E[28];
-      coarse_record<TS>(erec + e * 28, E);
+      coarse_record<TS>(erec + (e0 + lane) * 28, E);
       typename RecWord<TS>::U word;
-      memcpy(&word, erec + e * 28 + 27, sizeof(word));
-      const float4* wv = reinterpret_cast<const float4*>(wc + (int64_t)RecWord<TS>::cam(word) * ws);
-      float x[(NK * 9 + 3) / 4 * 4];
+      memcpy(&word, erec + (e0 + lane) * 28 + 27, sizeof(word));
+      lp = RecWord<TS>::lp(word);
+      const float4* wv = reinterpret_cast<const float4*>(wc + (int64_t)RecWord<TS>::cam(word) * 72);
 #pragma unroll
-      for (int i = 0; i < (NK * 9 + 3) / 4; ++i) {
-        const float4 a = __ldg(wv + i);
-        x[4 * i] = a.x; x[4 * i + 1] = a.y; x[4 * i + 2] = a.z; x[4 * i + 3] = a.w;
+      for (int c = 0; c < 9; ++c) {
+        const float4 lo = __ldg(wv + 2 * c), hi = __ldg(wv + 2 * c + 1);
+        const float x[NK] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z};
+#pragma unroll
+        for (int a = 0; a < NK; ++a)
+#pragma unroll
+          for (int p = 0; p < 3; ++p) u[a][p] += E[p * 9 + c] * x[a];
       }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
 #pragma unroll
       for (int a = 0; a < NK; ++a)
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
-          float v = 0.f;
-#pragma unroll
-          for (int c = 0; c < 9; ++c) v += E[p * 9 + c] * x[a * 9 + c];
-          u[a][p] += v;
+          const float v = __shfl_up_sync(0xffffffffu, u[a][p], off);
+          if (lane >= off && lo == lp) u[a][p] += v;
         }
     }
-    const TS* r = prec + pt * 8;
-    const double c00 = r[0], c10 = r[1], c20 = r[2], c11 = r[3], c21 = r[4], c22 = r[5];
-    int idx = 0;
+    const uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
+    if (lane < cnt && (lane == cnt - 1 || lpn != lp)) {
+      const TS* r = prec + (p0 + lp) * 8;
+      const double c00 = r[0], c10 = r[1], c20 = r[2], c11 = r[3], c21 = r[4], c22 = r[5];
+      int idx = 0;
 #pragma unroll
-    for (int a = 0; a < NK; ++a) {
-      const double t0 = c00 * u[a][0] + c10 * u[a][1] + c20 * u[a][2];
-      const double t1 = c10 * u[a][0] + c11 * u[a][1] + c21 * u[a][2];
-      const double t2 = c20 * u[a][0] + c21 * u[a][1] + c22 * u[a][2];
+      for (int a = 0; a < NK; ++a) {
+        const double t0 = c00 * u[a][0] + c10 * u[a][1] + c20 * u[a][2];
+        const double t1 = c10 * u[a][0] + c11 * u[a][1] + c21 * u[a][2];
+        const double t2 = c20 * u[a][0] + c21 * u[a][1] + c22 * u[a][2];
 #pragma unroll
-      for (int b = 0; b <= a; ++b) acc[idx++] += (double)u[b][0] * t0 + (double)u[b][1] * t1 + (double)u[b][2] * t2;
+        for (int b = 0; b <= a; ++b)
+          acc[idx++] += (double)u[b][0] * t0 + (double)u[b][1] * t1 + (double)u[b][2] * t2;
+      }
     }
   }
-  __shared__ double sh[COARSE_THREADS / 32][NL];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __shared__ double sh[COARSE_WARPS][NL];
 #pragma unroll
   for (int k = 0; k < NL; ++k) {
     double v = acc[k];
@@ -750,7 +763,7 @@ __global__ void __launch_bounds__(COARSE_THREADS)
   __syncthreads();
   if (threadIdx.x < NL) {
     double v = 0;
-    for (int q = 0; q < COARSE_THREADS / 32; ++q) v += sh[q][threadIdx.x];
+    for (int q = 0; q < COARSE_WARPS; ++q) v += sh[q][threadIdx.x];
     int a = 0, k = threadIdx.x;
     while (k > a) k -= ++a;  // packed lower index -> (a, b = k)
     atomicAdd(out + a * NK + k, -v);
@@ -774,7 +787,7 @@ __global__ void k_coarse_cams(int64_t ncam, int nk, const double* wd, const TS* 
     for (int a = 0; a < nk; ++a)
       for (int c = 0; c < 9; ++c) {
         w[a][c] = wd[a * n + cam * 9 + c];
-        wc[cam * ws + a * 9 + c] = (float)w[a][c];
+        wc[cam * ws + c * 8 + a] = (float)w[a][c];
       }
     for (int a = 0; a < nk; ++a) {
       double bw[9];  // B w_a (B symmetric from its lower triangle)
@@ -895,15 +908,16 @@ struct FastPath {
   template <class Impl>
   fg_status coarse_gram(Impl& s, double lambda, const double* wd, int nk, double* out) {
     if (nk != 7) return FG_UNSUPPORTED_STRUCTURE;
-    constexpr int NK = 7, WS = (NK * 9 + 3) / 4 * 4;
+    constexpr int WS = 72;
     FG_TRY(d_wc.resize((size_t)s.nC * WS));
     FG_CUDA(cudaMemsetAsync(d_wc.get(), 0, (size_t)s.nC * WS * sizeof(float), s.st));
     FG_CUDA(cudaMemsetAsync(out, 0, (size_t)nk * nk * sizeof(double), s.st));
     FG_LAUNCH(k_coarse_cams<TS>, grid_for(s.nC, 32), 32, 0, s.st, (int64_t)s.nC, nk, wd, s.d_gram.get(),
               s.d_observed.get(), lambda, d_wc.get(), WS, out);
-    FG_LAUNCH((k_coarse_points<TS, NK>), grid_for(s.nP, COARSE_THREADS), COARSE_THREADS, 0, s.st, (int64_t)s.nP,
-              s.d_pt_edge_off.get(), (const TS*)d_erec.get(), (const TS*)d_prec.get(), (const float*)d_wc.get(), WS,
-              out);
+    FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
+    const unsigned blocks = (unsigned)std::min<int64_t>((nwt + COARSE_WARPS - 1) / COARSE_WARPS, 8 * (int64_t)grid);
+    FG_LAUNCH(k_coarse_tiles<TS>, std::max(blocks, 1u), COARSE_WARPS * 32, 0, s.st, tl, (const TS*)d_erec.get(),
+              (const TS*)d_prec.get(), (const float*)d_wc.get(), out);
     return FG_OK;
   }
 

@@ -218,16 +218,48 @@ __global__ void __launch_bounds__(REC_T) k_edge_records2(int64_t nedges, const i
     double E[27];
 #pragma unroll
     for (int i = 0; i < 27; ++i) E[i] = 0;
-    for (int row = 0; row < l.rows; ++row) {
-      double jc[9], jp[3];
+    if (l.rows == 2 && r.rows == 2 && r.start == l.start + 18 && (l.start & 3) == 0) {
+      // the BAL emission layout: 24 contiguous values, 16-byte aligned
+      TS v[24];
+      if (sizeof(TS) == 4) {
+        const float4* q = reinterpret_cast<const float4*>(values + l.start);
 #pragma unroll
-      for (int c = 0; c < 9; ++c) jc[c] = (double)values[l.start + (int64_t)c * l.rows + row] * ic[c];
+        for (int i = 0; i < 6; ++i) {
+          const float4 a = q[i];
+          v[4 * i] = (TS)a.x; v[4 * i + 1] = (TS)a.y; v[4 * i + 2] = (TS)a.z; v[4 * i + 3] = (TS)a.w;
+        }
+      } else {
+        const double2* q = reinterpret_cast<const double2*>(values + l.start);
 #pragma unroll
-      for (int p = 0; p < 3; ++p) jp[p] = (double)values[r.start + (int64_t)p * r.rows + row] * ip[p];
+        for (int i = 0; i < 12; ++i) {
+          const double2 a = q[i];
+          v[2 * i] = (TS)a.x; v[2 * i + 1] = (TS)a.y;
+        }
+      }
 #pragma unroll
-      for (int p = 0; p < 3; ++p)
+      for (int row = 0; row < 2; ++row) {
+        double jc[9], jp[3];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) E[p * 9 + c] += jc[c] * jp[p];
+        for (int c = 0; c < 9; ++c) jc[c] = (double)v[2 * c + row] * ic[c];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) jp[p] = (double)v[18 + 2 * p + row] * ip[p];
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+#pragma unroll
+          for (int c = 0; c < 9; ++c) E[p * 9 + c] += jc[c] * jp[p];
+      }
+    } else {
+      for (int row = 0; row < l.rows; ++row) {
+        double jc[9], jp[3];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) jc[c] = (double)values[l.start + (int64_t)c * l.rows + row] * ic[c];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) jp[p] = (double)values[r.start + (int64_t)p * r.rows + row] * ip[p];
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+#pragma unroll
+          for (int c = 0; c < 9; ++c) E[p * 9 + c] += jc[c] * jp[p];
+      }
     }
     bool ok = true;
     TS* t = tile + threadIdx.x * 29;
