@@ -250,6 +250,15 @@ __global__ void k_bal_stage(int64_t nc9, int64_t np3, const double* cams, const 
   else if (i < nc9 + np3) tpts[i - nc9] = pts[i - nc9] + delta[i];
 }
 
+// px[k] = pixels of observation order[k] (emission order).
+__global__ void k_bal_permute_pixels(int64_t o, const uint32_t* order, const double* raw, double* px) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= o) return;
+  const int64_t i = order[k];
+  px[2 * k] = raw[2 * i];
+  px[2 * k + 1] = raw[2 * i + 1];
+}
+
 fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const double* pp, const uint32_t* ocam,
                            const uint32_t* opt, const double* pix, int device, bool on_device) {
   id = g_next_id.fetch_add(1);
@@ -258,42 +267,54 @@ fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const
   FG_TRY(select_device(dev));
   FG_TRY(device_stream(dev, &st));
   nsm = sm_count(dev);
-  std::vector<uint32_t> hc(o), hp(o);
-  std::vector<double> hx(2 * o);
-  if (on_device) {
-    if (o) {
-      FG_CUDA(cudaMemcpy(hc.data(), ocam, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-      FG_CUDA(cudaMemcpy(hp.data(), opt, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-      FG_CUDA(cudaMemcpy(hx.data(), pix, 2 * o * sizeof(double), cudaMemcpyDeviceToHost));
-    }
-  } else {
-    std::copy(ocam, ocam + o, hc.begin());
-    std::copy(opt, opt + o, hp.begin());
-    std::copy(pix, pix + 2 * o, hx.begin());
+  // Host views of the observations (device inputs are copied down once).
+  std::vector<uint32_t> dc, dp;
+  std::vector<double> dx;
+  const uint32_t* hc = ocam;
+  const uint32_t* hp = opt;
+  const double* hx = pix;
+  if (on_device && o) {
+    dc.resize(o);
+    dp.resize(o);
+    dx.resize(2 * o);
+    FG_CUDA(cudaMemcpy(dc.data(), ocam, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    FG_CUDA(cudaMemcpy(dp.data(), opt, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    FG_CUDA(cudaMemcpy(dx.data(), pix, 2 * o * sizeof(double), cudaMemcpyDeviceToHost));
+    hc = dc.data();
+    hp = dp.data();
+    hx = dx.data();
   }
   for (size_t i = 0; i < o; ++i)
     if (hc[i] >= nc || hp[i] >= np || !std::isfinite(hx[2 * i]) || !std::isfinite(hx[2 * i + 1])) {
       set_error("invalid observation index or value");
       return FG_INVALID_EMISSION;
     }
-  // Emission order: frames in camera order, factors in insertion order.
+  // Emission order: frames in camera order, factors in insertion order (a
+  // stable counting sort by camera); the pixels are permuted on the device.
   std::vector<size_t> off(nc + 1, 0);
   for (size_t i = 0; i < o; ++i) off[hc[i] + 1]++;
   for (size_t i = 0; i < nc; ++i) off[i + 1] += off[i];
-  order.assign(o, 0);
-  for (size_t i = 0; i < o; ++i) order[off[hc[i]]++] = i;
+  order.resize(o);
+  for (size_t i = 0; i < o; ++i) order[off[hc[i]]++] = (uint32_t)i;
   h_oc.resize(o);
   h_op.resize(o);
-  std::vector<double> ex(2 * o);
   for (size_t k = 0; k < o; ++k) {
     h_oc[k] = hc[order[k]];
     h_op[k] = hp[order[k]];
-    ex[2 * k] = hx[2 * order[k]];
-    ex[2 * k + 1] = hx[2 * order[k] + 1];
   }
   FG_TRY(upload(oc, h_oc.data(), o, st));
   FG_TRY(upload(op, h_op.data(), o, st));
-  FG_TRY(upload(px, ex.data(), 2 * o, st));
+  FG_TRY(px.resize(std::max<size_t>(2 * o, 1)));
+  if (o) {
+    DBuf<double> raw;
+    DBuf<uint32_t> ord;
+    FG_TRY(raw.resize(2 * o));
+    FG_TRY(upload(ord, order.data(), o, st));
+    FG_CUDA(cudaMemcpyAsync(raw.get(), hx, 2 * o * sizeof(double), on_device ? cudaMemcpyDeviceToDevice
+                                                                              : cudaMemcpyHostToDevice, st));
+    FG_LAUNCH(k_bal_permute_pixels, grid_for(o, 256), 256, 0, st, (int64_t)o, ord.get(), raw.get(), px.get());
+    FG_CUDA(cudaStreamSynchronize(st));  // raw and ord die here
+  }
   FG_TRY(cams.resize(std::max<size_t>(9 * nc, 1)));
   FG_TRY(pts.resize(std::max<size_t>(3 * np, 1)));
   FG_TRY(tcams.resize(std::max<size_t>(9 * nc, 1)));

@@ -48,7 +48,7 @@ struct BalProblem {
   int dev = 0, nsm = 148;
   cudaStream_t st = nullptr;
   size_t nc = 0, np = 0, no = 0;
-  std::vector<size_t> order;  // emission position -> insertion index
+  std::vector<uint32_t> order;  // emission position -> insertion index
   std::vector<uint32_t> h_oc, h_op;
   DBuf<uint32_t> oc, op;
   DBuf<double> px, cams, pts, tcams, tpts, prep, tprep, partials, result, init_cams, init_pts, gauge;

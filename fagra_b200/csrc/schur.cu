@@ -105,6 +105,8 @@ class SchurImpl final : public Backend {
   // the FP32 solve ended on an FP64 replacement residual of the z in d_zred
   // (h_pcg holds it), so verification need not recompute S z - b
   bool final_residual_known = false;
+  HBuf<uint32_t> h_bal_stage;  // pinned staging of the BAL emission arrays and orders
+  DBuf<uint32_t> d_bal_stage;
   int nk = 0;
   bool coarse_on = false, basis_scaled = false;
   DBuf<double> d_basis, d_Wd, d_E, d_G;
@@ -319,6 +321,69 @@ class SchurImpl final : public Backend {
     FG_TRY(d_jd.resize(std::max<size_t>(rows, 1)));
     // synchronize so host vectors may be released safely
     FG_CUDA(cudaStreamSynchronize(st));
+    structure_valid = true;
+    fast.invalidate();
+    drop_graphs();
+    return FG_OK;
+  }
+
+  // The maps build_structure derives, for the BAL emission layout: the host
+  // only counts and orders emissions by camera and by point (stable counting
+  // sorts over 32-bit indices); the kernel writes every device map.
+  fg_status build_structure_bal(size_t cams, size_t pts, size_t obs, const uint32_t* ocam, const uint32_t* opt) {
+    rows = 2 * obs;
+    nblocks = 2 * obs;
+    nedges = obs;
+    const size_t nvar = nC + nP;
+    std::vector<int64_t> cam_off(nC + 1, 0), pt_off(nP + 1, 0);
+    for (size_t k = 0; k < obs; ++k) {
+      if (ocam[k] >= cams || opt[k] >= pts) {
+        set_error("BAL observation index out of range");
+        return FG_DIMENSION_MISMATCH;
+      }
+      cam_off[ocam[k] + 1]++;
+      pt_off[opt[k] + 1]++;
+    }
+    for (size_t c = 0; c < nC; ++c) cam_off[c + 1] += cam_off[c];
+    for (size_t p = 0; p < nP; ++p) pt_off[p + 1] += pt_off[p];
+    FG_TRY(h_bal_stage.resize(std::max<size_t>(4 * obs, 1)));  // ocam | opt | cam_order | pt_order
+    uint32_t* h = h_bal_stage.get();
+    std::memcpy(h, ocam, obs * sizeof(uint32_t));
+    std::memcpy(h + obs, opt, obs * sizeof(uint32_t));
+    {
+      std::vector<int64_t> fc(cam_off.begin(), cam_off.end() - 1), fp(pt_off.begin(), pt_off.end() - 1);
+      for (size_t k = 0; k < obs; ++k) {
+        h[2 * obs + fc[ocam[k]]++] = (uint32_t)k;
+        h[3 * obs + fp[opt[k]]++] = (uint32_t)k;
+      }
+    }
+    std::vector<int64_t> var_off(nvar + 1, 0);
+    for (size_t c = 0; c <= nC; ++c) var_off[c] = cam_off[c];
+    for (size_t p = 1; p <= nP; ++p) var_off[nC + p] = (int64_t)obs + pt_off[p];
+    h_observed.assign(nvar, 0);
+    for (size_t v = 0; v < nvar; ++v) h_observed[v] = var_off[v + 1] > var_off[v];
+    DBuf<uint32_t>& d_stage = d_bal_stage;
+    FG_TRY(d_stage.resize(std::max<size_t>(4 * obs, 1)));
+    if (obs) FG_CUDA(cudaMemcpyAsync(d_stage.get(), h, 4 * obs * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    FG_TRY(d_blocks.resize(std::max<size_t>(nblocks, 1)));
+    FG_TRY(d_edges.resize(std::max<size_t>(nedges, 1)));
+    FG_TRY(d_var_blk.resize(std::max<size_t>(nblocks, 1)));
+    FG_TRY(d_cam_edge.resize(std::max<size_t>(nedges, 1)));
+    FG_TRY(d_pt_edge.resize(std::max<size_t>(nedges, 1)));
+    FG_TRY(d_emi_off.resize(obs + 1));
+    FG_LAUNCH(k_bal_structure, grid_for(obs + 1, 256), 256, 0, st, (int64_t)obs, (int64_t)cams, d_stage.get(),
+              d_stage.get() + obs, d_stage.get() + 2 * obs, d_stage.get() + 3 * obs, d_blocks.get(), d_edges.get(),
+              d_var_blk.get(), d_cam_edge.get(), d_pt_edge.get(), d_emi_off.get());
+    FG_TRY(upload(d_var_off, var_off.data(), var_off.size(), st));
+    FG_TRY(upload(d_pt_edge_off, pt_off.data(), pt_off.size(), st));
+    FG_TRY(upload(d_cam_edge_off, cam_off.data(), cam_off.size(), st));
+    FG_TRY(upload(d_observed, h_observed.data(), h_observed.size(), st));
+    h_pt_off = pt_off;
+    nemissions = obs;
+    pure_pairs = obs > 0;
+    FG_TRY(d_cross.resize(std::max<size_t>(nedges * cw * pw, 1)));
+    FG_TRY(d_jd.resize(std::max<size_t>(rows, 1)));
+    FG_CUDA(cudaStreamSynchronize(st));  // the host staging may be reused after this
     structure_valid = true;
     fast.invalidate();
     drop_graphs();
@@ -1153,14 +1218,7 @@ class SchurImpl final : public Backend {
     if (retained != 9 * cams || dim != 9 * cams + 3 * pts) return FG_DIMENSION_MISMATCH;
     if (bal_bound == id && structure_valid) return FG_OK;
     // Emission order: one Frame batch per camera, factors in insertion order.
-    std::vector<HostBlock> blocks(2 * obs);
-    std::vector<HostEdge> edges(obs);
-    for (size_t k = 0; k < obs; ++k) {
-      blocks[2 * k] = {2 * k, 9 * (size_t)ocam[k], 2, 9, 24 * k};
-      blocks[2 * k + 1] = {2 * k, 9 * cams + 3 * (size_t)opt_[k], 2, 3, 24 * k + 18};
-      edges[k] = {9 * (size_t)ocam[k], 3 * (size_t)opt_[k], 2 * k, 2 * k + 1};
-    }
-    FG_TRY(build_structure(blocks, edges, 2 * obs));
+    FG_TRY(build_structure_bal(cams, pts, obs, ocam, opt_));
     up_blocks.clear();
     up_edges.clear();
     nvalues = 24 * obs;

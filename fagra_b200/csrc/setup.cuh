@@ -279,4 +279,30 @@ __global__ void __launch_bounds__(REC_T) k_edge_records2(int64_t nedges, const i
   for (int i = threadIdx.x; i < nk * 28; i += REC_T) out[i] = tile[(i / 28) * 29 + (i % 28)];
 }
 
+// Index maps of a BAL linearization (emission k: rows 2k, 2k+1; block 2k =
+// camera ocam[k] (2x9 at 24k), block 2k+1 = point opt[k] (2x3 at 24k+18)),
+// written on the device from the emission arrays and the two stable orders
+// (emissions sorted by camera / by point) the host computed by counting.
+__global__ void k_bal_structure(int64_t obs, int64_t ncam, const uint32_t* ocam, const uint32_t* opt,
+                                const uint32_t* cam_order, const uint32_t* pt_order, DBlockMeta* blocks,
+                                DEdgeMeta* edges, int64_t* var_blk, int64_t* cam_edge, int64_t* pt_edge,
+                                int64_t* emi_off) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k > obs) return;
+  if (k == obs) {
+    emi_off[obs] = 2 * obs;
+    return;
+  }
+  const int64_t c = ocam[k], p = opt[k];
+  blocks[2 * k] = DBlockMeta{2 * k, 24 * k, 9 * c, 2, 9};
+  blocks[2 * k + 1] = DBlockMeta{2 * k, 24 * k + 18, 9 * ncam + 3 * p, 2, 3};
+  edges[k] = DEdgeMeta{(int32_t)c, (int32_t)p, 2 * k, 2 * k + 1};
+  emi_off[k] = 2 * k;
+  const int64_t ec = cam_order[k], ep = pt_order[k];
+  var_blk[k] = 2 * ec;            // camera variables first, each in emission order
+  var_blk[obs + k] = 2 * ep + 1;  // then the points
+  cam_edge[k] = ec;
+  pt_edge[k] = ep;
+}
+
 }  // namespace fg
