@@ -908,9 +908,6 @@ class SchurImpl final : public Backend {
     }
   }
   fg_status iteration_body(bool mixed, double* xd, PcgState* ps, double lambda, int k) {
-    Layout L = layout();
-    const unsigned bw = wide_block(), gw = wide_grid();
-    const size_t shm = bw * sizeof(TS);
     double* tsum = d_partials.get() + 4 * 65536;
     PView<TS> pv{d_z.get(), d_pp.get(), &ps->beta};
     FG_TRY(apply_reduced<TS>(pv, lambda, lambda, true, d_t.get(), d_q.get(), tsum, ps, nullptr, &ps->lambda));
@@ -955,7 +952,6 @@ class SchurImpl final : public Backend {
   // preconditioner. b is a double retained vector; the solution lands in d_x.
   fg_status pcg(const double* b, double lambda, double rel_tol, size_t max_iters, unsigned* its, int* term,
                 double* rel_est) {
-    Layout L = layout();
     PcgState* ps = d_pcg.get();
     {
       PcgState init{};
@@ -1013,7 +1009,6 @@ class SchurImpl final : public Backend {
       set_error("local block factorization failed");
       return FG_LINEAR_SOLVE_FAILED;
     }
-    Layout L = layout();
     // scaled_work = -g/D; eliminated part through C^-1; reduced rhs (src/schur.rs:216-242)
     FG_TRY(launch_neg_scaled_gradient());
     FG_TRY(launch_point_solve(lambda));
@@ -1121,7 +1116,6 @@ class SchurImpl final : public Backend {
   // (and before declaring convergence) it is replaced by b - S x evaluated in
   // FP64 arithmetic. Convergence is only ever declared on that FP64 residual.
   fg_status refine(double lambda, unsigned* its_out, int* term_out, double* est_out, size_t* rounds) {
-    Layout L = layout();
     PcgState* ps = d_pcg.get();
     double* xd = d_zred.get();
     {
@@ -1171,9 +1165,6 @@ class SchurImpl final : public Backend {
 
   // Gated FP64 residual replacement: runs only while the device flag is set.
   fg_status replacement(double lambda, double* xd, PcgState* ps) {
-    Layout L = layout();
-    const unsigned bw = wide_block(), gw = wide_grid();
-    const size_t shm = bw * sizeof(TS);
     PView<double> xv{xd, nullptr, nullptr};
     FG_TRY(apply_reduced<double>(xv, lambda, lambda, true, d_tmpd.get(), d_qd.get(), nullptr, nullptr, &ps->replace,
                                  &ps->lambda));
