@@ -572,6 +572,7 @@ class LsmrImpl final : public Backend {
     D.factors = block ? d_factors.get() : nullptr;
     D.s_fac = block ? d_active.get() : nullptr;
     D.scales = scales;
+    D.bal = source == DEVICE ? 1 : 0;
     return D;
   }
 

@@ -61,7 +61,57 @@ struct LsmrDev {
   const double* factors;  // per segment: w*w lower Cholesky factor, column-major
   const int64_t* s_fac;   // factor offset per segment; -1 = identity
   const double* scales;   // null = unscaled operator
+  // 1: the device BAL layout — emission e has rows 2e, 2e+1, blocks 2e (camera,
+  // 2x9) and 2e+1 (point, 2x3), values [24e, 24e + 24), and every segment is
+  // one whole block — so rows and pieces are read with 16-byte loads and the
+  // row / row count of a piece follow from its start.
+  int bal;
 };
+
+// n contiguous values at p into double (p 16-byte aligned when n is a
+// multiple of 4 / 2 for float / double, 8-byte aligned otherwise).
+template <int N>
+__device__ __forceinline__ void load_vals(const float* p, double (&v)[N]) {
+  if (N % 4 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i) {
+      const float4 a = reinterpret_cast<const float4*>(p)[i];
+      v[4 * i] = a.x; v[4 * i + 1] = a.y; v[4 * i + 2] = a.z; v[4 * i + 3] = a.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const float2 a = reinterpret_cast<const float2*>(p)[i];
+      v[2 * i] = a.x; v[2 * i + 1] = a.y;
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ void load_vals(const double* p, double (&v)[N]) {
+#pragma unroll
+  for (int i = 0; i < N / 2; ++i) {
+    const double2 a = reinterpret_cast<const double2*>(p)[i];
+    v[2 * i] = a.x; v[2 * i + 1] = a.y;
+  }
+}
+
+// emission_rows for the BAL layout, with the same summation order.
+template <class TS, class F>
+__device__ __forceinline__ void emission_rows_bal(const LsmrDev<TS>& D, int64_t e, const double* w, F f) {
+  double v[24];
+  load_vals<24>(D.values + 24 * e, v);
+  const double* wc = w + D.b_col[2 * e];
+  const double* wp = w + D.b_col[2 * e + 1];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    double acc = 0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) acc += v[2 * j + i] * wc[j];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc += v[18 + 2 * j + i] * wp[j];
+    f(2 * e + i, acc);
+  }
+}
 
 constexpr int LSMR_NT = 256;          // threads per block
 constexpr int LSMR_WIDE_DEGREE = 48;  // pieces above which a segment gets a CTA
@@ -113,7 +163,7 @@ __global__ void __launch_bounds__(LSMR_NT) k_lsmr_rows(LsmrDev<TS> D, unsigned e
           sq[0] += x * x;
         }
       } else {
-        emission_rows(D, e, w, [&](int64_t r, double acc) {
+        auto body = [&](int64_t r, double acc) {
           if (MODE == ROWS_ITER) {
             double x = acc - f * (double)u[r];
             u[r] = (TS)x;
@@ -124,7 +174,9 @@ __global__ void __launch_bounds__(LSMR_NT) k_lsmr_rows(LsmrDev<TS> D, unsigned e
             pr[r] = acc - negres[r];
             sq[0] += acc * acc;
           }
-        });
+        };
+        if (D.bal) emission_rows_bal(D, e, w, body);
+        else emission_rows(D, e, w, body);
       }
     }
   } else if (MODE == ROWS_ITER || MODE == ROWS_PRODUCT) {
@@ -159,6 +211,30 @@ template <class TS, int MAXW, bool SQUARES, class V>
 __device__ __forceinline__ void segment_accumulate(const LsmrDev<TS>& D, int64_t s, int w, int64_t first,
                                                    int64_t stride, const V* vec, double (&acc)[MAXW]) {
   const int64_t p1 = D.s_pc[s + 1];
+  if (D.bal && (w == 9 || w == 3) && MAXW >= 9) {
+    // camera piece: 18 values at 24e; point piece: 6 values at 24e + 18; rows 2e, 2e + 1
+    for (int64_t p = D.s_pc[s] + first; p < p1; p += stride) {
+      const int64_t start = D.p_start[p], row = 2 * (start / 24);
+      const double x0 = SQUARES ? 0.0 : (double)vec[row], x1 = SQUARES ? 0.0 : (double)vec[row + 1];
+      double a[18];
+      if (w == 9) {
+        load_vals<18>(D.values + start, a);
+      } else {
+        double b[6];
+        load_vals<6>(D.values + start, b);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) a[k] = b[k];
+      }
+#pragma unroll
+      for (int j = 0; j < (MAXW < 9 ? MAXW : 9); ++j) {
+        if (j < w) {
+          acc[j] += SQUARES ? a[2 * j] * a[2 * j] : a[2 * j] * x0;
+          acc[j] += SQUARES ? a[2 * j + 1] * a[2 * j + 1] : a[2 * j + 1] * x1;
+        }
+      }
+    }
+    return;
+  }
   for (int64_t p = D.s_pc[s] + first; p < p1; p += stride) {
     const int64_t start = D.p_start[p], row = D.p_row[p];
     const int rows = D.p_rows[p];
