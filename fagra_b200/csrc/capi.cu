@@ -106,7 +106,7 @@ FG_API void fg_schur_default_options(fg_schur_options* o) {
   o->precision = FG_PRECISION_F64;
   o->preconditioner = FG_PRECOND_RETAINED_BLOCKS;
   o->device = 0;
-  o->residual_replacement = 1e-3;
+  o->residual_replacement = 1e-4;
   o->operator_variant = 0;
   o->coarse_correction = 0;
 }

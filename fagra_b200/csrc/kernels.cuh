@@ -720,6 +720,45 @@ __global__ void k_coarse_scale(int64_t n, int nk, const double* basis, const dou
   wt[k] = (TS)v;
 }
 
+// G = E^-1 for the nk x nk coarse matrix (Cholesky of its symmetric part, one
+// thread); G = 0 — a one-level preconditioner — when E is not positive
+// definite. *ok reports which.
+static __global__ void k_coarse_factor(int nk, const double* E, double* G, int* ok) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double L[MAXK * MAXK];
+  bool spd = true;
+  for (int j = 0; j < nk && spd; ++j)
+    for (int i = j; i < nk; ++i) {
+      double v = 0.5 * (E[i * nk + j] + E[j * nk + i]);
+      for (int k = 0; k < j; ++k) v -= L[i * nk + k] * L[j * nk + k];
+      if (i == j) {
+        if (!(v > 0) || !isfinite(v)) {
+          spd = false;
+          break;
+        }
+        L[j * nk + j] = sqrt(v);
+      } else {
+        L[i * nk + j] = v / L[j * nk + j];
+      }
+    }
+  for (int c = 0; c < nk; ++c) {
+    double y[MAXK];
+    for (int i = 0; i < nk; ++i) {
+      double v = i == c ? 1.0 : 0.0;
+      if (spd)
+        for (int k = 0; k < i; ++k) v -= L[i * nk + k] * y[k];
+      y[i] = spd ? v / L[i * nk + i] : 0.0;
+    }
+    for (int i = nk - 1; i >= 0; --i) {
+      double v = y[i];
+      if (spd)
+        for (int k = i + 1; k < nk; ++k) v -= L[k * nk + i] * G[k * nk + c];
+      G[i * nk + c] = spd ? v / L[i * nk + i] : 0.0;
+    }
+  }
+  *ok = spd ? 1 : 0;
+}
+
 // E[a][b] = W_a . (S W)_b, one block per entry.
 template <class TS>
 __global__ void k_coarse_gram(int64_t n, int nk, const double* wd, const TS* sw, double* e) {

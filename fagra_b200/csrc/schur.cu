@@ -110,6 +110,7 @@ class SchurImpl final : public Backend {
   int nk = 0;
   bool coarse_on = false, basis_scaled = false;
   DBuf<double> d_basis, d_Wd, d_E, d_G;
+  DBuf<int> d_coarse_ok;
   DBuf<TS> d_Wt, d_SWt;
   const void* graph_coarse[3] = {nullptr, nullptr, nullptr};  // W, G, on: what the PCG graphs captured
 
@@ -554,6 +555,7 @@ class SchurImpl final : public Backend {
     FG_TRY(d_SWt.resize(n));
     FG_TRY(d_E.resize(MAXK * MAXK));
     FG_TRY(d_G.resize(MAXK * MAXK));
+    FG_TRY(d_coarse_ok.resize(1));
     FG_LAUNCH(k_coarse_scale<TS>, grid_for(n, 256), 256, 0, st, (int64_t)retained, nk, d_basis.get(), d_scales.get(),
               d_Wd.get(), d_Wt.get());
     basis_scaled = true;
@@ -584,37 +586,9 @@ class SchurImpl final : public Backend {
       FG_LAUNCH(k_coarse_gram<TS>, (unsigned)(nk * nk), 256, 0, st, (int64_t)retained, nk, d_Wd.get(),
                 (const TS*)d_SWt.get(), d_E.get());
     }
-    double E[MAXK * MAXK], Lm[MAXK * MAXK] = {0}, G[MAXK * MAXK];
-    FG_CUDA(cudaMemcpyAsync(E, d_E.get(), (size_t)nk * nk * sizeof(double), cudaMemcpyDeviceToHost, st));
-    FG_CUDA(cudaStreamSynchronize(st));
-    // Cholesky of the symmetrized E, then G = E^-1 column by column
-    for (int j = 0; j < nk; ++j) {
-      for (int i = j; i < nk; ++i) {
-        double v = 0.5 * (E[i * nk + j] + E[j * nk + i]);
-        for (int k = 0; k < j; ++k) v -= Lm[i * nk + k] * Lm[j * nk + k];
-        if (i == j) {
-          if (!(v > 0) || !std::isfinite(v)) return sync_graph_coarse();
-          Lm[j * nk + j] = std::sqrt(v);
-        } else {
-          Lm[i * nk + j] = v / Lm[j * nk + j];
-        }
-      }
-    }
-    for (int c = 0; c < nk; ++c) {
-      double y[MAXK];
-      for (int i = 0; i < nk; ++i) {
-        double v = i == c ? 1.0 : 0.0;
-        for (int k = 0; k < i; ++k) v -= Lm[i * nk + k] * y[k];
-        y[i] = v / Lm[i * nk + i];
-      }
-      for (int i = nk - 1; i >= 0; --i) {
-        double v = y[i];
-        for (int k = i + 1; k < nk; ++k) v -= Lm[k * nk + i] * G[k * nk + c];
-        G[i * nk + c] = v / Lm[i * nk + i];
-      }
-    }
-    FG_CUDA(cudaMemcpyAsync(d_G.get(), G, (size_t)nk * nk * sizeof(double), cudaMemcpyHostToDevice, st));
-    FG_CUDA(cudaStreamSynchronize(st));
+    // G on the device (no host round trip); a non-SPD E gives G = 0, i.e.
+    // one-level PCG, and the verification readback reports it
+    FG_LAUNCH(k_coarse_factor, 1, 32, 0, st, nk, (const double*)d_E.get(), d_G.get(), d_coarse_ok.get());
     coarse_on = true;
     return sync_graph_coarse();
   }
@@ -954,20 +928,24 @@ class SchurImpl final : public Backend {
                 double* rel_est) {
     PcgState* ps = d_pcg.get();
     {
-      PcgState init{};
+      // from the pinned mirror, so the copy is asynchronous; the mirror is
+      // rewritten only by the polls below, which the stream orders after it
+      PcgState& init = *h_pcg.get();
+      init = PcgState{};
       init.max_iterations = (unsigned)std::min<size_t>(max_iters, 0xffffffffu);
       init.lambda = lambda;
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
-      FG_CUDA(cudaStreamSynchronize(st));
     }
     FG_TRY(launch_start<TS>(b, d_x.get(), rel_tol));
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
     const bool graphed = fast.enabled();
-    for (;;) {
-      FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-      FG_CUDA(cudaStreamSynchronize(st));
-      if (h_pcg.get()->done) break;
+    for (bool first = graphed;; first = false) {
+      if (!first) {  // the first graph follows the start without a poll (its kernels gate on done)
+        FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        FG_CUDA(cudaStreamSynchronize(st));
+        if (h_pcg.get()->done) break;
+      }
       if (launched >= max_iters + 2) break;  // device enforces the limit; host bound is a guard
       if (graphed) {
         FG_TRY(launch_graph(false, nullptr, ps, lambda));
@@ -1119,23 +1097,25 @@ class SchurImpl final : public Backend {
     PcgState* ps = d_pcg.get();
     double* xd = d_zred.get();
     {
-      PcgState init{};
+      PcgState& init = *h_pcg.get();  // pinned mirror: asynchronous copy (see pcg())
+      init = PcgState{};
       init.max_iterations = (unsigned)std::min<size_t>(opt.max_iterations, 0xffffffffu);
       init.lambda = lambda;
-      double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-3;
+      double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-4;
       init.delta2 = d * d;
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
-      FG_CUDA(cudaStreamSynchronize(st));
     }
     FG_TRY(launch_start<double>(d_rhs.get(), xd, opt.relative_tolerance));
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
     const size_t max_iters = opt.max_iterations;
     const bool graphed = fast.enabled();
-    for (;;) {
-      FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-      FG_CUDA(cudaStreamSynchronize(st));
-      if (h_pcg.get()->done == 1) break;
+    for (bool first = graphed;; first = false) {
+      if (!first) {  // the first graph follows the start without a poll
+        FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        FG_CUDA(cudaStreamSynchronize(st));
+        if (h_pcg.get()->done == 1) break;
+      }
       if (launched >= max_iters + 8) break;  // guard; the device enforces the limit
       if (graphed) {
         FG_TRY(launch_graph(true, xd, ps, lambda));

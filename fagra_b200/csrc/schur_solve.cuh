@@ -369,10 +369,13 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
               d_blocks.get(), d_values.get(), d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
               lambda, nC ? d_camjt.get() : (const double*)nullptr, d_partials.get() + 4 * 65536, vs);
   FG_CUDA(cudaMemcpyAsync(h_ver.get(), vs, sizeof(VerifyState), cudaMemcpyDeviceToHost, st));
+  if (coarse_on)  // whether the coarse matrix of this solve was positive definite
+    FG_CUDA(cudaMemcpyAsync(h_count.get() + 3, d_coarse_ok.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
   if (retained && !known)
     FG_CUDA(cudaMemcpyAsync(h_scalar.get() + 2, d_norm.get() + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   FG_CUDA(cudaStreamSynchronize(st));
   if (retained && !known) { red2 = h_scalar.get()[2]; rhs2 = h_scalar.get()[3]; }
+  if (coarse_on && h_count.get()[3] == 0) diag.coarse_vectors = 0;
   const VerifyState& v = *h_ver.get();
   auto rel = [](double n, double r) { return r == 0 ? n : n / r; };
   diag.reduced_relative_residual = rel(std::sqrt(red2), std::sqrt(rhs2));
