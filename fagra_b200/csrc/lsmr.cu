@@ -217,6 +217,12 @@ class LsmrImpl final : public Backend {
       return FG_INVALID_OPTIONS;
     }
     FG_TRY(sync_model());
+    if (source == DEVICE && npieces > pp0) {  // the point halves, contiguous (BAL segment pass)
+      FG_TRY(d_ptvals.resize((size_t)(npieces - pp0) * 6));
+      FG_LAUNCH(k_lsmr_point_copy<TS>, grid_for(npieces - pp0, 256), 256, 0, st, npieces - pp0, pp0, d_pstart.get(),
+                d_values.get(), d_ptvals.get());
+      ptvals_current = true;
+    }
     // Column norms with the floor (LinearizedModel::prepare_scales).
     {
       LsmrState s0{};
@@ -344,6 +350,7 @@ class LsmrImpl final : public Backend {
     source = DEVICE;
     rows = nrows;
     model_current = true;
+    ptvals_current = false;
     gradient_current = false;
     prepared_mode = MODE_NONE;
   }
@@ -371,6 +378,7 @@ class LsmrImpl final : public Backend {
       h_erow[obs] = 2 * (int64_t)obs;
       h_eblk[obs] = 2 * (int64_t)obs;
       rows = 2 * obs;
+      point_col0 = 9 * (int64_t)cams;
       FG_TRY(build_structure());
       bal_bound = id;
     }
@@ -497,6 +505,9 @@ class LsmrImpl final : public Backend {
 
   // structure sizes
   int64_t E = 0, S = 0, npieces = 0, n_entries = 0, n_fac = 0;
+  int64_t point_col0 = -1, pp0 = 0;  // BAL: first point column / first point piece
+  bool ptvals_current = false;
+  DBuf<TS> d_ptvals;
   int32_t n_wide = 0, n_narrow = 0;
   int maxw = 4;
   bool variables_consistent = true, variables_too_wide = false;
@@ -573,6 +584,8 @@ class LsmrImpl final : public Backend {
     D.s_fac = block ? d_active.get() : nullptr;
     D.scales = scales;
     D.bal = source == DEVICE ? 1 : 0;
+    D.ptvals = D.bal && ptvals_current ? d_ptvals.get() : nullptr;
+    D.pp0 = pp0;
     return D;
   }
 
@@ -671,6 +684,10 @@ class LsmrImpl final : public Backend {
         }
       }
     }
+    // BAL: the first point piece (point columns start at point_col0)
+    pp0 = npieces;
+    if (point_col0 >= 0 && point_col0 < n) pp0 = spc[segof[point_col0]];
+    ptvals_current = false;
     // Wide / narrow segment lists.
     std::vector<int32_t> wide, narrow;
     for (int64_t s = 0; s < S; ++s) (spc[s + 1] - spc[s] > LSMR_WIDE_DEGREE ? wide : narrow).push_back((int32_t)s);
@@ -749,6 +766,7 @@ class LsmrImpl final : public Backend {
       return FG_OK;
     }
     if (model_current) return FG_OK;
+    point_col0 = -1;  // host emissions: generic layout
     if (!structure_built || b_erow != h_erow || b_eblk != h_eblk || b_bcol != h_bcol || b_bcols != h_bcols)
       FG_TRY(build_structure());
     nvalues = h_values.size();

@@ -66,7 +66,22 @@ struct LsmrDev {
   // one whole block — so rows and pieces are read with 16-byte loads and the
   // row / row count of a piece follow from its start.
   int bal;
+  // BAL: the point pieces' 6 values copied contiguously, in piece order from
+  // piece pp0 on (null until copied for the current linearization)
+  const TS* ptvals;
+  int64_t pp0;
 };
+
+// ptvals[6 i + k] = values[p_start[pp0 + i] + k], the point halves of the BAL
+// emissions in the segment pass's piece order (one pass per linearization).
+template <class TS>
+__global__ void k_lsmr_point_copy(int64_t npp, int64_t pp0, const int64_t* p_start, const TS* values, TS* ptvals) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= npp) return;
+  const int64_t start = p_start[pp0 + i];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ptvals[6 * i + k] = values[start + k];
+}
 
 // n contiguous values at p into double (p 16-byte aligned when n is a
 // multiple of 4 / 2 for float / double, 8-byte aligned otherwise).
@@ -221,7 +236,7 @@ __device__ __forceinline__ void segment_accumulate(const LsmrDev<TS>& D, int64_t
         load_vals<18>(D.values + start, a);
       } else {
         double b[6];
-        load_vals<6>(D.values + start, b);
+        load_vals<6>(D.ptvals ? D.ptvals + 6 * (p - D.pp0) : D.values + start, b);
 #pragma unroll
         for (int k = 0; k < 6; ++k) a[k] = b[k];
       }
