@@ -3,8 +3,11 @@
 // kept on the device. Observations are stored in emission order.
 #include "bal.cuh"
 #include "kernels.cuh"
+#include "sort.cuh"
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 
 namespace fg {
 
@@ -250,13 +253,45 @@ __global__ void k_bal_stage(int64_t nc9, int64_t np3, const double* cams, const 
   else if (i < nc9 + np3) tpts[i - nc9] = pts[i - nc9] + delta[i];
 }
 
-// px[k] = pixels of observation order[k] (emission order).
-__global__ void k_bal_permute_pixels(int64_t o, const uint32_t* order, const double* raw, double* px) {
+// Per-device staging of problem ingestion: the raw observations and the sort
+// scratch, reused by every problem created on the device (allocated once, kept
+// for the life of the process).
+struct Ingest {
+  std::mutex m;
+  DBuf<uint32_t> cam, pt, order;
+  DBuf<double> pix;
+  DBuf<int> bad;
+  HBuf<int> h_bad;
+  SortScratch sort;
+};
+Ingest& ingest(int dev) {
+  static std::mutex g;
+  static std::map<int, Ingest*> pools;
+  std::lock_guard<std::mutex> lock(g);
+  Ingest*& p = pools[dev];
+  if (!p) p = new Ingest();
+  return *p;
+}
+
+// Observation checks of examples/bal/model.rs:78-79 (indices in range, finite
+// pixels): any failure sets *bad.
+__global__ void k_bal_validate(int64_t o, uint32_t nc, uint32_t np, const uint32_t* cam, const uint32_t* pt,
+                               const double2* pix, int* bad) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= o) return;
+  const double2 x = pix[i];
+  if (cam[i] >= nc || pt[i] >= np || !isfinite(x.x) || !isfinite(x.y)) *bad = 1;
+}
+
+// Emission k takes insertion index order[k]: camera, point and pixels.
+__global__ void k_bal_gather(int64_t o, const uint32_t* order, const uint32_t* rc, const uint32_t* rp,
+                             const double2* rx, uint32_t* oc, uint32_t* op, double2* px) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= o) return;
-  const int64_t i = order[k];
-  px[2 * k] = raw[2 * i];
-  px[2 * k + 1] = raw[2 * i + 1];
+  const uint32_t i = order[k];
+  oc[k] = rc[i];
+  op[k] = rp[i];
+  px[k] = rx[i];
 }
 
 fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const double* pp, const uint32_t* ocam,
@@ -267,53 +302,41 @@ fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const
   FG_TRY(select_device(dev));
   FG_TRY(device_stream(dev, &st));
   nsm = sm_count(dev);
-  // Host views of the observations (device inputs are copied down once).
-  std::vector<uint32_t> dc, dp;
-  std::vector<double> dx;
-  const uint32_t* hc = ocam;
-  const uint32_t* hp = opt;
-  const double* hx = pix;
-  if (on_device && o) {
-    dc.resize(o);
-    dp.resize(o);
-    dx.resize(2 * o);
-    FG_CUDA(cudaMemcpy(dc.data(), ocam, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    FG_CUDA(cudaMemcpy(dp.data(), opt, o * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    FG_CUDA(cudaMemcpy(dx.data(), pix, 2 * o * sizeof(double), cudaMemcpyDeviceToHost));
-    hc = dc.data();
-    hp = dp.data();
-    hx = dx.data();
+  if (c >= ((size_t)1 << 32) || p >= ((size_t)1 << 32) || o >= ((size_t)1 << 32)) {
+    set_error("BAL problem sizes must be below 2^32");
+    return FG_INVALID_EMISSION;
   }
-  for (size_t i = 0; i < o; ++i)
-    if (hc[i] >= nc || hp[i] >= np || !std::isfinite(hx[2 * i]) || !std::isfinite(hx[2 * i + 1])) {
+  const auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  FG_TRY(oc.resize(std::max<size_t>(o, 1)));
+  FG_TRY(op.resize(std::max<size_t>(o, 1)));
+  FG_TRY(px.resize(std::max<size_t>(2 * o, 1)));
+  if (o) {
+    // Emission order: frames in camera order, factors in insertion order (a
+    // stable order by camera); validated and gathered on the device.
+    Ingest& in = ingest(dev);
+    std::lock_guard<std::mutex> lock(in.m);
+    FG_TRY(in.cam.resize(o));
+    FG_TRY(in.pt.resize(o));
+    FG_TRY(in.order.resize(o));
+    FG_TRY(in.pix.resize(2 * o));
+    FG_TRY(in.bad.resize(1));
+    FG_TRY(in.h_bad.resize(1));
+    FG_CUDA(cudaMemsetAsync(in.bad.get(), 0, sizeof(int), st));
+    FG_CUDA(cudaMemcpyAsync(in.cam.get(), ocam, o * sizeof(uint32_t), kind, st));
+    FG_CUDA(cudaMemcpyAsync(in.pt.get(), opt, o * sizeof(uint32_t), kind, st));
+    FG_CUDA(cudaMemcpyAsync(in.pix.get(), pix, 2 * o * sizeof(double), kind, st));
+    const double2* raw = reinterpret_cast<const double2*>(in.pix.get());
+    FG_LAUNCH(k_bal_validate, grid_for(o, 256), 256, 0, st, (int64_t)o, (uint32_t)nc, (uint32_t)np, in.cam.get(),
+              in.pt.get(), raw, in.bad.get());
+    FG_TRY(stable_order(in.cam.get(), o, (uint32_t)nc, in.order.get(), nullptr, in.sort, st));
+    FG_LAUNCH(k_bal_gather, grid_for(o, 256), 256, 0, st, (int64_t)o, in.order.get(), in.cam.get(), in.pt.get(), raw,
+              oc.get(), op.get(), reinterpret_cast<double2*>(px.get()));
+    FG_CUDA(cudaMemcpyAsync(in.h_bad.get(), in.bad.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));  // the staging is free for the next problem after this
+    if (in.h_bad.get()[0]) {
       set_error("invalid observation index or value");
       return FG_INVALID_EMISSION;
     }
-  // Emission order: frames in camera order, factors in insertion order (a
-  // stable counting sort by camera); the pixels are permuted on the device.
-  std::vector<size_t> off(nc + 1, 0);
-  for (size_t i = 0; i < o; ++i) off[hc[i] + 1]++;
-  for (size_t i = 0; i < nc; ++i) off[i + 1] += off[i];
-  order.resize(o);
-  for (size_t i = 0; i < o; ++i) order[off[hc[i]]++] = (uint32_t)i;
-  h_oc.resize(o);
-  h_op.resize(o);
-  for (size_t k = 0; k < o; ++k) {
-    h_oc[k] = hc[order[k]];
-    h_op[k] = hp[order[k]];
-  }
-  FG_TRY(upload(oc, h_oc.data(), o, st));
-  FG_TRY(upload(op, h_op.data(), o, st));
-  FG_TRY(px.resize(std::max<size_t>(2 * o, 1)));
-  if (o) {
-    DBuf<double> raw;
-    DBuf<uint32_t> ord;
-    FG_TRY(raw.resize(2 * o));
-    FG_TRY(upload(ord, order.data(), o, st));
-    FG_CUDA(cudaMemcpyAsync(raw.get(), hx, 2 * o * sizeof(double), on_device ? cudaMemcpyDeviceToDevice
-                                                                              : cudaMemcpyHostToDevice, st));
-    FG_LAUNCH(k_bal_permute_pixels, grid_for(o, 256), 256, 0, st, (int64_t)o, ord.get(), raw.get(), px.get());
-    FG_CUDA(cudaStreamSynchronize(st));  // raw and ord die here
   }
   FG_TRY(cams.resize(std::max<size_t>(9 * nc, 1)));
   FG_TRY(pts.resize(std::max<size_t>(3 * np, 1)));
@@ -328,7 +351,6 @@ fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const
   FG_TRY(h_flag.resize(2));
   FG_TRY(d_flag.resize(2));
   FG_CUDA(cudaMemsetAsync(counters.get(), 0, 4 * sizeof(unsigned), st));
-  auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   if (nc) FG_CUDA(cudaMemcpyAsync(cams.get(), cp, 9 * nc * sizeof(double), kind, st));
   if (np) FG_CUDA(cudaMemcpyAsync(pts.get(), pp, 3 * np * sizeof(double), kind, st));
   FG_TRY(init_cams.resize(std::max<size_t>(9 * nc, 1)));
@@ -336,6 +358,22 @@ fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const
   if (nc) FG_CUDA(cudaMemcpyAsync(init_cams.get(), cams.get(), 9 * nc * sizeof(double), cudaMemcpyDeviceToDevice, st));
   if (np) FG_CUDA(cudaMemcpyAsync(init_pts.get(), pts.get(), 3 * np * sizeof(double), cudaMemcpyDeviceToDevice, st));
   FG_CUDA(cudaStreamSynchronize(st));
+  return FG_OK;
+}
+
+fg_status BalProblem::host_observations(const uint32_t** cam, const uint32_t** pt) {
+  if (!host_obs) {
+    h_oc.resize(no);
+    h_op.resize(no);
+    if (no) {
+      FG_CUDA(cudaMemcpyAsync(h_oc.data(), oc.get(), no * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      FG_CUDA(cudaMemcpyAsync(h_op.data(), op.get(), no * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      FG_CUDA(cudaStreamSynchronize(st));
+    }
+    host_obs = true;
+  }
+  *cam = h_oc.data();
+  *pt = h_op.data();
   return FG_OK;
 }
 
@@ -383,7 +421,15 @@ fg_status BalProblem::cost(bool trial, double* out) {
 
 fg_status BalProblem::linearize(Backend* b) {
   FG_TRY(b->clear());
-  FG_TRY(b->bind_bal(id, nc, np, no, h_oc.data(), h_op.data()));
+  BalObservations ob;
+  ob.problem_id = id;
+  ob.cameras = nc;
+  ob.points = np;
+  ob.observations = no;
+  ob.cam = oc.get();
+  ob.pt = op.get();
+  ob.host = [this](const uint32_t** c, const uint32_t** p) { return host_observations(c, p); };
+  FG_TRY(b->bind_bal(ob));
   if (nc) FG_LAUNCH(k_bal_camera_prep, grid_for(nc, 128), 128, 0, st, (int64_t)nc, cams.get(), prep.get());
   FG_CUDA(cudaMemsetAsync(d_flag.get(), 0, sizeof(int), st));
   if (no) {

@@ -48,8 +48,8 @@ struct BalProblem {
   int dev = 0, nsm = 148;
   cudaStream_t st = nullptr;
   size_t nc = 0, np = 0, no = 0;
-  std::vector<uint32_t> order;  // emission position -> insertion index
-  std::vector<uint32_t> h_oc, h_op;
+  std::vector<uint32_t> h_oc, h_op;  // host copies of oc and op, downloaded on first use
+  bool host_obs = false;
   DBuf<uint32_t> oc, op;
   DBuf<double> px, cams, pts, tcams, tpts, prep, tprep, partials, result, init_cams, init_pts, gauge;
   DBuf<unsigned> counters;
@@ -64,6 +64,7 @@ struct BalProblem {
   fg_status get_parameters(double* cp, double* pp);
   fg_status cost(bool trial, double* out);
   fg_status linearize(Backend* b);
+  fg_status host_observations(const uint32_t** cam, const uint32_t** pt);
   fg_status stage(const double* d_delta);
   void accept();
   void reject();

@@ -632,7 +632,7 @@ class DenseImpl final : public Backend {
     *s = solves;
     *i = 0;
   }
-  fg_status bind_bal(uint64_t, size_t, size_t, size_t, const uint32_t*, const uint32_t*) override {
+  fg_status bind_bal(const BalObservations&) override {
     set_error("the dense backends take host emissions only");
     return FG_UNSUPPORTED_STRUCTURE;
   }

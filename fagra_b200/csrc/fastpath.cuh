@@ -22,6 +22,7 @@
 // length alpha from p.q in the last block.
 #pragma once
 #include "kernels.cuh"
+#include "sort.cuh"
 #include <vector>
 
 namespace fg {
@@ -825,6 +826,48 @@ __global__ void k_coarse_cams(int64_t ncam, int nk, const double* wd, const TS* 
   }
 }
 
+// Warp tiles over point-major edges, built on the device: each segment of
+// TILE_SEG points is tiled greedily (contiguous point ranges of at most 32
+// edges and 32 points, the first tile starting at the segment's first point),
+// one thread per segment. Pass 0 counts each segment's tiles and flags a point
+// with more than 32 edges; after an exclusive scan of the counts, pass 1 writes
+// each tile's first edge and point and every edge's tile-local point index.
+constexpr int TILE_SEG = 1024;
+__global__ void k_fast_tiles(int pass, int64_t npt, const int64_t* pt_off, uint32_t* seg, uint32_t* total,
+                             uint32_t* too_deep, int64_t* e0, int64_t* p0, uint32_t* lp) {
+  const int64_t nseg = (npt + TILE_SEG - 1) / TILE_SEG;
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  const int64_t pa = s * TILE_SEG, pb = min(pa + TILE_SEG, npt);
+  int64_t te = pt_off[pa], tp = pa;
+  uint32_t t = pass ? seg[s] : 0u, count = 1;
+  if (pass) {
+    e0[t] = te;
+    p0[t] = tp;
+  }
+  for (int64_t p = pa; p < pb; ++p) {
+    const int64_t ea = pt_off[p], eb = pt_off[p + 1];
+    if (eb - ea > 32 && !pass) *too_deep = 1u;
+    if (p > tp && (eb - te > 32 || p + 1 - tp > 32)) {
+      te = ea;
+      tp = p;
+      ++count;
+      if (pass) {
+        ++t;
+        e0[t] = te;
+        p0[t] = tp;
+      }
+    }
+    if (pass)
+      for (int64_t k = ea; k < eb; ++k) lp[k] = (uint32_t)(p - tp);
+  }
+  if (!pass) seg[s] = count;
+  if (pass && s == nseg - 1) {
+    e0[*total] = pt_off[npt];
+    p0[*total] = npt;
+  }
+}
+
 template <class TS>
 struct FastPath {
   bool on = false;          // records are current and the shape qualifies
@@ -847,36 +890,36 @@ struct FastPath {
     tuned = false;
   }
 
-  // Warp tiles over point-major edges: greedy contiguous point ranges of at
-  // most 32 edges; a point with more than 32 observations keeps the generic path.
+  // Tiles for the current structure from the device point offsets; a point
+  // with more than 32 observations leaves the generic operator in place.
+  DBuf<uint32_t> d_tile_aux;  // per-segment tile counts | total | too-deep flag
+  HBuf<uint32_t> h_tile_aux;
   template <class Impl>
-  fg_status build(Impl& s, const std::vector<int64_t>& pt_off) {
-    std::vector<int64_t> e0{0}, p0{0};
-    std::vector<uint32_t> lp(s.nedges);
-    for (int64_t p = 0; p < (int64_t)s.nP; ++p) {
-      int64_t c = pt_off[p + 1] - pt_off[p];
-      if (c > 32) return FG_OK;
-      if ((pt_off[p + 1] - e0.back()) > 32 || (p + 1 - p0.back()) > 32) {
-        e0.push_back(pt_off[p]);
-        p0.push_back(p);
-      }
-    }
-    e0.push_back((int64_t)s.nedges);
-    p0.push_back((int64_t)s.nP);
-    nwt = (int64_t)e0.size() - 1;
-    for (int64_t t = 0; t < nwt; ++t)
-      for (int64_t p = p0[t]; p < p0[t + 1]; ++p)
-        for (int64_t k = pt_off[p]; k < pt_off[p + 1]; ++k) lp[k] = (uint32_t)(p - p0[t]);
-    nstages = (nwt + FastShape<TS>::WPS - 1) / FastShape<TS>::WPS;
+  fg_status build(Impl& s) {
+    const int64_t nP = (int64_t)s.nP, nseg = (nP + TILE_SEG - 1) / TILE_SEG;
     cudaStream_t st = s.st;
-    FG_TRY(upload(d_pbeg, p0.data(), p0.size(), st));
-    FG_TRY(upload(d_ebeg, e0.data(), e0.size(), st));
-    FG_TRY(upload(d_lp, lp.data(), lp.size(), st));
+    FG_TRY(d_tile_aux.resize((size_t)nseg + 2));
+    FG_TRY(h_tile_aux.resize(2));
+    FG_TRY(d_pbeg.resize((size_t)nP + 1));
+    FG_TRY(d_ebeg.resize((size_t)nP + 1));
+    FG_TRY(d_lp.resize(std::max<size_t>(s.nedges, 1)));
+    uint32_t* aux = d_tile_aux.get();
+    FG_CUDA(cudaMemsetAsync(aux, 0, ((size_t)nseg + 2) * sizeof(uint32_t), st));
+    const int64_t* off = s.d_pt_edge_off.get();
+    FG_LAUNCH(k_fast_tiles, grid_for(nseg, 128), 128, 0, st, 0, nP, off, aux, aux + nseg, aux + nseg + 1,
+              d_ebeg.get(), d_pbeg.get(), d_lp.get());
+    FG_LAUNCH(k_scan_exclusive_u32, 1, 1024, 0, st, aux, nseg, aux + nseg);
+    FG_LAUNCH(k_fast_tiles, grid_for(nseg, 128), 128, 0, st, 1, nP, off, aux, aux + nseg, aux + nseg + 1,
+              d_ebeg.get(), d_pbeg.get(), d_lp.get());
+    FG_CUDA(cudaMemcpyAsync(h_tile_aux.get(), aux + nseg, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (h_tile_aux.get()[1]) return FG_OK;
+    nwt = (int64_t)h_tile_aux.get()[0];
+    nstages = (nwt + FastShape<TS>::WPS - 1) / FastShape<TS>::WPS;
     FG_TRY(d_erec.resize(std::max<size_t>(s.nedges * 28, 1)));
     FG_TRY(d_prec.resize(std::max<size_t>(s.nP * 8, 1)));
     FG_TRY(d_error.resize(1));
     FG_CUDA(cudaMemsetAsync(d_error.get(), 0, sizeof(int), st));
-    FG_CUDA(cudaStreamSynchronize(st));
     structure = true;
     return FG_OK;
   }
@@ -892,7 +935,7 @@ struct FastPath {
                            FastSmem<TS, TS>::bytes((int64_t)s.nC, false));
     if (need > (size_t)optin) return false;  // accumulator does not fit one SM's shared memory
     if (!structure) {
-      if (build(s, s.h_pt_off) != FG_OK || !structure) return false;
+      if (build(s) != FG_OK || !structure) return false;
       attr_set[0][0] = attr_set[0][1] = attr_set[1][0] = attr_set[1][1] = 0;
     }
     grid = sm_count(s.dev);

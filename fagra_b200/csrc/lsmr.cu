@@ -355,11 +355,14 @@ class LsmrImpl final : public Backend {
     prepared_mode = MODE_NONE;
   }
 
-  fg_status bind_bal(uint64_t id, size_t cams, size_t pts, size_t obs, const uint32_t* ocam,
-                     const uint32_t* opt_) override {
+  fg_status bind_bal(const BalObservations& ob) override {
+    const uint64_t id = ob.problem_id;
+    const size_t cams = ob.cameras, pts = ob.points, obs = ob.observations;
     if (dim != 9 * cams + 3 * pts) return FG_DIMENSION_MISMATCH;
     prepared_mode = MODE_NONE;
     if (!(bal_bound == id && structure_built)) {
+      const uint32_t *ocam = nullptr, *opt_ = nullptr;
+      FG_TRY(ob.host(&ocam, &opt_));
       // Emission k: rows 2k..2k+1, camera block (9 columns) then point block.
       h_erow.resize(obs + 1);
       h_eblk.resize(obs + 1);

@@ -5,9 +5,13 @@
 #include "camside.cuh"
 #include "fastpath.cuh"
 #include "setup.cuh"
+#include "sort.cuh"
 #include "gnn.cuh"
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 
 namespace fg {
 
@@ -79,7 +83,6 @@ class SchurImpl final : public Backend {
 
   // ---- numerics
   DBuf<double> d_g, d_scales, d_work, d_rhs, d_zred, d_step, d_tmpd, d_qd, d_jd, d_camjt;
-  std::vector<int64_t> h_pt_off;  // point -> first point-major edge (host copy)
   DBuf<TS> d_gram, d_factors, d_precond, d_cross, d_minv;
   DBuf<TS> d_x, d_r, d_z, d_pp, d_q, d_t;  // PCG vectors in the storage precision
   DBuf<double> d_partials, d_norm;
@@ -105,8 +108,8 @@ class SchurImpl final : public Backend {
   // the FP32 solve ended on an FP64 replacement residual of the z in d_zred
   // (h_pcg holds it), so verification need not recompute S z - b
   bool final_residual_known = false;
-  HBuf<uint32_t> h_bal_stage;  // pinned staging of the BAL emission arrays and orders
-  DBuf<uint32_t> d_bal_stage;
+  DBuf<uint32_t> d_bal_stage;  // emission orders by camera and by point, and the sorted keys
+  SortScratch sort_scratch;
   int nk = 0;
   bool coarse_on = false, basis_scaled = false;
   DBuf<double> d_basis, d_Wd, d_E, d_G;
@@ -312,7 +315,6 @@ class SchurImpl final : public Backend {
     FG_TRY(upload(d_var_off, var_off.data(), var_off.size(), st));
     FG_TRY(upload(d_var_blk, var_blk.data(), var_blk.size(), st));
     FG_TRY(upload(d_pt_edge_off, pt_off.data(), pt_off.size(), st));
-    h_pt_off = pt_off;
     FG_TRY(upload(d_pt_edge, pt_e.data(), pt_e.size(), st));
     FG_TRY(upload(d_cam_edge_off, cam_off.data(), cam_off.size(), st));
     FG_TRY(upload(d_cam_edge, cam_e.data(), cam_e.size(), st));
@@ -328,63 +330,44 @@ class SchurImpl final : public Backend {
     return FG_OK;
   }
 
-  // The maps build_structure derives, for the BAL emission layout: the host
-  // only counts and orders emissions by camera and by point (stable counting
-  // sorts over 32-bit indices); the kernel writes every device map.
+  // The maps build_structure derives, for the BAL emission layout, built on
+  // the device: stable orders of the emissions by camera and by point (radix
+  // sorts), their offsets, then every map in one pass over the emissions.
   fg_status build_structure_bal(size_t cams, size_t pts, size_t obs, const uint32_t* ocam, const uint32_t* opt) {
     rows = 2 * obs;
     nblocks = 2 * obs;
     nedges = obs;
     const size_t nvar = nC + nP;
-    std::vector<int64_t> cam_off(nC + 1, 0), pt_off(nP + 1, 0);
-    for (size_t k = 0; k < obs; ++k) {
-      if (ocam[k] >= cams || opt[k] >= pts) {
-        set_error("BAL observation index out of range");
-        return FG_DIMENSION_MISMATCH;
-      }
-      cam_off[ocam[k] + 1]++;
-      pt_off[opt[k] + 1]++;
-    }
-    for (size_t c = 0; c < nC; ++c) cam_off[c + 1] += cam_off[c];
-    for (size_t p = 0; p < nP; ++p) pt_off[p + 1] += pt_off[p];
-    FG_TRY(h_bal_stage.resize(std::max<size_t>(4 * obs, 1)));  // ocam | opt | cam_order | pt_order
-    uint32_t* h = h_bal_stage.get();
-    std::memcpy(h, ocam, obs * sizeof(uint32_t));
-    std::memcpy(h + obs, opt, obs * sizeof(uint32_t));
-    {
-      std::vector<int64_t> fc(cam_off.begin(), cam_off.end() - 1), fp(pt_off.begin(), pt_off.end() - 1);
-      for (size_t k = 0; k < obs; ++k) {
-        h[2 * obs + fc[ocam[k]]++] = (uint32_t)k;
-        h[3 * obs + fp[opt[k]]++] = (uint32_t)k;
-      }
-    }
-    std::vector<int64_t> var_off(nvar + 1, 0);
-    for (size_t c = 0; c <= nC; ++c) var_off[c] = cam_off[c];
-    for (size_t p = 1; p <= nP; ++p) var_off[nC + p] = (int64_t)obs + pt_off[p];
-    h_observed.assign(nvar, 0);
-    for (size_t v = 0; v < nvar; ++v) h_observed[v] = var_off[v + 1] > var_off[v];
-    DBuf<uint32_t>& d_stage = d_bal_stage;
-    FG_TRY(d_stage.resize(std::max<size_t>(4 * obs, 1)));
-    if (obs) FG_CUDA(cudaMemcpyAsync(d_stage.get(), h, 4 * obs * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    if (cams >= ((size_t)1 << 32) || pts >= ((size_t)1 << 32)) return FG_UNSUPPORTED_STRUCTURE;
+    FG_TRY(d_bal_stage.resize(std::max<size_t>(4 * obs, 1)));  // cam_order | pt_order | sorted cams | sorted points
+    uint32_t* stage = d_bal_stage.get();
+    FG_TRY(d_cam_edge_off.resize(nC + 1));
+    FG_TRY(d_pt_edge_off.resize(nP + 1));
+    FG_TRY(d_var_off.resize(nvar + 1));
+    FG_TRY(d_observed.resize(std::max<size_t>(nvar, 1)));
+    FG_TRY(stable_order(ocam, obs, (uint32_t)cams, stage, stage + 2 * obs, sort_scratch, st));
+    FG_TRY(key_offsets(stage + 2 * obs, obs, (uint32_t)cams, d_cam_edge_off.get(), st));
+    FG_TRY(stable_order(opt, obs, (uint32_t)pts, stage + obs, stage + 3 * obs, sort_scratch, st));
+    FG_TRY(key_offsets(stage + 3 * obs, obs, (uint32_t)pts, d_pt_edge_off.get(), st));
     FG_TRY(d_blocks.resize(std::max<size_t>(nblocks, 1)));
     FG_TRY(d_edges.resize(std::max<size_t>(nedges, 1)));
     FG_TRY(d_var_blk.resize(std::max<size_t>(nblocks, 1)));
     FG_TRY(d_cam_edge.resize(std::max<size_t>(nedges, 1)));
     FG_TRY(d_pt_edge.resize(std::max<size_t>(nedges, 1)));
     FG_TRY(d_emi_off.resize(obs + 1));
-    FG_LAUNCH(k_bal_structure, grid_for(obs + 1, 256), 256, 0, st, (int64_t)obs, (int64_t)cams, d_stage.get(),
-              d_stage.get() + obs, d_stage.get() + 2 * obs, d_stage.get() + 3 * obs, d_blocks.get(), d_edges.get(),
-              d_var_blk.get(), d_cam_edge.get(), d_pt_edge.get(), d_emi_off.get());
-    FG_TRY(upload(d_var_off, var_off.data(), var_off.size(), st));
-    FG_TRY(upload(d_pt_edge_off, pt_off.data(), pt_off.size(), st));
-    FG_TRY(upload(d_cam_edge_off, cam_off.data(), cam_off.size(), st));
-    FG_TRY(upload(d_observed, h_observed.data(), h_observed.size(), st));
-    h_pt_off = pt_off;
+    FG_LAUNCH(k_bal_structure, grid_for(obs + 1, 256), 256, 0, st, (int64_t)obs, (int64_t)cams, ocam, opt, stage,
+              stage + obs, d_blocks.get(), d_edges.get(), d_var_blk.get(), d_cam_edge.get(), d_pt_edge.get(),
+              d_emi_off.get());
+    FG_LAUNCH(k_bal_var_offsets, grid_for(nvar + 1, 256), 256, 0, st, (int64_t)nC, (int64_t)nP, (int64_t)obs,
+              d_cam_edge_off.get(), d_pt_edge_off.get(), d_var_off.get(), d_observed.get());
+    h_observed.resize(nvar);
+    if (nvar)
+      FG_CUDA(cudaMemcpyAsync(h_observed.data(), d_observed.get(), nvar, cudaMemcpyDeviceToHost, st));
     nemissions = obs;
     pure_pairs = obs > 0;
     FG_TRY(d_cross.resize(std::max<size_t>(nedges * cw * pw, 1)));
     FG_TRY(d_jd.resize(std::max<size_t>(rows, 1)));
-    FG_CUDA(cudaStreamSynchronize(st));  // the host staging may be reused after this
+    FG_CUDA(cudaStreamSynchronize(st));
     structure_valid = true;
     fast.invalidate();
     drop_graphs();
@@ -778,9 +761,29 @@ class SchurImpl final : public Backend {
   }
   // Operator autotuner: times each FP32 single-pass variant (TMA-staged
   // stages, direct global loads, prefetching direct loads) on this structure
-  // and keeps the fastest. Runs once per structure; the factorization it needs
-  // is redone by every solve.
+  // and keeps the fastest. Runs once per structure shape (device, cameras,
+  // points, edges, warp tiles) in the process; the factorization it needs is
+  // redone by every solve.
   static constexpr int NVARIANTS = 3;
+  struct TunedShape {
+    int dev;
+    int64_t ncam, npt, nedge, nwt;
+    bool operator<(const TunedShape& o) const {
+      return std::tie(dev, ncam, npt, nedge, nwt) < std::tie(o.dev, o.ncam, o.npt, o.nedge, o.nwt);
+    }
+  };
+  struct TunedChoice {
+    int variant;
+    double seconds[NVARIANTS];
+  };
+  static std::mutex& tuned_mutex() {
+    static std::mutex m;
+    return m;
+  }
+  static std::map<TunedShape, TunedChoice>& tuned_shapes() {
+    static auto* m = new std::map<TunedShape, TunedChoice>();
+    return *m;
+  }
   double tuned_seconds[NVARIANTS] = {0, 0, 0};
   void operator_info(int* variant, double* seconds) const override {
     *variant = fast.enabled() ? fast.variant : 0;
@@ -794,6 +797,18 @@ class SchurImpl final : public Backend {
       fast.tuned = true;
       drop_graphs();
       return FG_OK;
+    }
+    const TunedShape shape{dev, (int64_t)nC, (int64_t)nP, (int64_t)nedges, fast.nwt};
+    {
+      std::lock_guard<std::mutex> lock(tuned_mutex());
+      auto it = tuned_shapes().find(shape);
+      if (it != tuned_shapes().end()) {
+        fast.variant = it->second.variant;
+        for (int v = 0; v < NVARIANTS; ++v) tuned_seconds[v] = it->second.seconds[v];
+        fast.tuned = true;
+        drop_graphs();
+        return FG_OK;
+      }
     }
     unsigned fb = 0;
     FG_TRY(factor(1.0, &fb));
@@ -825,6 +840,12 @@ class SchurImpl final : public Backend {
     cudaEventDestroy(b);
     fast.variant = best_v;
     fast.tuned = true;
+    {
+      std::lock_guard<std::mutex> lock(tuned_mutex());
+      TunedChoice c{best_v, {}};
+      for (int v = 0; v < NVARIANTS; ++v) c.seconds[v] = tuned_seconds[v];
+      tuned_shapes()[shape] = c;
+    }
     drop_graphs();
     return FG_OK;
   }
@@ -1183,13 +1204,13 @@ class SchurImpl final : public Backend {
     ready = false;
   }
 
-  fg_status bind_bal(uint64_t id, size_t cams, size_t pts, size_t obs, const uint32_t* ocam,
-                     const uint32_t* opt_) override {
+  fg_status bind_bal(const BalObservations& ob) override {
+    const uint64_t id = ob.problem_id;
+    const size_t cams = ob.cameras, pts = ob.points, obs = ob.observations;
     if (cw != 9 || pw != 3) return FG_UNSUPPORTED_STRUCTURE;
     if (retained != 9 * cams || dim != 9 * cams + 3 * pts) return FG_DIMENSION_MISMATCH;
     if (bal_bound == id && structure_valid) return FG_OK;
-    // Emission order: one Frame batch per camera, factors in insertion order.
-    FG_TRY(build_structure_bal(cams, pts, obs, ocam, opt_));
+    FG_TRY(build_structure_bal(cams, pts, obs, ob.cam, ob.pt));
     up_blocks.clear();
     up_edges.clear();
     nvalues = 24 * obs;

@@ -2,6 +2,7 @@
 // backend (src/schur.rs) over a block-sparse linearization (src/linear_model.rs).
 #pragma once
 #include "common.cuh"
+#include <functional>
 
 namespace fg {
 
@@ -17,6 +18,16 @@ struct DEdgeMeta {
 };
 struct HostBlock {
   size_t row, col, rows, cols, start;
+};
+// Observations of a device BAL problem in emission order: one Frame batch per
+// camera (examples/bal/model.rs:187-200), factors in insertion order.
+struct BalObservations {
+  uint64_t problem_id = 0;
+  size_t cameras = 0, points = 0, observations = 0;
+  const uint32_t* cam = nullptr;  // device: camera of each emission (nondecreasing)
+  const uint32_t* pt = nullptr;   // device: point of each emission
+  // Host copies of cam and pt, downloaded on first use.
+  std::function<fg_status(const uint32_t**, const uint32_t**)> host;
 };
 struct HostEdge {
   size_t retained, eliminated, lblk, rblk;  // column offsets (partition local) + block ids
@@ -79,8 +90,7 @@ class Backend {
   virtual size_t dimension() const = 0;
   virtual void work(size_t* solves, size_t* iterations) const = 0;
   // Device BAL path: bind an implicit BAL structure and expose raw model storage.
-  virtual fg_status bind_bal(uint64_t problem_id, size_t cameras, size_t points, size_t observations,
-                             const uint32_t* order_cam, const uint32_t* order_pt) = 0;
+  virtual fg_status bind_bal(const BalObservations& obs) = 0;
   virtual void* values_device() = 0;   // T*, packed Jacobian values
   virtual double* negres_device() = 0;  // -r
   virtual bool is_f32() const = 0;

@@ -305,4 +305,16 @@ __global__ void k_bal_structure(int64_t obs, int64_t ncam, const uint32_t* ocam,
   pt_edge[k] = ep;
 }
 
+// Variable offsets of the BAL structure (cameras, then points; every variable
+// lists its emissions) and which variables any emission touches.
+__global__ void k_bal_var_offsets(int64_t ncam, int64_t npt, int64_t obs, const int64_t* cam_off,
+                                  const int64_t* pt_off, int64_t* var_off, uint8_t* observed) {
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v > ncam + npt) return;
+  auto at = [&](int64_t u) { return u <= ncam ? cam_off[u] : obs + pt_off[u - ncam]; };
+  const int64_t o = at(v);
+  var_off[v] = o;
+  if (v < ncam + npt) observed[v] = at(v + 1) > o;
+}
+
 }  // namespace fg
