@@ -6,8 +6,9 @@ bal1k: 1,000 cameras, 200,000 points, ~1.1M observations) from its initial
 estimates until the accepted cost is within 1e-6 relative of the f64 oracle's
 final cost (tests/golden/<workload>_oracle.json). `value` is the device time
 of that solve with all inputs resident in HBM (CUDA events on the library
-stream); `e2e` is the same metric through the public C ABI from host arrays
-(problem upload, solve, parameter read-back inside the timed region).
+stream); `e2e` is the same metric through the public C ABI from page-locked
+host arrays (problem upload and ingestion, solve, parameter read-back into
+page-locked arrays, problem release: all inside the timed region).
 
 Forms: `fast` = FP32 bulk storage and Krylov recurrences with FP64 iterate,
 dots, cost and residual replacement, CG relative tolerance 1e-8 (the per-step
@@ -309,9 +310,18 @@ def run_gpu(args, rank: int, world: int, device: int):
     e2e = None
     if not args.no_e2e:
         backend = head_backend
-        cams = np.ascontiguousarray(data.cameras)
-        pts = np.ascontiguousarray(data.points)
-        oc, op, px = (np.ascontiguousarray(a) for a in (data.obs_camera, data.obs_point, data.obs_pixel))
+        keep = []
+
+        def pinned(a):  # host array in page-locked memory (the inputs' and results' home)
+            buf = torch.empty(max(a.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+            keep.append(buf)
+            v = buf.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
+            v[...] = a
+            return v
+
+        cams, pts = pinned(np.ascontiguousarray(data.cameras)), pinned(np.ascontiguousarray(data.points))
+        oc, op, px = (pinned(np.ascontiguousarray(a)) for a in (data.obs_camera, data.obs_point, data.obs_pixel))
+        out = (pinned(np.zeros_like(cams)), pinned(np.zeros_like(pts)))
         h2d = cams.nbytes + pts.nbytes + oc.nbytes + op.nbytes + px.nbytes
         d2h = cams.nbytes + pts.nbytes
         lmo, oo = fg.LmOptions().c(), opts.c()
@@ -321,7 +331,7 @@ def run_gpu(args, rank: int, world: int, device: int):
             rep, st = _lib.ReportC(), _lib.LmStatisticsC()
             code = _lib.lib.fg_lm_solve_bal_to_cost(backend.handle, p._bal_handle, C.byref(oo), C.byref(lmo),
                                                     target, C.byref(rep), C.byref(st))
-            c2, p2 = p.parameters()
+            p.parameters(out=out)
             p.close()
             return code, rep.termination
 

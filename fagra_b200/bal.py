@@ -41,9 +41,16 @@ class BalProblem:
         raise_for_status(lib.fg_bal_cost(self._bal_handle, C.byref(out)))
         return out.value
 
-    def parameters(self) -> tuple[np.ndarray, np.ndarray]:
-        cams = np.zeros((self.num_cameras, 9))
-        pts = np.zeros((self.num_points, 3))
+    def parameters(self, out=None) -> tuple[np.ndarray, np.ndarray]:
+        """Current cameras (C,9) and points (P,3); `out` = (cams, pts), C-contiguous
+        float64 arrays of those shapes (e.g. pinned host memory), receives them."""
+        if out is None:
+            cams, pts = np.zeros((self.num_cameras, 9)), np.zeros((self.num_points, 3))
+        else:
+            cams, pts = out
+            for a, n in ((cams, 9 * self.num_cameras), (pts, 3 * self.num_points)):
+                if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n:
+                    raise ValueError("out arrays must be C-contiguous float64 of the parameter shapes")
         raise_for_status(lib.fg_bal_get_parameters(self._bal_handle, cams.ctypes.data_as(dptr),
                                                    pts.ctypes.data_as(dptr)))
         return cams, pts

@@ -307,6 +307,15 @@ fg_status BalProblem::init(size_t c, size_t p, size_t o, const double* cp, const
     return FG_INVALID_EMISSION;
   }
   const auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  // Problem storage comes from the library pool in the library stream's order:
+  // creating and destroying problems maps and unmaps no device memory.
+  oc.use_pool(dev, st);
+  op.use_pool(dev, st);
+  for (DBuf<double>* b : {&px, &cams, &pts, &tcams, &tpts, &prep, &tprep, &partials, &result, &init_cams, &init_pts,
+                          &gauge})
+    b->use_pool(dev, st);
+  counters.use_pool(dev, st);
+  d_flag.use_pool(dev, st);
   FG_TRY(oc.resize(std::max<size_t>(o, 1)));
   FG_TRY(op.resize(std::max<size_t>(o, 1)));
   FG_TRY(px.resize(std::max<size_t>(2 * o, 1)));

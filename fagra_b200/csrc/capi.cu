@@ -55,6 +55,33 @@ fg_status device_stream(int device, cudaStream_t* out) {
   return FG_OK;
 }
 
+cudaMemPool_t library_pool(int device) {
+  static cudaMemPool_t pools[64] = {};
+  static bool tried[64] = {};
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!tried[device]) {
+    tried[device] = true;
+    int supported = 0;
+    cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, device);
+    if (supported) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = device;
+      cudaMemPool_t p = nullptr;
+      if (cudaMemPoolCreate(&p, &props) == cudaSuccess) {
+        uint64_t keep = (uint64_t)4 << 30;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = p;
+      } else {
+        cudaGetLastError();
+      }
+    }
+  }
+  return pools[device];
+}
+
 int sm_count(int device) { return (device >= 0 && device < 64 && g_sms[device]) ? g_sms[device] : 148; }
 
 }  // namespace fg
@@ -106,7 +133,7 @@ FG_API void fg_schur_default_options(fg_schur_options* o) {
   o->precision = FG_PRECISION_F64;
   o->preconditioner = FG_PRECOND_RETAINED_BLOCKS;
   o->device = 0;
-  o->residual_replacement = 1e-4;
+  o->residual_replacement = 0;  // automatic spacing
   o->operator_variant = 0;
   o->coarse_correction = 0;
 }

@@ -41,23 +41,44 @@ extern std::atomic<uint64_t> g_launches;
 fg_status device_stream(int device, cudaStream_t* out);
 fg_status select_device(int device);
 int sm_count(int device);
+// The library's stream-ordered memory pool on a device (keeps up to 4 GiB of
+// freed memory mapped for reuse); nullptr if the device has none.
+cudaMemPool_t library_pool(int device);
 
-// Grow-only device buffer: a warm workspace never reallocates.
+// Grow-only device buffer: a warm workspace never reallocates. A buffer given
+// a stream with use_pool() allocates from the library pool in that stream's
+// order and frees without a device synchronization (for objects whose memory
+// only that stream touches, e.g. per-problem storage).
 template <class T>
 struct DBuf {
   T* ptr = nullptr;
   size_t n = 0, cap = 0;
+  cudaStream_t pool_stream = nullptr;
+  cudaMemPool_t pool = nullptr;
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
-  ~DBuf() { if (ptr) cudaFree(ptr); }
+  ~DBuf() { release(); }
+  void use_pool(int device, cudaStream_t s) {
+    if (ptr) return;  // only before the first allocation
+    pool = library_pool(device);
+    pool_stream = pool ? s : nullptr;
+  }
+  void release() {
+    if (ptr) {
+      if (pool_stream) cudaFreeAsync(ptr, pool_stream);
+      else cudaFree(ptr);
+    }
+    ptr = nullptr;
+  }
   fg_status resize(size_t count) {
     if (count > cap) {
-      if (ptr) cudaFree(ptr);
-      ptr = nullptr;
+      release();
       cap = 0;
       size_t want = count + count / 8 + 16;
-      cudaError_t e = cudaMalloc(&ptr, want * sizeof(T));
+      cudaError_t e = pool_stream ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr), want * sizeof(T), pool,
+                                                            pool_stream)
+                                  : cudaMalloc(&ptr, want * sizeof(T));
       if (e != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation failed");

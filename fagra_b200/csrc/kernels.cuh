@@ -527,6 +527,9 @@ __global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q,
       if (MIXED && (conv || st->iterations >= st->max_iterations)) {
         st->done = 2;
         st->replace = 1;
+        // the search direction continues if the FP64 residual disagrees
+        st->beta = st->rz > 0 ? tot[1] / st->rz : 0.0;
+        st->rz = tot[1];
       } else if (!MIXED && conv) {
         st->done = 1;
         st->termination = FG_TERM_CONVERGED;
@@ -621,8 +624,10 @@ __global__ void k_pcg_start(Layout L, const double* b, TX* x, TS* r, TS* z, TS* 
 
 // FP64 residual replacement, gated by st->replace: r = b - S xd (qd = S xd in
 // FP64 arithmetic), z = Minv r, rz = r.z. Ends the solve when the FP64 residual
-// meets the threshold; restarts the search direction (beta = 0) when the
-// recurrence had claimed convergence but the FP64 residual disagrees.
+// meets the threshold. When the recurrence had claimed convergence but the
+// FP64 residual disagrees, the iteration goes on along the same search
+// direction (beta from the recurrence, as after a periodic replacement):
+// restarting from steepest descent would discard the Krylov space built so far.
 template <int CW, class TS, bool CO>
 __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* r, TS* z, const TS* minv,
                                double* partials, PcgState* st, const TS* W, const double* G, int nk) {
@@ -684,7 +689,6 @@ __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* 
         st->termination = FG_TERM_ITERATION_LIMIT;
       } else if (st->done == 2) {
         st->done = 0;
-        st->beta = 0;
       }
       st->counter3 = 0;
     }

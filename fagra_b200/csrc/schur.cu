@@ -1122,7 +1122,7 @@ class SchurImpl final : public Backend {
       init = PcgState{};
       init.max_iterations = (unsigned)std::min<size_t>(opt.max_iterations, 0xffffffffu);
       init.lambda = lambda;
-      double d = opt.residual_replacement > 0 && opt.residual_replacement < 1 ? opt.residual_replacement : 1e-4;
+      const double d = replacement_factor();
       init.delta2 = d * d;
       FG_CUDA(cudaMemcpyAsync(ps, &init, sizeof(PcgState), cudaMemcpyHostToDevice, st));
     }
@@ -1162,6 +1162,21 @@ class SchurImpl final : public Backend {
     *rounds = h.replacements;
     final_residual_known = h.done == 1 && h.termination == FG_TERM_CONVERGED;
     return FG_OK;
+  }
+
+  // Spacing of the FP64 residual replacements: the requested factor, or the
+  // reduction from ||b|| to the relative tolerance split into the fewest equal
+  // factors of at most 1e-4 (four decades per FP32 stretch). Longer stretches
+  // let the FP32 recurrence drift far enough to delay convergence by tens of
+  // iterations at tolerances far below FP32 precision; shorter ones cost
+  // replacements.
+  double replacement_factor() const {
+    const double r = opt.residual_replacement;
+    if (r > 0 && r < 1) return r;
+    const double tol = opt.relative_tolerance > 0 && opt.relative_tolerance < 1 ? opt.relative_tolerance : 1e-10;
+    const double decades = -std::log10(tol);
+    const double stretches = std::max(1.0, std::ceil(decades / 4.0 - 1e-9));
+    return std::pow(tol, 1.0 / stretches);
   }
 
   // Gated FP64 residual replacement: runs only while the device flag is set.

@@ -83,7 +83,9 @@ typedef struct {
   int preconditioner;        /* fg_preconditioner; default FG_PRECOND_RETAINED_BLOCKS */
   int device;                /* CUDA device ordinal; default 0 */
   double residual_replacement; /* FP32 mode: the recurrence residual is replaced by the FP64
-                                  residual b - S x each time it falls by this factor; default 1e-4 */
+                                  residual b - S x each time it falls by this factor; default 0 =
+                                  automatic: the reduction to the relative tolerance split into the
+                                  fewest equal factors of at most 1e-4 */
   int operator_variant;        /* FP32 BAL-shaped systems: 0 = autotune (default), 1..3 = force the
                                   reduced-operator variant of fg_schur_operator_info */
   int coarse_correction;       /* 1: two-level PCG, z = M r + W (W^T S W)^-1 W^T r with the coarse
