@@ -266,19 +266,27 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
     const unsigned parity = (k / FAST_STAGES) & 1;
     // Bounded wait; a timeout is made uniform across the group through the
     // flag read after the stage barrier, so no thread is left at the barrier.
+    // The warp tile's bounds come from global memory: load them before the
+    // wait so their latency overlaps the stage's arrival.
+    const int64_t wt = sidx * WPS + w;
+    int64_t e_lo = 0, p_lo = 0, gp0 = 0;  // gp0: global index of the tile's first point
+    int cnt = 0;
+    if (wt < tiles.nwt) {
+      const int64_t se0 = tiles.wt_e0[sidx * WPS], sp0 = tiles.wt_p0[sidx * WPS];
+      const int64_t ew = tiles.wt_e0[wt], ew1 = tiles.wt_e0[wt + 1];
+      gp0 = tiles.wt_p0[wt];
+      e_lo = ew - se0;
+      p_lo = gp0 - sp0;
+      cnt = (int)(ew1 - ew);
+    }
     const bool ok = mbar_wait_bounded(&gbar[b], parity, 1u << 22);
     if (!ok) fail[g] = 1;
-    const int64_t wt = sidx * WPS + w;
     if (ok && wt < tiles.nwt) {
       const TS* er = reinterpret_cast<const TS*>(gstage + b * sbytes);
       const TS* pr = er + (size_t)SE * 28;
-      const int64_t se0 = tiles.wt_e0[sidx * WPS], sp0 = tiles.wt_p0[sidx * WPS];
-      const int64_t e_lo = tiles.wt_e0[wt] - se0, p_lo = tiles.wt_p0[wt] - sp0;
-      const int cnt = (int)(tiles.wt_e0[wt + 1] - tiles.wt_e0[wt]);
       TV E[27];
       uint32_t cam = 0, lp = 0xFFFFu;
       TV u0 = 0, u1 = 0, u2 = 0;
-      const int64_t gp0 = tiles.wt_p0[wt];  // global index of the tile's first point
       if (lane < cnt) load_record<TV>(er + (size_t)(e_lo + lane) * 28, E, cam, lp);
       if (MODE != FAST_RHS && lane < cnt) {
         TV xc[9];
@@ -592,28 +600,31 @@ __global__ void __launch_bounds__(PF_THREADS, 1)
 }
 
 // q = lambda x + B x + sum_b partials[b] with x = z (+ beta p); 32 coordinates
-// x 8 partial-vector chunks per block. Optional p.q -> alpha in the last block.
+// x 32 rows of partial vectors per block, so each thread sums only a handful
+// of partials (one or two rounds of independent loads: the pass is latency-
+// bound, 5 MB). Optional p.q -> alpha in the last block.
+constexpr int FR_ROWS = 32;
 template <class TS, class TV>
-__global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram,
+__global__ void __launch_bounds__(FR_ROWS * 32) k_fast_reduce(int64_t ncam, int nparts, const TV* partials, const TS* gram,
                                                       const uint8_t* observed, const TV* z, const TV* pv,
                                                       const double* beta, double lambda, const double* lam_dev,
                                                       int use_gram, TV* q, double* dparts,
                                                       PcgState* st, const int* gate) {
   if (st && st->done) return;
   if (gate && !*gate) return;
-  __shared__ TV acc_s[8][33];
+  __shared__ TV acc_s[FR_ROWS][33];
   const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
   const int64_t ny = ncam * 9;
   const int64_t i = (int64_t)blockIdx.x * 32 + lx;
   TV acc = 0;
   if (i < ny) {
     int b = ly;
-    for (; b + 24 < nparts; b += 32) {
-      TV a0 = partials[(int64_t)b * ny + i], a1 = partials[(int64_t)(b + 8) * ny + i];
-      TV a2 = partials[(int64_t)(b + 16) * ny + i], a3 = partials[(int64_t)(b + 24) * ny + i];
+    for (; b + 3 * FR_ROWS < nparts; b += 4 * FR_ROWS) {
+      TV a0 = partials[(int64_t)b * ny + i], a1 = partials[(int64_t)(b + FR_ROWS) * ny + i];
+      TV a2 = partials[(int64_t)(b + 2 * FR_ROWS) * ny + i], a3 = partials[(int64_t)(b + 3 * FR_ROWS) * ny + i];
       acc += (a0 + a1) + (a2 + a3);
     }
-    for (; b < nparts; b += 8) acc += partials[(int64_t)b * ny + i];
+    for (; b < nparts; b += FR_ROWS) acc += partials[(int64_t)b * ny + i];
   }
   acc_s[ly][lx] = acc;
   __syncthreads();
@@ -621,7 +632,7 @@ __global__ void __launch_bounds__(256) k_fast_reduce(int64_t ncam, int nparts, c
   if (ly == 0 && i < ny) {
     TV sum = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) sum += acc_s[k][lx];
+    for (int k = 0; k < FR_ROWS; ++k) sum += acc_s[k][lx];
     const TV bv = pv ? (TV)*beta : (TV)0;
     int64_t cam = i / 9;
     int r = (int)(i % 9);
@@ -1001,7 +1012,7 @@ struct FastPath {
     if (std::is_same<TS, float>::value && std::is_same<TV, float>::value && (variant == 2 || variant == 3)) {
       FG_TRY(apply_direct(s, (const float*)x.z, (const float*)x.pprev, x.beta, (float*)parts,
                           pst ? &pst->done : nullptr, gate, variant == 3));
-      FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
+      FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
                 (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
                 dparts, pst, gate);
       return FG_OK;
@@ -1030,7 +1041,7 @@ struct FastPath {
       FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
                 parts, skip, gate, d_error.get(), FastExtra{});
     }
-    FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
+    FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
               (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
               dparts, pst, gate);
     return FG_OK;
@@ -1089,7 +1100,7 @@ struct FastPath {
     FG_LAUNCH(kern, grid, FAST_GROUPS * FastShape<TS>::WPS * 32, sm, s.st, (int64_t)s.nC, tl, d_erec.get(),
               d_prec.get(), w, (const double*)nullptr, (const double*)nullptr, d_parts_d.get(), (const int*)nullptr,
               (const int*)nullptr, d_error.get(), ex);
-    FG_LAUNCH((k_fast_reduce<TS, double>), grid_for(s.nC * 9, 32), 256, 0, s.st, (int64_t)s.nC, grid,
+    FG_LAUNCH((k_fast_reduce<TS, double>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
               (const double*)d_parts_d.get(), s.d_gram.get(), s.d_observed.get(), w, (const double*)nullptr,
               (const double*)nullptr, 1.0, (const double*)nullptr, 0, rhs_out, (double*)nullptr, (PcgState*)nullptr,
               (const int*)nullptr);

@@ -62,6 +62,11 @@ class SchurImpl final : public Backend {
   size_t up_rows = 0;
   bool structure_valid = false;
   bool pure_pairs = false;     // every emission is exactly one camera-point edge
+  // The device BAL layout: emission k is one camera-point edge with rows 2k,
+  // 2k+1 and values [24k, 24k+24) (camera 2x9, then point 2x3).
+  bool bal_layout() const { return source == DEVICE_BAL && pure_pairs && cw == 9 && pw == 3; }
+  DBuf<double> d_raw;  // BAL layout: raw Gram blocks (45 per camera, 6 per point) of the current model
+  DBuf<double> d_inv_scales;  // BAL layout: 1 / column scale
   bool cross_current = false;  // d_cross holds this linearization's cross blocks
 
   // ---- model source
@@ -420,6 +425,18 @@ class SchurImpl final : public Backend {
       gradient_current = false;
     }
     if (source == NONE) return FG_INVALID_OPTIONS;
+    if (!gradient_current && bal_layout()) {
+      // the gradient and the raw Gram blocks (for the column scales) in one pass
+      FG_TRY(d_raw.resize(45 * nC + 6 * nP + 1));
+      if (nC)
+        FG_LAUNCH((k_bal_cam_pass<TS, BAL_MOMENTS>), (unsigned)nC, 128, 0, st, (int64_t)nC, d_cam_edge_off.get(),
+                  d_values.get(), d_negres.get(), (const double*)nullptr, d_g.get(), d_raw.get());
+      if (nP)
+        FG_LAUNCH(k_bal_point_moments<TS>, grid_for(nP, 128), 128, 0, st, (int64_t)nP, (int64_t)retained,
+                  d_pt_edge_off.get(), d_pt_edge.get(), d_values.get(), d_negres.get(), d_g.get(),
+                  d_raw.get() + 45 * nC);
+      gradient_current = true;
+    }
     if (!gradient_current) {
       Layout L = layout();
       if (nC) {
@@ -470,14 +487,19 @@ class SchurImpl final : public Backend {
     Layout L = layout();
     int* bad = d_flags.get();
     FG_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(int), st));
-    if (nC) {
+    if (bal_layout()) {  // from the raw moments sync_model computed with the gradient
+      FG_TRY(d_inv_scales.resize(std::max<size_t>(dim, 1)));
+      if (nC + nP)
+        FG_LAUNCH(k_bal_scales_gram<TS>, grid_for(nC + nP, 128), 128, 0, st, (int64_t)nC, (int64_t)nP, d_raw.get(),
+                  d_raw.get() + 45 * nC, floor, d_scales.get(), d_inv_scales.get(), d_gram.get(), bad);
+    } else if (nC) {
       FG_CUDA(cudaMemsetAsync(d_gram.get(), 0, nC * cw * cw * sizeof(TS), st));
       FG_DISPATCH_WIDTHS(cw, pw, {
         FG_LAUNCH((k_cam_scales_gram<CW_, TS>), (unsigned)nC, 128, 0, st, L, d_var_off.get(), d_var_blk.get(),
                   d_blocks.get(), d_values.get(), floor, d_scales.get(), d_gram.get(), bad);
       });
     }
-    if (nP) {
+    if (nP && !bal_layout()) {
       FG_DISPATCH_WIDTHS(cw, pw, {
         FG_LAUNCH((k_point_scales_gram<PW_, TS>), grid_for(nP, 128), 128, 0, st, L, d_var_off.get(),
                   d_var_blk.get(), d_blocks.get(), d_values.get(), floor, d_scales.get(), d_gram.get(), bad);
@@ -488,9 +510,14 @@ class SchurImpl final : public Backend {
         // the reference-layout cross array is only needed by the generic
         // right-hand side / back-substitution and the Schur-diagonal factor
         cross_current = !pure_pairs || opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL || learned_active();
-        FG_LAUNCH(k_edge_records2<TS>, grid_for(nedges, REC_T), REC_T, 0, st, (int64_t)nedges, d_pt_edge.get(),
-                  d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), fast.d_lp.get(), fast.d_erec.get(),
-                  cross_current ? d_cross.get() : (TS*)nullptr, bad + 1);
+        if (bal_layout())
+          FG_LAUNCH(k_edge_records_bal<TS>, grid_for(nedges, REC_T), REC_T, 0, st, (int64_t)nedges,
+                    (int64_t)retained, d_pt_edge.get(), d_edges.get(), d_values.get(), d_inv_scales.get(),
+                    fast.d_lp.get(), fast.d_erec.get(), cross_current ? d_cross.get() : (TS*)nullptr, bad + 1);
+        else
+          FG_LAUNCH(k_edge_records2<TS>, grid_for(nedges, REC_T), REC_T, 0, st, (int64_t)nedges, d_pt_edge.get(),
+                    d_edges.get(), d_blocks.get(), d_values.get(), d_scales.get(), fast.d_lp.get(), fast.d_erec.get(),
+                    cross_current ? d_cross.get() : (TS*)nullptr, bad + 1);
         fast.on = true;
       } else {
         fast.on = false;

@@ -157,7 +157,8 @@ template <class TS>
 static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const int64_t* var_blk, const DBlockMeta* blocks,
                                   const TS* values, const double* jd, const double* negres, const double* g,
                                   const double* scales, const double* delta, double lambda, const double* camjt,
-                                  double* partials, VerifyState* vs) {
+                                  double* partials, VerifyState* vs, const int64_t* bal_pt_off,
+                                  const int64_t* bal_pt_edge) {
   int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   if (j < L.dim) {
@@ -165,8 +166,16 @@ static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const
     int off;
     L.locate(j, &v, &off);
     double nr = 0;
-    if (camjt && j < L.retained) nr = camjt[j];
-    else for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
+    if (camjt && j < L.retained) {
+      nr = camjt[j];
+    } else if (bal_pt_off) {  // device BAL layout: the point's emissions, 2 rows each
+      const int64_t pt = v - L.nC;
+      for (int64_t k = bal_pt_off[pt]; k < bal_pt_off[pt + 1]; ++k) {
+        const int64_t e = bal_pt_edge[k];
+        const TS* col = values + 24 * e + 18 + 2 * off;
+        nr += (double)col[0] * (jd[2 * e] - negres[2 * e]) + (double)col[1] * (jd[2 * e + 1] - negres[2 * e + 1]);
+      }
+    } else for (int64_t k = var_off[v]; k < var_off[v + 1]; ++k) {
       DBlockMeta b = blocks[var_blk[k]];
       const TS* col = values + b.start + (int64_t)off * b.rows;
       double s = 0;
@@ -358,7 +367,11 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
   else if (nemissions)
     FG_LAUNCH(k_jdelta<TS>, grid_for(nemissions, NT), NT, 0, st, (int64_t)nemissions, d_emi_off.get(), d_blocks.get(),
               d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
-  if (nC) {
+  const bool bal = bal_layout();
+  if (nC && bal) {
+    FG_LAUNCH((k_bal_cam_pass<TS, BAL_NORMAL>), (unsigned)nC, 128, 0, st, (int64_t)nC, d_cam_edge_off.get(),
+              d_values.get(), d_negres.get(), d_jd.get(), d_camjt.get(), (double*)nullptr);
+  } else if (nC) {
     FG_DISPATCH_WIDTHS(cw, pw, {
       FG_LAUNCH((k_cam_jt_block<CW_, TS, CAM_NORMAL>), (unsigned)nC, 128, 0, st, L, d_var_off.get(),
                 d_var_blk.get(), d_blocks.get(), d_values.get(), d_negres.get(), d_jd.get(), d_camjt.get());
@@ -367,7 +380,8 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
   if (dim)
     FG_LAUNCH(k_normal_residual<TS>, grid_for(dim, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(),
               d_blocks.get(), d_values.get(), d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
-              lambda, nC ? d_camjt.get() : (const double*)nullptr, d_partials.get() + 4 * 65536, vs);
+              lambda, nC ? d_camjt.get() : (const double*)nullptr, d_partials.get() + 4 * 65536, vs,
+              bal ? d_pt_edge_off.get() : (const int64_t*)nullptr, bal ? d_pt_edge.get() : (const int64_t*)nullptr);
   FG_CUDA(cudaMemcpyAsync(h_ver.get(), vs, sizeof(VerifyState), cudaMemcpyDeviceToHost, st));
   if (coarse_on)  // whether the coarse matrix of this solve was positive definite
     FG_CUDA(cudaMemcpyAsync(h_count.get() + 3, d_coarse_ok.get(), sizeof(int), cudaMemcpyDeviceToHost, st));

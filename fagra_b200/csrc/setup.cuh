@@ -135,6 +135,159 @@ __global__ void k_point_scales_gram(Layout L, const int64_t* var_off, const int6
     for (int r = 0; r < pw; ++r) g[c * pw + r] = (TS)(r >= c ? acc[c * pw + r] / (d[c] * d[r]) : 0.0);
 }
 
+// ---- Device BAL layout (one emission per observation k: rows 2k and 2k+1;
+// values [24k, 24k+18) the camera block, [24k+18, 24k+24) the point block, each
+// 2 rows column-major, so element (row i, column c) sits at 2c + i). A camera's
+// emissions are contiguous; a point's are listed by pt_edge. These kernels
+// replace the block-metadata walks of the generic kernels above with direct
+// 16-byte (8-byte for point blocks) loads.
+template <class TS>
+__device__ __forceinline__ void bal_cam_block(const TS* values, int64_t k, double (&v)[18]) {
+  if (sizeof(TS) == 4) {
+    const float4* q = reinterpret_cast<const float4*>(values + 24 * k);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float4 a = q[i];
+      v[4 * i] = a.x; v[4 * i + 1] = a.y; v[4 * i + 2] = a.z; v[4 * i + 3] = a.w;
+    }
+    const float2 b = *reinterpret_cast<const float2*>(values + 24 * k + 16);
+    v[16] = b.x;
+    v[17] = b.y;
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(values + 24 * k);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const double2 a = q[i];
+      v[2 * i] = a.x; v[2 * i + 1] = a.y;
+    }
+  }
+}
+template <class TS>
+__device__ __forceinline__ void bal_pt_block(const TS* values, int64_t k, double (&v)[6]) {
+  if (sizeof(TS) == 4) {
+    const float2* q = reinterpret_cast<const float2*>(values + 24 * k + 18);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float2 a = q[i];
+      v[2 * i] = a.x; v[2 * i + 1] = a.y;
+    }
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(values + 24 * k + 18);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double2 a = q[i];
+      v[2 * i] = a.x; v[2 * i + 1] = a.y;
+    }
+  }
+}
+
+// One block per camera over its contiguous emissions. MOMENTS: the gradient
+// J^T r (g) and the raw Gram J^T J (raw: 45 entries, columns c <= r in
+// column-major lower order) in one pass; NORMAL: J^T (jd - negres) (out).
+constexpr int BAL_MOMENTS = 0, BAL_NORMAL = 1;
+template <class TS, int MODE>
+__global__ void __launch_bounds__(128) k_bal_cam_pass(int64_t ncam, const int64_t* cam_off, const TS* values,
+                                                      const double* negres, const double* jd, double* out,
+                                                      double* raw) {
+  constexpr int NA = MODE == BAL_MOMENTS ? 54 : 9;
+  __shared__ double sh[32 * NA];
+  const int64_t cam = blockIdx.x;
+  if (cam >= ncam) return;
+  double acc[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) acc[k] = 0;
+  for (int64_t k = cam_off[cam] + threadIdx.x; k < cam_off[cam + 1]; k += blockDim.x) {
+    double v[18];
+    bal_cam_block<TS>(values, k, v);
+    const double2 nr = *reinterpret_cast<const double2*>(negres + 2 * k);
+    double w0 = -nr.x, w1 = -nr.y;
+    if (MODE == BAL_NORMAL) {
+      const double2 j = *reinterpret_cast<const double2*>(jd + 2 * k);
+      w0 = j.x - nr.x;
+      w1 = j.y - nr.y;
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) acc[NA - 9 + c] += v[2 * c] * w0 + v[2 * c + 1] * w1;
+    if (MODE == BAL_MOMENTS) {
+      int idx = 0;
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+#pragma unroll
+        for (int r = c; r < 9; ++r) acc[idx++] += v[2 * c] * v[2 * r] + v[2 * c + 1] * v[2 * r + 1];
+    }
+  }
+  block_allsums<NA>(acc, sh);
+  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
+    if (k >= NA - 9) out[cam * 9 + (k - (NA - 9))] = acc[k];
+    else raw[cam * 45 + k] = acc[k];
+  }
+}
+
+// One thread per point over its emissions (pt_edge): gradient J^T r into
+// g[retained + 3p + c] and the raw Gram (6 entries: 00, 10, 20, 11, 21, 22).
+template <class TS>
+__global__ void k_bal_point_moments(int64_t npt, int64_t retained, const int64_t* pt_off, const int64_t* pt_edge,
+                                    const TS* values, const double* negres, double* g, double* raw) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= npt) return;
+  double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t k = pt_off[p]; k < pt_off[p + 1]; ++k) {
+    const int64_t e = pt_edge[k];
+    double v[6];
+    bal_pt_block<TS>(values, e, v);
+    const double2 nr = *reinterpret_cast<const double2*>(negres + 2 * e);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a[6 + c] -= v[2 * c] * nr.x + v[2 * c + 1] * nr.y;
+    int idx = 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = c; r < 3; ++r) a[idx++] += v[2 * c] * v[2 * r] + v[2 * c + 1] * v[2 * r + 1];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g[retained + 3 * p + c] = a[6 + c];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) raw[6 * p + k] = a[k];
+}
+
+// Floored column scales and the normalized Gram blocks from the raw moments
+// (src/linear_model.rs:211-224, block_factors.rs:87-99): one thread per
+// variable, cameras then points; the blocks are written whole (column-major,
+// lower triangle, zeros above).
+template <class TS>
+__global__ void k_bal_scales_gram(int64_t ncam, int64_t npt, const double* raw_cam, const double* raw_pt,
+                                  double floor, double* scales, double* inv_scales, TS* gram, int* bad) {
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= ncam + npt) return;
+  const bool cam = v < ncam;
+  const int w = cam ? 9 : 3;
+  const double* r = cam ? raw_cam + 45 * v : raw_pt + 6 * (v - ncam);
+  double d[9];
+  int idx = 0;
+  for (int c = 0; c < w; ++c) {  // diagonal entries: the squared column norms
+    const double n = sqrt(r[idx]);
+    if (!isfinite(n)) atomicOr(bad, 1);
+    d[c] = fmax(n, floor);
+    idx += w - c;
+  }
+  const int64_t s0 = cam ? 9 * v : 9 * ncam + 3 * (v - ncam);
+  for (int c = 0; c < w; ++c) {
+    scales[s0 + c] = d[c];
+    inv_scales[s0 + c] = 1.0 / d[c];
+  }
+  TS* gb = gram + (cam ? 81 * v : 81 * ncam + 9 * (v - ncam));
+  idx = 0;
+  for (int c = 0; c < w; ++c)
+    for (int rr = 0; rr < w; ++rr) {
+      if (rr < c) {
+        gb[c * w + rr] = (TS)0;
+      } else {
+        gb[c * w + rr] = (TS)(r[idx] / (d[c] * d[rr]));
+        ++idx;
+      }
+    }
+}
+
 // One block per retained variable: out[cam*cw + c] = sum over its blocks of
 // GRADIENT: sum_i J[i,c] r[row+i]; NORMAL: sum_i J[i,c] (jd - negres)[row+i].
 template <int CW, class TS, int MODE>
@@ -279,10 +432,68 @@ __global__ void __launch_bounds__(REC_T) k_edge_records2(int64_t nedges, const i
   for (int i = threadIdx.x; i < nk * 28; i += REC_T) out[i] = tile[(i / 28) * 29 + (i % 28)];
 }
 
+// Edge records of the device BAL layout (as k_edge_records2, whose record
+// format and arithmetic they share): the emission's 24 values with six 16-byte
+// loads, its camera and point from the edge list, and the inverse column
+// scales k_bal_scales_gram wrote, without the block metadata.
+template <class TS>
+__global__ void __launch_bounds__(REC_T) k_edge_records_bal(int64_t nedges, int64_t retained, const int64_t* pt_edge,
+                                                            const DEdgeMeta* edges, const TS* values,
+                                                            const double* inv_scales, const uint32_t* local_point,
+                                                            TS* rec, TS* cross, int* bad) {
+  __shared__ TS tile[REC_T * 29];
+  const int64_t k0 = (int64_t)blockIdx.x * REC_T, k = k0 + threadIdx.x;
+  const int nk = (int)min((int64_t)REC_T, nedges - k0);
+  if (k < nedges) {
+    const int64_t e = pt_edge[k];
+    const int2 cp = *reinterpret_cast<const int2*>(edges + e);  // (camera, point)
+    const double* icp = inv_scales + 9 * (int64_t)cp.x;
+    const double* ipp = inv_scales + retained + 3 * (int64_t)cp.y;
+    double ic[9], ip[3];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) ic[c] = icp[c];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) ip[q] = ipp[q];
+    double v[18], w[6];
+    bal_cam_block<TS>(values, e, v);
+    bal_pt_block<TS>(values, e, w);
+    double E[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) E[i] = 0;
+#pragma unroll
+    for (int row = 0; row < 2; ++row) {
+      double jc[9], jp[3];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) jc[c] = v[2 * c + row] * ic[c];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) jp[q] = w[2 * q + row] * ip[q];
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) E[q * 9 + c] += jc[c] * jp[q];
+    }
+    bool ok = true;
+    TS* t = tile + threadIdx.x * 29;
+#pragma unroll
+    for (int i = 0; i < 27; ++i) {
+      ok = ok && isfinite(E[i]);
+      t[i] = (TS)E[i];
+    }
+    typename RecWord<TS>::U word = RecWord<TS>::pack((uint32_t)cp.x, local_point[k]);
+    memcpy(&t[27], &word, sizeof(word));
+    if (!ok) atomicOr(bad, 1);
+    if (cross)
+      for (int i = 0; i < 27; ++i) cross[e * 27 + i] = t[i];
+  }
+  __syncthreads();
+  TS* out = rec + k0 * 28;
+  for (int i = threadIdx.x; i < nk * 28; i += REC_T) out[i] = tile[(i / 28) * 29 + (i % 28)];
+}
+
 // Index maps of a BAL linearization (emission k: rows 2k, 2k+1; block 2k =
 // camera ocam[k] (2x9 at 24k), block 2k+1 = point opt[k] (2x3 at 24k+18)),
-// written on the device from the emission arrays and the two stable orders
-// (emissions sorted by camera / by point) the host computed by counting.
+// written on the device from the emission arrays and their two stable orders
+// (by camera and by point, from the device radix orders).
 __global__ void k_bal_structure(int64_t obs, int64_t ncam, const uint32_t* ocam, const uint32_t* opt,
                                 const uint32_t* cam_order, const uint32_t* pt_order, DBlockMeta* blocks,
                                 DEdgeMeta* edges, int64_t* var_blk, int64_t* cam_edge, int64_t* pt_edge,
