@@ -101,42 +101,35 @@ static __global__ void k_jdelta(int64_t nemi, const int64_t* emi_off, const DBlo
 
 // J delta for the device BAL layout (one emission per observation: rows 2k and
 // 2k+1, values [24k, 24k+24) = camera 2x9 then point 2x3, column major) with
-// 16-byte loads of each emission's values; same sums as k_jdelta.
+// 16-byte loads of each emission's values; same sums as k_jdelta. Grid-stride
+// over the emissions with a grid of a few blocks per SM, so the last block
+// sums only a few hundred partials.
 template <class TS>
 static __global__ void k_jdelta_bal(int64_t nobs, int64_t retained, const DEdgeMeta* edges, const TS* values,
                                     const double* delta, double* jd, double* partials, VerifyState* vs) {
-  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double s2 = 0;
-  if (k < nobs) {
-    TS v[24];
-    if (sizeof(TS) == 4) {
-      const float4* q = reinterpret_cast<const float4*>(values + 24 * k);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nobs; k += (int64_t)gridDim.x * blockDim.x) {
+    double v[18], w[6];
+    bal_cam_block<TS>(values, k, v);
+    bal_pt_block<TS>(values, k, w);
+    const int2 cp = *reinterpret_cast<const int2*>(edges + k);  // (camera, point)
+    const double* dc = delta + 9 * (int64_t)cp.x;
+    const double* dp = delta + retained + 3 * (int64_t)cp.y;
+    double y0 = 0, y1 = 0;
 #pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        const float4 a = q[i];
-        v[4 * i] = (TS)a.x; v[4 * i + 1] = (TS)a.y; v[4 * i + 2] = (TS)a.z; v[4 * i + 3] = (TS)a.w;
-      }
-    } else {
-      const double2* q = reinterpret_cast<const double2*>(values + 24 * k);
-#pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        const double2 a = q[i];
-        v[2 * i] = (TS)a.x; v[2 * i + 1] = (TS)a.y;
-      }
+    for (int c = 0; c < 9; ++c) {
+      const double d = dc[c];
+      y0 += v[2 * c] * d;
+      y1 += v[2 * c + 1] * d;
     }
-    const DEdgeMeta m = edges[k];
-    const double* dc = delta + 9 * (int64_t)m.cam;
-    const double* dp = delta + retained + 3 * (int64_t)m.pt;
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      double y = 0;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) y += (double)v[2 * c + i] * dc[c];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) y += (double)v[18 + 2 * c + i] * dp[c];
-      jd[2 * k + i] = y;
-      s2 += y * y;
+    for (int c = 0; c < 3; ++c) {
+      const double d = dp[c];
+      y0 += w[2 * c] * d;
+      y1 += w[2 * c + 1] * d;
     }
+    *reinterpret_cast<double2*>(jd + 2 * k) = make_double2(y0, y1);
+    s2 += y0 * y0 + y1 * y1;
   }
   double w[1] = {s2};
   block_sums<1>(w);
@@ -159,9 +152,9 @@ static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const
                                   const double* scales, const double* delta, double lambda, const double* camjt,
                                   double* partials, VerifyState* vs, const int64_t* bal_pt_off,
                                   const int64_t* bal_pt_edge) {
-  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  if (j < L.dim) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < L.dim;
+       j += (int64_t)gridDim.x * blockDim.x) {
     int64_t v;
     int off;
     L.locate(j, &v, &off);
@@ -185,12 +178,12 @@ static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const
     double s = scales[j], d = delta[j];
     nr += (lambda * (s * d)) * s;
     double gj = g[j];
-    acc[0] = nr * nr;
-    acc[1] = gj * gj;
-    acc[2] = (nr / s) * (nr / s);
-    acc[3] = (gj / s) * (gj / s);
-    acc[4] = gj * d;
-    acc[5] = isfinite(d) ? 0.0 : 1.0;
+    acc[0] += nr * nr;
+    acc[1] += gj * gj;
+    acc[2] += (nr / s) * (nr / s);
+    acc[3] += (gj / s) * (gj / s);
+    acc[4] += gj * d;
+    acc[5] += isfinite(d) ? 0.0 : 1.0;
   }
   block_sums<6>(acc);
   if (threadIdx.x == 0)
@@ -362,7 +355,8 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
   }
   if (rows) FG_CUDA(cudaMemsetAsync(d_jd.get(), 0, rows * sizeof(double), st));
   if (nemissions && source == DEVICE_BAL && pure_pairs && cw == 9 && pw == 3)
-    FG_LAUNCH(k_jdelta_bal<TS>, grid_for(nemissions, NT), NT, 0, st, (int64_t)nemissions, (int64_t)retained,
+    FG_LAUNCH(k_jdelta_bal<TS>, std::min<unsigned>(grid_for(nemissions, NT), 4 * nsm), NT, 0, st,
+              (int64_t)nemissions, (int64_t)retained,
               d_edges.get(), d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
   else if (nemissions)
     FG_LAUNCH(k_jdelta<TS>, grid_for(nemissions, NT), NT, 0, st, (int64_t)nemissions, d_emi_off.get(), d_blocks.get(),
@@ -378,7 +372,8 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
     });
   }
   if (dim)
-    FG_LAUNCH(k_normal_residual<TS>, grid_for(dim, NT), NT, 0, st, L, d_var_off.get(), d_var_blk.get(),
+    FG_LAUNCH(k_normal_residual<TS>, std::min<unsigned>(grid_for(dim, NT), 4 * nsm), NT, 0, st, L,
+              d_var_off.get(), d_var_blk.get(),
               d_blocks.get(), d_values.get(), d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
               lambda, nC ? d_camjt.get() : (const double*)nullptr, d_partials.get() + 4 * 65536, vs,
               bal ? d_pt_edge_off.get() : (const int64_t*)nullptr, bal ? d_pt_edge.get() : (const int64_t*)nullptr);

@@ -217,9 +217,12 @@ __global__ void __launch_bounds__(128) k_bal_cam_pass(int64_t ncam, const int64_
     }
   }
   block_allsums<NA>(acc, sh);
-  for (int k = threadIdx.x; k < NA; k += blockDim.x) {
-    if (k >= NA - 9) out[cam * 9 + (k - (NA - 9))] = acc[k];
-    else raw[cam * 45 + k] = acc[k];
+  if (threadIdx.x == 0) {  // static indices keep acc in registers
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+      if (k >= NA - 9) out[cam * 9 + (k - (NA - 9))] = acc[k];
+      else raw[cam * 45 + k] = acc[k];
+    }
   }
 }
 
@@ -254,38 +257,45 @@ __global__ void k_bal_point_moments(int64_t npt, int64_t retained, const int64_t
 // (src/linear_model.rs:211-224, block_factors.rs:87-99): one thread per
 // variable, cameras then points; the blocks are written whole (column-major,
 // lower triangle, zeros above).
+template <int W, class TS>
+__device__ __forceinline__ void bal_scale_block(const double* r, double floor, double* scales, double* inv_scales,
+                                                TS* gb, int* bad) {
+  double d[W], id[W];
+  int idx = 0;
+#pragma unroll
+  for (int c = 0; c < W; ++c) {  // diagonal entries: the squared column norms
+    const double n = sqrt(r[idx]);
+    if (!isfinite(n)) atomicOr(bad, 1);
+    d[c] = fmax(n, floor);
+    id[c] = 1.0 / d[c];
+    scales[c] = d[c];
+    inv_scales[c] = id[c];
+    idx += W - c;
+  }
+  idx = 0;
+#pragma unroll
+  for (int c = 0; c < W; ++c)
+#pragma unroll
+    for (int rr = 0; rr < W; ++rr) {
+      if (rr < c) {
+        gb[c * W + rr] = (TS)0;
+      } else {
+        gb[c * W + rr] = (TS)(r[idx] * id[c] * id[rr]);
+        ++idx;
+      }
+    }
+}
 template <class TS>
 __global__ void k_bal_scales_gram(int64_t ncam, int64_t npt, const double* raw_cam, const double* raw_pt,
                                   double floor, double* scales, double* inv_scales, TS* gram, int* bad) {
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (v >= ncam + npt) return;
-  const bool cam = v < ncam;
-  const int w = cam ? 9 : 3;
-  const double* r = cam ? raw_cam + 45 * v : raw_pt + 6 * (v - ncam);
-  double d[9];
-  int idx = 0;
-  for (int c = 0; c < w; ++c) {  // diagonal entries: the squared column norms
-    const double n = sqrt(r[idx]);
-    if (!isfinite(n)) atomicOr(bad, 1);
-    d[c] = fmax(n, floor);
-    idx += w - c;
+  if (v < ncam) {
+    bal_scale_block<9, TS>(raw_cam + 45 * v, floor, scales + 9 * v, inv_scales + 9 * v, gram + 81 * v, bad);
+  } else if (v < ncam + npt) {
+    const int64_t p = v - ncam;
+    bal_scale_block<3, TS>(raw_pt + 6 * p, floor, scales + 9 * ncam + 3 * p, inv_scales + 9 * ncam + 3 * p,
+                           gram + 81 * ncam + 9 * p, bad);
   }
-  const int64_t s0 = cam ? 9 * v : 9 * ncam + 3 * (v - ncam);
-  for (int c = 0; c < w; ++c) {
-    scales[s0 + c] = d[c];
-    inv_scales[s0 + c] = 1.0 / d[c];
-  }
-  TS* gb = gram + (cam ? 81 * v : 81 * ncam + 9 * (v - ncam));
-  idx = 0;
-  for (int c = 0; c < w; ++c)
-    for (int rr = 0; rr < w; ++rr) {
-      if (rr < c) {
-        gb[c * w + rr] = (TS)0;
-      } else {
-        gb[c * w + rr] = (TS)(r[idx] / (d[c] * d[rr]));
-        ++idx;
-      }
-    }
 }
 
 // One block per retained variable: out[cam*cw + c] = sum over its blocks of
