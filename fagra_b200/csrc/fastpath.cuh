@@ -783,57 +783,61 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
   }
 }
 
-// Camera part of the coarse matrix (thread per camera) and the camera-major
-// copy of W used by k_coarse_points. B_cam: the normalized Gram block (lower,
-// column major), wd: W row-major (nk x n).
+// Camera part of the coarse matrix and the camera-major copy of W used by
+// k_coarse_tiles. Each block runs four groups of 64 threads, a group per
+// camera: thread (a, c) stages w_a[c], computes (B w_a + lambda w_a)[c], and
+// threads 0..27 accumulate the 28 products w_b . (B + lambda) w_a (b <= a)
+// over the group's cameras; a block adds its sums to out with atomics.
+// B_cam: the normalized Gram block (lower, column major), wd: W row-major
+// (NK x n), NK = 7.
 template <class TS>
-__global__ void k_coarse_cams(int64_t ncam, int nk, const double* wd, const TS* gram, const uint8_t* observed,
-                              double lambda, float* wc, int ws, double* out) {
-  const int64_t cam = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_coarse_cams(int64_t ncam, const double* wd, const TS* gram,
+                                                     const uint8_t* observed, double lambda, float* wc, int ws,
+                                                     double* out) {
+  constexpr int NK = 7, NL = NK * (NK + 1) / 2;
+  __shared__ double w_s[4][NK][9], bw_s[4][NK][9], sum_s[4][NL];
+  const int g = threadIdx.x >> 6, t = threadIdx.x & 63;
   const int64_t n = ncam * 9;
-  double part[36];
-  for (int k = 0; k < 36; ++k) part[k] = 0;
-  if (cam < ncam) {
-    const TS* g = gram + cam * 81;
-    double w[8][9];
-    for (int a = 0; a < nk; ++a)
-      for (int c = 0; c < 9; ++c) {
-        w[a][c] = wd[a * n + cam * 9 + c];
-        wc[cam * ws + c * 8 + a] = (float)w[a][c];
-      }
-    for (int a = 0; a < nk; ++a) {
-      double bw[9];  // B w_a (B symmetric from its lower triangle)
-      for (int r = 0; r < 9; ++r) {
-        double v = 0;
-        if (observed[cam])
-          for (int c = 0; c < 9; ++c) v += (double)(r >= c ? g[c * 9 + r] : g[r * 9 + c]) * w[a][c];
-        bw[r] = v + lambda * w[a][r];
-      }
-      for (int b = 0; b <= a; ++b) {
-        double v = 0;
-        for (int r = 0; r < 9; ++r) v += w[b][r] * bw[r];
-        part[a * (a + 1) / 2 + b] = v;
-      }
+  int pa = 0, pb = 0;  // thread t < NL owns the pair (pa, pb), pb <= pa
+  if (t < NL) {
+    while ((pa + 1) * (pa + 2) / 2 <= t) ++pa;
+    pb = t - pa * (pa + 1) / 2;
+  }
+  double acc = 0;
+  // uniform trip count across the block (the barriers), a group idles past ncam
+  for (int64_t base = (int64_t)blockIdx.x * 4; base < ncam; base += (int64_t)gridDim.x * 4) {
+    const int64_t cam = base + g;
+    const bool live = cam < ncam;
+    const int a = t / 9, c = t % 9;
+    if (live && t < NK * 9) {
+      const double v = wd[a * n + cam * 9 + c];
+      w_s[g][a][c] = v;
+      wc[cam * ws + c * 8 + a] = (float)v;
     }
+    __syncthreads();
+    if (live && t < NK * 9) {  // row c of (B + lambda) w_a
+      const TS* gb = gram + cam * 81;
+      double v = lambda * w_s[g][a][c];
+      if (observed[cam])
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v += (double)(c >= k ? gb[k * 9 + c] : gb[c * 9 + k]) * w_s[g][a][k];
+      bw_s[g][a][c] = v;
+    }
+    __syncthreads();
+    if (live && t < NL) {
+      double v = 0;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) v += w_s[g][pb][r] * bw_s[g][pa][r];
+      acc += v;
+    }
+    __syncthreads();
   }
-  __shared__ double sh[8][36];
-  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-  const int nl = nk * (nk + 1) / 2;
-  for (int k = 0; k < nl; ++k) {
-    double v = part[k];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) sh[wp][k] = v;
-  }
+  if (t < NL) sum_s[g][t] = acc;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const int nw = blockDim.x >> 5;
-    for (int a = 0; a < nk; ++a)
-      for (int b = 0; b <= a; ++b) {
-        double v = 0;
-        for (int q = 0; q < nw; ++q) v += sh[q][a * (a + 1) / 2 + b];
-        atomicAdd(out + a * nk + b, v);
-        if (a != b) atomicAdd(out + b * nk + a, v);
-      }
+  if (threadIdx.x < NL) {
+    const double v = sum_s[0][t] + sum_s[1][t] + sum_s[2][t] + sum_s[3][t];
+    atomicAdd(out + pa * NK + pb, v);
+    if (pa != pb) atomicAdd(out + pb * NK + pa, v);
   }
 }
 
@@ -966,8 +970,8 @@ struct FastPath {
     FG_TRY(d_wc.resize((size_t)s.nC * WS));
     FG_CUDA(cudaMemsetAsync(d_wc.get(), 0, (size_t)s.nC * WS * sizeof(float), s.st));
     FG_CUDA(cudaMemsetAsync(out, 0, (size_t)nk * nk * sizeof(double), s.st));
-    FG_LAUNCH(k_coarse_cams<TS>, grid_for(s.nC, 32), 32, 0, s.st, (int64_t)s.nC, nk, wd, s.d_gram.get(),
-              s.d_observed.get(), lambda, d_wc.get(), WS, out);
+    FG_LAUNCH(k_coarse_cams<TS>, std::max(1u, std::min<unsigned>(grid_for(s.nC, 4), (unsigned)grid)), 256, 0, s.st,
+              (int64_t)s.nC, wd, s.d_gram.get(), s.d_observed.get(), lambda, d_wc.get(), WS, out);
     FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
     const unsigned blocks = (unsigned)std::min<int64_t>((nwt + COARSE_WARPS - 1) / COARSE_WARPS, 8 * (int64_t)grid);
     FG_LAUNCH(k_coarse_tiles<TS>, std::max(blocks, 1u), COARSE_WARPS * 32, 0, s.st, tl, (const TS*)d_erec.get(),

