@@ -726,15 +726,28 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
       typename RecWord<TS>::U word;
       memcpy(&word, erec + (e0 + lane) * 28 + 27, sizeof(word));
       lp = RecWord<TS>::lp(word);
+      // W is the similarity gauge of k_bal_gauge: the rotation directions
+      // (a < 3) move only the angle-axis coordinates 0..2, the translation
+      // and scale directions (a >= 3) only the translation 3..5, and none the
+      // intrinsics, so E^T W needs 6 of the 9 camera columns and 63 products.
       const float4* wv = reinterpret_cast<const float4*>(wc + (int64_t)RecWord<TS>::cam(word) * 72);
 #pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        const float4 lo = __ldg(wv + 2 * c), hi = __ldg(wv + 2 * c + 1);
-        const float x[NK] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z};
+      for (int c = 0; c < 3; ++c) {
+        const float4 lo = __ldg(wv + 2 * c);
+        const float x[3] = {lo.x, lo.y, lo.z};
 #pragma unroll
-        for (int a = 0; a < NK; ++a)
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
           for (int p = 0; p < 3; ++p) u[a][p] += E[p * 9 + c] * x[a];
+      }
+#pragma unroll
+      for (int c = 3; c < 6; ++c) {
+        const float4 lo = __ldg(wv + 2 * c), hi = __ldg(wv + 2 * c + 1);
+        const float x[4] = {lo.w, hi.x, hi.y, hi.z};
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int p = 0; p < 3; ++p) u[3 + a][p] += E[p * 9 + c] * x[a];
       }
     }
 #pragma unroll
