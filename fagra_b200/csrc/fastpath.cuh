@@ -223,10 +223,14 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   const int g = tid / GT, w = (tid % GT) >> 5, gtid = tid % GT;
   const int64_t ny = ncam * 9;
   const size_t vb = FastSmem<TS, TV>::vec_bytes(ncam);
+  // the accumulator ys (every mode but FAST_RECOVER, which scatters nothing)
+  // and, with XS, the staged x
+  constexpr bool NEED_Y = MODE != FAST_RECOVER;
+  constexpr int NVEC = (NEED_Y ? 1 : 0) + (XS ? 1 : 0);
   TV* ys = reinterpret_cast<TV*>(smem);
-  TV* xs = reinterpret_cast<TV*>(smem + vb);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + vb * (XS ? 2 : 1));
-  unsigned char* stage_base = smem + vb * (XS ? 2 : 1) + 128;
+  TV* xs = reinterpret_cast<TV*>(smem + (NEED_Y ? vb : 0));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + vb * NVEC);
+  unsigned char* stage_base = smem + vb * NVEC + 128;
   constexpr size_t sbytes = FastSmem<TS, TV>::stage_bytes();
   unsigned char* gstage = stage_base + (size_t)g * FAST_STAGES * sbytes;
   TV* tpw = reinterpret_cast<TV*>(stage_base + FAST_GROUPS * FAST_STAGES * sbytes) + (size_t)(g * WPS + w) * 96;
@@ -235,7 +239,7 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
 
   const TV bv = pv ? (TV)*beta : (TV)0;
   for (int64_t i = tid; i < ny; i += NTHR) {
-    ys[i] = 0;
+    if (NEED_Y) ys[i] = 0;
     if (XS) xs[i] = pv ? z[i] + bv * pv[i] : z[i];
   }
   if (tid == 0) {
@@ -1129,8 +1133,9 @@ struct FastPath {
   template <class Impl>
   fg_status recover(Impl& s, const double* zred, const double* g, const double* scales, double* step) {
     if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    // x staged in the space the other modes give their accumulator
     size_t sm = FastSmem<TS, double>::bytes((int64_t)s.nC, false);
-    auto kern = k_fast_apply<TS, double, false, FAST_RECOVER>;
+    auto kern = k_fast_apply<TS, double, true, FAST_RECOVER>;
     FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
     FastExtra ex{g + s.retained, scales + s.retained, step + s.retained};
