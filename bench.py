@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
     ap.add_argument("--workload", default="bal1k")
     ap.add_argument("--forms", default="learned,fastc,fast,f64")
+    ap.add_argument("--operator-variant", type=int, default=0,
+                    help="FP32 reduced-operator variant (0: autotune; 1..3 force one, e.g. for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows", "learned"],
@@ -238,6 +240,8 @@ def run_gpu(args, rank: int, world: int, device: int):
         tol = kw.pop("tol")
         backend = fg.Schur(9 * data.num_cameras, 9, 3, device=device, **kw)
         backend.relative_tolerance = tol
+        if args.operator_variant:
+            backend.operator_variant = args.operator_variant
         kw["relative_tolerance"] = tol
         lmo = fg.LmOptions().c()
         oo = opts.c()

@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive_u32(uint32_t* a, int64_
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int64_t chunk = (m + 1023) / 1024, lo = min((int64_t)t * chunk, m), hi = min(lo + chunk, m);
   uint32_t s = 0;
+#pragma unroll 8
   for (int64_t i = lo; i < hi; ++i) s += a[i];
   uint32_t incl = s;  // inclusive scan of the chunk sums across the block
 #pragma unroll
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(1024) k_scan_exclusive_u32(uint32_t* a, int64_
   }
   __syncthreads();
   uint32_t run = warp_sums[w] + incl - s;
+#pragma unroll 8
   for (int64_t i = lo; i < hi; ++i) {
     const uint32_t v = a[i];
     a[i] = run;
