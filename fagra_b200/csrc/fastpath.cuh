@@ -149,15 +149,15 @@ struct FastTiles {
 template <class TS, class TV>
 struct FastSmem {
   static constexpr int WPS = FastShape<TS>::WPS, SE = WPS * 32;
-  __host__ __device__ static constexpr size_t stage_bytes() {
-    return (size_t)SE * 28 * sizeof(TS) + (size_t)SE * 8 * sizeof(TS);
-  }
+  // FP32 operator: the accumulator is 64-bit fixed point held as two 32-bit
+  // words per coordinate (see k_fast_apply)
+  static constexpr bool FIXED = std::is_same<TS, float>::value && std::is_same<TV, float>::value;
+  __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)SE * 28 * sizeof(TS); }
   __host__ __device__ static constexpr size_t vec_bytes(int64_t ncam) {
     return ((size_t)ncam * 9 * sizeof(TV) + 127) & ~(size_t)127;
   }
   __host__ __device__ static constexpr size_t bytes(int64_t ncam, bool stage_x) {
-    return vec_bytes(ncam) * (stage_x ? 2 : 1) + 128 + FAST_GROUPS * FAST_STAGES * stage_bytes() +
-           (size_t)FAST_GROUPS * WPS * 96 * sizeof(TV);
+    return vec_bytes(ncam) * ((FIXED ? 2 : 1) + (stage_x ? 1 : 0)) + 128 + FAST_GROUPS * FAST_STAGES * stage_bytes();
   }
 };
 
@@ -198,6 +198,20 @@ __device__ __forceinline__ void load_record(const double* rec, TV (&E)[27], uint
   lp = RecWord<double>::lp(w);
 }
 
+// The packed lower C^-1 of a point record (the first 6 of its 8 words).
+template <class TS, class TV>
+__device__ __forceinline__ void load_point(const TS* r, TV& c0, TV& c1, TV& c2, TV& c3, TV& c4, TV& c5) {
+  if (sizeof(TS) == 4) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(r));
+    const float2 b = __ldg(reinterpret_cast<const float2*>(r) + 2);
+    c0 = (TV)a.x; c1 = (TV)a.y; c2 = (TV)a.z; c3 = (TV)a.w; c4 = (TV)b.x; c5 = (TV)b.y;
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(r);
+    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    c0 = (TV)a.x; c1 = (TV)a.y; c2 = (TV)b.x; c3 = (TV)b.y; c4 = (TV)c.x; c5 = (TV)c.y;
+  }
+}
+
 // Modes of the edge-record pass (all read every record once):
 //   FAST_APPLY:   partials <- -E C^-1 E^T x                 (x = z + beta p)
 //   FAST_RHS:     partials <- -E w_p, w_p read per point     (src/schur.rs:230-242)
@@ -224,23 +238,43 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   const int64_t ny = ncam * 9;
   const size_t vb = FastSmem<TS, TV>::vec_bytes(ncam);
   // the accumulator ys (every mode but FAST_RECOVER, which scatters nothing)
-  // and, with XS, the staged x
+  // and, with XS, the staged x. FP32 operator (FIXED): the accumulator is 64-bit
+  // fixed point in units of 2^-k (k from the largest |x|), held as low and high
+  // 32-bit words; a contribution adds its low word with a 32-bit atomic whose
+  // returned old value gives the carry, then high word + carry (two integer
+  // shared-memory atomics cost less than one FP32 atomic here, and the sums are
+  // exact, so the result does not depend on the order of the atomics).
+  constexpr bool FIXED = FastSmem<TS, TV>::FIXED && MODE == FAST_APPLY;
   constexpr bool NEED_Y = MODE != FAST_RECOVER;
-  constexpr int NVEC = (NEED_Y ? 1 : 0) + (XS ? 1 : 0);
+  constexpr int NVEC = (NEED_Y ? (FastSmem<TS, TV>::FIXED ? 2 : 1) : 0) + (XS ? 1 : 0);
   TV* ys = reinterpret_cast<TV*>(smem);
-  TV* xs = reinterpret_cast<TV*>(smem + (NEED_Y ? vb : 0));
+  uint32_t* ylo = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* yhi = reinterpret_cast<uint32_t*>(smem + vb);
+  TV* xs = reinterpret_cast<TV*>(smem + (NEED_Y ? vb * (FastSmem<TS, TV>::FIXED ? 2 : 1) : 0));
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + vb * NVEC);
   unsigned char* stage_base = smem + vb * NVEC + 128;
   constexpr size_t sbytes = FastSmem<TS, TV>::stage_bytes();
   unsigned char* gstage = stage_base + (size_t)g * FAST_STAGES * sbytes;
-  TV* tpw = reinterpret_cast<TV*>(stage_base + FAST_GROUPS * FAST_STAGES * sbytes) + (size_t)(g * WPS + w) * 96;
   uint64_t* gbar = bars + FAST_STAGES * g;
   volatile int* fail = reinterpret_cast<volatile int*>(bars + FAST_GROUPS * FAST_STAGES);  // one flag per group
 
   const TV bv = pv ? (TV)*beta : (TV)0;
+  float xmax = 0.f;
   for (int64_t i = tid; i < ny; i += NTHR) {
     if (NEED_Y) ys[i] = 0;
-    if (XS) xs[i] = pv ? z[i] + bv * pv[i] : z[i];
+    if (FIXED) yhi[i] = 0;
+    const TV xi = pv ? z[i] + bv * pv[i] : z[i];
+    if (XS) xs[i] = xi;
+    if (FIXED) xmax = fmaxf(xmax, fabsf((float)xi));  // NaN propagates through the nonfinite check below
+    if (FIXED && !isfinite((float)xi)) xmax = INFINITY;
+  }
+  // FIXED: every block stages the same x, so every block derives the same unit
+  __shared__ float wmax[32];
+  __shared__ double fx_mul_s, fx_unit_s;
+  if (FIXED) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) xmax = fmaxf(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+    if (lane == 0) wmax[tid >> 5] = xmax;
   }
   if (tid == 0) {
     for (int i = 0; i < FAST_GROUPS * FAST_STAGES; ++i) mbar_init(&bars[i], 1);
@@ -248,15 +282,26 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
     mbar_fence_init();
   }
   __syncthreads();
+  if (FIXED && tid == 0) {
+    float m = 0.f;
+    for (int w2 = 0; w2 < NTHR / 32; ++w2) m = fmaxf(m, wmax[w2]);
+    // unit 2^-k with |x| < 2^(40-k): contributions stay below 2^48 units and
+    // a block's partial sums (bounded by a few hundred |x|max) below 2^62
+    int e = 0;
+    if (m > 0.f && isfinite(m)) frexpf(m, &e);
+    fx_mul_s = isfinite(m) ? ldexp(1.0, 40 - e) : 0.0;
+    fx_unit_s = isfinite(m) ? ldexp(1.0, e - 40) : (double)NAN;
+  }
+  if (FIXED) __syncthreads();
+  const double fx_mul = FIXED ? fx_mul_s : 0.0;
 
   auto issue = [&](int64_t sidx, int b) {
     int64_t wt0 = sidx * WPS, wt1 = min(wt0 + WPS, tiles.nwt);
-    int64_t e0 = tiles.wt_e0[wt0], e1 = tiles.wt_e0[wt1], p0 = tiles.wt_p0[wt0], p1 = tiles.wt_p0[wt1];
-    unsigned eb = (unsigned)((e1 - e0) * 28 * sizeof(TS)), pb = (unsigned)((p1 - p0) * 8 * sizeof(TS));
+    int64_t e0 = tiles.wt_e0[wt0], e1 = tiles.wt_e0[wt1];
+    unsigned eb = (unsigned)((e1 - e0) * 28 * sizeof(TS));
     unsigned char* dst = gstage + b * sbytes;
-    mbar_expect_tx(&gbar[b], eb + pb);
+    mbar_expect_tx(&gbar[b], eb);
     if (eb) tma_load_1d(dst, erec + e0 * 28, eb, &gbar[b]);
-    if (pb) tma_load_1d(dst + (size_t)SE * 28 * sizeof(TS), prec + p0 * 8, pb, &gbar[b]);
   };
 
   const int64_t first = (int64_t)blockIdx.x * FAST_GROUPS + g, stride = (int64_t)gridDim.x * FAST_GROUPS;
@@ -273,25 +318,29 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
     // The warp tile's bounds come from global memory: load them before the
     // wait so their latency overlaps the stage's arrival.
     const int64_t wt = sidx * WPS + w;
-    int64_t e_lo = 0, p_lo = 0, gp0 = 0;  // gp0: global index of the tile's first point
+    int64_t e_lo = 0, gp0 = 0;  // gp0: global index of the tile's first point
     int cnt = 0;
     if (wt < tiles.nwt) {
-      const int64_t se0 = tiles.wt_e0[sidx * WPS], sp0 = tiles.wt_p0[sidx * WPS];
+      const int64_t se0 = tiles.wt_e0[sidx * WPS];
       const int64_t ew = tiles.wt_e0[wt], ew1 = tiles.wt_e0[wt + 1];
       gp0 = tiles.wt_p0[wt];
       e_lo = ew - se0;
-      p_lo = gp0 - sp0;
       cnt = (int)(ew1 - ew);
     }
     const bool ok = mbar_wait_bounded(&gbar[b], parity, 1u << 22);
     if (!ok) fail[g] = 1;
     if (ok && wt < tiles.nwt) {
       const TS* er = reinterpret_cast<const TS*>(gstage + b * sbytes);
-      const TS* pr = er + (size_t)SE * 28;
       TV E[27];
       uint32_t cam = 0, lp = 0xFFFFu;
       TV u0 = 0, u1 = 0, u2 = 0;
-      if (lane < cnt) load_record<TV>(er + (size_t)(e_lo + lane) * 28, E, cam, lp);
+      TV c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;  // the point's C^-1 (packed lower)
+      if (lane < cnt) {
+        load_record<TV>(er + (size_t)(e_lo + lane) * 28, E, cam, lp);
+        // every lane fetches its point's C^-1 now (L1 serves the point's other
+        // lanes), so its latency overlaps the x gather and the scan
+        if (MODE != FAST_RHS) load_point<TS, TV>(prec + (gp0 + lp) * 8, c0, c1, c2, c3, c4, c5);
+      }
       if (MODE != FAST_RHS && lane < cnt) {
         TV xc[9];
         if (XS) {
@@ -325,16 +374,15 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
       }
       uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
       bool last = lane < cnt && (lane == cnt - 1 || lpn != lp);
+      TV t0 = 0, t1 = 0, t2 = 0;
       if (MODE == FAST_RHS) {
         if (last) {
           const double* w3 = ex.wp + 3 * (gp0 + lp);
-          tpw[lp * 3] = (TV)w3[0];
-          tpw[lp * 3 + 1] = (TV)w3[1];
-          tpw[lp * 3 + 2] = (TV)w3[2];
+          t0 = (TV)w3[0];
+          t1 = (TV)w3[1];
+          t2 = (TV)w3[2];
         }
       } else if (last) {
-        const TS* r = pr + (size_t)(p_lo + lp) * 8;
-        TV c0 = (TV)r[0], c1 = (TV)r[1], c2 = (TV)r[2], c3 = (TV)r[3], c4 = (TV)r[4], c5 = (TV)r[5];
         if (MODE == FAST_RECOVER) {
           const int64_t q = 3 * (gp0 + lp);
           TV a0 = (TV)(-ex.wp[q] / ex.scales[q]) - u0, a1 = (TV)(-ex.wp[q + 1] / ex.scales[q + 1]) - u1;
@@ -343,19 +391,37 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
           ex.step[q + 1] = (double)(c1 * a0 + c3 * a1 + c4 * a2) / ex.scales[q + 1];
           ex.step[q + 2] = (double)(c2 * a0 + c4 * a1 + c5 * a2) / ex.scales[q + 2];
         } else {
-          tpw[lp * 3] = c0 * u0 + c1 * u1 + c2 * u2;
-          tpw[lp * 3 + 1] = c1 * u0 + c3 * u1 + c4 * u2;
-          tpw[lp * 3 + 2] = c2 * u0 + c4 * u1 + c5 * u2;
+          t0 = c0 * u0 + c1 * u1 + c2 * u2;
+          t1 = c1 * u0 + c3 * u1 + c4 * u2;
+          t2 = c2 * u0 + c4 * u1 + c5 * u2;
         }
       }
-      __syncwarp();
-      if (MODE != FAST_RECOVER && lane < cnt) {
-        TV t0 = tpw[lp * 3], t1 = tpw[lp * 3 + 1], t2 = tpw[lp * 3 + 2];
-        TV* y = ys + (int64_t)cam * 9;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
+      if (MODE != FAST_RECOVER) {
+        // each lane takes its point's t from the point's last lane: the first
+        // flagged lane at or after this one
+        const unsigned ends = __ballot_sync(0xffffffffu, last) & ~((1u << lane) - 1u);
+        const int src = ends ? __ffs(ends) - 1 : lane;
+        t0 = __shfl_sync(0xffffffffu, t0, src);
+        t1 = __shfl_sync(0xffffffffu, t1, src);
+        t2 = __shfl_sync(0xffffffffu, t2, src);
       }
-      __syncwarp();
+      if (MODE != FAST_RECOVER && lane < cnt) {
+        if (FIXED) {
+          const int64_t y0 = (int64_t)cam * 9;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) {
+            const float v = -(float)(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2);
+            const long long q = __double2ll_rn((double)v * fx_mul);
+            const uint32_t lo = (uint32_t)q;
+            const uint32_t old = atomicAdd(&ylo[y0 + c], lo);
+            atomicAdd(&yhi[y0 + c], (uint32_t)(q >> 32) + ((uint32_t)(old + lo) < old ? 1u : 0u));
+          }
+        } else {
+          TV* y = ys + (int64_t)cam * 9;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) atomicAdd(&y[c], -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2));
+        }
+      }
     }
     group_sync(1 + g, GT);  // every warp of the group is done with stage b
     if (fail[g]) {
@@ -371,7 +437,15 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   __syncthreads();
   if (MODE == FAST_RECOVER) return;
   TV* out = partials + (int64_t)blockIdx.x * ny;
-  for (int64_t i = tid; i < ny; i += NTHR) out[i] = ys[i];
+  if (FIXED) {
+    const double unit = fx_unit_s;
+    for (int64_t i = tid; i < ny; i += NTHR) {
+      const long long q = (long long)(((unsigned long long)yhi[i] << 32) | (unsigned long long)ylo[i]);
+      out[i] = (TV)((double)q * unit);
+    }
+  } else {
+    for (int64_t i = tid; i < ny; i += NTHR) out[i] = ys[i];
+  }
 }
 
 // Direct variant of the FAST_APPLY pass: no shared-memory staging of records.
