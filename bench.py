@@ -34,7 +34,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 REL = 1e-6
-MEASURED_TRAFFIC = {"bal1k": {"f32": 134.59e6}}
+MEASURED_TRAFFIC = {"bal1k": {"f32": 133.83e6}}
 
 
 def parse():
@@ -589,7 +589,7 @@ def main():
         op = results[head].get("operator", {})
         achieved = op["bytes"] / op["seconds"] / 1e9 if op.get("seconds") else None
         # DRAM bytes (read + write) of one k_fast_apply launch from an ncu --set full
-        # capture on bal1k (FP32 records, TMA-staged variant): 130.29 MB + 4.30 MB
+        # capture on bal1k (FP32 records, TMA-staged variant): 130.29 MB + 3.53 MB
         traffic = MEASURED_TRAFFIC.get(args.workload, {}).get(results[head]["precision"])
         line = dict(
             metric=f"BA time to 1e-6 relative cost ({args.workload})", value=vals[head], unit="s", n_gpus=world,
