@@ -187,7 +187,7 @@ class SchurImpl final : public Backend {
       return FG_INVALID_OPTIONS;
     }
     FG_TRY(select_device(dev));
-    drop_graphs();
+    // the PCG graphs stay: launch_graph re-captures them if a buffer moves
     if (dimension != dim) structure_valid = false;
     dim = dimension;
     nC = retained / cw;
@@ -923,11 +923,28 @@ class SchurImpl final : public Backend {
   static constexpr int GRAPH_ITERS = 8;
   cudaGraphExec_t g_exec[2] = {nullptr, nullptr};
   uint64_t g_nodes[2] = {0, 0};
+  std::vector<uintptr_t> g_key[2];  // what each instantiated graph baked in
   void drop_graphs() {
     for (int k = 0; k < 2; ++k) {
       if (g_exec[k]) cudaGraphExecDestroy(g_exec[k]);
       g_exec[k] = nullptr;
+      g_key[k].clear();
     }
+  }
+  // Every pointer, size and kernel choice a captured iteration bakes in; a
+  // graph whose key no longer matches (a buffer reallocated, another operator
+  // variant or coarse state) is re-captured, so a new solve or linearization
+  // on the same structure reuses the instantiation.
+  std::vector<uintptr_t> graph_key(bool mixed, const double* xd, const PcgState* ps) const {
+    return {(uintptr_t)mixed, (uintptr_t)xd, (uintptr_t)ps, (uintptr_t)d_z.get(), (uintptr_t)d_pp.get(),
+            (uintptr_t)d_q.get(), (uintptr_t)d_t.get(), (uintptr_t)d_r.get(), (uintptr_t)d_x.get(),
+            (uintptr_t)d_partials.get(), (uintptr_t)d_minv.get(), (uintptr_t)d_gram.get(),
+            (uintptr_t)d_observed.get(), (uintptr_t)d_tmpd.get(), (uintptr_t)d_qd.get(), (uintptr_t)d_rhs.get(),
+            (uintptr_t)d_Wt.get(), (uintptr_t)d_G.get(), (uintptr_t)fast.d_ebeg.get(), (uintptr_t)fast.d_pbeg.get(),
+            (uintptr_t)fast.d_erec.get(), (uintptr_t)fast.d_prec.get(), (uintptr_t)fast.d_parts_f.get(),
+            (uintptr_t)fast.d_parts_d.get(), (uintptr_t)fast.d_error.get(), (uintptr_t)fast.variant,
+            (uintptr_t)fast.nwt, (uintptr_t)fast.nstages, (uintptr_t)fast.grid, (uintptr_t)coarse_on,
+            (uintptr_t)nk, (uintptr_t)nC, (uintptr_t)nP, (uintptr_t)retained, (uintptr_t)dim};
   }
   fg_status iteration_body(bool mixed, double* xd, PcgState* ps, double lambda, int k) {
     double* tsum = d_partials.get() + 4 * 65536;
@@ -943,7 +960,13 @@ class SchurImpl final : public Backend {
   }
   fg_status launch_graph(bool mixed, double* xd, PcgState* ps, double lambda) {
     const int g = mixed ? 1 : 0;
+    std::vector<uintptr_t> key = graph_key(mixed, xd, ps);
+    if (g_exec[g] && key != g_key[g]) {
+      cudaGraphExecDestroy(g_exec[g]);
+      g_exec[g] = nullptr;
+    }
     if (!g_exec[g]) {
+      g_key[g] = key;
       cudaGraph_t graph = nullptr;
       uint64_t before = g_launches.load();
       FG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
