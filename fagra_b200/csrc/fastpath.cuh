@@ -149,15 +149,24 @@ struct FastTiles {
 template <class TS, class TV>
 struct FastSmem {
   static constexpr int WPS = FastShape<TS>::WPS, SE = WPS * 32;
-  // FP32 operator: the accumulator is 64-bit fixed point held as two 32-bit
-  // words per coordinate (see k_fast_apply)
-  static constexpr bool FIXED = std::is_same<TS, float>::value && std::is_same<TV, float>::value;
+  // FP32 records: the operator's accumulator is 64-bit fixed point held as two
+  // 32-bit words per coordinate (see k_fast_apply)
+  static constexpr bool FIXED = std::is_same<TS, float>::value;
+  // fractional bits below the largest |x| (FP32 vectors 40, FP64 vectors 44)
+  static constexpr int FIXED_BITS = std::is_same<TV, float>::value ? 40 : 44;
   __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)SE * 28 * sizeof(TS); }
   __host__ __device__ static constexpr size_t vec_bytes(int64_t ncam) {
     return ((size_t)ncam * 9 * sizeof(TV) + 127) & ~(size_t)127;
   }
+  __host__ __device__ static constexpr size_t word_bytes(int64_t ncam) {
+    return ((size_t)ncam * 9 * sizeof(uint32_t) + 127) & ~(size_t)127;
+  }
+  // the accumulator region: two 32-bit words per coordinate (FIXED) or one TV
+  __host__ __device__ static constexpr size_t acc_bytes(int64_t ncam) {
+    return FIXED ? (2 * word_bytes(ncam) > vec_bytes(ncam) ? 2 * word_bytes(ncam) : vec_bytes(ncam)) : vec_bytes(ncam);
+  }
   __host__ __device__ static constexpr size_t bytes(int64_t ncam, bool stage_x) {
-    return vec_bytes(ncam) * ((FIXED ? 2 : 1) + (stage_x ? 1 : 0)) + 128 + FAST_GROUPS * FAST_STAGES * stage_bytes();
+    return acc_bytes(ncam) + (stage_x ? vec_bytes(ncam) : 0) + 128 + FAST_GROUPS * FAST_STAGES * stage_bytes();
   }
 };
 
@@ -246,34 +255,40 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   // exact, so the result does not depend on the order of the atomics).
   constexpr bool FIXED = FastSmem<TS, TV>::FIXED && MODE == FAST_APPLY;
   constexpr bool NEED_Y = MODE != FAST_RECOVER;
-  constexpr int NVEC = (NEED_Y ? (FastSmem<TS, TV>::FIXED ? 2 : 1) : 0) + (XS ? 1 : 0);
+  const size_t acc = FastSmem<TS, TV>::acc_bytes(ncam);
+  const size_t x0 = NEED_Y ? acc : 0, bar0 = x0 + (XS ? vb : 0);
   TV* ys = reinterpret_cast<TV*>(smem);
   uint32_t* ylo = reinterpret_cast<uint32_t*>(smem);
-  uint32_t* yhi = reinterpret_cast<uint32_t*>(smem + vb);
-  TV* xs = reinterpret_cast<TV*>(smem + (NEED_Y ? vb * (FastSmem<TS, TV>::FIXED ? 2 : 1) : 0));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + vb * NVEC);
-  unsigned char* stage_base = smem + vb * NVEC + 128;
+  uint32_t* yhi = reinterpret_cast<uint32_t*>(smem + FastSmem<TS, TV>::word_bytes(ncam));
+  TV* xs = reinterpret_cast<TV*>(smem + x0);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + bar0);
+  unsigned char* stage_base = smem + bar0 + 128;
   constexpr size_t sbytes = FastSmem<TS, TV>::stage_bytes();
   unsigned char* gstage = stage_base + (size_t)g * FAST_STAGES * sbytes;
   uint64_t* gbar = bars + FAST_STAGES * g;
   volatile int* fail = reinterpret_cast<volatile int*>(bars + FAST_GROUPS * FAST_STAGES);  // one flag per group
 
   const TV bv = pv ? (TV)*beta : (TV)0;
-  float xmax = 0.f;
+  double xmax = 0.0;
   for (int64_t i = tid; i < ny; i += NTHR) {
-    if (NEED_Y) ys[i] = 0;
-    if (FIXED) yhi[i] = 0;
+    if (NEED_Y) {
+      if (FIXED) {
+        ylo[i] = 0;
+        yhi[i] = 0;
+      } else {
+        ys[i] = 0;
+      }
+    }
     const TV xi = pv ? z[i] + bv * pv[i] : z[i];
     if (XS) xs[i] = xi;
-    if (FIXED) xmax = fmaxf(xmax, fabsf((float)xi));  // NaN propagates through the nonfinite check below
-    if (FIXED && !isfinite((float)xi)) xmax = INFINITY;
+    if (FIXED) xmax = isfinite((double)xi) ? fmax(xmax, fabs((double)xi)) : (double)INFINITY;
   }
-  // FIXED: every block stages the same x, so every block derives the same unit
-  __shared__ float wmax[32];
+  // FIXED: every block sees the same x, so every block derives the same unit
+  __shared__ double wmax[32];
   __shared__ double fx_mul_s, fx_unit_s;
   if (FIXED) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) xmax = fmaxf(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+    for (int o = 16; o > 0; o >>= 1) xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
     if (lane == 0) wmax[tid >> 5] = xmax;
   }
   if (tid == 0) {
@@ -283,14 +298,16 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   }
   __syncthreads();
   if (FIXED && tid == 0) {
-    float m = 0.f;
-    for (int w2 = 0; w2 < NTHR / 32; ++w2) m = fmaxf(m, wmax[w2]);
-    // unit 2^-k with |x| < 2^(40-k): contributions stay below 2^48 units and
-    // a block's partial sums (bounded by a few hundred |x|max) below 2^62
+    double m = 0.0;
+    for (int w2 = 0; w2 < NTHR / 32; ++w2) m = fmax(m, wmax[w2]);
+    // unit 2^-k with |x| < 2^(B-k), B = 40 (FP32 vectors) or 44: a contribution
+    // (at most a few hundred |x|max) stays below 2^(B+9) units and a block's
+    // partial sums far below 2^63
+    constexpr int B = FastSmem<TS, TV>::FIXED_BITS;
     int e = 0;
-    if (m > 0.f && isfinite(m)) frexpf(m, &e);
-    fx_mul_s = isfinite(m) ? ldexp(1.0, 40 - e) : 0.0;
-    fx_unit_s = isfinite(m) ? ldexp(1.0, e - 40) : (double)NAN;
+    if (m > 0.0 && isfinite(m)) frexp(m, &e);
+    fx_mul_s = isfinite(m) ? ldexp(1.0, B - e) : 0.0;
+    fx_unit_s = isfinite(m) ? ldexp(1.0, e - B) : (double)NAN;
   }
   if (FIXED) __syncthreads();
   const double fx_mul = FIXED ? fx_mul_s : 0.0;
@@ -410,7 +427,7 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
           const int64_t y0 = (int64_t)cam * 9;
 #pragma unroll
           for (int c = 0; c < 9; ++c) {
-            const float v = -(float)(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2);
+            const TV v = -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2);
             const long long q = __double2ll_rn((double)v * fx_mul);
             const uint32_t lo = (uint32_t)q;
             const uint32_t old = atomicAdd(&ylo[y0 + c], lo);
