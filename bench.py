@@ -40,7 +40,7 @@ MEASURED_TRAFFIC = {"bal1k": {"f32": 133.83e6}}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
     ap.add_argument("--workload", default="bal1k")
