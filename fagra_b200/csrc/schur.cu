@@ -429,7 +429,7 @@ class SchurImpl final : public Backend {
       // the gradient and the raw Gram blocks (for the column scales) in one pass
       FG_TRY(d_raw.resize(45 * nC + 6 * nP + 1));
       if (nC)
-        FG_LAUNCH((k_bal_cam_pass<TS, BAL_MOMENTS>), (unsigned)nC, 128, 0, st, (int64_t)nC, d_cam_edge_off.get(),
+        FG_LAUNCH((k_bal_cam_pass<TS, BAL_MOMENTS>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC, d_cam_edge_off.get(),
                   d_values.get(), d_negres.get(), (const double*)nullptr, d_g.get(), d_raw.get());
       if (nP)
         FG_LAUNCH(k_bal_point_moments<TS>, grid_for(nP, 128), 128, 0, st, (int64_t)nP, (int64_t)retained,

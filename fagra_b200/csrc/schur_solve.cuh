@@ -153,8 +153,42 @@ static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const
                                   double* partials, VerifyState* vs, const int64_t* bal_pt_off,
                                   const int64_t* bal_pt_edge) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < L.dim;
-       j += (int64_t)gridDim.x * blockDim.x) {
+  auto add = [&](double nr, int64_t j) {  // the per-coordinate terms of the diagnostics
+    const double s = scales[j], d = delta[j];
+    nr += (lambda * (s * d)) * s;
+    const double gj = g[j];
+    acc[0] += nr * nr;
+    acc[1] += gj * gj;
+    acc[2] += (nr / s) * (nr / s);
+    acc[3] += (gj / s) * (gj / s);
+    acc[4] += gj * d;
+    acc[5] += isfinite(d) ? 0.0 : 1.0;
+  };
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (bal_pt_off && camjt) {
+    // device BAL layout: camera coordinates from camjt, then one thread per
+    // point walks its emissions once for its 3 coordinates
+    for (int64_t j = t0; j < L.retained; j += stride) add(camjt[j], j);
+    for (int64_t pt = t0; pt < L.nP; pt += stride) {
+      double n0 = 0, n1 = 0, n2 = 0;
+      for (int64_t k = bal_pt_off[pt]; k < bal_pt_off[pt + 1]; ++k) {
+        const int64_t e = bal_pt_edge[k];
+        double w[6];
+        bal_pt_block<TS>(values, e, w);
+        const double2 jj = *reinterpret_cast<const double2*>(jd + 2 * e);
+        const double2 nn = *reinterpret_cast<const double2*>(negres + 2 * e);
+        const double r0 = jj.x - nn.x, r1 = jj.y - nn.y;
+        n0 += w[0] * r0 + w[1] * r1;
+        n1 += w[2] * r0 + w[3] * r1;
+        n2 += w[4] * r0 + w[5] * r1;
+      }
+      const int64_t j = L.retained + 3 * pt;
+      add(n0, j);
+      add(n1, j + 1);
+      add(n2, j + 2);
+    }
+  }
+  for (int64_t j = t0; !(bal_pt_off && camjt) && j < L.dim; j += stride) {
     int64_t v;
     int off;
     L.locate(j, &v, &off);
@@ -175,15 +209,7 @@ static __global__ void k_normal_residual(Layout L, const int64_t* var_off, const
       for (int i = 0; i < b.rows; ++i) s += (double)col[i] * (jd[b.row + i] - negres[b.row + i]);
       nr += s;
     }
-    double s = scales[j], d = delta[j];
-    nr += (lambda * (s * d)) * s;
-    double gj = g[j];
-    acc[0] += nr * nr;
-    acc[1] += gj * gj;
-    acc[2] += (nr / s) * (nr / s);
-    acc[3] += (gj / s) * (gj / s);
-    acc[4] += gj * d;
-    acc[5] += isfinite(d) ? 0.0 : 1.0;
+    add(nr, j);
   }
   block_sums<6>(acc);
   if (threadIdx.x == 0)
@@ -363,7 +389,7 @@ fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
               d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
   const bool bal = bal_layout();
   if (nC && bal) {
-    FG_LAUNCH((k_bal_cam_pass<TS, BAL_NORMAL>), (unsigned)nC, 128, 0, st, (int64_t)nC, d_cam_edge_off.get(),
+    FG_LAUNCH((k_bal_cam_pass<TS, BAL_NORMAL>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC, d_cam_edge_off.get(),
               d_values.get(), d_negres.get(), d_jd.get(), d_camjt.get(), (double*)nullptr);
   } else if (nC) {
     FG_DISPATCH_WIDTHS(cw, pw, {

@@ -181,14 +181,40 @@ __device__ __forceinline__ void bal_pt_block(const TS* values, int64_t k, double
   }
 }
 
-// One block per camera over its contiguous emissions. MOMENTS: the gradient
-// J^T r (g) and the raw Gram J^T J (raw: 45 entries, columns c <= r in
-// column-major lower order) in one pass; NORMAL: J^T (jd - negres) (out).
+// A camera block's 18 values in the storage type (16-byte loads).
+template <class TS>
+__device__ __forceinline__ void bal_cam_raw(const TS* values, int64_t k, TS (&v)[18]) {
+  if (sizeof(TS) == 4) {
+    const float4* q = reinterpret_cast<const float4*>(values + 24 * k);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float4 a = q[i];
+      v[4 * i] = (TS)a.x; v[4 * i + 1] = (TS)a.y; v[4 * i + 2] = (TS)a.z; v[4 * i + 3] = (TS)a.w;
+    }
+    const float2 b = *reinterpret_cast<const float2*>(values + 24 * k + 16);
+    v[16] = (TS)b.x;
+    v[17] = (TS)b.y;
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(values + 24 * k);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const double2 a = q[i];
+      v[2 * i] = (TS)a.x; v[2 * i + 1] = (TS)a.y;
+    }
+  }
+}
+
+// One block of 64 threads per camera over its contiguous emissions, each
+// thread loading its next emission while it accumulates the current one.
+// MOMENTS: the gradient J^T r (g) and the raw Gram J^T J (raw: 45 entries,
+// columns c <= r in column-major lower order) in one pass; NORMAL:
+// J^T (jd - negres) (out).
 constexpr int BAL_MOMENTS = 0, BAL_NORMAL = 1;
+constexpr int BAL_CAM_THREADS = 64;
 template <class TS, int MODE>
-__global__ void __launch_bounds__(128) k_bal_cam_pass(int64_t ncam, const int64_t* cam_off, const TS* values,
-                                                      const double* negres, const double* jd, double* out,
-                                                      double* raw) {
+__global__ void __launch_bounds__(BAL_CAM_THREADS) k_bal_cam_pass(int64_t ncam, const int64_t* cam_off,
+                                                                  const TS* values, const double* negres,
+                                                                  const double* jd, double* out, double* raw) {
   constexpr int NA = MODE == BAL_MOMENTS ? 54 : 9;
   __shared__ double sh[32 * NA];
   const int64_t cam = blockIdx.x;
@@ -196,32 +222,53 @@ __global__ void __launch_bounds__(128) k_bal_cam_pass(int64_t ncam, const int64_
   double acc[NA];
 #pragma unroll
   for (int k = 0; k < NA; ++k) acc[k] = 0;
-  for (int64_t k = cam_off[cam] + threadIdx.x; k < cam_off[cam + 1]; k += blockDim.x) {
-    double v[18];
-    bal_cam_block<TS>(values, k, v);
-    const double2 nr = *reinterpret_cast<const double2*>(negres + 2 * k);
+  const int64_t k1 = cam_off[cam + 1];
+  int64_t k = cam_off[cam] + threadIdx.x;
+  TS v[18];
+  double2 nr = make_double2(0, 0), jj = make_double2(0, 0);
+  if (k < k1) {
+    bal_cam_raw<TS>(values, k, v);
+    nr = *reinterpret_cast<const double2*>(negres + 2 * k);
+    if (MODE == BAL_NORMAL) jj = *reinterpret_cast<const double2*>(jd + 2 * k);
+  }
+  while (k < k1) {
+    const int64_t kn = k + BAL_CAM_THREADS;
+    TS vn[18];
+    double2 nrn = make_double2(0, 0), jjn = make_double2(0, 0);
+    if (kn < k1) {  // the next emission's loads are in flight during this one's arithmetic
+      bal_cam_raw<TS>(values, kn, vn);
+      nrn = *reinterpret_cast<const double2*>(negres + 2 * kn);
+      if (MODE == BAL_NORMAL) jjn = *reinterpret_cast<const double2*>(jd + 2 * kn);
+    }
     double w0 = -nr.x, w1 = -nr.y;
     if (MODE == BAL_NORMAL) {
-      const double2 j = *reinterpret_cast<const double2*>(jd + 2 * k);
-      w0 = j.x - nr.x;
-      w1 = j.y - nr.y;
+      w0 = jj.x - nr.x;
+      w1 = jj.y - nr.y;
     }
 #pragma unroll
-    for (int c = 0; c < 9; ++c) acc[NA - 9 + c] += v[2 * c] * w0 + v[2 * c + 1] * w1;
+    for (int c = 0; c < 9; ++c) acc[NA - 9 + c] += (double)v[2 * c] * w0 + (double)v[2 * c + 1] * w1;
     if (MODE == BAL_MOMENTS) {
       int idx = 0;
 #pragma unroll
       for (int c = 0; c < 9; ++c)
 #pragma unroll
-        for (int r = c; r < 9; ++r) acc[idx++] += v[2 * c] * v[2 * r] + v[2 * c + 1] * v[2 * r + 1];
+        for (int r = c; r < 9; ++r)
+          acc[idx++] += (double)v[2 * c] * (double)v[2 * r] + (double)v[2 * c + 1] * (double)v[2 * r + 1];
     }
+    if (kn < k1) {
+#pragma unroll
+      for (int i = 0; i < 18; ++i) v[i] = vn[i];
+      nr = nrn;
+      jj = jjn;
+    }
+    k = kn;
   }
   block_allsums<NA>(acc, sh);
   if (threadIdx.x == 0) {  // static indices keep acc in registers
 #pragma unroll
-    for (int k = 0; k < NA; ++k) {
-      if (k >= NA - 9) out[cam * 9 + (k - (NA - 9))] = acc[k];
-      else raw[cam * 45 + k] = acc[k];
+    for (int q = 0; q < NA; ++q) {
+      if (q >= NA - 9) out[cam * 9 + (q - (NA - 9))] = acc[q];
+      else raw[cam * 45 + q] = acc[q];
     }
   }
 }
