@@ -307,6 +307,11 @@ def run_gpu(args, rank: int, world: int, device: int):
             fg.errors.raise_for_status(_lib.lib.fg_schur_time_operator(backend.handle, 1e-3, 50, C.byref(sec_op),
                                                                         C.byref(bytes_op)))
             results[name]["operator"] = dict(seconds=sec_op.value, bytes=bytes_op.value)
+            # the single-pass kernel alone, back-to-back launches between CUDA events
+            sec_k, bytes_k = C.c_double(), C.c_double()
+            if _lib.lib.fg_schur_time_operator_kernel(backend.handle, 1e-3, 50, C.byref(sec_k),
+                                                     C.byref(bytes_k)) == 0:
+                results[name]["operator"].update(kernel_seconds=sec_k.value, kernel_bytes=bytes_k.value)
             var, tuned = C.c_int(), (C.c_double * 3)()
             _lib.lib.fg_schur_operator_info(backend.handle, C.byref(var), tuned)
             results[name]["operator"].update(variant=var.value, tuned_seconds=list(tuned))
@@ -587,7 +592,12 @@ def main():
     if rank == 0:
         pk, src = peaks()
         op = results[head].get("operator", {})
-        achieved = op["bytes"] / op["seconds"] / 1e9 if op.get("seconds") else None
+        # the dominant kernel: the single-pass operator kernel when it ran, else the operator
+        kern = op.get("kernel_seconds") is not None
+        k_sec = op["kernel_seconds"] if kern else op.get("seconds")
+        k_bytes = op["kernel_bytes"] if kern else op.get("bytes")
+        achieved = k_bytes / k_sec / 1e9 if k_sec else None
+        op_achieved = op["bytes"] / op["seconds"] / 1e9 if op.get("seconds") else None
         # DRAM bytes (read + write) of one k_fast_apply launch from an ncu --set full
         # capture on bal1k (FP32 records, TMA-staged variant): 130.29 MB + 3.53 MB
         traffic = MEASURED_TRAFFIC.get(args.workload, {}).get(results[head]["precision"])
@@ -613,16 +623,19 @@ def main():
             speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,
             pcg_iterations=results[head]["cg_iterations"],
             roofline=dict(bound="hbm", kernel={0: "reduced operator, generic (k_points + k_cams)",
-                                               1: "reduced operator, TMA-staged single pass (k_fast_apply + k_fast_reduce)",
-                                               2: "reduced operator, direct-load single pass (k_fast_apply_direct + "
-                                                  "k_fast_reduce)",
-                                               3: "reduced operator, prefetching direct-load single pass "
-                                                  "(k_fast_apply_pf + k_fast_reduce)"}.get(op.get("variant"),
-                                                                                           "reduced operator"),
-                          operator_variant_seconds=op.get("tuned_seconds"), achieved=achieved, peak=pk,
+                                               1: "k_fast_apply (reduced operator, TMA-staged single pass)",
+                                               2: "k_fast_apply_direct (reduced operator, direct-load single pass)",
+                                               3: "k_fast_apply_pf (reduced operator, prefetching direct-load "
+                                                  "single pass)"}.get(op.get("variant"), "reduced operator")
+                          if kern else "reduced operator", achieved=achieved, peak=pk,
                           peak_source=src, unit="GB/s", frac=(achieved / pk) if achieved else None,
-                          algorithmic_bytes_per_launch=op.get("bytes"), seconds_per_launch=op.get("seconds"),
-                          traffic=traffic, traffic_kernel="k_fast_apply" if traffic else None),
+                          algorithmic_bytes_per_launch=k_bytes, seconds_per_launch=k_sec,
+                          traffic=traffic if kern else None,
+                          operator=dict(what="the pass + k_fast_reduce (partial sums, lambda x + B x, alpha), "
+                                             "back-to-back applications", seconds_per_application=op.get("seconds"),
+                                        algorithmic_bytes=op.get("bytes"), achieved=op_achieved,
+                                        frac=(op_achieved / pk) if op_achieved else None,
+                                        variant_seconds=op.get("tuned_seconds"))),
             clocks=clocks_info, gpu_launches=launches, e2e=e2e)
         if world == 1 and not args.no_cpu_baseline:
             cs = cpu_sample(data, g)

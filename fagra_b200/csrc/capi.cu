@@ -359,6 +359,13 @@ FG_API fg_status fg_bal_restore_initial(fg_bal_problem* p) {
   if (!p) return FG_NULL_ARGUMENT;
   return p->impl.restore_initial();
 }
+FG_API fg_status fg_schur_time_operator_kernel(fg_backend* b, double lambda, size_t reps, double* seconds,
+                                               double* bytes) {
+  FG_NEED(b);
+  if (!seconds || !bytes) return FG_NULL_ARGUMENT;
+  FG_GUARD_BEGIN return b->impl->time_operator_kernel(lambda, reps, seconds, bytes);
+  FG_GUARD_END
+}
 FG_API fg_status fg_schur_time_operator(fg_backend* b, double lambda, size_t reps, double* seconds, double* bytes) {
   FG_NEED(b);
   if (!seconds || !bytes) return FG_NULL_ARGUMENT;

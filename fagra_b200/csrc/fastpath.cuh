@@ -1137,13 +1137,15 @@ struct FastPath {
 
   int variant = 1;  // FP32 operator: 1 = TMA-staged stages, 2 = direct global loads, 3 = prefetching direct
 
+  // reduce = false: the pass alone, leaving the per-CTA partial vectors (timing)
   template <class Impl, class TV>
   fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst,
-                  const int* gate = nullptr, const double* lam_dev = nullptr) {
+                  const int* gate = nullptr, const double* lam_dev = nullptr, bool reduce = true) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
     if (std::is_same<TS, float>::value && std::is_same<TV, float>::value && (variant == 2 || variant == 3)) {
       FG_TRY(apply_direct(s, (const float*)x.z, (const float*)x.pprev, x.beta, (float*)parts,
                           pst ? &pst->done : nullptr, gate, variant == 3));
+      if (!reduce) return FG_OK;
       FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
                 (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
                 dparts, pst, gate);
@@ -1173,6 +1175,7 @@ struct FastPath {
       FG_LAUNCH(kern, grid, NTHR, sm, s.st, (int64_t)s.nC, tl, d_erec.get(), d_prec.get(), x.z, x.pprev, x.beta,
                 parts, skip, gate, d_error.get(), FastExtra{});
     }
+    if (!reduce) return FG_OK;
     FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
               (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
               dparts, pst, gate);

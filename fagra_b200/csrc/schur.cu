@@ -1415,6 +1415,35 @@ class SchurImpl final : public Backend {
     return FG_OK;
   }
 
+  fg_status time_operator_kernel(double lambda, size_t reps, double* seconds, double* bytes) override {
+    if (!ready) return FG_INVALID_OPTIONS;
+    if (!fast.enabled()) return FG_UNSUPPORTED_STRUCTURE;
+    unsigned fb = 0;
+    FG_TRY(factor(lambda, &fb));
+    FG_CUDA(cudaMemsetAsync(d_z.get(), 0, retained * sizeof(TS), st));
+    PView<TS> pv{d_z.get(), nullptr, nullptr};
+    FG_TRY(fast.apply(*this, pv, lambda, d_q.get(), nullptr, nullptr, nullptr, nullptr, false));  // warm
+    cudaEvent_t a, b;
+    FG_CUDA(cudaEventCreate(&a));
+    FG_CUDA(cudaEventCreate(&b));
+    FG_CUDA(cudaEventRecord(a, st));
+    for (size_t k = 0; k < reps; ++k)
+      FG_TRY(fast.apply(*this, pv, lambda, d_q.get(), nullptr, nullptr, nullptr, nullptr, false));
+    FG_CUDA(cudaEventRecord(b, st));
+    FG_CUDA(cudaEventSynchronize(b));
+    FG_TRY(fast.check(*this));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *seconds = reps ? ms * 1e-3 / (double)reps : 0.0;
+    const double s = (double)sizeof(TS);
+    // cross blocks + edge index, point factor (lower) + edge offset, x in, camera sums out
+    *bytes = (double)nedges * (cw * pw * s + 4.0) + (double)nP * (pw * (pw + 1) / 2 * s + 4.0) +
+             (double)nC * (2.0 * cw * s);
+    return FG_OK;
+  }
+
   fg_status reduced_apply(double lambda, const double* x, double* y) override {
     if (!ready) return FG_INVALID_OPTIONS;
     unsigned fb = 0;

@@ -118,6 +118,7 @@ class Backend {
   virtual fg_status export_model(double*, double*, double*, double*, double*, double*) { return not_schur(); }
   virtual fg_status reduced_apply(double, const double*, double*) { return not_schur(); }
   virtual fg_status time_operator(double, size_t, double*, double*) { return not_schur(); }
+  virtual fg_status time_operator_kernel(double, size_t, double*, double*) { return not_schur(); }
   virtual fg_status attach_learned(fg_gnn*) { return not_schur(); }
   virtual fg_status capture_system(fg_gnn*, double, size_t, uint64_t, int, size_t*) { return not_schur(); }
   virtual void operator_info(int* variant, double* seconds3) const {

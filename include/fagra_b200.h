@@ -355,6 +355,14 @@ FG_API fg_status fg_bal_restore_initial(fg_bal_problem* problem);
  * blocks, input and output vectors). */
 FG_API fg_status fg_schur_time_operator(fg_backend* backend, double lambda, size_t repetitions,
                                         double* seconds_per_apply, double* bytes_out);
+/* The single-pass operator kernel alone (BAL-shaped systems on the fast path):
+ * mean device time of one launch over `repetitions` back-to-back launches
+ * (CUDA events on the library stream), and the algorithmic bytes it must move (cross blocks and indices,
+ * point factors, x in, the camera sums out once; not the camera Gram blocks,
+ * which the reduction step reads). FG_UNSUPPORTED_STRUCTURE without the fast
+ * path. */
+FG_API fg_status fg_schur_time_operator_kernel(fg_backend* backend, double lambda, size_t repetitions,
+                                               double* seconds_per_launch, double* bytes_out);
 
 /* The reduced-operator implementation the autotuner chose for the current
  * structure: 0 generic (any widths), 1 TMA-staged single pass, 2 direct-load

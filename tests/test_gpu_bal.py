@@ -169,3 +169,22 @@ def test_fp32_operator_variants_give_the_same_step():
         assert np.linalg.norm(steps[v] - steps[1]) <= 1e-6 * ref, v
         # FP32 accumulation order (atomics, per-CTA partials) moves the count by a few iterations
         assert abs(its[v] - its[1]) <= 6, (v, its)
+
+
+def test_operator_kernel_timing_entry_point():
+    """fg_schur_time_operator_kernel times the single-pass kernel alone and
+    reports its algorithmic bytes; it is shorter than a whole application."""
+    import ctypes as C
+    from fagra_b200 import _lib
+    d = synthetic.generate("bal1k", cameras=64, points=8000, seed=5)
+    b = fg.Schur(9 * d.num_cameras, 9, 3, precision="f32")
+    p = fg.BalProblem.from_data(d)
+    b.prepare(p.dimension())
+    p.linearize(b)
+    b.prepare_damping(1e-6)
+    sk, bk, so, bo = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    assert _lib.lib.fg_schur_time_operator_kernel(b.handle, 1e-3, 5, C.byref(sk), C.byref(bk)) == 0
+    assert _lib.lib.fg_schur_time_operator(b.handle, 1e-3, 5, C.byref(so), C.byref(bo)) == 0
+    o, n_p, n_c = d.num_observations, d.num_points, d.num_cameras
+    assert bk.value == o * (27 * 4 + 4) + n_p * (6 * 4 + 4) + n_c * 2 * 9 * 4
+    assert 0 < sk.value < so.value
