@@ -457,6 +457,14 @@ __global__ void k_precond_inverse(Layout L, const uint8_t* observed, const TS* p
 // block forms c, adds d.c to r.z and leaves c for k_coarse_add, which adds
 // W c to z before any consumer reads it.
 constexpr int MAXK = 8;
+// G staged in shared memory by every thread of the (last) block, so the
+// coarse products below read it without one global round trip per entry.
+__device__ __forceinline__ const double* stage_coarse(const double* G, int nk) {
+  __shared__ double gs[MAXK * MAXK];
+  for (int i = threadIdx.x; i < nk * nk; i += blockDim.x) gs[i] = G[i];
+  __syncthreads();
+  return gs;
+}
 __device__ __forceinline__ double coarse_finish(const double* G, int nk, const double* d, PcgState* st) {
   double extra = 0;
   for (int i = 0; i < nk; ++i) {
@@ -519,8 +527,9 @@ __global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q,
   if (arrive_last(&st->counter1)) {
     double tot[K];
     finish_sums<K>(partials, tot);
+    const double* Gs = CO ? stage_coarse(G, nk) : G;
     if (threadIdx.x == 0) {
-      if (CO) tot[1] += coarse_finish(G, nk, tot + 2, st);
+      if (CO) tot[1] += coarse_finish(Gs, nk, tot + 2, st);
       st->iterations += 1;
       st->rr = tot[0];
       bool conv = sqrt(tot[0]) < st->threshold;
@@ -596,10 +605,11 @@ __global__ void k_pcg_start(Layout L, const double* b, TX* x, TS* r, TS* z, TS* 
   if (arrive_last(&st->counter2)) {
     double tot[K];
     finish_sums<K>(partials, tot);
+    const double* Gs = CO ? stage_coarse(G, nk) : G;
     if (threadIdx.x == 0) {
       st->coarse_pending = 0;
       st->counter4 = 0;
-      if (CO) tot[1] += coarse_finish(G, nk, tot + 2, st);
+      if (CO) tot[1] += coarse_finish(Gs, nk, tot + 2, st);
       double bn = sqrt(tot[0]);
       st->bnorm = bn;
       st->threshold = rel_tol * bn;
@@ -674,8 +684,9 @@ __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* 
   if (arrive_last(&st->counter3)) {
     double tot[K];
     finish_sums<K>(partials, tot);
+    const double* Gs = CO ? stage_coarse(G, nk) : G;
     if (threadIdx.x == 0) {
-      if (CO) tot[1] += coarse_finish(G, nk, tot + 2, st);
+      if (CO) tot[1] += coarse_finish(Gs, nk, tot + 2, st);
       st->rr_last = tot[0];
       st->rr = tot[0];
       st->replacements += 1;
