@@ -740,14 +740,16 @@ __global__ void k_coarse_scale(int64_t n, int nk, const double* basis, const dou
 // G = 0 — a one-level preconditioner — when E is not positive definite. *ok
 // reports which. Launched with one warp.
 static __global__ void k_coarse_factor(int nk, const double* E, double* G, int* ok) {
-  __shared__ double L[MAXK][MAXK];
+  __shared__ double L[MAXK][MAXK], Es[MAXK * MAXK];
   __shared__ int spd_s;
   const int t = threadIdx.x;
+  for (int i = t; i < nk * nk; i += blockDim.x) Es[i] = E[i];  // one parallel round trip
+  __syncwarp();
   if (t == 0) {
     int spd = 1;
     for (int j = 0; j < nk && spd; ++j)
       for (int i = j; i < nk; ++i) {
-        double v = 0.5 * (E[i * nk + j] + E[j * nk + i]);
+        double v = 0.5 * (Es[i * nk + j] + Es[j * nk + i]);
         for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k];
         if (i == j) {
           if (!(v > 0) || !isfinite(v)) {
