@@ -21,12 +21,14 @@ replicas (the path has no exchange step); value = max over ranks.
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import signal
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -44,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
     ap.add_argument("--workload", default="bal1k")
-    ap.add_argument("--forms", default="learned,fastc,fast,f64")
+    ap.add_argument("--forms", default="learned,learned_always,fastc,fast,f64")
     ap.add_argument("--operator-variant", type=int, default=0,
                     help="FP32 reduced-operator variant (0: autotune; 1..3 force one, e.g. for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -79,11 +81,44 @@ def peaks() -> tuple[float, str]:
 
 
 # ------------------------------------------------------------------ CPU legs
+def load_synthetic():
+    """The seeded generator, loaded from its file without importing the
+    fagra_b200 package (whose import maps the product library): the CPU legs
+    run the oracle alone."""
+    spec = importlib.util.spec_from_file_location("_bal_synthetic", ROOT / "fagra_b200" / "synthetic.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses resolve their module by name
+    spec.loader.exec_module(mod)
+    return mod
+
+
+FULL_SOLVE_LIMIT = 90.0  # seconds of the oracle's recorded run up to the target
+REF_BUDGET = 150.0  # seconds of full solves in the reference arm
+
+
+def cpu_full_solve(data, g) -> dict:
+    """One full oracle LM solve (sequential f64 restatement, 1 core) from the
+    initial estimates until the accepted cost is within 1e-6 relative of the
+    oracle's own final cost: the same stopping rule as the GPU step."""
+    import oracle
+    bal = oracle.Bal.from_data(data)
+    s = oracle.Schur(9 * data.num_cameras, 9, 3)
+    t0 = time.perf_counter()
+    code, rep, st = bal.lm_to_cost(s, g["final_cost"] * (1 + REL))
+    secs = time.perf_counter() - t0
+    if code != 0 or rep.termination != 5:
+        raise RuntimeError(f"oracle did not reach the target: status {code}, termination {rep.termination}")
+    return dict(value=secs, accepted=st.accepted_steps, linearizations=st.linearizations,
+                cg=st.linear_iterations, cost=st.cost,
+                sample=f"{data.name}: one full oracle LM solve to the target ({st.linearizations} linearizations, "
+                       f"{st.linear_solves} damped solves, {st.linear_iterations} CG iterations), timed")
+
+
 def cpu_sample(data, g, cg_sample: int = 4) -> dict:
-    """Times the oracle (sequential f64 restatement, 1 core) on a bounded
-    sample of the workload: one cost evaluation, one linearization with damping
-    preparation, and `cg_sample` CG iterations of one damped solve. The
-    time-to-target estimate scales these by the oracle's own counts."""
+    """Estimate for workloads whose full oracle solve takes too long to time in
+    a bench run: one cost evaluation, one linearization with damping
+    preparation, and `cg_sample` CG iterations of one damped solve, scaled by
+    the oracle's own counts to the target."""
     import oracle
     bal = oracle.Bal.from_data(data)
     s = oracle.Schur(9 * data.num_cameras, 9, 3)
@@ -106,13 +141,32 @@ def cpu_sample(data, g, cg_sample: int = 4) -> dict:
         times.append(time.perf_counter() - t0)
     t_cg = max(times[1] - times[0], 0.0) / cg_sample
     t_fix = max(times[0] - t_cg, 0.0)
-    n_lin, n_cg, _ = target_counts(g)
+    n_lin, n_cg, recorded = target_counts(g)
     solves = n_lin - 1
     est = n_lin * t_lin + n_cg * t_cg + solves * t_fix + (solves + 1) * t_cost
-    return dict(value=est, t_lin=t_lin, t_cg=t_cg, t_fix=t_fix, t_cost=t_cost, n_lin=n_lin, n_cg=n_cg,
-                sample=f"{data.name}: 1 cost + 1 linearization/damping prep + 2 damped solves of 1 and "
-                       f"{1 + cg_sample} CG iterations, scaled by the oracle's {n_lin} linearizations, "
-                       f"{solves} solves and {n_cg} CG iterations to the target")
+    return dict(value=est, estimated=True, recorded_full_solve_seconds=recorded,
+                sample=f"{data.name}: ESTIMATE from 1 cost + 1 linearization/damping prep + 2 damped solves of 1 "
+                       f"and {1 + cg_sample} CG iterations, scaled by the oracle's {n_lin} linearizations, "
+                       f"{solves} solves and {n_cg} CG iterations to the target (the oracle's recorded full run "
+                       f"reached the target after {recorded:.1f} s on the machine that made the golden file)")
+
+
+def cpu_baseline(data, g) -> dict:
+    """The oracle timed on this host: a full solve when its recorded run to the
+    target is short enough, else the sampled estimate."""
+    if target_counts(g)[2] <= FULL_SOLVE_LIMIT:
+        return cpu_full_solve(data, g)
+    return cpu_sample(data, g)
+
+
+def workload_config(data, g, world: int) -> dict:
+    """The `config` both arms print for the same workload."""
+    return dict(workload=f"{data.name}: {data.num_cameras} cameras, {data.num_points} points, "
+                         f"{data.num_observations} observations; LM until cost <= (1+1e-6) x f64 oracle "
+                         f"cost {g['final_cost']:.6f}",
+                parallelism=f"replicas x{world}",
+                l2="inputs larger than L2 (cross blocks alone are "
+                   f"{data.num_observations * 27 * 4 / 1e6:.0f} MB in f32)")
 
 
 # ------------------------------------------------------------------ GPU legs
@@ -120,8 +174,9 @@ class Clocks:
     """nvidia-smi clock/throttle sampler running during a timed region."""
 
     def __init__(self, device: int):
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
-        self.path.parent.mkdir(exist_ok=True)
+        fd, name = tempfile.mkstemp(prefix="fagra_clocks_", suffix=".csv")
+        os.close(fd)
+        self.path = Path(name)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -153,7 +208,9 @@ class Clocks:
         self.proc.wait(timeout=10)
         t_end = time.time()
         rows = []
-        for line in self.path.read_text().splitlines():
+        text = self.path.read_text()
+        self.path.unlink(missing_ok=True)
+        for line in text.splitlines():
             f = [x.strip() for x in line.split(",")]
             if len(f) >= 9:
                 rows.append(f)
@@ -225,6 +282,8 @@ def run_gpu(args, rank: int, world: int, device: int):
     # correction); learned: fastc with the learned block preconditioner
     # (block-Jacobi fallback); f64: fagra's Schur arithmetic and default tolerance.
     forms = {"learned": dict(precision="f32", preconditioner="learned", coarse_correction=True, tol=1e-8),
+             "learned_always": dict(precision="f32", preconditioner="learned", coarse_correction=True, tol=1e-8,
+                                    learned_policy="always"),
              "fastc": dict(precision="f32", preconditioner="retained_blocks", coarse_correction=True, tol=1e-8),
              "fast": dict(precision="f32", preconditioner="retained_blocks", tol=1e-8),
              "f64": dict(precision="f64", preconditioner="retained_blocks", tol=1e-10),
@@ -232,6 +291,7 @@ def run_gpu(args, rank: int, world: int, device: int):
              "f64sd": dict(precision="f64", preconditioner="schur_diagonal", tol=1e-10),
              "fastsd": dict(precision="f32", preconditioner="schur_diagonal", tol=1e-8)}
     results = {}
+    net_cache = None
     head = args.forms.split(",")[0]
     problem = fg.BalProblem.from_data(data, device=device)
     clocks_info = None
@@ -239,8 +299,12 @@ def run_gpu(args, rank: int, world: int, device: int):
     for name in args.forms.split(","):
         kw = dict(forms[name])
         tol = kw.pop("tol")
+        policy = kw.pop("learned_policy", None)
         backend = fg.Schur(9 * data.num_cameras, 9, 3, device=device, **kw)
         backend.relative_tolerance = tol
+        if policy:
+            backend.learned_policy = policy
+            kw["learned_policy"] = policy
         if args.operator_variant:
             backend.operator_variant = args.operator_variant
         kw["relative_tolerance"] = tol
@@ -248,8 +312,12 @@ def run_gpu(args, rank: int, world: int, device: int):
         oo = opts.c()
         learned_info = None
         if kw["preconditioner"] == "learned":
-            net, learned_info = train_network(fg, synthetic, args.workload, device)
+            if net_cache is None:
+                net_cache = train_network(fg, synthetic, args.workload, device)
+            net, info = net_cache
+            learned_info = dict(info)
             backend.attach_learned(net)
+        if kw["preconditioner"] == "learned" and policy is None:
             # the one-time block-Jacobi comparison, on the first LM system (untimed)
             _lib.lib.fg_bal_restore_initial(problem._bal_handle)
             backend.prepare(problem.dimension())
@@ -288,6 +356,8 @@ def run_gpu(args, rank: int, world: int, device: int):
         ev[1].record(stream)
         barrier()
         secs = ev[0].elapsed_time(ev[1]) * 1e-3 / args.steps
+        # the preconditioner the last damped solve of the last timed step kept
+        used = backend.diagnostics().preconditioner_used
         if name == head:
             clk.mark(False)
             launches = (fg.kernel_launches() - l0) // args.steps
@@ -296,7 +366,8 @@ def run_gpu(args, rank: int, world: int, device: int):
         results[name] = dict(seconds=secs, reached_target=reached, cg_iterations=per[-1]["cg"],
                              linearizations=per[-1]["lin"], accepted=per[-1]["accepted"],
                              rejected=per[-1]["rejected"], final_cost=per[-1]["cost"],
-                             rel_cost_error=(per[-1]["cost"] - g["final_cost"]) / g["final_cost"], **kw)
+                             rel_cost_error=(per[-1]["cost"] - g["final_cost"]) / g["final_cost"],
+                             preconditioner_used=used, **kw)
         if learned_info:
             results[name]["network"] = learned_info
         if name == head:
@@ -541,6 +612,43 @@ def run_lsmr(args, device: int) -> dict:
                                          frac=ach / pk, traffic=None), e2e=None)
 
 
+def run_reference(args, world: int) -> int:
+    """The reference arm: the oracle (the sequential f64 CPU restatement of
+    fagra's path; the Rust reference cannot be built here) on this host, with
+    no product library loaded. Each step is one full LM solve to the target;
+    steps run until --steps are done or REF_BUDGET seconds have passed (at
+    least one), so the arm ends within a few minutes. Warm-up steps solve the
+    16-camera problem."""
+    synthetic = load_synthetic()
+    import oracle
+    g = gold(args.workload)
+    data = synthetic.generate(args.workload)
+    g16 = gold("bal16")
+    d16 = synthetic.generate("bal16")
+    for _ in range(args.warmup):
+        cpu_full_solve(d16, g16)
+    full = target_counts(g)[2] <= FULL_SOLVE_LIMIT
+    runs, t0 = [], time.perf_counter()
+    while len(runs) < max(args.steps, 1):
+        runs.append(cpu_full_solve(data, g) if full else cpu_sample(data, g))
+        if time.perf_counter() - t0 > REF_BUDGET:
+            break
+    v = statistics.median(r["value"] for r in runs)
+    loaded = sorted({ln.split()[-1] for ln in open("/proc/self/maps") if ln.rstrip().endswith(".so")
+                     and str(ROOT) in ln})
+    line = dict(metric=f"BA time to 1e-6 relative cost ({args.workload})", value=v, unit="s", n_gpus=world,
+                steps=len(runs), steps_requested=args.steps, warmup=args.warmup, ms_per_step=v * 1e3,
+                higher_is_better=False, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                impl="reference", config=workload_config(data, g, world),
+                form="f64 CPU restatement of fagra's path (oracle port, 1 core: the reference is sequential), "
+                     "Schur-CG with block-Jacobi on B, CG tolerance 1e-10",
+                cpu_baseline=dict(value=v, unit="s", cores=1, kind="port", sample=runs[0]["sample"]),
+                e2e=dict(value=v, unit="s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                libraries_loaded=[str(Path(x).relative_to(ROOT)) for x in loaded])
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.suite != "ba" and args.impl != "reference":
@@ -556,24 +664,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        from fagra_b200 import synthetic
-        g = gold(args.workload)
-        data = synthetic.generate(args.workload)
-        for _ in range(args.warmup):
-            cpu_sample(data, g, cg_sample=2)
-        t0 = time.perf_counter()
-        samples = [cpu_sample(data, g) for _ in range(args.steps)]
-        wall = (time.perf_counter() - t0) / args.steps
-        v = statistics.median(s["value"] for s in samples)
-        line = dict(metric=f"BA time to 1e-6 relative cost ({args.workload})", value=v, unit="s", n_gpus=args.gpus,
-                    steps=args.steps, warmup=args.warmup, ms_per_step=wall * 1e3, higher_is_better=False,
-                    scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
-                    config=dict(workload=args.workload, form="f64 CPU restatement (oracle port), Schur-CG "
-                                "block-Jacobi on B, 1e-10 CG tolerance"),
-                    cpu_baseline=dict(value=v, unit="s", cores=1, kind="port", sample=samples[0]["sample"]),
-                    e2e=dict(value=v, unit="s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
-        print(json.dumps(line), flush=True)
-        return 0
+        return run_reference(args, world)
 
     if world > 1:
         import datetime
@@ -601,24 +692,36 @@ def main():
         # DRAM bytes (read + write) of one k_fast_apply launch from an ncu --set full
         # capture on bal1k (FP32 records, TMA-staged variant): 130.29 MB + 3.53 MB
         traffic = MEASURED_TRAFFIC.get(args.workload, {}).get(results[head]["precision"])
+        descriptions = {
+            "learned": "FP32 bulk + FP64 reductions, learned block preconditioner with the block-Jacobi comparison "
+                       "policy, two-level PCG (gauge coarse correction), CG tolerance 1e-8",
+            "learned_always": "FP32 bulk + FP64 reductions, learned block preconditioner on every solve (network "
+                              "inference inside the timed region), two-level PCG, CG tolerance 1e-8",
+            "fastc": "FP32 bulk + FP64 reductions, block-Jacobi, two-level PCG (gauge coarse correction), "
+                     "CG tolerance 1e-8",
+            "fast": "FP32 bulk + FP64 reductions, block-Jacobi, CG tolerance 1e-8",
+            "f64": "f64, block-Jacobi, CG tolerance 1e-10 (fagra's Schur arithmetic)"}
+        form, form_note = head, None
+        if head == "learned" and results[head].get("preconditioner_used") != "learned":
+            # the comparison policy dropped the network: the timed steps ran block-Jacobi
+            form = "fastc"
+            form_note = ("the learned form's one-time comparison kept block-Jacobi, so its timed steps ran the "
+                         "fastc form; the learned preconditioner's own wall time is forms.learned_always")
+        learned = None
+        if "learned" in results or "learned_always" in results:
+            la = results.get("learned_always")
+            learned = dict(policy_kept=results.get("learned", {}).get("preconditioner_used"),
+                           comparison=results.get("learned", {}).get("network", {}).get("comparison"),
+                           always=None if la is None else dict(seconds=la["seconds"], cg_iterations=la["cg_iterations"],
+                                                               reached_target=la["reached_target"],
+                                                               preconditioner_used=la["preconditioner_used"]))
         line = dict(
             metric=f"BA time to 1e-6 relative cost ({args.workload})", value=vals[head], unit="s", n_gpus=world,
             steps=args.steps, warmup=args.warmup, ms_per_step=vals[head] * 1e3, higher_is_better=False,
             scaling="weak", vs_baseline=None,
             dtype="f32 bulk + f64 reductions" if results[head]["precision"] == "f32" else "f64",
-            data="synthetic",
-            config=dict(workload=f"{args.workload}: {data.num_cameras} cameras, {data.num_points} points, "
-                                 f"{data.num_observations} observations; LM until cost <= (1+1e-6) x f64 oracle "
-                                 f"cost {g['final_cost']:.6f}",
-                        form=head, form_description={
-                            "learned": "FP32 bulk + FP64 reductions, learned block preconditioner with block-Jacobi "
-                                       "fallback, two-level PCG (gauge coarse correction), CG tolerance 1e-8",
-                            "fastc": "FP32 bulk + FP64 reductions, block-Jacobi, two-level PCG (gauge coarse "
-                                     "correction), CG tolerance 1e-8",
-                            "fast": "FP32 bulk + FP64 reductions, block-Jacobi, CG tolerance 1e-8",
-                            "f64": "f64, block-Jacobi, CG tolerance 1e-10 (fagra's Schur arithmetic)"}.get(head, head),
-                        parallelism=f"replicas x{world}",
-                        l2="inputs larger than L2 (cross blocks alone are 119 MB in f32, 238 MB in f64)"),
+            data="synthetic", config=workload_config(data, g, world),
+            form=form, form_description=descriptions.get(form, form), form_note=form_note, learned=learned,
             forms={k: {kk: vv for kk, vv in v.items() if kk != "operator"} for k, v in results.items()},
             speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,
             pcg_iterations=results[head]["cg_iterations"],
@@ -638,7 +741,7 @@ def main():
                                         variant_seconds=op.get("tuned_seconds"))),
             clocks=clocks_info, gpu_launches=launches, e2e=e2e)
         if world == 1 and not args.no_cpu_baseline:
-            cs = cpu_sample(data, g)
+            cs = cpu_baseline(data, g)
             line["cpu_baseline"] = dict(value=cs["value"], unit="s", cores=1, kind="port", sample=cs["sample"])
         print(json.dumps(line), flush=True)
     if world > 1:

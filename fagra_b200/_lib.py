@@ -28,6 +28,7 @@ class SchurOptions(C.Structure):
         ("residual_replacement", C.c_double),
         ("operator_variant", C.c_int),
         ("coarse_correction", C.c_int),
+        ("learned_policy", C.c_int),
     ]
 
 

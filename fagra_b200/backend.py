@@ -122,6 +122,10 @@ class Schur:
     operator_variant = property(lambda s: s._get("operator_variant"), lambda s, v: s._set("operator_variant", v))
     coarse_correction = property(lambda s: bool(s._get("coarse_correction")),
                                  lambda s, v: s._set("coarse_correction", int(bool(v))))
+    # learned preconditioner: "compare" (default; one block-Jacobi comparison,
+    # the network is dropped when it loses) or "always"
+    learned_policy = property(lambda s: ("compare", "always")[s._get("learned_policy")],
+                              lambda s, v: s._set("learned_policy", {"compare": 0, "always": 1}[v]))
 
     def operator_info(self):
         """(variant in use, measured seconds per application of variants 1..3)."""

@@ -136,6 +136,7 @@ FG_API void fg_schur_default_options(fg_schur_options* o) {
   o->residual_replacement = 0;  // automatic spacing
   o->operator_variant = 0;
   o->coarse_correction = 0;
+  o->learned_policy = 0;
 }
 
 FG_API fg_status fg_schur_create(size_t retained, size_t cw, size_t pw, const fg_schur_options* options,

@@ -167,7 +167,12 @@ class SchurImpl final : public Backend {
       set_error("operator_variant must be 0 (autotune) or 1..3");
       return FG_INVALID_OPTIONS;
     }
-    if (o.preconditioner != opt.preconditioner) learned_compared = learned_off = false;
+    if (o.learned_policy != 0 && o.learned_policy != 1) {
+      set_error("learned_policy must be 0 (compare once) or 1 (always)");
+      return FG_INVALID_OPTIONS;
+    }
+    if (o.preconditioner != opt.preconditioner || o.learned_policy != opt.learned_policy)
+      learned_compared = learned_off = false;
     if (!o.coarse_correction) nk = 0;
     if (o.operator_variant != opt.operator_variant) fast.tuned = false;
     int keep = dev;
@@ -722,11 +727,12 @@ class SchurImpl final : public Backend {
     if (*fallbacks == 0 && nC) FG_TRY(write_block_inverses(lambda));
     if (*fallbacks == 0 && nC && learned_blocks) {
       EventTimer ti;
-      if (!learned_compared) ti.start(st);
+      const bool timed = !learned_compared && opt.learned_policy == 0;  // inference time of the comparison
+      if (timed) ti.start(st);
       FG_TRY(ensure_cross());
       unsigned nonfinite = 0;
       FG_TRY(gnn_precondition(learned, view_at(lambda), d_minv.get(), st, &nonfinite));
-      if (!learned_compared) learned_infer_seconds = ti.stop(st);
+      if (timed) learned_infer_seconds = ti.stop(st);
     }
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
     return FG_OK;
@@ -1070,7 +1076,7 @@ class SchurImpl final : public Backend {
     int term = FG_TERM_NONE;
     double est = 0;
     size_t refinements = 0;
-    const bool compare = use_learned && !learned_compared;
+    const bool compare = use_learned && !learned_compared && opt.learned_policy == 0;
     EventTimer tc;
     if (compare) tc.start(st);
     FG_TRY(run_cg(lambda, &its, &term, &est, &refinements));

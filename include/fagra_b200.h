@@ -91,6 +91,12 @@ typedef struct {
   int coarse_correction;       /* 1: two-level PCG, z = M r + W (W^T S W)^-1 W^T r with the coarse
                                   basis W a device problem supplies (BAL: the 7 similarity-gauge
                                   directions of the cameras); 0 (default): the reference's PCG */
+  int learned_policy;          /* FG_PRECOND_LEARNED only. 0 (default): the first learned solve is
+                                  compared once with a block-Jacobi solve of the same system, and
+                                  the network is switched off for this backend when block-Jacobi
+                                  needs fewer iterations or less device time; 1: the network
+                                  preconditions every solve, block-Jacobi only redoes a solve that
+                                  meets non-positive curvature or does not converge */
 } fg_schur_options;
 
 /* src/schur.rs:44-60 SchurDiagnostics (has_* = Some) */

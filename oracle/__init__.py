@@ -111,6 +111,8 @@ _sig = {
     "or_bal_linearize": (C.c_int, [C.c_void_p, C.c_void_p]),
     "or_lm_bal": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(LmOpts), C.POINTER(Report),
                             C.POINTER(LmStats), ACCEPT, C.c_void_p]),
+    "or_lm_bal_to_cost": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(LmOpts), C.c_double,
+                                    C.POINTER(Report), C.POINTER(LmStats)]),
     "or_gn_bal": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptOpts), C.POINTER(Report)]),
     "or_cbproblem_create": (C.c_void_p, [size_t, dptr, COST, LIN, C.c_void_p]),
     "or_cbproblem_destroy": (None, [C.c_void_p]),
@@ -574,6 +576,18 @@ class Bal:
         rep, st = Report(), LmStats()
         cb = ACCEPT(lambda _u, s: on_accept(s.contents)) if on_accept else ACCEPT()
         code = lib.or_lm_bal(schur.h, self.h, C.byref(o), C.byref(lo), C.byref(rep), C.byref(st), cb, None)
+        return code, rep, st
+
+    def lm_to_cost(self, schur: Schur, target_cost: float, max_iterations=50, gradient_tolerance=1e-8,
+                   lm_options=None):
+        """LM from the current estimates until an accepted cost is at or below
+        target_cost (termination 5), or the usual LM stopping rules."""
+        schur._limits()
+        o = OptOpts(max_iterations, gradient_tolerance, 0.0, 0.0)
+        lo = LmOpts(*(lm_options or (1e-3, 1e-12, 1e12, 1e-6, 1e-4, 16)))
+        rep, st = Report(), LmStats()
+        code = lib.or_lm_bal_to_cost(schur.h, self.h, C.byref(o), C.byref(lo), target_cost, C.byref(rep),
+                                     C.byref(st))
         return code, rep, st
 
     def gn(self, schur: Schur, max_iterations=20, gradient_tolerance=1e-8, step_tolerance=0.0, cost_tolerance=0.0):

@@ -5,6 +5,7 @@ checker by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs.
 """
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -20,11 +21,15 @@ def build(force: bool = False) -> Path:
         return OUT
     # -ffp-contract=off keeps the sequential f64 arithmetic free of fused
     # multiply-adds, like the Rust reference.
-    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fopenmp",
-           str(SRC), "-o", str(OUT)]
+    # written next to the target and renamed, so a process that has the old
+    # library mapped keeps a consistent file
+    tmp = OUT.with_suffix(f".so.{os.getpid()}")
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",
+           str(SRC), "-o", str(tmp)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, OUT)
     return OUT
 
 

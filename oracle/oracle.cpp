@@ -1168,8 +1168,10 @@ int validate(const LmOptions& o) {  // levenberg_marquardt.rs:47-67
 }
 
 // levenberg_marquardt.rs:330-472
+// target_cost > 0: also stop (termination 5) once an accepted cost is at or
+// below it, the stopping rule of the time-to-cost measurement.
 int lm_optimize(Linear& s, Problem& pb, const OptimizeOptions& opt, const LmOptions& lo, Report* rep, LmStats* st,
-                accept_cb_t on_accept, void* user) {
+                accept_cb_t on_accept, void* user, double target_cost = 0.0) {
   *st = LmStats{};
   int e;
   if ((e = validate(opt)) || (e = validate(lo))) return e;
@@ -1251,6 +1253,7 @@ int lm_optimize(Linear& s, Problem& pb, const OptimizeOptions& opt, const LmOpti
               st->linear_solves = s.solves;
               st->linear_iterations = s.iterations;
               if (on_accept) on_accept(user, st);
+              if (target_cost > 0 && current <= target_cost) return finish(5);
               break;
             }
             pb.reject();
@@ -1535,6 +1538,10 @@ OR_API int or_bal_linearize(void* bal, void* schur) { return ((BalProblem*)bal)-
 OR_API int or_lm_bal(void* schur, void* bal, const OptimizeOptions* opt, const LmOptions* lo, Report* rep,
                      LmStats* st, accept_cb_t cb, void* user) {
   return lm_optimize(*(Linear*)schur, *(BalProblem*)bal, *opt, *lo, rep, st, cb, user);
+}
+OR_API int or_lm_bal_to_cost(void* schur, void* bal, const OptimizeOptions* opt, const LmOptions* lo,
+                             double target_cost, Report* rep, LmStats* st) {
+  return lm_optimize(*(Linear*)schur, *(BalProblem*)bal, *opt, *lo, rep, st, nullptr, nullptr, target_cost);
 }
 OR_API int or_gn_bal(void* schur, void* bal, const OptimizeOptions* opt, Report* rep) {
   return gn_optimize(*(Linear*)schur, *(BalProblem*)bal, *opt, rep);

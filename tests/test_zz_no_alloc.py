@@ -46,6 +46,63 @@ def test_noalloc_cost_matches_handle_cost_on_two_calls(name):
         assert abs(cost - expected) <= 1e-12 * expected, (cost, expected)
 
 
+def _call(d, cams, pts, oc, op, px, out):
+    from fagra_b200 import _lib
+    from fagra_b200.errors import raise_for_status
+    raise_for_status(_lib.lib.fg_bal_cost_noalloc(
+        d.num_cameras, d.num_points, d.num_observations, C.c_void_p(cams.data_ptr()), C.c_void_p(pts.data_ptr()),
+        C.c_void_p(oc.data_ptr()), C.c_void_p(op.data_ptr()), C.c_void_p(px.data_ptr()),
+        C.c_void_p(out.data_ptr()), 0, None))
+
+
+def test_noalloc_cost_flags_out_of_range_indices_then_recovers():
+    """An observation whose camera or point index is out of range is counted
+    as an invalid evaluation on the device (out[1] = 1) and never read; the
+    next call with valid indices reports a clean evaluation again, which also
+    shows that the shared arrival counter was reset."""
+    import torch
+    import fagra_b200 as fg
+    from fagra_b200 import synthetic
+
+    d = synthetic.generate("bal16")
+    expected = fg.BalProblem.from_data(d).cost()
+    cams, pts, oc, op, px = _device_inputs(torch, d)
+    out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda:0")
+    bad_oc, bad_op = oc.clone(), op.clone()
+    bad_oc[5] = d.num_cameras          # camera index one past the end
+    bad_op[17] = d.num_points + 1000   # point index past the end
+    for a, b in ((bad_oc, op), (oc, bad_op), (bad_oc, bad_op)):
+        out.fill_(-1.0)
+        _call(d, cams, pts, a, b, px, out)
+        torch.cuda.synchronize()
+        assert out[1].item() == 1.0
+    out.fill_(-1.0)
+    _call(d, cams, pts, oc, op, px, out)
+    torch.cuda.synchronize()
+    cost, invalid = out.cpu().tolist()
+    assert invalid == 0.0
+    assert abs(cost - expected) <= 1e-12 * expected
+
+
+def test_noalloc_cost_leaves_device_memory_untouched():
+    """After a warm-up call, a call changes the device's free memory by
+    nothing: the entry point allocates no device memory of its own."""
+    import torch
+    from fagra_b200 import synthetic
+
+    d = synthetic.generate("bal16")
+    cams, pts, oc, op, px = _device_inputs(torch, d)
+    out = torch.zeros(2, dtype=torch.float64, device="cuda:0")
+    _call(d, cams, pts, oc, op, px, out)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        _call(d, cams, pts, oc, op, px, out)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_cost_rejects_oversized_problems():
     import torch
     import fagra_b200 as fg
