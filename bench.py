@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--workload", default="bal1k")
     ap.add_argument("--forms", default="learned,learned_always,fastc,fast,f64")
     ap.add_argument("--operator-variant", type=int, default=0,
-                    help="FP32 reduced-operator variant (0: autotune; 1..3 force one, e.g. for profiling)")
+                    help="FP32 reduced-operator variant (0: autotune; 1..4 force one, e.g. for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--suite", default="ba", choices=["ba", "lsmr", "windows", "learned"],
@@ -383,7 +383,7 @@ def run_gpu(args, rank: int, world: int, device: int):
             if _lib.lib.fg_schur_time_operator_kernel(backend.handle, 1e-3, 50, C.byref(sec_k),
                                                      C.byref(bytes_k)) == 0:
                 results[name]["operator"].update(kernel_seconds=sec_k.value, kernel_bytes=bytes_k.value)
-            var, tuned = C.c_int(), (C.c_double * 3)()
+            var, tuned = C.c_int(), (C.c_double * 4)()
             _lib.lib.fg_schur_operator_info(backend.handle, C.byref(var), tuned)
             results[name]["operator"].update(variant=var.value, tuned_seconds=list(tuned))
             head_backend = backend
@@ -726,10 +726,12 @@ def main():
             speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,
             pcg_iterations=results[head]["cg_iterations"],
             roofline=dict(bound="hbm", kernel={0: "reduced operator, generic (k_points + k_cams)",
-                                               1: "k_fast_apply (reduced operator, TMA-staged single pass)",
+                                               1: "k_ring (reduced operator, per-warp TMA-ring single pass)",
                                                2: "k_fast_apply_direct (reduced operator, direct-load single pass)",
                                                3: "k_fast_apply_pf (reduced operator, prefetching direct-load "
-                                                  "single pass)"}.get(op.get("variant"), "reduced operator")
+                                                  "single pass)",
+                                               4: "k_fast_apply (reduced operator, TMA-staged stage groups)"}
+                          .get(op.get("variant"), "reduced operator")
                           if kern else "reduced operator", achieved=achieved, peak=pk,
                           peak_source=src, unit="GB/s", frac=(achieved / pk) if achieved else None,
                           algorithmic_bytes_per_launch=k_bytes, seconds_per_launch=k_sec,

@@ -127,9 +127,14 @@ class Schur:
     learned_policy = property(lambda s: ("compare", "always")[s._get("learned_policy")],
                               lambda s, v: s._set("learned_policy", {"compare": 0, "always": 1}[v]))
 
+    def set_poll_limit(self, polls: int) -> None:
+        """Test hook: polls after which the ring operator's slot wait gives up
+        (the solve then raises DeviceTimeout); 0 restores the default."""
+        raise_for_status(lib.fg_schur_set_poll_limit(self._h, polls))
+
     def operator_info(self):
-        """(variant in use, measured seconds per application of variants 1..3)."""
-        var, sec = C.c_int(), (C.c_double * 3)()
+        """(variant in use, measured seconds per application of variants 1..4)."""
+        var, sec = C.c_int(), (C.c_double * 4)()
         raise_for_status(lib.fg_schur_operator_info(self._h, C.byref(var), sec))
         return var.value, list(sec)
 

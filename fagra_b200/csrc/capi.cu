@@ -373,11 +373,16 @@ FG_API fg_status fg_schur_time_operator(fg_backend* b, double lambda, size_t rep
   FG_GUARD_BEGIN return b->impl->time_operator(lambda, reps, seconds, bytes);
   FG_GUARD_END
 }
-FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds3) {
+FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds4) {
   FG_NEED(b);
   if (!variant) return FG_NULL_ARGUMENT;
-  b->impl->operator_info(variant, seconds3);
+  b->impl->operator_info(variant, seconds4);
   return FG_OK;
+}
+FG_API fg_status fg_schur_set_poll_limit(fg_backend* b, unsigned polls) {
+  FG_NEED(b);
+  FG_GUARD_BEGIN return b->impl->set_poll_limit(polls);
+  FG_GUARD_END
 }
 FG_API fg_status fg_schur_attach_learned(fg_backend* b, fg_gnn* g) {
   FG_NEED(b);

@@ -56,6 +56,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
+// Non-blocking probe of the phase (mbarrier.test_wait).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait: gives up after `limit` polls and reports failure.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned limit) {
   for (unsigned i = 0; i < limit; ++i) {
@@ -799,6 +809,49 @@ __device__ __forceinline__ void coarse_record<double>(const double* rec, float (
     E[2 * i] = (float)a.x; E[2 * i + 1] = (float)a.y;
   }
 }
+// u[a] += E_e^T W_a(cam) for one edge record (the gauge's block structure, as
+// in k_coarse_tiles).
+template <class TS>
+__device__ __forceinline__ void coarse_edge(const TS* rec, const float* wc, float (&u)[7][3]) {
+  float E[28];
+  coarse_record<TS>(rec, E);
+  typename RecWord<TS>::U word;
+  memcpy(&word, rec + 27, sizeof(word));
+  const float4* wv = reinterpret_cast<const float4*>(wc + (int64_t)RecWord<TS>::cam(word) * 72);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float4 lo = __ldg(wv + 2 * c);
+    const float x[3] = {lo.x, lo.y, lo.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int p = 0; p < 3; ++p) u[a][p] += E[p * 9 + c] * x[a];
+  }
+#pragma unroll
+  for (int c = 3; c < 6; ++c) {
+    const float4 lo = __ldg(wv + 2 * c), hi = __ldg(wv + 2 * c + 1);
+    const float x[4] = {lo.w, hi.x, hi.y, hi.z};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int p = 0; p < 3; ++p) u[3 + a][p] += E[p * 9 + c] * x[a];
+  }
+}
+// acc (packed lower 7x7) += u^T C^-1 u for one point record.
+template <class TS>
+__device__ __forceinline__ void coarse_point(const TS* r, const float (&u)[7][3], double (&acc)[28]) {
+  const double c00 = r[0], c10 = r[1], c20 = r[2], c11 = r[3], c21 = r[4], c22 = r[5];
+  int idx = 0;
+#pragma unroll
+  for (int a = 0; a < 7; ++a) {
+    const double t0 = c00 * u[a][0] + c10 * u[a][1] + c20 * u[a][2];
+    const double t1 = c10 * u[a][0] + c11 * u[a][1] + c21 * u[a][2];
+    const double t2 = c20 * u[a][0] + c21 * u[a][1] + c22 * u[a][2];
+#pragma unroll
+    for (int b = 0; b <= a; ++b) acc[idx++] += (double)u[b][0] * t0 + (double)u[b][1] * t1 + (double)u[b][2] * t2;
+  }
+}
+
 template <class TS>
 __global__ void __launch_bounds__(COARSE_WARPS * 32)
     k_coarse_tiles(FastTiles tiles, const TS* erec, const TS* prec, const float* wc, double* out) {
@@ -815,6 +868,18 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
 #pragma unroll
     for (int a = 0; a < NK; ++a) u[a][0] = u[a][1] = u[a][2] = 0.f;
     uint32_t lp = 0xFFFFu;
+    if (cnt > 32) {
+      // a point with more than 32 observations: chunks of 32 edges, one sum
+      for (int c0 = lane; c0 < cnt; c0 += 32) coarse_edge<TS>(erec + (e0 + c0) * 28, wc, u);
+#pragma unroll
+      for (int a = 0; a < NK; ++a)
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) u[a][p] += __shfl_xor_sync(0xffffffffu, u[a][p], o);
+      if (lane == 0) coarse_point(prec + p0 * 8, u, acc);
+      continue;
+    }
     if (lane < cnt) {
       float E[28];
       coarse_record<TS>(erec + (e0 + lane) * 28, E);
@@ -1011,13 +1076,23 @@ __global__ void k_fast_tiles(int pass, int64_t npt, const int64_t* pt_off, uint3
   }
 }
 
+}  // namespace fg
+
+#include "ring.cuh"
+
+namespace fg {
+
 template <class TS>
 struct FastPath {
   bool on = false;          // records are current and the shape qualifies
   bool structure = false;   // tiles and local indices built for the current structure
   bool disabled = false;    // force the generic operator (tests)
+  bool has_deep = false;    // some point has more than 32 observations (a tile of its own)
+  bool global_acc = false;  // FP32 records: the camera sums do not fit one SM (ring kernel, global accumulator)
   int64_t nwt = 0, nstages = 0;
   int grid = 0;
+  DBuf<unsigned char> d_gacc;  // global accumulator of the ring kernel (cleared by its reduction)
+  unsigned poll_limit = RING_POLL_LIMIT;  // consumer-wait polls of the ring kernel
   DBuf<int64_t> d_pbeg, d_ebeg;
   DBuf<uint32_t> d_lp;
   DBuf<TS> d_erec, d_prec;
@@ -1034,7 +1109,9 @@ struct FastPath {
   }
 
   // Tiles for the current structure from the device point offsets; a point
-  // with more than 32 observations leaves the generic operator in place.
+  // with more than 32 observations becomes a tile of its own, which only the
+  // FP32 ring kernel and the coarse pass handle (the FP64 records then keep
+  // the generic operator).
   DBuf<uint32_t> d_tile_aux;  // per-segment tile counts | total | too-deep flag
   HBuf<uint32_t> h_tile_aux;
   template <class Impl>
@@ -1056,7 +1133,8 @@ struct FastPath {
               d_ebeg.get(), d_pbeg.get(), d_lp.get());
     FG_CUDA(cudaMemcpyAsync(h_tile_aux.get(), aux + nseg, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
-    if (h_tile_aux.get()[1]) return FG_OK;
+    has_deep = h_tile_aux.get()[1] != 0;
+    if (has_deep && !std::is_same<TS, float>::value) return FG_OK;
     nwt = (int64_t)h_tile_aux.get()[0];
     nstages = (nwt + FastShape<TS>::WPS - 1) / FastShape<TS>::WPS;
     FG_TRY(d_erec.resize(std::max<size_t>(s.nedges * 28, 1)));
@@ -1074,17 +1152,80 @@ struct FastPath {
     if (disabled || s.cw != 9 || s.pw != 3 || s.nC == 0 || s.nP == 0 || s.nedges == 0) return false;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
-    size_t need = std::max(FastSmem<TS, double>::bytes((int64_t)s.nC, false),
-                           FastSmem<TS, TS>::bytes((int64_t)s.nC, false));
-    if (need > (size_t)optin) return false;  // accumulator does not fit one SM's shared memory
+    const int64_t nc = (int64_t)s.nC;
+    if (std::is_same<TS, float>::value) {
+      // the ring kernel takes any camera count: shared accumulator when the
+      // operator's and the right-hand side's fit next to the rings, else global
+      const size_t need = std::max(RingSmem<float, FAST_APPLY, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED),
+                                   RingSmem<double, FAST_RHS, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED));
+      global_acc = need > (size_t)optin;
+    } else {
+      size_t need = std::max(FastSmem<TS, double>::bytes(nc, false), FastSmem<TS, TS>::bytes(nc, false));
+      if (need > (size_t)optin) return false;  // accumulator does not fit one SM's shared memory
+    }
     if (!structure) {
       if (build(s) != FG_OK || !structure) return false;
       attr_set[0][0] = attr_set[0][1] = attr_set[1][0] = attr_set[1][1] = 0;
     }
     grid = sm_count(s.dev);
+    if (global_acc) {
+      const size_t gb = std::max((size_t)GACC_COPIES * s.nC * GACC_STRIDE * sizeof(float), s.nC * 9 * sizeof(double));
+      if (d_gacc.size() < gb) {
+        if (d_gacc.resize(gb) != FG_OK) return false;
+        if (cudaMemsetAsync(d_gacc.get(), 0, gb, s.st) != cudaSuccess) return false;
+      }
+      return true;
+    }
     if (d_parts_f.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
     if (d_parts_d.resize((size_t)grid * s.nC * 9) != FG_OK) return false;
     return true;
+  }
+
+  // Whether operator variant v can run on this structure (the direct and
+  // stage-group kernels need the shared accumulator and tiles of <= 32 edges).
+  bool variant_ok(int v) const {
+    if (!std::is_same<TS, float>::value) return true;
+    return v == 1 || (!global_acc && !has_deep);
+  }
+
+  // The ring kernel in mode MODE on vectors TV; `reduce` as in apply.
+  template <class TV, int MODE, class Impl>
+  fg_status launch_ring(Impl& s, const TV* z, const TV* pv, const double* beta, TV* parts, const int* skip,
+                        const int* gate, FastExtra ex) {
+    if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
+    FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
+    const int64_t nc = (int64_t)s.nC;
+    const float* er = reinterpret_cast<const float*>(d_erec.get());
+    const float* pr = reinterpret_cast<const float*>(d_prec.get());
+    if (!global_acc) {
+      constexpr int NW = RING_WARPS_SHARED;
+      const bool xs = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, true, NW) <= (size_t)optin;
+      const size_t sm = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, xs, NW);
+      auto kern = xs ? k_ring<TV, MODE, RACC_SHARED, true, NW> : k_ring<TV, MODE, RACC_SHARED, false, NW>;
+      FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      FG_LAUNCH(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, parts, (void*)nullptr, skip, gate,
+                d_error.get(), ex, poll_limit);
+    } else {
+      constexpr int NW = RING_WARPS_GLOBAL;
+      const size_t sm = RingSmem<TV, MODE, RACC_GLOBAL>::bytes(nc, false, NW);
+      auto kern = k_ring<TV, MODE, RACC_GLOBAL, false, NW>;
+      FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      FG_LAUNCH(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, (TV*)nullptr, (void*)d_gacc.get(), skip,
+                gate, d_error.get(), ex, poll_limit);
+    }
+    return FG_OK;
+  }
+
+  // The reduction after a ring pass with the global accumulator.
+  template <class TV, class Impl>
+  fg_status launch_gacc_reduce(Impl& s, const TV* z, const TV* pv, const double* beta, double lambda,
+                               const double* lam_dev, int use_gram, TV* out, double* dparts, PcgState* pst,
+                               const int* gate, bool fp64) {
+    const int64_t ny = (int64_t)s.nC * 9;
+    FG_LAUNCH((k_gacc_reduce<TV>), grid_for(ny, 256), 256, 0, s.st, (int64_t)s.nC, (void*)d_gacc.get(), (int)fp64,
+              reinterpret_cast<const float*>(s.d_gram.get()), s.d_observed.get(), z, pv, beta, lambda, lam_dev,
+              use_gram, out, dparts, pst, gate);
+    return FG_OK;
   }
 
   // The coarse Galerkin matrix W^T S(lambda) W in two passes (cameras, then
@@ -1116,6 +1257,14 @@ struct FastPath {
     return FG_OK;
   }
 
+  // After passes launched without their reduction (timing): clear the global
+  // accumulator they left behind.
+  template <class Impl>
+  fg_status settle(Impl& s) {
+    if (global_acc && d_gacc.size()) FG_CUDA(cudaMemsetAsync(d_gacc.get(), 0, d_gacc.size(), s.st));
+    return FG_OK;
+  }
+
   // A bounded TMA wait that gave up leaves 1 in d_error.
   template <class Impl>
   fg_status check(Impl& s) {
@@ -1124,6 +1273,8 @@ struct FastPath {
     FG_CUDA(cudaMemcpyAsync(&h, d_error.get(), sizeof(int), cudaMemcpyDeviceToHost, s.st));
     FG_CUDA(cudaStreamSynchronize(s.st));
     if (h) {
+      // reported once: the next solve starts with a clear flag
+      FG_CUDA(cudaMemsetAsync(d_error.get(), 0, sizeof(int), s.st));
       set_error("reduced operator: a bounded shared-memory pipeline wait timed out");
       return FG_DEVICE_TIMEOUT;
     }
@@ -1142,6 +1293,20 @@ struct FastPath {
   fg_status apply(Impl& s, PView<TV> x, double lambda, TV* out, double* dparts, PcgState* pst,
                   const int* gate = nullptr, const double* lam_dev = nullptr, bool reduce = true) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
+    if constexpr (std::is_same<TS, float>::value) {
+      if (variant == 1 || !variant_ok(variant)) {
+        FG_TRY((launch_ring<TV, FAST_APPLY>(s, x.z, x.pprev, x.beta, parts, pst ? &pst->done : nullptr, gate,
+                                            FastExtra{})));
+        if (!reduce) return FG_OK;
+        if (global_acc)
+          return launch_gacc_reduce<TV>(s, x.z, x.pprev, x.beta, lambda, lam_dev, 1, out, dparts, pst, gate,
+                                        !std::is_same<TV, float>::value);
+        FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
+                  (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
+                  dparts, pst, gate);
+        return FG_OK;
+      }
+    }
     if (std::is_same<TS, float>::value && std::is_same<TV, float>::value && (variant == 2 || variant == 3)) {
       FG_TRY(apply_direct(s, (const float*)x.z, (const float*)x.pprev, x.beta, (float*)parts,
                           pst ? &pst->done : nullptr, gate, variant == 3));
@@ -1226,6 +1391,20 @@ struct FastPath {
   // to its eliminated part.
   template <class Impl>
   fg_status rhs(Impl& s, const double* w, double* rhs_out) {
+    if constexpr (std::is_same<TS, float>::value) {
+      FG_TRY((launch_ring<double, FAST_RHS>(s, w, (const double*)nullptr, (const double*)nullptr, d_parts_d.get(),
+                                            (const int*)nullptr, (const int*)nullptr,
+                                            FastExtra{w + s.retained, nullptr, nullptr})));
+      if (global_acc)
+        return launch_gacc_reduce<double>(s, w, (const double*)nullptr, (const double*)nullptr, 1.0,
+                                          (const double*)nullptr, 0, rhs_out, (double*)nullptr, (PcgState*)nullptr,
+                                          (const int*)nullptr, true);
+      FG_LAUNCH((k_fast_reduce<TS, double>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
+                (const double*)d_parts_d.get(), s.d_gram.get(), s.d_observed.get(), w, (const double*)nullptr,
+                (const double*)nullptr, 1.0, (const double*)nullptr, 0, rhs_out, (double*)nullptr, (PcgState*)nullptr,
+                (const int*)nullptr);
+      return FG_OK;
+    }
     if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
     size_t sm = FastSmem<TS, double>::bytes((int64_t)s.nC, false);
     auto kern = k_fast_apply<TS, double, false, FAST_RHS>;
@@ -1246,6 +1425,11 @@ struct FastPath {
   // with observations (src/schur.rs:312-344); g is the gradient.
   template <class Impl>
   fg_status recover(Impl& s, const double* zred, const double* g, const double* scales, double* step) {
+    if constexpr (std::is_same<TS, float>::value) {
+      return launch_ring<double, FAST_RECOVER>(s, zred, (const double*)nullptr, (const double*)nullptr,
+                                               (double*)nullptr, (const int*)nullptr, (const int*)nullptr,
+                                               FastExtra{g + s.retained, scales + s.retained, step + s.retained});
+    }
     if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
     // x staged in the space the other modes give their accumulator
     size_t sm = FastSmem<TS, double>::bytes((int64_t)s.nC, false);

@@ -164,7 +164,7 @@ class SchurImpl final : public Backend {
       return FG_INVALID_OPTIONS;
     }
     if (o.operator_variant < 0 || o.operator_variant > NVARIANTS) {
-      set_error("operator_variant must be 0 (autotune) or 1..3");
+      set_error("operator_variant must be 0 (autotune) or 1..4");
       return FG_INVALID_OPTIONS;
     }
     if (o.learned_policy != 0 && o.learned_policy != 1) {
@@ -792,12 +792,12 @@ class SchurImpl final : public Backend {
     if (kind == 1) return gnn_capture(g, view_at(lambda), probes, seed, 1, solve, d_work.get(), d_qd.get(), st, index);
     return gnn_capture(g, view_at(lambda), probes, seed, 0, apply, d_work.get(), d_qd.get(), st, index);
   }
-  // Operator autotuner: times each FP32 single-pass variant (TMA-staged
-  // stages, direct global loads, prefetching direct loads) on this structure
-  // and keeps the fastest. Runs once per structure shape (device, cameras,
-  // points, edges, warp tiles) in the process; the factorization it needs is
-  // redone by every solve.
-  static constexpr int NVARIANTS = 3;
+  // Operator autotuner: times each FP32 single-pass variant that applies to
+  // this structure (per-warp TMA rings, direct global loads, prefetching
+  // direct loads, TMA-staged stage groups) and keeps the fastest. Runs once
+  // per structure shape (device, cameras, points, edges, warp tiles) in the
+  // process; the factorization it needs is redone by every solve.
+  static constexpr int NVARIANTS = 4;
   struct TunedShape {
     int dev;
     int64_t ncam, npt, nedge, nwt;
@@ -817,7 +817,12 @@ class SchurImpl final : public Backend {
     static auto* m = new std::map<TunedShape, TunedChoice>();
     return *m;
   }
-  double tuned_seconds[NVARIANTS] = {0, 0, 0};
+  double tuned_seconds[NVARIANTS] = {0, 0, 0, 0};
+  fg_status set_poll_limit(unsigned polls) override {
+    fast.poll_limit = polls ? polls : RING_POLL_LIMIT;
+    drop_graphs();
+    return FG_OK;
+  }
   void operator_info(int* variant, double* seconds) const override {
     *variant = fast.enabled() ? fast.variant : 0;
     if (seconds)
@@ -826,7 +831,7 @@ class SchurImpl final : public Backend {
   fg_status autotune_operator() {
     if (!fast.on || !is_f32() || fast.tuned) return FG_OK;
     if (opt.operator_variant >= 1 && opt.operator_variant <= NVARIANTS) {
-      fast.variant = opt.operator_variant;
+      fast.variant = fast.variant_ok(opt.operator_variant) ? opt.operator_variant : 1;
       fast.tuned = true;
       drop_graphs();
       return FG_OK;
@@ -854,6 +859,8 @@ class SchurImpl final : public Backend {
     float best = 1e30f;
     int best_v = 1;
     for (int v = 1; v <= NVARIANTS; ++v) {
+      tuned_seconds[v - 1] = 0;
+      if (!fast.variant_ok(v)) continue;
       fast.variant = v;
       FG_TRY(apply_reduced<TS>(pv, 1.0, 1.0, true, d_t.get(), d_q.get(), nullptr, nullptr));
       cudaEventRecord(a, st);
@@ -949,6 +956,7 @@ class SchurImpl final : public Backend {
             (uintptr_t)d_Wt.get(), (uintptr_t)d_G.get(), (uintptr_t)fast.d_ebeg.get(), (uintptr_t)fast.d_pbeg.get(),
             (uintptr_t)fast.d_erec.get(), (uintptr_t)fast.d_prec.get(), (uintptr_t)fast.d_parts_f.get(),
             (uintptr_t)fast.d_parts_d.get(), (uintptr_t)fast.d_error.get(), (uintptr_t)fast.variant,
+            (uintptr_t)fast.d_gacc.get(), (uintptr_t)fast.global_acc, (uintptr_t)fast.poll_limit,
             (uintptr_t)fast.nwt, (uintptr_t)fast.nstages, (uintptr_t)fast.grid, (uintptr_t)coarse_on,
             (uintptr_t)nk, (uintptr_t)nC, (uintptr_t)nP, (uintptr_t)retained, (uintptr_t)dim};
   }
@@ -1437,6 +1445,7 @@ class SchurImpl final : public Backend {
       FG_TRY(fast.apply(*this, pv, lambda, d_q.get(), nullptr, nullptr, nullptr, nullptr, false));
     FG_CUDA(cudaEventRecord(b, st));
     FG_CUDA(cudaEventSynchronize(b));
+    FG_TRY(fast.settle(*this));
     FG_TRY(fast.check(*this));
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);

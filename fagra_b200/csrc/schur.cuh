@@ -121,10 +121,11 @@ class Backend {
   virtual fg_status time_operator_kernel(double, size_t, double*, double*) { return not_schur(); }
   virtual fg_status attach_learned(fg_gnn*) { return not_schur(); }
   virtual fg_status capture_system(fg_gnn*, double, size_t, uint64_t, int, size_t*) { return not_schur(); }
-  virtual void operator_info(int* variant, double* seconds3) const {
+  virtual void operator_info(int* variant, double* seconds4) const {
     *variant = 0;
-    if (seconds3) seconds3[0] = seconds3[1] = seconds3[2] = 0;
+    if (seconds4) seconds4[0] = seconds4[1] = seconds4[2] = seconds4[3] = 0;
   }
+  virtual fg_status set_poll_limit(unsigned) { return not_schur(); }
   // LSMR-only extras.
   virtual fg_status set_lsmr_options(const fg_lsmr_options&) { return not_lsmr(); }
   virtual void lsmr_diagnostics(fg_lsmr_diagnostics* d) const { *d = fg_lsmr_diagnostics{}; }
