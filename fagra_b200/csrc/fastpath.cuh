@@ -231,6 +231,55 @@ __device__ __forceinline__ void load_point(const TS* r, TV& c0, TV& c1, TV& c2, 
   }
 }
 
+// Adds 9 values to the 64-bit fixed-point accumulator held as low and high
+// 32-bit words: all nine low-word atomics are issued first (their returned
+// old values give the carries), then the nine high words as reductions
+// without a return, so the round trips overlap instead of forming a chain.
+// An FP32 value times a power of two converts exactly from FP32 (fmf != 0)
+// or from FP64: the integer is the same.
+template <class TV>
+__device__ __forceinline__ void fixed_scatter(uint32_t* ylo, uint32_t* yhi, int64_t y0, const TV (&v)[9], double fm,
+                                              float fmf) {
+  uint32_t lo[9], hi[9], old[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const long long q = (std::is_same<TV, float>::value && fmf != 0.f) ? __float2ll_rn((float)v[c] * fmf)
+                                                                       : __double2ll_rn((double)v[c] * fm);
+    lo[c] = (uint32_t)q;
+    hi[c] = (uint32_t)((unsigned long long)q >> 32);
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) old[c] = atomicAdd(&ylo[y0 + c], lo[c]);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) atomicAdd(&yhi[y0 + c], hi[c] + ((uint32_t)(old[c] + lo[c]) < old[c] ? 1u : 0u));
+}
+
+// fx_mul in FP32 for fixed_scatter: nonzero only when it is exactly
+// representable as a normal FP32 number (a power of two in [2^-120, 2^120]).
+__device__ __forceinline__ float fixed_mulf(double fm) {
+  return (fm >= 0x1p-120 && fm <= 0x1p120) ? (float)fm : 0.f;
+}
+
+// Inclusive segmented sum over the lanes of each run of equal keys, with an
+// early exit once no lane has a run predecessor at the current distance
+// (short tracks need 3 steps instead of 5).
+template <class TV>
+__device__ __forceinline__ void seg_scan3(TV& u0, TV& u1, TV& u2, uint32_t key, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t lo = __shfl_up_sync(0xffffffffu, key, off);
+    const bool take = lane >= off && lo == key;
+    if (!__any_sync(0xffffffffu, take)) break;
+    const TV v0 = __shfl_up_sync(0xffffffffu, u0, off), v1 = __shfl_up_sync(0xffffffffu, u1, off);
+    const TV v2 = __shfl_up_sync(0xffffffffu, u2, off);
+    if (take) {
+      u0 += v0;
+      u1 += v1;
+      u2 += v2;
+    }
+  }
+}
+
 // Modes of the edge-record pass (all read every record once):
 //   FAST_APPLY:   partials <- -E C^-1 E^T x                 (x = z + beta p)
 //   FAST_RHS:     partials <- -E w_p, w_p read per point     (src/schur.rs:230-242)
@@ -321,6 +370,7 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
   }
   if (FIXED) __syncthreads();
   const double fx_mul = FIXED ? fx_mul_s : 0.0;
+  const float fx_mulf = FIXED ? fixed_mulf(fx_mul_s) : 0.f;
 
   auto issue = [&](int64_t sidx, int b) {
     int64_t wt0 = sidx * WPS, wt1 = min(wt0 + WPS, tiles.nwt);
@@ -387,18 +437,9 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
           u2 += E[18 + c] * xc[c];
         }
       }
-      // segmented inclusive scan over the lanes of each point
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        TV v0 = __shfl_up_sync(0xffffffffu, u0, off), v1 = __shfl_up_sync(0xffffffffu, u1, off);
-        TV v2 = __shfl_up_sync(0xffffffffu, u2, off);
-        uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
-        if (lane >= off && lo == lp) {
-          u0 += v0;
-          u1 += v1;
-          u2 += v2;
-        }
-      }
+      // segmented inclusive scan over the lanes of each point (inactive lanes
+      // get keys of their own)
+      seg_scan3<TV>(u0, u1, u2, lane < cnt ? lp : 0x10000u + lane, lane);
       uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
       bool last = lane < cnt && (lane == cnt - 1 || lpn != lp);
       TV t0 = 0, t1 = 0, t2 = 0;
@@ -434,15 +475,10 @@ __global__ void __launch_bounds__(FAST_GROUPS * FastShape<TS>::WPS * 32, 1)
       }
       if (MODE != FAST_RECOVER && lane < cnt) {
         if (FIXED) {
-          const int64_t y0 = (int64_t)cam * 9;
+          TV v[9];
 #pragma unroll
-          for (int c = 0; c < 9; ++c) {
-            const TV v = -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2);
-            const long long q = __double2ll_rn((double)v * fx_mul);
-            const uint32_t lo = (uint32_t)q;
-            const uint32_t old = atomicAdd(&ylo[y0 + c], lo);
-            atomicAdd(&yhi[y0 + c], (uint32_t)(q >> 32) + ((uint32_t)(old + lo) < old ? 1u : 0u));
-          }
+          for (int c = 0; c < 9; ++c) v[c] = -(E[c] * t0 + E[9 + c] * t1 + E[18 + c] * t2);
+          fixed_scatter(ylo, yhi, (int64_t)cam * 9, v, fx_mul, fx_mulf);
         } else {
           TV* y = ys + (int64_t)cam * 9;
 #pragma unroll
@@ -1156,8 +1192,9 @@ struct FastPath {
     if (std::is_same<TS, float>::value) {
       // the ring kernel takes any camera count: shared accumulator when the
       // operator's and the right-hand side's fit next to the rings, else global
-      const size_t need = std::max(RingSmem<float, FAST_APPLY, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED),
-                                   RingSmem<double, FAST_RHS, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED));
+      const size_t need =
+          std::max(RingSmem<float, FAST_APPLY, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED, RING_SLOTS_SHARED),
+                   RingSmem<double, FAST_RHS, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED, RING_SLOTS_SHARED));
       global_acc = need > (size_t)optin;
     } else {
       size_t need = std::max(FastSmem<TS, double>::bytes(nc, false), FastSmem<TS, TS>::bytes(nc, false));
@@ -1198,17 +1235,17 @@ struct FastPath {
     const float* er = reinterpret_cast<const float*>(d_erec.get());
     const float* pr = reinterpret_cast<const float*>(d_prec.get());
     if (!global_acc) {
-      constexpr int NW = RING_WARPS_SHARED;
-      const bool xs = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, true, NW) <= (size_t)optin;
-      const size_t sm = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, xs, NW);
-      auto kern = xs ? k_ring<TV, MODE, RACC_SHARED, true, NW> : k_ring<TV, MODE, RACC_SHARED, false, NW>;
+      constexpr int NW = RING_WARPS_SHARED, R = RING_SLOTS_SHARED;
+      const bool xs = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, true, NW, R) <= (size_t)optin;
+      const size_t sm = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, xs, NW, R);
+      auto kern = xs ? k_ring<TV, MODE, RACC_SHARED, true, NW, R> : k_ring<TV, MODE, RACC_SHARED, false, NW, R>;
       FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       FG_LAUNCH(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, parts, (void*)nullptr, skip, gate,
                 d_error.get(), ex, poll_limit);
     } else {
-      constexpr int NW = RING_WARPS_GLOBAL;
-      const size_t sm = RingSmem<TV, MODE, RACC_GLOBAL>::bytes(nc, false, NW);
-      auto kern = k_ring<TV, MODE, RACC_GLOBAL, false, NW>;
+      constexpr int NW = RING_WARPS_GLOBAL, R = RING_SLOTS_GLOBAL;
+      const size_t sm = RingSmem<TV, MODE, RACC_GLOBAL>::bytes(nc, false, NW, R);
+      auto kern = k_ring<TV, MODE, RACC_GLOBAL, false, NW, R>;
       FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       FG_LAUNCH(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, (TV*)nullptr, (void*)d_gacc.get(), skip,
                 gate, d_error.get(), ex, poll_limit);

@@ -1,15 +1,19 @@
 // Per-warp TMA rings for the single-pass BAL reduced operator (FP32 edge
-// records). Replaces the stage-group pipeline of k_fast_apply for the FP32
-// records: every warp streams its own warp tiles through a private ring of
-// RING_SLOTS shared-memory slots, so no barrier couples the warps of a CTA
-// inside the main loop and a slow tile stalls only its own warp.
+// records). Every warp streams its own warp tiles (tile first + k G) through
+// a private ring of R shared-memory slots, so no barrier couples the warps of
+// a CTA inside the main loop and a slow tile stalls only its own warp.
 //
 // A slot holds one warp tile: its edge records (<= 32 x 112 bytes) and the
 // point records of the tile's points (<= 32 x 32 bytes), both fetched by
 // lane 0 with 1-D bulk copies (cp.async.bulk) onto the slot's mbarrier, so
 // neither the cross blocks nor C^-1 is a dependent global load of the
-// consumer. The bounds of the tile two ahead are loaded by lane 0 while the
-// current tile is processed.
+// consumer. Two things keep enough bytes in flight with few slots:
+//  * a slot is handed to the next tile as soon as its lanes hold the tile's
+//    records and C^-1 in registers, before the tile's arithmetic, so the
+//    copy of tile k + R overlaps the work on tile k;
+//  * the bounds of the warp's tiles are loaded 32 tiles at a time (lane l
+//    holds tile 32 c + l) one batch ahead, so no refill waits on a global
+//    load of its bounds.
 //
 // Camera accumulation, chosen by the number of cameras:
 //  * shared (RACC_SHARED): the CTA-private 9C accumulator of k_fast_apply
@@ -31,11 +35,12 @@
 
 namespace fg {
 
-constexpr int RING_SLOTS = 2;
 constexpr int RING_EDGE_BYTES = 32 * 28 * 4;                 // edge records of one warp tile
 constexpr int RING_SLOT_BYTES = RING_EDGE_BYTES + 32 * 8 * 4;  // + its point records
-constexpr int RING_WARPS_SHARED = 12;
-constexpr int RING_WARPS_GLOBAL = 16;
+constexpr int RING_WARPS_SHARED = 16;  // with one slot per warp (shared accumulator)
+constexpr int RING_SLOTS_SHARED = 1;
+constexpr int RING_WARPS_GLOBAL = 16;  // with two slots per warp (global accumulator)
+constexpr int RING_SLOTS_GLOBAL = 2;
 constexpr int GACC_COPIES = 8;   // FP32 global accumulator copies
 constexpr int GACC_STRIDE = 12;  // floats per camera in an FP32 copy (three 16-byte vectors)
 constexpr unsigned RING_POLL_LIMIT = 1u << 22;
@@ -54,9 +59,9 @@ struct RingSmem {
   __host__ __device__ static size_t xs_bytes(int64_t ncam, bool xs) {
     return xs && MODE != FAST_RHS ? FastSmem<float, TV>::vec_bytes(ncam) : 0;
   }
-  __host__ __device__ static size_t bytes(int64_t ncam, bool xs, int nw) {
-    const size_t bars = ((size_t)nw * RING_SLOTS * 8 + 127) & ~(size_t)127;
-    return acc_bytes(ncam) + xs_bytes(ncam, xs) + bars + (size_t)nw * RING_SLOTS * RING_SLOT_BYTES;
+  __host__ __device__ static size_t bytes(int64_t ncam, bool xs, int nw, int slots) {
+    const size_t bars = ((size_t)nw * slots * 8 + 127) & ~(size_t)127;
+    return acc_bytes(ncam) + xs_bytes(ncam, xs) + bars + (size_t)nw * slots * RING_SLOT_BYTES;
   }
 };
 
@@ -72,14 +77,18 @@ __device__ __forceinline__ bool warp_wait(uint64_t* bar, unsigned parity, unsign
   return false;
 }
 
-// One tile's bounds, held by every lane of the warp.
+// One tile's bounds.
 struct RingTile {
   int64_t e0, p0;
   int cnt, np;
 };
-__device__ __forceinline__ RingTile ring_bounds(const FastTiles& t, int64_t wt) {
+// Bounds of the warp's tiles kb + lane (tile index first + (kb + lane) G),
+// zero past the warp's last tile.
+__device__ __forceinline__ RingTile ring_batch(const FastTiles& t, int64_t first, int64_t G, int64_t nmine, int64_t kb,
+                                               int lane) {
   RingTile r{0, 0, 0, 0};
-  if (wt < t.nwt) {
+  if (kb + lane < nmine) {
+    const int64_t wt = first + (kb + lane) * G;
     r.e0 = t.wt_e0[wt];
     r.cnt = (int)(t.wt_e0[wt + 1] - r.e0);
     r.p0 = t.wt_p0[wt];
@@ -87,12 +96,13 @@ __device__ __forceinline__ RingTile ring_bounds(const FastTiles& t, int64_t wt) 
   }
   return r;
 }
-__device__ __forceinline__ RingTile ring_bcast(const RingTile& r) {
+// The bounds lane l holds in batch a (cur) or b, for every lane.
+__device__ __forceinline__ RingTile ring_pick(const RingTile& a, const RingTile& b, bool cur, int l) {
   RingTile o;
-  o.e0 = __shfl_sync(0xffffffffu, r.e0, 0);
-  o.p0 = __shfl_sync(0xffffffffu, r.p0, 0);
-  o.cnt = __shfl_sync(0xffffffffu, r.cnt, 0);
-  o.np = __shfl_sync(0xffffffffu, r.np, 0);
+  o.e0 = __shfl_sync(0xffffffffu, cur ? a.e0 : b.e0, l);
+  o.p0 = __shfl_sync(0xffffffffu, cur ? a.p0 : b.p0, l);
+  o.cnt = __shfl_sync(0xffffffffu, cur ? a.cnt : b.cnt, l);
+  o.np = __shfl_sync(0xffffffffu, cur ? a.np : b.np, l);
   return o;
 }
 
@@ -104,17 +114,11 @@ struct RingScatter {
   double* yd;   // shared FP64 (RHS) or global FP64 copy
   float* gf;    // global FP32 copy of this CTA
   double fx_mul;
+  float fx_mulf;  // fx_mul in FP32 when it is a normal FP32 number, else 0
   __device__ __forceinline__ void add(uint32_t cam, const TV (&v)[9]) const {
     if (ACC == RACC_SHARED) {
       if (RingSmem<TV, MODE, ACC>::FIXED) {
-        const int64_t y0 = (int64_t)cam * 9;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-          const long long q = __double2ll_rn((double)v[c] * fx_mul);
-          const uint32_t lo = (uint32_t)q;
-          const uint32_t old = atomicAdd(&ylo[y0 + c], lo);
-          atomicAdd(&yhi[y0 + c], (uint32_t)(q >> 32) + ((uint32_t)(old + lo) < old ? 1u : 0u));
-        }
+        fixed_scatter(ylo, yhi, (int64_t)cam * 9, v, fx_mul, fx_mulf);
       } else {
         double* y = yd + (int64_t)cam * 9;
 #pragma unroll
@@ -147,7 +151,7 @@ __device__ __forceinline__ void ring_x(uint32_t cam, const TV* xs, const TV* z, 
   }
 }
 
-template <class TV, int MODE, int ACC, bool XS, int NW>
+template <class TV, int MODE, int ACC, bool XS, int NW, int R>
 __global__ void __launch_bounds__(NW * 32, 1)
     k_ring(int64_t ncam, FastTiles tiles, const float* erec, const float* prec, const TV* z, const TV* pv,
            const double* beta, TV* partials, void* gacc, const int* skip, const int* gate, int* error,
@@ -169,9 +173,8 @@ __global__ void __launch_bounds__(NW * 32, 1)
   double* yds = reinterpret_cast<double*>(smem);
   TV* xs = reinterpret_cast<TV*>(smem + acc);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + acc + xsb);
-  unsigned char* ring =
-      smem + acc + xsb + (((size_t)NW * RING_SLOTS * 8 + 127) & ~(size_t)127) + (size_t)w * RING_SLOTS * RING_SLOT_BYTES;
-  uint64_t* wbar = bars + w * RING_SLOTS;
+  unsigned char* ring = smem + acc + xsb + (((size_t)NW * R * 8 + 127) & ~(size_t)127) + (size_t)w * R * RING_SLOT_BYTES;
+  uint64_t* wbar = bars + w * R;
 
   const TV bv = pv ? (TV)*beta : (TV)0;
   double xmax = 0.0;
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
     if (lane == 0) wmax[w] = xmax;
   }
   if (lane == 0) {
-    for (int b = 0; b < RING_SLOTS; ++b) mbar_init(&wbar[b], 1);
+    for (int b = 0; b < R; ++b) mbar_init(&wbar[b], 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -221,12 +224,20 @@ __global__ void __launch_bounds__(NW * 32, 1)
   sc.ylo = ylo;
   sc.yhi = yhi;
   sc.fx_mul = FIXED ? fx_mul_s : 0.0;
+  sc.fx_mulf = FIXED ? fixed_mulf(fx_mul_s) : 0.f;
   sc.gf = ACC == RACC_GLOBAL ? reinterpret_cast<float*>(gacc) + (int64_t)(blockIdx.x % GACC_COPIES) * ncam * GACC_STRIDE
                              : nullptr;
   sc.yd = ACC == RACC_SHARED ? yds : reinterpret_cast<double*>(gacc);
 
   const int64_t G = (int64_t)gridDim.x * NW;
   const int64_t first = (int64_t)blockIdx.x * NW + w;
+  const int64_t nmine = first < tiles.nwt ? (tiles.nwt - 1 - first) / G + 1 : 0;  // this warp's tiles
+  // Lane l holds the bounds of this warp's tile 32 c + l for the current batch
+  // c (ba) and the next (bb): one coalesced round of loads per 32 tiles, off
+  // the critical path of the refills.
+  RingTile ba = ring_batch(tiles, first, G, nmine, 0, lane), bb = ring_batch(tiles, first, G, nmine, 32, lane);
+  int64_t cbatch = 0;
+  auto bounds = [&](int64_t kk) { return ring_pick(ba, bb, (kk >> 5) == cbatch, (int)(kk & 31)); };
   // lane 0 issues the copies of a tile into slot b (a deep tile needs none:
   // an arrival without transaction bytes completes the slot's phase)
   auto issue = [&](const RingTile& t, int b) {
@@ -239,22 +250,24 @@ __global__ void __launch_bounds__(NW * 32, 1)
     if (eb) tma_load_1d(dst, erec + t.e0 * 28, eb, &wbar[b]);
     if (pb) tma_load_1d(dst + RING_EDGE_BYTES, prec + t.p0 * 8, pb, &wbar[b]);
   };
-  RingTile cur[RING_SLOTS];
+  // the slot's data is in registers: hand the slot to the tile R ahead
+  auto refill = [&](int64_t k, int b) {
+    __syncwarp();
+    if (k + R < nmine) {
+      const RingTile n = bounds(k + R);
+      if (lane == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(n, b);
+    }
+  };
 #pragma unroll
-  for (int b = 0; b < RING_SLOTS; ++b) {
-    cur[b] = ring_bcast(ring_bounds(tiles, first + b * G));
-    if (first + b * G < tiles.nwt) issue(cur[b], b);
-  }
+  for (int b = 0; b < R; ++b)
+    if (b < nmine) issue(bounds(b), b);
   bool failed = false;
   int64_t k = 0;
-  for (int64_t wt = first; wt < tiles.nwt; wt += G, ++k) {
-    const int b = (int)(k & (RING_SLOTS - 1));
-    const unsigned parity = (unsigned)((k / RING_SLOTS) & 1);
-    const RingTile t = b == 0 ? cur[0] : cur[1];
-    // bounds of the tile this slot takes next, loaded while this one is processed
-    const int64_t wn = wt + RING_SLOTS * G;
-    RingTile nx{0, 0, 0, 0};
-    if (lane == 0 && wn < tiles.nwt) nx = ring_bounds(tiles, wn);
+  for (; k < nmine; ++k) {
+    const int b = (int)(k % R);
+    const unsigned parity = (unsigned)((k / R) & 1);
+    const RingTile t = bounds(k);
     if (!warp_wait(&wbar[b], parity, poll_limit)) {
       failed = true;
       break;
@@ -264,33 +277,29 @@ __global__ void __launch_bounds__(NW * 32, 1)
       // ---------------------------------------------------- shallow tile
       TV E[27];
       uint32_t cam = 0, lp = 0xFFFFu;
-      TV u0 = 0, u1 = 0, u2 = 0;
+      TV c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;  // the lane's point C^-1 (packed lower)
       if (lane < t.cnt) {
         load_record<TV>(reinterpret_cast<const float*>(slot) + lane * 28, E, cam, lp);
-        if (NEED_X) {
-          TV xc[9];
-          ring_x<TV, XS>(cam, xs, z, pv, bv, xc);
-#pragma unroll
-          for (int c = 0; c < 9; ++c) {
-            u0 += E[c] * xc[c];
-            u1 += E[9 + c] * xc[c];
-            u2 += E[18 + c] * xc[c];
-          }
+        if (MODE != FAST_RHS) {
+          const float4* pr = reinterpret_cast<const float4*>(slot + RING_EDGE_BYTES + (size_t)lp * 32);
+          const float4 ca = pr[0], cb = pr[1];
+          c0 = ca.x; c1 = ca.y; c2 = ca.z; c3 = ca.w; c4 = cb.x; c5 = cb.y;
         }
       }
-      if (NEED_X) {
+      refill(k, b);
+      TV u0 = 0, u1 = 0, u2 = 0;
+      if (NEED_X && lane < t.cnt) {
+        TV xc[9];
+        ring_x<TV, XS>(cam, xs, z, pv, bv, xc);
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-          const TV v0 = __shfl_up_sync(0xffffffffu, u0, off), v1 = __shfl_up_sync(0xffffffffu, u1, off);
-          const TV v2 = __shfl_up_sync(0xffffffffu, u2, off);
-          const uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
-          if (lane >= off && lo == lp) {
-            u0 += v0;
-            u1 += v1;
-            u2 += v2;
-          }
+        for (int c = 0; c < 9; ++c) {
+          u0 += E[c] * xc[c];
+          u1 += E[9 + c] * xc[c];
+          u2 += E[18 + c] * xc[c];
         }
       }
+      // inactive lanes get keys of their own so they never extend a run
+      if (NEED_X) seg_scan3<TV>(u0, u1, u2, lane < t.cnt ? lp : 0x10000u + lane, lane);
       const uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
       const bool last = lane < t.cnt && (lane == t.cnt - 1 || lpn != lp);
       TV t0 = 0, t1 = 0, t2 = 0;
@@ -300,22 +309,17 @@ __global__ void __launch_bounds__(NW * 32, 1)
           t0 = (TV)w3[0];
           t1 = (TV)w3[1];
           t2 = (TV)w3[2];
+        } else if (MODE == FAST_RECOVER) {
+          const int64_t q = 3 * (t.p0 + lp);
+          const TV a0 = (TV)(-ex.wp[q] / ex.scales[q]) - u0, a1 = (TV)(-ex.wp[q + 1] / ex.scales[q + 1]) - u1;
+          const TV a2 = (TV)(-ex.wp[q + 2] / ex.scales[q + 2]) - u2;
+          ex.step[q] = (double)(c0 * a0 + c1 * a1 + c2 * a2) / ex.scales[q];
+          ex.step[q + 1] = (double)(c1 * a0 + c3 * a1 + c4 * a2) / ex.scales[q + 1];
+          ex.step[q + 2] = (double)(c2 * a0 + c4 * a1 + c5 * a2) / ex.scales[q + 2];
         } else {
-          const float4* pr = reinterpret_cast<const float4*>(slot + RING_EDGE_BYTES + (size_t)lp * 32);
-          const float4 ca = pr[0], cb = pr[1];
-          const TV c0 = ca.x, c1 = ca.y, c2 = ca.z, c3 = ca.w, c4 = cb.x, c5 = cb.y;
-          if (MODE == FAST_RECOVER) {
-            const int64_t q = 3 * (t.p0 + lp);
-            const TV a0 = (TV)(-ex.wp[q] / ex.scales[q]) - u0, a1 = (TV)(-ex.wp[q + 1] / ex.scales[q + 1]) - u1;
-            const TV a2 = (TV)(-ex.wp[q + 2] / ex.scales[q + 2]) - u2;
-            ex.step[q] = (double)(c0 * a0 + c1 * a1 + c2 * a2) / ex.scales[q];
-            ex.step[q + 1] = (double)(c1 * a0 + c3 * a1 + c4 * a2) / ex.scales[q + 1];
-            ex.step[q + 2] = (double)(c2 * a0 + c4 * a1 + c5 * a2) / ex.scales[q + 2];
-          } else {
-            t0 = c0 * u0 + c1 * u1 + c2 * u2;
-            t1 = c1 * u0 + c3 * u1 + c4 * u2;
-            t2 = c2 * u0 + c4 * u1 + c5 * u2;
-          }
+          t0 = c0 * u0 + c1 * u1 + c2 * u2;
+          t1 = c1 * u0 + c3 * u1 + c4 * u2;
+          t2 = c2 * u0 + c4 * u1 + c5 * u2;
         }
       }
       if (SCATTER) {
@@ -334,6 +338,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
       }
     } else {
       // ---------------------------------------------------- deep tile: one point
+      refill(k, b);  // its slot carries no data
       TV u0 = 0, u1 = 0, u2 = 0;
       if (NEED_X) {
         for (int c0 = 0; c0 < t.cnt; c0 += 32) {
@@ -399,19 +404,19 @@ __global__ void __launch_bounds__(NW * 32, 1)
         }
       }
     }
-    __syncwarp();
-    // refill this slot with the tile two ahead
-    const RingTile n = ring_bcast(nx);
-    if (b == 0) cur[0] = n; else cur[1] = n;
-    if (wn < tiles.nwt) issue(n, b);
+    if (((k + 1) & 31) == 0) {  // batch used up: the next becomes current, load the one after
+      ba = bb;
+      ++cbatch;
+      bb = ring_batch(tiles, first, G, nmine, 32 * (cbatch + 1), lane);
+    }
   }
   if (failed) {
     // drain: wait (bounded) for every copy this warp still has in flight
+    // (tiles k .. k+R-1: the slot refill happens only after a successful wait)
     if (lane == 0) atomicExch(error, 1);
-    for (int j = 0; j < RING_SLOTS; ++j) {
-      const int64_t kj = k + j;  // the slot of tile kj holds a copy when that tile exists
-      if (first + kj * G < tiles.nwt)
-        warp_wait(&wbar[kj & (RING_SLOTS - 1)], (unsigned)((kj / RING_SLOTS) & 1), RING_POLL_LIMIT);
+    for (int j = 0; j < R; ++j) {
+      const int64_t kj = k + j;
+      if (kj < nmine) warp_wait(&wbar[kj % R], (unsigned)((kj / R) & 1), RING_POLL_LIMIT);
     }
   }
   if (ACC != RACC_SHARED || !SCATTER) return;

@@ -94,11 +94,11 @@ def test_ring_lm_with_deep_points_reaches_oracle_cost():
 
 @pytest.mark.parametrize("lam", [1e-3, 1.0])
 def test_ring_global_accumulator_matches_oracle(lam):
-    """2,000 cameras: the operator's fixed-point camera sums and the rings no
-    longer fit one SM's shared memory (2 x 72 KB per 1,000 cameras + 110 KB of
-    rings), so the camera sums go to the global accumulator (FP32 vector
-    reductions into 8 copies, summed in FP64)."""
-    d = synthetic.generate("bal1k", cameras=2000, points=30000, seed=11)
+    """3,000 cameras: the operator's fixed-point camera sums (72 bytes per
+    camera) and the slots (74 KB) no longer fit one SM's shared memory, so the
+    camera sums go to the global accumulator (FP32 vector reductions into 8
+    copies, summed in FP64)."""
+    d = synthetic.generate("bal1k", cameras=3000, points=30000, seed=11)
     o = _oracle(d)
     b, _ = _device(d)
     assert b.operator_info()[0] == 1
@@ -112,7 +112,7 @@ def test_ring_global_accumulator_matches_oracle(lam):
 
 
 def test_ring_global_accumulator_steps_match_oracle():
-    d = synthetic.generate("bal1k", cameras=2000, points=30000, seed=11)
+    d = synthetic.generate("bal1k", cameras=3000, points=30000, seed=11)
     o = _oracle(d)
     _, ref, pred = o.solve_damped(1e-3)
     for coarse in (False, True):
