@@ -1192,9 +1192,12 @@ struct FastPath {
     if (std::is_same<TS, float>::value) {
       // the ring kernel takes any camera count: shared accumulator when the
       // operator's and the right-hand side's fit next to the rings, else global
-      const size_t need =
-          std::max(RingSmem<float, FAST_APPLY, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED, RING_SLOTS_SHARED),
-                   RingSmem<double, FAST_RHS, RACC_SHARED>::bytes(nc, false, RING_WARPS_SHARED, RING_SLOTS_SHARED));
+      const size_t need = std::max(
+          std::max(RingSmem<float, FAST_APPLY, RACC_SHARED>::bytes(nc, false, ring_warps_shared<float>(),
+                                                                   RING_SLOTS_SHARED),
+                   RingSmem<double, FAST_APPLY, RACC_SHARED>::bytes(nc, false, ring_warps_shared<double>(),
+                                                                    RING_SLOTS_SHARED)),
+          RingSmem<double, FAST_RHS, RACC_SHARED>::bytes(nc, false, ring_warps_shared<double>(), RING_SLOTS_SHARED));
       global_acc = need > (size_t)optin;
     } else {
       size_t need = std::max(FastSmem<TS, double>::bytes(nc, false), FastSmem<TS, TS>::bytes(nc, false));
@@ -1235,7 +1238,7 @@ struct FastPath {
     const float* er = reinterpret_cast<const float*>(d_erec.get());
     const float* pr = reinterpret_cast<const float*>(d_prec.get());
     if (!global_acc) {
-      constexpr int NW = RING_WARPS_SHARED, R = RING_SLOTS_SHARED;
+      constexpr int NW = ring_warps_shared<TV>(), R = RING_SLOTS_SHARED;
       const bool xs = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, true, NW, R) <= (size_t)optin;
       const size_t sm = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, xs, NW, R);
       auto kern = xs ? k_ring<TV, MODE, RACC_SHARED, true, NW, R> : k_ring<TV, MODE, RACC_SHARED, false, NW, R>;

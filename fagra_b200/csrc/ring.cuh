@@ -37,7 +37,12 @@ namespace fg {
 
 constexpr int RING_EDGE_BYTES = 32 * 28 * 4;                 // edge records of one warp tile
 constexpr int RING_SLOT_BYTES = RING_EDGE_BYTES + 32 * 8 * 4;  // + its point records
-constexpr int RING_WARPS_SHARED = 16;  // with one slot per warp (shared accumulator)
+// Shared accumulator: one slot per warp; 20 warps for FP32 vectors (96
+// registers a thread), 16 for FP64 vectors, which need more registers.
+template <class TV>
+constexpr int ring_warps_shared() {
+  return std::is_same<TV, float>::value ? 20 : 16;
+}
 constexpr int RING_SLOTS_SHARED = 1;
 constexpr int RING_WARPS_GLOBAL = 16;  // with two slots per warp (global accumulator)
 constexpr int RING_SLOTS_GLOBAL = 2;
