@@ -223,6 +223,8 @@ SIGNATURES = {
     "fg_schur_time_operator_kernel": (C.c_int, [C.c_void_p, C.c_double, size_t, dptr, dptr]),
     "fg_schur_operator_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), dptr]),
     "fg_schur_set_poll_limit": (C.c_int, [C.c_void_p, C.c_uint]),
+    "fg_schur_accumulate_pairs_device": (C.c_int, [C.c_void_p, size_t, size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                   C.c_void_p, C.c_void_p]),
     "fg_gn_solve_bal": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(OptimizeOptionsC), C.POINTER(ReportC)]),
     "fg_lm_optimize": (C.c_int, [C.c_void_p, C.POINTER(ProblemCallbacksC), C.c_void_p, dptr,
                                  C.POINTER(OptimizeOptionsC), C.POINTER(LmOptionsC), C.POINTER(ReportC),

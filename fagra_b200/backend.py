@@ -127,6 +127,14 @@ class Schur:
     learned_policy = property(lambda s: ("compare", "always")[s._get("learned_policy")],
                               lambda s, v: s._set("learned_policy", {"compare": 0, "always": 1}[v]))
 
+    def accumulate_pairs_device(self, count: int, rows: int, retained_variable: int, eliminated_variable: int,
+                                residual: int, retained_jacobian: int, eliminated_jacobian: int) -> None:
+        """A device batch of `count` bipartite emissions (device pointers,
+        SoA layout of fg_schur_accumulate_pairs_device)."""
+        raise_for_status(lib.fg_schur_accumulate_pairs_device(
+            self._h, count, rows, C.c_void_p(retained_variable), C.c_void_p(eliminated_variable),
+            C.c_void_p(residual), C.c_void_p(retained_jacobian), C.c_void_p(eliminated_jacobian)))
+
     def set_poll_limit(self, polls: int) -> None:
         """Test hook: polls after which the ring operator's slot wait gives up
         (the solve then raises DeviceTimeout); 0 restores the default."""

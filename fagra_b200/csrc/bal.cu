@@ -473,6 +473,15 @@ fg_status BalProblem::stage(const double* d_delta) {
   return FG_OK;
 }
 
+fg_status BalProblem::stage_and_cost_device(const double* d_delta) {
+  FG_TRY(stage(d_delta));
+  if (nc) FG_LAUNCH(k_bal_camera_prep, grid_for(nc, 128), 128, 0, st, (int64_t)nc, tcams.get(), tprep.get());
+  unsigned g = std::min<unsigned>(grid_for(std::max<size_t>(no, 1), 256), 4 * nsm);
+  FG_LAUNCH(k_bal_cost, g, 256, 0, st, (int64_t)no, oc.get(), op.get(), px.get(), tcams.get(), tpts.get(),
+            tprep.get(), partials.get(), counters.get(), result.get());
+  return FG_OK;
+}
+
 void BalProblem::accept() {
   if (trial_active) {
     std::swap(cams.ptr, tcams.ptr);

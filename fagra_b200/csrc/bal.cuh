@@ -54,6 +54,9 @@ struct BalProblem {
   DBuf<double> px, cams, pts, tcams, tpts, prep, tprep, partials, result, init_cams, init_pts, gauge;
   DBuf<unsigned> counters;
   DBuf<int> d_flag;
+  // device LM trials: the trial state (lm.cuh LmTrialState) and the step norm
+  DBuf<double> lm_state;
+  HBuf<double> h_lm_state;
   HBuf<double> h_result;
   HBuf<int> h_flag;
   bool trial_active = false;
@@ -66,6 +69,8 @@ struct BalProblem {
   fg_status linearize(Backend* b);
   fg_status host_observations(const uint32_t** cam, const uint32_t** pt);
   fg_status stage(const double* d_delta);
+  // stage + trial cost enqueued without a sync; [cost, invalid] at result
+  fg_status stage_and_cost_device(const double* d_delta);
   void accept();
   void reject();
   fg_status restore_initial();

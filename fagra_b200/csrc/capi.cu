@@ -379,6 +379,16 @@ FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* sec
   b->impl->operator_info(variant, seconds4);
   return FG_OK;
 }
+FG_API fg_status fg_schur_accumulate_pairs_device(fg_backend* b, size_t count, size_t rows,
+                                                  const uint32_t* retained_variable,
+                                                  const uint32_t* eliminated_variable, const double* residual,
+                                                  const double* retained_jacobian,
+                                                  const double* eliminated_jacobian) {
+  FG_NEED(b);
+  FG_GUARD_BEGIN return b->impl->accumulate_pairs(count, rows, retained_variable, eliminated_variable, residual,
+                                                  retained_jacobian, eliminated_jacobian);
+  FG_GUARD_END
+}
 FG_API fg_status fg_schur_set_poll_limit(fg_backend* b, unsigned polls) {
   FG_NEED(b);
   FG_GUARD_BEGIN return b->impl->set_poll_limit(polls);

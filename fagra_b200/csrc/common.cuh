@@ -89,6 +89,35 @@ struct DBuf {
     n = count;
     return FG_OK;
   }
+  // Grow to `count` elements keeping the first `keep` (device copy on `s`).
+  fg_status grow_keep(size_t count, size_t keep, cudaStream_t s) {
+    if (count <= cap) {
+      n = count;
+      return FG_OK;
+    }
+    T* old = ptr;
+    const size_t oldcap = cap;
+    ptr = nullptr;
+    cap = 0;
+    fg_status st = resize(count);
+    if (st != FG_OK) {
+      ptr = old;
+      cap = oldcap;
+      return st;
+    }
+    if (old && keep) {
+      cudaError_t e = cudaMemcpyAsync(ptr, old, keep * sizeof(T), cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return cuda_status(e, "grow_keep copy");
+    }
+    if (old) {
+      if (pool_stream) cudaFreeAsync(old, pool_stream);
+      else {
+        cudaStreamSynchronize(s);
+        cudaFree(old);
+      }
+    }
+    return FG_OK;
+  }
   T* get() const { return ptr; }
   size_t size() const { return n; }
   size_t bytes() const { return n * sizeof(T); }

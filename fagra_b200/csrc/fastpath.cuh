@@ -946,15 +946,20 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
           for (int p = 0; p < 3; ++p) u[3 + a][p] += E[p * 9 + c] * x[a];
       }
     }
+    // segmented sums over each point's lanes; inactive lanes get keys of
+    // their own, and the scan stops once no run is longer than the offset
+    const uint32_t key = lane < cnt ? lp : 0x10000u + lane;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t lo = __shfl_up_sync(0xffffffffu, lp, off);
+      const uint32_t lo = __shfl_up_sync(0xffffffffu, key, off);
+      const bool take = lane >= off && lo == key;
+      if (!__any_sync(0xffffffffu, take)) break;
 #pragma unroll
       for (int a = 0; a < NK; ++a)
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
           const float v = __shfl_up_sync(0xffffffffu, u[a][p], off);
-          if (lane >= off && lo == lp) u[a][p] += v;
+          if (take) u[a][p] += v;
         }
     }
     const uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);

@@ -39,7 +39,61 @@ struct BalAdapter : ProblemAdapter {
   fg_status stage(const double* delta) override { return p->stage(delta); }
   void accept() override { p->accept(); }
   void reject() override { p->reject(); }
+  bool device_trials() const override { return true; }
+  fg_status stage_and_cost_device(const double* d_delta, const double** result) override {
+    FG_TRY(p->stage_and_cost_device(d_delta));
+    *result = p->result.get();
+    return FG_OK;
+  }
 };
+
+// The decision of one LM trial on the device, statement for statement as the
+// host loop below (levenberg_marquardt.rs:406-467): gain ratio clamped at 2,
+// acceptance, stagnation, Nielsen's damping update, or the growth after a
+// rejection. Products are rounded one at a time (no fused multiply-add), so
+// the damping sequence is the host loop's bit for bit.
+__global__ void k_lm_decide(LmTrialState* s, const double* norm, const double* result, fg_lm_options lo,
+                            double step_tolerance, double cost_tolerance, int undamped) {
+  LmTrialState t = *s;
+  t.norm = norm[0];
+  t.norm_bad = norm[1] != 0 || !isfinite(norm[0]);
+  t.accepted = t.rejection = t.stalled = t.stop = 0;
+  if (t.norm_bad) {
+    *s = t;
+    return;
+  }
+  if (!isfinite(t.predicted) || t.predicted <= 0) {
+    t.rejection = 2;
+  } else {
+    t.value = result[0];
+    if (result[1] != 0 || !isfinite(t.value) || t.value < 0) {  // checked_cost
+      t.rejection = 3;
+    } else {
+      t.actual = __dsub_rn(t.current, t.value);
+      t.ratio = fmin(__ddiv_rn(t.actual, t.predicted), 2.0);
+      if (t.actual > 0 && t.ratio >= lo.acceptance_threshold) {
+        t.accepted = 1;
+        t.stalled = step_tolerance > 0 && t.norm <= step_tolerance &&
+                    (cost_tolerance == 0 || __ddiv_rn(t.actual, fmax(t.current, 1.0)) <= cost_tolerance);
+        const double c = __dsub_rn(__dmul_rn(2.0, fmin(t.ratio, 1.0)), 1.0);
+        const double update = fmax(__dsub_rn(1.0, __dmul_rn(__dmul_rn(c, c), c)), 1.0 / 3.0);
+        t.lambda = fmin(fmax(__dmul_rn(t.lambda, update), lo.min_damping), lo.max_damping);
+        t.current = t.value;
+      } else {
+        t.rejection = 4;
+      }
+    }
+  }
+  if (!t.accepted) {
+    if (undamped || t.lambda == lo.max_damping) {
+      t.stop = 1;
+    } else {
+      t.lambda = fmin(__dmul_rn(t.lambda, t.growth), lo.max_damping);
+      t.growth = fmin(__dmul_rn(t.growth, 2.0), fmax(lo.max_damping, 2.0));
+    }
+  }
+  *s = t;
+}
 
 // Host callback adapter: additive coordinates owned by the caller.
 struct CallbackAdapter : ProblemAdapter {
@@ -119,6 +173,19 @@ fg_status lm_optimize(Backend* b, ProblemAdapter& pb, const fg_optimize_options&
     return s;
   };
   const bool dev = pb.device_steps();
+  // device trials: a device problem and a backend that reduces its step norm
+  // on the device; the state lives in the problem's buffers
+  constexpr size_t LMW = (sizeof(LmTrialState) + sizeof(double) - 1) / sizeof(double);
+  double* d_lm = nullptr;
+  LmTrialState* h_lm = nullptr;
+  BalProblem* bp = nullptr;
+  if (pb.device_trials()) {
+    bp = static_cast<BalAdapter&>(pb).p;
+    FG_TRY(bp->lm_state.resize(LMW + 2));
+    FG_TRY(bp->h_lm_state.resize(LMW));
+    d_lm = bp->lm_state.get();
+    h_lm = reinterpret_cast<LmTrialState*>(bp->h_lm_state.get());
+  }
   for (;;) {
     if (pb.dimension() == 0) return finish(1);
     st->linearizations += 1;
@@ -143,10 +210,58 @@ fg_status lm_optimize(Backend* b, ProblemAdapter& pb, const fg_optimize_options&
       double predicted = 0;
       int rejection = 0;
       fg_status r = b->solve_damped(damping, &predicted, !dev);
+      fg_status na = FG_UNSUPPORTED_STRUCTURE;
+      if (r == FG_OK && d_lm) na = b->step_norm_async(d_lm + LMW);
       if (r == FG_LINEAR_SOLVE_FAILED) {
         rejection = 1;
       } else if (r) {
         return fail(r);
+      } else if (na == FG_OK) {
+        // the whole trial on the device, one read back
+        LmTrialState in{};
+        in.current = current;
+        in.lambda = lambda;
+        in.growth = growth;
+        in.predicted = predicted;
+        *h_lm = in;
+        const bool costed = std::isfinite(predicted) && predicted > 0;
+        FG_CUDA(cudaMemcpyAsync(d_lm, h_lm, sizeof(LmTrialState), cudaMemcpyHostToDevice, bp->st));
+        const double* d_result = nullptr;
+        if (costed) {
+          if ((s = pb.stage_and_cost_device(b->step_device(), &d_result))) return fail(s);
+        } else {
+          d_result = bp->result.get();  // not read: the decision rejects on the prediction
+        }
+        FG_LAUNCH(k_lm_decide, 1, 1, 0, bp->st, reinterpret_cast<LmTrialState*>(d_lm), d_lm + LMW, d_result, lo,
+                  opt.step_tolerance, opt.cost_tolerance, (int)undamped);
+        FG_CUDA(cudaMemcpyAsync(h_lm, d_lm, sizeof(LmTrialState), cudaMemcpyDeviceToHost, bp->st));
+        FG_CUDA(cudaStreamSynchronize(bp->st));
+        const LmTrialState& o = *h_lm;
+        if (o.norm_bad) return fail(FG_LINEAR_SOLVE_FAILED);
+        st->step_norm = o.norm;
+        st->has_step_norm = 1;
+        if (costed) st->cost_evaluations += 1;
+        if (o.accepted) {
+          pb.accept();
+          st->accepted_steps += 1;
+          st->cost = o.value;
+          st->has_cost = 1;
+          stalled = o.stalled != 0;
+          current = o.current;
+          lambda = o.lambda;
+          accepted = true;
+          record_work(b, st);
+          if (on_accept) on_accept(user, st);
+          if (o.value <= target_cost) return finish(5);
+          break;
+        }
+        if (costed) pb.reject();
+        st->rejected_steps += 1;
+        st->last_rejection = o.rejection;
+        if (o.stop) break;
+        lambda = o.lambda;
+        growth = o.growth;
+        continue;
       } else {
         double norm;
         if (b->step_norm_inf(&norm) != FG_OK) return fail(FG_LINEAR_SOLVE_FAILED);

@@ -18,6 +18,22 @@ struct ProblemAdapter {
   virtual fg_status stage(const double* delta) = 0;
   virtual void accept() = 0;
   virtual void reject() = 0;
+  // Device trials: stage the device step and evaluate the trial cost without
+  // a host round trip, leaving [cost, invalid flag] at *result (device).
+  virtual bool device_trials() const { return false; }
+  virtual fg_status stage_and_cost_device(const double*, const double** result) {
+    *result = nullptr;
+    return FG_UNSUPPORTED_STRUCTURE;
+  }
+};
+
+// One LM trial decided on the device (levenberg_marquardt.rs:388-467): the
+// step's infinity norm, the trial cost, the gain ratio, acceptance, the
+// stagnation test and the damping update, read back by the host in one copy.
+struct LmTrialState {
+  double current, lambda, growth, predicted;  // in (predicted from the backend's verification)
+  double norm, value, actual, ratio;          // step norm, trial cost
+  int norm_bad, accepted, rejection, stalled, stop;
 };
 
 fg_status lm_optimize(Backend* b, ProblemAdapter& pb, const fg_optimize_options& opt, const fg_lm_options& lo,

@@ -70,7 +70,16 @@ class SchurImpl final : public Backend {
   bool cross_current = false;  // d_cross holds this linearization's cross blocks
 
   // ---- model source
-  enum Source { NONE, HOST, DEVICE_BAL } source = NONE;
+  enum Source { NONE, HOST, DEVICE_BAL, DEVICE_PAIRS } source = NONE;
+  // device pair batches (accumulate_pairs): emissions so far, their rows and
+  // values, per-emission variables / first row / first value / rows, and the
+  // variables and rows of the structure built last (to reuse it)
+  size_t dp_em = 0, dp_rows = 0, dp_vals = 0, dp_built = 0;
+  DBuf<uint32_t> d_em_cam, d_em_pt, d_em_prev;
+  DBuf<int64_t> d_em_row, d_em_val;
+  DBuf<int32_t> d_em_rows;
+  DBuf<int> d_dp_flags;
+  HBuf<int> h_dp_flags;
   bool device_model_current = false;  // device values/negres are current
   bool gradient_current = false;
   uint64_t bal_bound = 0;             // id of the BAL structure currently bound
@@ -232,8 +241,132 @@ class SchurImpl final : public Backend {
     h_edges.clear();
     h_rows = 0;
     source = HOST;
+    dp_em = dp_rows = dp_vals = 0;
     device_model_current = false;
     gradient_current = false;
+    return FG_OK;
+  }
+
+  // A device batch of bipartite emissions (k_pairs_pack), appended after the
+  // batches since the last clear; emission order = batch order, then k.
+  fg_status accumulate_pairs(size_t count, size_t prow, const uint32_t* cam, const uint32_t* pt, const double* r,
+                             const double* jr, const double* je) override {
+    ready = false;
+    if (source != DEVICE_PAIRS) {
+      FG_TRY(clear());
+      source = DEVICE_PAIRS;
+    }
+    if (count == 0) return FG_OK;
+    if (!cam || !pt || !r || !jr || !je) return FG_NULL_ARGUMENT;
+    if (prow == 0 || prow > (size_t)MAXW) {
+      set_error("device emission batches take 1..16 rows per emission");
+      return FG_DIMENSION_MISMATCH;
+    }
+    if (nC == 0 || nP == 0) {
+      set_error("device emission batches need retained and eliminated variables");
+      return FG_UNSUPPORTED_STRUCTURE;
+    }
+    FG_TRY(select_device(dev));
+    const size_t em = dp_em + count, nr = dp_rows + count * prow, nv = dp_vals + count * prow * (cw + pw);
+    FG_TRY(d_em_cam.grow_keep(em, dp_em, st));
+    FG_TRY(d_em_pt.grow_keep(em, dp_em, st));
+    FG_TRY(d_em_row.grow_keep(em, dp_em, st));
+    FG_TRY(d_em_val.grow_keep(em, dp_em, st));
+    FG_TRY(d_em_rows.grow_keep(em, dp_em, st));
+    FG_TRY(d_negres.grow_keep(nr, dp_rows, st));
+    FG_TRY(d_values.grow_keep(nv, dp_vals, st));
+    FG_TRY(d_dp_flags.resize(2));
+    FG_TRY(h_dp_flags.resize(2));
+    FG_CUDA(cudaMemsetAsync(d_dp_flags.get(), 0, 2 * sizeof(int), st));
+    FG_LAUNCH(k_pairs_pack<TS>, grid_for(count, 128), 128, 0, st, (int64_t)count, (int)prow, (int)cw, (int)pw,
+              (int64_t)nC, (int64_t)nP, cam, pt, r, jr, je, (int64_t)dp_em, (int64_t)dp_rows, (int64_t)dp_vals,
+              d_em_cam.get(), d_em_pt.get(), d_em_row.get(), d_em_val.get(), d_em_rows.get(), d_negres.get(),
+              d_values.get(), d_dp_flags.get());
+    FG_CUDA(cudaMemcpyAsync(h_dp_flags.get(), d_dp_flags.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (h_dp_flags.get()[0]) {  // src/optimization.rs:575-584: a variable outside the layout
+      set_error("device emission batch: a variable index outside the layout");
+      return FG_INVALID_EMISSION;
+    }
+    if (h_dp_flags.get()[1]) {  // src/optimization.rs:556-558, 596-598
+      set_error("device emission batch: nonfinite residual or Jacobian");
+      return FG_INVALID_EVALUATION;
+    }
+    dp_em = em;
+    dp_rows = nr;
+    dp_vals = nv;
+    device_model_current = false;
+    gradient_current = false;
+    return FG_OK;
+  }
+
+  // The maps build_structure derives, for the device pair emissions: as
+  // build_structure_bal with the emissions' own rows, widths and starts.
+  fg_status build_structure_pairs() {
+    const size_t obs = dp_em;
+    rows = dp_rows;
+    nblocks = 2 * obs;
+    nedges = obs;
+    const size_t nvar = nC + nP;
+    if (nC >= ((size_t)1 << 31) || nP >= ((size_t)1 << 31)) return FG_UNSUPPORTED_STRUCTURE;
+    FG_TRY(d_bal_stage.resize(std::max<size_t>(4 * obs, 1)));  // cam_order | pt_order | sorted cams | sorted points
+    uint32_t* stage = d_bal_stage.get();
+    FG_TRY(d_cam_edge_off.resize(nC + 1));
+    FG_TRY(d_pt_edge_off.resize(nP + 1));
+    FG_TRY(d_var_off.resize(nvar + 1));
+    FG_TRY(d_observed.resize(std::max<size_t>(nvar, 1)));
+    FG_TRY(stable_order(d_em_cam.get(), obs, (uint32_t)nC, stage, stage + 2 * obs, sort_scratch, st));
+    FG_TRY(key_offsets(stage + 2 * obs, obs, (uint32_t)nC, d_cam_edge_off.get(), st));
+    FG_TRY(stable_order(d_em_pt.get(), obs, (uint32_t)nP, stage + obs, stage + 3 * obs, sort_scratch, st));
+    FG_TRY(key_offsets(stage + 3 * obs, obs, (uint32_t)nP, d_pt_edge_off.get(), st));
+    FG_TRY(d_blocks.resize(std::max<size_t>(nblocks, 1)));
+    FG_TRY(d_edges.resize(std::max<size_t>(nedges, 1)));
+    FG_TRY(d_var_blk.resize(std::max<size_t>(nblocks, 1)));
+    FG_TRY(d_cam_edge.resize(std::max<size_t>(nedges, 1)));
+    FG_TRY(d_pt_edge.resize(std::max<size_t>(nedges, 1)));
+    FG_TRY(d_emi_off.resize(obs + 1));
+    FG_LAUNCH(k_pairs_structure, grid_for(obs + 1, 256), 256, 0, st, (int64_t)obs, (int64_t)retained, (int)cw,
+              (int)pw, d_em_cam.get(), d_em_pt.get(), d_em_row.get(), d_em_val.get(), d_em_rows.get(), stage,
+              stage + obs, d_blocks.get(), d_edges.get(), d_var_blk.get(), d_cam_edge.get(), d_pt_edge.get(),
+              d_emi_off.get());
+    FG_LAUNCH(k_bal_var_offsets, grid_for(nvar + 1, 256), 256, 0, st, (int64_t)nC, (int64_t)nP, (int64_t)obs,
+              d_cam_edge_off.get(), d_pt_edge_off.get(), d_var_off.get(), d_observed.get());
+    h_observed.resize(nvar);
+    if (nvar) FG_CUDA(cudaMemcpyAsync(h_observed.data(), d_observed.get(), nvar, cudaMemcpyDeviceToHost, st));
+    nemissions = obs;
+    pure_pairs = obs > 0;
+    FG_TRY(d_cross.resize(std::max<size_t>(nedges * cw * pw, 1)));
+    FG_TRY(d_jd.resize(std::max<size_t>(rows, 1)));
+    // remember what this structure was built from (cameras | points | rows)
+    FG_TRY(d_em_prev.resize(std::max<size_t>(3 * obs, 1)));
+    if (obs) {
+      FG_CUDA(cudaMemcpyAsync(d_em_prev.get(), d_em_cam.get(), obs * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+      FG_CUDA(cudaMemcpyAsync(d_em_prev.get() + obs, d_em_pt.get(), obs * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                              st));
+      FG_CUDA(cudaMemcpyAsync(d_em_prev.get() + 2 * obs, d_em_rows.get(), obs * sizeof(uint32_t),
+                              cudaMemcpyDeviceToDevice, st));
+    }
+    dp_built = obs;
+    FG_CUDA(cudaStreamSynchronize(st));
+    structure_valid = true;
+    fast.invalidate();
+    drop_graphs();
+    return FG_OK;
+  }
+
+  // Whether the pair emissions are the ones the current structure was built
+  // from (same variables and rows in the same order).
+  fg_status same_pairs(bool* same) {
+    *same = false;
+    if (!structure_valid || bal_bound || !up_blocks.empty() || dp_built != dp_em || dp_em == 0) return FG_OK;
+    FG_TRY(d_dp_flags.resize(2));
+    FG_TRY(h_dp_flags.resize(2));
+    FG_CUDA(cudaMemsetAsync(d_dp_flags.get(), 0, sizeof(int), st));
+    FG_LAUNCH(k_pairs_differ, grid_for(dp_em, 256), 256, 0, st, (int64_t)dp_em, d_em_cam.get(), d_em_pt.get(),
+              (const uint32_t*)d_em_rows.get(), d_em_prev.get(), d_dp_flags.get());
+    FG_CUDA(cudaMemcpyAsync(h_dp_flags.get(), d_dp_flags.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    *same = h_dp_flags.get()[0] == 0;
     return FG_OK;
   }
 
@@ -275,6 +408,7 @@ class SchurImpl final : public Backend {
 
   // Build and upload index maps for a structure (host integer bookkeeping).
   fg_status build_structure(const std::vector<HostBlock>& blocks, const std::vector<HostEdge>& edges, size_t nrows) {
+    dp_built = 0;
     rows = nrows;
     nblocks = blocks.size();
     nedges = edges.size();
@@ -344,6 +478,7 @@ class SchurImpl final : public Backend {
   // the device: stable orders of the emissions by camera and by point (radix
   // sorts), their offsets, then every map in one pass over the emissions.
   fg_status build_structure_bal(size_t cams, size_t pts, size_t obs, const uint32_t* ocam, const uint32_t* opt) {
+    dp_built = 0;
     rows = 2 * obs;
     nblocks = 2 * obs;
     nedges = obs;
@@ -426,6 +561,20 @@ class SchurImpl final : public Backend {
       FG_TRY(upload(d_negres, h_negres.data(), h_negres.size(), st));
       if (d_negres.cap == 0) FG_TRY(d_negres.resize(1));
       FG_CUDA(cudaStreamSynchronize(st));
+      device_model_current = true;
+      gradient_current = false;
+    }
+    if (source == DEVICE_PAIRS && !device_model_current) {
+      bool same = false;
+      FG_TRY(same_pairs(&same));
+      if (!same) {
+        bal_bound = 0;
+        up_blocks.clear();
+        up_edges.clear();
+        FG_TRY(build_structure_pairs());
+      }
+      nvalues = dp_vals;
+      rows = dp_rows;
       device_model_current = true;
       gradient_current = false;
     }
@@ -1089,7 +1238,10 @@ class SchurImpl final : public Backend {
     if (compare) tc.start(st);
     FG_TRY(run_cg(lambda, &its, &term, &est, &refinements));
     if (compare) diag.learned_seconds = learned_infer_seconds + tc.stop(st);
-    diag.preconditioner_used = use_learned ? FG_PRECOND_LEARNED : opt.preconditioner;
+    // a learned preconditioner the comparison switched off runs block-Jacobi
+    diag.preconditioner_used = use_learned ? FG_PRECOND_LEARNED
+                               : opt.preconditioner == FG_PRECOND_LEARNED ? FG_PRECOND_RETAINED_BLOCKS
+                                                                          : opt.preconditioner;
     if (use_learned) {
       // Block-Jacobi stays the yardstick: it takes over when the learned PCG
       // fails, and the first learned solve is compared against it once, on
@@ -1264,6 +1416,16 @@ class SchurImpl final : public Backend {
 
   // ------------------------------------------------------------- accessors
   fg_status step_norm_inf(double* out) override { return device_norm_inf(d_step.get(), dim, out); }
+  fg_status step_norm_async(double* d_out) override {
+    if (dim == 0) {
+      FG_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(double), st));
+      return FG_OK;
+    }
+    unsigned g = std::min<unsigned>(grid_for(dim, NT), 4 * nsm);
+    FG_LAUNCH(k_norm_inf<double>, g, NT, 0, st, (int64_t)dim, (const double*)d_step.get(), d_partials.get(),
+              d_counters.get() + 3, d_out);
+    return FG_OK;
+  }
   const double* step_host() const override { return h_step.get(); }
   const double* step_device() const override { return d_step.get(); }
   size_t dimension() const override { return dim; }

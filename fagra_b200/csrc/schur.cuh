@@ -85,6 +85,9 @@ class Backend {
     return solve_damped(0.0, &p, copy_to_host);
   }
   virtual fg_status step_norm_inf(double* out) = 0;
+  // max |step| and a nonfinite flag written to d_out[0..1] on the device,
+  // without a host synchronization (backends that cannot return unsupported)
+  virtual fg_status step_norm_async(double* /*d_out*/) { return FG_UNSUPPORTED_STRUCTURE; }
   virtual const double* step_host() const = 0;
   virtual const double* step_device() const = 0;
   virtual size_t dimension() const = 0;
@@ -126,6 +129,10 @@ class Backend {
     if (seconds4) seconds4[0] = seconds4[1] = seconds4[2] = seconds4[3] = 0;
   }
   virtual fg_status set_poll_limit(unsigned) { return not_schur(); }
+  virtual fg_status accumulate_pairs(size_t, size_t, const uint32_t*, const uint32_t*, const double*, const double*,
+                                     const double*) {
+    return not_schur();
+  }
   // LSMR-only extras.
   virtual fg_status set_lsmr_options(const fg_lsmr_options&) { return not_lsmr(); }
   virtual void lsmr_diagnostics(fg_lsmr_diagnostics* d) const { *d = fg_lsmr_diagnostics{}; }

@@ -573,6 +573,90 @@ __global__ void k_bal_structure(int64_t obs, int64_t ncam, const uint32_t* ocam,
   pt_edge[k] = ep;
 }
 
+// Device batches of bipartite emissions (fg_schur_accumulate_pairs_device):
+// emission e = e0 + k of a batch of `count` emissions with `rows` rows each
+// has one retained block (variable cam[k], width cw) and one eliminated block
+// (variable pt[k], width pw). Inputs are SoA so that consecutive threads read
+// consecutive words: residual[i * count + k], retained Jacobian element (i, j)
+// at jr[(j * rows + i) * count + k], eliminated at je[(j * rows + i) * count + k].
+// The pass packs the reference's layout (src/linear_model.rs:180-210: -r per
+// row, each block column-major, retained block first) and checks what
+// CheckedSink checks (src/optimization.rs:541-612): a variable outside the
+// layout is an invalid emission (flags[0]), a nonfinite value an invalid
+// evaluation (flags[1]).
+template <class TS>
+__global__ void k_pairs_pack(int64_t count, int rows, int cw, int pw, int64_t ncam, int64_t npt, const uint32_t* cam,
+                             const uint32_t* pt, const double* r, const double* jr, const double* je, int64_t e0,
+                             int64_t row0, int64_t v0, uint32_t* em_cam, uint32_t* em_pt, int64_t* em_row,
+                             int64_t* em_val, int32_t* em_rows, double* negres, TS* values, int* flags) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t c = cam[k], p = pt[k];
+  if ((int64_t)c >= ncam || (int64_t)p >= npt) atomicExch(&flags[0], 1);
+  const int64_t row = row0 + k * rows, v = v0 + k * (int64_t)rows * (cw + pw);
+  bool bad = false;
+  for (int i = 0; i < rows; ++i) {
+    const double x = r[(int64_t)i * count + k];
+    bad |= !isfinite(x);
+    negres[row + i] = -x;
+  }
+  for (int j = 0; j < cw; ++j)
+    for (int i = 0; i < rows; ++i) {
+      const double x = jr[((int64_t)j * rows + i) * count + k];
+      bad |= !isfinite(x);
+      values[v + (int64_t)j * rows + i] = (TS)x;
+    }
+  const int64_t vp = v + (int64_t)rows * cw;
+  for (int j = 0; j < pw; ++j)
+    for (int i = 0; i < rows; ++i) {
+      const double x = je[((int64_t)j * rows + i) * count + k];
+      bad |= !isfinite(x);
+      values[vp + (int64_t)j * rows + i] = (TS)x;
+    }
+  if (bad) atomicExch(&flags[1], 1);
+  em_cam[e0 + k] = c;
+  em_pt[e0 + k] = p;
+  em_row[e0 + k] = row;
+  em_val[e0 + k] = v;
+  em_rows[e0 + k] = rows;
+}
+
+// Index maps of the device pair emissions (as k_bal_structure, any widths and
+// rows): block 2e = retained, 2e + 1 = eliminated, edge e, variables listing
+// their blocks in emission order (from the stable orders by camera and point).
+__global__ void k_pairs_structure(int64_t obs, int64_t retained, int cw, int pw, const uint32_t* ocam,
+                                  const uint32_t* opt, const int64_t* em_row, const int64_t* em_val,
+                                  const int32_t* em_rows, const uint32_t* cam_order, const uint32_t* pt_order,
+                                  DBlockMeta* blocks, DEdgeMeta* edges, int64_t* var_blk, int64_t* cam_edge,
+                                  int64_t* pt_edge, int64_t* emi_off) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k > obs) return;
+  if (k == obs) {
+    emi_off[obs] = 2 * obs;
+    return;
+  }
+  const int64_t c = ocam[k], p = opt[k], row = em_row[k], v = em_val[k];
+  const int32_t rows = em_rows[k];
+  blocks[2 * k] = DBlockMeta{row, v, cw * c, rows, cw};
+  blocks[2 * k + 1] = DBlockMeta{row, v + (int64_t)rows * cw, retained + pw * p, rows, pw};
+  edges[k] = DEdgeMeta{(int32_t)c, (int32_t)p, 2 * k, 2 * k + 1};
+  emi_off[k] = 2 * k;
+  const int64_t ec = cam_order[k], ep = pt_order[k];
+  var_blk[k] = 2 * ec;
+  var_blk[obs + k] = 2 * ep + 1;
+  cam_edge[k] = ec;
+  pt_edge[k] = ep;
+}
+
+// flag = 1 if the emissions' cameras, points or rows differ from `prev`
+// (cameras | points | rows, each n long).
+__global__ void k_pairs_differ(int64_t n, const uint32_t* cam, const uint32_t* pt, const uint32_t* rows,
+                               const uint32_t* prev, int* flag) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  if (cam[k] != prev[k] || pt[k] != prev[n + k] || rows[k] != prev[2 * n + k]) *flag = 1;
+}
+
 // Variable offsets of the BAL structure (cameras, then points; every variable
 // lists its emissions) and which variables any emission touches.
 __global__ void k_bal_var_offsets(int64_t ncam, int64_t npt, int64_t obs, const int64_t* cam_off,

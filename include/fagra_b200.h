@@ -302,6 +302,30 @@ FG_API fg_status fg_bal_cost_noalloc(size_t cameras, size_t points, size_t obser
                                      const double* camera_params, const double* point_params,
                                      const uint32_t* obs_camera, const uint32_t* obs_point,
                                      const double* obs_pixel, double* out, int device, void* stream);
+/* A homogeneous batch of factor emissions straight from device memory, for
+ * factor families other than BAL (src/optimization.rs:541-612 CheckedSink +
+ * src/linear_model.rs:180-210 LinearizedModel::accumulate + src/schur.rs:438-482
+ * Schur::accumulate, for `count` emissions at once instead of one host call
+ * each). Every emission has `rows` rows (1..16), one retained block (the
+ * retained variable retained_variable[k], width = the backend's retained block
+ * width) and one eliminated block (eliminated_variable[k], the eliminated
+ * width); variables are numbered within their partition (coordinate offset =
+ * index x width, eliminated ones after the retained dimension). Device arrays,
+ * SoA: residual[i * count + k]; block element (i, j) of emission k at
+ * retained_jacobian[(j * rows + i) * count + k] and
+ * eliminated_jacobian[(j * rows + i) * count + k]. Batches after the last
+ * fg_backend_clear (or prepare) append in call order; they cannot be mixed
+ * with fg_backend_accumulate in one linearization. The packed values, index
+ * maps (blocks, edges, variables) and emission order equal those of the same
+ * emissions passed to fg_backend_accumulate one by one. Errors:
+ * FG_INVALID_EMISSION for a variable outside the layout, FG_INVALID_EVALUATION
+ * for a nonfinite value, FG_DIMENSION_MISMATCH for rows outside 1..16; the
+ * failing batch is dropped. Schur backends only. */
+FG_API fg_status fg_schur_accumulate_pairs_device(fg_backend* backend, size_t count, size_t rows,
+                                                  const uint32_t* retained_variable,
+                                                  const uint32_t* eliminated_variable, const double* residual,
+                                                  const double* retained_jacobian,
+                                                  const double* eliminated_jacobian);
 /* Workspace::linearize for BAL frames (src/optimization.rs:229-265 +
  * examples/bal/model.rs:214-236): residuals and Jacobians straight into the
  * backend's block storage, in emission order. */

@@ -188,3 +188,30 @@ def test_operator_kernel_timing_entry_point():
     o, n_p, n_c = d.num_observations, d.num_points, d.num_cameras
     assert bk.value == o * (27 * 4 + 4) + n_p * (6 * 4 + 4) + n_c * 2 * 9 * 4
     assert 0 < sk.value < so.value
+
+
+def test_device_trial_decisions_match_the_host_loop():
+    """The Schur backend runs LM trials on the device (step norm, retraction,
+    trial cost, gain ratio, acceptance and damping update in k_lm_decide, one
+    read back per trial); the LSMR backend, which has no device step norm,
+    takes the host loop. On bal16 both walk the same accept/reject sequence
+    with the same damping after every accepted step and reach the same cost."""
+    d = synthetic.generate("bal16")
+    runs = {}
+    for name, b in (("schur", fg.Schur(9 * d.num_cameras, 9, 3)), ("lsmr", fg.Lsmr())):
+        if name == "lsmr":
+            b.block_preconditioning = True
+            b.max_iterations = 100000
+        b.relative_tolerance = 1e-12
+        lm = fg.LevenbergMarquardt(b)
+        trace = []
+        lm.on_accept = lambda s: trace.append((s.accepted_steps, s.rejected_steps, s.damping, s.cost))
+        out = lm.solve_batch_with_outcome(fg.BalProblem.from_data(d), fg.OptimizeOptions(8, 1e-8, 0.0, 0.0))
+        runs[name] = (trace, out.statistics)
+    (ts, ss), (tl, sl) = runs["schur"], runs["lsmr"]
+    assert [t[:2] for t in ts] == [t[:2] for t in tl]
+    for a, b in zip(ts, tl):
+        assert abs(a[2] - b[2]) <= 1e-9 * b[2]  # the damping each accepted trial used
+        assert abs(a[3] - b[3]) <= 1e-9 * b[3]
+    assert (ss.accepted_steps, ss.rejected_steps, ss.attempts) == (sl.accepted_steps, sl.rejected_steps, sl.attempts)
+    assert abs(ss.damping - sl.damping) <= 1e-9 * sl.damping
