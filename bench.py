@@ -255,6 +255,36 @@ def train_network(fg, synthetic, workload: str, device: int, problems: int = 2) 
                      train_seconds=time.perf_counter() - t0, training_problems=f"{problems} x {workload} seeds 200+")
 
 
+def assembly_timing(problem, backend, stream, data, s: float, reps: int = 10) -> dict:
+    """Device time of the linearization (residuals, Jacobians, gradient and raw
+    moments: fagra's Workspace::linearize + LinearizedModel::accumulate) and of
+    the damping preparation (scales, Gram blocks, edge records with the cross
+    blocks: prepare_scales, BlockFactors::prepare, the cross loop of
+    Schur::prepare_damping), CUDA events on the library stream around
+    back-to-back calls, with their algorithmic bytes:
+    linearize O (31 s + 8); assembly O (24 s + 27 s + 4) + P 6 s + C 45 s."""
+    import torch
+    O, P, Cn = data.num_observations, data.num_points, data.num_cameras
+    pk, _ = peaks()
+    out = {}
+    for what, fn, nbytes in (
+            ("linearize", lambda: problem.linearize(backend), O * (31 * s + 8)),
+            ("prepare_damping", lambda: backend.prepare_damping(1e-6), O * (24 * s + 27 * s + 4) + P * 6 * s
+             + Cn * 45 * s)):
+        for _ in range(2):
+            fn()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(reps):
+            fn()
+        ev[1].record(stream)
+        ev[1].synchronize()
+        sec = ev[0].elapsed_time(ev[1]) * 1e-3 / reps
+        out[what] = dict(seconds=sec, algorithmic_bytes=nbytes, achieved_gbs=nbytes / sec / 1e9,
+                         frac=nbytes / sec / 1e9 / pk)
+    return out
+
+
 def run_gpu(args, rank: int, world: int, device: int):
     import numpy as np
     import torch
@@ -386,6 +416,8 @@ def run_gpu(args, rank: int, world: int, device: int):
             var, tuned = C.c_int(), (C.c_double * 4)()
             _lib.lib.fg_schur_operator_info(backend.handle, C.byref(var), tuned)
             results[name]["operator"].update(variant=var.value, tuned_seconds=list(tuned))
+            results[name]["assembly"] = assembly_timing(problem, backend, stream, data,
+                                                        4.0 if kw["precision"] == "f32" else 8.0)
             head_backend = backend
     # e2e: public C ABI from host arrays
     e2e = None
@@ -722,7 +754,9 @@ def main():
             dtype="f32 bulk + f64 reductions" if results[head]["precision"] == "f32" else "f64",
             data="synthetic", config=workload_config(data, g, world),
             form=form, form_description=descriptions.get(form, form), form_note=form_note, learned=learned,
-            forms={k: {kk: vv for kk, vv in v.items() if kk != "operator"} for k, v in results.items()},
+            forms={k: {kk: vv for kk, vv in v.items() if kk not in ("operator", "assembly")}
+                   for k, v in results.items()},
+            assembly=results[head].get("assembly"),
             speedup_vs_f64=(vals["f64"] / vals[head]) if "f64" in vals and head != "f64" else None,
             pcg_iterations=results[head]["cg_iterations"],
             roofline=dict(bound="hbm", kernel={0: "reduced operator, generic (k_points + k_cams)",
