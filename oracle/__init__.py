@@ -148,6 +148,12 @@ _sig = {
                                   C.POINTER(LmOpts), size_t, C.POINTER(Report), C.POINTER(LmStats), dptr, dptr, dptr,
                                   C.POINTER(size_t), C.POINTER(C.c_uint32), C.POINTER(size_t), C.POINTER(size_t)]),
     "or_window_cost": (C.c_int, [size_t, dptr, dptr, size_t, C.POINTER(C.c_uint32), dptr, dptr]),
+    "or_window_solve_prior": (C.c_int, [size_t, dptr, size_t, size_t, dptr, dptr, dptr, size_t,
+                                        C.POINTER(C.c_uint32), dptr, C.POINTER(OptOpts), C.POINTER(LmOpts), size_t,
+                                        C.POINTER(Report), C.POINTER(LmStats), dptr, dptr, dptr, C.POINTER(size_t),
+                                        C.POINTER(C.c_uint32), C.POINTER(size_t), C.POINTER(size_t)]),
+    "or_window_cost_prior": (C.c_int, [size_t, dptr, size_t, size_t, dptr, dptr, dptr, size_t,
+                                       C.POINTER(C.c_uint32), dptr, dptr]),
 }
 for _n, (_r, _a) in _sig.items():
     _f = getattr(lib, _n)
@@ -490,10 +496,20 @@ def pose_log_jacobian(d):
     return st, out.reshape(6, 6)
 
 
+def _marginal(marginal):
+    """(A m x 6s, b m, refs s x 7) -> column-major A, b, refs, m, s."""
+    A, b, refs = marginal
+    A = np.asarray(A, np.float64)
+    refs = np.ascontiguousarray(np.asarray(refs, np.float64).reshape(-1, 7))
+    return (np.ascontiguousarray(A.T).reshape(-1), np.ascontiguousarray(np.asarray(b, np.float64).reshape(-1)), refs,
+            A.shape[0], len(refs))
+
+
 def window_solve(poses, prior, rel_ij, rel_z, removed=10, max_iterations=20, gradient_tolerance=1e-8,
-                 step_tolerance=1e-10, cost_tolerance=1e-12, lm_options=None):
+                 step_tolerance=1e-10, cost_tolerance=1e-12, lm_options=None, marginal=None):
     """LM over DenseSchur(6n, []) for one pose-graph window, then square-root
-    marginalization of its oldest `removed` poses."""
+    marginalization of its oldest `removed` poses. marginal = (A, b, refs):
+    a prior on the first len(refs) poses in place of the anchor prior."""
     poses = np.ascontiguousarray(np.array(poses, np.float64).reshape(-1, 7))
     n = len(poses)
     prior = np.ascontiguousarray(prior, np.float64)
@@ -509,23 +525,36 @@ def window_solve(poses, prior, rel_ij, rel_z, removed=10, max_iterations=20, gra
     rows, nsep, rank = size_t(), size_t(), size_t()
     sep = np.zeros(max(n, 1), np.uint32)
     u32 = C.POINTER(C.c_uint32)
-    code = lib.or_window_solve(n, _dp(poses), _dp(prior), len(ij), ij.ctypes.data_as(u32), _dp(z), C.byref(o),
-                               C.byref(lo), removed, C.byref(rep), C.byref(st), _dp(a), _dp(b), C.byref(const),
-                               C.byref(rows), sep.ctypes.data_as(u32), C.byref(nsep), C.byref(rank))
+    if marginal is None:
+        code = lib.or_window_solve(n, _dp(poses), _dp(prior), len(ij), ij.ctypes.data_as(u32), _dp(z), C.byref(o),
+                                   C.byref(lo), removed, C.byref(rep), C.byref(st), _dp(a), _dp(b), C.byref(const),
+                                   C.byref(rows), sep.ctypes.data_as(u32), C.byref(nsep), C.byref(rank))
+    else:
+        A, bb, refs, m, ns = _marginal(marginal)
+        code = lib.or_window_solve_prior(n, _dp(poses), ns, m, _dp(A), _dp(bb), _dp(refs), len(ij),
+                                         ij.ctypes.data_as(u32), _dp(z), C.byref(o), C.byref(lo), removed,
+                                         C.byref(rep), C.byref(st), _dp(a), _dp(b), C.byref(const), C.byref(rows),
+                                         sep.ctypes.data_as(u32), C.byref(nsep), C.byref(rank))
     k, s = rows.value, 6 * nsep.value
     return dict(code=code, poses=poses, report=rep, stats=st, prior_a=a[:k * s].reshape(s, k).T.copy(),
                 prior_b=b[:k].copy(), prior_constant=const.value, separator=sep[:nsep.value].copy(),
                 rank=rank.value)
 
 
-def window_cost(poses, prior, rel_ij, rel_z):
+def window_cost(poses, prior, rel_ij, rel_z, marginal=None):
     poses = np.ascontiguousarray(np.array(poses, np.float64).reshape(-1, 7))
     prior = np.ascontiguousarray(prior, np.float64)
     ij = np.ascontiguousarray(np.asarray(rel_ij, np.uint32).reshape(-1, 2))
     z = np.ascontiguousarray(np.asarray(rel_z, np.float64).reshape(-1, 7))
     out = C.c_double()
-    st = lib.or_window_cost(len(poses), _dp(poses), _dp(prior), len(ij), ij.ctypes.data_as(C.POINTER(C.c_uint32)),
-                            _dp(z), C.byref(out))
+    u32 = C.POINTER(C.c_uint32)
+    if marginal is None:
+        st = lib.or_window_cost(len(poses), _dp(poses), _dp(prior), len(ij), ij.ctypes.data_as(u32), _dp(z),
+                                C.byref(out))
+    else:
+        A, bb, refs, m, ns = _marginal(marginal)
+        st = lib.or_window_cost_prior(len(poses), _dp(poses), ns, m, _dp(A), _dp(bb), _dp(refs), len(ij),
+                                      ij.ctypes.data_as(u32), _dp(z), C.byref(out))
     return st, out.value
 
 

@@ -1667,20 +1667,66 @@ OR_API int or_pose_log_jacobian(const double* d, double* out) { return log_jacob
 
 // ---- Pose-graph windows: LM over DenseSchur(6n, []) then marginalization of
 // the oldest `removed` poses. poses[7n] in/out; rel_ij[2*nrel]; rel_z[7*nrel].
-OR_API int or_window_solve(size_t n, double* poses, const double* prior, size_t nrel, const uint32_t* rel_ij,
-                           const double* rel_z, const OptimizeOptions* opt, const LmOptions* lo, size_t removed,
-                           Report* rep, LmStats* st, double* prior_a, double* prior_b, double* prior_constant,
-                           size_t* prior_rows, uint32_t* separator, size_t* nseparator, size_t* rank) {
-  PoseWindow w;
+static int window_solve(PoseWindow& w, size_t n, double* poses, const OptimizeOptions* opt, const LmOptions* lo,
+                        size_t removed, Report* rep, LmStats* st, double* prior_a, double* prior_b,
+                        double* prior_constant, size_t* prior_rows, uint32_t* separator, size_t* nseparator,
+                        size_t* rank);
+static void window_factors(PoseWindow& w, size_t n, const double* poses, size_t nrel, const uint32_t* rel_ij,
+                           const double* rel_z) {
   w.x.resize(n);
   for (size_t k = 0; k < n; ++k) w.x[k] = P7(poses + 7 * k);
-  w.prior = P7(prior);
   w.rel.resize(nrel);
   for (size_t k = 0; k < nrel; ++k) {
     w.rel[k].i = rel_ij[2 * k];
     w.rel[k].j = rel_ij[2 * k + 1];
     w.rel[k].z = P7(rel_z + 7 * k);
   }
+}
+static void window_prior(PoseWindow& w, size_t s, size_t m, const double* A, const double* b, const double* refs) {
+  w.prior.s = s;
+  w.prior.m = m;
+  w.prior.A.assign(A, A + m * 6 * s);
+  w.prior.b.assign(b, b + m);
+  w.prior.ref.resize(s);
+  for (size_t k = 0; k < s; ++k) w.prior.ref[k] = P7(refs + 7 * k);
+}
+// A window with a prior on its first s poses (m rows, A m x 6s column-major,
+// b, s reference poses) in place of the anchor.
+OR_API int or_window_solve_prior(size_t n, double* poses, size_t s, size_t m, const double* A, const double* b,
+                                 const double* refs, size_t nrel, const uint32_t* rel_ij, const double* rel_z,
+                                 const OptimizeOptions* opt, const LmOptions* lo, size_t removed, Report* rep,
+                                 LmStats* st, double* prior_a, double* prior_b, double* prior_constant,
+                                 size_t* prior_rows, uint32_t* separator, size_t* nseparator, size_t* rank) {
+  if (s == 0 || s > n || m == 0) return INVALID_OPTIONS;
+  PoseWindow w;
+  window_factors(w, n, poses, nrel, rel_ij, rel_z);
+  window_prior(w, s, m, A, b, refs);
+  return window_solve(w, n, poses, opt, lo, removed, rep, st, prior_a, prior_b, prior_constant, prior_rows, separator,
+                      nseparator, rank);
+}
+OR_API int or_window_cost_prior(size_t n, const double* poses, size_t s, size_t m, const double* A, const double* b,
+                                const double* refs, size_t nrel, const uint32_t* rel_ij, const double* rel_z,
+                                double* out) {
+  if (s == 0 || s > n || m == 0) return INVALID_OPTIONS;
+  PoseWindow w;
+  window_factors(w, n, poses, nrel, rel_ij, rel_z);
+  window_prior(w, s, m, A, b, refs);
+  return w.cost(false, out);
+}
+OR_API int or_window_solve(size_t n, double* poses, const double* prior, size_t nrel, const uint32_t* rel_ij,
+                           const double* rel_z, const OptimizeOptions* opt, const LmOptions* lo, size_t removed,
+                           Report* rep, LmStats* st, double* prior_a, double* prior_b, double* prior_constant,
+                           size_t* prior_rows, uint32_t* separator, size_t* nseparator, size_t* rank) {
+  PoseWindow w;
+  window_factors(w, n, poses, nrel, rel_ij, rel_z);
+  w.prior.anchor(P7(prior));
+  return window_solve(w, n, poses, opt, lo, removed, rep, st, prior_a, prior_b, prior_constant, prior_rows, separator,
+                      nseparator, rank);
+}
+static int window_solve(PoseWindow& w, size_t n, double* poses, const OptimizeOptions* opt, const LmOptions* lo,
+                        size_t removed, Report* rep, LmStats* st, double* prior_a, double* prior_b,
+                        double* prior_constant, size_t* prior_rows, uint32_t* separator, size_t* nseparator,
+                        size_t* rank) {
   DenseSchur solver;
   solver.retained = 6 * n;
   int code = lm_optimize(solver, w, *opt, *lo, rep, st, nullptr, nullptr);
@@ -1704,14 +1750,7 @@ OR_API int or_window_solve(size_t n, double* poses, const double* prior, size_t 
 OR_API int or_window_cost(size_t n, const double* poses, const double* prior, size_t nrel, const uint32_t* rel_ij,
                           const double* rel_z, double* out) {
   PoseWindow w;
-  w.x.resize(n);
-  for (size_t k = 0; k < n; ++k) w.x[k] = P7(poses + 7 * k);
-  w.prior = P7(prior);
-  w.rel.resize(nrel);
-  for (size_t k = 0; k < nrel; ++k) {
-    w.rel[k].i = rel_ij[2 * k];
-    w.rel[k].j = rel_ij[2 * k + 1];
-    w.rel[k].z = P7(rel_z + 7 * k);
-  }
+  window_factors(w, n, poses, nrel, rel_ij, rel_z);
+  w.prior.anchor(P7(prior));
   return w.cost(false, out);
 }

@@ -235,19 +235,55 @@ struct RelativeFactor {
   uint32_t i, j;
   Pose3 z;
 };
+// A prior on the window's first s poses, Priors::update (marginalization.rs:
+// 157-231): r = b + sum_i A_i Log(ref_i^-1 x_i) (anchors in order, columns in
+// order), J_i = A_i Jr^-1(Log(ref_i^-1 x_i)); A is m x 6s column-major. The
+// anchor PosePrior (examples/slam.rs:26-56, r = Log(z^-1 x_0), J = Jr^-1(r))
+// is the case s = 1, A = I, b = 0, ref = z, and gives its values exactly.
+struct WindowPriorFactor {
+  size_t s = 0, m = 0;
+  std::vector<double> A, b;
+  std::vector<Pose3> ref;
+  void anchor(const Pose3& z) {
+    s = 1;
+    m = 6;
+    A.assign(36, 0.0);
+    for (int k = 0; k < 6; ++k) A[k * 6 + k] = 1.0;
+    b.assign(6, 0.0);
+    ref.assign(1, z);
+  }
+};
 struct PoseWindow : Problem {
   std::vector<Pose3> x, tx;
-  Pose3 prior;  // anchor PosePrior on x_0
+  WindowPriorFactor prior;
   std::vector<RelativeFactor> rel;
   bool trial = false;
 
   size_t dimension() override { return 6 * x.size(); }
-  // PosePrior: r = Log(z^-1 x_0), J = Jr^-1(r).
+  // r (m values) and, with J, the m x 6s Jacobian (column-major).
   int prior_residual(const std::vector<Pose3>& X, double* r, double* J) const {
-    pose_local(prior, X[0], r);
-    if (J) return log_jacobian(r, J);
-    for (int k = 0; k < 6; ++k)
-      if (!is_fin(r[k])) return INVALID_EVALUATION;
+    const size_t m = prior.m;
+    for (size_t row = 0; row < m; ++row) r[row] = prior.b[row];
+    for (size_t i = 0; i < prior.s; ++i) {
+      double d[6], jr[36];
+      pose_local(prior.ref[i], X[i], d);
+      for (int k = 0; k < 6; ++k)
+        if (!is_fin(d[k])) return INVALID_EVALUATION;
+      for (size_t row = 0; row < m; ++row)
+        for (int col = 0; col < 6; ++col) r[row] += prior.A[(6 * i + col) * m + row] * d[col];
+      if (J) {
+        int st = log_jacobian(d, jr);
+        if (st) return st;
+        for (int col = 0; col < 6; ++col)
+          for (size_t row = 0; row < m; ++row) {
+            double v = 0;
+            for (int k = 0; k < 6; ++k) v += prior.A[(6 * i + k) * m + row] * jr[k * 6 + col];
+            J[(6 * i + col) * m + row] = v;
+          }
+      }
+    }
+    for (size_t row = 0; row < m; ++row)
+      if (!is_fin(r[row])) return INVALID_EVALUATION;
     return OK;
   }
   int rel_residual(const std::vector<Pose3>& X, const RelativeFactor& f, double* r, double* Ji, double* Jj) const {
@@ -273,10 +309,11 @@ struct PoseWindow : Problem {
   int cost(bool t, double* out) override {
     const std::vector<Pose3>& X = t ? tx : x;
     double total = 0, r[6];
-    int s = prior_residual(X, r, nullptr);
+    std::vector<double> rp(prior.m);
+    int s = prior_residual(X, rp.data(), nullptr);
     if (s) return s;
     double c = 0;
-    for (double e : r) c += 0.5 * e * e;
+    for (double e : rp) c += 0.5 * e * e;
     if ((s = checked(OK, c))) return s;
     total += c;
     for (const auto& f : rel) {
@@ -295,11 +332,21 @@ struct PoseWindow : Problem {
     double r[6], Ji[36], Jj[36];
     size_t cols[2], widths[2] = {6, 6};
     ptrdiff_t rs[2] = {6, 6}, cs[2] = {1, 1};
-    int st = prior_residual(x, r, Jj);
-    if (st) return st;
-    cols[0] = 0;
-    const double* jp[2] = {Jj, nullptr};
-    if ((st = s.accumulate(6, r, 1, cols, widths, jp, rs, cs))) return st;
+    {  // the prior: one emission with a block per anchored pose (marginalization.rs:249-277)
+      const size_t m = prior.m, np = prior.s;
+      std::vector<double> rp(m), jp(m * 6 * np);
+      int st = prior_residual(x, rp.data(), jp.data());
+      if (st) return st;
+      std::vector<size_t> pc(np), pw(np, 6);
+      std::vector<const double*> pj(np);
+      std::vector<ptrdiff_t> prs(np, 1), pcs(np, (ptrdiff_t)m);
+      for (size_t i = 0; i < np; ++i) {
+        pc[i] = 6 * i;
+        pj[i] = jp.data() + 6 * i * m;
+      }
+      if ((st = s.accumulate(m, rp.data(), np, pc.data(), pw.data(), pj.data(), prs.data(), pcs.data()))) return st;
+    }
+    int st = OK;
     for (const auto& f : rel) {
       if ((st = rel_residual(x, f, r, Ji, Jj))) return st;
       cols[0] = 6 * (size_t)f.i;
@@ -334,6 +381,8 @@ struct WindowPrior {
 int marginalize_window(const PoseWindow& w, size_t removed_poses, WindowPrior& out) {
   std::vector<char> touched(w.x.size(), 0);
   std::vector<const RelativeFactor*> facs;
+  // the window prior touches its poses [0, s), pose 0 among the removed ones
+  for (size_t k = 0; k < w.prior.s && k < w.x.size(); ++k) touched[k] = 1;
   for (const auto& f : w.rel)
     if (f.i < removed_poses || f.j < removed_poses) {
       facs.push_back(&f);
@@ -346,18 +395,23 @@ int marginalize_window(const PoseWindow& w, size_t removed_poses, WindowPrior& o
   for (size_t k = 0; k < removed_poses && k < w.x.size(); ++k) column[k] = 6 * k;
   for (size_t s = 0; s < out.separator.size(); ++s) column[out.separator[s]] = 6 * (removed_poses + s);
   const size_t n = 6 * (removed_poses + out.separator.size()), width = n + 1;
-  const size_t m = 6 * (1 + facs.size());
+  const size_t mp = w.prior.m, m = mp + 6 * facs.size();
   std::vector<double> rows(m * width, 0.);
   double r[6], Ji[36], Jj[36];
-  int st = w.prior_residual(w.x, r, Jj);
-  if (st) return st;
-  for (int a = 0; a < 6; ++a) {
-    for (int b = 0; b < 6; ++b) rows[a * width + column[0] + b] = Jj[a * 6 + b];
-    rows[a * width + n] = r[a];
+  {
+    std::vector<double> rp(mp), jp(mp * 6 * w.prior.s);
+    int st = w.prior_residual(w.x, rp.data(), jp.data());
+    if (st) return st;
+    for (size_t a = 0; a < mp; ++a) {
+      for (size_t i = 0; i < w.prior.s; ++i)
+        for (int b = 0; b < 6; ++b) rows[a * width + column[i] + b] = jp[(6 * i + b) * mp + a];
+      rows[a * width + n] = rp[a];
+    }
   }
+  int st = OK;
   for (size_t k = 0; k < facs.size(); ++k) {
     if ((st = w.rel_residual(w.x, *facs[k], r, Ji, Jj))) return st;
-    size_t base = 6 * (1 + k);
+    size_t base = mp + 6 * k;
     for (int a = 0; a < 6; ++a) {
       for (int b = 0; b < 6; ++b) {
         rows[(base + a) * width + column[facs[k]->i] + b] += Ji[a * 6 + b];

@@ -371,3 +371,41 @@ def test_pose_log_inverts_exp_and_adjoint_transports_tangents():
         lhs = oracle.pose_compose(x, oracle.pose_exp(d * 1e-3))
         rhs = oracle.pose_compose(oracle.pose_exp(oracle.pose_adjoint(x) @ (d * 1e-3)), x)
         assert np.allclose(lhs, rhs, atol=1e-12) or np.allclose(lhs, np.concatenate([-rhs[:4], rhs[4:]]), atol=1e-12)
+
+
+def _se3_log_rel(ref, x):
+    """Log(ref^-1 x) through the oracle's own pose primitives."""
+    import ctypes as C
+    dp = C.POINTER(C.c_double)
+    inv, rel, out = np.zeros(7), np.zeros(7), np.zeros(6)
+    a = np.ascontiguousarray(ref, np.float64)
+    b = np.ascontiguousarray(x, np.float64)
+    oracle.lib.or_pose_inverse(a.ctypes.data_as(dp), inv.ctypes.data_as(dp))
+    oracle.lib.or_pose_compose(inv.ctypes.data_as(dp), b.ctypes.data_as(dp), rel.ctypes.data_as(dp))
+    oracle.lib.or_pose_log(rel.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    return out
+
+
+def test_window_prior_generalizes_the_anchor_and_follows_priors_update():
+    """The window prior r = b + sum_i A_i Log(ref_i^-1 x_i) (src/marginalization.rs
+    157-231): with s = 1, A = I, b = 0, ref = z it is the anchor PosePrior and
+    the window solve is bit-identical; a two-pose prior's cost is the numpy
+    restatement's."""
+    from fagra_b200 import posegraph
+    batch = posegraph.generate(2, min_poses=24, max_poses=30)
+    poses, prior, ij, z = batch.window(0)
+    a = oracle.window_solve(poses, prior, ij, z, removed=10)
+    b = oracle.window_solve(poses, prior, ij, z, removed=10, marginal=(np.eye(6), np.zeros(6), prior[None, :]))
+    assert np.array_equal(a["poses"], b["poses"])
+    assert np.array_equal(a["prior_a"], b["prior_a"]) and np.array_equal(a["prior_b"], b["prior_b"])
+    rng = np.random.default_rng(4)
+    A = rng.normal(size=(9, 12))
+    bb = rng.normal(size=9)
+    refs = poses[:2] + 0.0
+    refs[:, 4:] += 0.01 * rng.normal(size=(2, 3))
+    st, c = oracle.window_cost(poses, prior, ij, z, marginal=(A, bb, refs))
+    assert st == 0
+    r = bb + A[:, :6] @ _se3_log_rel(refs[0], poses[0]) + A[:, 6:] @ _se3_log_rel(refs[1], poses[1])
+    st0, c_rel = oracle.window_cost(poses, prior, ij, z, marginal=(np.zeros((1, 6)), np.zeros(1), prior[None, :]))
+    assert st0 == 0
+    assert abs(c - (c_rel + 0.5 * r @ r)) <= 1e-12 * c
