@@ -236,6 +236,8 @@ SIGNATURES = {
     "fg_windows_destroy": (None, [C.c_void_p]),
     "fg_windows_prior_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                           C.POINTER(C.c_uint32)]),
+    "fg_windows_set_priors": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), dptr, dptr,
+                                        dptr]),
     "fg_windows_upload": (C.c_int, [C.c_void_p, dptr, dptr, dptr]),
     "fg_windows_run": (C.c_int, [C.c_void_p, C.POINTER(OptimizeOptionsC), C.POINTER(LmOptionsC)]),
     "fg_windows_download": (C.c_int, [C.c_void_p, dptr, C.POINTER(WindowReportC), dptr, dptr]),

@@ -10,10 +10,16 @@
 // src/marginalization.rs:458-513 (column-pivoted Householder QR of [J | r]
 // over the factors that touch them) into a prior on the separator poses.
 //
-// Factors, in emission order: an anchor PosePrior on pose 0 (examples/slam.rs:
-// 26-56, r = Log(z^-1 x_0), J = Jr^-1(r)) and relative-pose factors
+// Factors, in emission order: the window prior and relative-pose factors
 // r = Log(z^-1 x_i^-1 x_j) with dr/dd_j = Jr^-1(r), dr/dd_i = -Jr^-1(r)
-// Ad((x_i^-1 x_j)^-1), composed from the reference's SE(3) primitives.
+// Ad((x_i^-1 x_j)^-1), composed from the reference's SE(3) primitives. The
+// window prior is Priors::update (src/marginalization.rs:157-231) on the
+// window's first s poses, r = b + sum_i A_i Log(ref_i^-1 x_i) with Jacobian
+// blocks A_i Jr^-1(Log(ref_i^-1 x_i)): by default the anchor PosePrior of
+// examples/slam.rs:26-56 (s = 1, A = I, b = 0, ref = z: r = Log(z^-1 x_0)),
+// or a marginal prior from an earlier window's elimination
+// (fg_windows_set_priors), which is how a window's marginal prior feeds the
+// next window's device LM solve.
 //
 // Dense work stays inside the CTA: a right-looking blocked Cholesky (panel
 // CB, trailing tiles of 64 x 64 with 4 x 4 register blocks from shared
@@ -47,13 +53,21 @@ struct WinDev {
   const int64_t* rel_off;   // W+1
   const uint32_t* rel_ij;   // 2 per relative factor, window-local
   const double* rel_z;      // 7 per relative factor
-  const double* prior;      // 7 per window
+  const int32_t* pr_s;      // W: prior poses (the window's first s)
+  const int32_t* pr_m;      // W: prior rows
+  const int64_t* pr_aoff;   // W: start of the window's A (m x 6s, column-major) in pr_A
+  const int64_t* pr_boff;   // W: start of its b (m) in pr_b
+  const int64_t* pr_roff;   // W: first reference pose (7 each) in pr_ref
+  const int64_t* pf_off;    // W: scratch start: r (m) | J (m x 6s) | u (m) | d (6s) | Jr^-1 (36s)
+  const double* pr_A;
+  const double* pr_b;
+  const double* pr_ref;
   double* x;                // 7 per pose (in/out)
   double* xt;               // 7 per pose (trial)
   const int64_t* inc_off;   // per global pose, CSR of incident relative factors
   const int32_t* inc;       // (factor << 1) | side, side 1 = j
   double* fac;              // FS per relative factor: r, Ji, Jj, J d
-  double* pfac;             // PS per window: r, J, J d of the prior
+  double* pfac;             // prior scratch (pf_off)
   const int64_t* tile_off;  // W+1: 64-row tiles of each window's coordinates
   const int32_t* tile_cmin; // per tile: first 64-column tile of its rows' envelope
   const int64_t* mf_off;    // W+1: relative factors touching the eliminated poses
@@ -76,7 +90,8 @@ struct WinDev {
 };
 
 constexpr int FS = 84;    // doubles per relative factor in the scratch
-constexpr int PS = 48;    // doubles per window prior in the scratch
+constexpr int PR_MAX_POSES = 64;  // poses a window prior may cover
+constexpr int PR_MAX_ROWS = 384;  // rows a window prior may have
 
 // ------------------------------------------------------------ factors
 // Residual (and Jacobians) of relative factor f at poses X; false if nonfinite.
@@ -100,12 +115,56 @@ __device__ inline bool rel_eval(const WinDev& D, int64_t f, const double* X, dou
     }
   return true;
 }
-__device__ inline bool prior_eval(const WinDev& D, int w, const double* X0, double* r, double* J) {
-  se3_log(se3_compose(se3_inverse(load_pose(D.prior + 7 * (size_t)w)), load_pose(X0)), r);
-  if (J) return se3_log_jacobian(r, J);
-  for (int k = 0; k < 6; ++k)
-    if (!isfinite(r[k])) return false;
-  return true;
+// The window prior of window w at poses X, all threads of the CTA:
+// d_i = Log(ref_i^-1 x_i) (and Jr^-1(d_i) with `jac`), then r = b + sum_i A_i
+// d_i and, with `jac`, J = [A_i Jr^-1(d_i)]_i into the window's scratch, in
+// the order of Priors::update (anchors in order, columns in order). False if
+// any value is nonfinite (uniform across the CTA).
+struct WinPrior {
+  int s, m;
+  const double *A, *b, *ref;
+  double *r, *J, *u, *d, *jr;
+};
+__device__ inline WinPrior win_prior(const WinDev& D, int w) {
+  WinPrior P;
+  P.s = D.pr_s[w];
+  P.m = D.pr_m[w];
+  P.A = D.pr_A + D.pr_aoff[w];
+  P.b = D.pr_b + D.pr_boff[w];
+  P.ref = D.pr_ref + 7 * D.pr_roff[w];
+  P.r = D.pfac + D.pf_off[w];
+  P.J = P.r + P.m;
+  P.u = P.J + (size_t)P.m * 6 * P.s;
+  P.d = P.u + P.m;
+  P.jr = P.d + 6 * P.s;
+  return P;
+}
+__device__ inline bool prior_terms(const WinPrior& P, const double* X, bool jac, double* red) {
+  double bad = 0;
+  for (int i = threadIdx.x; i < P.s; i += WNT) {
+    se3_log(se3_compose(se3_inverse(load_pose(P.ref + 7 * (size_t)i)), load_pose(X + 7 * (size_t)i)), P.d + 6 * i);
+    for (int k = 0; k < 6; ++k)
+      if (!isfinite(P.d[6 * i + k])) bad = 1;
+    if (jac && !se3_log_jacobian(P.d + 6 * i, P.jr + 36 * i)) bad = 1;
+  }
+  __syncthreads();
+  for (int row = threadIdx.x; row < P.m; row += WNT) {
+    double v = P.b[row];
+    for (int i = 0; i < P.s; ++i)
+      for (int col = 0; col < 6; ++col) v += P.A[(size_t)(6 * i + col) * P.m + row] * P.d[6 * i + col];
+    P.r[row] = v;
+    if (!isfinite(v)) bad = 1;
+  }
+  if (jac)
+    for (int e = threadIdx.x; e < P.m * 6 * P.s; e += WNT) {
+      const int row = e % P.m, cc = e / P.m, i = cc / 6, col = cc % 6;
+      double v = 0;
+      for (int k = 0; k < 6; ++k) v += P.A[(size_t)(6 * i + k) * P.m + row] * P.jr[36 * i + k * 6 + col];
+      P.J[(size_t)cc * P.m + row] = v;
+      if (!isfinite(v)) bad = 1;
+    }
+  __syncthreads();
+  return wmax(bad, red) == 0;
 }
 
 // Cost of window w at poses X (pose base pb); bad = 1 if any factor is nonfinite.
@@ -121,10 +180,12 @@ __device__ inline double window_cost(const WinDev& D, int w, const double* X, do
     for (int k = 0; k < 6; ++k) e += 0.5 * r[k] * r[k];
     c += e;
   }
+  const WinPrior P = win_prior(D, w);
+  const bool pok = prior_terms(P, X, false, red);
   if (threadIdx.x == 0) {
-    if (!prior_eval(D, w, X, r, nullptr)) nb = 1;
+    if (!pok) nb = 1;
     else
-      for (int k = 0; k < 6; ++k) c += 0.5 * r[k] * r[k];
+      for (int k = 0; k < P.m; ++k) c += 0.5 * P.r[k] * P.r[k];
   }
   const double tot = wsum(c, red);
   *bad = wmax(nb, red) != 0 || !isfinite(tot) || tot < 0;
@@ -189,10 +250,8 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
         for (int k = 0; k < 78; ++k)
           if (!isfinite(o[k])) nb = 1;
       }
-      if (tid == 0) {
-        double* o = D.pfac + PS * (size_t)w;
-        if (!prior_eval(D, w, X, o, o + 6)) nb = 1;
-      }
+      const WinPrior P = win_prior(D, w);
+      if (!prior_terms(P, X, true, S.red)) nb = 1;
       if (wmax(nb, S.red) != 0) {
         status = FG_INVALID_EVALUATION;
         break;
@@ -201,12 +260,12 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
       double gmax = 0, gbad = 0;
       for (int p = tid; p < n; p += WNT) {
         double gg[6] = {0, 0, 0, 0, 0, 0}, ss[6] = {0, 0, 0, 0, 0, 0};
-        if (p == 0) {
-          const double* o = D.pfac + PS * (size_t)w;
+        if (p < P.s) {
           for (int c = 0; c < 6; ++c)
-            for (int k = 0; k < 6; ++k) {
-              gg[c] += o[6 + k * 6 + c] * o[k];
-              ss[c] += o[6 + k * 6 + c] * o[6 + k * 6 + c];
+            for (int k = 0; k < P.m; ++k) {
+              const double jv = P.J[(size_t)(6 * p + c) * P.m + k];
+              gg[c] += jv * P.r[k];
+              ss[c] += jv * jv;
             }
         }
         for (int64_t e = D.inc_off[p0 + p]; e < D.inc_off[p0 + p + 1]; ++e) {
@@ -258,11 +317,11 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
       for (int p = tid; p < n; p += WNT) {
         double blk[36];
         for (int k = 0; k < 36; ++k) blk[k] = 0;
-        if (p == 0) {
-          const double* J = D.pfac + PS * (size_t)w + 6;
+        if (p < P.s) {
+          const double* J = P.J + (size_t)6 * p * P.m;
           for (int a = 0; a < 6; ++a)
             for (int b = 0; b <= a; ++b)
-              for (int k = 0; k < 6; ++k) blk[a * 6 + b] += J[k * 6 + a] * J[k * 6 + b];
+              for (int k = 0; k < P.m; ++k) blk[a * 6 + b] += J[(size_t)a * P.m + k] * J[(size_t)b * P.m + k];
         }
         for (int64_t e = D.inc_off[p0 + p]; e < D.inc_off[p0 + p + 1]; ++e) {
           const int32_t code = D.inc[e];
@@ -287,6 +346,16 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
             const int row = i > j ? 6 * i + a : 6 * j + b, col = i > j ? 6 * j + b : 6 * i + a;
             atomicAdd(&G[(size_t)col * N + row], v);
           }
+      }
+      // the prior's blocks between its poses q < p (none for the anchor)
+      for (int e = tid; e < 18 * P.s * (P.s - 1); e += WNT) {
+        const int pq = e / 36, ab = e % 36, a = ab / 6, b = ab % 6;
+        int p = 1, q = pq;
+        while (q >= p) q -= p++;
+        double v = 0;
+        for (int k = 0; k < P.m; ++k) v += P.J[(size_t)(6 * p + a) * P.m + k] * P.J[(size_t)(6 * q + b) * P.m + k];
+        v /= sc[6 * p + a] * sc[6 * q + b];
+        atomicAdd(&G[(size_t)(6 * q + b) * N + 6 * p + a], v);
       }
       __syncthreads();
       const bool undamped = stalled;
@@ -343,23 +412,19 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
                   o[78 + a] = u;
                 }
               }
-              if (tid == 0) {
-                double* o = D.pfac + PS * (size_t)w;
-                for (int a = 0; a < 6; ++a) {
+              if (tid == 0)
+                for (int a = 0; a < P.m; ++a) {
                   double u = 0;
-                  for (int k = 0; k < 6; ++k) u += o[6 + a * 6 + k] * dv[k] / sc[k];
-                  o[42 + a] = u;
+                  for (int k = 0; k < 6 * P.s; ++k) u += P.J[(size_t)k * P.m + a] * dv[k] / sc[k];
+                  P.u[a] = u;
                 }
-              }
               __syncthreads();
               double rn = 0;
               for (int p = tid; p < n; p += WNT) {
                 double y[6] = {0, 0, 0, 0, 0, 0};
-                if (p == 0) {
-                  const double* o = D.pfac + PS * (size_t)w;
+                if (p < P.s)
                   for (int c = 0; c < 6; ++c)
-                    for (int k = 0; k < 6; ++k) y[c] += o[6 + k * 6 + c] * o[42 + k];
-                }
+                    for (int k = 0; k < P.m; ++k) y[c] += P.J[(size_t)(6 * p + c) * P.m + k] * P.u[k];
                 for (int64_t e = D.inc_off[p0 + p]; e < D.inc_off[p0 + p + 1]; ++e) {
                   const int32_t code = D.inc[e];
                   const double* o = D.fac + FS * (int64_t)(code >> 1);
@@ -399,14 +464,12 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
               jd += u * u;
             }
           }
-          if (tid == 0) {
-            const double* J = D.pfac + PS * (size_t)w + 6;
-            for (int a = 0; a < 6; ++a) {
+          if (tid == 0)
+            for (int a = 0; a < P.m; ++a) {
               double u = 0;
-              for (int k = 0; k < 6; ++k) u += J[a * 6 + k] * dv[k];
+              for (int k = 0; k < 6 * P.s; ++k) u += P.J[(size_t)k * P.m + a] * dv[k];
               jd += u * u;
             }
-          }
           gd = wsum(gd, S.red);
           jd = wsum(jd, S.red);
           fin = wmax(fin, S.red);
@@ -468,10 +531,11 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
       const int64_t m0 = D.mf_off[w], m1 = D.mf_off[w + 1];
       const int64_t s0 = D.sep_off[w];
       const int nsep = (int)(D.sep_off[w + 1] - s0);
-      const int m = 6 * (1 + (int)(m1 - m0));
+      const WinPrior P = win_prior(D, w);
+      const int m = P.m + 6 * (int)(m1 - m0);
       const int ncol = 6 * (removed + nsep), width = ncol + 1;
       for (int64_t e = tid; e < (int64_t)m * width; e += WNT) M[e] = 0;
-      __syncthreads();
+      const bool pok = prior_terms(P, X, true, S.red);  // r and J of the prior at the final estimate
       auto column = [&](int p) -> int {
         if (p < removed) return 6 * p;
         for (int s = 0; s < nsep; ++s)
@@ -481,16 +545,22 @@ __global__ void __launch_bounds__(WNT, MINB) k_windows(WinDev D, WinOptions O) {
       double mbad = 0;
       for (int k = tid; k <= (int)(m1 - m0); k += WNT) {
         double r[6], Ji[36], Jj[36];
-        const int base = 6 * k;
-        if (k == 0) {
-          if (!prior_eval(D, w, X, r, Jj)) {
+        const int base = P.m + 6 * (k - 1);
+        if (k == 0) {  // the prior's rows first (its emission comes first)
+          if (!pok) {
             mbad = 1;
             continue;
           }
-          for (int a = 0; a < 6; ++a) {
-            for (int b = 0; b < 6; ++b) M[(size_t)b * m + a] = Jj[a * 6 + b];
-            M[(size_t)ncol * m + a] = r[a];
+          for (int i = 0; i < P.s; ++i) {
+            const int ci = column(i);
+            if (ci < 0) {
+              mbad = 1;
+              break;
+            }
+            for (int a = 0; a < P.m; ++a)
+              for (int b = 0; b < 6; ++b) M[(size_t)(ci + b) * m + a] = P.J[(size_t)(6 * i + b) * P.m + a];
           }
+          for (int a = 0; a < P.m; ++a) M[(size_t)ncol * m + a] = P.r[a];
         } else {
           const int64_t f = D.mf[m0 + k - 1];
           if (!rel_eval(D, f, X, r, Ji, Jj)) {
@@ -566,12 +636,20 @@ struct WindowsImpl {
   std::vector<int32_t> tile_cmin;
   std::vector<uint32_t> rel_ij, sep;
   std::vector<int32_t> inc, mf, order;
+  // window priors (default: the anchor on pose 0): poses s and rows m per
+  // window, A (m x 6s column-major), b (m), references (7 per prior pose)
+  std::vector<int32_t> ps, pm;
+  std::vector<int64_t> pr_aoff, pr_boff, pr_roff, pf_off;
+  std::vector<double> prA, prb, pref;
+  bool custom_priors = false;
   int nmax = 0;
   size_t mcap = 0;
   DBuf<int64_t> d_pose_off, d_rel_off, d_inc_off, d_mf_off, d_sep_off, d_a_off, d_tile_off;
   DBuf<int32_t> d_tile_cmin;
   DBuf<uint32_t> d_rel_ij, d_sep, d_queue;
-  DBuf<int32_t> d_inc, d_mf, d_order;
+  DBuf<int32_t> d_inc, d_mf, d_order, d_pr_s, d_pr_m;
+  DBuf<int64_t> d_pr_aoff, d_pr_boff, d_pr_roff, d_pf_off;
+  DBuf<double> d_prA, d_prb, d_pref;
   DBuf<double> d_x, d_xt, d_prior, d_rel_z, d_fac, d_pfac, d_pa, d_pb, d_G, d_M, d_V;
   DBuf<unsigned char> d_F, d_TV;
   DBuf<fg_window_report> d_reports;
@@ -680,7 +758,15 @@ fg_status windows_view(WindowsImpl& h, const fg_optimize_options& o, const fg_lm
   d.rel_off = h.d_rel_off.get();
   d.rel_ij = h.d_rel_ij.get();
   d.rel_z = h.d_rel_z.get();
-  d.prior = h.d_prior.get();
+  d.pr_s = h.d_pr_s.get();
+  d.pr_m = h.d_pr_m.get();
+  d.pr_aoff = h.d_pr_aoff.get();
+  d.pr_boff = h.d_pr_boff.get();
+  d.pr_roff = h.d_pr_roff.get();
+  d.pf_off = h.d_pf_off.get();
+  d.pr_A = h.d_prA.get();
+  d.pr_b = h.d_prb.get();
+  d.pr_ref = h.custom_priors ? h.d_pref.get() : h.d_prior.get();
   d.x = h.d_x.get();
   d.xt = h.d_xt.get();
   d.inc_off = h.d_inc_off.get();
@@ -778,6 +864,185 @@ fg_status run_graph(WindowsImpl& h, const WinDev& D, const WinOptions& O) {
 }
 }  // namespace
 
+namespace {
+// The per-window structure that depends on the factors and the window
+// priors: incidence, the factors and separator of each elimination (the
+// prior touches its poses [0, s), pose 0 among the removed ones), the
+// normal-matrix envelope (the prior couples its poses densely) and the prior
+// scratch; uploaded to the device.
+fg_status plan_windows(WindowsImpl& h) {
+  const size_t W = h.W;
+  fg_status s = FG_OK;
+  cudaStream_t st = h.st;
+  // Validate factors, build incidence and the marginalization structure.
+  std::vector<int64_t> cnt(h.P + 1, 0);
+  h.mf_off.assign(W + 1, 0);
+  h.sep_off.assign(W + 1, 0);
+  h.a_off.assign(W + 1, 0);
+  h.nmax = 0;
+  h.mcap = 1;
+  std::vector<int32_t> mf;
+  std::vector<uint32_t> sep;
+  for (size_t w = 0; w < W; ++w) {
+    const int64_t n = h.pose_off[w + 1] - h.pose_off[w];
+    if (6 * n > 6 * 4096) {
+      set_error("windows hold at most 4096 poses");
+      return FG_UNSUPPORTED_STRUCTURE;
+    }
+    h.nmax = std::max<int>(h.nmax, (int)(6 * n));
+    const int rm = (int)std::min<int64_t>(h.removed, n);
+    if (h.ps[w] > n) {
+      set_error("a window prior covers more poses than its window holds");
+      return FG_DIMENSION_MISMATCH;
+    }
+    std::vector<char> touched(n, 0);
+    // the prior touches its poses [0, s); pose 0 is among the removed ones
+    if (rm > 0)
+      for (int k = 0; k < h.ps[w]; ++k) touched[k] = 1;
+    std::vector<std::pair<uint32_t, uint32_t>> pairs;
+    int64_t nmf = 0;
+    for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
+      const uint32_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
+      if (i >= (uint64_t)n || j >= (uint64_t)n) {
+        set_error("relative factor pose index outside its window");
+        return FG_DIMENSION_MISMATCH;
+      }
+      if (i == j) {
+        set_error("relative factor between a pose and itself");
+        return FG_UNSUPPORTED_STRUCTURE;
+      }
+      cnt[h.pose_off[w] + i + 1]++;
+      cnt[h.pose_off[w] + j + 1]++;
+      if ((int)i < rm || (int)j < rm) {
+        mf.push_back((int32_t)f);
+        ++nmf;
+        touched[i] = touched[j] = 1;
+      }
+    }
+    for (int64_t k = rm; k < n; ++k)
+      if (touched[k]) sep.push_back((uint32_t)k);
+    h.mf_off[w + 1] = (int64_t)mf.size();
+    h.sep_off[w + 1] = (int64_t)sep.size();
+    const int64_t nsep = h.sep_off[w + 1] - h.sep_off[w];
+    h.a_off[w + 1] = h.a_off[w] + 36 * nsep * nsep;
+    const size_t m = (size_t)h.pm[w] + 6 * (size_t)nmf, width = 6 * ((size_t)rm + (size_t)nsep) + 1;
+    h.mcap = std::max(h.mcap, m * width);
+    if (width - 1 > (size_t)6 * 4096) {
+      set_error("marginalization system too wide");
+      return FG_UNSUPPORTED_STRUCTURE;
+    }
+  }
+  // Envelope of each window's normal matrix: row block p starts at pose
+  // env[p] = min(p, lowest neighbour); per 64-row tile, its first 64-column tile.
+  h.tile_off.assign(W + 1, 0);
+  h.tile_cmin.clear();
+  for (size_t w = 0; w < W; ++w) {
+    const int64_t n = h.pose_off[w + 1] - h.pose_off[w], N = 6 * n;
+    std::vector<int64_t> env(n);
+    for (int64_t p = 0; p < n; ++p) env[p] = p < h.ps[w] ? 0 : p;  // the prior couples [0, s) densely
+    for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
+      const int64_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
+      const int64_t hi = std::max(i, j), lo = std::min(i, j);
+      env[hi] = std::min(env[hi], lo);
+    }
+    const int64_t nT = (N + 63) / 64;
+    for (int64_t T = 0; T < nT; ++T) {
+      int64_t first = T * 64;
+      for (int64_t r = T * 64; r < std::min(N, T * 64 + 64); ++r) first = std::min(first, 6 * env[r / 6]);
+      h.tile_cmin.push_back((int32_t)(first / 64));
+    }
+    h.tile_off[w + 1] = (int64_t)h.tile_cmin.size();
+  }
+  for (size_t p = 0; p < h.P; ++p) cnt[p + 1] += cnt[p];
+  h.inc_off = cnt;
+  h.inc.assign(std::max<int64_t>(cnt[h.P], 1), 0);
+  {
+    std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+    for (size_t w = 0; w < W; ++w)
+      for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
+        const uint32_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
+        h.inc[fill[h.pose_off[w] + i]++] = (int32_t)(f << 1);
+        h.inc[fill[h.pose_off[w] + j]++] = (int32_t)((f << 1) | 1);
+      }
+  }
+  if (h.R > (1u << 30)) {
+    set_error("too many relative factors");
+    return FG_UNSUPPORTED_STRUCTURE;
+  }
+  h.mf = mf;
+  h.sep = sep;
+  h.order.resize(W);
+  std::iota(h.order.begin(), h.order.end(), 0);
+  std::stable_sort(h.order.begin(), h.order.end(), [&](int a, int b) {
+    return h.pose_off[a + 1] - h.pose_off[a] > h.pose_off[b + 1] - h.pose_off[b];
+  });
+  if ((s = upload(h.d_pose_off, h.pose_off.data(), h.pose_off.size(), st))) return s;
+  if ((s = upload(h.d_rel_off, h.rel_off.data(), h.rel_off.size(), st))) return s;
+  std::vector<uint32_t> ij = h.rel_ij;
+  if (ij.empty()) ij.assign(2, 0);
+  if ((s = upload(h.d_rel_ij, ij.data(), ij.size(), st))) return s;
+  if ((s = upload(h.d_inc_off, h.inc_off.data(), h.inc_off.size(), st))) return s;
+  if ((s = upload(h.d_inc, h.inc.data(), h.inc.size(), st))) return s;
+  if ((s = upload(h.d_mf_off, h.mf_off.data(), h.mf_off.size(), st))) return s;
+  std::vector<int32_t> mfv = h.mf;
+  if (mfv.empty()) mfv.push_back(0);
+  if ((s = upload(h.d_mf, mfv.data(), mfv.size(), st))) return s;
+  if ((s = upload(h.d_sep_off, h.sep_off.data(), h.sep_off.size(), st))) return s;
+  std::vector<uint32_t> sv = h.sep;
+  if (sv.empty()) sv.push_back(0);
+  if ((s = upload(h.d_sep, sv.data(), sv.size(), st))) return s;
+  if ((s = upload(h.d_a_off, h.a_off.data(), h.a_off.size(), st))) return s;
+  if ((s = upload(h.d_tile_off, h.tile_off.data(), h.tile_off.size(), st))) return s;
+  std::vector<int32_t> tc = h.tile_cmin;
+  if (tc.empty()) tc.push_back(0);
+  if ((s = upload(h.d_tile_cmin, tc.data(), tc.size(), st))) return s;
+  std::vector<int32_t> ord = h.order;
+  if (ord.empty()) ord.push_back(0);
+  if ((s = upload(h.d_order, ord.data(), ord.size(), st))) return s;
+  // the window priors: shapes, data, scratch offsets
+  h.pr_aoff.assign(W + 1, 0);
+  h.pr_boff.assign(W + 1, 0);
+  h.pr_roff.assign(W + 1, 0);
+  h.pf_off.assign(W + 1, 0);
+  for (size_t w = 0; w < W; ++w) {
+  const int64_t ps = h.ps[w], pm = h.pm[w];
+  h.pr_aoff[w + 1] = h.pr_aoff[w] + pm * 6 * ps;
+  h.pr_boff[w + 1] = h.pr_boff[w] + pm;
+  h.pr_roff[w + 1] = h.pr_roff[w] + ps;
+  h.pf_off[w + 1] = h.pf_off[w] + pm + pm * 6 * ps + pm + 6 * ps + 36 * ps;
+  }
+  auto pad_i = [](std::vector<int32_t> v) {
+    if (v.empty()) v.push_back(0);
+    return v;
+  };
+  auto pad_d = [](std::vector<double> v) {
+    if (v.empty()) v.push_back(0);
+    return v;
+  };
+  const std::vector<int32_t> psv = pad_i(h.ps), pmv = pad_i(h.pm);
+  const std::vector<double> pav = pad_d(h.prA), pbv = pad_d(h.prb), prv = pad_d(h.pref);
+  if ((s = upload(h.d_pr_s, psv.data(), psv.size(), st))) return s;
+  if ((s = upload(h.d_pr_m, pmv.data(), pmv.size(), st))) return s;
+  if ((s = upload(h.d_pr_aoff, h.pr_aoff.data(), W + 1, st))) return s;
+  if ((s = upload(h.d_pr_boff, h.pr_boff.data(), W + 1, st))) return s;
+  if ((s = upload(h.d_pr_roff, h.pr_roff.data(), W + 1, st))) return s;
+  if ((s = upload(h.d_pf_off, h.pf_off.data(), W + 1, st))) return s;
+  if ((s = upload(h.d_prA, pav.data(), pav.size(), st))) return s;
+  if ((s = upload(h.d_prb, pbv.data(), pbv.size(), st))) return s;
+  if (h.custom_priors && (s = upload(h.d_pref, prv.data(), prv.size(), st))) return s;
+  if ((s = h.d_pfac.resize(std::max<int64_t>(h.pf_off[W], 1)))) return s;
+  if ((s = h.d_pa.resize(std::max<int64_t>(h.a_off[W], 1)))) return s;
+  if ((s = h.d_pb.resize(std::max<int64_t>(6 * h.sep_off[W], 1)))) return s;
+  h.slots = 0;  // the marginalization workspace (mcap) may have grown
+  if (h.graph) {
+  cudaGraphExecDestroy(h.graph);
+  h.graph = nullptr;
+  }
+  FG_CUDA(cudaStreamSynchronize(st));
+  return FG_OK;
+}
+}  // namespace
+
 FG_API fg_status fg_windows_create(size_t windows, const uint64_t* pose_offset, const uint64_t* rel_offset,
                                    const uint32_t* rel_ij, size_t removed_poses, int precision, int device,
                                    fg_windows** out) {
@@ -817,134 +1082,22 @@ FG_API fg_status fg_windows_create(size_t windows, const uint64_t* pose_offset, 
     h.R = (size_t)h.rel_off[windows];
     if (h.R && !rel_ij) return fail(FG_NULL_ARGUMENT);
     h.rel_ij.assign(rel_ij, rel_ij + 2 * h.R);
-    // Validate factors, build incidence and the marginalization structure.
-    std::vector<int64_t> cnt(h.P + 1, 0);
-    h.mf_off.assign(windows + 1, 0);
-    h.sep_off.assign(windows + 1, 0);
-    h.a_off.assign(windows + 1, 0);
-    h.nmax = 0;
-    h.mcap = 1;
-    std::vector<int32_t> mf;
-    std::vector<uint32_t> sep;
-    for (size_t w = 0; w < windows; ++w) {
-      const int64_t n = h.pose_off[w + 1] - h.pose_off[w];
-      if (6 * n > 6 * 4096) {
-        set_error("windows hold at most 4096 poses");
-        return fail(FG_UNSUPPORTED_STRUCTURE);
-      }
-      h.nmax = std::max<int>(h.nmax, (int)(6 * n));
-      const int rm = (int)std::min<int64_t>(h.removed, n);
-      std::vector<char> touched(n, 0);
-      std::vector<std::pair<uint32_t, uint32_t>> pairs;
-      int64_t nmf = 0;
-      for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
-        const uint32_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
-        if (i >= (uint64_t)n || j >= (uint64_t)n) {
-          set_error("relative factor pose index outside its window");
-          return fail(FG_DIMENSION_MISMATCH);
-        }
-        if (i == j) {
-          set_error("relative factor between a pose and itself");
-          return fail(FG_UNSUPPORTED_STRUCTURE);
-        }
-        cnt[h.pose_off[w] + i + 1]++;
-        cnt[h.pose_off[w] + j + 1]++;
-        if ((int)i < rm || (int)j < rm) {
-          mf.push_back((int32_t)f);
-          ++nmf;
-          touched[i] = touched[j] = 1;
-        }
-      }
-      for (int64_t k = rm; k < n; ++k)
-        if (touched[k]) sep.push_back((uint32_t)k);
-      h.mf_off[w + 1] = (int64_t)mf.size();
-      h.sep_off[w + 1] = (int64_t)sep.size();
-      const int64_t nsep = h.sep_off[w + 1] - h.sep_off[w];
-      h.a_off[w + 1] = h.a_off[w] + 36 * nsep * nsep;
-      const size_t m = 6 * (1 + (size_t)nmf), width = 6 * ((size_t)rm + (size_t)nsep) + 1;
-      h.mcap = std::max(h.mcap, m * width);
-      if (width - 1 > (size_t)6 * 4096) {
-        set_error("marginalization system too wide");
-        return fail(FG_UNSUPPORTED_STRUCTURE);
-      }
-    }
-    // Envelope of each window's normal matrix: row block p starts at pose
-    // env[p] = min(p, lowest neighbour); per 64-row tile, its first 64-column tile.
-    h.tile_off.assign(windows + 1, 0);
-    h.tile_cmin.clear();
-    for (size_t w = 0; w < windows; ++w) {
-      const int64_t n = h.pose_off[w + 1] - h.pose_off[w], N = 6 * n;
-      std::vector<int64_t> env(n);
-      for (int64_t p = 0; p < n; ++p) env[p] = p;
-      for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
-        const int64_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
-        const int64_t hi = std::max(i, j), lo = std::min(i, j);
-        env[hi] = std::min(env[hi], lo);
-      }
-      const int64_t nT = (N + 63) / 64;
-      for (int64_t T = 0; T < nT; ++T) {
-        int64_t first = T * 64;
-        for (int64_t r = T * 64; r < std::min(N, T * 64 + 64); ++r) first = std::min(first, 6 * env[r / 6]);
-        h.tile_cmin.push_back((int32_t)(first / 64));
-      }
-      h.tile_off[w + 1] = (int64_t)h.tile_cmin.size();
-    }
-    for (size_t p = 0; p < h.P; ++p) cnt[p + 1] += cnt[p];
-    h.inc_off = cnt;
-    h.inc.assign(std::max<int64_t>(cnt[h.P], 1), 0);
-    {
-      std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
-      for (size_t w = 0; w < windows; ++w)
-        for (int64_t f = h.rel_off[w]; f < h.rel_off[w + 1]; ++f) {
-          const uint32_t i = h.rel_ij[2 * f], j = h.rel_ij[2 * f + 1];
-          h.inc[fill[h.pose_off[w] + i]++] = (int32_t)(f << 1);
-          h.inc[fill[h.pose_off[w] + j]++] = (int32_t)((f << 1) | 1);
-        }
-    }
-    if (h.R > (1u << 30)) {
-      set_error("too many relative factors");
-      return fail(FG_UNSUPPORTED_STRUCTURE);
-    }
-    h.mf = mf;
-    h.sep = sep;
-    h.order.resize(windows);
-    std::iota(h.order.begin(), h.order.end(), 0);
-    std::stable_sort(h.order.begin(), h.order.end(), [&](int a, int b) {
-      return h.pose_off[a + 1] - h.pose_off[a] > h.pose_off[b + 1] - h.pose_off[b];
-    });
+    // default window priors: the anchor PosePrior on pose 0 (s = 1, A = I, b = 0)
+    h.ps.assign(windows, 1);
+    h.pm.assign(windows, 6);
+    h.prA.assign(36 * windows, 0.0);
+    h.prb.assign(6 * windows, 0.0);
+    for (size_t w = 0; w < windows; ++w)
+      for (int k = 0; k < 6; ++k) h.prA[36 * w + 7 * k] = 1.0;
+    h.custom_priors = false;
+    if ((s = plan_windows(h))) return fail(s);
     cudaStream_t st = h.st;
-    if ((s = upload(h.d_pose_off, h.pose_off.data(), h.pose_off.size(), st))) return fail(s);
-    if ((s = upload(h.d_rel_off, h.rel_off.data(), h.rel_off.size(), st))) return fail(s);
-    std::vector<uint32_t> ij = h.rel_ij;
-    if (ij.empty()) ij.assign(2, 0);
-    if ((s = upload(h.d_rel_ij, ij.data(), ij.size(), st))) return fail(s);
-    if ((s = upload(h.d_inc_off, h.inc_off.data(), h.inc_off.size(), st))) return fail(s);
-    if ((s = upload(h.d_inc, h.inc.data(), h.inc.size(), st))) return fail(s);
-    if ((s = upload(h.d_mf_off, h.mf_off.data(), h.mf_off.size(), st))) return fail(s);
-    std::vector<int32_t> mfv = h.mf;
-    if (mfv.empty()) mfv.push_back(0);
-    if ((s = upload(h.d_mf, mfv.data(), mfv.size(), st))) return fail(s);
-    if ((s = upload(h.d_sep_off, h.sep_off.data(), h.sep_off.size(), st))) return fail(s);
-    std::vector<uint32_t> sv = h.sep;
-    if (sv.empty()) sv.push_back(0);
-    if ((s = upload(h.d_sep, sv.data(), sv.size(), st))) return fail(s);
-    if ((s = upload(h.d_a_off, h.a_off.data(), h.a_off.size(), st))) return fail(s);
-    if ((s = upload(h.d_tile_off, h.tile_off.data(), h.tile_off.size(), st))) return fail(s);
-    std::vector<int32_t> tc = h.tile_cmin;
-    if (tc.empty()) tc.push_back(0);
-    if ((s = upload(h.d_tile_cmin, tc.data(), tc.size(), st))) return fail(s);
-    std::vector<int32_t> ord = h.order;
-    if (ord.empty()) ord.push_back(0);
-    if ((s = upload(h.d_order, ord.data(), ord.size(), st))) return fail(s);
     if ((s = h.d_queue.resize(1))) return fail(s);
     if ((s = h.d_x.resize(std::max<size_t>(7 * h.P, 1)))) return fail(s);
     if ((s = h.d_xt.resize(std::max<size_t>(7 * h.P, 1)))) return fail(s);
     if ((s = h.d_prior.resize(std::max<size_t>(7 * windows, 1)))) return fail(s);
     if ((s = h.d_rel_z.resize(std::max<size_t>(7 * h.R, 1)))) return fail(s);
     if ((s = h.d_fac.resize(std::max<size_t>(FS * h.R, 1)))) return fail(s);
-    if ((s = h.d_pfac.resize(std::max<size_t>(PS * windows, 1)))) return fail(s);
-    if ((s = h.d_pa.resize(std::max<int64_t>(h.a_off[windows], 1)))) return fail(s);
-    if ((s = h.d_pb.resize(std::max<int64_t>(6 * h.sep_off[windows], 1)))) return fail(s);
     if ((s = h.d_reports.resize(std::max<size_t>(windows, 1)))) return fail(s);
     if (cudaStreamSynchronize(st) != cudaSuccess) return fail(cuda_status(cudaGetLastError(), "create"));
     *out = H;
@@ -967,6 +1120,69 @@ FG_API fg_status fg_windows_prior_layout(const fg_windows* H, uint64_t* separato
   }
   if (separators) std::copy(h.sep.begin(), h.sep.end(), separators);
   return FG_OK;
+}
+
+FG_API fg_status fg_windows_set_priors(fg_windows* H, const uint32_t* prior_poses, const uint32_t* prior_rows,
+                                       const double* A, const double* b, const double* refs) {
+  if (!H) return FG_NULL_ARGUMENT;
+  WindowsImpl& h = H->impl;
+  if (h.W && (!prior_poses || !prior_rows || !A || !b || !refs)) return FG_NULL_ARGUMENT;
+  try {
+    std::vector<int32_t> ps(h.W), pm(h.W);
+    size_t na = 0, nb = 0, nr = 0;
+    for (size_t w = 0; w < h.W; ++w) {
+      const int64_t n = h.pose_off[w + 1] - h.pose_off[w];
+      if (prior_poses[w] < 1 || prior_poses[w] > (uint32_t)PR_MAX_POSES || prior_poses[w] > n) {
+        set_error("a window prior covers 1 to min(64, window poses) poses");
+        return FG_DIMENSION_MISMATCH;
+      }
+      if (prior_rows[w] < 1 || prior_rows[w] > (uint32_t)PR_MAX_ROWS) {
+        set_error("a window prior has 1 to 384 rows");
+        return FG_DIMENSION_MISMATCH;
+      }
+      ps[w] = (int32_t)prior_poses[w];
+      pm[w] = (int32_t)prior_rows[w];
+      na += (size_t)pm[w] * 6 * ps[w];
+      nb += (size_t)pm[w];
+      nr += 7 * (size_t)ps[w];
+    }
+    for (size_t k = 0; k < na; ++k)
+      if (!std::isfinite(A[k])) {
+        set_error("nonfinite window prior matrix");
+        return FG_INVALID_EVALUATION;
+      }
+    for (size_t k = 0; k < nb; ++k)
+      if (!std::isfinite(b[k])) {
+        set_error("nonfinite window prior vector");
+        return FG_INVALID_EVALUATION;
+      }
+    FG_TRY(select_device(h.dev));
+    // keep the current priors until the new plan is known to be valid
+    auto keep_ps = h.ps, keep_pm = h.pm;
+    auto keep_a = h.prA, keep_b = h.prb, keep_r = h.pref;
+    const bool keep_custom = h.custom_priors;
+    h.ps = ps;
+    h.pm = pm;
+    h.prA.assign(A, A + na);
+    h.prb.assign(b, b + nb);
+    h.pref.assign(refs, refs + nr);
+    h.custom_priors = true;
+    fg_status s = plan_windows(h);
+    if (s != FG_OK) {
+      h.ps = keep_ps;
+      h.pm = keep_pm;
+      h.prA = keep_a;
+      h.prb = keep_b;
+      h.pref = keep_r;
+      h.custom_priors = keep_custom;
+      const fg_status s2 = plan_windows(h);
+      return s2 != FG_OK ? s2 : s;
+    }
+    return FG_OK;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return FG_OUT_OF_MEMORY;
+  }
 }
 
 FG_API fg_status fg_windows_upload(fg_windows* H, const double* poses, const double* priors, const double* rel_z) {

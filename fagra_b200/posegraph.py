@@ -185,13 +185,47 @@ class WindowSolver:
                                                ij.ctypes.data_as(C.POINTER(C.c_uint32)), removed,
                                                {"f64": 0, "f32": 1}[precision], device, C.byref(h)))
         self._h = h
-        so = np.zeros(batch.windows + 1, np.uint64)
-        ao = np.zeros(batch.windows + 1, np.uint64)
-        raise_for_status(lib.fg_windows_prior_layout(h, so.ctypes.data_as(u64), ao.ctypes.data_as(u64), None))
+        self._layout()
+
+    def _layout(self):
+        C, lib, h = self._C, self._lib, self._h
+        u64 = C.POINTER(C.c_uint64)
+        so = np.zeros(self.batch.windows + 1, np.uint64)
+        ao = np.zeros(self.batch.windows + 1, np.uint64)
+        self._raise(lib.fg_windows_prior_layout(h, so.ctypes.data_as(u64), ao.ctypes.data_as(u64), None))
         sep = np.zeros(max(int(so[-1]), 1), np.uint32)
-        raise_for_status(lib.fg_windows_prior_layout(h, None, None, sep.ctypes.data_as(C.POINTER(C.c_uint32))))
+        self._raise(lib.fg_windows_prior_layout(h, None, None, sep.ctypes.data_as(C.POINTER(C.c_uint32))))
         self.separator_offset, self.a_offset = so.astype(np.int64), ao.astype(np.int64)
         self.separators = sep[:int(so[-1])]
+
+    def set_priors(self, priors):
+        """Per window (A m x 6s, b m, refs s x 7): the prior r = b + sum_i A_i
+        Log(ref_i^-1 x_i) on its first s poses in place of the anchor
+        (Priors::update, src/marginalization.rs:157-231). The separator layout
+        is re-read: prior poses past the removed ones join the separator."""
+        C = self._C
+        if len(priors) != self.batch.windows:
+            raise ValueError("one prior per window")
+        ps, pm, As, bs, rs = [], [], [], [], []
+        for A, b, refs in priors:
+            A = np.asarray(A, np.float64)
+            refs = np.asarray(refs, np.float64).reshape(-1, 7)
+            m, s6 = A.shape
+            if s6 != 6 * len(refs):
+                raise ValueError("A needs 6 columns per reference pose")
+            ps.append(len(refs))
+            pm.append(m)
+            As.append(np.ascontiguousarray(A.T).reshape(-1))
+            bs.append(np.asarray(b, np.float64).reshape(-1))
+            rs.append(refs.reshape(-1))
+        cat = lambda v: np.ascontiguousarray(np.concatenate(v) if v else np.zeros(1))
+        psa, pma = np.asarray(ps, np.uint32), np.asarray(pm, np.uint32)
+        A, b, r = cat(As), cat(bs), cat(rs)
+        dp, u32 = C.POINTER(C.c_double), C.POINTER(C.c_uint32)
+        self._raise(self._lib.fg_windows_set_priors(self._h, psa.ctypes.data_as(u32), pma.ctypes.data_as(u32),
+                                                    A.ctypes.data_as(dp), b.ctypes.data_as(dp),
+                                                    r.ctypes.data_as(dp)))
+        self._layout()
 
     def close(self):
         if getattr(self, "_h", None):
@@ -253,6 +287,17 @@ class WindowSolver:
         A = a[int(self.a_offset[w]):int(self.a_offset[w]) + rows * cols].reshape(cols, rows).T.copy()
         return A, b[6 * s0:6 * s0 + rows].copy(), report.prior_constant
 
+    def slide(self, poses, reports, a, b):
+        """The next batch of a sliding window after this solve (slide_windows
+        over this solve's poses, separators and priors)."""
+        seps, pri = [], []
+        for w in range(self.batch.windows):
+            s0, s1 = int(self.separator_offset[w]), int(self.separator_offset[w + 1])
+            seps.append([int(k) for k in self.separators[s0:s1]])
+            A, bv, _ = self.prior(w, reports[w], a, b)
+            pri.append((A, bv))
+        return slide_windows(self.batch, self.removed, poses, seps, pri)
+
     def tuning(self):
         C = self._C
         panel, per = C.c_int(), C.c_int()
@@ -265,3 +310,42 @@ class WindowSolver:
         s = C.c_void_p()
         self._lib.fg_windows_stream(self._h, C.byref(s))
         return s.value or 0
+
+
+def slide_windows(batch: WindowBatch, removed: int, poses, separators, eliminations):
+    """The next batch of a sliding window: window w keeps its poses past the
+    `removed` oldest, separator poses first (in increasing order) then the
+    rest, with the relative factors among them re-indexed; initial estimates
+    are `poses` (the solve's result, all windows stacked); its prior is the
+    elimination (A, b) on the separator poses linearized at those poses — the
+    marginal prior of Priors::update (src/marginalization.rs:157-231).
+    Returns (WindowBatch, priors) for WindowSolver.set_priors."""
+    sizes, pose_rows, ij_rows, z_rows, priors, prior_x = [], [], [], [], [], []
+    rel_off = [0]
+    for w in range(batch.windows):
+        p0, p1 = int(batch.pose_offset[w]), int(batch.pose_offset[w + 1])
+        n = p1 - p0
+        rm = min(removed, n)
+        sep = list(separators[w])
+        if not sep:
+            raise ValueError("window %d keeps no separator pose" % w)
+        keep = set(sep)
+        order = sep + [k for k in range(rm, n) if k not in keep]
+        local = {k: i for i, k in enumerate(order)}
+        for f in range(int(batch.rel_offset[w]), int(batch.rel_offset[w + 1])):
+            i, j = (int(v) for v in batch.rel_ij[f])
+            if i >= rm and j >= rm:
+                ij_rows.append((local[i], local[j]))
+                z_rows.append(batch.rel_z[f])
+        rel_off.append(len(ij_rows))
+        x = np.asarray(poses[p0:p1], np.float64)[order]
+        sizes.append(len(order))
+        pose_rows.append(x)
+        A, bv = eliminations[w]
+        priors.append((np.asarray(A, np.float64), np.asarray(bv, np.float64), x[:len(sep)].copy()))
+        prior_x.append(x[0])
+    sizes = np.asarray(sizes, np.int64)
+    out = WindowBatch(sizes, np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64), np.concatenate(pose_rows),
+                      np.concatenate(pose_rows), np.asarray(prior_x, np.float64), np.asarray(rel_off, np.int64),
+                      np.asarray(ij_rows, np.uint32).reshape(-1, 2), np.asarray(z_rows, np.float64).reshape(-1, 7))
+    return out, priors

@@ -525,6 +525,20 @@ FG_API void fg_windows_destroy(fg_windows* batch);
  * matrix at a_offset[w] and its b starts at 6 * separator_offset[w]. */
 FG_API fg_status fg_windows_prior_layout(const fg_windows* batch, uint64_t* separator_offset,
                                          uint64_t* a_offset, uint32_t* separators);
+/* Replace every window's anchor prior by a general prior on its first
+ * prior_poses[w] poses (1 to min(64, window poses)) with prior_rows[w] rows
+ * (1 to 384): r = b + sum_i A_i Log(ref_i^-1 x_i), J_i = A_i Jr^-1(Log(ref_i^-1
+ * x_i)), the prior that Priors::update (src/marginalization.rs:157-231) feeds
+ * into the next solve of a chained window. Per window, concatenated in window
+ * order: A (prior_rows x 6 prior_poses, column-major — the layout
+ * fg_windows_download writes prior_a in, packed to prior_rows rows), b
+ * (prior_rows) and refs (7 per prior pose). The anchor is the case s = 1, A = I,
+ * b = 0, ref = the anchor pose, with the same results bit for bit. The priors
+ * argument of fg_windows_upload / fg_windows_solve is ignored after this call.
+ * Rejects nonfinite A or b (FG_INVALID_EVALUATION) and out-of-range shapes
+ * (FG_DIMENSION_MISMATCH), keeping the previous priors. */
+FG_API fg_status fg_windows_set_priors(fg_windows* batch, const uint32_t* prior_poses, const uint32_t* prior_rows,
+                                       const double* A, const double* b, const double* refs);
 /* Host -> device inputs, the device-only solve, device -> host results. */
 FG_API fg_status fg_windows_upload(fg_windows* batch, const double* poses, const double* priors,
                                    const double* rel_z);

@@ -409,3 +409,34 @@ def test_window_prior_generalizes_the_anchor_and_follows_priors_update():
     st0, c_rel = oracle.window_cost(poses, prior, ij, z, marginal=(np.zeros((1, 6)), np.zeros(1), prior[None, :]))
     assert st0 == 0
     assert abs(c - (c_rel + 0.5 * r @ r)) <= 1e-12 * c
+
+
+def test_sliding_window_chain_on_the_oracle():
+    """One sliding-window step on the oracle: the retained poses with the
+    marginal prior (separators first) solve to a finite cost no worse than the
+    prior-free restart's prior term, and the elimination of the next window
+    succeeds with its separator inside the window."""
+    from fagra_b200 import posegraph
+    batch = posegraph.generate(3, min_poses=32, max_poses=44, seed=23)
+    poses = batch.poses.copy()
+    seps, elims = [], []
+    for w in range(batch.windows):
+        x, pr, ij, z = batch.window(w)
+        r = oracle.window_solve(x, pr, ij, z, removed=10)
+        assert r["code"] in (0, 9, 10)
+        poses[batch.pose_offset[w]:batch.pose_offset[w + 1]] = r["poses"]
+        seps.append(list(r["separator"]))
+        elims.append((r["prior_a"], r["prior_b"]))
+    nb, priors = posegraph.slide_windows(batch, 10, poses, seps, elims)
+    for w in range(nb.windows):
+        x, pr, ij, z = nb.window(w)
+        assert len(x) == batch.sizes[w] - 10
+        # at the linearization point the marginal prior's residual is b
+        st, c = oracle.window_cost(x, pr, ij, z, marginal=priors[w])
+        A, bv, refs = priors[w]
+        st0, c0 = oracle.window_cost(x, pr, ij, z, marginal=(np.zeros((1, A.shape[1])), np.zeros(1), refs))
+        assert st == 0 and st0 == 0
+        assert abs(c - (c0 + 0.5 * bv @ bv)) <= 1e-10 * max(c, 1.0)
+        r = oracle.window_solve(x, pr, ij, z, removed=10, marginal=priors[w])
+        assert r["code"] in (0, 9, 10) and r["rank"] > 0
+        assert r["stats"].cost <= c + 1e-12
