@@ -1,6 +1,6 @@
 // Learned block preconditioner: a message-passing network over the camera
 // covisibility graph of the reduced camera system, with BF16 tensor-core GEMMs
-// (mma.sync m16n8k16, FP32 accumulation) for inference and training, Adam on
+// (tcgen05.mma, FP32 accumulation in tensor memory) for inference and training, Adam on
 // the device, and the feature / probe kernels that turn a Schur backend's
 // factors into training systems. fagra has no learned preconditioner; the
 // network reshapes the retained block-Jacobi preconditioner of
@@ -16,6 +16,7 @@
 //   head      A_c = I + 0.1 tril(O_c), M_c = L_c^-T (A_c A_c^T + 1e-3 I) L_c^-1 (SPD);
 //   loss      mean ||x - M_hat S_hat x||^2 over whitened probes x.
 #include "gnn.cuh"
+#include "umma.cuh"
 #include <cuda_bf16.h>
 #include <algorithm>
 #include <memory>
@@ -50,9 +51,13 @@ struct PLayout {
 
 // ------------------------------------------------------------------ GEMM
 // C (M x N) = op(A) (M x K) * op(B) (K x N); A(m,k) = TRA ? A[k*lda+m] : A[m*lda+k],
-// B(k,n) = TRB ? B[n*ldb+k] : B[k*ldb+n]. Operands are rounded to bf16 into
-// shared memory; 64x64 CTA tile, 4 warps of 32x32, K step 32; split-K over
-// gridDim.z (EPI_STORE only, atomic accumulation into C).
+// B(k,n) = TRB ? B[n*ldb+k] : B[k*ldb+n], on the fifth-generation tensor cores:
+// operands rounded to bf16 into 128-byte-swizzled K-major shared-memory tiles
+// (two stages of 128 x 64 A and 64 x 64 B), tcgen05.mma M=128 N=64 K=16 issued
+// by one thread with the FP32 accumulator in tensor memory (64 columns), each
+// stage released by a tcgen05.commit on its mbarrier, the accumulator read back
+// with tcgen05.ld (thread = row) for the fused epilogue. Split-K over gridDim.z
+// (EPI_STORE only, atomic accumulation into C).
 enum Epilogue { EPI_STORE = 0, EPI_BIAS_RELU = 1, EPI_BIAS = 2, EPI_SPLIT = 3, EPI_STORE_MASK = 4 };
 struct Epi {
   const float* bias = nullptr;
@@ -73,134 +78,206 @@ struct Epi {
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+constexpr int UM = 128, UN = 64, UK = 64;
+constexpr int UTILE_A = UM * UK * 2, UTILE_B = UN * UK * 2;  // bytes of one stage's tiles
+constexpr size_t UMMA_SMEM = 2 * (UTILE_A + UTILE_B) + 1024;  // two stages + alignment slack
+constexpr uint32_t UIDESC = umma_idesc_bf16_f32(UM, UN);
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+// 8 consecutive elements of a row (contiguous in memory) as bf16; vec when the
+// 8 are inside the chunk and 16-byte loads are aligned, else guarded scalars.
+template <class T>
+__device__ __forceinline__ uint4 load8(const T* p, int valid, bool vec);
+template <>
+__device__ __forceinline__ uint4 load8<float>(const float* p, int valid, bool vec) {
+  float v[8];
+  if (vec && valid >= 8) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = i < valid ? p[i] : 0.f;
+  }
+  return make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
+}
+template <>
+__device__ __forceinline__ uint4 load8<__nv_bfloat16>(const __nv_bfloat16* p, int valid, bool vec) {
+  if (vec && valid >= 8) return __ldg(reinterpret_cast<const uint4*>(p));
+  uint16_t h[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) h[i] = i < valid ? *reinterpret_cast<const uint16_t*>(p + i) : (uint16_t)0;
+  return make_uint4(h[0] | ((uint32_t)h[1] << 16), h[2] | ((uint32_t)h[3] << 16), h[4] | ((uint32_t)h[5] << 16),
+                    h[6] | ((uint32_t)h[7] << 16));
 }
 
-constexpr int GT = 64, GK = 32, GPAD = 40;
+// One operand tile of R rows x UK columns of K into swizzled shared memory:
+// element (row, k) = src(r0 + row, k0 + k); KCONTIG: src(r, k) = src[r*ld + k]
+// (16-byte chunks along K), else src[k*ld + r] (8 rows per thread, scattered
+// 2-byte stores). Rows >= rows and k >= kend are zero.
+template <int R, bool KCONTIG, class T>
+__device__ __forceinline__ void load_tile(uint8_t* tile, const T* src, int ld, int r0, int rows, int k0, int kend,
+                                          bool vec) {
+  constexpr int CH = R * UK / 8;  // 16-byte chunks
+#pragma unroll 4
+  for (int q = threadIdx.x; q < CH; q += 128) {
+    if (KCONTIG) {
+      const int row = q >> 3, kq = (q & 7) * 8;
+      const int gr = r0 + row, gk = k0 + kq;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (gr < rows && gk < kend) v = load8<T>(src + (size_t)gr * ld + gk, kend - gk, vec);
+      *reinterpret_cast<uint4*>(tile + umma_sw128_offset(row, kq)) = v;
+    } else {
+      const int rq = (q % (R / 8)) * 8, k = q / (R / 8);
+      const int gr = r0 + rq, gk = k0 + k;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (gk < kend && gr < rows) v = load8<T>(src + (size_t)gk * ld + gr, rows - gr, vec);
+      const uint16_t* h = reinterpret_cast<const uint16_t*>(&v);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) *reinterpret_cast<uint16_t*>(tile + umma_sw128_offset(rq + i, k)) = h[i];
+    }
+  }
+}
 
 template <class TA, class TB, bool TRA, bool TRB, int EPI>
-__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const TA* __restrict__ A, int lda,
-                                              const TB* __restrict__ B, int ldb, float* __restrict__ Cm, int ldc,
-                                              Epi ep, int kchunk) {
-  __shared__ __align__(16) __nv_bfloat16 As[GT][GPAD];
-  __shared__ __align__(16) __nv_bfloat16 Bs[GT][GPAD];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
+__global__ void __launch_bounds__(128, 1) k_gemm(int M, int N, int K, const TA* __restrict__ A, int lda,
+                                                 const TB* __restrict__ B, int ldb, float* __restrict__ Cm, int ldc,
+                                                 Epi ep, int kchunk, int vec_a, int vec_b, int* err) {
+  extern __shared__ uint8_t gemm_smem[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  uint8_t* base = reinterpret_cast<uint8_t*>(((uintptr_t)gemm_smem + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * UM, n0 = blockIdx.y * UN;
   const int kb = blockIdx.z * kchunk;
   const int ke = min(K, kb + kchunk);
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int g = lane >> 2, t = lane & 3;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
-  for (int k0 = kb; k0 < ke; k0 += GK) {
-#pragma unroll 4
-    for (int j = 0; j < GT * GK / 128; ++j) {
-      const int i = tid + 128 * j;
-      const int m = TRA ? (i & 63) : (i >> 5);
-      const int k = TRA ? (i >> 6) : (i & 31);
-      const int gm = m0 + m, gk = k0 + k;
-      float v = 0.f;
-      if (gm < M && gk < ke) v = to_f(TRA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]);
-      As[m][k] = __float2bfloat16_rn(v);
-    }
-#pragma unroll 4
-    for (int j = 0; j < GT * GK / 128; ++j) {
-      const int i = tid + 128 * j;
-      const int n = TRB ? (i >> 5) : (i & 63);
-      const int k = TRB ? (i & 31) : (i >> 6);
-      const int gn = n0 + n, gk = k0 + k;
-      float v = 0.f;
-      if (gn < N && gk < ke) v = to_f(TRB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn]);
-      Bs[n][k] = __float2bfloat16_rn(v);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int ks = 0; ks < GK; ks += 16) {
-      uint32_t a[2][4], b[4][2];
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi) {
-        const int r = wm + mi * 16 + g;
-        a[mi][0] = *reinterpret_cast<const uint32_t*>(&As[r][ks + 2 * t]);
-        a[mi][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][ks + 2 * t]);
-        a[mi][2] = *reinterpret_cast<const uint32_t*>(&As[r][ks + 2 * t + 8]);
-        a[mi][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][ks + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const int c = wn + ni * 8 + g;
-        b[ni][0] = *reinterpret_cast<const uint32_t*>(&Bs[c][ks + 2 * t]);
-        b[ni][1] = *reinterpret_cast<const uint32_t*>(&Bs[c][ks + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], a[mi], b[ni]);
-    }
-    __syncthreads();
+  const int nchunks = ke > kb ? (ke - kb + UK - 1) / UK : 0;
+  const uint32_t bar0 = umma_smem_addr(&mbar[0]), bar1 = umma_smem_addr(&mbar[1]);
+  if (warp == 0) {
+    tmem_alloc(umma_smem_addr(&tmem_base), UN);
+    tmem_relinquish();
   }
+  if (tid == 0) {
+    umma_mbar_init(bar0, 1);
+    umma_mbar_init(bar1, 1);
+    umma_mbar_init_fence();
+  }
+  tcgen05_before_sync();
+  __syncthreads();
+  tcgen05_after_sync();
+  const uint32_t tmem = tmem_base;
+  bool ok = true;
+  int issued = 0;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c & 1;
+    if (c >= 2) ok = umma_wait(s ? bar1 : bar0, ((c - 2) >> 1) & 1, err);
+    if (!__syncthreads_and(ok)) break;  // stage s is free again (or the wait gave up everywhere)
+    const int k0 = kb + c * UK;
+    uint8_t* sa = base + s * UTILE_A;
+    uint8_t* sb = base + 2 * UTILE_A + s * UTILE_B;
+    load_tile<UM, !TRA>(sa, A, lda, m0, M, k0, ke, vec_a != 0);
+    load_tile<UN, TRB>(sb, B, ldb, n0, N, k0, ke, vec_b != 0);
+    umma_fence_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tcgen05_after_sync();
+      const uint32_t a0 = umma_smem_addr(sa), b0 = umma_smem_addr(sb);
+#pragma unroll
+      for (int kk = 0; kk < UK / 16; ++kk)
+        umma_bf16(tmem, umma_desc_sw128(a0 + 32 * kk), umma_desc_sw128(b0 + 32 * kk), UIDESC, (c | kk) != 0);
+      umma_commit(s ? bar1 : bar0);
+    }
+    issued = c + 1;
+  }
+  // every issued MMA has completed once the last commits of both stages arrived
+  bool done = true;
+  if (issued >= 1) done = umma_wait(((issued - 1) & 1) ? bar1 : bar0, ((issued - 1) >> 1) & 1, err) && done;
+  if (issued >= 2) done = umma_wait(((issued - 2) & 1) ? bar1 : bar0, ((issued - 2) >> 1) & 1, err) && done;
+  done = __syncthreads_and(done && issued == nchunks);
+  tcgen05_after_sync();
+  uint32_t r[2][32];
+  if (done && nchunks > 0) {
+    const uint32_t row_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    tmem_ld32(row_addr, r[0]);
+    tmem_ld32(row_addr + 32, r[1]);
+    tmem_wait_ld();
+  } else {
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int j = 0; j < 32; ++j) r[h][j] = 0u;
+  }
+  tcgen05_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tcgen05_after_sync();
+    tmem_dealloc(tmem, UN);
+  }
+  if (!done) return;  // the error flag is set; nothing is written
+  const int m = m0 + warp * 32 + lane;
+  if (m >= M) return;
   const bool split = gridDim.z > 1;
 #pragma unroll
-  for (int mi = 0; mi < 2; ++mi)
+  for (int h = 0; h < 2; ++h)
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int m = m0 + wm + mi * 16 + g + (q >> 1) * 8;
-        const int n = n0 + wn + ni * 8 + 2 * t + (q & 1);
-        if (m >= M || n >= N) continue;
-        const float v = acc[mi][ni][q];
-        if (EPI == EPI_STORE) {
-          float* c = Cm + (size_t)m * ldc + n;
-          if (split) atomicAdd(c, v);
-          else *c = ep.accumulate ? *c + v : v;
-        } else if (EPI == EPI_BIAS_RELU) {
-          const float z = v + ep.bias[n];
-          ep.z[(size_t)m * ep.ldz + n] = z;
-          const float res = ep.r ? ep.r[(size_t)m * ep.ldr + n] : 0.f;
-          ep.h[(size_t)m * ep.ldh + n] = res + fmaxf(z, 0.f);
-        } else if (EPI == EPI_BIAS) {
-          Cm[(size_t)m * ldc + n] = v + ep.bias[n];
-        } else if (EPI == EPI_SPLIT) {
-          if (n < ep.split_at) Cm[(size_t)m * ldc + n] = v + ep.r[(size_t)m * ep.ldr + n];
-          else ep.h[(size_t)m * ep.ldh + (n - ep.split_at)] = v;
-        } else if (EPI == EPI_STORE_MASK) {
-          Cm[(size_t)m * ldc + n] = v;
-          ep.d2[(size_t)m * ep.ldd2 + n] = ep.zmask[(size_t)m * ep.ldzm + n] > 0.f ? v : 0.f;
-        }
+    for (int j = 0; j < 32; ++j) {
+      const int n = n0 + 32 * h + j;
+      if (n >= N) continue;
+      const float v = __uint_as_float(r[h][j]);
+      if (EPI == EPI_STORE) {
+        float* c = Cm + (size_t)m * ldc + n;
+        if (split) atomicAdd(c, v);
+        else *c = ep.accumulate ? *c + v : v;
+      } else if (EPI == EPI_BIAS_RELU) {
+        const float z = v + ep.bias[n];
+        ep.z[(size_t)m * ep.ldz + n] = z;
+        const float res = ep.r ? ep.r[(size_t)m * ep.ldr + n] : 0.f;
+        ep.h[(size_t)m * ep.ldh + n] = res + fmaxf(z, 0.f);
+      } else if (EPI == EPI_BIAS) {
+        Cm[(size_t)m * ldc + n] = v + ep.bias[n];
+      } else if (EPI == EPI_SPLIT) {
+        if (n < ep.split_at) Cm[(size_t)m * ldc + n] = v + ep.r[(size_t)m * ep.ldr + n];
+        else ep.h[(size_t)m * ep.ldh + (n - ep.split_at)] = v;
+      } else if (EPI == EPI_STORE_MASK) {
+        Cm[(size_t)m * ldc + n] = v;
+        ep.d2[(size_t)m * ep.ldd2 + n] = ep.zmask[(size_t)m * ep.ldzm + n] > 0.f ? v : 0.f;
       }
+    }
+}
+
+template <class T>
+bool vec16(const T* p, int ld) {
+  constexpr int per = 16 / (int)sizeof(T);
+  return ((uintptr_t)p % 16) == 0 && ld % per == 0;
 }
 
 template <class TA, class TB, bool TRA, bool TRB, int EPI>
 fg_status gemm(cudaStream_t st, int nsm, int M, int N, int K, const TA* A, int lda, const TB* B, int ldb, float* Cm,
-               int ldc, const Epi& ep, bool allow_split) {
+               int ldc, const Epi& ep, bool allow_split, int* err) {
   if (M <= 0 || N <= 0) return FG_OK;
-  const unsigned gx = (unsigned)((M + GT - 1) / GT), gy = (unsigned)((N + GT - 1) / GT);
+  const unsigned gx = (unsigned)((M + UM - 1) / UM), gy = (unsigned)((N + UN - 1) / UN);
   int splits = 1;
-  if (allow_split && EPI == EPI_STORE && K > 256) {
+  if (allow_split && EPI == EPI_STORE && K > 2 * UK) {
     const int want = std::max(1, (2 * nsm) / (int)(gx * gy));
-    splits = std::min(want, (K + 255) / 256);
+    splits = std::min(want, (K + UK - 1) / UK);
   }
   int kchunk = (K + splits - 1) / splits;
-  kchunk = std::max(GK, (kchunk + GK - 1) / GK * GK);
+  kchunk = std::max(UK, (kchunk + UK - 1) / UK * UK);
   splits = std::max(1, (K + kchunk - 1) / kchunk);
   if (K <= 0) {  // empty reduction: the product is zero
     splits = 1;
-    kchunk = GK;
+    kchunk = UK;
   }
   if (EPI == EPI_STORE && splits > 1 && !ep.accumulate)
     FG_CUDA(cudaMemset2DAsync(Cm, (size_t)ldc * sizeof(float), 0, (size_t)N * sizeof(float), (size_t)M, st));
+  auto kern = k_gemm<TA, TB, TRA, TRB, EPI>;
+  FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UMMA_SMEM));
+  // 16-byte loads need aligned rows: along K for K-contiguous operands, along M / N otherwise
+  const int va = vec16(A, lda) ? 1 : 0, vb = vec16(B, ldb) ? 1 : 0;
   dim3 grid(gx, gy, (unsigned)splits);
-  FG_LAUNCH((k_gemm<TA, TB, TRA, TRB, EPI>), grid, 128, 0, st, M, N, K, A, lda, B, ldb, Cm, ldc, ep, kchunk);
+  FG_LAUNCH(kern, grid, 128, UMMA_SMEM, st, M, N, K, A, lda, B, ldb, Cm, ldc, ep, kchunk, va, vb, err);
   return FG_OK;
 }
 
@@ -412,9 +489,20 @@ __global__ void k_edge_k(Layout L, int64_t nedges, const DEdgeMeta* edges, const
   for (int k = 0; k < 16; ++k) out[k] = k < pw * pw ? (float)K[k] : 0.f;
 }
 
+// Pair weights are summed in 64-bit fixed point (2^-36 units), so the
+// covisibility matrix does not depend on the order of the atomic additions.
+// Each weight is a trace of a product of two PSD matrices whose eigenvalues
+// are at most 1 in the whitened coordinates (E (C + lambda)^-1 E^T <= B), so
+// a pair adds at most pw <= 4; weights are clamped to [0, 64] before the
+// conversion, which keeps 2^27 pairs per camera pair away from overflow.
+constexpr double PAIR_SCALE = 68719476736.0;  // 2^36
+__device__ __forceinline__ unsigned long long pair_fixed(double w) {
+  return (unsigned long long)__double2ll_rn(fmin(fmax(w, 0.0), 64.0) * PAIR_SCALE);
+}
+
 // Pair weights w_ij += <K_e, K_f> over the edge pairs of each point (warp per point).
 __global__ void k_pairs(int64_t nP, int64_t nC, const int64_t* pt_edge_off, const int64_t* pt_edge,
-                        const DEdgeMeta* edges, const float* Kin, int pw, float* adj) {
+                        const DEdgeMeta* edges, const float* Kin, int pw, unsigned long long* adj) {
   const int lane = threadIdx.x & 31;
   const int64_t pt = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   if (pt >= nP) return;
@@ -431,23 +519,27 @@ __global__ void k_pairs(int64_t nP, int64_t nC, const int64_t* pt_edge_off, cons
       if (ci == cj) continue;
       float w = 0.f;
       for (int k = 0; k < nk; ++k) w += ka[k] * Kin[f * 16 + k];
-      atomicAdd(adj + (int64_t)ci * nC + cj, w);
-      atomicAdd(adj + (int64_t)cj * nC + ci, w);
+      const unsigned long long q = pair_fixed((double)w);
+      atomicAdd(adj + (int64_t)ci * nC + cj, q);
+      atomicAdd(adj + (int64_t)cj * nC + ci, q);
     }
   }
 }
 
-// Row-normalized sqrt weights in bf16, plus features 45 (log1p degree / 4) and
-// 46 (log1p coupling) of observed cameras. Block of 256 per row.
-__global__ void k_normalize(int64_t nC, const float* adj, const uint8_t* mask, float* X0, __nv_bfloat16* Abf) {
+// Row-normalized sqrt weights in bf16 (row stride lda, zero past column nC),
+// plus features 45 (log1p degree / 4) and 46 (log1p coupling) of observed
+// cameras; the fixed-point row is cleared for the next system. Block of 256
+// per row, sums in a fixed order.
+__global__ void k_normalize(int64_t nC, int64_t lda, unsigned long long* adj, const uint8_t* mask, float* X0,
+                            __nv_bfloat16* Abf) {
   const int64_t i = blockIdx.x;
-  const float* row = adj + i * nC;
+  unsigned long long* row = adj + i * nC;
   double s = 0;
   int cnt = 0;
   for (int64_t j = threadIdx.x; j < nC; j += blockDim.x) {
-    const float w = row[j];
-    if (w > 0.f) {
-      s += sqrt((double)w);
+    const unsigned long long v = row[j];
+    if (v) {
+      s += sqrt((double)v / PAIR_SCALE);
       ++cnt;
     }
   }
@@ -465,13 +557,229 @@ __global__ void k_normalize(int64_t nC, const float* adj, const uint8_t* mask, f
   }
   const double tot = ss[0];
   const double inv = tot > 0 ? 1.0 / tot : 0.0;
-  for (int64_t j = threadIdx.x; j < nC; j += blockDim.x) {
-    const float w = row[j];
-    Abf[i * nC + j] = __float2bfloat16_rn(w > 0.f ? (float)(sqrt((double)w) * inv) : 0.f);
+  for (int64_t j = threadIdx.x; j < lda; j += blockDim.x) {
+    float a = 0.f;
+    if (j < nC) {
+      const unsigned long long v = row[j];
+      if (v) a = (float)(sqrt((double)v / PAIR_SCALE) * inv);
+      row[j] = 0;
+    }
+    Abf[i * lda + j] = __float2bfloat16_rn(a);
   }
   if (threadIdx.x == 0 && mask[i]) {
     X0[i * NF + 45] = (float)(log1p((double)sc[0]) / 4.0);
     X0[i * NF + 46] = (float)log1p(tot);
+  }
+}
+
+// ---- the 9/3 (BAL) feature pass, the same quantities in three kernels that
+// read every edge once. V_e = E_e L_p^-T (so V_e V_e^T = E_e C_p^-1 E_e^T) and
+// G_e = L_c^-1 V_e (so K_e = G_e^T G_e); unobserved variables use
+// L = sqrt(lambda) I as above.
+
+// Thread per edge in the point-sorted order of pt_edge: E_e from the edge
+// records (28 words, position k) or the cross array (27 words, edge e); V_e by
+// edge (column-major 9 x 3) and, by position, K_e lower (6 floats) with the
+// camera index in slot 6 (8 floats per edge).
+template <class TS>
+__global__ void __launch_bounds__(128) k_gnn_edge93(Layout L, int64_t nedges, const TS* src, int by_edge,
+                                                    const int64_t* pt_edge, const DEdgeMeta* edges,
+                                                    const uint8_t* observed, const TS* factors, double lambda, TS* V,
+                                                    float* Kout) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= nedges) return;
+  const int64_t e = pt_edge[k];
+  const int2 cp = *reinterpret_cast<const int2*>(edges + e);
+  const TS* E = src + (by_edge ? e * 27 : k * 28);
+  double v[27];  // v[q * 9 + c] = V(c, q)
+  const bool pobs = observed[L.nC + cp.y];
+  const TS* lp = factors + L.gram_offset(L.nC + cp.y);
+  double p00 = 0, p10 = 0, p20 = 0, p11 = 0, p21 = 0, p22 = 0;
+  if (pobs) {
+    p00 = (double)lp[0]; p10 = (double)lp[1]; p20 = (double)lp[2];
+    p11 = (double)lp[4]; p21 = (double)lp[5]; p22 = (double)lp[8];
+  }
+  const double isl = 1.0 / sqrt(lambda);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const double e0 = (double)E[c], e1 = (double)E[9 + c], e2 = (double)E[18 + c];
+    if (pobs) {  // row c of E times L_p^-T: solve L_p y = E(c, :)^T
+      const double y0 = e0 / p00;
+      const double y1 = (e1 - p10 * y0) / p11;
+      const double y2 = (e2 - p20 * y0 - p21 * y1) / p22;
+      v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
+    } else {
+      v[c] = e0 * isl; v[9 + c] = e1 * isl; v[18 + c] = e2 * isl;
+    }
+  }
+  TS* vo = V + e * 27;
+#pragma unroll
+  for (int i = 0; i < 27; ++i) vo[i] = (TS)v[i];
+  float4* ko = reinterpret_cast<float4*>(Kout + k * 8);
+  if (!observed[cp.x]) {
+    ko[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    ko[1] = make_float4(0.f, 0.f, __int_as_float(cp.x), 0.f);
+    return;
+  }
+  const TS* lc = factors + L.gram_offset(cp.x);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {  // column q of G = L_c^-1 V
+    double* g = v + 9 * q;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      double s = g[i];
+#pragma unroll
+      for (int j = 0; j < i; ++j) s -= (double)lc[j * 9 + i] * g[j];
+      g[i] = s / (double)lc[i * 9 + i];
+    }
+  }
+  double K[6];  // K00, K10, K20, K11, K21, K22
+  int idx = 0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int r = q; r < 3; ++r) {
+      double s = 0;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) s += v[9 * r + c] * v[9 * q + c];
+      K[idx++] = s;
+    }
+  ko[0] = make_float4((float)K[0], (float)K[1], (float)K[2], (float)K[3]);
+  ko[1] = make_float4((float)K[4], (float)K[5], __int_as_float(cp.x), 0.f);
+}
+
+// Block of 128 per camera: U = sum_e V_e V_e^T over the camera's edges, then
+// P = L_c^-1 U L_c^-T and the node-feature row as k_node_features writes it.
+template <class TS>
+__global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge,
+                                                    const TS* V, const uint8_t* observed, const TS* factors,
+                                                    double lambda, float* X0, uint8_t* mask) {
+  const int64_t cam = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float* row = X0 + cam * NF;
+  if (!observed[cam]) {
+    if (tid == 0) mask[cam] = 0;
+    if (tid < NF) row[tid] = tid == 49 ? 1.f : 0.f;
+    return;
+  }
+  double acc[45];
+#pragma unroll
+  for (int i = 0; i < 45; ++i) acc[i] = 0;
+  for (int64_t k = cam_edge_off[cam] + tid; k < cam_edge_off[cam + 1]; k += 128) {
+    const TS* v = V + cam_edge[k] * 27;
+    double w[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) w[i] = (double)v[i];
+    int idx = 0;
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+#pragma unroll
+      for (int r = c; r < 9; ++r) acc[idx++] += w[r] * w[c] + w[9 + r] * w[9 + c] + w[18 + r] * w[18 + c];
+  }
+  __shared__ double red[4][45];
+  __shared__ double U[81], W[81];
+#pragma unroll
+  for (int i = 0; i < 45; ++i) {
+    const double s = lane_allsum(acc[i]);
+    if (lane == 0) red[warp][i] = s;
+  }
+  __syncthreads();
+  const TS* lc = factors + L.gram_offset(cam);
+  if (tid < 45) {
+    const double s = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+    int c = 0, r = tid;  // lower entry tid (column-major) -> (r, c)
+    while (r >= 9 - c) {
+      r -= 9 - c;
+      ++c;
+    }
+    r += c;
+    U[c * 9 + r] = s;
+    U[r * 9 + c] = s;
+  }
+  __syncthreads();
+  if (tid < 9) {  // W = L^-1 U, column tid
+    double x[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) x[i] = U[tid * 9 + i];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      double s = x[i];
+#pragma unroll
+      for (int j = 0; j < i; ++j) s -= (double)lc[j * 9 + i] * x[j];
+      x[i] = s / (double)lc[i * 9 + i];
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) W[tid * 9 + i] = x[i];
+  }
+  __syncthreads();
+  if (tid < 9) {  // P = L^-1 W^T, column tid (row tid of W)
+    double x[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) x[i] = W[i * 9 + tid];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      double s = x[i];
+#pragma unroll
+      for (int j = 0; j < i; ++j) s -= (double)lc[j * 9 + i] * x[j];
+      x[i] = s / (double)lc[i * 9 + i];
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) U[tid * 9 + i] = x[i];  // U now holds P (column-major)
+  }
+  __syncthreads();
+  if (tid < NF) {
+    float f = 0.f;
+    if (tid < 45) {
+      int c = 0, r = tid;
+      while (r >= 9 - c) {
+        r -= 9 - c;
+        ++c;
+      }
+      r += c;
+      f = (float)(0.5 * (U[c * 9 + r] + U[r * 9 + c]));
+    } else if (tid == 47) {
+      f = (float)(log10(fmax(lambda, 1e-12)) / 12.0);
+    } else if (tid == 48) {
+      double tr = 0;
+      for (int c = 0; c < 9; ++c) tr += U[c * 9 + c];
+      f = (float)(tr / 9);
+    } else if (tid == 49) {
+      f = 1.f;
+    }
+    if (tid != 45 && tid != 46) row[tid] = f;  // 45 and 46 are k_normalize's
+  }
+  if (tid == 0) mask[cam] = 1;
+}
+
+// Warp per point: the pairs (a, b) of its edges spread over the lanes;
+// w = <K_a, K_b>_F into the fixed-point covisibility of both orders.
+__global__ void __launch_bounds__(128) k_gnn_pairs93(int64_t nP, int64_t nC, const int64_t* pt_edge_off,
+                                                     const float* Kin, unsigned long long* adj) {
+  const int lane = threadIdx.x & 31;
+  const int64_t pt = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (pt >= nP) return;
+  const int64_t o = pt_edge_off[pt];
+  const int64_t t = pt_edge_off[pt + 1] - o;
+  const int64_t np = t * (t - 1) / 2;
+  for (int64_t q = lane; q < np; q += 32) {
+    int64_t a = 0, r = q;
+    while (r >= t - 1 - a) {
+      r -= t - 1 - a;
+      ++a;
+    }
+    const int64_t b = a + 1 + r;
+    const float4* ka = reinterpret_cast<const float4*>(Kin + (o + a) * 8);
+    const float4* kb = reinterpret_cast<const float4*>(Kin + (o + b) * 8);
+    const float4 a0 = ka[0], a1 = ka[1], b0 = kb[0], b1 = kb[1];
+    const int ci = __float_as_int(a1.z), cj = __float_as_int(b1.z);
+    if (ci == cj) continue;
+    const double w = (double)a0.x * b0.x + (double)a0.w * b0.w + (double)a1.y * b1.y +
+                     2.0 * ((double)a0.y * b0.y + (double)a0.z * b0.z + (double)a1.x * b1.x);
+    const unsigned long long fx = pair_fixed(w);
+    if (fx) {
+      atomicAdd(adj + (int64_t)ci * nC + cj, fx);
+      atomicAdd(adj + (int64_t)cj * nC + ci, fx);
+    }
   }
 }
 
@@ -488,6 +796,98 @@ __device__ __forceinline__ void head_metric(const double* A, int cw, double* Mh)
       double s = 0;
       for (int k = 0; k < cw; ++k) s += A[i * cw + k] * A[j * cw + k];
       Mh[i * cw + j] = s + (i == j ? (double)EPSILON : 0.0);
+    }
+}
+
+// The 9-wide head as k_head_minv below, warp per camera with the 9 x 9
+// products spread over the lanes (shared memory per warp).
+template <class TS>
+__global__ void __launch_bounds__(128) k_head_minv93(Layout L, const float* O, const uint8_t* mask,
+                                                     const TS* factors, TS* minv, unsigned* nonfinite) {
+  __shared__ double sh[4][4][81];  // per warp: A (row-major), Li (row-major), Mh, T
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t cam = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (cam >= L.nC || !mask[cam]) return;  // uniform across the warp
+  double* A = sh[warp][0];
+  double* Li = sh[warp][1];
+  double* Mh = sh[warp][2];
+  double* T = sh[warp][3];
+  const float* o = O + cam * NH;
+  for (int k = lane; k < 81; k += 32) A[k] = 0;
+  __syncwarp();
+  if (lane < 45) {
+    int c = 0, r = lane;
+    while (r >= 9 - c) {
+      r -= 9 - c;
+      ++c;
+    }
+    r += c;
+    A[r * 9 + c] = (double)OUT_SCALE * (double)o[lane];
+  }
+  __syncwarp();
+  if (lane < 9) A[lane * 9 + lane] += 1.0;
+  const TS* l = factors + L.gram_offset(cam);
+  if (lane < 9) {  // column lane of L^-1
+    double x[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      double s = i == lane ? 1.0 : 0.0;
+#pragma unroll
+      for (int j = 0; j < i; ++j) s -= (double)l[j * 9 + i] * x[j];
+      x[i] = s / (double)l[i * 9 + i];
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Li[i * 9 + lane] = x[i];
+  }
+  __syncwarp();
+  for (int e = lane; e < 81; e += 32) {  // Mh = A A^T + eps I
+    const int i = e / 9, j = e % 9;
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s += A[i * 9 + k] * A[j * 9 + k];
+    Mh[e] = s + (i == j ? (double)EPSILON : 0.0);
+  }
+  __syncwarp();
+  for (int e = lane; e < 81; e += 32) {  // T = Mh L^-1
+    const int a = e / 9, j = e % 9;
+    double t = 0;
+#pragma unroll
+    for (int b = 0; b < 9; ++b) t += Mh[a * 9 + b] * Li[b * 9 + j];
+    T[e] = t;
+  }
+  __syncwarp();
+  double out[2];
+  int pi[2], pj[2];
+  bool ok = true;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {  // upper pairs (i <= j) lane and lane + 32
+    const int p = lane + 32 * u;
+    pi[u] = -1;
+    if (p >= 45) continue;
+    int i = 0, r = p;
+    while (r >= 9 - i) {
+      r -= 9 - i;
+      ++i;
+    }
+    const int j = i + r;
+    double s = 0;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) s += Li[a * 9 + i] * T[a * 9 + j];
+    ok = ok && isfinite(s);
+    out[u] = s;
+    pi[u] = i;
+    pj[u] = j;
+  }
+  if (__any_sync(0xffffffffu, !ok)) {
+    if (lane == 0) atomicAdd(nonfinite, 1u);
+    return;
+  }
+  TS* dst = minv + cam * 81;
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+    if (pi[u] >= 0) {
+      dst[pi[u] * 9 + pj[u]] = (TS)out[u];
+      dst[pj[u] * 9 + pi[u]] = (TS)out[u];
     }
 }
 
@@ -625,6 +1025,7 @@ __global__ void k_whiten(Layout L, const uint8_t* observed, const TS* factors, d
 // One training system: node features, covisibility (bf16), whitened probes.
 struct GnnSystem {
   int64_t C = 0, observed = 0;
+  int64_t ldA = 0;  // row stride of A: C rounded up to 64, zero padded
   int cw = 0, K = 0;
   double lambda = 0;
   DBuf<float> X0, PX, PY;
@@ -644,11 +1045,16 @@ class Gnn {
   GnnSystem live;  // inference system of the attached backend
   // activations / gradients, sized to the largest C seen
   int64_t cap = 0;
-  DBuf<float> Z[NLAYER + 1], HA[NLAYER], H3, O, dO, dHa, dHb, dA, dZ, adj, edgeK;
+  DBuf<float> Z[NLAYER + 1], HA[NLAYER], H3, O, dO, dHa, dHb, dA, dZ, edgeK;
+  DBuf<unsigned long long> adj;  // fixed-point covisibility, C x C, left cleared by k_normalize
+  int64_t adj_cap = -1;          // entries of adj known to be zero
+  DBuf<unsigned char> edgeV;     // V_e of the 9/3 feature pass (27 storage words per edge)
   DBuf<double> dloss;
   DBuf<unsigned> dcount;
+  DBuf<int> gemm_err;  // set by a GEMM whose tensor-core wait ran out
   HBuf<double> hloss;
   HBuf<unsigned> hcount;
+  HBuf<int> herr;
   std::mt19937_64 order_rng;
 
   fg_status init(uint64_t seed, int device) {
@@ -663,6 +1069,9 @@ class Gnn {
     FG_TRY(wbf.resize(P.total));
     FG_TRY(dloss.resize(1));
     FG_TRY(dcount.resize(1));
+    FG_TRY(gemm_err.resize(1));
+    FG_CUDA(cudaMemsetAsync(gemm_err.get(), 0, sizeof(int), st));
+    FG_TRY(herr.resize(1));
     FG_TRY(hloss.resize(1));
     FG_TRY(hcount.resize(1));
     order_rng.seed(seed ^ 0x5DEECE66Dull);
@@ -675,6 +1084,19 @@ class Gnn {
     for (int l = 0; l < NLAYER; ++l)
       for (size_t i = 0; i < (size_t)2 * NH * NH; ++i) h[P.w[l] + i] = (float)(nd(rng) * 0.5 * std::sqrt(2.0 / (2 * NH)));
     return set_parameters(h.data());
+  }
+
+  // FG_DEVICE_TIMEOUT (and the flag cleared) when a GEMM gave up waiting on
+  // its tensor-core commits since the last check; call after a stream sync.
+  fg_status check_gemm() {
+    FG_CUDA(cudaMemcpyAsync(herr.get(), gemm_err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (herr.get()[0]) {
+      FG_CUDA(cudaMemsetAsync(gemm_err.get(), 0, sizeof(int), st));
+      set_error("a tensor-core GEMM of the learned preconditioner timed out");
+      return FG_DEVICE_TIMEOUT;
+    }
+    return FG_OK;
   }
 
   fg_status set_parameters(const float* h) {
@@ -705,24 +1127,45 @@ class Gnn {
     s.C = C;
     s.cw = L.cw;
     s.lambda = v.lambda;
+    s.ldA = std::max<int64_t>((C + 63) / 64 * 64, 64);
     FG_TRY(s.X0.resize(C * NF));
-    FG_TRY(s.A.resize(std::max<int64_t>(C * C, 1)));
+    FG_TRY(s.A.resize(std::max<int64_t>(C * s.ldA, 1)));
     FG_TRY(s.mask.resize(std::max<int64_t>(C, 1)));
-    FG_TRY(adj.resize(std::max<int64_t>(C * C, 1)));
-    FG_TRY(edgeK.resize(std::max<int64_t>(v.nedges * 16, 1)));
-    const TS* fac = (const TS*)v.factors;
-    const TS* cr = (const TS*)v.cross;
-    FG_LAUNCH(k_node_features<TS>, grid_for((size_t)C * 32, 128), 128, 0, st, L, v.cam_edge_off, v.cam_edge, v.edges,
-              cr, v.observed, fac, v.lambda, s.X0.get(), s.mask.get());
-    FG_CUDA(cudaMemsetAsync(adj.get(), 0, (size_t)C * C * sizeof(float), st));
-    if (v.nedges) {
-      FG_LAUNCH(k_edge_k<TS>, grid_for(v.nedges, 128), 128, 0, st, L, v.nedges, v.edges, cr, v.observed, fac,
-                v.lambda, edgeK.get());
-      if (L.nP)
-        FG_LAUNCH(k_pairs, grid_for((size_t)L.nP * 32, 128), 128, 0, st, (int64_t)L.nP, C, v.pt_edge_off, v.pt_edge,
-                  v.edges, edgeK.get(), L.pw, adj.get());
+    if (adj_cap < C * C) {
+      FG_TRY(adj.resize(std::max<int64_t>(C * C, 1)));
+      FG_CUDA(cudaMemsetAsync(adj.get(), 0, (size_t)std::max<int64_t>(C * C, 1) * sizeof(unsigned long long), st));
     }
-    FG_LAUNCH(k_normalize, (unsigned)C, 256, 0, st, C, adj.get(), s.mask.get(), s.X0.get(), s.A.get());
+    adj_cap = -1;  // dirty until k_normalize has cleared the rows again
+    const TS* fac = (const TS*)v.factors;
+    if (L.cw == 9 && L.pw == 3) {
+      FG_TRY(edgeK.resize(std::max<int64_t>(v.nedges * 8, 1)));
+      FG_TRY(edgeV.resize(std::max<int64_t>(v.nedges * 27 * (int64_t)sizeof(TS), 1)));
+      TS* V = reinterpret_cast<TS*>(edgeV.get());
+      if (v.nedges) {
+        const TS* src = v.rec ? (const TS*)v.rec : (const TS*)v.cross;
+        FG_LAUNCH(k_gnn_edge93<TS>, grid_for(v.nedges, 128), 128, 0, st, L, v.nedges, src, v.rec ? 0 : 1,
+                  v.pt_edge, v.edges, v.observed, fac, v.lambda, V, edgeK.get());
+      }
+      FG_LAUNCH(k_gnn_cams93<TS>, (unsigned)C, 128, 0, st, L, v.cam_edge_off, v.cam_edge, (const TS*)V, v.observed,
+                fac, v.lambda, s.X0.get(), s.mask.get());
+      if (v.nedges && L.nP)
+        FG_LAUNCH(k_gnn_pairs93, grid_for((size_t)L.nP * 32, 128), 128, 0, st, (int64_t)L.nP, C, v.pt_edge_off,
+                  edgeK.get(), adj.get());
+    } else {
+      FG_TRY(edgeK.resize(std::max<int64_t>(v.nedges * 16, 1)));
+      const TS* cr = (const TS*)v.cross;
+      FG_LAUNCH(k_node_features<TS>, grid_for((size_t)C * 32, 128), 128, 0, st, L, v.cam_edge_off, v.cam_edge,
+                v.edges, cr, v.observed, fac, v.lambda, s.X0.get(), s.mask.get());
+      if (v.nedges) {
+        FG_LAUNCH(k_edge_k<TS>, grid_for(v.nedges, 128), 128, 0, st, L, v.nedges, v.edges, cr, v.observed, fac,
+                  v.lambda, edgeK.get());
+        if (L.nP)
+          FG_LAUNCH(k_pairs, grid_for((size_t)L.nP * 32, 128), 128, 0, st, (int64_t)L.nP, C, v.pt_edge_off,
+                    v.pt_edge, v.edges, edgeK.get(), L.pw, adj.get());
+      }
+    }
+    FG_LAUNCH(k_normalize, (unsigned)C, 256, 0, st, C, s.ldA, adj.get(), s.mask.get(), s.X0.get(), s.A.get());
+    adj_cap = C * C;
     return FG_OK;
   }
   fg_status features(const SchurView& v, GnnSystem& s) {
@@ -741,11 +1184,11 @@ class Gnn {
     e0.h = HA[0].get();
     e0.ldh = 2 * NH;
     FG_TRY((gemm<float, __nv_bfloat16, false, false, EPI_BIAS_RELU>(st, nsm, C, NH, NF, s.X0.get(), NF, W + P.w_in, NH,
-                                                                     nullptr, 0, e0, false)));
+                                                                     nullptr, 0, e0, false, gemm_err.get())));
     for (int l = 0; l < NLAYER; ++l) {
       Epi ea;
-      FG_TRY((gemm<__nv_bfloat16, float, false, false, EPI_STORE>(st, nsm, C, NH, C, s.A.get(), C, HA[l].get(), 2 * NH,
-                                                                   HA[l].get() + NH, 2 * NH, ea, true)));
+      FG_TRY((gemm<__nv_bfloat16, float, false, false, EPI_STORE>(st, nsm, C, NH, C, s.A.get(), (int)s.ldA, HA[l].get(), 2 * NH,
+                                                                   HA[l].get() + NH, 2 * NH, ea, true, gemm_err.get())));
       Epi ez;
       ez.bias = w.get() + P.b[l];
       ez.z = Z[l + 1].get();
@@ -755,12 +1198,12 @@ class Gnn {
       ez.r = HA[l].get();
       ez.ldr = 2 * NH;
       FG_TRY((gemm<float, __nv_bfloat16, false, false, EPI_BIAS_RELU>(st, nsm, C, NH, 2 * NH, HA[l].get(), 2 * NH,
-                                                                       W + P.w[l], NH, nullptr, 0, ez, false)));
+                                                                       W + P.w[l], NH, nullptr, 0, ez, false, gemm_err.get())));
     }
     Epi eo;
     eo.bias = w.get() + P.b_out;
     FG_TRY((gemm<float, __nv_bfloat16, false, false, EPI_BIAS>(st, nsm, C, NH, NH, H3.get(), NH, W + P.w_out, NH,
-                                                                O.get(), NH, eo, false)));
+                                                                O.get(), NH, eo, false, gemm_err.get())));
     return FG_OK;
   }
 
@@ -778,7 +1221,7 @@ class Gnn {
     Epi none;
     // output layer
     FG_TRY((gemm<float, float, true, false, EPI_STORE>(st, nsm, NH, NH, C, H3.get(), NH, dO.get(), NH, G + P.w_out,
-                                                        NH, none, true)));
+                                                        NH, none, true, gemm_err.get())));
     FG_LAUNCH(k_colsum, 1, 256, 0, st, C, dO.get(), NH, G + P.b_out);
     Epi em;
     em.zmask = Z[NLAYER].get();
@@ -786,12 +1229,12 @@ class Gnn {
     em.d2 = dZ.get();
     em.ldd2 = NH;
     FG_TRY((gemm<float, __nv_bfloat16, false, true, EPI_STORE_MASK>(st, nsm, C, NH, NH, dO.get(), NH, W + P.w_out, NH,
-                                                                     dHa.get(), NH, em, false)));
+                                                                     dHa.get(), NH, em, false, gemm_err.get())));
     float* dh = dHa.get();
     float* dh2 = dHb.get();
     for (int l = NLAYER - 1; l >= 0; --l) {
       FG_TRY((gemm<float, float, true, false, EPI_STORE>(st, nsm, 2 * NH, NH, C, HA[l].get(), 2 * NH, dZ.get(), NH,
-                                                          G + P.w[l], NH, none, true)));
+                                                          G + P.w[l], NH, none, true, gemm_err.get())));
       FG_LAUNCH(k_colsum, 1, 256, 0, st, C, dZ.get(), NH, G + P.b[l]);
       Epi es;
       es.split_at = NH;
@@ -800,16 +1243,16 @@ class Gnn {
       es.h = dA.get();
       es.ldh = NH;
       FG_TRY((gemm<float, __nv_bfloat16, false, true, EPI_SPLIT>(st, nsm, C, 2 * NH, NH, dZ.get(), NH, W + P.w[l], NH,
-                                                                  dh2, NH, es, false)));
+                                                                  dh2, NH, es, false, gemm_err.get())));
       Epi acc;
       acc.accumulate = 1;
-      FG_TRY((gemm<__nv_bfloat16, float, true, false, EPI_STORE>(st, nsm, C, NH, C, s.A.get(), C, dA.get(), NH, dh2,
-                                                                  NH, acc, true)));
+      FG_TRY((gemm<__nv_bfloat16, float, true, false, EPI_STORE>(st, nsm, C, NH, C, s.A.get(), (int)s.ldA, dA.get(), NH, dh2,
+                                                                  NH, acc, true, gemm_err.get())));
       FG_LAUNCH(k_relu_mask, grid_for((size_t)C * NH, 256), 256, 0, st, (int64_t)C * NH, dh2, Z[l].get(), dZ.get());
       std::swap(dh, dh2);
     }
     FG_TRY((gemm<float, float, true, false, EPI_STORE>(st, nsm, NF, NH, C, s.X0.get(), NF, dZ.get(), NH, G + P.w_in,
-                                                        NH, none, true)));
+                                                        NH, none, true, gemm_err.get())));
     FG_LAUNCH(k_colsum, 1, 256, 0, st, C, dZ.get(), NH, G + P.b_in);
     return FG_OK;
   }
@@ -829,10 +1272,14 @@ class Gnn {
     FG_TRY(features(v, live));
     FG_TRY(forward(live));
     FG_CUDA(cudaMemsetAsync(dcount.get(), 0, sizeof(unsigned), st));
-    FG_LAUNCH(k_head_minv<TS>, grid_for(live.C, 64), 64, 0, st, v.L, O.get(), live.mask.get(), (const TS*)v.factors,
+    if (v.L.cw == 9)
+      FG_LAUNCH(k_head_minv93<TS>, grid_for((size_t)live.C * 32, 128), 128, 0, st, v.L, O.get(), live.mask.get(),
+                (const TS*)v.factors, (TS*)minv, dcount.get());
+    else
+      FG_LAUNCH(k_head_minv<TS>, grid_for(live.C, 64), 64, 0, st, v.L, O.get(), live.mask.get(), (const TS*)v.factors,
               (TS*)minv, dcount.get());
     FG_CUDA(cudaMemcpyAsync(hcount.get(), dcount.get(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    FG_CUDA(cudaStreamSynchronize(st));
+    FG_TRY(check_gemm());
     *nonfinite = hcount.get()[0];
     return FG_OK;
   }
@@ -902,7 +1349,7 @@ class Gnn {
       FG_TRY(adam(lr));
     }
     FG_CUDA(cudaMemcpyAsync(hloss.get(), dloss.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
-    FG_CUDA(cudaStreamSynchronize(st));
+    FG_TRY(check_gemm());
     *mean_loss = steps ? hloss.get()[0] / (double)steps : 0.0;
     return FG_OK;
   }
@@ -922,7 +1369,7 @@ class Gnn {
     if (gradient) FG_CUDA(cudaMemcpyAsync(gradient, grad.get(), P.total * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (outputs && sys.C)
       FG_CUDA(cudaMemcpyAsync(outputs, O.get(), (size_t)sys.C * NH * sizeof(float), cudaMemcpyDeviceToHost, st));
-    FG_CUDA(cudaStreamSynchronize(st));
+    FG_TRY(check_gemm());
     *loss = hloss.get()[0];
     return FG_OK;
   }
@@ -1058,10 +1505,12 @@ FG_API fg_status fg_gnn_export_system(fg_gnn* g, size_t index, float* features, 
   const size_t C = (size_t)s.C, n = C * s.cw * (size_t)s.K;
   if (features && C) FG_CUDA(cudaMemcpyAsync(features, s.X0.get(), C * fg::NF * sizeof(float), cudaMemcpyDeviceToHost, st));
   if (adjacency && C) {
-    std::vector<__nv_bfloat16> tmp(C * C);
-    FG_CUDA(cudaMemcpyAsync(tmp.data(), s.A.get(), C * C * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost, st));
+    const size_t ld = (size_t)s.ldA;
+    std::vector<__nv_bfloat16> tmp(C * ld);
+    FG_CUDA(cudaMemcpyAsync(tmp.data(), s.A.get(), C * ld * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < C * C; ++i) adjacency[i] = __bfloat162float(tmp[i]);
+    for (size_t i = 0; i < C; ++i)
+      for (size_t j = 0; j < C; ++j) adjacency[i * C + j] = __bfloat162float(tmp[i * ld + j]);
   }
   if (probe_x && n) FG_CUDA(cudaMemcpyAsync(probe_x, s.PX.get(), n * sizeof(float), cudaMemcpyDeviceToHost, st));
   if (probe_y && n) FG_CUDA(cudaMemcpyAsync(probe_y, s.PY.get(), n * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -1091,15 +1540,18 @@ FG_API fg_status fg_gnn_import_system(fg_gnn* g, size_t cameras, size_t width, s
   s->cw = (int)width;
   s->K = (int)probes;
   FG_TRY(s->X0.resize(std::max<size_t>(C * fg::NF, 1)));
-  FG_TRY(s->A.resize(std::max<size_t>(C * C, 1)));
+  s->ldA = std::max<int64_t>(((int64_t)C + 63) / 64 * 64, 64);
+  const size_t ld = (size_t)s->ldA;
+  FG_TRY(s->A.resize(std::max<size_t>(C * ld, 1)));
   FG_TRY(s->mask.resize(std::max<size_t>(C, 1)));
   FG_TRY(s->PX.resize(std::max<size_t>(n, 1)));
   FG_TRY(s->PY.resize(std::max<size_t>(n, 1)));
-  std::vector<__nv_bfloat16> tmp(C * C);
-  for (size_t i = 0; i < C * C; ++i) tmp[i] = __float2bfloat16_rn(adjacency[i]);
+  std::vector<__nv_bfloat16> tmp(C * ld, __float2bfloat16_rn(0.f));
+  for (size_t i = 0; i < C; ++i)
+    for (size_t j = 0; j < C; ++j) tmp[i * ld + j] = __float2bfloat16_rn(adjacency[i * C + j]);
   if (C) {
     FG_CUDA(cudaMemcpyAsync(s->X0.get(), features, C * fg::NF * sizeof(float), cudaMemcpyHostToDevice, G.st));
-    FG_CUDA(cudaMemcpyAsync(s->A.get(), tmp.data(), C * C * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, G.st));
+    FG_CUDA(cudaMemcpyAsync(s->A.get(), tmp.data(), C * ld * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, G.st));
     FG_CUDA(cudaMemcpyAsync(s->mask.get(), mask, C, cudaMemcpyHostToDevice, G.st));
   }
   if (n) {

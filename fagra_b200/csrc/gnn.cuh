@@ -22,6 +22,10 @@ struct SchurView {
   const int64_t *pt_edge_off, *pt_edge, *cam_edge_off, *cam_edge;
   const uint8_t* observed;
   double lambda;
+  // point-sorted edge records (28 storage words per edge: E_e column-major
+  // cw x pw, then the packed camera / point word) in the order of pt_edge, or
+  // null when the backend keeps none; with them the features need no cross array
+  const void* rec = nullptr;
 };
 
 // y = S x for device vectors of the retained length (f64), S at the view's damping.

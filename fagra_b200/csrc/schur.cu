@@ -663,7 +663,8 @@ class SchurImpl final : public Backend {
       if (fast.ready_for(*this)) {
         // the reference-layout cross array is only needed by the generic
         // right-hand side / back-substitution and the Schur-diagonal factor
-        cross_current = !pure_pairs || opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL || learned_active();
+        cross_current = !pure_pairs || opt.preconditioner == FG_PRECOND_SCHUR_DIAGONAL ||
+                        (learned_active() && !(cw == 9 && pw == 3));  // the 9/3 features read the records
         if (bal_layout())
           FG_LAUNCH(k_edge_records_bal<TS>, grid_for(nedges, REC_T), REC_T, 0, st, (int64_t)nedges,
                     (int64_t)retained, d_pt_edge.get(), d_edges.get(), d_values.get(), d_inv_scales.get(),
@@ -839,6 +840,7 @@ class SchurImpl final : public Backend {
     v.cam_edge = d_cam_edge.get();
     v.observed = d_observed.get();
     v.lambda = lambda;
+    v.rec = fast.on && cw == 9 && pw == 3 ? (const void*)fast.d_erec.get() : nullptr;
     return v;
   }
   // Explicit block-Jacobi (or Schur-diagonal) inverses into d_minv.
@@ -878,9 +880,10 @@ class SchurImpl final : public Backend {
       EventTimer ti;
       const bool timed = !learned_compared && opt.learned_policy == 0;  // inference time of the comparison
       if (timed) ti.start(st);
-      FG_TRY(ensure_cross());
+      const SchurView view = view_at(lambda);
+      if (!view.rec) FG_TRY(ensure_cross());
       unsigned nonfinite = 0;
-      FG_TRY(gnn_precondition(learned, view_at(lambda), d_minv.get(), st, &nonfinite));
+      FG_TRY(gnn_precondition(learned, view, d_minv.get(), st, &nonfinite));
       if (timed) learned_infer_seconds = ti.stop(st);
     }
     if (*fallbacks == 0) FG_TRY(fast.refresh_points(*this, lambda));
