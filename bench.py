@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fagra_b200", choices=["fagra_b200", "reference"])
     ap.add_argument("--workload", default="bal1k")
-    ap.add_argument("--forms", default="learned,learned_always,fastc,fast,f64")
+    ap.add_argument("--forms", default="learned_always,learned,fastc,fast,f64")
     ap.add_argument("--operator-variant", type=int, default=0,
                     help="FP32 reduced-operator variant (0: autotune; 1..4 force one, e.g. for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -116,25 +116,41 @@ __device__ __forceinline__ uint4 load8<__nv_bfloat16>(const __nv_bfloat16* p, in
 // One operand tile of R rows x UK columns of K into swizzled shared memory:
 // element (row, k) = src(r0 + row, k0 + k); KCONTIG: src(r, k) = src[r*ld + k]
 // (16-byte chunks along K), else src[k*ld + r] (8 rows per thread, scattered
-// 2-byte stores). Rows >= rows and k >= kend are zero.
+// 2-byte stores). Rows >= rows and k >= kend are zero. All of a thread's loads
+// are issued before its shared-memory stores (fetch, then place), so they
+// overlap instead of waiting on stores the compiler cannot disambiguate.
+template <int R>
+struct TileRegs {
+  static constexpr int N = R * UK / 8 / 128;
+  uint4 v[N];
+};
 template <int R, bool KCONTIG, class T>
-__device__ __forceinline__ void load_tile(uint8_t* tile, const T* src, int ld, int r0, int rows, int k0, int kend,
-                                          bool vec) {
-  constexpr int CH = R * UK / 8;  // 16-byte chunks
-#pragma unroll 4
-  for (int q = threadIdx.x; q < CH; q += 128) {
+__device__ __forceinline__ void fetch_tile(TileRegs<R>& t, const T* src, int ld, int r0, int rows, int k0, int kend,
+                                           bool vec) {
+#pragma unroll
+  for (int j = 0; j < TileRegs<R>::N; ++j) {
+    const int q = threadIdx.x + 128 * j;
+    uint4 v = make_uint4(0, 0, 0, 0);
     if (KCONTIG) {
-      const int row = q >> 3, kq = (q & 7) * 8;
-      const int gr = r0 + row, gk = k0 + kq;
-      uint4 v = make_uint4(0, 0, 0, 0);
+      const int gr = r0 + (q >> 3), gk = k0 + (q & 7) * 8;
       if (gr < rows && gk < kend) v = load8<T>(src + (size_t)gr * ld + gk, kend - gk, vec);
-      *reinterpret_cast<uint4*>(tile + umma_sw128_offset(row, kq)) = v;
+    } else {
+      const int gr = r0 + (q % (R / 8)) * 8, gk = k0 + q / (R / 8);
+      if (gk < kend && gr < rows) v = load8<T>(src + (size_t)gk * ld + gr, rows - gr, vec);
+    }
+    t.v[j] = v;
+  }
+}
+template <int R, bool KCONTIG>
+__device__ __forceinline__ void place_tile(uint8_t* tile, const TileRegs<R>& t) {
+#pragma unroll
+  for (int j = 0; j < TileRegs<R>::N; ++j) {
+    const int q = threadIdx.x + 128 * j;
+    if (KCONTIG) {
+      *reinterpret_cast<uint4*>(tile + umma_sw128_offset(q >> 3, (q & 7) * 8)) = t.v[j];
     } else {
       const int rq = (q % (R / 8)) * 8, k = q / (R / 8);
-      const int gr = r0 + rq, gk = k0 + k;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (gk < kend && gr < rows) v = load8<T>(src + (size_t)gk * ld + gr, rows - gr, vec);
-      const uint16_t* h = reinterpret_cast<const uint16_t*>(&v);
+      const uint16_t* h = reinterpret_cast<const uint16_t*>(&t.v[j]);
 #pragma unroll
       for (int i = 0; i < 8; ++i) *reinterpret_cast<uint16_t*>(tile + umma_sw128_offset(rq + i, k)) = h[i];
     }
@@ -144,7 +160,7 @@ __device__ __forceinline__ void load_tile(uint8_t* tile, const T* src, int ld, i
 template <class TA, class TB, bool TRA, bool TRB, int EPI>
 __global__ void __launch_bounds__(128, 1) k_gemm(int M, int N, int K, const TA* __restrict__ A, int lda,
                                                  const TB* __restrict__ B, int ldb, float* __restrict__ Cm, int ldc,
-                                                 Epi ep, int kchunk, int vec_a, int vec_b, int* err) {
+                                                 Epi ep, int kchunk, int vec_a, int vec_b, int vec2, int* err) {
   extern __shared__ uint8_t gemm_smem[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
@@ -177,8 +193,12 @@ __global__ void __launch_bounds__(128, 1) k_gemm(int M, int N, int K, const TA* 
     const int k0 = kb + c * UK;
     uint8_t* sa = base + s * UTILE_A;
     uint8_t* sb = base + 2 * UTILE_A + s * UTILE_B;
-    load_tile<UM, !TRA>(sa, A, lda, m0, M, k0, ke, vec_a != 0);
-    load_tile<UN, TRB>(sb, B, ldb, n0, N, k0, ke, vec_b != 0);
+    TileRegs<UM> ta;
+    TileRegs<UN> tb;
+    fetch_tile<UM, !TRA>(ta, A, lda, m0, M, k0, ke, vec_a != 0);
+    fetch_tile<UN, TRB>(tb, B, ldb, n0, N, k0, ke, vec_b != 0);
+    place_tile<UM, !TRA>(sa, ta);
+    place_tile<UN, TRB>(sb, tb);
     umma_fence_smem();
     __syncthreads();
     if (tid == 0) {
@@ -197,17 +217,24 @@ __global__ void __launch_bounds__(128, 1) k_gemm(int M, int N, int K, const TA* 
   if (issued >= 2) done = umma_wait(((issued - 2) & 1) ? bar1 : bar0, ((issued - 2) >> 1) & 1, err) && done;
   done = __syncthreads_and(done && issued == nchunks);
   tcgen05_after_sync();
-  uint32_t r[2][32];
+  // accumulator rows (thread = row) into shared memory over the finished
+  // operand tiles, 65-float row pitch (conflict-free both ways)
+  float* stage = reinterpret_cast<float*>(base);
   if (done && nchunks > 0) {
+    uint32_t r[32];
     const uint32_t row_addr = tmem + ((uint32_t)(warp * 32) << 16);
-    tmem_ld32(row_addr, r[0]);
-    tmem_ld32(row_addr + 32, r[1]);
-    tmem_wait_ld();
+    float* srow = stage + (warp * 32 + lane) * 65;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      tmem_ld32(row_addr + 32 * h, r);
+      tmem_wait_ld();
+#pragma unroll
+      for (int j = 0; j < 32; ++j) srow[32 * h + j] = __uint_as_float(r[j]);
+    }
   } else {
+    float* srow = stage + (warp * 32 + lane) * 65;
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int j = 0; j < 32; ++j) r[h][j] = 0u;
+    for (int j = 0; j < 64; ++j) srow[j] = 0.f;
   }
   tcgen05_before_sync();
   __syncthreads();
@@ -216,35 +243,92 @@ __global__ void __launch_bounds__(128, 1) k_gemm(int M, int N, int K, const TA* 
     tmem_dealloc(tmem, UN);
   }
   if (!done) return;  // the error flag is set; nothing is written
-  const int m = m0 + warp * 32 + lane;
-  if (m >= M) return;
+  // epilogue, warp per row: lane owns columns 2 lane, 2 lane + 1 (float2
+  // accesses when every stride and base allows them)
   const bool split = gridDim.z > 1;
-#pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const int n = n0 + 32 * h + j;
-      if (n >= N) continue;
-      const float v = __uint_as_float(r[h][j]);
+  const int nloc = min(UN, N - n0);
+  for (int rr = warp; rr < UM; rr += 4) {
+    const int m = m0 + rr;
+    if (m >= M) break;
+    const float* srow = stage + rr * 65;
+    const int j = 2 * lane;
+    const int n = n0 + j;
+    if (j >= nloc) continue;
+    const bool pair = vec2 && j + 1 < nloc;
+    float v0 = srow[j], v1 = pair ? srow[j + 1] : 0.f;
+    auto ld2 = [&](const float* p, float& a, float& b) {
+      if (pair) {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        a = t.x;
+        b = t.y;
+      } else {
+        a = *p;
+      }
+    };
+    auto st2 = [&](float* p, float a, float b) {
+      if (pair) *reinterpret_cast<float2*>(p) = make_float2(a, b);
+      else *p = a;
+    };
+    if (EPI == EPI_STORE) {
+      float* c = Cm + (size_t)m * ldc + n;
+      if (split) {
+        if (pair) atomicAdd(reinterpret_cast<float2*>(c), make_float2(v0, v1));
+        else atomicAdd(c, v0);
+      } else {
+        if (ep.accumulate) {
+          float a0 = 0.f, a1 = 0.f;
+          ld2(c, a0, a1);
+          v0 += a0;
+          v1 += a1;
+        }
+        st2(c, v0, v1);
+      }
+    } else if (EPI == EPI_BIAS_RELU) {
+      const float z0 = v0 + __ldg(ep.bias + n), z1 = pair ? v1 + __ldg(ep.bias + n + 1) : 0.f;
+      float r0 = 0.f, r1 = 0.f;
+      if (ep.r) ld2(ep.r + (size_t)m * ep.ldr + n, r0, r1);
+      st2(ep.z + (size_t)m * ep.ldz + n, z0, z1);
+      st2(ep.h + (size_t)m * ep.ldh + n, r0 + fmaxf(z0, 0.f), r1 + fmaxf(z1, 0.f));
+    } else if (EPI == EPI_BIAS) {
+      st2(Cm + (size_t)m * ldc + n, v0 + __ldg(ep.bias + n), pair ? v1 + __ldg(ep.bias + n + 1) : 0.f);
+    } else if (EPI == EPI_SPLIT) {
+      // split_at is even, so a pair never straddles it
+      if (n < ep.split_at) {
+        float r0 = 0.f, r1 = 0.f;
+        ld2(ep.r + (size_t)m * ep.ldr + n, r0, r1);
+        st2(Cm + (size_t)m * ldc + n, v0 + r0, v1 + r1);
+      } else {
+        st2(ep.h + (size_t)m * ep.ldh + (n - ep.split_at), v0, v1);
+      }
+    } else if (EPI == EPI_STORE_MASK) {
+      float q0 = 0.f, q1 = 0.f;
+      ld2(ep.zmask + (size_t)m * ep.ldzm + n, q0, q1);
+      st2(Cm + (size_t)m * ldc + n, v0, v1);
+      st2(ep.d2 + (size_t)m * ep.ldd2 + n, q0 > 0.f ? v0 : 0.f, q1 > 0.f ? v1 : 0.f);
+    }
+    if (!pair && j + 1 < nloc) {  // the second column alone
+      const int n1 = n + 1;
+      const float w = srow[j + 1];
       if (EPI == EPI_STORE) {
-        float* c = Cm + (size_t)m * ldc + n;
-        if (split) atomicAdd(c, v);
-        else *c = ep.accumulate ? *c + v : v;
+        float* c = Cm + (size_t)m * ldc + n1;
+        if (split) atomicAdd(c, w);
+        else *c = ep.accumulate ? *c + w : w;
       } else if (EPI == EPI_BIAS_RELU) {
-        const float z = v + ep.bias[n];
-        ep.z[(size_t)m * ep.ldz + n] = z;
-        const float res = ep.r ? ep.r[(size_t)m * ep.ldr + n] : 0.f;
-        ep.h[(size_t)m * ep.ldh + n] = res + fmaxf(z, 0.f);
+        const float z = w + __ldg(ep.bias + n1);
+        const float res = ep.r ? ep.r[(size_t)m * ep.ldr + n1] : 0.f;
+        ep.z[(size_t)m * ep.ldz + n1] = z;
+        ep.h[(size_t)m * ep.ldh + n1] = res + fmaxf(z, 0.f);
       } else if (EPI == EPI_BIAS) {
-        Cm[(size_t)m * ldc + n] = v + ep.bias[n];
+        Cm[(size_t)m * ldc + n1] = w + __ldg(ep.bias + n1);
       } else if (EPI == EPI_SPLIT) {
-        if (n < ep.split_at) Cm[(size_t)m * ldc + n] = v + ep.r[(size_t)m * ep.ldr + n];
-        else ep.h[(size_t)m * ep.ldh + (n - ep.split_at)] = v;
+        if (n1 < ep.split_at) Cm[(size_t)m * ldc + n1] = w + ep.r[(size_t)m * ep.ldr + n1];
+        else ep.h[(size_t)m * ep.ldh + (n1 - ep.split_at)] = w;
       } else if (EPI == EPI_STORE_MASK) {
-        Cm[(size_t)m * ldc + n] = v;
-        ep.d2[(size_t)m * ep.ldd2 + n] = ep.zmask[(size_t)m * ep.ldzm + n] > 0.f ? v : 0.f;
+        Cm[(size_t)m * ldc + n1] = w;
+        ep.d2[(size_t)m * ep.ldd2 + n1] = ep.zmask[(size_t)m * ep.ldzm + n1] > 0.f ? w : 0.f;
       }
     }
+  }
 }
 
 template <class T>
@@ -276,8 +360,14 @@ fg_status gemm(cudaStream_t st, int nsm, int M, int N, int K, const TA* A, int l
   FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UMMA_SMEM));
   // 16-byte loads need aligned rows: along K for K-contiguous operands, along M / N otherwise
   const int va = vec16(A, lda) ? 1 : 0, vb = vec16(B, ldb) ? 1 : 0;
+  // float2 epilogue accesses: every output / input row stride even and base 8-byte aligned
+  auto ok2 = [](const float* p, int ld) { return !p || (((uintptr_t)p % 8) == 0 && ld % 2 == 0); };
+  const int v2 = ok2(Cm, ldc) && ok2(ep.z, ep.ldz) && ok2(ep.h, ep.ldh) && ok2(ep.r, ep.ldr) &&
+                         ok2(ep.zmask, ep.ldzm) && ok2(ep.d2, ep.ldd2) && ep.split_at % 2 == 0
+                     ? 1
+                     : 0;
   dim3 grid(gx, gy, (unsigned)splits);
-  FG_LAUNCH(kern, grid, 128, UMMA_SMEM, st, M, N, K, A, lda, B, ldb, Cm, ldc, ep, kchunk, va, vb, err);
+  FG_LAUNCH(kern, grid, 128, UMMA_SMEM, st, M, N, K, A, lda, B, ldb, Cm, ldc, ep, kchunk, va, vb, v2, err);
   return FG_OK;
 }
 
@@ -577,124 +667,162 @@ __global__ void k_normalize(int64_t nC, int64_t lda, unsigned long long* adj, co
 // G_e = L_c^-1 V_e (so K_e = G_e^T G_e); unobserved variables use
 // L = sqrt(lambda) I as above.
 
-// Thread per edge in the point-sorted order of pt_edge: E_e from the edge
-// records (28 words, position k) or the cross array (27 words, edge e); V_e by
-// edge (column-major 9 x 3) and, by position, K_e lower (6 floats) with the
-// camera index in slot 6 (8 floats per edge).
+// Thread per edge in the point-sorted order of pt_edge (position k): E_e from
+// the edge records (28 words, staged through shared memory with coalesced
+// loads) or the cross array (27 words, edge e), V_e = E_e L_p^-T written by
+// position (column-major 9 x 3, coalesced through shared memory), and the
+// position of every edge (pos[e] = k).
 template <class TS>
 __global__ void __launch_bounds__(128) k_gnn_edge93(Layout L, int64_t nedges, const TS* src, int by_edge,
                                                     const int64_t* pt_edge, const DEdgeMeta* edges,
                                                     const uint8_t* observed, const TS* factors, double lambda, TS* V,
-                                                    float* Kout) {
-  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= nedges) return;
-  const int64_t e = pt_edge[k];
-  const int2 cp = *reinterpret_cast<const int2*>(edges + e);
-  const TS* E = src + (by_edge ? e * 27 : k * 28);
-  double v[27];  // v[q * 9 + c] = V(c, q)
-  const bool pobs = observed[L.nC + cp.y];
-  const TS* lp = factors + L.gram_offset(L.nC + cp.y);
-  double p00 = 0, p10 = 0, p20 = 0, p11 = 0, p21 = 0, p22 = 0;
-  if (pobs) {
-    p00 = (double)lp[0]; p10 = (double)lp[1]; p20 = (double)lp[2];
-    p11 = (double)lp[4]; p21 = (double)lp[5]; p22 = (double)lp[8];
-  }
-  const double isl = 1.0 / sqrt(lambda);
-#pragma unroll
-  for (int c = 0; c < 9; ++c) {
-    const double e0 = (double)E[c], e1 = (double)E[9 + c], e2 = (double)E[18 + c];
-    if (pobs) {  // row c of E times L_p^-T: solve L_p y = E(c, :)^T
-      const double y0 = e0 / p00;
-      const double y1 = (e1 - p10 * y0) / p11;
-      const double y2 = (e2 - p20 * y0 - p21 * y1) / p22;
-      v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
+                                                    int32_t* pos) {
+  using T = TS;  // arithmetic in the storage precision: the factors and records carry no more
+  __shared__ TS tile[128 * 29];
+  const int64_t k0 = (int64_t)blockIdx.x * 128, k = k0 + threadIdx.x;
+  const int nk = (int)min((int64_t)128, nedges - k0);
+  if (!by_edge)
+    for (int i = threadIdx.x; i < nk * 28; i += 128) tile[(i / 28) * 29 + i % 28] = src[k0 * 28 + i];
+  __syncthreads();
+  if (k < nedges) {
+    const int64_t e = pt_edge[k];
+    const int2 cp = *reinterpret_cast<const int2*>(edges + e);
+    pos[e] = (int32_t)k;
+    TS* t = tile + threadIdx.x * 29;
+    if (by_edge)
+      for (int i = 0; i < 27; ++i) t[i] = src[e * 27 + i];
+    const bool pobs = observed[L.nC + cp.y];
+    const TS* lp = factors + L.gram_offset(L.nC + cp.y);
+    T p10 = 0, p20 = 0, p21 = 0, r0, r1, r2;
+    if (pobs) {
+      p10 = lp[1]; p20 = lp[2]; p21 = lp[5];
+      r0 = (T)1 / lp[0]; r1 = (T)1 / lp[4]; r2 = (T)1 / lp[8];
     } else {
-      v[c] = e0 * isl; v[9 + c] = e1 * isl; v[18 + c] = e2 * isl;
+      r0 = r1 = r2 = (T)(1.0 / sqrt(lambda));
     }
-  }
-  TS* vo = V + e * 27;
+    T v[27];
 #pragma unroll
-  for (int i = 0; i < 27; ++i) vo[i] = (TS)v[i];
-  float4* ko = reinterpret_cast<float4*>(Kout + k * 8);
-  if (!observed[cp.x]) {
-    ko[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-    ko[1] = make_float4(0.f, 0.f, __int_as_float(cp.x), 0.f);
-    return;
-  }
-  const TS* lc = factors + L.gram_offset(cp.x);
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {  // column q of G = L_c^-1 V
-    double* g = v + 9 * q;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      double s = g[i];
-#pragma unroll
-      for (int j = 0; j < i; ++j) s -= (double)lc[j * 9 + i] * g[j];
-      g[i] = s / (double)lc[i * 9 + i];
+    for (int c = 0; c < 9; ++c) {  // row c of E times L_p^-T: solve L_p y = E(c, :)^T
+      const T y0 = t[c] * r0;
+      const T y1 = (t[9 + c] - p10 * y0) * r1;
+      const T y2 = (t[18 + c] - p20 * y0 - p21 * y1) * r2;
+      v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
     }
+#pragma unroll
+    for (int i = 0; i < 27; ++i) t[i] = v[i];  // own row only: no barrier needed before
   }
-  double K[6];  // K00, K10, K20, K11, K21, K22
-  int idx = 0;
-#pragma unroll
-  for (int q = 0; q < 3; ++q)
-#pragma unroll
-    for (int r = q; r < 3; ++r) {
-      double s = 0;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) s += v[9 * r + c] * v[9 * q + c];
-      K[idx++] = s;
-    }
-  ko[0] = make_float4((float)K[0], (float)K[1], (float)K[2], (float)K[3]);
-  ko[1] = make_float4((float)K[4], (float)K[5], __int_as_float(cp.x), 0.f);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nk * 27; i += 128) V[k0 * 27 + i] = tile[(i / 27) * 29 + i % 27];
 }
 
-// Block of 128 per camera: U = sum_e V_e V_e^T over the camera's edges, then
-// P = L_c^-1 U L_c^-T and the node-feature row as k_node_features writes it.
+// Block of 128 per camera (L_c in shared memory): over the camera's edges,
+// U = sum_e V_e V_e^T in FP64 and K_e = G_e^T G_e with G_e = L_c^-1 V_e,
+// written at the edge's point-sorted position (K lower, 6 floats, camera
+// index in slot 6); then P = L_c^-1 U L_c^-T and the node-feature row as
+// k_node_features writes it.
 template <class TS>
 __global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge,
-                                                    const TS* V, const uint8_t* observed, const TS* factors,
-                                                    double lambda, float* X0, uint8_t* mask) {
+                                                    const int32_t* pos, const TS* V, const uint8_t* observed,
+                                                    const TS* factors, double lambda, float* X0, uint8_t* mask,
+                                                    float* Kout) {
+  using T = TS;
   const int64_t cam = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float* row = X0 + cam * NF;
+  const int64_t e0 = cam_edge_off[cam], e1 = cam_edge_off[cam + 1];
   if (!observed[cam]) {
     if (tid == 0) mask[cam] = 0;
     if (tid < NF) row[tid] = tid == 49 ? 1.f : 0.f;
+    for (int64_t k = e0 + tid; k < e1; k += 128) {
+      float4* ko = reinterpret_cast<float4*>(Kout + (int64_t)pos[cam_edge[k]] * 8);
+      ko[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+      ko[1] = make_float4(0.f, 0.f, __int_as_float((int)cam), 0.f);
+    }
     return;
   }
-  double acc[45];
+  __shared__ T sl[81], srd[9];
+  __shared__ double red[4][45];
+  __shared__ double U[81], W[81];
+  const TS* lc = factors + L.gram_offset(cam);
+  if (tid < 81) sl[tid] = lc[tid];
+  if (tid < 9) srd[tid] = (T)1 / lc[tid * 9 + tid];
+  __syncthreads();
+  // per-thread partial sums in the storage precision (a thread sees about
+  // 1/128 of the camera's edges), combined in FP64 below
+  T acc[45];
 #pragma unroll
   for (int i = 0; i < 45; ++i) acc[i] = 0;
-  for (int64_t k = cam_edge_off[cam] + tid; k < cam_edge_off[cam + 1]; k += 128) {
-    const TS* v = V + cam_edge[k] * 27;
-    double w[27];
+  // the next edge's loads are issued before the current edge's arithmetic
+  int64_t k = e0 + tid;
+  int64_t p = k < e1 ? (int64_t)pos[cam_edge[k]] : 0;
+  T vn[27];
+  if (k < e1) {
+    const TS* vp = V + p * 27;
 #pragma unroll
-    for (int i = 0; i < 27; ++i) w[i] = (double)v[i];
+    for (int i = 0; i < 27; ++i) vn[i] = vp[i];
+  }
+  for (; k < e1; k += 128) {
+    T v[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) v[i] = vn[i];
+    const int64_t pc = p;
+    const int64_t kn = k + 128;
+    if (kn < e1) {
+      p = pos[cam_edge[kn]];
+      const TS* vp = V + p * 27;
+#pragma unroll
+      for (int i = 0; i < 27; ++i) vn[i] = vp[i];
+    }
     int idx = 0;
 #pragma unroll
     for (int c = 0; c < 9; ++c)
 #pragma unroll
-      for (int r = c; r < 9; ++r) acc[idx++] += w[r] * w[c] + w[9 + r] * w[9 + c] + w[18 + r] * w[18 + c];
+      for (int r = c; r < 9; ++r) acc[idx++] += v[r] * v[c] + v[9 + r] * v[9 + c] + v[18 + r] * v[18 + c];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {  // G = L_c^-1 V, the three columns together
+      T s0 = v[i], s1 = v[9 + i], s2 = v[18 + i];
+#pragma unroll
+      for (int j = 0; j < i; ++j) {
+        const T l = sl[j * 9 + i];
+        s0 -= l * v[j];
+        s1 -= l * v[9 + j];
+        s2 -= l * v[18 + j];
+      }
+      v[i] = s0 * srd[i];
+      v[9 + i] = s1 * srd[i];
+      v[18 + i] = s2 * srd[i];
+    }
+    T K[6];  // K00, K10, K20, K11, K21, K22
+    int kx = 0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int r = q; r < 3; ++r) {
+        T sk = 0;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) sk += v[9 * r + c] * v[9 * q + c];
+        K[kx++] = sk;
+      }
+    float4* ko = reinterpret_cast<float4*>(Kout + pc * 8);
+    ko[0] = make_float4((float)K[0], (float)K[1], (float)K[2], (float)K[3]);
+    ko[1] = make_float4((float)K[4], (float)K[5], __int_as_float((int)cam), 0.f);
   }
-  __shared__ double red[4][45];
-  __shared__ double U[81], W[81];
 #pragma unroll
   for (int i = 0; i < 45; ++i) {
-    const double s = lane_allsum(acc[i]);
-    if (lane == 0) red[warp][i] = s;
+    const double sum = lane_allsum((double)acc[i]);
+    if (lane == 0) red[warp][i] = sum;
   }
   __syncthreads();
-  const TS* lc = factors + L.gram_offset(cam);
   if (tid < 45) {
-    const double s = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+    const double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
     int c = 0, r = tid;  // lower entry tid (column-major) -> (r, c)
     while (r >= 9 - c) {
       r -= 9 - c;
       ++c;
     }
     r += c;
-    U[c * 9 + r] = s;
-    U[r * 9 + c] = s;
+    U[c * 9 + r] = sum;
+    U[r * 9 + c] = sum;
   }
   __syncthreads();
   if (tid < 9) {  // W = L^-1 U, column tid
@@ -703,10 +831,10 @@ __global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam
     for (int i = 0; i < 9; ++i) x[i] = U[tid * 9 + i];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      double s = x[i];
+      double t = x[i];
 #pragma unroll
-      for (int j = 0; j < i; ++j) s -= (double)lc[j * 9 + i] * x[j];
-      x[i] = s / (double)lc[i * 9 + i];
+      for (int j = 0; j < i; ++j) t -= (double)lc[j * 9 + i] * x[j];
+      x[i] = t / (double)lc[i * 9 + i];
     }
 #pragma unroll
     for (int i = 0; i < 9; ++i) W[tid * 9 + i] = x[i];
@@ -718,10 +846,10 @@ __global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam
     for (int i = 0; i < 9; ++i) x[i] = W[i * 9 + tid];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      double s = x[i];
+      double t = x[i];
 #pragma unroll
-      for (int j = 0; j < i; ++j) s -= (double)lc[j * 9 + i] * x[j];
-      x[i] = s / (double)lc[i * 9 + i];
+      for (int j = 0; j < i; ++j) t -= (double)lc[j * 9 + i] * x[j];
+      x[i] = t / (double)lc[i * 9 + i];
     }
 #pragma unroll
     for (int i = 0; i < 9; ++i) U[tid * 9 + i] = x[i];  // U now holds P (column-major)
@@ -1049,6 +1177,7 @@ class Gnn {
   DBuf<unsigned long long> adj;  // fixed-point covisibility, C x C, left cleared by k_normalize
   int64_t adj_cap = -1;          // entries of adj known to be zero
   DBuf<unsigned char> edgeV;     // V_e of the 9/3 feature pass (27 storage words per edge)
+  DBuf<int32_t> edgePos;         // point-sorted position of every edge
   DBuf<double> dloss;
   DBuf<unsigned> dcount;
   DBuf<int> gemm_err;  // set by a GEMM whose tensor-core wait ran out
@@ -1140,14 +1269,16 @@ class Gnn {
     if (L.cw == 9 && L.pw == 3) {
       FG_TRY(edgeK.resize(std::max<int64_t>(v.nedges * 8, 1)));
       FG_TRY(edgeV.resize(std::max<int64_t>(v.nedges * 27 * (int64_t)sizeof(TS), 1)));
+      FG_TRY(edgePos.resize(std::max<int64_t>(v.nedges, 1)));
       TS* V = reinterpret_cast<TS*>(edgeV.get());
       if (v.nedges) {
         const TS* src = v.rec ? (const TS*)v.rec : (const TS*)v.cross;
         FG_LAUNCH(k_gnn_edge93<TS>, grid_for(v.nedges, 128), 128, 0, st, L, v.nedges, src, v.rec ? 0 : 1,
-                  v.pt_edge, v.edges, v.observed, fac, v.lambda, V, edgeK.get());
+                  v.pt_edge, v.edges, v.observed, fac, v.lambda, V, edgePos.get());
       }
-      FG_LAUNCH(k_gnn_cams93<TS>, (unsigned)C, 128, 0, st, L, v.cam_edge_off, v.cam_edge, (const TS*)V, v.observed,
-                fac, v.lambda, s.X0.get(), s.mask.get());
+      FG_LAUNCH(k_gnn_cams93<TS>, (unsigned)C, 128, 0, st, L, v.cam_edge_off, v.cam_edge,
+                (const int32_t*)edgePos.get(), (const TS*)V, v.observed, fac, v.lambda, s.X0.get(), s.mask.get(),
+                edgeK.get());
       if (v.nedges && L.nP)
         FG_LAUNCH(k_gnn_pairs93, grid_for((size_t)L.nP * 32, 128), 128, 0, st, (int64_t)L.nP, C, v.pt_edge_off,
                   edgeK.get(), adj.get());
