@@ -413,7 +413,7 @@ def run_gpu(args, rank: int, world: int, device: int):
             if _lib.lib.fg_schur_time_operator_kernel(backend.handle, 1e-3, 50, C.byref(sec_k),
                                                      C.byref(bytes_k)) == 0:
                 results[name]["operator"].update(kernel_seconds=sec_k.value, kernel_bytes=bytes_k.value)
-            var, tuned = C.c_int(), (C.c_double * 5)()
+            var, tuned = C.c_int(), (C.c_double * 4)()
             _lib.lib.fg_schur_operator_info(backend.handle, C.byref(var), tuned)
             results[name]["operator"].update(variant=var.value, tuned_seconds=list(tuned))
             results[name]["assembly"] = assembly_timing(problem, backend, stream, data,
@@ -764,9 +764,7 @@ def main():
                                                2: "k_fast_apply_direct (reduced operator, direct-load single pass)",
                                                3: "k_fast_apply_pf (reduced operator, prefetching direct-load "
                                                   "single pass)",
-                                               4: "k_fast_apply (reduced operator, TMA-staged stage groups)",
-                                               5: "k_ring with FP32 shared camera sums (reduced operator, per-warp "
-                                                  "TMA-ring single pass)"}
+                                               4: "k_fast_apply (reduced operator, TMA-staged stage groups)"}
                           .get(op.get("variant"), "reduced operator")
                           if kern else "reduced operator", achieved=achieved, peak=pk,
                           peak_source=src, unit="GB/s", frac=(achieved / pk) if achieved else None,

@@ -141,8 +141,8 @@ class Schur:
         raise_for_status(lib.fg_schur_set_poll_limit(self._h, polls))
 
     def operator_info(self):
-        """(variant in use, measured seconds per application of variants 1..5)."""
-        var, sec = C.c_int(), (C.c_double * 5)()
+        """(variant in use, measured seconds per application of variants 1..4)."""
+        var, sec = C.c_int(), (C.c_double * 4)()
         raise_for_status(lib.fg_schur_operator_info(self._h, C.byref(var), sec))
         return var.value, list(sec)
 

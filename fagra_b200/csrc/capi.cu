@@ -373,10 +373,10 @@ FG_API fg_status fg_schur_time_operator(fg_backend* b, double lambda, size_t rep
   FG_GUARD_BEGIN return b->impl->time_operator(lambda, reps, seconds, bytes);
   FG_GUARD_END
 }
-FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds5) {
+FG_API fg_status fg_schur_operator_info(fg_backend* b, int* variant, double* seconds4) {
   FG_NEED(b);
   if (!variant) return FG_NULL_ARGUMENT;
-  b->impl->operator_info(variant, seconds5);
+  b->impl->operator_info(variant, seconds4);
   return FG_OK;
 }
 FG_API fg_status fg_schur_accumulate_pairs_device(fg_backend* b, size_t count, size_t rows,

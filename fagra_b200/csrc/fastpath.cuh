@@ -1204,8 +1204,6 @@ struct FastPath {
                                                                     RING_SLOTS_SHARED)),
           RingSmem<double, FAST_RHS, RACC_SHARED>::bytes(nc, false, ring_warps_shared<double>(), RING_SLOTS_SHARED));
       global_acc = need > (size_t)optin;
-      f32acc_fits = RingSmem<float, FAST_APPLY, RACC_SHARED_F32>::bytes(nc, false, ring_warps_shared<float>(),
-                                                                        RING_SLOTS_SHARED) <= (size_t)optin;
     } else {
       size_t need = std::max(FastSmem<TS, double>::bytes(nc, false), FastSmem<TS, TS>::bytes(nc, false));
       if (need > (size_t)optin) return false;  // accumulator does not fit one SM's shared memory
@@ -1232,33 +1230,18 @@ struct FastPath {
   // stage-group kernels need the shared accumulator and tiles of <= 32 edges).
   bool variant_ok(int v) const {
     if (!std::is_same<TS, float>::value) return true;
-    if (v == 5) return !global_acc && f32acc_fits;
     return v == 1 || (!global_acc && !has_deep);
   }
-  bool f32acc_fits = false;  // the FP32 shared accumulator (variant 5) fits next to the rings
 
   // The ring kernel in mode MODE on vectors TV; `reduce` as in apply.
   template <class TV, int MODE, class Impl>
   fg_status launch_ring(Impl& s, const TV* z, const TV* pv, const double* beta, TV* parts, const int* skip,
-                        const int* gate, FastExtra ex, bool f32acc = false) {
+                        const int* gate, FastExtra ex) {
     if (!optin) cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s.dev);
     FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
     const int64_t nc = (int64_t)s.nC;
     const float* er = reinterpret_cast<const float*>(d_erec.get());
     const float* pr = reinterpret_cast<const float*>(d_prec.get());
-    if constexpr (std::is_same<TV, float>::value && MODE == FAST_APPLY) {
-      if (f32acc && !global_acc && f32acc_fits) {
-        constexpr int NW = ring_warps_shared<TV>(), R = RING_SLOTS_SHARED;
-        using SM = RingSmem<TV, MODE, RACC_SHARED_F32>;
-        const bool xs = SM::bytes(nc, true, NW, R) <= (size_t)optin;
-        const size_t sm = SM::bytes(nc, xs, NW, R);
-        auto kern = xs ? k_ring<TV, MODE, RACC_SHARED_F32, true, NW, R> : k_ring<TV, MODE, RACC_SHARED_F32, false, NW, R>;
-        FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        FG_LAUNCH(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, parts, (void*)nullptr, skip, gate,
-                  d_error.get(), ex, poll_limit);
-        return FG_OK;
-      }
-    }
     if (!global_acc) {
       constexpr int NW = ring_warps_shared<TV>(), R = RING_SLOTS_SHARED;
       const bool xs = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, true, NW, R) <= (size_t)optin;
@@ -1348,8 +1331,7 @@ struct FastPath {
   int optin = 0;
   size_t attr_set[2][2] = {{0, 0}, {0, 0}};  // [TV is double][stage x] -> smem size already granted
 
-  int variant = 1;  // FP32 operator: 1 = ring (fixed point), 2 = direct global loads, 3 = prefetching direct,
-                    // 4 = TMA-staged stage groups, 5 = ring with the FP32 shared accumulator
+  int variant = 1;  // FP32 operator: 1 = TMA-staged stages, 2 = direct global loads, 3 = prefetching direct
 
   // reduce = false: the pass alone, leaving the per-CTA partial vectors (timing)
   template <class Impl, class TV>
@@ -1357,9 +1339,9 @@ struct FastPath {
                   const int* gate = nullptr, const double* lam_dev = nullptr, bool reduce = true) {
     TV* parts = std::is_same<TV, float>::value ? (TV*)d_parts_f.get() : (TV*)d_parts_d.get();
     if constexpr (std::is_same<TS, float>::value) {
-      if (variant == 1 || variant == 5 || !variant_ok(variant)) {
+      if (variant == 1 || !variant_ok(variant)) {
         FG_TRY((launch_ring<TV, FAST_APPLY>(s, x.z, x.pprev, x.beta, parts, pst ? &pst->done : nullptr, gate,
-                                            FastExtra{}, variant == 5 && variant_ok(5))));
+                                            FastExtra{})));
         if (!reduce) return FG_OK;
         if (global_acc)
           return launch_gacc_reduce<TV>(s, x.z, x.pprev, x.beta, lambda, lam_dev, 1, out, dparts, pst, gate,

@@ -18,13 +18,7 @@
 // Camera accumulation, chosen by the number of cameras:
 //  * shared (RACC_SHARED): the CTA-private 9C accumulator of k_fast_apply
 //    (64-bit fixed point in two 32-bit words for the operator, FP64 for the
-//    right-hand side), flushed to one partial row per CTA; the sums do not
-//    depend on the order of the additions;
-//  * shared FP32 (RACC_SHARED_F32, FP32 operator only): one FP32 shared
-//    reduction per value instead of two fixed-point atomics, with x staged at
-//    12 floats per camera and read with 16-byte loads; about 40 fewer shared-
-//    memory wavefronts per warp tile, the CTA's sums rounded in the order the
-//    warps arrive;
+//    right-hand side), flushed to one partial row per CTA;
 //  * global (RACC_GLOBAL, when 9C does not fit one SM): vector reductions
 //    red.global.add.v4.f32 into GACC_COPIES copies of a camera-padded
 //    accumulator (12 floats per camera), the copy chosen by CTA, summed in
@@ -55,8 +49,7 @@ constexpr int RING_SLOTS_GLOBAL = 2;
 constexpr int GACC_COPIES = 8;   // FP32 global accumulator copies
 constexpr int GACC_STRIDE = 12;  // floats per camera in an FP32 copy (three 16-byte vectors)
 constexpr unsigned RING_POLL_LIMIT = 1u << 22;
-enum RingAcc { RACC_SHARED = 0, RACC_GLOBAL = 1, RACC_SHARED_F32 = 2 };
-constexpr int XS12 = 12;  // floats per camera of the staged x of RACC_SHARED_F32
+enum RingAcc { RACC_SHARED = 0, RACC_GLOBAL = 1 };
 
 template <class TV, int MODE, int ACC>
 struct RingSmem {
@@ -64,13 +57,11 @@ struct RingSmem {
   static constexpr bool FIXED = MODE == FAST_APPLY && ACC == RACC_SHARED;
   static constexpr int FIXED_BITS = std::is_same<TV, float>::value ? 40 : 44;
   __host__ __device__ static size_t acc_bytes(int64_t ncam) {
-    if (ACC == RACC_SHARED_F32) return ((size_t)ncam * 9 * sizeof(float) + 127) & ~(size_t)127;
     if (ACC != RACC_SHARED || MODE == FAST_RECOVER) return 0;
     if (FIXED) return 2 * FastSmem<float, float>::word_bytes(ncam);
     return FastSmem<float, double>::vec_bytes(ncam);  // FAST_RHS: FP64
   }
   __host__ __device__ static size_t xs_bytes(int64_t ncam, bool xs) {
-    if (ACC == RACC_SHARED_F32) return xs ? ((size_t)ncam * XS12 * sizeof(float) + 127) & ~(size_t)127 : 0;
     return xs && MODE != FAST_RHS ? FastSmem<float, TV>::vec_bytes(ncam) : 0;
   }
   __host__ __device__ static size_t bytes(int64_t ncam, bool xs, int nw, int slots) {
@@ -130,11 +121,7 @@ struct RingScatter {
   double fx_mul;
   float fx_mulf;  // fx_mul in FP32 when it is a normal FP32 number, else 0
   __device__ __forceinline__ void add(uint32_t cam, const TV (&v)[9]) const {
-    if (ACC == RACC_SHARED_F32) {
-      float* y = reinterpret_cast<float*>(ylo) + (int64_t)cam * 9;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) atomicAdd(&y[c], (float)v[c]);
-    } else if (ACC == RACC_SHARED) {
+    if (ACC == RACC_SHARED) {
       if (RingSmem<TV, MODE, ACC>::FIXED) {
         fixed_scatter(ylo, yhi, (int64_t)cam * 9, v, fx_mul, fx_mulf);
       } else {
@@ -160,16 +147,8 @@ struct RingScatter {
 };
 
 // x for camera coordinates: staged copy, or z + beta p from global memory.
-template <class TV, bool XS, int ACC = RACC_SHARED>
+template <class TV, bool XS>
 __device__ __forceinline__ void ring_x(uint32_t cam, const TV* xs, const TV* z, const TV* pv, TV bv, TV (&xc)[9]) {
-  if constexpr (XS && ACC == RACC_SHARED_F32 && std::is_same<TV, float>::value) {
-    const float4* q = reinterpret_cast<const float4*>(xs + (int64_t)cam * XS12);
-    const float4 a = q[0], b = q[1];
-    xc[0] = a.x; xc[1] = a.y; xc[2] = a.z; xc[3] = a.w;
-    xc[4] = b.x; xc[5] = b.y; xc[6] = b.z; xc[7] = b.w;
-    xc[8] = xs[(int64_t)cam * XS12 + 8];
-    return;
-  }
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
     const int64_t i = (int64_t)cam * 9 + c;
@@ -204,9 +183,8 @@ __global__ void __launch_bounds__(NW * 32, 1)
 
   const TV bv = pv ? (TV)*beta : (TV)0;
   double xmax = 0.0;
-  if (ACC == RACC_SHARED || ACC == RACC_SHARED_F32 || XS || FIXED) {
+  if (ACC == RACC_SHARED || XS || FIXED) {
     for (int64_t i = tid; i < ny; i += NTHR) {
-      if (ACC == RACC_SHARED_F32) ylo[i] = 0u;  // FP32 zero
       if (ACC == RACC_SHARED && SCATTER) {
         if (FIXED) {
           ylo[i] = 0;
@@ -217,7 +195,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
       }
       if (NEED_X && (XS || FIXED)) {
         const TV xi = pv ? z[i] + bv * pv[i] : z[i];
-        if (XS) xs[ACC == RACC_SHARED_F32 ? (i / 9) * XS12 + i % 9 : i] = xi;
+        if (XS) xs[i] = xi;
         if (FIXED) xmax = isfinite((double)xi) ? fmax(xmax, fabs((double)xi)) : (double)INFINITY;
       }
     }
@@ -254,7 +232,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
   sc.fx_mulf = FIXED ? fixed_mulf(fx_mul_s) : 0.f;
   sc.gf = ACC == RACC_GLOBAL ? reinterpret_cast<float*>(gacc) + (int64_t)(blockIdx.x % GACC_COPIES) * ncam * GACC_STRIDE
                              : nullptr;
-  sc.yd = ACC == RACC_SHARED || ACC == RACC_SHARED_F32 ? yds : reinterpret_cast<double*>(gacc);
+  sc.yd = ACC == RACC_SHARED ? yds : reinterpret_cast<double*>(gacc);
 
   const int64_t G = (int64_t)gridDim.x * NW;
   const int64_t first = (int64_t)blockIdx.x * NW + w;
@@ -317,7 +295,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
       TV u0 = 0, u1 = 0, u2 = 0;
       if (NEED_X && lane < t.cnt) {
         TV xc[9];
-        ring_x<TV, XS, ACC>(cam, xs, z, pv, bv, xc);
+        ring_x<TV, XS>(cam, xs, z, pv, bv, xc);
 #pragma unroll
         for (int c = 0; c < 9; ++c) {
           u0 += E[c] * xc[c];
@@ -377,7 +355,7 @@ __global__ void __launch_bounds__(NW * 32, 1)
 #pragma unroll
             for (int i = 0; i < 27; ++i) E[i] = (TV)Ef[i];
             TV xc[9];
-            ring_x<TV, XS, ACC>(cam, xs, z, pv, bv, xc);
+            ring_x<TV, XS>(cam, xs, z, pv, bv, xc);
 #pragma unroll
             for (int c = 0; c < 9; ++c) {
               u0 += E[c] * xc[c];
@@ -446,13 +424,10 @@ __global__ void __launch_bounds__(NW * 32, 1)
       if (kj < nmine) warp_wait(&wbar[kj % R], (unsigned)((kj / R) & 1), RING_POLL_LIMIT);
     }
   }
-  if ((ACC != RACC_SHARED && ACC != RACC_SHARED_F32) || !SCATTER) return;
+  if (ACC != RACC_SHARED || !SCATTER) return;
   __syncthreads();
   TV* out = partials + (int64_t)blockIdx.x * ny;
-  if (ACC == RACC_SHARED_F32) {
-    const float* yf = reinterpret_cast<const float*>(ylo);
-    for (int64_t i = tid; i < ny; i += NTHR) out[i] = (TV)yf[i];
-  } else if (FIXED) {
+  if (FIXED) {
     const double unit = fx_unit_s;
     for (int64_t i = tid; i < ny; i += NTHR) {
       const long long q = (long long)(((unsigned long long)yhi[i] << 32) | (unsigned long long)ylo[i]);

@@ -173,7 +173,7 @@ class SchurImpl final : public Backend {
       return FG_INVALID_OPTIONS;
     }
     if (o.operator_variant < 0 || o.operator_variant > NVARIANTS) {
-      set_error("operator_variant must be 0 (autotune) or 1..5");
+      set_error("operator_variant must be 0 (autotune) or 1..4");
       return FG_INVALID_OPTIONS;
     }
     if (o.learned_policy != 0 && o.learned_policy != 1) {
@@ -949,7 +949,7 @@ class SchurImpl final : public Backend {
   // direct loads, TMA-staged stage groups) and keeps the fastest. Runs once
   // per structure shape (device, cameras, points, edges, warp tiles) in the
   // process; the factorization it needs is redone by every solve.
-  static constexpr int NVARIANTS = 5;
+  static constexpr int NVARIANTS = 4;
   struct TunedShape {
     int dev;
     int64_t ncam, npt, nedge, nwt;
@@ -969,7 +969,7 @@ class SchurImpl final : public Backend {
     static auto* m = new std::map<TunedShape, TunedChoice>();
     return *m;
   }
-  double tuned_seconds[NVARIANTS] = {0, 0, 0, 0, 0};
+  double tuned_seconds[NVARIANTS] = {0, 0, 0, 0};
   fg_status set_poll_limit(unsigned polls) override {
     fast.poll_limit = polls ? polls : RING_POLL_LIMIT;
     drop_graphs();

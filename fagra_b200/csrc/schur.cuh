@@ -124,10 +124,9 @@ class Backend {
   virtual fg_status time_operator_kernel(double, size_t, double*, double*) { return not_schur(); }
   virtual fg_status attach_learned(fg_gnn*) { return not_schur(); }
   virtual fg_status capture_system(fg_gnn*, double, size_t, uint64_t, int, size_t*) { return not_schur(); }
-  virtual void operator_info(int* variant, double* seconds5) const {
+  virtual void operator_info(int* variant, double* seconds4) const {
     *variant = 0;
-    if (seconds5)
-      for (int v = 0; v < 5; ++v) seconds5[v] = 0;
+    if (seconds4) seconds4[0] = seconds4[1] = seconds4[2] = seconds4[3] = 0;
   }
   virtual fg_status set_poll_limit(unsigned) { return not_schur(); }
   virtual fg_status accumulate_pairs(size_t, size_t, const uint32_t*, const uint32_t*, const double*, const double*,

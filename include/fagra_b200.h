@@ -86,7 +86,7 @@ typedef struct {
                                   residual b - S x each time it falls by this factor; default 0 =
                                   automatic: the reduction to the relative tolerance split into the
                                   fewest equal factors of at most 1e-4 */
-  int operator_variant;        /* FP32 BAL-shaped systems: 0 = autotune (default), 1..5 = force the
+  int operator_variant;        /* FP32 BAL-shaped systems: 0 = autotune (default), 1..4 = force the
                                   reduced-operator variant of fg_schur_operator_info (a variant
                                   that does not apply to the structure falls back to 1) */
   int coarse_correction;       /* 1: two-level PCG, z = M r + W (W^T S W)^-1 W^T r with the coarse
@@ -396,14 +396,13 @@ FG_API fg_status fg_schur_time_operator_kernel(fg_backend* backend, double lambd
                                                double* seconds_per_launch, double* bytes_out);
 
 /* The reduced-operator implementation the autotuner chose for the current
- * structure: 0 generic (any widths), 1 per-warp TMA-ring single pass with
- * fixed-point camera sums (the only one for more cameras than one SM's shared
- * memory holds; sums independent of the order of additions), 2 direct-load
- * single pass, 3 prefetching direct-load single pass, 4 TMA-staged stage
- * groups, 5 the ring pass with FP32 shared camera sums (rounded in arrival
- * order); seconds5[v-1] (may be NULL, 5 entries) = measured time per
- * application of variant v (0 if not measured or not applicable). */
-FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds5);
+ * structure: 0 generic (any widths), 1 per-warp TMA-ring single pass (the only
+ * one for more cameras than one SM's shared memory holds, or points with more
+ * than 32 observations), 2 direct-load single pass, 3 prefetching direct-load
+ * single pass, 4 TMA-staged stage groups; seconds4[v-1] (may be NULL) =
+ * measured time per application of variant v (0 if not measured or not
+ * applicable). */
+FG_API fg_status fg_schur_operator_info(fg_backend* backend, int* variant, double* seconds4);
 /* Test hook (no reference counterpart): the number of polls after which the
  * ring operator's consumer wait on a shared-memory slot gives up; the kernel
  * then drains its copies in flight (with the full limit), raises the error

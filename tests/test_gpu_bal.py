@@ -150,7 +150,7 @@ def test_fp32_operator_variants_give_the_same_step():
     itself at ~1e-7, hence the looser bound against the f64 step)."""
     d = synthetic.generate("bal1k", cameras=64, points=8000, seed=5)
     steps, its = {}, {}
-    for variant in (0, 1, 2, 3, 4, 5):
+    for variant in (0, 1, 2, 3, 4):
         b = fg.Schur(9 * d.num_cameras, 9, 3, precision="f64" if variant == 0 else "f32")
         if variant:
             b.operator_variant = variant
@@ -164,7 +164,7 @@ def test_fp32_operator_variants_give_the_same_step():
             assert b.operator_info()[0] == variant
             assert b.diagnostics().reduced_relative_residual < 1e-8
     ref = np.linalg.norm(steps[0])
-    for v in (1, 2, 3, 4, 5):
+    for v in (1, 2, 3, 4):
         assert np.linalg.norm(steps[v] - steps[0]) <= 1e-4 * ref, v
         assert np.linalg.norm(steps[v] - steps[1]) <= 1e-6 * ref, v
         # FP32 accumulation order (atomics, per-CTA partials) moves the count by a few iterations
