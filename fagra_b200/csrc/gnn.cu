@@ -186,19 +186,26 @@ __global__ void __launch_bounds__(128, 1) k_gemm(int M, int N, int K, const TA* 
   const uint32_t tmem = tmem_base;
   bool ok = true;
   int issued = 0;
+  // chunk c + 1 is fetched into registers while chunk c is placed and issued
+  TileRegs<UM> ta;
+  TileRegs<UN> tb;
+  if (nchunks > 0) {
+    fetch_tile<UM, !TRA>(ta, A, lda, m0, M, kb, ke, vec_a != 0);
+    fetch_tile<UN, TRB>(tb, B, ldb, n0, N, kb, ke, vec_b != 0);
+  }
   for (int c = 0; c < nchunks; ++c) {
     const int s = c & 1;
     if (c >= 2) ok = umma_wait(s ? bar1 : bar0, ((c - 2) >> 1) & 1, err);
     if (!__syncthreads_and(ok)) break;  // stage s is free again (or the wait gave up everywhere)
-    const int k0 = kb + c * UK;
     uint8_t* sa = base + s * UTILE_A;
     uint8_t* sb = base + 2 * UTILE_A + s * UTILE_B;
-    TileRegs<UM> ta;
-    TileRegs<UN> tb;
-    fetch_tile<UM, !TRA>(ta, A, lda, m0, M, k0, ke, vec_a != 0);
-    fetch_tile<UN, TRB>(tb, B, ldb, n0, N, k0, ke, vec_b != 0);
     place_tile<UM, !TRA>(sa, ta);
     place_tile<UN, TRB>(sb, tb);
+    if (c + 1 < nchunks) {
+      const int k1 = kb + (c + 1) * UK;
+      fetch_tile<UM, !TRA>(ta, A, lda, m0, M, k1, ke, vec_a != 0);
+      fetch_tile<UN, TRB>(tb, B, ldb, n0, N, k1, ke, vec_b != 0);
+    }
     umma_fence_smem();
     __syncthreads();
     if (tid == 0) {
@@ -344,7 +351,9 @@ fg_status gemm(cudaStream_t st, int nsm, int M, int N, int K, const TA* A, int l
   const unsigned gx = (unsigned)((M + UM - 1) / UM), gy = (unsigned)((N + UN - 1) / UN);
   int splits = 1;
   if (allow_split && EPI == EPI_STORE && K > 2 * UK) {
-    const int want = std::max(1, (2 * nsm) / (int)(gx * gy));
+    // up to four CTAs per SM (50 KB of shared memory each): the K chunks of a
+    // CTA run one after another, so the memory parallelism is in the CTA count
+    const int want = std::max(1, (4 * nsm) / (int)(gx * gy));
     splits = std::min(want, (K + UK - 1) / UK);
   }
   int kchunk = (K + splits - 1) / splits;
