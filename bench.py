@@ -55,6 +55,8 @@ def parse():
                     help="ba: Schur-PCG time to cost (default); lsmr: the same with the LSMR backend; "
                          "windows: the batched pose-graph windows; learned: the learned preconditioner's "
                          "training and inference steps")
+    ap.add_argument("--cameras", type=int, default=0,
+                    help="learned suite: time the network on a seeded system of this many cameras")
     ap.add_argument("--windows", type=int, default=4096)
     ap.add_argument("--max-poses", type=int, default=300)
     return ap.parse_args()
@@ -558,8 +560,23 @@ def run_learned(args, device: int) -> dict:
     from fagra_b200 import synthetic
     torch.cuda.set_device(device)
     stream = torch.cuda.ExternalStream(fg.device_stream(device), device=device)
-    net, info = train_network(fg, synthetic, args.workload, device, problems=1)
-    C = net.export_system(0)["features"].shape[0]
+    if args.cameras:
+        # a seeded system of the given size instead of captured ones: node features
+        # N(0, 0.01), a 20%-filled row-normalized covisibility, two probe pairs
+        import numpy as np
+        C = args.cameras
+        rng = np.random.default_rng(7)
+        net = fg.LearnedPreconditioner(seed=7, device=device)
+        X0 = (rng.normal(size=(C, 64)) * 0.1).astype(np.float32)
+        A = (rng.random((C, C), dtype=np.float32) < 0.2).astype(np.float32)
+        A /= np.maximum(A.sum(1, keepdims=True), 1)
+        px = rng.normal(size=(2, C, 9)).astype(np.float32)
+        net.import_system(X0, A, px, 0.5 * px, np.ones(C, np.uint8))
+        del A
+        info = dict(system=f"seeded: {C} cameras, 20% covisibility, 2 probe pairs")
+    else:
+        net, info = train_network(fg, synthetic, args.workload, device, problems=1)
+        C = net.export_system(0)["features"].shape[0]
     # GEMM FLOPs: forward 2C(64*64 + 3(C*64 + 128*64) + 64*64); backward twice that
     fwd = 2.0 * C * (64 * 64 + 3 * (C * 64 + 128 * 64) + 64 * 64)
     for _ in range(args.warmup):
@@ -582,12 +599,13 @@ def run_learned(args, device: int) -> dict:
     return dict(metric=f"learned preconditioner training step ({args.workload} reduced camera systems)",
                 value=t_train, unit="s", n_gpus=1, steps=n, warmup=args.warmup, ms_per_step=t_train * 1e3,
                 higher_is_better=False, scaling="weak", vs_baseline=None, dtype="bf16 operands, f32 accumulate",
-                data="synthetic", config=dict(workload=args.workload, cameras=C, network="3 layers, hidden 64",
+                data="synthetic", config=dict(workload=args.workload if not args.cameras else "seeded system",
+                                              cameras=C, network="3 layers, hidden 64",
                                               training=info),
                 forward_seconds=t_fwd,
                 roofline=dict(bound="tensor", unit="TFLOP/s", achieved=achieved, peak=pk,
                               frac=(achieved / pk) if pk else None, flops_per_step=3 * fwd,
-                              note="GEMMs of 16-64 CTAs: latency-bound at this size"))
+                              note="tcgen05 GEMMs, load-latency-bound at these shapes (N = 64)"))
 
 
 def run_lsmr(args, device: int) -> dict:

@@ -511,6 +511,8 @@ class LsmrImpl final : public Backend {
   int64_t point_col0 = -1, pp0 = 0;  // BAL: first point column / first point piece
   bool ptvals_current = false;
   DBuf<TS> d_ptvals;
+  int fused_ncam = 0;            // > 0: the fused BAL iteration pass applies (camera segments)
+  DBuf<double> d_csum, d_pcon;   // its camera column sums and per-emission point contributions
   int32_t n_wide = 0, n_narrow = 0;
   int maxw = 4;
   bool variables_consistent = true, variables_too_wide = false;
@@ -747,8 +749,33 @@ class LsmrImpl final : public Backend {
     FG_TRY(upload(d_entry_rc, erc.data(), erc.size(), st));
     FG_TRY(d_gram.resize(std::max<int64_t>(n_fac, 1)));
     FG_TRY(d_factors.resize(std::max<int64_t>(n_fac, 1)));
-    const size_t parts =
-        std::max<size_t>((size_t)std::max<unsigned>(segment_grid() * SEG_K, emission_grid() + bottom_grid()), 8192);
+    // The fused iteration pass (device BAL layout): camera segments first, one
+    // 9-column camera block each, their pieces the camera blocks of one
+    // contiguous range of emissions in order; then 3-column point segments of
+    // point blocks.
+    fused_ncam = 0;
+    if (point_col0 > 0 && point_col0 <= n) {
+      const int64_t ncs = point_col0 == n ? S : segof[point_col0];
+      bool ok = ncs * 9 == point_col0;
+      for (int64_t sg = 0; sg < ncs && ok; ++sg) {
+        ok = scol[sg + 1] - scol[sg] == 9;
+        const int64_t q0 = spc[sg], q1 = spc[sg + 1];
+        for (int64_t q = q0; q < q1 && ok; ++q) ok = pstart[q] % 24 == 0 && pstart[q] == pstart[q0] + 24 * (q - q0);
+      }
+      for (int64_t sg = ncs; sg < S && ok; ++sg) {
+        ok = scol[sg + 1] - scol[sg] == 3;
+        for (int64_t q = spc[sg]; q < spc[sg + 1] && ok; ++q) ok = pstart[q] % 24 == 18;
+      }
+      if (ok && ncs > 0 && ncs < (int64_t)1 << 30) fused_ncam = (int)ncs;
+    }
+    if (fused_ncam) {
+      FG_TRY(d_csum.resize((size_t)9 * fused_ncam));
+      FG_TRY(d_pcon.resize(std::max<size_t>((size_t)3 * E, 1)));
+    }
+    const size_t parts = std::max<size_t>(
+        (size_t)std::max<unsigned>(std::max<unsigned>(segment_grid() * SEG_K, emission_grid() + bottom_grid()),
+                                   (unsigned)fused_ncam + bottom_grid()),
+        8192);
     FG_TRY(d_partials.resize(parts));
     FG_TRY(resize_rows(rows));
     FG_CUDA(cudaStreamSynchronize(st));  // host staging vectors die here
@@ -887,13 +914,27 @@ class LsmrImpl final : public Backend {
     const bool block = gmode == GRAPH_BLOCK;
     LsmrDev<TS> D = view(graph_scales(gmode), block);
     const unsigned eb = emission_grid(), bb = gmode == GRAPH_UNDAMPED ? 0 : bottom_grid();
-    if (tf) tf->start(st);
-    FG_LAUNCH((k_lsmr_rows<TS, ROWS_ITER>), eb + bb, LSMR_NT, 0, st, D, eb, d_w.get(), d_u.get(), d_ub.get(),
-              d_negres.get(), d_pr.get(), d_partials.get(), d_state.get(), d_ver.get());
-    if (tf) tim.forward += tf->stop(st);
-    if (tt) tt->start(st);
-    FG_TRY(launch_segments<SEG_ITER>(iteration_args(gmode), D));
-    if (tt) tim.transpose += tt->stop(st);
+    if (fused_ncam && D.bal) {
+      // one read of the emissions: u <- J w - alpha u with the camera sums and
+      // point contributions of J^T u, then every segment's finish
+      if (tf) tf->start(st);
+      FG_LAUNCH((k_lsmr_fused_rows<TS>), (unsigned)fused_ncam + bb, LSMR_NT, 0, st, D, fused_ncam, d_w.get(),
+                d_u.get(), d_ub.get(), d_csum.get(), d_pcon.get(), d_partials.get(), d_state.get());
+      if (tf) tim.forward += tf->stop(st);
+      if (tt) tt->start(st);
+      LSMR_DISPATCH(maxw, FG_LAUNCH((k_lsmr_fused_segments<TS, MW_>), grid_for(std::max<int64_t>(S, 1), LSMR_NT),
+                                    LSMR_NT, 0, st, D, iteration_args(gmode), fused_ncam, d_csum.get(),
+                                    d_pcon.get(), d_partials.get(), d_state.get()));
+      if (tt) tim.transpose += tt->stop(st);
+    } else {
+      if (tf) tf->start(st);
+      FG_LAUNCH((k_lsmr_rows<TS, ROWS_ITER>), eb + bb, LSMR_NT, 0, st, D, eb, d_w.get(), d_u.get(), d_ub.get(),
+                d_negres.get(), d_pr.get(), d_partials.get(), d_state.get(), d_ver.get());
+      if (tf) tim.forward += tf->stop(st);
+      if (tt) tt->start(st);
+      FG_TRY(launch_segments<SEG_ITER>(iteration_args(gmode), D));
+      if (tt) tim.transpose += tt->stop(st);
+    }
     if (tp) tp->start(st);
     FG_TRY(launch_update(gmode, D));
     if (tp) tim.preconditioner += tp->stop(st);
@@ -1029,6 +1070,14 @@ class LsmrImpl final : public Backend {
     const double nb = (double)b_bcol.size();
     double fwd = nv * s + 2 * m * s + (double)E * 24 + nb * 12 + n * 8;
     double tr = nv * s + m * s + (double)npieces * 20 + (double)S * 20;
+    if (fused_ncam && source == DEVICE) {
+      // one read of the values: u in and out, the point block's column index
+      // and w, the point contributions out and back in (3 doubles per
+      // emission), the camera sums out and in, the point pieces' starts
+      const double nc = (double)fused_ncam, E_ = (double)E;
+      fwd = nv * s + 2 * m * s + E_ * (8 + 24) + E_ * 24 + nc * (72 + 72);
+      tr = E_ * 24 + E_ * 8 + nc * 72 + (double)S * 16;
+    }
     double upd = n * 8 * 9 + (double)S * 8;
     if (gmode != GRAPH_UNDAMPED) {
       fwd += n * 8 * 3;  // scales, bottom rows in and out

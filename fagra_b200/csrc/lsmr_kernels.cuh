@@ -395,68 +395,10 @@ __device__ __forceinline__ void segment_finish(const LsmrDev<TS>& D, int64_t s, 
   }
 }
 
-// Segment pass: blocks [0, n_wide) take one wide segment each with all their
-// threads; the remaining blocks take one narrow segment per thread.
-template <class TS, int MAXW, int MODE>
-__global__ void __launch_bounds__(LSMR_NT) k_lsmr_segments(LsmrDev<TS> D, SegArgs a, double* partials,
-                                                            LsmrState* st, LsmrVerify* vs) {
-  if ((MODE == SEG_ITER) && st->stop) return;
-  constexpr bool SQ = MODE == SEG_SQUARES;
-  double part[SEG_K] = {0, 0, 0, 0, 0, 0};
-  double mn = INFINITY, mx = 0;
-  double acc[MAXW];
-#pragma unroll
-  for (int j = 0; j < MAXW; ++j) acc[j] = 0;
-  if ((int)blockIdx.x < D.n_wide) {
-    const int64_t s = D.s_wide[blockIdx.x];
-    const int w = (int)(D.s_col[s + 1] - D.s_col[s]);
-    if (MODE == SEG_VERIFY || MODE == SEG_GRADIENT || MODE == SEG_PRODUCT)
-      segment_accumulate<TS, MAXW, SQ>(D, s, w, threadIdx.x, blockDim.x, (const double*)a.vec, acc);
-    else
-      segment_accumulate<TS, MAXW, SQ>(D, s, w, threadIdx.x, blockDim.x, (const TS*)a.vec, acc);
-    __shared__ double red[LSMR_NT / 32][MAXW];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int j = 0; j < MAXW; ++j) {
-      double x = warp_sum(acc[j]);
-      if (lane == 0) red[warp][j] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int j = 0; j < MAXW; ++j) {
-        double x = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) x += red[k][j];
-        acc[j] = x;
-      }
-      segment_finish<TS, MAXW, MODE>(D, s, w, acc, a, st, part, mn, mx);
-    }
-  } else {
-    const int64_t idx = (blockIdx.x - D.n_wide) * (int64_t)blockDim.x + threadIdx.x;
-    if (idx < D.n_narrow) {
-      const int64_t s = D.s_narrow[idx];
-      const int w = (int)(D.s_col[s + 1] - D.s_col[s]);
-      if (MODE == SEG_VERIFY || MODE == SEG_GRADIENT || MODE == SEG_PRODUCT)
-        segment_accumulate<TS, MAXW, SQ>(D, s, w, 0, 1, (const double*)a.vec, acc);
-      else
-        segment_accumulate<TS, MAXW, SQ>(D, s, w, 0, 1, (const TS*)a.vec, acc);
-      segment_finish<TS, MAXW, MODE>(D, s, w, acc, a, st, part, mn, mx);
-    }
-  }
-  if (MODE == SEG_GRADIENT || MODE == SEG_PRODUCT) return;
-  if (MODE == SEG_SQUARES) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
-      mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-      if (mn < INFINITY) atomicMin(&((LsmrState*)st)->min_scale_bits, (unsigned long long)__double_as_longlong(mn));
-      if (mx > 0) atomicMax(&((LsmrState*)st)->max_scale_bits, (unsigned long long)__double_as_longlong(mx));
-      if (part[5] != 0) ((LsmrState*)st)->nonfinite_scales = 1;
-    }
-    return;
-  }
+// The end of a segment pass: block sums of the partials, the last block's
+// totals, and for ITER / START the scalar recurrences.
+template <int MODE>
+__device__ __forceinline__ void seg_tail(double (&part)[SEG_K], double* partials, LsmrState* st, LsmrVerify* vs) {
   block_sums<SEG_K>(part);
   if (threadIdx.x == 0)
 #pragma unroll
@@ -535,6 +477,190 @@ __global__ void __launch_bounds__(LSMR_NT) k_lsmr_segments(LsmrDev<TS> D, SegArg
     st->termination = 1;
   }
   st->upd = 1;
+}
+
+// Segment pass: blocks [0, n_wide) take one wide segment each with all their
+// threads; the remaining blocks take one narrow segment per thread.
+template <class TS, int MAXW, int MODE>
+__global__ void __launch_bounds__(LSMR_NT) k_lsmr_segments(LsmrDev<TS> D, SegArgs a, double* partials,
+                                                            LsmrState* st, LsmrVerify* vs) {
+  if ((MODE == SEG_ITER) && st->stop) return;
+  constexpr bool SQ = MODE == SEG_SQUARES;
+  double part[SEG_K] = {0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = 0;
+  double acc[MAXW];
+#pragma unroll
+  for (int j = 0; j < MAXW; ++j) acc[j] = 0;
+  if ((int)blockIdx.x < D.n_wide) {
+    const int64_t s = D.s_wide[blockIdx.x];
+    const int w = (int)(D.s_col[s + 1] - D.s_col[s]);
+    if (MODE == SEG_VERIFY || MODE == SEG_GRADIENT || MODE == SEG_PRODUCT)
+      segment_accumulate<TS, MAXW, SQ>(D, s, w, threadIdx.x, blockDim.x, (const double*)a.vec, acc);
+    else
+      segment_accumulate<TS, MAXW, SQ>(D, s, w, threadIdx.x, blockDim.x, (const TS*)a.vec, acc);
+    __shared__ double red[LSMR_NT / 32][MAXW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < MAXW; ++j) {
+      double x = warp_sum(acc[j]);
+      if (lane == 0) red[warp][j] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int j = 0; j < MAXW; ++j) {
+        double x = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) x += red[k][j];
+        acc[j] = x;
+      }
+      segment_finish<TS, MAXW, MODE>(D, s, w, acc, a, st, part, mn, mx);
+    }
+  } else {
+    const int64_t idx = (blockIdx.x - D.n_wide) * (int64_t)blockDim.x + threadIdx.x;
+    if (idx < D.n_narrow) {
+      const int64_t s = D.s_narrow[idx];
+      const int w = (int)(D.s_col[s + 1] - D.s_col[s]);
+      if (MODE == SEG_VERIFY || MODE == SEG_GRADIENT || MODE == SEG_PRODUCT)
+        segment_accumulate<TS, MAXW, SQ>(D, s, w, 0, 1, (const double*)a.vec, acc);
+      else
+        segment_accumulate<TS, MAXW, SQ>(D, s, w, 0, 1, (const TS*)a.vec, acc);
+      segment_finish<TS, MAXW, MODE>(D, s, w, acc, a, st, part, mn, mx);
+    }
+  }
+  if (MODE == SEG_GRADIENT || MODE == SEG_PRODUCT) return;
+  if (MODE == SEG_SQUARES) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+      mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (mn < INFINITY) atomicMin(&((LsmrState*)st)->min_scale_bits, (unsigned long long)__double_as_longlong(mn));
+      if (mx > 0) atomicMax(&((LsmrState*)st)->max_scale_bits, (unsigned long long)__double_as_longlong(mx));
+      if (part[5] != 0) ((LsmrState*)st)->nonfinite_scales = 1;
+    }
+    return;
+  }
+  seg_tail<MODE>(part, partials, st, vs);
+}
+
+// ------------------------------------------------ fused BAL iteration pass
+// For the device BAL layout with camera-major emissions (camera c's emissions
+// are one contiguous range, the pieces of camera segment c) the row pass and
+// the transposed pass of an ITER step read each emission's 24 values once:
+// k_lsmr_fused_rows: one CTA per camera segment: u <- J w - alpha u for the
+//   camera's emissions (u written back, ||u||^2), the camera's column sums of
+//   J^T u (FP64, threads strided over the emissions, warp then CTA sums, as the
+//   wide-segment pass), and each emission's point contribution J_p^T u (3
+//   doubles at 3e); the remaining blocks update the bottom rows as k_lsmr_rows.
+// k_lsmr_fused_segments: thread per segment: camera sums, or the point's
+//   contributions summed in piece order, then segment_finish / seg_tail.
+template <class TS>
+__global__ void __launch_bounds__(LSMR_NT) k_lsmr_fused_rows(LsmrDev<TS> D, int ncam, const double* w, TS* u,
+                                                              double* ub, double* csum, double* pcon,
+                                                              double* partials, LsmrState* st) {
+  if (st->stop) return;
+  const double f = st->alpha * lsmr_inv(st->beta), root = st->root;
+  double sq[1] = {0.0};
+  if ((int)blockIdx.x < ncam) {
+    const int64_t s = blockIdx.x;
+    const int64_t p0 = D.s_pc[s], np = D.s_pc[s + 1] - p0;
+    const int64_t e0 = np ? D.p_start[p0] / 24 : 0;
+    __shared__ double wc[9];
+    __shared__ double red[LSMR_NT / 32][9];
+    if (threadIdx.x < 9) wc[threadIdx.x] = w[D.s_col[s] + threadIdx.x];
+    __syncthreads();
+    double acc[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) acc[j] = 0;
+    for (int64_t i = threadIdx.x; i < np; i += LSMR_NT) {
+      const int64_t e = e0 + i;
+      double v[24];
+      load_vals<24>(D.values + 24 * e, v);
+      const double* wp = w + D.b_col[2 * e + 1];
+      const double wp0 = wp[0], wp1 = wp[1], wp2 = wp[2];
+      double x[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {  // emission_rows_bal's summation order
+        double a = 0;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) a += v[2 * j + r] * wc[j];
+        a += v[18 + r] * wp0;
+        a += v[20 + r] * wp1;
+        a += v[22 + r] * wp2;
+        const double y = a - f * (double)u[2 * e + r];
+        u[2 * e + r] = (TS)y;
+        sq[0] += y * y;
+        x[r] = (double)(TS)y;  // the transposed pass reads the stored u
+      }
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        acc[j] += v[2 * j] * x[0];
+        acc[j] += v[2 * j + 1] * x[1];
+      }
+      double* pc = pcon + 3 * e;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) pc[j] = v[18 + 2 * j] * x[0] + v[18 + 2 * j + 1] * x[1];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const double t = warp_sum(acc[j]);
+      if (lane == 0) red[warp][j] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 9) {
+      double t = 0;
+      for (int k = 0; k < LSMR_NT / 32; ++k) t += red[k][threadIdx.x];
+      csum[9 * s + threadIdx.x] = t;
+    }
+  } else {
+    const int64_t j = (blockIdx.x - ncam) * (int64_t)blockDim.x + threadIdx.x;
+    if (j < D.n) {
+      const double sc = D.scales ? D.scales[j] : 1.0;
+      const double x = root * sc * w[j] - f * ub[j];
+      ub[j] = x;
+      sq[0] += x * x;
+    }
+  }
+  block_sums<1>(sq);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sq[0];
+  if (arrive_last(&st->counter0)) {
+    double tot[1];
+    finish_sums<1>(partials, tot);
+    if (threadIdx.x == 0) {
+      st->beta_next = sqrt(tot[0]);
+      st->counter0 = 0;
+    }
+  }
+}
+
+template <class TS, int MAXW>
+__global__ void __launch_bounds__(LSMR_NT) k_lsmr_fused_segments(LsmrDev<TS> D, SegArgs a, int ncam,
+                                                                  const double* csum, const double* pcon,
+                                                                  double* partials, LsmrState* st) {
+  if (st->stop) return;
+  double part[SEG_K] = {0, 0, 0, 0, 0, 0};
+  double mn = INFINITY, mx = 0;
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s < D.S) {
+    const int w = (int)(D.s_col[s + 1] - D.s_col[s]);
+    double acc[MAXW];
+#pragma unroll
+    for (int j = 0; j < MAXW; ++j) acc[j] = 0;
+    if (s < ncam) {
+#pragma unroll
+      for (int j = 0; j < (MAXW < 9 ? MAXW : 9); ++j) acc[j] = csum[9 * s + j];
+    } else {
+      for (int64_t p = D.s_pc[s]; p < D.s_pc[s + 1]; ++p) {
+        const double* pc = pcon + 3 * (D.p_start[p] / 24);
+#pragma unroll
+        for (int j = 0; j < (MAXW < 3 ? MAXW : 3); ++j) acc[j] += pc[j];
+      }
+    }
+    segment_finish<TS, MAXW, SEG_ITER>(D, s, w, acc, a, st, part, mn, mx);
+  }
+  seg_tail<SEG_ITER>(part, partials, st, nullptr);
 }
 
 // v /= alpha; hbar = h - c_hbar hbar; y += c_y hbar; h = v - c_h h; w = M v (/ D).
