@@ -321,7 +321,13 @@ def run_gpu(args, rank: int, world: int, device: int):
              "f64": dict(precision="f64", preconditioner="retained_blocks", tol=1e-10),
              "f32": dict(precision="f32", preconditioner="retained_blocks", tol=1e-10),
              "f64sd": dict(precision="f64", preconditioner="schur_diagonal", tol=1e-10),
-             "fastsd": dict(precision="f32", preconditioner="schur_diagonal", tol=1e-8)}
+             "fastsd": dict(precision="f32", preconditioner="schur_diagonal", tol=1e-8),
+             # fastc for the first five accepted steps, then the f64 form from
+             # those estimates (FP32 records stop being accurate enough near the
+             # optimum of the ill-conditioned bal10k systems)
+             "fastc_f64": dict(precision="f32", preconditioner="retained_blocks", coarse_correction=True, tol=1e-8,
+                               then=dict(precision="f64", preconditioner="retained_blocks", tol=1e-10),
+                               switch_after=5)}
     results = {}
     net_cache = None
     head = args.forms.split(",")[0]
@@ -332,8 +338,18 @@ def run_gpu(args, rank: int, world: int, device: int):
         kw = dict(forms[name])
         tol = kw.pop("tol")
         policy = kw.pop("learned_policy", None)
+        then = kw.pop("then", None)
+        switch_after = kw.pop("switch_after", None)
         backend = fg.Schur(9 * data.num_cameras, 9, 3, device=device, **kw)
         backend.relative_tolerance = tol
+        then_backend = None
+        if then:
+            tk = dict(then)
+            ttol = tk.pop("tol")
+            then_backend = fg.Schur(9 * data.num_cameras, 9, 3, device=device, **tk)
+            then_backend.relative_tolerance = ttol
+            oo_first = fg.OptimizeOptions(switch_after, 1e-8, 0.0, 0.0).c()
+            kw["then"] = dict(then, switch_after=switch_after)
         if policy:
             backend.learned_policy = policy
             kw["learned_policy"] = policy
@@ -366,9 +382,21 @@ def run_gpu(args, rank: int, world: int, device: int):
         def step():
             _lib.lib.fg_bal_restore_initial(problem._bal_handle)
             rep, st = _lib.ReportC(), _lib.LmStatisticsC()
-            code = _lib.lib.fg_lm_solve_bal_to_cost(backend.handle, problem._bal_handle, C.byref(oo),
+            if then_backend is None:
+                code = _lib.lib.fg_lm_solve_bal_to_cost(backend.handle, problem._bal_handle, C.byref(oo),
+                                                        C.byref(lmo), target, C.byref(rep), C.byref(st))
+                return code, rep, st
+            # first phase: stops at the target or after switch_after accepted steps
+            code = _lib.lib.fg_lm_solve_bal_to_cost(backend.handle, problem._bal_handle, C.byref(oo_first),
                                                     C.byref(lmo), target, C.byref(rep), C.byref(st))
-            return code, rep, st
+            if rep.termination == 5:
+                return code, rep, st
+            rep2, st2 = _lib.ReportC(), _lib.LmStatisticsC()
+            code = _lib.lib.fg_lm_solve_bal_to_cost(then_backend.handle, problem._bal_handle, C.byref(oo),
+                                                    C.byref(lmo), target, C.byref(rep2), C.byref(st2))
+            for f in ("accepted_steps", "rejected_steps", "linear_iterations", "linearizations"):
+                setattr(st2, f, getattr(st2, f) + getattr(st, f))
+            return code, rep2, st2
 
         if name == head:
             clk = Clocks(device)  # started before the warm-up so it samples from the first timed step

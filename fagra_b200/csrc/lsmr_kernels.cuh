@@ -110,6 +110,24 @@ __device__ __forceinline__ void load_vals(const double* p, double (&v)[N]) {
   }
 }
 
+// load_vals through the read-only path (the values do not change during a pass).
+template <int N>
+__device__ __forceinline__ void load_vals_ro(const float* p, double (&v)[N]) {
+#pragma unroll
+  for (int i = 0; i < N / 4; ++i) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p) + i);
+    v[4 * i] = a.x; v[4 * i + 1] = a.y; v[4 * i + 2] = a.z; v[4 * i + 3] = a.w;
+  }
+}
+template <int N>
+__device__ __forceinline__ void load_vals_ro(const double* p, double (&v)[N]) {
+#pragma unroll
+  for (int i = 0; i < N / 2; ++i) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p) + i);
+    v[2 * i] = a.x; v[2 * i + 1] = a.y;
+  }
+}
+
 // emission_rows for the BAL layout, with the same summation order.
 template <class TS, class F>
 __device__ __forceinline__ void emission_rows_bal(const LsmrDev<TS>& D, int64_t e, const double* w, F f) {
@@ -576,8 +594,8 @@ __global__ void __launch_bounds__(LSMR_NT) k_lsmr_fused_rows(LsmrDev<TS> D, int 
     for (int64_t i = threadIdx.x; i < np; i += LSMR_NT) {
       const int64_t e = e0 + i;
       double v[24];
-      load_vals<24>(D.values + 24 * e, v);
-      const double* wp = w + D.b_col[2 * e + 1];
+      load_vals_ro<24>(D.values + 24 * e, v);
+      const double* wp = w + __ldg(D.b_col + 2 * e + 1);
       const double wp0 = wp[0], wp1 = wp[1], wp2 = wp[2];
       double x[2];
 #pragma unroll
