@@ -392,8 +392,11 @@ def run_gpu(args, rank: int, world: int, device: int):
             if rep.termination == 5:
                 return code, rep, st
             rep2, st2 = _lib.ReportC(), _lib.LmStatisticsC()
+            # the second phase continues from the first one's damping
+            lmo2 = fg.LmOptions().c()
+            lmo2.initial_damping = min(max(st.damping, lmo2.min_damping), lmo2.max_damping)
             code = _lib.lib.fg_lm_solve_bal_to_cost(then_backend.handle, problem._bal_handle, C.byref(oo),
-                                                    C.byref(lmo), target, C.byref(rep2), C.byref(st2))
+                                                    C.byref(lmo2), target, C.byref(rep2), C.byref(st2))
             for f in ("accepted_steps", "rejected_steps", "linear_iterations", "linearizations"):
                 setattr(st2, f, getattr(st2, f) + getattr(st, f))
             return code, rep2, st2

@@ -57,6 +57,7 @@ def test_bal10k_fp32_then_f64_reaches_the_oracle_cost(bal10k):
         assert abs(got - ref) <= 1e-6 * ref, (got, ref)
     target = GOLD["final_cost"]
     lm64 = fg.LevenbergMarquardt(fg.Schur(9 * d.num_cameras, 9, 3))
+    lm64.options = fg.LmOptions(initial_damping=first.statistics.damping)  # continue from the first phase
     final = []
     lm64.on_accept = lambda s: final.append(s.cost)
     lm64.solve_batch_with_outcome(p, fg.OptimizeOptions(30, 1e-8, 0.0, 0.0))
