@@ -55,6 +55,8 @@ def parse():
                     help="ba: Schur-PCG time to cost (default); lsmr: the same with the LSMR backend; "
                          "windows: the batched pose-graph windows; learned: the learned preconditioner's "
                          "training and inference steps")
+    ap.add_argument("--train-problems", type=int, default=2,
+                    help="learned forms: problems whose LM runs supply the training systems (0: untrained network)")
     ap.add_argument("--cameras", type=int, default=0,
                     help="learned suite: time the network on a seeded system of this many cameras")
     ap.add_argument("--windows", type=int, default=4096)
@@ -361,7 +363,10 @@ def run_gpu(args, rank: int, world: int, device: int):
         learned_info = None
         if kw["preconditioner"] == "learned":
             if net_cache is None:
-                net_cache = train_network(fg, synthetic, args.workload, device)
+                if args.train_problems:
+                    net_cache = train_network(fg, synthetic, args.workload, device, problems=args.train_problems)
+                else:  # untrained (block-Jacobi x 1.001): the same kernels, for launch lists
+                    net_cache = (fg.LearnedPreconditioner(seed=7, device=device), dict(systems=0, untrained=True))
             net, info = net_cache
             learned_info = dict(info)
             backend.attach_learned(net)

@@ -97,17 +97,13 @@ __global__ void k_bal_gauge(int64_t nc, const double* cams, const double* prep, 
 // values[24k .. 24k+18) = camera block (2x9 column major), [24k+18, 24k+24) =
 // point block (2x3 column major), negres[2k..2k+1] = -r.
 // Block of LIN_T observations; the 24 values of each are staged in shared
-// memory (stride 25 words to spread banks) and stored with coalesced writes;
-// values64 (may be null): the same values in FP64 for a storage-precision
-// backend's gradient.
+// memory (stride 25 words to spread banks) and stored with coalesced writes.
 constexpr int LIN_T = 128;
 template <class TS>
 __global__ void __launch_bounds__(LIN_T) k_bal_linearize(int64_t no, const uint32_t* oc, const uint32_t* op,
                                                          const double* px, const double* cams, const double* pts,
-                                                         const double* prep, TS* values, double* values64,
-                                                         double* negres, int* error) {
+                                                         const double* prep, TS* values, double* negres, int* error) {
   __shared__ TS tile[LIN_T * 25];
-  __shared__ double tile64[std::is_same<TS, double>::value ? 1 : LIN_T * 25];
   __shared__ double nr[LIN_T * 2];
   const int64_t k0 = (int64_t)blockIdx.x * LIN_T;
   const int64_t k = k0 + threadIdx.x;
@@ -175,11 +171,6 @@ __global__ void __launch_bounds__(LIN_T) k_bal_linearize(int64_t no, const uint3
     v[18 + i] = (TS)jp[i];
     ok = ok && isfinite(jp[i]);
   }
-  if (!std::is_same<TS, double>::value && values64) {
-    double* v64 = tile64 + threadIdx.x * 25;
-    for (int i = 0; i < 18; ++i) v64[i] = jc[i];
-    for (int i = 0; i < 6; ++i) v64[18 + i] = jp[i];
-  }
   nr[2 * threadIdx.x] = -r[0];
   nr[2 * threadIdx.x + 1] = -r[1];
   if (!ok) atomicOr(error, 1);
@@ -187,10 +178,6 @@ __global__ void __launch_bounds__(LIN_T) k_bal_linearize(int64_t no, const uint3
   __syncthreads();
   TS* out = values + 24 * k0;
   for (int i = threadIdx.x; i < nk * 24; i += LIN_T) out[i] = tile[(i / 24) * 25 + (i % 24)];
-  if (!std::is_same<TS, double>::value && values64) {
-    double* o64 = values64 + 24 * k0;
-    for (int i = threadIdx.x; i < nk * 24; i += LIN_T) o64[i] = tile64[(i / 24) * 25 + (i % 24)];
-  }
   for (int i = threadIdx.x; i < nk * 2; i += LIN_T) negres[2 * k0 + i] = nr[i];
 }
 
@@ -457,12 +444,10 @@ fg_status BalProblem::linearize(Backend* b) {
   if (no) {
     if (b->is_f32()) {
       FG_LAUNCH(k_bal_linearize<float>, grid_for(no, LIN_T), LIN_T, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
-                cams.get(), pts.get(), prep.get(), (float*)b->values_device(), b->values64_device(),
-                b->negres_device(), d_flag.get());
+                cams.get(), pts.get(), prep.get(), (float*)b->values_device(), b->negres_device(), d_flag.get());
     } else {
       FG_LAUNCH(k_bal_linearize<double>, grid_for(no, LIN_T), LIN_T, 0, st, (int64_t)no, oc.get(), op.get(), px.get(),
-                cams.get(), pts.get(), prep.get(), (double*)b->values_device(), (double*)nullptr,
-                b->negres_device(), d_flag.get());
+                cams.get(), pts.get(), prep.get(), (double*)b->values_device(), b->negres_device(), d_flag.get());
     }
   }
   FG_CUDA(cudaMemcpyAsync(h_flag.get(), d_flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -93,7 +93,6 @@ class SchurImpl final : public Backend {
   DBuf<uint8_t> d_observed;
   std::vector<uint8_t> h_observed;
   DBuf<TS> d_values;
-  DBuf<double> d_values64;  // FP32 storage, device BAL layout: the FP64 Jacobian for the gradient
   DBuf<double> d_negres;
 
   // ---- numerics
@@ -583,25 +582,13 @@ class SchurImpl final : public Backend {
     if (!gradient_current && bal_layout()) {
       // the gradient and the raw Gram blocks (for the column scales) in one pass
       FG_TRY(d_raw.resize(45 * nC + 6 * nP + 1));
-      if (is_f32() && d_values64.size() >= nvalues && source == DEVICE_BAL) {
-        if (nC)
-          FG_LAUNCH((k_bal_cam_pass<double, BAL_MOMENTS>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC,
-                    d_cam_edge_off.get(), d_values64.get(), d_negres.get(), (const double*)nullptr, d_g.get(),
-                    d_raw.get());
-        if (nP)
-          FG_LAUNCH(k_bal_point_moments<double>, grid_for(nP, 128), 128, 0, st, (int64_t)nP, (int64_t)retained,
-                    d_pt_edge_off.get(), d_pt_edge.get(), d_values64.get(), d_negres.get(), d_g.get(),
-                    d_raw.get() + 45 * nC);
-      } else {
-        if (nC)
-          FG_LAUNCH((k_bal_cam_pass<TS, BAL_MOMENTS>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC,
-                    d_cam_edge_off.get(), d_values.get(), d_negres.get(), (const double*)nullptr, d_g.get(),
-                    d_raw.get());
-        if (nP)
-          FG_LAUNCH(k_bal_point_moments<TS>, grid_for(nP, 128), 128, 0, st, (int64_t)nP, (int64_t)retained,
-                    d_pt_edge_off.get(), d_pt_edge.get(), d_values.get(), d_negres.get(), d_g.get(),
-                    d_raw.get() + 45 * nC);
-      }
+      if (nC)
+        FG_LAUNCH((k_bal_cam_pass<TS, BAL_MOMENTS>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC, d_cam_edge_off.get(),
+                  d_values.get(), d_negres.get(), (const double*)nullptr, d_g.get(), d_raw.get());
+      if (nP)
+        FG_LAUNCH(k_bal_point_moments<TS>, grid_for(nP, 128), 128, 0, st, (int64_t)nP, (int64_t)retained,
+                  d_pt_edge_off.get(), d_pt_edge.get(), d_values.get(), d_negres.get(), d_g.get(),
+                  d_raw.get() + 45 * nC);
       gradient_current = true;
     }
     if (!gradient_current) {
@@ -1427,12 +1414,6 @@ class SchurImpl final : public Backend {
   fg_status launch_axpy_widen(const TS* x, double* out, size_t n);
   fg_status launch_recover(double lambda);
   fg_status verify(double lambda, double* predicted);
-  template <class TJ>
-  fg_status verify_t(double lambda, double* predicted, const TJ* vals);
-  bool values64_ready() const {
-    return is_f32() && bal_layout() && d_values64.size() >= nvalues && nvalues > 0;
-  }
-
   fg_status device_dot(const double* a, const double* b, size_t n, double* out);
   fg_status reduced_residual_d(double lambda, const double* z, double* res, double* rnorm);
 
@@ -1458,7 +1439,6 @@ class SchurImpl final : public Backend {
   int device() const override { return dev; }
   cudaStream_t stream() const override { return st; }
   void* values_device() override { return d_values.get(); }
-  double* values64_device() override { return is_f32() && d_values64.size() ? d_values64.get() : nullptr; }
   double* negres_device() override { return d_negres.get(); }
   void mark_device_model(size_t nrows) override {
     source = DEVICE_BAL;
@@ -1479,9 +1459,6 @@ class SchurImpl final : public Backend {
     up_edges.clear();
     nvalues = 24 * obs;
     FG_TRY(d_values.resize(std::max<size_t>(nvalues, 1)));
-    // FP32 records: the gradient is summed from the FP64 Jacobian, so LM
-    // converges to the stationary point of the FP64 model, not of its rounding
-    if (is_f32()) FG_TRY(d_values64.resize(std::max<size_t>(nvalues, 1)));
     FG_TRY(d_negres.resize(std::max<size_t>(2 * obs, 1)));
     bal_bound = id;
     bal_obs = obs;

@@ -95,9 +95,6 @@ class Backend {
   // Device BAL path: bind an implicit BAL structure and expose raw model storage.
   virtual fg_status bind_bal(const BalObservations& obs) = 0;
   virtual void* values_device() = 0;   // T*, packed Jacobian values
-  // FP32 storage: an FP64 copy of the packed values for the gradient and the
-  // raw Gram blocks (null when the backend keeps none)
-  virtual double* values64_device() { return nullptr; }
   virtual double* negres_device() = 0;  // -r
   virtual bool is_f32() const = 0;
   virtual void mark_device_model(size_t rows) = 0;

@@ -364,16 +364,6 @@ fg_status SchurImpl<TS>::reduced_residual_d(double lambda, const double* z, doub
 // src/schur.rs:346-397 with src/linear_model.rs:254-282.
 template <class TS>
 fg_status SchurImpl<TS>::verify(double lambda, double* predicted) {
-  // FP32 records of the device BAL layout: J delta, J^T (J delta + r) and the
-  // predicted reduction from the FP64 Jacobian, so the diagnostics (and the
-  // refinement residual) describe the FP64 model
-  if (values64_ready()) return verify_t<double>(lambda, predicted, d_values64.get());
-  return verify_t<TS>(lambda, predicted, d_values.get());
-}
-
-template <class TS>
-template <class TJ>
-fg_status SchurImpl<TS>::verify_t(double lambda, double* predicted, const TJ* vals) {
   Layout L = layout();
   VerifyState* vs = d_ver.get();
   FG_CUDA(cudaMemsetAsync(vs, 0, sizeof(VerifyState), st));
@@ -391,16 +381,16 @@ fg_status SchurImpl<TS>::verify_t(double lambda, double* predicted, const TJ* va
   }
   if (rows) FG_CUDA(cudaMemsetAsync(d_jd.get(), 0, rows * sizeof(double), st));
   if (nemissions && source == DEVICE_BAL && pure_pairs && cw == 9 && pw == 3)
-    FG_LAUNCH(k_jdelta_bal<TJ>, std::min<unsigned>(grid_for(nemissions, NT), 4 * nsm), NT, 0, st,
+    FG_LAUNCH(k_jdelta_bal<TS>, std::min<unsigned>(grid_for(nemissions, NT), 4 * nsm), NT, 0, st,
               (int64_t)nemissions, (int64_t)retained,
-              d_edges.get(), vals, d_step.get(), d_jd.get(), d_partials.get(), vs);
+              d_edges.get(), d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
   else if (nemissions)
     FG_LAUNCH(k_jdelta<TS>, grid_for(nemissions, NT), NT, 0, st, (int64_t)nemissions, d_emi_off.get(), d_blocks.get(),
               d_values.get(), d_step.get(), d_jd.get(), d_partials.get(), vs);
   const bool bal = bal_layout();
   if (nC && bal) {
-    FG_LAUNCH((k_bal_cam_pass<TJ, BAL_NORMAL>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC, d_cam_edge_off.get(),
-              vals, d_negres.get(), d_jd.get(), d_camjt.get(), (double*)nullptr);
+    FG_LAUNCH((k_bal_cam_pass<TS, BAL_NORMAL>), (unsigned)nC, BAL_CAM_THREADS, 0, st, (int64_t)nC, d_cam_edge_off.get(),
+              d_values.get(), d_negres.get(), d_jd.get(), d_camjt.get(), (double*)nullptr);
   } else if (nC) {
     FG_DISPATCH_WIDTHS(cw, pw, {
       FG_LAUNCH((k_cam_jt_block<CW_, TS, CAM_NORMAL>), (unsigned)nC, 128, 0, st, L, d_var_off.get(),
@@ -408,9 +398,9 @@ fg_status SchurImpl<TS>::verify_t(double lambda, double* predicted, const TJ* va
     });
   }
   if (dim)
-    FG_LAUNCH(k_normal_residual<TJ>, std::min<unsigned>(grid_for(dim, NT), 4 * nsm), NT, 0, st, L,
+    FG_LAUNCH(k_normal_residual<TS>, std::min<unsigned>(grid_for(dim, NT), 4 * nsm), NT, 0, st, L,
               d_var_off.get(), d_var_blk.get(),
-              d_blocks.get(), vals, d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
+              d_blocks.get(), d_values.get(), d_jd.get(), d_negres.get(), d_g.get(), d_scales.get(), d_step.get(),
               lambda, nC ? d_camjt.get() : (const double*)nullptr, d_partials.get() + 4 * 65536, vs,
               bal ? d_pt_edge_off.get() : (const int64_t*)nullptr, bal ? d_pt_edge.get() : (const int64_t*)nullptr);
   FG_CUDA(cudaMemcpyAsync(h_ver.get(), vs, sizeof(VerifyState), cudaMemcpyDeviceToHost, st));
