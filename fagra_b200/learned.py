@@ -111,6 +111,33 @@ class LearnedPreconditioner:
         lm.on_accept = on_accept
         return lm.solve_batch_with_outcome(problem, options)
 
+    def collect_set(self, systems: int, *, cameras=(200, 2000), points_per_camera: int = 200, seed: int = 0,
+                    max_lm_iterations: int = 4, probes: int = 8, kind: str = "products", device: int = 0):
+        """A training set of `systems` reduced camera systems from LM runs on
+        seeded BAL problems of uneven size: camera counts uniform in
+        [cameras[0], cameras[1]], points_per_camera points per camera (the
+        defaults span 200-2,000 cameras and 40,000-400,000 points), track
+        lengths 2 + geometric with mean 4 (uneven observation counts per camera
+        and point); one system per accepted LM step. Returns the (cameras,
+        points, observations) of every problem used."""
+        from .backend import Schur
+        from .bal import BalProblem
+        from .optimize import OptimizeOptions
+        from .synthetic import generate, uniform
+        goal = self.system_count() + systems
+        sizes, k = [], 0
+        while self.system_count() < goal:
+            u = float(uniform(seed, 77, 1, offset=k)[0])
+            nc = int(cameras[0] + u * (cameras[1] - cameras[0] + 1))
+            d = generate("bal10k", cameras=nc, points=points_per_camera * nc, seed=seed * 7919 + 1000 + k)
+            left = goal - self.system_count()
+            self.collect(BalProblem.from_data(d, device=device), Schur(9 * nc, 9, 3, precision="f32", device=device),
+                         OptimizeOptions(max_iterations=min(max_lm_iterations, left)), probes=probes,
+                         seed=seed * 104729 + 31 * k, kind=kind)
+            sizes.append((d.num_cameras, d.num_points, d.num_observations))
+            k += 1
+        return sizes
+
     def import_system(self, features, adjacency, probe_x, probe_y, mask) -> int:
         f = np.ascontiguousarray(features, np.float32)
         a = np.ascontiguousarray(adjacency, np.float32)

@@ -217,3 +217,33 @@ def test_learned_preconditioner_rejects_unsupported_widths():
     b = fg.Schur(24, 12, 3, preconditioner="learned")
     with pytest.raises(fg.UnsupportedStructure):
         b.attach_learned(net)
+
+
+def test_training_set_of_uneven_systems_and_the_reported_comparison():
+    """A training set in the shape of the learned-preconditioner workload
+    (reduced camera systems of LM runs on problems of uneven size, uneven
+    tracks), trained on the device; on a held-out problem the first learned
+    solve reports both iteration counts and both device times, and the policy
+    keeps the network exactly when it needed no more iterations and no more
+    time than block-Jacobi."""
+    net = fg.LearnedPreconditioner(seed=5)
+    sizes = net.collect_set(6, cameras=(120, 200), points_per_camera=100, seed=3)
+    assert net.system_count() == 6 and len(sizes) >= 2
+    assert all(120 <= c <= 200 and p == 100 * c for c, p, _ in sizes)
+    assert len({o / c for c, _, o in sizes}) > 1  # uneven observation counts per camera
+    before = net.mean_loss()
+    net.train(steps=200, learning_rate=1e-3)
+    assert net.mean_loss() < before
+    d = synthetic.generate("bal10k", cameras=160, points=16000, seed=77)
+    b = fg.Schur(9 * d.num_cameras, 9, 3, precision="f32", preconditioner="learned", coarse_correction=True)
+    p = fg.BalProblem.from_data(d)
+    b.prepare(p.dimension())
+    p.linearize(b)
+    b.prepare_damping(1e-6)
+    b.attach_learned(net)
+    b.solve_damped(1e-3)
+    di = b.diagnostics()
+    assert di.learned_iterations > 0 and di.block_jacobi_iterations > 0
+    assert di.learned_seconds > 0 and di.block_jacobi_seconds > 0
+    keep = di.learned_iterations <= di.block_jacobi_iterations and di.learned_seconds <= di.block_jacobi_seconds
+    assert di.preconditioner_used == ("learned" if keep else "retained_blocks")

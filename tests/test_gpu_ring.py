@@ -140,3 +140,23 @@ def test_ring_slot_wait_times_out_then_recovers():
     b.set_poll_limit(0)
     got = b.solve_damped(1e-3).delta
     assert np.linalg.norm(got - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("lam", [1e-3, 1.0])
+def test_ring_fixed_point_sums_of_high_degree_cameras(lam):
+    """16 cameras seeing 40,000 points four times each: every camera holds
+    about 10,000 observations, so each CTA adds hundreds of contributions into
+    a camera's 64-bit fixed-point sums; the FP32-record operator matches the
+    f64-record operator and the oracle to FP32 accuracy."""
+    d = synthetic.generate("bal16", points=40_000, seed=3)
+    counts = np.bincount(d.obs_camera, minlength=d.num_cameras)
+    assert counts.min() > 9_000
+    o = _oracle(d)
+    b32, _ = _device(d)
+    assert b32.operator_info()[0] == 1
+    b64, _ = _device(d, precision="f64")
+    x = np.random.default_rng(7).normal(size=9 * d.num_cameras)
+    ref = o.reduced_apply(lam, x)
+    got32, got64 = b32.reduced_apply(lam, x), b64.reduced_apply(lam, x)
+    assert np.linalg.norm(got64 - ref) <= 1e-10 * np.linalg.norm(ref)
+    assert np.linalg.norm(got32 - got64) <= 2e-5 * np.linalg.norm(got64)
