@@ -671,57 +671,39 @@ __global__ void k_normalize(int64_t nC, int64_t lda, unsigned long long* adj, co
   }
 }
 
-// ---- the 9/3 (BAL) feature pass, the same quantities in three kernels that
-// read every edge once. V_e = E_e L_p^-T (so V_e V_e^T = E_e C_p^-1 E_e^T) and
+// ---- the 9/3 (BAL) feature pass, the same quantities in two kernels that
+// read every edge once (after the positions). V_e = E_e L_p^-T (so V_e V_e^T = E_e C_p^-1 E_e^T) and
 // G_e = L_c^-1 V_e (so K_e = G_e^T G_e); unobserved variables use
 // L = sqrt(lambda) I as above.
 
-// Thread per edge in the point-sorted order of pt_edge (position k): E_e from
-// the edge records (28 words, staged through shared memory with coalesced
-// loads) or the cross array (27 words, edge e), V_e = E_e L_p^-T written by
-// position (column-major 9 x 3, coalesced through shared memory), and the
-// position of every edge (pos[e] = k).
+// The point-sorted position of every edge: pos[pt_edge[k]] = k.
+__global__ void k_gnn_pos(int64_t nedges, const int64_t* pt_edge, int32_t* pos) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < nedges) pos[pt_edge[k]] = (int32_t)k;
+}
+
+// One edge's inputs for the camera pass: E_e (from the point-sorted records
+// at position p, or the cross array at e), its position, and the point's
+// factor entries (or sqrt(lambda) I for an unobserved point).
 template <class TS>
-__global__ void __launch_bounds__(128) k_gnn_edge93(Layout L, int64_t nedges, const TS* src, int by_edge,
-                                                    const int64_t* pt_edge, const DEdgeMeta* edges,
-                                                    const uint8_t* observed, const TS* factors, double lambda, TS* V,
-                                                    int32_t* pos) {
-  using T = TS;  // arithmetic in the storage precision: the factors and records carry no more
-  __shared__ TS tile[128 * 29];
-  const int64_t k0 = (int64_t)blockIdx.x * 128, k = k0 + threadIdx.x;
-  const int nk = (int)min((int64_t)128, nedges - k0);
-  if (!by_edge)
-    for (int i = threadIdx.x; i < nk * 28; i += 128) tile[(i / 28) * 29 + i % 28] = src[k0 * 28 + i];
-  __syncthreads();
-  if (k < nedges) {
-    const int64_t e = pt_edge[k];
-    const int2 cp = *reinterpret_cast<const int2*>(edges + e);
-    pos[e] = (int32_t)k;
-    TS* t = tile + threadIdx.x * 29;
-    if (by_edge)
-      for (int i = 0; i < 27; ++i) t[i] = src[e * 27 + i];
-    const bool pobs = observed[L.nC + cp.y];
-    const TS* lp = factors + L.gram_offset(L.nC + cp.y);
-    T p10 = 0, p20 = 0, p21 = 0, r0, r1, r2;
-    if (pobs) {
-      p10 = lp[1]; p20 = lp[2]; p21 = lp[5];
-      r0 = (T)1 / lp[0]; r1 = (T)1 / lp[4]; r2 = (T)1 / lp[8];
-    } else {
-      r0 = r1 = r2 = (T)(1.0 / sqrt(lambda));
-    }
-    T v[27];
+struct Edge93 {
+  TS E[27];
+  TS p00, p10, p20, p11, p21, p22;
+  int64_t pos;
+  bool pobs;
+};
+template <class TS>
+__device__ __forceinline__ void load_edge93(Edge93<TS>& d, const Layout& L, int64_t e, const int32_t* pos,
+                                            const TS* src, int by_edge, const DEdgeMeta* edges,
+                                            const uint8_t* observed, const TS* factors) {
+  const int2 cp = *reinterpret_cast<const int2*>(edges + e);
+  d.pos = pos[e];
+  const TS* E = src + (by_edge ? e * 27 : d.pos * 28);
 #pragma unroll
-    for (int c = 0; c < 9; ++c) {  // row c of E times L_p^-T: solve L_p y = E(c, :)^T
-      const T y0 = t[c] * r0;
-      const T y1 = (t[9 + c] - p10 * y0) * r1;
-      const T y2 = (t[18 + c] - p20 * y0 - p21 * y1) * r2;
-      v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
-    }
-#pragma unroll
-    for (int i = 0; i < 27; ++i) t[i] = v[i];  // own row only: no barrier needed before
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nk * 27; i += 128) V[k0 * 27 + i] = tile[(i / 27) * 29 + i % 27];
+  for (int i = 0; i < 27; ++i) d.E[i] = E[i];
+  d.pobs = observed[L.nC + cp.y];
+  const TS* lp = factors + L.gram_offset(L.nC + cp.y);
+  d.p00 = lp[0]; d.p10 = lp[1]; d.p20 = lp[2]; d.p11 = lp[4]; d.p21 = lp[5]; d.p22 = lp[8];
 }
 
 // Block of 128 per camera (L_c in shared memory): over the camera's edges,
@@ -731,7 +713,8 @@ __global__ void __launch_bounds__(128) k_gnn_edge93(Layout L, int64_t nedges, co
 // k_node_features writes it.
 template <class TS>
 __global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge,
-                                                    const int32_t* pos, const TS* V, const uint8_t* observed,
+                                                    const int32_t* pos, const TS* src, int by_edge,
+                                                    const DEdgeMeta* edges, const uint8_t* observed,
                                                     const TS* factors, double lambda, float* X0, uint8_t* mask,
                                                     float* Kout) {
   using T = TS;
@@ -762,25 +745,28 @@ __global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam
 #pragma unroll
   for (int i = 0; i < 45; ++i) acc[i] = 0;
   // the next edge's loads are issued before the current edge's arithmetic
+  const T isl = (T)(1.0 / sqrt(lambda));
   int64_t k = e0 + tid;
-  int64_t p = k < e1 ? (int64_t)pos[cam_edge[k]] : 0;
-  T vn[27];
-  if (k < e1) {
-    const TS* vp = V + p * 27;
-#pragma unroll
-    for (int i = 0; i < 27; ++i) vn[i] = vp[i];
-  }
+  Edge93<TS> nx;
+  if (k < e1) load_edge93<TS>(nx, L, cam_edge[k], pos, src, by_edge, edges, observed, factors);
   for (; k < e1; k += 128) {
+    const Edge93<TS> cu = nx;
+    const int64_t pc = cu.pos;
+    const int64_t kn = k + 128;
+    if (kn < e1) load_edge93<TS>(nx, L, cam_edge[kn], pos, src, by_edge, edges, observed, factors);
+    // V = E L_p^-T: row c solves L_p y = E(c, :)^T
+    T r0 = isl, r1 = isl, r2 = isl, p10 = 0, p20 = 0, p21 = 0;
+    if (cu.pobs) {
+      r0 = (T)1 / cu.p00; r1 = (T)1 / cu.p11; r2 = (T)1 / cu.p22;
+      p10 = cu.p10; p20 = cu.p20; p21 = cu.p21;
+    }
     T v[27];
 #pragma unroll
-    for (int i = 0; i < 27; ++i) v[i] = vn[i];
-    const int64_t pc = p;
-    const int64_t kn = k + 128;
-    if (kn < e1) {
-      p = pos[cam_edge[kn]];
-      const TS* vp = V + p * 27;
-#pragma unroll
-      for (int i = 0; i < 27; ++i) vn[i] = vp[i];
+    for (int c = 0; c < 9; ++c) {
+      const T y0 = cu.E[c] * r0;
+      const T y1 = (cu.E[9 + c] - p10 * y0) * r1;
+      const T y2 = (cu.E[18 + c] - p20 * y0 - p21 * y1) * r2;
+      v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
     }
     int idx = 0;
 #pragma unroll
@@ -1185,7 +1171,6 @@ class Gnn {
   DBuf<float> Z[NLAYER + 1], HA[NLAYER], H3, O, dO, dHa, dHb, dA, dZ, edgeK;
   DBuf<unsigned long long> adj;  // fixed-point covisibility, C x C, left cleared by k_normalize
   int64_t adj_cap = -1;          // entries of adj known to be zero
-  DBuf<unsigned char> edgeV;     // V_e of the 9/3 feature pass (27 storage words per edge)
   DBuf<int32_t> edgePos;         // point-sorted position of every edge
   DBuf<double> dloss;
   DBuf<unsigned> dcount;
@@ -1224,9 +1209,36 @@ class Gnn {
     return set_parameters(h.data());
   }
 
+  // The previous precondition call's read-back, when it has landed: the
+  // nonfinite count goes to *nonfinite, a set GEMM flag becomes
+  // FG_DEVICE_TIMEOUT (and is cleared).
+  cudaEvent_t status_ev = nullptr;
+  bool status_pending = false;
+  fg_status take_async_status(unsigned* nonfinite) {
+    if (!status_ev) FG_CUDA(cudaEventCreateWithFlags(&status_ev, cudaEventDisableTiming));
+    if (!status_pending || cudaEventQuery(status_ev) != cudaSuccess) return FG_OK;
+    status_pending = false;
+    *nonfinite = hcount.get()[0];
+    if (herr.get()[0]) {
+      herr.get()[0] = 0;
+      FG_CUDA(cudaMemsetAsync(gemm_err.get(), 0, sizeof(int), st));
+      set_error("a tensor-core GEMM of the learned preconditioner timed out");
+      return FG_DEVICE_TIMEOUT;
+    }
+    return FG_OK;
+  }
+  ~Gnn() {
+    if (status_ev) cudaEventDestroy(status_ev);
+  }
+
   // FG_DEVICE_TIMEOUT (and the flag cleared) when a GEMM gave up waiting on
   // its tensor-core commits since the last check; call after a stream sync.
   fg_status check_gemm() {
+    if (status_pending) {  // this sync lands the pending read-back too
+      FG_CUDA(cudaStreamSynchronize(st));
+      unsigned ignored = 0;
+      FG_TRY(take_async_status(&ignored));
+    }
     FG_CUDA(cudaMemcpyAsync(herr.get(), gemm_err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
     if (herr.get()[0]) {
@@ -1277,17 +1289,13 @@ class Gnn {
     const TS* fac = (const TS*)v.factors;
     if (L.cw == 9 && L.pw == 3) {
       FG_TRY(edgeK.resize(std::max<int64_t>(v.nedges * 8, 1)));
-      FG_TRY(edgeV.resize(std::max<int64_t>(v.nedges * 27 * (int64_t)sizeof(TS), 1)));
       FG_TRY(edgePos.resize(std::max<int64_t>(v.nedges, 1)));
-      TS* V = reinterpret_cast<TS*>(edgeV.get());
-      if (v.nedges) {
-        const TS* src = v.rec ? (const TS*)v.rec : (const TS*)v.cross;
-        FG_LAUNCH(k_gnn_edge93<TS>, grid_for(v.nedges, 128), 128, 0, st, L, v.nedges, src, v.rec ? 0 : 1,
-                  v.pt_edge, v.edges, v.observed, fac, v.lambda, V, edgePos.get());
-      }
+      const TS* src = v.rec ? (const TS*)v.rec : (const TS*)v.cross;
+      if (v.nedges)
+        FG_LAUNCH(k_gnn_pos, grid_for(v.nedges, 256), 256, 0, st, v.nedges, v.pt_edge, edgePos.get());
       FG_LAUNCH(k_gnn_cams93<TS>, (unsigned)C, 128, 0, st, L, v.cam_edge_off, v.cam_edge,
-                (const int32_t*)edgePos.get(), (const TS*)V, v.observed, fac, v.lambda, s.X0.get(), s.mask.get(),
-                edgeK.get());
+                (const int32_t*)edgePos.get(), src, v.rec ? 0 : 1, v.edges, v.observed, fac, v.lambda, s.X0.get(),
+                s.mask.get(), edgeK.get());
       if (v.nedges && L.nP)
         FG_LAUNCH(k_gnn_pairs93, grid_for((size_t)L.nP * 32, 128), 128, 0, st, (int64_t)L.nP, C, v.pt_edge_off,
                   edgeK.get(), adj.get());
@@ -1418,9 +1426,14 @@ class Gnn {
     else
       FG_LAUNCH(k_head_minv<TS>, grid_for(live.C, 64), 64, 0, st, v.L, O.get(), live.mask.get(), (const TS*)v.factors,
               (TS*)minv, dcount.get());
+    // No host sync on the solve path: the count and the GEMM flag of this call
+    // are read back asynchronously and reported by the next call once its copy
+    // has landed (the PCG that follows polls the stream anyway).
+    FG_TRY(take_async_status(nonfinite));
     FG_CUDA(cudaMemcpyAsync(hcount.get(), dcount.get(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    FG_TRY(check_gemm());
-    *nonfinite = hcount.get()[0];
+    FG_CUDA(cudaMemcpyAsync(herr.get(), gemm_err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaEventRecord(status_ev, st));
+    status_pending = true;
     return FG_OK;
   }
 
