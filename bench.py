@@ -57,6 +57,8 @@ def parse():
                          "training and inference steps")
     ap.add_argument("--train-problems", type=int, default=2,
                     help="learned forms: problems whose LM runs supply the training systems (0: untrained network)")
+    ap.add_argument("--train-steps", type=int, default=400, help="learned forms: Adam steps")
+    ap.add_argument("--train-lr", type=float, default=1e-3, help="learned forms: Adam learning rate")
     ap.add_argument("--cameras", type=int, default=0,
                     help="learned suite: time the network on a seeded system of this many cameras")
     ap.add_argument("--windows", type=int, default=4096)
@@ -243,7 +245,8 @@ class Clocks:
                     samples=len(sm))
 
 
-def train_network(fg, synthetic, workload: str, device: int, problems: int = 2) -> tuple:
+def train_network(fg, synthetic, workload: str, device: int, problems: int = 2, steps: int = 400,
+                  learning_rate: float = 1e-3) -> tuple:
     """Learned preconditioner trained (untimed) on reduced camera systems of LM
     runs over problems of the workload's shape with other seeds."""
     net = fg.LearnedPreconditioner(seed=7, device=device)
@@ -254,8 +257,9 @@ def train_network(fg, synthetic, workload: str, device: int, problems: int = 2) 
         net.collect(fg.BalProblem.from_data(d, device=device), be, fg.OptimizeOptions(max_iterations=4), probes=8,
                     seed=1000 * k)
     before = net.mean_loss()
-    net.train(steps=400, learning_rate=1e-3)
+    net.train(steps=steps, learning_rate=learning_rate)
     return net, dict(systems=net.system_count(), loss_before=before, loss_after=net.mean_loss(),
+                     steps=steps, learning_rate=learning_rate,
                      train_seconds=time.perf_counter() - t0, training_problems=f"{problems} x {workload} seeds 200+")
 
 
@@ -364,7 +368,8 @@ def run_gpu(args, rank: int, world: int, device: int):
         if kw["preconditioner"] == "learned":
             if net_cache is None:
                 if args.train_problems:
-                    net_cache = train_network(fg, synthetic, args.workload, device, problems=args.train_problems)
+                    net_cache = train_network(fg, synthetic, args.workload, device, problems=args.train_problems,
+                                              steps=args.train_steps, learning_rate=args.train_lr)
                 else:  # untrained (block-Jacobi x 1.001): the same kernels, for launch lists
                     net_cache = (fg.LearnedPreconditioner(seed=7, device=device), dict(systems=0, untrained=True))
             net, info = net_cache
