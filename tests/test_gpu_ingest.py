@@ -94,3 +94,31 @@ def test_parameters_into_caller_arrays():
     assert np.array_equal(c0, c1) and np.array_equal(p0, p1) and np.array_equal(c0, d.cameras)
     with pytest.raises(ValueError):
         p.parameters(out=(np.zeros((d.num_cameras, 9), np.float32), out[1]))
+
+
+def test_bal_text_file_end_to_end(tmp_path):
+    """A problem written in the BAL text format (examples/bal/model.rs:58-114)
+    and read back with synthetic.parse_bal (exactly: every value round-trips)
+    runs through device ingestion and LM like the in-memory problem it was
+    written from."""
+    d = synthetic.generate("bal16", points=600, seed=4)
+    lines = [f"{d.num_cameras} {d.num_points} {d.num_observations}"]
+    lines += [f"{int(c)} {int(p)} {float(x)!r} {float(y)!r}" for c, p, (x, y) in zip(d.obs_camera, d.obs_point,
+                                                                                   d.obs_pixel)]
+    lines += [repr(float(v)) for v in d.cameras.reshape(-1)]
+    lines += [repr(float(v)) for v in d.points.reshape(-1)]
+    path = tmp_path / "problem.txt"
+    path.write_text("\n".join(lines) + "\n")
+    cams, pts, oc, op, px = synthetic.parse_bal(path.read_text())
+    assert np.array_equal(cams, d.cameras) and np.array_equal(pts, d.points)
+    assert np.array_equal(px, d.obs_pixel)
+    opts = fg.OptimizeOptions(max_iterations=6)
+    runs = []
+    for prob in (fg.BalProblem(cams, pts, oc, op, px), fg.BalProblem.from_data(d)):
+        lm = fg.LevenbergMarquardt(fg.Schur(9 * d.num_cameras, 9, 3))
+        out = lm.solve_batch_with_outcome(prob, opts)
+        runs.append((out.statistics.cost, out.statistics.accepted_steps, prob.parameters()))
+    # the same inputs; the f64 operator's shared FP64 atomics may round in a different order
+    assert abs(runs[0][0] - runs[1][0]) <= 1e-12 * runs[1][0] and runs[0][1] == runs[1][1]
+    for a, b in zip(runs[0][2], runs[1][2]):
+        assert np.allclose(a, b, rtol=1e-9, atol=1e-12)
