@@ -682,42 +682,24 @@ __global__ void k_gnn_pos(int64_t nedges, const int64_t* pt_edge, int32_t* pos) 
   if (k < nedges) pos[pt_edge[k]] = (int32_t)k;
 }
 
-// One edge's inputs for the camera pass: E_e (from the point-sorted records
-// at position p, or the cross array at e), its position, and the point's
-// factor entries (or sqrt(lambda) I for an unobserved point).
-template <class TS>
-struct Edge93 {
-  TS E[27];
-  TS p00, p10, p20, p11, p21, p22;
-  int64_t pos;
-  bool pobs;
-};
-template <class TS>
-__device__ __forceinline__ void load_edge93(Edge93<TS>& d, const Layout& L, int64_t e, const int32_t* pos,
-                                            const TS* src, int by_edge, const DEdgeMeta* edges,
-                                            const uint8_t* observed, const TS* factors) {
-  const int2 cp = *reinterpret_cast<const int2*>(edges + e);
-  d.pos = pos[e];
-  const TS* E = src + (by_edge ? e * 27 : d.pos * 28);
-#pragma unroll
-  for (int i = 0; i < 27; ++i) d.E[i] = E[i];
-  d.pobs = observed[L.nC + cp.y];
-  const TS* lp = factors + L.gram_offset(L.nC + cp.y);
-  d.p00 = lp[0]; d.p10 = lp[1]; d.p20 = lp[2]; d.p11 = lp[4]; d.p21 = lp[5]; d.p22 = lp[8];
-}
-
-// Block of 128 per camera (L_c in shared memory): over the camera's edges,
+// Block of 128 per camera (L_c in shared memory), the camera's edges in
+// chunks of 128: each thread first reads its edge's position, point index and
+// point factor entries, then the block copies the chunk's records (E_e from
+// the fast path's point-sorted records, 28 storage words each, as 16-byte
+// vectors spread over all threads; the reference-layout cross array, 27 words
+// per edge, thread per edge) into shared memory. Then, thread per edge:
 // U = sum_e V_e V_e^T in FP64 and K_e = G_e^T G_e with G_e = L_c^-1 V_e,
 // written at the edge's point-sorted position (K lower, 6 floats, camera
 // index in slot 6); then P = L_c^-1 U L_c^-T and the node-feature row as
 // k_node_features writes it.
+constexpr int CAMS93_NT = 128;
 template <class TS>
-__global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge,
-                                                    const int32_t* pos, const TS* src, int by_edge,
-                                                    const DEdgeMeta* edges, const uint8_t* observed,
-                                                    const TS* factors, double lambda, float* X0, uint8_t* mask,
-                                                    float* Kout) {
+__global__ void __launch_bounds__(CAMS93_NT, sizeof(TS) == 4 ? 4 : 2)
+    k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge, const int32_t* pos, const TS* src,
+                 int by_edge, const DEdgeMeta* edges, const uint8_t* observed, const TS* factors, double lambda,
+                 float* X0, uint8_t* mask, float* Kout) {
   using T = TS;
+  constexpr int VPR = 28 * (int)sizeof(TS) / 16;  // 16-byte vectors per record
   const int64_t cam = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float* row = X0 + cam * NF;
@@ -725,82 +707,147 @@ __global__ void __launch_bounds__(128) k_gnn_cams93(Layout L, const int64_t* cam
   if (!observed[cam]) {
     if (tid == 0) mask[cam] = 0;
     if (tid < NF) row[tid] = tid == 49 ? 1.f : 0.f;
-    for (int64_t k = e0 + tid; k < e1; k += 128) {
+    for (int64_t k = e0 + tid; k < e1; k += CAMS93_NT) {
       float4* ko = reinterpret_cast<float4*>(Kout + (int64_t)pos[cam_edge[k]] * 8);
       ko[0] = make_float4(0.f, 0.f, 0.f, 0.f);
       ko[1] = make_float4(0.f, 0.f, __int_as_float((int)cam), 0.f);
     }
     return;
   }
+  __shared__ __align__(16) T srec[CAMS93_NT * 28];
+  __shared__ int32_t spos[CAMS93_NT];
   __shared__ T sl[81], srd[9];
   __shared__ double red[4][45];
   __shared__ double U[81], W[81];
   const TS* lc = factors + L.gram_offset(cam);
   if (tid < 81) sl[tid] = lc[tid];
   if (tid < 9) srd[tid] = (T)1 / lc[tid * 9 + tid];
-  __syncthreads();
   // per-thread partial sums in the storage precision (a thread sees about
   // 1/128 of the camera's edges), combined in FP64 below
   T acc[45];
 #pragma unroll
   for (int i = 0; i < 45; ++i) acc[i] = 0;
-  // the next edge's loads are issued before the current edge's arithmetic
   const T isl = (T)(1.0 / sqrt(lambda));
-  int64_t k = e0 + tid;
-  Edge93<TS> nx;
-  if (k < e1) load_edge93<TS>(nx, L, cam_edge[k], pos, src, by_edge, edges, observed, factors);
-  for (; k < e1; k += 128) {
-    const Edge93<TS> cu = nx;
-    const int64_t pc = cu.pos;
-    const int64_t kn = k + 128;
-    if (kn < e1) load_edge93<TS>(nx, L, cam_edge[kn], pos, src, by_edge, edges, observed, factors);
-    // V = E L_p^-T: row c solves L_p y = E(c, :)^T
+  // the first chunk's edge metadata; a later chunk's is fetched while the
+  // chunk before it is computed
+  int64_t ne = 0;
+  int32_t npc = 0, npy = 0;
+  if (e0 + tid < e1) {
+    ne = cam_edge[e0 + tid];
+    npc = pos[ne];
+    npy = reinterpret_cast<const int2*>(edges + ne)->y;
+  }
+  for (int64_t base = e0; base < e1; base += CAMS93_NT) {
+    const int nv = (int)(e1 - base < CAMS93_NT ? e1 - base : CAMS93_NT);
+    const bool have = base + tid < e1;
+    const int64_t e = ne, pc = npc;
+    const int py = npy;
     T r0 = isl, r1 = isl, r2 = isl, p10 = 0, p20 = 0, p21 = 0;
-    if (cu.pobs) {
-      r0 = (T)1 / cu.p00; r1 = (T)1 / cu.p11; r2 = (T)1 / cu.p22;
-      p10 = cu.p10; p20 = cu.p20; p21 = cu.p21;
-    }
-    T v[27];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) {
-      const T y0 = cu.E[c] * r0;
-      const T y1 = (cu.E[9 + c] - p10 * y0) * r1;
-      const T y2 = (cu.E[18 + c] - p20 * y0 - p21 * y1) * r2;
-      v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
-    }
-    int idx = 0;
-#pragma unroll
-    for (int c = 0; c < 9; ++c)
-#pragma unroll
-      for (int r = c; r < 9; ++r) acc[idx++] += v[r] * v[c] + v[9 + r] * v[9 + c] + v[18 + r] * v[18 + c];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {  // G = L_c^-1 V, the three columns together
-      T s0 = v[i], s1 = v[9 + i], s2 = v[18 + i];
-#pragma unroll
-      for (int j = 0; j < i; ++j) {
-        const T l = sl[j * 9 + i];
-        s0 -= l * v[j];
-        s1 -= l * v[9 + j];
-        s2 -= l * v[18 + j];
+    if (have) {
+      spos[tid] = (int32_t)pc;
+      // the factor entries are read whether or not the point is observed
+      // (every variable has its block), so the two loads go out together
+      const TS* lp = factors + L.gram_offset(L.nC + py);
+      const T f0 = lp[0], f1 = lp[1], f2 = lp[2], f4 = lp[4], f5 = lp[5], f8 = lp[8];
+      if (observed[L.nC + py]) {
+        r0 = (T)1 / f0; r1 = (T)1 / f4; r2 = (T)1 / f8;
+        p10 = f1; p20 = f2; p21 = f5;
       }
-      v[i] = s0 * srd[i];
-      v[9 + i] = s1 * srd[i];
-      v[18 + i] = s2 * srd[i];
-    }
-    T K[6];  // K00, K10, K20, K11, K21, K22
-    int kx = 0;
+      if (by_edge) {
+        const TS* E = src + e * 27;
 #pragma unroll
-    for (int q = 0; q < 3; ++q)
-#pragma unroll
-      for (int r = q; r < 3; ++r) {
-        T sk = 0;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) sk += v[9 * r + c] * v[9 * q + c];
-        K[kx++] = sk;
+        for (int i = 0; i < 27; ++i) srec[tid * 28 + i] = E[i];
       }
-    float4* ko = reinterpret_cast<float4*>(Kout + pc * 8);
-    ko[0] = make_float4((float)K[0], (float)K[1], (float)K[2], (float)K[3]);
-    ko[1] = make_float4((float)K[4], (float)K[5], __int_as_float((int)cam), 0.f);
+    }
+    __syncthreads();
+    if (!by_edge) {
+      // all of a thread's vector loads are issued before its shared stores
+      const uint4* s4 = reinterpret_cast<const uint4*>(src);
+      uint4* d4 = reinterpret_cast<uint4*>(srec);
+      uint4 t[VPR];
+#pragma unroll
+      for (int j = 0; j < VPR; ++j) {
+        const int i = tid + j * CAMS93_NT;
+        if (i < nv * VPR) {
+          const int r = i / VPR;
+          t[j] = s4[(int64_t)spos[r] * VPR + (i - r * VPR)];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < VPR; ++j) {
+        const int i = tid + j * CAMS93_NT;
+        if (i < nv * VPR) d4[i] = t[j];
+      }
+    }
+    if (base + CAMS93_NT + tid < e1) {
+      ne = cam_edge[base + CAMS93_NT + tid];
+      npc = pos[ne];
+      npy = reinterpret_cast<const int2*>(edges + ne)->y;
+    }
+    if (!by_edge) __syncthreads();
+    if (have) {
+      // V = E L_p^-T: row c solves L_p y = E(c, :)^T
+      T v[27];
+      {
+        T E[28];
+        if constexpr (sizeof(TS) == 4) {
+          const float4* r4 = reinterpret_cast<const float4*>(srec + tid * 28);
+#pragma unroll
+          for (int q = 0; q < 7; ++q) {
+            const float4 t = r4[q];
+            E[4 * q] = t.x; E[4 * q + 1] = t.y; E[4 * q + 2] = t.z; E[4 * q + 3] = t.w;
+          }
+        } else {
+          const double2* r2v = reinterpret_cast<const double2*>(srec + tid * 28);
+#pragma unroll
+          for (int q = 0; q < 14; ++q) {
+            const double2 t = r2v[q];
+            E[2 * q] = t.x; E[2 * q + 1] = t.y;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          const T y0 = E[c] * r0;
+          const T y1 = (E[9 + c] - p10 * y0) * r1;
+          const T y2 = (E[18 + c] - p20 * y0 - p21 * y1) * r2;
+          v[c] = y0; v[9 + c] = y1; v[18 + c] = y2;
+        }
+      }
+      int idx = 0;
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+#pragma unroll
+        for (int r = c; r < 9; ++r) acc[idx++] += v[r] * v[c] + v[9 + r] * v[9 + c] + v[18 + r] * v[18 + c];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {  // G = L_c^-1 V, the three columns together
+        T s0 = v[i], s1 = v[9 + i], s2 = v[18 + i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) {
+          const T l = sl[j * 9 + i];
+          s0 -= l * v[j];
+          s1 -= l * v[9 + j];
+          s2 -= l * v[18 + j];
+        }
+        v[i] = s0 * srd[i];
+        v[9 + i] = s1 * srd[i];
+        v[18 + i] = s2 * srd[i];
+      }
+      T K[6];  // K00, K10, K20, K11, K21, K22
+      int kx = 0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int r = q; r < 3; ++r) {
+          T sk = 0;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) sk += v[9 * r + c] * v[9 * q + c];
+          K[kx++] = sk;
+        }
+      float4* ko = reinterpret_cast<float4*>(Kout + pc * 8);
+      ko[0] = make_float4((float)K[0], (float)K[1], (float)K[2], (float)K[3]);
+      ko[1] = make_float4((float)K[4], (float)K[5], __int_as_float((int)cam), 0.f);
+    }
+    __syncthreads();  // the next chunk overwrites srec and spos
   }
 #pragma unroll
   for (int i = 0; i < 45; ++i) {
