@@ -695,9 +695,9 @@ __global__ void k_gnn_pos(int64_t nedges, const int64_t* pt_edge, int32_t* pos) 
 constexpr int CAMS93_NT = 128;
 template <class TS>
 __global__ void __launch_bounds__(CAMS93_NT, sizeof(TS) == 4 ? 4 : 2)
-    k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge, const int32_t* pos, const TS* src,
-                 int by_edge, const DEdgeMeta* edges, const uint8_t* observed, const TS* factors, double lambda,
-                 float* X0, uint8_t* mask, float* Kout) {
+    k_gnn_cams93(Layout L, const int64_t* cam_edge_off, const int64_t* cam_edge, const int2* meta, const int32_t* pos,
+                 const TS* src, int by_edge, const DEdgeMeta* edges, const uint8_t* observed, const TS* factors,
+                 double lambda, float* X0, uint8_t* mask, float* Kout) {
   using T = TS;
   constexpr int VPR = 28 * (int)sizeof(TS) / 16;  // 16-byte vectors per record
   const int64_t cam = blockIdx.x;
@@ -708,7 +708,7 @@ __global__ void __launch_bounds__(CAMS93_NT, sizeof(TS) == 4 ? 4 : 2)
     if (tid == 0) mask[cam] = 0;
     if (tid < NF) row[tid] = tid == 49 ? 1.f : 0.f;
     for (int64_t k = e0 + tid; k < e1; k += CAMS93_NT) {
-      float4* ko = reinterpret_cast<float4*>(Kout + (int64_t)pos[cam_edge[k]] * 8);
+      float4* ko = reinterpret_cast<float4*>(Kout + (int64_t)(meta ? meta[k].x : pos[cam_edge[k]]) * 8);
       ko[0] = make_float4(0.f, 0.f, 0.f, 0.f);
       ko[1] = make_float4(0.f, 0.f, __int_as_float((int)cam), 0.f);
     }
@@ -728,15 +728,25 @@ __global__ void __launch_bounds__(CAMS93_NT, sizeof(TS) == 4 ? 4 : 2)
 #pragma unroll
   for (int i = 0; i < 45; ++i) acc[i] = 0;
   const T isl = (T)(1.0 / sqrt(lambda));
+  // an edge's source index (cross array only), point-sorted position and
+  // point: one coalesced int2 from the camera-major array, else gathered
+  auto fetch = [&](int64_t k, int64_t& e, int32_t& pc, int32_t& py) {
+    if (meta) {
+      const int2 m = meta[k];
+      pc = m.x;
+      py = m.y;
+      e = by_edge ? cam_edge[k] : 0;
+    } else {
+      e = cam_edge[k];
+      pc = pos[e];
+      py = edges[e].pt;
+    }
+  };
   // the first chunk's edge metadata; a later chunk's is fetched while the
   // chunk before it is computed
   int64_t ne = 0;
   int32_t npc = 0, npy = 0;
-  if (e0 + tid < e1) {
-    ne = cam_edge[e0 + tid];
-    npc = pos[ne];
-    npy = reinterpret_cast<const int2*>(edges + ne)->y;
-  }
+  if (e0 + tid < e1) fetch(e0 + tid, ne, npc, npy);
   for (int64_t base = e0; base < e1; base += CAMS93_NT) {
     const int nv = (int)(e1 - base < CAMS93_NT ? e1 - base : CAMS93_NT);
     const bool have = base + tid < e1;
@@ -779,11 +789,7 @@ __global__ void __launch_bounds__(CAMS93_NT, sizeof(TS) == 4 ? 4 : 2)
         if (i < nv * VPR) d4[i] = t[j];
       }
     }
-    if (base + CAMS93_NT + tid < e1) {
-      ne = cam_edge[base + CAMS93_NT + tid];
-      npc = pos[ne];
-      npy = reinterpret_cast<const int2*>(edges + ne)->y;
-    }
+    if (base + CAMS93_NT + tid < e1) fetch(base + CAMS93_NT + tid, ne, npc, npy);
     if (!by_edge) __syncthreads();
     if (have) {
       // V = E L_p^-T: row c solves L_p y = E(c, :)^T
@@ -1336,13 +1342,15 @@ class Gnn {
     const TS* fac = (const TS*)v.factors;
     if (L.cw == 9 && L.pw == 3) {
       FG_TRY(edgeK.resize(std::max<int64_t>(v.nedges * 8, 1)));
-      FG_TRY(edgePos.resize(std::max<int64_t>(v.nedges, 1)));
       const TS* src = v.rec ? (const TS*)v.rec : (const TS*)v.cross;
-      if (v.nedges)
-        FG_LAUNCH(k_gnn_pos, grid_for(v.nedges, 256), 256, 0, st, v.nedges, v.pt_edge, edgePos.get());
-      FG_LAUNCH(k_gnn_cams93<TS>, (unsigned)C, 128, 0, st, L, v.cam_edge_off, v.cam_edge,
-                (const int32_t*)edgePos.get(), src, v.rec ? 0 : 1, v.edges, v.observed, fac, v.lambda, s.X0.get(),
-                s.mask.get(), edgeK.get());
+      if (!v.cam_meta) {  // positions gathered through pos
+        FG_TRY(edgePos.resize(std::max<int64_t>(v.nedges, 1)));
+        if (v.nedges)
+          FG_LAUNCH(k_gnn_pos, grid_for(v.nedges, 256), 256, 0, st, v.nedges, v.pt_edge, edgePos.get());
+      }
+      FG_LAUNCH(k_gnn_cams93<TS>, (unsigned)C, CAMS93_NT, 0, st, L, v.cam_edge_off, v.cam_edge, v.cam_meta,
+                v.cam_meta ? (const int32_t*)nullptr : (const int32_t*)edgePos.get(), src, v.rec ? 0 : 1, v.edges,
+                v.observed, fac, v.lambda, s.X0.get(), s.mask.get(), edgeK.get());
       if (v.nedges && L.nP)
         FG_LAUNCH(k_gnn_pairs93, grid_for((size_t)L.nP * 32, 128), 128, 0, st, (int64_t)L.nP, C, v.pt_edge_off,
                   edgeK.get(), adj.get());

@@ -26,6 +26,9 @@ struct SchurView {
   // cw x pw, then the packed camera / point word) in the order of pt_edge, or
   // null when the backend keeps none; with them the features need no cross array
   const void* rec = nullptr;
+  // per edge in camera-major order (cam_edge): x = the edge's point-sorted
+  // position, y = its point; null when the backend has not built it
+  const int2* cam_meta = nullptr;
 };
 
 // y = S x for device vectors of the retained length (f64), S at the view's damping.

@@ -30,6 +30,23 @@ namespace {
 template <class T>
 struct TypeTag {};
 
+// For the learned preconditioner's camera pass: every edge's index in the
+// camera-major order (cam_edge), then, point-major, each edge's point-sorted
+// position and point index at that index, so the pass reads one coalesced
+// int2 per edge instead of gathering the edge's position and metadata.
+__global__ void k_cam_rank(int64_t nedges, const int64_t* cam_edge, int32_t* rank) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < nedges) rank[cam_edge[k]] = (int32_t)k;
+}
+__global__ void k_cam_meta(int64_t nedges, const int64_t* pt_edge, const DEdgeMeta* edges, const int32_t* rank,
+                           int2* meta) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < nedges) {
+    const int64_t e = pt_edge[j];
+    meta[rank[e]] = make_int2((int32_t)j, edges[e].pt);
+  }
+}
+
 }  // namespace
 
 template <class TS>
@@ -92,6 +109,11 @@ class SchurImpl final : public Backend {
   DBuf<int64_t> d_var_off, d_var_blk, d_pt_edge_off, d_pt_edge, d_cam_edge_off, d_cam_edge, d_emi_off;
   DBuf<uint8_t> d_observed;
   std::vector<uint8_t> h_observed;
+  // camera-major (point-sorted position, point) per edge, built on first use
+  // after each structure build (ensure_cam_meta)
+  DBuf<int2> d_cam_meta;
+  DBuf<int32_t> d_cam_rank;
+  bool cam_meta_ok = false;
   DBuf<TS> d_values;
   DBuf<double> d_negres;
 
@@ -350,6 +372,7 @@ class SchurImpl final : public Backend {
     FG_CUDA(cudaStreamSynchronize(st));
     structure_valid = true;
     fast.invalidate();
+    cam_meta_ok = false;
     drop_graphs();
     return FG_OK;
   }
@@ -470,6 +493,7 @@ class SchurImpl final : public Backend {
     FG_CUDA(cudaStreamSynchronize(st));
     structure_valid = true;
     fast.invalidate();
+    cam_meta_ok = false;
     drop_graphs();
     return FG_OK;
   }
@@ -515,6 +539,7 @@ class SchurImpl final : public Backend {
     FG_CUDA(cudaStreamSynchronize(st));
     structure_valid = true;
     fast.invalidate();
+    cam_meta_ok = false;
     drop_graphs();
     return FG_OK;
   }
@@ -841,7 +866,21 @@ class SchurImpl final : public Backend {
     v.observed = d_observed.get();
     v.lambda = lambda;
     v.rec = fast.on && cw == 9 && pw == 3 ? (const void*)fast.d_erec.get() : nullptr;
+    v.cam_meta = cam_meta_ok ? d_cam_meta.get() : nullptr;
     return v;
+  }
+  // The camera-major (position, point) array of the learned preconditioner's
+  // BAL-width camera pass: two passes over the edges, once per structure
+  // (positions are 32-bit, so larger structures go without it).
+  fg_status ensure_cam_meta() {
+    if (cam_meta_ok || cw != 9 || pw != 3 || !nedges || nedges > (size_t)INT32_MAX) return FG_OK;
+    FG_TRY(d_cam_rank.resize(nedges));
+    FG_TRY(d_cam_meta.resize(nedges));
+    FG_LAUNCH(k_cam_rank, grid_for(nedges, 256), 256, 0, st, (int64_t)nedges, d_cam_edge.get(), d_cam_rank.get());
+    FG_LAUNCH(k_cam_meta, grid_for(nedges, 256), 256, 0, st, (int64_t)nedges, d_pt_edge.get(), d_edges.get(),
+              (const int32_t*)d_cam_rank.get(), d_cam_meta.get());
+    cam_meta_ok = true;
+    return FG_OK;
   }
   // Explicit block-Jacobi (or Schur-diagonal) inverses into d_minv.
   fg_status write_block_inverses(double lambda) {
@@ -880,6 +919,7 @@ class SchurImpl final : public Backend {
       EventTimer ti;
       const bool timed = !learned_compared && opt.learned_policy == 0;  // inference time of the comparison
       if (timed) ti.start(st);
+      FG_TRY(ensure_cam_meta());
       const SchurView view = view_at(lambda);
       if (!view.rec) FG_TRY(ensure_cross());
       unsigned nonfinite = 0;
@@ -941,6 +981,7 @@ class SchurImpl final : public Backend {
       FG_CUDA(cudaMemcpyAsync(y, d_zred.get(), retained * sizeof(double), cudaMemcpyDeviceToDevice, st));
       return FG_OK;
     };
+    FG_TRY(ensure_cam_meta());
     if (kind == 1) return gnn_capture(g, view_at(lambda), probes, seed, 1, solve, d_work.get(), d_qd.get(), st, index);
     return gnn_capture(g, view_at(lambda), probes, seed, 0, apply, d_work.get(), d_qd.get(), st, index);
   }
