@@ -37,6 +37,30 @@ extern std::atomic<uint64_t> g_launches;
     cudaError_t e__ = cudaGetLastError();                                      \
     if (e__ != cudaSuccess) return ::fg::cuda_status(e__, #kernel);            \
   } while (0)
+// Programmatic dependent launch for the kernels of a PCG iteration: the
+// kernel may be scheduled while the kernel before it on the stream is still
+// running (once every CTA of that one has called pdl_trigger or exited), so
+// its launch latency hides behind the previous kernel's tail. Every kernel
+// launched this way calls pdl_wait() before its first global memory access
+// (including early-exit tests): the wait returns when the previous grid has
+// completed and its writes are visible, and because each such kernel waits
+// before it can complete, completion is transitive along the stream.
+#define FG_LAUNCH_PDL(kernel, grid_, block_, smem_, stream_, ...)      \
+  do {                                                                 \
+    cudaLaunchConfig_t cfg__ = {};                                     \
+    cfg__.gridDim = dim3(grid_);                                       \
+    cfg__.blockDim = dim3(block_);                                     \
+    cfg__.dynamicSmemBytes = (smem_);                                  \
+    cfg__.stream = (stream_);                                          \
+    cudaLaunchAttribute at__[1];                                       \
+    at__[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;   \
+    at__[0].val.programmaticStreamSerializationAllowed = 1;            \
+    cfg__.attrs = at__;                                                \
+    cfg__.numAttrs = 1;                                                \
+    cudaError_t e__ = cudaLaunchKernelEx(&cfg__, kernel, __VA_ARGS__); \
+    ::fg::g_launches.fetch_add(1, std::memory_order_relaxed);          \
+    if (e__ != cudaSuccess) return ::fg::cuda_status(e__, #kernel);    \
+  } while (0)
 
 fg_status device_stream(int device, cudaStream_t* out);
 fg_status select_device(int device);
@@ -193,5 +217,10 @@ inline unsigned grid_for(size_t n, unsigned block) {
   if (g > 0x7fffffffu) g = 0x7fffffffu;
   return (unsigned)g;
 }
+
+// The device side of FG_LAUNCH_PDL (griddepcontrol, sm_90 and later; both are
+// no-ops in a grid launched without the attribute).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 }  // namespace fg

@@ -751,6 +751,8 @@ __global__ void __launch_bounds__(FR_ROWS * 32) k_fast_reduce(int64_t ncam, int 
                                                       const double* beta, double lambda, const double* lam_dev,
                                                       int use_gram, TV* q, double* dparts,
                                                       PcgState* st, const int* gate) {
+  pdl_wait();
+  pdl_trigger();
   if (st && st->done) return;
   if (gate && !*gate) return;
   __shared__ TV acc_s[FR_ROWS][33];
@@ -1248,8 +1250,8 @@ struct FastPath {
       const size_t sm = RingSmem<TV, MODE, RACC_SHARED>::bytes(nc, xs, NW, R);
       auto kern = xs ? k_ring<TV, MODE, RACC_SHARED, true, NW, R> : k_ring<TV, MODE, RACC_SHARED, false, NW, R>;
       FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      FG_LAUNCH(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, parts, (void*)nullptr, skip, gate,
-                d_error.get(), ex, poll_limit);
+      FG_LAUNCH_PDL(kern, grid, NW * 32, sm, s.st, nc, tl, er, pr, z, pv, beta, parts, (void*)nullptr, skip, gate,
+                    d_error.get(), ex, poll_limit);
     } else {
       constexpr int NW = RING_WARPS_GLOBAL, R = RING_SLOTS_GLOBAL;
       const size_t sm = RingSmem<TV, MODE, RACC_GLOBAL>::bytes(nc, false, NW, R);
@@ -1346,9 +1348,9 @@ struct FastPath {
         if (global_acc)
           return launch_gacc_reduce<TV>(s, x.z, x.pprev, x.beta, lambda, lam_dev, 1, out, dparts, pst, gate,
                                         !std::is_same<TV, float>::value);
-        FG_LAUNCH((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
-                  (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1, out,
-                  dparts, pst, gate);
+        FG_LAUNCH_PDL((k_fast_reduce<TS, TV>), grid_for(s.nC * 9, 32), FR_ROWS * 32, 0, s.st, (int64_t)s.nC, grid,
+                      (const TV*)parts, s.d_gram.get(), s.d_observed.get(), x.z, x.pprev, x.beta, lambda, lam_dev, 1,
+                      out, dparts, pst, gate);
         return FG_OK;
       }
     }

@@ -480,6 +480,8 @@ __device__ __forceinline__ double coarse_finish(const double* G, int nk, const d
 template <int CW, class TS, class TX, bool MIXED, bool CO>
 __global__ void k_update_wide(Layout L, TX* x, TS* r, TS* z, TS* p, const TS* q, const TS* minv,
                               double* partials, PcgState* st, const TS* W, const double* G, int nk) {
+  pdl_wait();
+  pdl_trigger();
   if (st->done) return;
   const int cw = CW ? CW : L.cw;
   extern __shared__ unsigned char sh_raw[];
@@ -710,6 +712,8 @@ __global__ void k_replace_wide(Layout L, const double* b, const double* qd, TS* 
 // block clears the flag after every block has read it.
 template <class TS>
 __global__ void k_coarse_add(int64_t n, int nk, const TS* W, PcgState* st, TS* z) {
+  pdl_wait();
+  pdl_trigger();
   if (!st->coarse_pending) return;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) {

@@ -165,6 +165,8 @@ __global__ void __launch_bounds__(NW * 32, 1)
   constexpr bool FIXED = SM::FIXED;
   constexpr bool NEED_X = MODE != FAST_RHS;
   constexpr bool SCATTER = MODE != FAST_RECOVER;
+  pdl_wait();
+  pdl_trigger();
   if (skip && *skip) return;
   if (gate && !*gate) return;
   extern __shared__ __align__(128) unsigned char smem[];

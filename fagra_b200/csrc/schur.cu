@@ -34,6 +34,18 @@ struct TypeTag {};
 // camera-major order (cam_edge), then, point-major, each edge's point-sorted
 // position and point index at that index, so the pass reads one coalesced
 // int2 per edge instead of gathering the edge's position and metadata.
+// The loop condition of the single-launch PCG graph (a WHILE node whose body
+// is a fixed number of iterations): continue while the solve runs (mixed
+// precision: until done == 1, so a pending FP64 verdict keeps it going) and
+// fewer trips than the iteration limit allows have run, the same bound as the
+// polling loop's (max_iterations + 8 launched iterations).
+__global__ void k_pcg_continue(cudaGraphConditionalHandle h, PcgState* st, int mixed, unsigned iters_per_trip) {
+  const bool running = mixed ? st->done != 1 : st->done == 0;
+  const unsigned trips = ++st->trips;
+  const unsigned long long limit = ((unsigned long long)st->max_iterations + 8 + iters_per_trip - 1) / iters_per_trip;
+  cudaGraphSetConditional(h, running && trips < limit ? 1u : 0u);
+}
+
 __global__ void k_cam_rank(int64_t nedges, const int64_t* cam_edge, int32_t* rank) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k < nedges) rank[cam_edge[k]] = (int32_t)k;
@@ -817,12 +829,13 @@ class SchurImpl final : public Backend {
     PcgState* ps = d_pcg.get();
     FG_DISPATCH_WIDTHS(cw, pw, {
       if (coarse_on)
-        FG_LAUNCH((k_update_wide<CW_, TS, TX, MIXED, true>), gw, bw, shm, st, L, x, d_r.get(), d_z.get(), d_pp.get(),
-                  d_q.get(), d_minv.get(), d_partials.get(), ps, (const TS*)d_Wt.get(), (const double*)d_G.get(), nk);
+        FG_LAUNCH_PDL((k_update_wide<CW_, TS, TX, MIXED, true>), gw, bw, shm, st, L, x, d_r.get(), d_z.get(),
+                      d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps, (const TS*)d_Wt.get(),
+                      (const double*)d_G.get(), nk);
       else
-        FG_LAUNCH((k_update_wide<CW_, TS, TX, MIXED, false>), gw, bw, shm, st, L, x, d_r.get(), d_z.get(),
-                  d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps, (const TS*)nullptr,
-                  (const double*)nullptr, 0);
+        FG_LAUNCH_PDL((k_update_wide<CW_, TS, TX, MIXED, false>), gw, bw, shm, st, L, x, d_r.get(), d_z.get(),
+                      d_pp.get(), d_q.get(), d_minv.get(), d_partials.get(), ps, (const TS*)nullptr,
+                      (const double*)nullptr, 0);
     });
     return launch_coarse_add();
   }
@@ -843,8 +856,8 @@ class SchurImpl final : public Backend {
   }
   fg_status launch_coarse_add() {
     if (coarse_on)
-      FG_LAUNCH(k_coarse_add<TS>, grid_for(retained, 256), 256, 0, st, (int64_t)retained, nk, (const TS*)d_Wt.get(),
-                d_pcg.get(), d_z.get());
+      FG_LAUNCH_PDL(k_coarse_add<TS>, grid_for(retained, 256), 256, 0, st, (int64_t)retained, nk,
+                    (const TS*)d_Wt.get(), d_pcg.get(), d_z.get());
     return FG_OK;
   }
 
@@ -1130,11 +1143,24 @@ class SchurImpl final : public Backend {
   cudaGraphExec_t g_exec[2] = {nullptr, nullptr};
   uint64_t g_nodes[2] = {0, 0};
   std::vector<uintptr_t> g_key[2];  // what each instantiated graph baked in
+  // The whole solve as one graph launch: a WHILE node whose body is
+  // COND_ITERS iterations and k_pcg_continue, so the device decides when to
+  // stop (no host poll between batches, no gated no-op iterations past
+  // convergence beyond the last trip). If the driver refuses the conditional
+  // graph, cond_failed switches this backend to the polled graphs above.
+  static constexpr int COND_ITERS = 4;
+  cudaGraphExec_t c_exec[2] = {nullptr, nullptr};
+  uint64_t c_nodes[2] = {0, 0};
+  std::vector<uintptr_t> c_key[2];
+  bool cond_failed = false;
   void drop_graphs() {
     for (int k = 0; k < 2; ++k) {
       if (g_exec[k]) cudaGraphExecDestroy(g_exec[k]);
       g_exec[k] = nullptr;
       g_key[k].clear();
+      if (c_exec[k]) cudaGraphExecDestroy(c_exec[k]);
+      c_exec[k] = nullptr;
+      c_key[k].clear();
     }
   }
   // Every pointer, size and kernel choice a captured iteration bakes in; a
@@ -1165,6 +1191,63 @@ class SchurImpl final : public Backend {
     }
     return FG_OK;
   }
+  fg_status launch_continue(cudaGraphConditionalHandle h, bool mixed, PcgState* ps) {
+    FG_LAUNCH(k_pcg_continue, 1, 1, 0, st, h, ps, mixed ? 1 : 0, (unsigned)COND_ITERS);
+    return FG_OK;
+  }
+  fg_status capture_cond_graph(bool mixed, double* xd, PcgState* ps, double lambda, cudaGraph_t* out,
+                               uint64_t* nodes) {
+    FG_CUDA(cudaGraphCreate(out, 0));
+    cudaGraphConditionalHandle h;
+    FG_CUDA(cudaGraphConditionalHandleCreate(&h, *out, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    FG_CUDA(cudaGraphAddNode(&node, *out, nullptr, 0, &np));
+    const uint64_t before = g_launches.load();
+    FG_CUDA(cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+    fg_status s = FG_OK;
+    for (int k = 0; k < COND_ITERS && s == FG_OK; ++k) s = iteration_body(mixed, xd, ps, lambda, k);
+    if (s == FG_OK) s = launch_continue(h, mixed, ps);
+    cudaGraph_t body = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &body);
+    *nodes = g_launches.load() - before;
+    g_launches.fetch_sub(*nodes);  // captured, not launched
+    FG_TRY(s);
+    FG_CUDA(e);
+    return FG_OK;
+  }
+  // Launches the single-launch solve graph (captured on first use per key);
+  // the caller reads PcgState back once and adds trips x nodes to the launch
+  // count (add_cond_launches).
+  fg_status launch_cond_graph(bool mixed, double* xd, PcgState* ps, double lambda) {
+    const int g = mixed ? 1 : 0;
+    std::vector<uintptr_t> key = graph_key(mixed, xd, ps);
+    if (c_exec[g] && key != c_key[g]) {
+      cudaGraphExecDestroy(c_exec[g]);
+      c_exec[g] = nullptr;
+    }
+    if (!c_exec[g]) {
+      cudaGraph_t graph = nullptr;
+      fg_status s = capture_cond_graph(mixed, xd, ps, lambda, &graph, &c_nodes[g]);
+      cudaError_t e = s == FG_OK ? cudaGraphInstantiate(&c_exec[g], graph, 0) : cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+      if (s != FG_OK || e != cudaSuccess) {
+        c_exec[g] = nullptr;
+        cudaGetLastError();
+        return s != FG_OK ? s : cuda_status(e, "cudaGraphInstantiate (conditional)");
+      }
+      c_key[g] = key;
+    }
+    FG_CUDA(cudaGraphLaunch(c_exec[g], st));
+    return FG_OK;
+  }
+  void add_cond_launches(bool mixed, const PcgState& h) { g_launches.fetch_add((uint64_t)h.trips * c_nodes[mixed]); }
+
   fg_status launch_graph(bool mixed, double* xd, PcgState* ps, double lambda) {
     const int g = mixed ? 1 : 0;
     std::vector<uintptr_t> key = graph_key(mixed, xd, ps);
@@ -1218,7 +1301,18 @@ class SchurImpl final : public Backend {
     double* tsum = d_partials.get() + 4 * 65536;
     size_t launched = 0, batch = 4;
     const bool graphed = fast.enabled();
-    for (bool first = graphed;; first = false) {
+    bool whole = false;  // the single-launch graph ran the solve
+    if (graphed && !cond_failed) {
+      if (launch_cond_graph(false, nullptr, ps, lambda) == FG_OK) {
+        FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        FG_CUDA(cudaStreamSynchronize(st));
+        add_cond_launches(false, *h_pcg.get());
+        whole = true;
+      } else {
+        cond_failed = true;
+      }
+    }
+    for (bool first = graphed; !whole; first = false) {
       if (!first) {  // the first graph follows the start without a poll (its kernels gate on done)
         FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
         FG_CUDA(cudaStreamSynchronize(st));
@@ -1391,7 +1485,18 @@ class SchurImpl final : public Backend {
     size_t launched = 0, batch = 4;
     const size_t max_iters = opt.max_iterations;
     const bool graphed = fast.enabled();
-    for (bool first = graphed;; first = false) {
+    bool whole = false;  // the single-launch graph ran the solve
+    if (graphed && !cond_failed) {
+      if (launch_cond_graph(true, xd, ps, lambda) == FG_OK) {
+        FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        FG_CUDA(cudaStreamSynchronize(st));
+        add_cond_launches(true, *h_pcg.get());
+        whole = true;
+      } else {
+        cond_failed = true;
+      }
+    }
+    for (bool first = graphed; !whole; first = false) {
       if (!first) {  // the first graph follows the start without a poll
         FG_CUDA(cudaMemcpyAsync(h_pcg.get(), ps, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
         FG_CUDA(cudaStreamSynchronize(st));

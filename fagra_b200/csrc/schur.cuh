@@ -46,6 +46,7 @@ struct PcgState {
   double coarse[8];
   int coarse_pending;
   unsigned counter4;
+  unsigned trips;  // loop trips of the single-launch PCG graph (k_pcg_continue)
 };
 struct VerifyState {
   double jd2;        // ||J delta||^2
