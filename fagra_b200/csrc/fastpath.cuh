@@ -828,23 +828,25 @@ __global__ void __launch_bounds__(FR_ROWS * 32) k_fast_reduce(int64_t ncam, int 
 // atomics (zeroed by the caller).
 constexpr int COARSE_WARPS = 8;
 template <class TS>
-__device__ __forceinline__ void coarse_record(const TS* rec, float (&E)[28]);
+__device__ __forceinline__ void coarse_record(const TS* rec, float (&E)[28], typename RecWord<TS>::U& word);
 template <>
-__device__ __forceinline__ void coarse_record<float>(const float* rec, float (&E)[28]) {
+__device__ __forceinline__ void coarse_record<float>(const float* rec, float (&E)[28], uint32_t& word) {
   const float4* v = reinterpret_cast<const float4*>(rec);
 #pragma unroll
   for (int i = 0; i < 7; ++i) {
     const float4 a = __ldg(v + i);
     E[4 * i] = a.x; E[4 * i + 1] = a.y; E[4 * i + 2] = a.z; E[4 * i + 3] = a.w;
   }
+  word = __float_as_uint(E[27]);
 }
 template <>
-__device__ __forceinline__ void coarse_record<double>(const double* rec, float (&E)[28]) {
+__device__ __forceinline__ void coarse_record<double>(const double* rec, float (&E)[28], uint64_t& word) {
   const double2* v = reinterpret_cast<const double2*>(rec);
 #pragma unroll
   for (int i = 0; i < 14; ++i) {
     const double2 a = __ldg(v + i);
     E[2 * i] = (float)a.x; E[2 * i + 1] = (float)a.y;
+    if (i == 13) word = (uint64_t)__double_as_longlong(a.y);
   }
 }
 // u[a] += E_e^T W_a(cam) for one edge record (the gauge's block structure, as
@@ -852,9 +854,8 @@ __device__ __forceinline__ void coarse_record<double>(const double* rec, float (
 template <class TS>
 __device__ __forceinline__ void coarse_edge(const TS* rec, const float* wc, float (&u)[7][3]) {
   float E[28];
-  coarse_record<TS>(rec, E);
   typename RecWord<TS>::U word;
-  memcpy(&word, rec + 27, sizeof(word));
+  coarse_record<TS>(rec, E, word);
   const float4* wv = reinterpret_cast<const float4*>(wc + (int64_t)RecWord<TS>::cam(word) * 72);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -890,25 +891,79 @@ __device__ __forceinline__ void coarse_point(const TS* r, const float (&u)[7][3]
   }
 }
 
+// 16-byte asynchronous global -> shared copies (cp.async, no registers held
+// while in flight); wait_all makes the thread's own copies visible to it.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// A warp takes its tiles first, first + G, ... (G warps in the grid, sized to
+// one resident wave): lane l holds the bounds of the warp's tile 32 c + l of
+// batch c (one coalesced load per 32 tiles, read by shuffle). FP32 records:
+// the next tile's records are copied into the lane's shared-memory slot
+// (cp.async) while the current tile's sums and point terms are computed; FP64
+// records (224 bytes) are loaded when their tile is processed.
 template <class TS>
-__global__ void __launch_bounds__(COARSE_WARPS * 32)
+__global__ void __launch_bounds__(COARSE_WARPS * 32, 2)
     k_coarse_tiles(FastTiles tiles, const TS* erec, const TS* prec, const float* wc, double* out) {
   constexpr int NK = 7, NL = NK * (NK + 1) / 2;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double acc[NL];
 #pragma unroll
   for (int k = 0; k < NL; ++k) acc[k] = 0;
-  for (int64_t wt = (int64_t)blockIdx.x * COARSE_WARPS + w; wt < tiles.nwt; wt += (int64_t)gridDim.x * COARSE_WARPS) {
-    const int64_t e0 = tiles.wt_e0[wt];
-    const int cnt = (int)(tiles.wt_e0[wt + 1] - e0);
-    const int64_t p0 = tiles.wt_p0[wt];
+  const int64_t G = (int64_t)gridDim.x * COARSE_WARPS;
+  const int64_t first = (int64_t)blockIdx.x * COARSE_WARPS + w;
+  const int64_t nmine = first < tiles.nwt ? (tiles.nwt - 1 - first) / G + 1 : 0;
+  __shared__ int64_t sb_e0[COARSE_WARPS][32], sb_p0[COARSE_WARPS][32];
+  __shared__ int sb_cnt[COARSE_WARPS][32];
+  auto load_batch = [&](int64_t c) {
+    const int64_t t = first + (c * 32 + lane) * G;
+    __syncwarp();  // every lane has read the batch it replaces
+    if (t < tiles.nwt) {
+      const int64_t a = tiles.wt_e0[t];
+      sb_e0[w][lane] = a;
+      sb_cnt[w][lane] = (int)(tiles.wt_e0[t + 1] - a);
+      sb_p0[w][lane] = tiles.wt_p0[t];
+    }
+    __syncwarp();
+  };
+  constexpr bool ASYNC = sizeof(TS) == 4;
+  __shared__ __align__(16) float srec[ASYNC ? COARSE_WARPS * 32 * 28 : 4];
+  float* slot = srec + (ASYNC ? (w * 32 + lane) * 28 : 0);
+  // for a shallow FP32 tile k (warp-uniform, k < nmine), the copy of this
+  // lane's record into its slot (the batch holding tile k is loaded first)
+  auto fetch = [&](int64_t k) {
+    if (k > 0 && (k & 31) == 0) load_batch(k >> 5);
+    if constexpr (ASYNC) {
+      const int src = (int)(k & 31);
+      const int64_t e0 = sb_e0[w][src];
+      const int cnt = sb_cnt[w][src];
+      if (cnt <= 32 && lane < cnt) {
+        const float* g = reinterpret_cast<const float*>(erec + (e0 + lane) * 28);
+#pragma unroll
+        for (int q = 0; q < 7; ++q) cp_async16(slot + 4 * q, g + 4 * q);
+      }
+      cp_async_commit();
+    }
+  };
+  if (nmine) {
+    load_batch(0);
+    fetch(0);
+  }
+  for (int64_t k = 0; k < nmine; ++k) {
+    // this tile's bounds, read before fetch(k + 1) may replace the batch
+    const int64_t e0 = sb_e0[w][k & 31], p0 = sb_p0[w][k & 31];
+    const int cnt = sb_cnt[w][k & 31];
     float u[NK][3];
 #pragma unroll
     for (int a = 0; a < NK; ++a) u[a][0] = u[a][1] = u[a][2] = 0.f;
-    uint32_t lp = 0xFFFFu;
     if (cnt > 32) {
       // a point with more than 32 observations: chunks of 32 edges, one sum
       for (int c0 = lane; c0 < cnt; c0 += 32) coarse_edge<TS>(erec + (e0 + c0) * 28, wc, u);
+      if (k + 1 < nmine) fetch(k + 1);
 #pragma unroll
       for (int a = 0; a < NK; ++a)
 #pragma unroll
@@ -918,11 +973,22 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
       if (lane == 0) coarse_point(prec + p0 * 8, u, acc);
       continue;
     }
+    uint32_t lp = 0xFFFFu;
     if (lane < cnt) {
       float E[28];
-      coarse_record<TS>(erec + (e0 + lane) * 28, E);
       typename RecWord<TS>::U word;
-      memcpy(&word, erec + (e0 + lane) * 28 + 27, sizeof(word));
+      if constexpr (ASYNC) {
+        cp_async_wait_all();
+        const float4* v = reinterpret_cast<const float4*>(slot);
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+          const float4 t = v[q];
+          E[4 * q] = t.x; E[4 * q + 1] = t.y; E[4 * q + 2] = t.z; E[4 * q + 3] = t.w;
+        }
+        word = (typename RecWord<TS>::U)__float_as_uint(E[27]);
+      } else {
+        coarse_record<TS>(erec + (e0 + lane) * 28, E, word);
+      }
       lp = RecWord<TS>::lp(word);
       // W is the similarity gauge of k_bal_gauge: the rotation directions
       // (a < 3) move only the angle-axis coordinates 0..2, the translation
@@ -948,6 +1014,8 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
           for (int p = 0; p < 3; ++p) u[3 + a][p] += E[p * 9 + c] * x[a];
       }
     }
+    // this tile's records are in u: the next tile's copies go out now
+    if (k + 1 < nmine) fetch(k + 1);
     // segmented sums over each point's lanes; inactive lanes get keys of
     // their own, and the scan stops once no run is longer than the offset
     const uint32_t key = lane < cnt ? lp : 0x10000u + lane;
@@ -965,20 +1033,7 @@ __global__ void __launch_bounds__(COARSE_WARPS * 32)
         }
     }
     const uint32_t lpn = __shfl_down_sync(0xffffffffu, lp, 1);
-    if (lane < cnt && (lane == cnt - 1 || lpn != lp)) {
-      const TS* r = prec + (p0 + lp) * 8;
-      const double c00 = r[0], c10 = r[1], c20 = r[2], c11 = r[3], c21 = r[4], c22 = r[5];
-      int idx = 0;
-#pragma unroll
-      for (int a = 0; a < NK; ++a) {
-        const double t0 = c00 * u[a][0] + c10 * u[a][1] + c20 * u[a][2];
-        const double t1 = c10 * u[a][0] + c11 * u[a][1] + c21 * u[a][2];
-        const double t2 = c20 * u[a][0] + c21 * u[a][1] + c22 * u[a][2];
-#pragma unroll
-        for (int b = 0; b <= a; ++b)
-          acc[idx++] += (double)u[b][0] * t0 + (double)u[b][1] * t1 + (double)u[b][2] * t2;
-      }
-    }
+    if (lane < cnt && (lane == cnt - 1 || lpn != lp)) coarse_point(prec + (p0 + lp) * 8, u, acc);
   }
   __shared__ double sh[COARSE_WARPS][NL];
 #pragma unroll
@@ -1289,7 +1344,9 @@ struct FastPath {
     FG_LAUNCH(k_coarse_cams<TS>, std::max(1u, std::min<unsigned>(grid_for(s.nC, 4), (unsigned)grid)), 256, 0, s.st,
               (int64_t)s.nC, wd, s.d_gram.get(), s.d_observed.get(), lambda, d_wc.get(), WS, out);
     FastTiles tl{d_ebeg.get(), d_pbeg.get(), nwt, nstages};
-    const unsigned blocks = (unsigned)std::min<int64_t>((nwt + COARSE_WARPS - 1) / COARSE_WARPS, 8 * (int64_t)grid);
+    // one resident wave (two CTAs per SM); the warps walk their tiles with the
+    // next tile's loads in flight
+    const unsigned blocks = (unsigned)std::min<int64_t>((nwt + COARSE_WARPS - 1) / COARSE_WARPS, 2 * (int64_t)grid);
     FG_LAUNCH(k_coarse_tiles<TS>, std::max(blocks, 1u), COARSE_WARPS * 32, 0, s.st, tl, (const TS*)d_erec.get(),
               (const TS*)d_prec.get(), (const float*)d_wc.get(), out);
     return FG_OK;
