@@ -1115,61 +1115,75 @@ __global__ void __launch_bounds__(256) k_coarse_cams(int64_t ncam, const double*
 // Warp tiles over point-major edges, built on the device: each segment of
 // TILE_SEG points is tiled greedily (contiguous point ranges of at most 32
 // edges and 32 points, the first tile starting at the segment's first point),
-// one warp per segment. The warp fetches the point offsets 32 at a time with
-// one coalesced load and lane 0 walks them from registers (shuffles), so the
-// sequential greedy costs no memory round trip per point. Pass 0 counts each
-// segment's tiles and flags a point with more than 32 edges; after an
-// exclusive scan of the counts, pass 1 writes each tile's first edge and point
-// and, lane per point, every edge's tile-local point index.
+// one single-warp CTA per segment. The warp stages the segment's point offsets
+// in shared memory with coalesced loads; lane 0 walks them there (four points
+// per step, loads ahead of the greedy decisions) and records each point's
+// tile start, so the sequential greedy costs neither a memory round trip nor
+// a shuffle per point. Pass 0 counts each segment's tiles and flags a point
+// with more than 32 edges; after an exclusive scan of the counts, pass 1
+// writes each tile's first edge and point and, lane per point, every edge's
+// tile-local point index.
 constexpr int TILE_SEG = 1024;
-__global__ void k_fast_tiles(int pass, int64_t npt, const int64_t* pt_off, uint32_t* seg, uint32_t* total,
-                             uint32_t* too_deep, int64_t* e0, int64_t* p0, uint32_t* lp) {
-  const int64_t nseg = (npt + TILE_SEG - 1) / TILE_SEG;
-  const int lane = threadIdx.x & 31;
-  const int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  if (s >= nseg) return;
+__global__ void __launch_bounds__(32) k_fast_tiles(int pass, int64_t npt, const int64_t* pt_off, uint32_t* seg,
+                                                   uint32_t* total, uint32_t* too_deep, int64_t* e0, int64_t* p0,
+                                                   uint32_t* lp) {
+  __shared__ int64_t soff[TILE_SEG + 1];
+  __shared__ int32_t stp[TILE_SEG];
+  const int64_t s = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (s >= (npt + TILE_SEG - 1) / TILE_SEG) return;  // no points: nothing to tile
   const int64_t pa = s * TILE_SEG, pb = min(pa + TILE_SEG, npt);
-  int64_t te = pt_off[pa], tp = pa;  // lane 0's greedy state
-  uint32_t t = pass ? seg[s] : 0u, count = 1;
+  const int np = (int)(pb - pa);
   bool deep = false;
-  if (pass && lane == 0) {
-    e0[t] = te;
-    p0[t] = tp;
-  }
-  for (int64_t c0 = pa; c0 < pb; c0 += 32) {
-    const int64_t p = c0 + lane;
-    const bool live = p < pb;
-    const int64_t ea = live ? pt_off[p] : 0, eb = live ? pt_off[p + 1] : 0;
-    if (live && eb - ea > 32) deep = true;
-    const int n = (int)min((int64_t)32, pb - c0);
-    int64_t my_tp = 0;  // the tile start lane 0 assigns to this lane's point
-    for (int k = 0; k < n; ++k) {
-      const int64_t ka = __shfl_sync(0xffffffffu, ea, k), kb = __shfl_sync(0xffffffffu, eb, k);
-      if (lane == 0) {
-        const int64_t q = c0 + k;
-        if (q > tp && (kb - te > 32 || q + 1 - tp > 32)) {
-          te = ka;
-          tp = q;
-          ++count;
-          if (pass) {
-            ++t;
-            e0[t] = te;
-            p0[t] = tp;
+  for (int i = lane; i <= np; i += 32) soff[i] = pt_off[pa + i];
+  __syncwarp();
+  for (int i = lane; i < np; i += 32) deep |= soff[i + 1] - soff[i] > 32;
+  if (lane == 0) {
+    int64_t te = soff[0];
+    int tp = 0;  // segment-local first point of the current tile
+    uint32_t t = pass ? seg[s] : 0u, count = 1;
+    if (pass) {
+      e0[t] = te;
+      p0[t] = pa;
+    }
+    stp[0] = 0;
+    for (int q0 = 1; q0 < np; q0 += 4) {
+      int64_t ka[4], kb[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        ka[j] = soff[min(q0 + j, np)];
+        kb[j] = soff[min(q0 + j + 1, np)];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int q = q0 + j;
+        if (q < np) {
+          if (kb[j] - te > 32 || q + 1 - tp > 32) {
+            te = ka[j];
+            tp = q;
+            ++count;
+            if (pass) {
+              ++t;
+              e0[t] = te;
+              p0[t] = pa + q;
+            }
           }
+          stp[q] = tp;
         }
       }
-      const int64_t tpk = __shfl_sync(0xffffffffu, tp, 0);
-      if (lane == k) my_tp = tpk;
     }
-    if (pass && live)
-      for (int64_t k = ea; k < eb; ++k) lp[k] = (uint32_t)(p - my_tp);
-  }
-  if (!pass && __any_sync(0xffffffffu, deep) && lane == 0) *too_deep = 1u;
-  if (lane == 0) {
     if (!pass) seg[s] = count;
-    if (pass && s == nseg - 1) {
+    if (pass && s == (npt + TILE_SEG - 1) / TILE_SEG - 1) {
       e0[*total] = pt_off[npt];
       p0[*total] = npt;
+    }
+  }
+  if (!pass && __any_sync(0xffffffffu, deep) && lane == 0) *too_deep = 1u;
+  if (pass) {
+    __syncwarp();
+    for (int q = lane; q < np; q += 32) {
+      const uint32_t v = (uint32_t)(q - stp[q]);
+      for (int64_t k = soff[q]; k < soff[q + 1]; ++k) lp[k] = v;
     }
   }
 }
@@ -1224,10 +1238,10 @@ struct FastPath {
     uint32_t* aux = d_tile_aux.get();
     FG_CUDA(cudaMemsetAsync(aux, 0, ((size_t)nseg + 2) * sizeof(uint32_t), st));
     const int64_t* off = s.d_pt_edge_off.get();
-    FG_LAUNCH(k_fast_tiles, grid_for(nseg * 32, 128), 128, 0, st, 0, nP, off, aux, aux + nseg, aux + nseg + 1,
+    FG_LAUNCH(k_fast_tiles, (unsigned)std::max<int64_t>(nseg, 1), 32, 0, st, 0, nP, off, aux, aux + nseg, aux + nseg + 1,
               d_ebeg.get(), d_pbeg.get(), d_lp.get());
     FG_LAUNCH(k_scan_exclusive_u32, 1, 1024, 0, st, aux, nseg, aux + nseg);
-    FG_LAUNCH(k_fast_tiles, grid_for(nseg * 32, 128), 128, 0, st, 1, nP, off, aux, aux + nseg, aux + nseg + 1,
+    FG_LAUNCH(k_fast_tiles, (unsigned)std::max<int64_t>(nseg, 1), 32, 0, st, 1, nP, off, aux, aux + nseg, aux + nseg + 1,
               d_ebeg.get(), d_pbeg.get(), d_lp.get());
     FG_CUDA(cudaMemcpyAsync(h_tile_aux.get(), aux + nseg, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
