@@ -69,3 +69,31 @@ def test_coarse_correction_without_a_basis_is_one_level():
     b.prepare_damping(0.1)
     b.solve_damped(0.01)
     assert b.diagnostics().coarse_vectors == 0
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_single_launch_and_polled_pcg_take_the_same_steps(precision, monkeypatch):
+    """A damped solve runs its CG loop as one conditional-graph launch (the
+    device decides when to stop); FAGRA_B200_POLLED_PCG at backend creation
+    selects the fallback, graphs of 8 iterations polled from the host. Both
+    run the same kernels in the same order: the same iterations and the same
+    step (FP64 atomic sums may reorder the last bits, which the FP32
+    recurrences carry further: 1e-9 / 1e-7 relative, far inside the CG
+    tolerance), with different launch counts showing that the two paths ran."""
+    d = synthetic.generate("bal1k", cameras=100, points=15000, seed=9)
+    one = _backend(d, precision=precision, coarse_correction=True)
+    monkeypatch.setenv("FAGRA_B200_POLLED_PCG", "1")
+    two = _backend(d, precision=precision, coarse_correction=True)
+    monkeypatch.delenv("FAGRA_B200_POLLED_PCG")
+    for lam in (1e-4, 1e-2, 1.0):
+        l0 = fg.kernel_launches()
+        a = one.solve_damped(lam)
+        l1 = fg.kernel_launches()
+        b = two.solve_damped(lam)
+        l2 = fg.kernel_launches()
+        da, db = one.diagnostics(), two.diagnostics()
+        assert da.termination == db.termination == "Converged"
+        assert abs(da.iterations - db.iterations) <= 1, lam
+        tol = 1e-9 if precision == "f64" else 1e-7
+        assert np.linalg.norm(b.delta - a.delta) <= tol * np.linalg.norm(a.delta), lam
+        assert l1 - l0 != l2 - l1, lam
