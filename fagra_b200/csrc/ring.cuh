@@ -165,10 +165,6 @@ __global__ void __launch_bounds__(NW * 32, 1)
   constexpr bool FIXED = SM::FIXED;
   constexpr bool NEED_X = MODE != FAST_RHS;
   constexpr bool SCATTER = MODE != FAST_RECOVER;
-  pdl_wait();
-  pdl_trigger();
-  if (skip && *skip) return;
-  if (gate && !*gate) return;
   extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   constexpr int NTHR = NW * 32;
@@ -183,23 +179,34 @@ __global__ void __launch_bounds__(NW * 32, 1)
   unsigned char* ring = smem + acc + xsb + (((size_t)NW * R * 8 + 127) & ~(size_t)127) + (size_t)w * R * RING_SLOT_BYTES;
   uint64_t* wbar = bars + w * R;
 
+  // this CTA's own shared memory (the accumulator and the slot barriers) is
+  // set up before the dependency wait, overlapping the previous kernel's tail;
+  // every global access comes after it
+  if (ACC == RACC_SHARED && SCATTER) {
+    for (int64_t i = tid; i < ny; i += NTHR) {
+      if (FIXED) {
+        ylo[i] = 0;
+        yhi[i] = 0;
+      } else {
+        yds[i] = 0;
+      }
+    }
+  }
+  if (lane == 0) {
+    for (int b = 0; b < R; ++b) mbar_init(&wbar[b], 1);
+    mbar_fence_init();
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (skip && *skip) return;
+  if (gate && !*gate) return;
   const TV bv = pv ? (TV)*beta : (TV)0;
   double xmax = 0.0;
-  if (ACC == RACC_SHARED || XS || FIXED) {
+  if (NEED_X && (XS || FIXED)) {
     for (int64_t i = tid; i < ny; i += NTHR) {
-      if (ACC == RACC_SHARED && SCATTER) {
-        if (FIXED) {
-          ylo[i] = 0;
-          yhi[i] = 0;
-        } else {
-          yds[i] = 0;
-        }
-      }
-      if (NEED_X && (XS || FIXED)) {
-        const TV xi = pv ? z[i] + bv * pv[i] : z[i];
-        if (XS) xs[i] = xi;
-        if (FIXED) xmax = isfinite((double)xi) ? fmax(xmax, fabs((double)xi)) : (double)INFINITY;
-      }
+      const TV xi = pv ? z[i] + bv * pv[i] : z[i];
+      if (XS) xs[i] = xi;
+      if (FIXED) xmax = isfinite((double)xi) ? fmax(xmax, fabs((double)xi)) : (double)INFINITY;
     }
   }
   __shared__ double wmax[32];
@@ -208,10 +215,6 @@ __global__ void __launch_bounds__(NW * 32, 1)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
     if (lane == 0) wmax[w] = xmax;
-  }
-  if (lane == 0) {
-    for (int b = 0; b < R; ++b) mbar_init(&wbar[b], 1);
-    mbar_fence_init();
   }
   __syncthreads();
   if (FIXED && tid == 0) {
