@@ -18,6 +18,7 @@
 #include "lsmr_kernels.cuh"
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 
 namespace fg {
 
@@ -27,6 +28,18 @@ enum { MODE_NONE = -1, MODE_IDENTITY = 0, MODE_DIAGONAL = 1, MODE_BLOCK = 2 };
 // diagonal, block-Jacobi.
 enum { GRAPH_UNDAMPED = 0, GRAPH_IDENTITY = 1, GRAPH_DIAGONAL = 2, GRAPH_BLOCK = 3 };
 constexpr int LSMR_GRAPH_ITERS = 8;
+constexpr int LSMR_COND_ITERS = 2;  // iterations per trip of the single-launch graph
+
+// The loop condition of the single-launch LSMR graph (a WHILE node whose body
+// is LSMR_COND_ITERS iterations): continue until the device's stopping rules
+// set stop, and for fewer trips than the polled loop's bound allows
+// (max_iterations + 2 x 8 launched iterations), so the loop always ends.
+__global__ void k_lsmr_continue(cudaGraphConditionalHandle h, LsmrState* st) {
+  const unsigned trips = ++st->trips;
+  const unsigned long long limit =
+      ((unsigned long long)st->max_iterations + 2 * LSMR_GRAPH_ITERS + LSMR_COND_ITERS - 1) / LSMR_COND_ITERS;
+  cudaGraphSetConditional(h, !st->stop && trips < limit ? 1u : 0u);
+}
 
 int width_class(int64_t w) { return w <= 4 ? 4 : w <= 8 ? 8 : w <= 16 ? 16 : 32; }
 }  // namespace
@@ -60,6 +73,10 @@ class LsmrImpl final : public Backend {
   fg_status init() {
     FG_TRY(select_device(dev));
     FG_TRY(device_stream(dev, &st));
+    // FAGRA_B200_POLLED_GRAPHS set when the backend is created: the polled
+    // graphs instead of the single-launch conditional graph (the fallback
+    // path, selectable so that it stays tested)
+    cond_failed = std::getenv("FAGRA_B200_POLLED_GRAPHS") != nullptr;
     FG_TRY(d_state.resize(1));
     FG_TRY(h_state.resize(1));
     FG_TRY(d_ver.resize(1));
@@ -532,6 +549,13 @@ class LsmrImpl final : public Backend {
 
   cudaGraphExec_t g_exec[4] = {nullptr, nullptr, nullptr, nullptr};
   uint64_t g_nodes[4] = {0, 0, 0, 0};
+  // A solve as one graph launch: a WHILE node over LSMR_COND_ITERS iterations
+  // and k_lsmr_continue (no host poll between batches, no gated iterations
+  // past the stop beyond the last trip); the polled graphs above are the
+  // fallback if the driver refuses the conditional graph.
+  cudaGraphExec_t c_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t c_nodes[4] = {0, 0, 0, 0};
+  bool cond_failed = false;
 
   int requested_mode() const {  // src/lsmr.rs:391-399
     return opt.block_preconditioning ? MODE_BLOCK : opt.diagonal_preconditioning ? MODE_DIAGONAL : MODE_IDENTITY;
@@ -541,6 +565,8 @@ class LsmrImpl final : public Backend {
     for (int k = 0; k < 4; ++k) {
       if (g_exec[k]) cudaGraphExecDestroy(g_exec[k]);
       g_exec[k] = nullptr;
+      if (c_exec[k]) cudaGraphExecDestroy(c_exec[k]);
+      c_exec[k] = nullptr;
     }
   }
 
@@ -968,6 +994,51 @@ class LsmrImpl final : public Backend {
     return FG_OK;
   }
 
+  fg_status launch_continue(cudaGraphConditionalHandle h) {
+    FG_LAUNCH(k_lsmr_continue, 1, 1, 0, st, h, d_state.get());
+    return FG_OK;
+  }
+  fg_status capture_cond_graph(int gmode, cudaGraph_t* out) {
+    FG_CUDA(cudaGraphCreate(out, 0));
+    cudaGraphConditionalHandle h;
+    FG_CUDA(cudaGraphConditionalHandleCreate(&h, *out, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    FG_CUDA(cudaGraphAddNode(&node, *out, nullptr, 0, &np));
+    const uint64_t before = g_launches.load();
+    FG_CUDA(cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+    fg_status s = FG_OK;
+    for (int k = 0; k < LSMR_COND_ITERS && s == FG_OK; ++k) s = iteration_body(gmode, nullptr, nullptr, nullptr);
+    if (s == FG_OK) s = launch_continue(h);
+    cudaGraph_t body = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &body);
+    c_nodes[gmode] = g_launches.load() - before;
+    g_launches.fetch_sub(c_nodes[gmode]);  // captured, not launched
+    FG_TRY(s);
+    FG_CUDA(e);
+    return FG_OK;
+  }
+  fg_status launch_cond_graph(int gmode) {
+    if (!c_exec[gmode]) {
+      cudaGraph_t graph = nullptr;
+      fg_status s = capture_cond_graph(gmode, &graph);
+      cudaError_t e = s == FG_OK ? cudaGraphInstantiate(&c_exec[gmode], graph, 0) : cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+      if (s != FG_OK || e != cudaSuccess) {
+        c_exec[gmode] = nullptr;
+        cudaGetLastError();
+        return s != FG_OK ? s : cuda_status(e, "cudaGraphInstantiate (conditional)");
+      }
+    }
+    FG_CUDA(cudaGraphLaunch(c_exec[gmode], st));
+    return FG_OK;
+  }
+
   fg_status read_state() {
     FG_CUDA(cudaMemcpyAsync(h_state.get(), d_state.get(), sizeof(LsmrState), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
@@ -987,7 +1058,17 @@ class LsmrImpl final : public Backend {
     FG_TRY(read_state());
     size_t launched = 0, batch = 1;
     EventTimer tf, tt, tp;
-    while (!h_state.get()->stop) {
+    bool whole = false;  // the single-launch graph ran the solve
+    if (!h_state.get()->stop && !opt.collect_timings && !cond_failed) {
+      if (launch_cond_graph(gmode) == FG_OK) {
+        FG_TRY(read_state());
+        g_launches.fetch_add((uint64_t)h_state.get()->trips * c_nodes[gmode]);
+        whole = true;
+      } else {
+        cond_failed = true;
+      }
+    }
+    while (!whole && !h_state.get()->stop) {
       if (launched > (size_t)max_its + 2 * LSMR_GRAPH_ITERS) break;  // the device enforces the limit
       if (opt.collect_timings) {
         FG_TRY(iteration_body(gmode, &tf, &tt, &tp));

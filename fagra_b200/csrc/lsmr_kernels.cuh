@@ -38,6 +38,7 @@ struct LsmrState {
   int stop, upd, termination, nonfinite_scales;
   unsigned iterations, max_iterations;
   unsigned counter0, counter1, counter2, counter3;
+  unsigned trips;  // loop trips of the single-launch solve graph (k_lsmr_continue)
 };
 
 struct LsmrVerify {

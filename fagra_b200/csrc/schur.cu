@@ -184,10 +184,10 @@ class SchurImpl final : public Backend {
     FG_TRY(select_device(dev));
     FG_TRY(device_stream(dev, &st));
     nsm = sm_count(dev);
-    // FAGRA_B200_POLLED_PCG set when the backend is created: the polled
+    // FAGRA_B200_POLLED_GRAPHS set when the backend is created: the polled
     // 8-iteration graphs instead of the single-launch conditional graph (the
     // fallback path, selectable so that it stays tested)
-    cond_failed = std::getenv("FAGRA_B200_POLLED_PCG") != nullptr;
+    cond_failed = std::getenv("FAGRA_B200_POLLED_GRAPHS") != nullptr;
     FG_TRY(d_pcg.resize(1));
     FG_TRY(d_ver.resize(1));
     FG_TRY(h_pcg.resize(1));

@@ -74,7 +74,7 @@ def test_coarse_correction_without_a_basis_is_one_level():
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_single_launch_and_polled_pcg_take_the_same_steps(precision, monkeypatch):
     """A damped solve runs its CG loop as one conditional-graph launch (the
-    device decides when to stop); FAGRA_B200_POLLED_PCG at backend creation
+    device decides when to stop); FAGRA_B200_POLLED_GRAPHS at backend creation
     selects the fallback, graphs of 8 iterations polled from the host. Both
     run the same kernels in the same order: the same iterations and the same
     step (FP64 atomic sums may reorder the last bits, which the FP32
@@ -82,9 +82,9 @@ def test_single_launch_and_polled_pcg_take_the_same_steps(precision, monkeypatch
     tolerance), with different launch counts showing that the two paths ran."""
     d = synthetic.generate("bal1k", cameras=100, points=15000, seed=9)
     one = _backend(d, precision=precision, coarse_correction=True)
-    monkeypatch.setenv("FAGRA_B200_POLLED_PCG", "1")
+    monkeypatch.setenv("FAGRA_B200_POLLED_GRAPHS", "1")
     two = _backend(d, precision=precision, coarse_correction=True)
-    monkeypatch.delenv("FAGRA_B200_POLLED_PCG")
+    monkeypatch.delenv("FAGRA_B200_POLLED_GRAPHS")
     for lam in (1e-4, 1e-2, 1.0):
         l0 = fg.kernel_launches()
         a = one.solve_damped(lam)

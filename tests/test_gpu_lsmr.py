@@ -317,3 +317,39 @@ def test_bal16_lm_with_lsmr_reaches_the_oracle_cost():
     np.testing.assert_allclose(costs[:n], gold[:n], rtol=1e-6)
     assert abs(out.statistics.cost - ost.cost) <= 1e-6 * ost.cost
     assert out.work.linear_solve.iterations > 0
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_single_launch_and_polled_lsmr_take_the_same_steps(precision, monkeypatch):
+    """An LSMR solve runs as one conditional-graph launch (the device decides
+    when to stop); FAGRA_B200_POLLED_GRAPHS at backend creation selects the
+    fallback, graphs of 8 iterations polled from the host in doubling
+    batches. Same kernels in the same order: the same iterations and the same
+    step, with different launch counts showing that the two paths ran."""
+    d = synthetic.generate("bal1k", cameras=60, points=6000, seed=5)
+
+    def backend():
+        problem = fg.BalProblem.from_data(d)
+        b = fg.Lsmr(precision=precision)
+        b.block_preconditioning = True
+        b.prepare(problem.dimension())
+        problem.linearize(b)
+        b.prepare_damping(1e-6)
+        return b
+
+    one = backend()
+    monkeypatch.setenv("FAGRA_B200_POLLED_GRAPHS", "1")
+    two = backend()
+    monkeypatch.delenv("FAGRA_B200_POLLED_GRAPHS")
+    for lam in (1e-4, 1e-2):
+        l0 = fg.kernel_launches()
+        a = one.solve_damped(lam)
+        l1 = fg.kernel_launches()
+        b = two.solve_damped(lam)
+        l2 = fg.kernel_launches()
+        da, db = one.diagnostics(), two.diagnostics()
+        assert da.termination == db.termination == "Converged"
+        assert da.iterations == db.iterations, lam
+        tol = 1e-9 if precision == "f64" else 1e-6
+        assert np.linalg.norm(b.delta - a.delta) <= tol * np.linalg.norm(a.delta), lam
+        assert l1 - l0 != l2 - l1, lam
