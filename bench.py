@@ -82,6 +82,17 @@ def target_counts(g: dict) -> tuple[int, int, float]:
     return g["linearizations"], g["cg_iterations"], g.get("seconds", 0.0)
 
 
+def max_over_ranks(values: list, device: str) -> list:
+    """Each value's maximum over the ranks of the default process group: the
+    whole job's time per step is its slowest replica's (every rank calls this
+    with the same number of values)."""
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -768,12 +779,10 @@ def main():
     import torch
     vals = {k: v["seconds"] for k, v in results.items()}
     if world > 1:
-        import torch.distributed as tdist
-        t = torch.tensor([vals[head]] + ([e2e["value"]] if e2e else []), device=f"cuda:{local}", dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        vals[head] = float(t[0])
+        t = max_over_ranks([vals[head]] + ([e2e["value"]] if e2e else []), f"cuda:{local}")
+        vals[head] = t[0]
         if e2e:
-            e2e["value"] = float(t[1])
+            e2e["value"] = t[1]
     if rank == 0:
         pk, src = peaks()
         op = results[head].get("operator", {})
