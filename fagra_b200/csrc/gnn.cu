@@ -676,7 +676,8 @@ __global__ void k_normalize(int64_t nC, int64_t lda, unsigned long long* adj, co
 // G_e = L_c^-1 V_e (so K_e = G_e^T G_e); unobserved variables use
 // L = sqrt(lambda) I as above.
 
-// The point-sorted position of every edge: pos[pt_edge[k]] = k.
+// The point-sorted position of every edge: pos[pt_edge[k]] = k (for a view
+// without the backend's camera-major (position, point) array).
 __global__ void k_gnn_pos(int64_t nedges, const int64_t* pt_edge, int32_t* pos) {
   const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k < nedges) pos[pt_edge[k]] = (int32_t)k;
@@ -1224,7 +1225,7 @@ class Gnn {
   DBuf<float> Z[NLAYER + 1], HA[NLAYER], H3, O, dO, dHa, dHb, dA, dZ, edgeK;
   DBuf<unsigned long long> adj;  // fixed-point covisibility, C x C, left cleared by k_normalize
   int64_t adj_cap = -1;          // entries of adj known to be zero
-  DBuf<int32_t> edgePos;         // point-sorted position of every edge
+  DBuf<int32_t> edgePos;         // point-sorted position of every edge (views without cam_meta)
   DBuf<double> dloss;
   DBuf<unsigned> dcount;
   DBuf<int> gemm_err;  // set by a GEMM whose tensor-core wait ran out
